@@ -1,0 +1,147 @@
+"""Generate the golden fixtures: outputs of the reference CLI on seeded inputs.
+
+Run in a container where the reference tree is present and the reference
+CLI has been compiled from its own sources (``make -C oracle``):
+
+    python tests/golden/make_golden.py
+
+For every case in CASES this script
+
+1. draws the inputs with ``omicabelnomm_b200.synth`` (seeded, so the test
+   suite regenerates them byte for byte; the manifest keeps their sha256),
+2. runs ``oracle/_ref/omicabelnomm_ref`` with the case's flags,
+3. stores the reference's ``_dis.txt`` (gzip) and, with ``-b``, its
+   ``_sto.ibin`` / ``_sto.dbin`` plus the printed "Number of Significant
+   Results" in ``tests/golden/<case>/``.
+
+The inputs themselves are not committed; only these outputs are.
+"""
+from __future__ import annotations
+
+import gzip
+import hashlib
+import json
+import os
+import shutil
+import subprocess
+import sys
+import tempfile
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, ROOT)
+
+from omicabelnomm_b200 import synth  # noqa: E402
+
+REF_BIN = os.path.join(ROOT, "oracle", "_ref", "omicabelnomm_ref")
+
+# name -> (workload overrides on config 0, post-processing, [flag sets])
+CASES = {
+    # plain r = 1, 5 % uniform NaN per trait
+    "r1_uniform": (dict(n=400, m=120, t=12, seed=11), None,
+                   [["-f"], [], ["-i"], ["-f", "-i"], ["-b"], ["-b", "-i"], ["-b", "-f"]]),
+    # shared missingness patterns, two SNP blocks (m > 500)
+    "r1_patterns": (dict(n=300, m=620, t=6, l=4, miss_mode="patterns", n_patterns=3,
+                         miss_hi=0.1, seed=12), None, [["-f"], [], ["-b"]]),
+    # two trait blocks (t > 1000)
+    "r1_tblocks": (dict(n=60, m=3, t=1010, seed=13), None, [[], ["-b"]]),
+    # covariate NaNs and an exclusion list drop individuals
+    "r1_exclude": (dict(n=300, m=80, t=8, xl_nan_rows=7, seed=14), "exclude",
+                   [["-f", "-x", "{excl}"], ["-x", "{excl}", "-b"]]),
+    # NaN dosages are mean-imputed
+    "r1_xrnan": (dict(n=300, m=80, t=8, xr_nan_frac=0.02, seed=15), None, [["-f"]]),
+    # observed phenotypes that are exactly 0 are skipped by the RSS loop
+    "r1_yzero": (dict(n=300, m=80, t=8, seed=16), "yzero", [["-f"]]),
+    # strong planted effects: trait j with SNP j (known-answer structure)
+    "r1_strong": (dict(n=500, m=40, t=20, effect=1.0, seed=17), None, [[], ["-b"]]),
+    # r = 2 (SNP x sex, SNP) without phenotype missingness
+    "r2_complete": (dict(n=400, m=60, t=6, l=4, r=2, miss_mode="none", seed=18), None,
+                    [["-n", "2", "-f"], ["-n", "2", "-i"], ["-n", "2", "-b"]]),
+    # r = 2 with missingness (the reference's downdate bug applies)
+    "r2_missing": (dict(n=400, m=60, t=6, l=4, r=2, seed=19), None, [["-n", "2", "-f"]]),
+}
+
+EXCLUDE_LIST = "1 2\n5\n7\n9 11\n13\n40 44\n"
+
+
+def build_inputs(case: str, where: str):
+    over, post, _ = CASES[case]
+    w = synth.scaled(0, **over)
+    ds = synth.generate(w)
+    if post == "yzero":
+        # set a few observed entries of every trait to exactly zero
+        import numpy as np
+        rng = np.random.Generator(np.random.PCG64(w.seed + 99))
+        for j in range(ds.Y.shape[0]):
+            obs = np.nonzero(~np.isnan(ds.Y[j]))[0]
+            ds.Y[j, rng.choice(obs, 5, replace=False)] = 0.0
+    pre = os.path.join(where, case + "_")
+    synth.write_dataset(ds, pre)
+    extra = {}
+    if post == "exclude":
+        p = os.path.join(where, case + "_excl.txt")
+        with open(p, "w") as f:
+            f.write(EXCLUDE_LIST)
+        extra["excl"] = p
+    return pre, extra
+
+
+def sha256(path: str) -> str:
+    h = hashlib.sha256()
+    with open(path, "rb") as f:
+        for blk in iter(lambda: f.read(1 << 20), b""):
+            h.update(blk)
+    return h.hexdigest()
+
+
+def input_digests(pre: str) -> dict:
+    return {k: sha256(pre + k + ".fvd") for k in ("XL", "XR", "Y")} | \
+           {k + ".fvi": sha256(pre + k + ".fvi") for k in ("XL", "XR", "Y")}
+
+
+def flag_tag(flags) -> str:
+    t = "".join(f.strip("-") for f in flags if not f.startswith("{") and not f.isdigit()
+                and f != "{excl}")
+    return t or "default"
+
+
+def main():
+    if not os.path.exists(REF_BIN):
+        sys.exit("build the reference first: make -C oracle")
+    manifest = {}
+    tmp = tempfile.mkdtemp(prefix="oa_golden_")
+    try:
+        for case, (over, post, flagsets) in CASES.items():
+            pre, extra = build_inputs(case, tmp)
+            cdir = os.path.join(HERE, case)
+            os.makedirs(cdir, exist_ok=True)
+            entry = {"workload": over, "post": post, "inputs": input_digests(pre), "runs": {}}
+            for flags in flagsets:
+                tag = flag_tag(flags)
+                args = [f.format(**extra) for f in flags]
+                out = os.path.join(tmp, f"{case}_{tag}")
+                cmd = [REF_BIN, "-c", pre + "XL", "-g", pre + "XR", "-p", pre + "Y", "-o", out] + args
+                p = subprocess.run(cmd, capture_output=True, text=True, timeout=600)
+                if p.returncode != 0:
+                    raise RuntimeError(f"{case} {flags}: exit {p.returncode}\n{p.stdout[-2000:]}")
+                sig = int(p.stdout.split("Number of Significant Results:")[1].split()[0])
+                with open(out + "_dis.txt", "rb") as f, \
+                        open(os.path.join(cdir, f"{tag}_dis.txt.gz"), "wb") as raw, \
+                        gzip.GzipFile(fileobj=raw, mode="wb", mtime=0, filename="") as g:
+                    shutil.copyfileobj(f, g)
+                files = ["dis.txt.gz"]
+                if "-b" in flags:
+                    for ext in ("ibin", "dbin"):
+                        shutil.copy(out + f"_sto.{ext}", os.path.join(cdir, f"{tag}_sto.{ext}"))
+                        files.append(f"sto.{ext}")
+                entry["runs"][tag] = {"flags": flags, "significant": sig, "files": files}
+                print(f"{case:12s} {tag:10s} significant={sig}")
+            manifest[case] = entry
+        with open(os.path.join(HERE, "manifest.json"), "w") as f:
+            json.dump({"exclude_list": EXCLUDE_LIST, "cases": manifest}, f, indent=1, sort_keys=True)
+    finally:
+        shutil.rmtree(tmp, ignore_errors=True)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,192 @@
+"""Helpers shared by the parity tests: regenerate golden inputs and compare result sets.
+
+The golden fixtures are outputs of the reference CLI (see
+tests/golden/make_golden.py).  Their inputs are regenerated here from the
+same seeds and checked against the sha256 digests in the manifest, so the
+comparison runs on exactly the bytes the reference read.
+"""
+from __future__ import annotations
+
+import gzip
+import json
+import math
+import os
+import tempfile
+from dataclasses import dataclass
+
+import numpy as np
+
+import oa_oracle as O
+from golden import make_golden as MG
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+GOLDEN = os.path.join(HERE, "golden")
+
+
+def manifest():
+    with open(os.path.join(GOLDEN, "manifest.json")) as f:
+        return json.load(f)
+
+
+def all_runs():
+    man = manifest()
+    out = []
+    for case, entry in sorted(man["cases"].items()):
+        for tag, run in sorted(entry["runs"].items()):
+            out.append((case, tag))
+    return out
+
+
+def materialise(case: str, where: str):
+    """Write the case's inputs under ``where`` and verify their digests."""
+    pre, extra = MG.build_inputs(case, where)
+    want = manifest()["cases"][case]["inputs"]
+    got = MG.input_digests(pre)
+    if got != want:
+        raise AssertionError(f"{case}: regenerated inputs differ from the golden digests")
+    return pre, extra
+
+
+def settings_for(flags, extra) -> O.Settings:
+    s = O.Settings()
+    it = iter(flags)
+    for f in it:
+        if f == "-f":
+            s.storePInd = True
+        elif f == "-i":
+            s.disp_cov = True
+        elif f == "-b":
+            s.storeBin = True
+        elif f == "-n":
+            s.r = int(next(it))
+        elif f == "-x":
+            s.fname_excludelist = next(it).format(**extra)
+        else:
+            raise ValueError(f)
+    return s
+
+
+def golden_rows(case: str, tag: str):
+    path = os.path.join(GOLDEN, case, f"{tag}_dis.txt.gz")
+    with gzip.open(path, "rt") as f:
+        tmp = tempfile.NamedTemporaryFile("w", suffix="_dis.txt", delete=False)
+        tmp.write(f.read())
+        tmp.close()
+    try:
+        return O.parse_dis(tmp.name)
+    finally:
+        os.unlink(tmp.name)
+
+
+def t_display(minPdisp: float) -> float:
+    """|t| at which P(t) = minPdisp on the erfc branch (t >= 1.6)."""
+    return math.sqrt(2.0) * _erfcinv(minPdisp)
+
+
+def _erfcinv(p: float) -> float:
+    lo, hi = 0.0, 40.0
+    for _ in range(200):
+        mid = 0.5 * (lo + hi)
+        if math.erfc(mid) > p:
+            lo = mid
+        else:
+            hi = mid
+    return 0.5 * (lo + hi)
+
+
+@dataclass
+class Tol:
+    t_rel: float
+    t_abs: float
+    se_rel: float
+    r2_abs: float
+
+
+# the reference's FP32 answers scatter this much around FP64 (measured on the
+# golden cases: |dt| <= 1.2e-3 |t| + 7e-3); parity vs the reference uses it
+REF_TOL = Tol(t_rel=2e-3, t_abs=1e-2, se_rel=2e-4, r2_abs=2e-4)
+
+
+def compare_rows(ref_rows, our_rows, tol: Tol, near_boundary):
+    """Compare two lists of _dis rows keyed by (Phe, SNP).
+
+    ``near_boundary(phe, snp)`` says whether a row present on one side
+    only sits within tolerance of a store/display threshold.  Returns a
+    dict of diagnostics; raises AssertionError on a real mismatch.
+    """
+    rk = {(r["Phe"], r["SNP"]): r for r in ref_rows}
+    ok = {(r["Phe"], r["SNP"]): r for r in our_rows}
+    if len(rk) != len(ref_rows) or len(ok) != len(our_rows):
+        raise AssertionError("duplicate (Phe, SNP) rows")
+    only_ref = [k for k in rk if k not in ok]
+    only_our = [k for k in ok if k not in rk]
+    bad = [k for k in only_ref + only_our if not near_boundary(*k)]
+    if bad:
+        raise AssertionError(f"{len(bad)} rows differ away from thresholds, e.g. {bad[:5]}")
+    worst = dict(t=0.0, se=0.0, r2=0.0)
+    for k in rk.keys() & ok.keys():
+        a, b = rk[k], ok[k]
+        if a["n"] != b["n"] or a["nPct"] != b["nPct"]:
+            raise AssertionError(f"{k}: n/nPct {a['n']},{a['nPct']} vs {b['n']},{b['nPct']}")
+        dt = abs(a["T"] - b["T"])
+        lim = tol.t_rel * abs(a["T"]) + tol.t_abs
+        worst["t"] = max(worst["t"], dt / lim)
+        if dt > lim:
+            raise AssertionError(f"{k}: T {a['T']} vs {b['T']}")
+        dse = abs(a["SE"] - b["SE"]) / max(abs(a["SE"]), 1e-30)
+        worst["se"] = max(worst["se"], dse / tol.se_rel)
+        if dse > tol.se_rel and abs(a["SE"] - b["SE"]) > 1.5e-7:
+            raise AssertionError(f"{k}: SE {a['SE']} vs {b['SE']}")
+        # B agrees to the same number of standard errors as T
+        if abs(a["B"] - b["B"]) > lim * max(a["SE"], b["SE"]) + 1.5e-7:
+            raise AssertionError(f"{k}: B {a['B']} vs {b['B']}")
+        if abs(a["R2"] - b["R2"]) > tol.r2_abs * max(1.0, abs(a["R2"])):
+            raise AssertionError(f"{k}: R2 {a['R2']} vs {b['R2']}")
+    # order of the common rows must agree
+    order_r = [k for k in (tuple((r["Phe"], r["SNP"])) for r in ref_rows) if k in ok]
+    order_o = [k for k in (tuple((r["Phe"], r["SNP"])) for r in our_rows) if k in rk]
+    if order_r != order_o:
+        raise AssertionError("row order differs")
+    return dict(common=len(rk.keys() & ok.keys()), only_ref=len(only_ref), only_our=len(only_our), worst=worst)
+
+
+def oracle_rows(res: O.Results, inp: O.Inputs, s: O.Settings):
+    """The _dis rows the oracle's results print as (numeric fields as float)."""
+    disp = O.displayed(res, s)
+    names = O.result_names(res, inp, res.l, res.r)
+    rows = []
+    for i in np.nonzero(disp)[0]:
+        rows.append(dict(Phe=names[i][0], SNP=names[i][1], n=int(res.nUsed[i]),
+                         nPct=f"{float(res.nUsedPct[i]):.2f}", B=float(res.B[i]),
+                         R2=float(np.float32(res.R2[i])), SE=float(res.SE[i]), T=float(res.T[i]),
+                         P=None))
+    return rows
+
+
+def boundary_fn(res_dense: O.Results, inp: O.Inputs, s: O.Settings, tol: Tol):
+    """near_boundary(phe, snp) from the oracle's dense t of that test's SNP terms."""
+    minR2store, minPstore, minT = O.thresholds(s)
+    td = t_display(float(np.float32(s.minPdisp)))
+    tp = 1.2834  # the 0.5-0.1(4.4-t)t branch reaches P = 0.1 here; displays can flip near it
+    yidx = {name: j for j, name in enumerate(inp.y_names)}
+    l, r = res_dense.l, res_dense.r
+    names = {}
+    for i in range(len(inp.xr_names) // r):
+        for h in range(r):
+            names[" " + inp.xr_names[i * r + h]] = i
+        for a in inp.xl_names:
+            names[a + ":" + inp.xr_names[i * r]] = i
+    D = res_dense.dense
+
+    def near(phe, snp):
+        j, i = yidx[phe], names[snp]
+        for h in range(l, l + r):
+            t = D.tstat[j, i, h]
+            lim = 2 * (tol.t_rel * abs(t) + tol.t_abs)
+            if min(abs(t - float(minT)), abs(t - td), abs(t - 1.6), abs(t - tp)) <= lim:
+                return True
+        if abs(D.r2[j, i] - float(minR2store)) <= 2 * tol.r2_abs:
+            return True
+        return False
+
+    return near

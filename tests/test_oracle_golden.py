@@ -1,0 +1,73 @@
+"""The FP64 oracle against the reference's own outputs (golden fixtures).
+
+These pin the oracle: the reference CLI, compiled from its sources, wrote
+tests/golden/*; the oracle must reproduce every row within the reference's
+FP32 noise, with identical n, nPct, names and order, and differ only on
+rows within tolerance of a threshold.
+"""
+import math
+
+import numpy as np
+import pytest
+
+import golden_util as GU
+import oa_oracle as O
+
+
+@pytest.mark.parametrize("case,tag", GU.all_runs())
+def test_oracle_matches_reference(case, tag, tmp_path):
+    pre, extra = GU.materialise(case, str(tmp_path))
+    run = GU.manifest()["cases"][case]["runs"][tag]
+    s = GU.settings_for(run["flags"], extra)
+    if case == "r2_missing":
+        s.quirk_r2 = True        # the reference's r >= 2 downdate
+    res, inp = O.run_files(pre + "XL", pre + "XR", pre + "Y", s, keep_dense=True)
+    ref = GU.golden_rows(case, tag)
+    ours = GU.oracle_rows(res, inp, s)
+    near = GU.boundary_fn(res, inp, s, GU.REF_TOL)
+    info = GU.compare_rows(ref, ours, GU.REF_TOL, near)
+    assert info["common"] >= 0.95 * len(ref)
+    # the printed significant count differs only by boundary results
+    assert abs(res.total_sig - run["significant"]) <= max(2, 0.01 * run["significant"])
+
+
+def test_known_answer_structure(tmp_path):
+    """Trait j is driven by SNP j with effect 1 (like the reference's example data)."""
+    pre, extra = GU.materialise("r1_strong", str(tmp_path))
+    s = O.Settings()
+    res, inp = O.run_files(pre + "XL", pre + "XR", pre + "Y", s, keep_dense=True)
+    D = res.dense
+    t = D.tstat[:, :, res.l]
+    for j in range(t.shape[0]):
+        assert np.argmax(t[j]) == j % t.shape[1]
+        assert t[j, j % t.shape[1]] > 8
+    # the reference's test asserts at least one significant result per trait
+    assert res.total_sig >= t.shape[0]
+
+
+def test_thresholds_match_reference_defaults():
+    mr2, mp, mt = O.thresholds(O.Settings())
+    assert mp == np.float32(0.1) and mr2 == np.float32(1e-5)
+    assert abs(float(mt) - 1.6448536) < 1e-6
+    mr2, mp, mt = O.thresholds(O.Settings(storeBin=True))
+    assert mp == np.float32(0.05) and mr2 == np.float32(1e-6)
+    assert abs(float(mt) - 1.959964) < 1e-5
+
+
+def test_pvalue_branches():
+    assert O.pvalue(0.0) == pytest.approx(0.5)
+    assert O.pvalue(1.5) == pytest.approx(0.5 - 0.1 * float(np.float32(4.4 - 1.5)) * 1.5)
+    assert O.pvalue(1.6) == pytest.approx(math.erfc(1.6 / math.sqrt(2)))
+
+
+def test_exclusion_list_semantics(tmp_path):
+    p = tmp_path / "ex.txt"
+    p.write_text("1 2\n5\n7\n9 11\n13\n")
+    rows = O.exclusion_rows(str(p), 100)
+    assert rows.tolist() == [0, 1, 4, 6, 8, 9, 10, 12]
+    p.write_text("5 3\n")
+    with pytest.raises(ValueError):
+        O.exclusion_rows(str(p), 100)
+    p.write_text("7 9\n3 4\n")
+    with pytest.raises(ValueError):
+        O.exclusion_rows(str(p), 100)
