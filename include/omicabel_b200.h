@@ -1,0 +1,189 @@
+/*
+ * omicabel_b200.h — C ABI of the B200 association engine.
+ *
+ * Drop-in for the blocked normal-equation OLS path of OmicABELnoMM
+ * (Algorithm::partialNEQ_Blocked_STL_MD, src/Algorithm.cpp:322-886 of the
+ * reference).  Two levels:
+ *
+ *  1. Whole-run entry points that replace the reference's process and
+ *     solver entry:  oa_cli_main  ≙ main            (src/main.cpp:440-500)
+ *                    oa_solve     ≙ Algorithm::solve(params, out, P_NEQ_B_OPT_MD)
+ *                                                    (src/Algorithm.cpp:37-48)
+ *     They read .fvi/.fvd inputs and write <out>_dis.txt (+ _sto.ibin and
+ *     _sto.dbin with store_bin) exactly as the reference does.
+ *
+ *  2. A block engine for embedding, the device-side replacement of the
+ *     solver's per-block work: covariates once (≙ AIOwrapper::load_AL +
+ *     the Stl/rank-check steps, src/Algorithm.cpp:475-522), one trait block
+ *     (≙ load_Yblock + replace_nans/sumSquares/XL'Y/Stl_corr,
+ *     src/Algorithm.cpp:550-595), then SNP blocks (≙ load_ARblock through
+ *     hpc_statistics, src/Algorithm.cpp:610-813).  It returns the stored
+ *     results (the reference's list<resultH>) as flat arrays.
+ *
+ * Conventions: plain C types, column-major float32 matrices with the
+ * individual (row) index contiguous — the layout of a .fvd file.  The
+ * library never calls exit(); every entry point returns an oa_status and
+ * oa_last_error() describes the last failure of the calling thread.  An
+ * engine owns its device memory and is used from one host thread at a time.
+ */
+#ifndef OMICABEL_B200_H
+#define OMICABEL_B200_H
+
+#include <stdint.h>
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define OA_ABI_VERSION 1
+#define OA_MAX_L 16   /* covariates, intercept included */
+#define OA_MAX_R 4    /* columns per SNP */
+
+typedef enum oa_status {
+    OA_OK = 0,
+    OA_ERR_ARG = 1,            /* invalid argument or size */
+    OA_ERR_CUDA = 2,           /* CUDA runtime failure (message in oa_last_error) */
+    OA_ERR_COLLINEAR = 3,      /* covariates linearly dependent (src/Algorithm.cpp:510-522) */
+    OA_ERR_IO = 4,             /* file missing, short or malformed */
+    OA_ERR_STATE = 5,          /* call out of order (e.g. SNP block before traits) */
+    OA_ERR_NOMEM = 6,          /* device or host allocation failed */
+    OA_ERR_UNSUPPORTED = 7,    /* sizes beyond this build's limits */
+    OA_ERR_NUMERIC = 8         /* e.g. negative sum of squares (src/Algorithm.cpp:1096-1099) */
+} oa_status;
+
+typedef enum oa_precision {
+    OA_PLAIN_FP32 = 0,   /* FP32 data, FP32 SIMT GEMM, FP64 small systems */
+    OA_MIXED_BF16X3 = 1  /* XR'Y on tcgen05 tensor cores, BF16 hi/lo 3-product, FP32 accumulate */
+} oa_precision;
+
+/* ---------------------------------------------------------------------------
+ * Block engine
+ * ------------------------------------------------------------------------- */
+typedef struct oa_engine oa_engine;
+
+typedef struct oa_config {
+    int32_t n;             /* individuals after exclusions (rows) */
+    int32_t l;             /* covariates incl. intercept, 1..OA_MAX_L */
+    int32_t r;             /* columns per SNP, 1..OA_MAX_R */
+    int32_t max_traits;    /* largest trait block passed to oa_set_traits */
+    int32_t max_snps;      /* largest SNP block passed to oa_run_snps* */
+    int32_t precision;     /* oa_precision */
+    int32_t device;        /* CUDA device ordinal */
+    int32_t disp_cov;      /* -i: also report covariate terms of stored rows */
+    int32_t store_all;     /* -f: store every test (thresholds ignored) */
+    int32_t quirk_r2;      /* reproduce the reference's r>=2 downdate (src/Algorithm.cpp:1390-1396) */
+    float min_r2_store;    /* effective R2 store threshold (src/Algorithm.cpp:338-339) */
+    float min_t_store;     /* effective |t| store threshold (src/Algorithm.cpp:359) */
+    float min_p_disp;      /* display P threshold, used for the significant-result count */
+    int32_t real_n;        /* individuals before exclusions (nPct denominator) */
+} oa_config;
+
+/* Stored results of one SNP block, in reference output order
+ * (trait, then SNP; coefficients h = p-1 .. start_h).  One row per
+ * (trait, SNP) test that has at least one stored SNP term
+ * (≙ resultH, src/Definitions.h:271-280); its stored coefficients are the
+ * bits of coef_mask (bit h).  coef_* hold p entries per row. */
+typedef struct oa_rows {
+    int64_t count;             /* rows */
+    const int32_t* trait;      /* trait index within the trait block */
+    const int32_t* snp;        /* SNP index within the SNP block */
+    const float* r2;           /* R2 of the test */
+    const int32_t* n_used;     /* n - missing of the trait */
+    const uint32_t* coef_mask; /* bit h set: coefficient h stored */
+    const float* coef_b;       /* [count * p] beta */
+    const float* coef_se;      /* [count * p] standard error */
+    const float* coef_t;       /* [count * p] |t| */
+    int64_t sig_cov_unrowed;   /* covariate terms with P < min_p_disp in tests without a stored row */
+    int64_t tests;             /* tests evaluated */
+    int64_t singular;          /* tests skipped as singular (the reference emits undefined values) */
+} oa_rows;
+
+/* Create an engine on cfg->device.  Replaces the allocations of
+ * src/Algorithm.cpp:417-456 with device buffers sized by cfg. */
+oa_status oa_engine_create(const oa_config* cfg, oa_engine** out);
+oa_status oa_engine_destroy(oa_engine* e);
+
+/* Covariates, host column-major n x l (NaN-free: the reader drops such rows).
+ * ≙ load_AL + ssyrk Stl + sgesvd rank check (src/Algorithm.cpp:475-522). */
+oa_status oa_set_covariates(oa_engine* e, const float* xl_host);
+
+/* One trait block, host column-major n x t, NaN = missing.
+ * ≙ load_Yblock, replace_nans, sumSquares, XL'Y, Stl_corr (src/Algorithm.cpp:550-595).
+ * Traits are grouped by missingness pattern on the device. */
+oa_status oa_set_traits(oa_engine* e, const float* y_host, int32_t t);
+/* Same with a device pointer (column stride n). */
+oa_status oa_set_traits_device(oa_engine* e, const float* y_dev, int32_t t);
+
+/* One SNP block, host column-major n x (r*mb), NaN = missing dosage.
+ * ≙ load_ARblock .. hpc_statistics (src/Algorithm.cpp:610-813).  Results
+ * stay valid until the next call on this engine. */
+oa_status oa_run_snps(oa_engine* e, const float* xr_host, int32_t mb, oa_rows* out);
+/* Same with the SNP block already in device memory (column stride n).
+ * With results_on_host = 0 the oa_rows pointers are device pointers and
+ * are not sorted; with 1 they are host pointers in reference order. */
+oa_status oa_run_snps_device(oa_engine* e, const float* xr_dev, int32_t mb,
+                             int32_t results_on_host, oa_rows* out);
+
+/* Dense per-test output for checking: beta/se/t of the r SNP terms
+ * ([t][mb][r], trait-major) and R2 ([t][mb]) of the last SNP block,
+ * copied to host arrays the caller provides.  Tests that are singular or
+ * have RSS <= 0 hold NaN. */
+oa_status oa_dense_last(oa_engine* e, float* beta, float* se, float* tstat, float* r2);
+oa_status oa_enable_dense(oa_engine* e, int32_t on);
+
+/* Number of kernel launches this engine issued so far (instrumentation). */
+int64_t oa_kernel_launches(const oa_engine* e);
+/* Device time (ms) of the dominant kernel in the last SNP block and its name. */
+float oa_last_kernel_ms(const oa_engine* e, const char** name);
+
+/* ---------------------------------------------------------------------------
+ * Whole-run entry points
+ * ------------------------------------------------------------------------- */
+typedef struct oa_settings {
+    const char* fname_xl;        /* -c, without extension */
+    const char* fname_xr;        /* -g */
+    const char* fname_y;         /* -p */
+    const char* fname_out;       /* -o */
+    const char* fname_exclude;   /* -x, NULL or "" for none */
+    int32_t r;                   /* -n */
+    float min_p_disp;            /* -d */
+    float min_p_store;           /* -s */
+    float min_r2_disp;           /* -r */
+    float min_r2_store;          /* -e */
+    int32_t store_bin;           /* -b */
+    int32_t disp_cov;            /* -i */
+    int32_t store_all;           /* -f */
+    int32_t precision;           /* oa_precision (default plain) */
+    int32_t device;
+    int32_t quirk_r2;
+    int32_t verbose;             /* progress characters and messages on stdout */
+} oa_settings;
+
+typedef struct oa_outputs {
+    uint64_t total_sig_results;  /* ≙ Outputs.total_sig_results (src/Definitions.h:256) */
+    double duration_s;
+    int64_t tests;
+    int64_t rows_written;
+    int64_t singular;
+} oa_outputs;
+
+/* Fill s with the reference defaults (src/Algorithm.cpp:277-311). */
+void oa_default_settings(oa_settings* s);
+/* ≙ Algorithm::solve(params, out, P_NEQ_B_OPT_MD). */
+oa_status oa_solve(const oa_settings* s, oa_outputs* out);
+/* ≙ main of the reference CLI: same flags, exit status 0 / 1. */
+int oa_cli_main(int argc, char** argv);
+
+/* |t| -> P exactly as the reference (long double, src/Algorithm.cpp:1159-1167). */
+long double oa_pvalue(float t);
+/* P threshold -> |t| threshold (src/Utility.cpp:244-250). */
+float oa_t_threshold(float p);
+
+const char* oa_last_error(void);
+int32_t oa_abi_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* OMICABEL_B200_H */

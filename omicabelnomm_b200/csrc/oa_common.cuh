@@ -1,0 +1,129 @@
+// Shared device helpers and engine-internal types of the B200 association engine.
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+#include <cuda_bf16.h>
+
+#include "omicabel_b200.h"
+
+#define OA_NTHREADS 256
+#define OA_SETS_MAX 4096   // row sets (missingness patterns + zero sets) per trait block
+
+namespace oa {
+
+// One stored row (a (trait, SNP) test with at least one stored SNP term),
+// the device form of the reference's resultH (src/Definitions.h:271-280).
+struct alignas(16) Rec {
+    int32_t trait;      // trait index within the trait block
+    int32_t snp;        // SNP index within the SNP block
+    float r2;           // R2 (src/Algorithm.cpp:1092)
+    uint32_t mask;      // bit a: SNP term a (coefficient h = l + a) stored
+    float sig;          // sqrt(RSS / n_corrected) (src/Algorithm.cpp:1100)
+    float pad[3];
+    float b[OA_MAX_R];
+    float se[OA_MAX_R];
+    float t[OA_MAX_R];
+};
+static_assert(sizeof(Rec) == 80, "Rec layout");
+
+// Everything the fused statistics epilogue reads, per trait and per SNP.
+struct EpiArgs {
+    int n, l, r, p, mb, G;
+    // per trait
+    const int* pat;          // missingness pattern of the trait
+    const int* zset;         // zero set of the trait or -1
+    const double* rss0;      // RSS of the covariate-only fit over observed rows
+    const float* sst;        // SST as the reference computes it (src/Algorithm.cpp:1222-1251)
+    const int* nobs;         // n - missing
+    const double* b0;        // covariate-only coefficients in the orthonormal basis [t][l]
+    // per SNP (and pattern)
+    const double* sinv;      // inverse Schur complement per (pattern, SNP): [G][mb][r*r]
+    const float* varx;       // diag of the all-rows inverse for the SNP terms [mb][r]
+    const uint8_t* sing;     // singular flag per (pattern, SNP) [G][mb]
+    const float* aobs;       // Q_obs' X per (pattern, SNP) [G][mb][l][r]  (zero-set path)
+    const float* zA;         // per (zero set, SNP) sum over zero rows of q x' [Z][mb][l][r]
+    const float* zD;         // per (zero set, SNP) sum over zero rows of x x' [Z][mb][r][r]
+    const double* zQ;        // per zero set sum of q q' [Z][l][l]
+    const double* W;         // (Q_obs'Q_obs)^-1 per pattern [G][l][l]
+    // thresholds
+    float min_r2, min_t;
+    int store_all;
+    // outputs
+    Rec* rec;
+    unsigned long long* rec_count;
+    long long cap;
+    unsigned long long* n_singular;
+    // dense outputs (optional): beta/se/t [t][mb][r], r2 [t][mb], sig [t][mb]
+    float* d_beta;
+    float* d_se;
+    float* d_t;
+    float* d_r2;
+    float* d_sig;
+    int t;
+    int snp_base;            // index of the block's first SNP within the API call
+    long long dense_ld;      // SNPs per trait row of the dense outputs
+};
+
+__device__ __forceinline__ unsigned long long mix64(unsigned long long z) {
+    // splitmix64 finaliser (Steele, Lea, Flood 2014)
+    z += 0x9e3779b97f4a7c15ULL;
+    z = (z ^ (z >> 30)) * 0xbf58476d1ce4e5b9ULL;
+    z = (z ^ (z >> 27)) * 0x94d049bb133111ebULL;
+    return z ^ (z >> 31);
+}
+
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+__device__ __forceinline__ float warp_sumf(float v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+// In-place inverse of a small SPD matrix (row-major k x k, k <= OA_MAX_R or
+// OA_MAX_L) by Cholesky.  Returns false if a pivot is not positive
+// relative to the diagonal scale (the system is treated as singular).
+template <int K>
+__device__ __host__ inline bool spd_inverse(double* A, int k, double rel_tol) {
+    double L[K * K];
+    double dmax = 0.0;
+    for (int i = 0; i < k; ++i) dmax = fmax(dmax, fabs(A[i * k + i]));
+    if (!(dmax > 0.0)) return false;
+    for (int i = 0; i < k * k; ++i) L[i] = 0.0;
+    for (int j = 0; j < k; ++j) {
+        double s = A[j * k + j];
+        for (int q = 0; q < j; ++q) s -= L[j * k + q] * L[j * k + q];
+        if (!(s > rel_tol * fmax(fabs(A[j * k + j]), 1e-300))) return false;
+        double d = sqrt(s);
+        L[j * k + j] = d;
+        for (int i = j + 1; i < k; ++i) {
+            double u = A[i * k + j];
+            for (int q = 0; q < j; ++q) u -= L[i * k + q] * L[j * k + q];
+            L[i * k + j] = u / d;
+        }
+    }
+    // inverse of L (lower), then A^-1 = L^-T L^-1
+    double Li[K * K];
+    for (int i = 0; i < k * k; ++i) Li[i] = 0.0;
+    for (int i = 0; i < k; ++i) {
+        Li[i * k + i] = 1.0 / L[i * k + i];
+        for (int j = 0; j < i; ++j) {
+            double s = 0.0;
+            for (int q = j; q < i; ++q) s += L[i * k + q] * Li[q * k + j];
+            Li[i * k + j] = -s / L[i * k + i];
+        }
+    }
+    for (int i = 0; i < k; ++i)
+        for (int j = 0; j <= i; ++j) {
+            double s = 0.0;
+            for (int q = i; q < k; ++q) s += Li[q * k + i] * Li[q * k + j];
+            A[i * k + j] = s;
+            A[j * k + i] = s;
+        }
+    return true;
+}
+
+}  // namespace oa

@@ -1,0 +1,942 @@
+// Block engine of the B200 association engine: device memory, kernel
+// sequencing and the C ABI declared in include/omicabel_b200.h.
+//
+// Per trait block (≙ src/Algorithm.cpp:550-595):
+//   k_trait_stats -> host groups traits by missingness pattern (and by the
+//   set of observed exact zeros) -> k_set_rows -> k_set_gram -> k_trait_resid
+// Per SNP chunk (≙ src/Algorithm.cpp:610-813):
+//   k_snp_stats -> XR'Y~ GEMM with fused statistics epilogue -> (covariate terms)
+// Per API call: sort of the stored rows into reference order (trait, SNP).
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <string>
+#include <tuple>
+#include <vector>
+
+#include <cub/cub.cuh>
+
+#include "oa_cov.cuh"
+#include "oa_kernels.cuh"
+#include "oa_launch.h"
+
+using namespace oa;
+
+namespace {
+
+thread_local std::string g_err;
+
+void set_err(const char* fmt, ...) {
+    char buf[1024];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof buf, fmt, ap);
+    va_end(ap);
+    g_err = buf;
+}
+
+#define OA_CU(x)                                                                              \
+    do {                                                                                      \
+        cudaError_t e_ = (x);                                                                 \
+        if (e_ != cudaSuccess) {                                                              \
+            set_err("%s:%d: %s: %s", __FILE__, __LINE__, #x, cudaGetErrorString(e_));         \
+            return OA_ERR_CUDA;                                                               \
+        }                                                                                     \
+    } while (0)
+
+#define OA_CHECK(x)                    \
+    do {                               \
+        oa_status s_ = (x);            \
+        if (s_ != OA_OK) return s_;    \
+    } while (0)
+
+template <class T>
+struct DBuf {
+    T* p = nullptr;
+    size_t n = 0;
+    oa_status ensure(size_t cnt) {
+        if (cnt <= n && p) return OA_OK;
+        if (p) cudaFree(p);
+        p = nullptr;
+        n = 0;
+        if (cnt == 0) cnt = 1;
+        if (cudaMalloc(&p, cnt * sizeof(T)) != cudaSuccess) {
+            cudaGetLastError();
+            set_err("device allocation of %zu bytes failed", cnt * sizeof(T));
+            return OA_ERR_NOMEM;
+        }
+        n = cnt;
+        return OA_OK;
+    }
+    void release() {
+        if (p) cudaFree(p);
+        p = nullptr;
+        n = 0;
+    }
+};
+
+int pad_l(int l) { return l <= 4 ? 4 : (l <= 8 ? 8 : 16); }
+
+// Householder QR of the n x l column-major matrix A (FP64): Q (n x l,
+// column-major, orthonormal columns) and R (l x l, row-major upper
+// triangular) with a positive diagonal.
+void householder_qr(const std::vector<double>& A, int n, int l, std::vector<double>& Q, std::vector<double>& R) {
+    std::vector<double> Wm(A);
+    std::vector<std::vector<double>> V(l);
+    for (int k = 0; k < l; ++k) {
+        double nrm = 0.0;
+        for (int i = k; i < n; ++i) nrm += Wm[(size_t)k * n + i] * Wm[(size_t)k * n + i];
+        nrm = std::sqrt(nrm);
+        const double x0 = Wm[(size_t)k * n + k];
+        const double alpha = x0 >= 0 ? -nrm : nrm;
+        std::vector<double> v(n - k);
+        for (int i = k; i < n; ++i) v[i - k] = Wm[(size_t)k * n + i];
+        v[0] -= alpha;
+        double vn = 0.0;
+        for (double e : v) vn += e * e;
+        vn = std::sqrt(vn);
+        if (vn > 0)
+            for (double& e : v) e /= vn;
+        for (int c = k; c < l; ++c) {
+            double d = 0.0;
+            for (int i = k; i < n; ++i) d += v[i - k] * Wm[(size_t)c * n + i];
+            for (int i = k; i < n; ++i) Wm[(size_t)c * n + i] -= 2.0 * d * v[i - k];
+        }
+        V[k] = std::move(v);
+    }
+    R.assign((size_t)l * l, 0.0);
+    for (int i = 0; i < l; ++i)
+        for (int j = i; j < l; ++j) R[(size_t)i * l + j] = Wm[(size_t)j * n + i];
+    Q.assign((size_t)n * l, 0.0);
+    for (int c = 0; c < l; ++c) Q[(size_t)c * n + c] = 1.0;
+    for (int k = l - 1; k >= 0; --k) {
+        const std::vector<double>& v = V[k];
+        for (int c = 0; c < l; ++c) {
+            double d = 0.0;
+            for (int i = k; i < n; ++i) d += v[i - k] * Q[(size_t)c * n + i];
+            for (int i = k; i < n; ++i) Q[(size_t)c * n + i] -= 2.0 * d * v[i - k];
+        }
+    }
+    for (int i = 0; i < l; ++i)
+        if (R[(size_t)i * l + i] < 0) {
+            for (int j = 0; j < l; ++j) R[(size_t)i * l + j] = -R[(size_t)i * l + j];
+            for (int k = 0; k < n; ++k) Q[(size_t)i * n + k] = -Q[(size_t)i * n + k];
+        }
+}
+
+// Singular values of a small square matrix (one-sided Jacobi, FP64).
+std::vector<double> singular_values(std::vector<double> A /* row-major k x k */, int k) {
+    for (int sweep = 0; sweep < 60; ++sweep) {
+        double off = 0.0;
+        for (int p = 0; p < k; ++p)
+            for (int q = p + 1; q < k; ++q) {
+                double a = 0, b = 0, c = 0;
+                for (int i = 0; i < k; ++i) {
+                    a += A[(size_t)i * k + p] * A[(size_t)i * k + p];
+                    b += A[(size_t)i * k + q] * A[(size_t)i * k + q];
+                    c += A[(size_t)i * k + p] * A[(size_t)i * k + q];
+                }
+                if (std::fabs(c) <= 1e-300) continue;
+                off = std::max(off, std::fabs(c) / std::sqrt(a * b));
+                const double zeta = (b - a) / (2 * c);
+                const double t = (zeta >= 0 ? 1.0 : -1.0) / (std::fabs(zeta) + std::sqrt(1 + zeta * zeta));
+                const double cs = 1 / std::sqrt(1 + t * t), sn = cs * t;
+                for (int i = 0; i < k; ++i) {
+                    const double x = A[(size_t)i * k + p], y = A[(size_t)i * k + q];
+                    A[(size_t)i * k + p] = cs * x - sn * y;
+                    A[(size_t)i * k + q] = sn * x + cs * y;
+                }
+            }
+        if (off < 1e-15) break;
+    }
+    std::vector<double> s(k);
+    for (int p = 0; p < k; ++p) {
+        double a = 0;
+        for (int i = 0; i < k; ++i) a += A[(size_t)i * k + p] * A[(size_t)i * k + p];
+        s[p] = std::sqrt(a);
+    }
+    return s;
+}
+
+}  // namespace
+
+struct oa_engine {
+    oa_config cfg{};
+    int n = 0, l = 0, r = 0, p = 0, LP = 4, n_pad = 0;
+    cudaStream_t st = nullptr, cp = nullptr;
+    cudaEvent_t ev_copied[2]{}, ev_used[2]{}, k0 = nullptr, k1 = nullptr;
+    long long launches = 0;
+    float last_ms = 0.f;
+    const char* last_name = "";
+    // covariates
+    DBuf<double> Q64, Rinv;
+    DBuf<float> Qr;
+    bool have_cov = false;
+    // traits
+    int t = 0;
+    DBuf<float> Yraw, Yt;
+    DBuf<__nv_bfloat16> Yhi, Ylo;
+    DBuf<double> tsums, rss0, b0, W, zQ;
+    DBuf<int> tcounts, pat, zset, nobs, set_off, set_rows, set_rep, set_kind, set_slot;
+    DBuf<unsigned long long> thash;
+    DBuf<float> sst;
+    DBuf<uint8_t> pat_bad;
+    int G = 0, Z = 0, nsets = 0;
+    std::vector<int> h_nobs;
+    // SNP chunk buffers
+    int chunk = 0;
+    DBuf<float> Xstage[2];
+    DBuf<__nv_bfloat16> Xhi, Xlo;
+    DBuf<float> mean, varx, aobs, afull, zA, zD;
+    DBuf<int> has_nan;
+    DBuf<double> sinv, sfinv;
+    DBuf<uint8_t> sing;
+    // stored rows
+    DBuf<Rec> rec, rec2;
+    DBuf<float> cov, cov2;
+    long long cap = 0;
+    DBuf<unsigned long long> counters;  // [0] rows, [1] singular, [2] significant covariate terms
+    DBuf<unsigned long long> keys, keys2;
+    DBuf<int> perm, perm2;
+    DBuf<unsigned char> cub_tmp;
+    // dense outputs
+    bool dense_on = false;
+    DBuf<float> d_beta, d_se, d_t, d_r2, d_sig;
+    long long dense_ld = 0;
+    int last_mb = 0;
+    // host results
+    std::vector<Rec> h_rec;
+    std::vector<float> h_cov;
+    std::vector<int32_t> o_trait, o_snp, o_nused;
+    std::vector<float> o_r2, o_b, o_se, o_t;
+    std::vector<uint32_t> o_mask;
+};
+
+namespace {
+
+oa_status set_traits_impl(oa_engine* e, const float* y, int32_t t, bool device_ptr) {
+    if (!e->have_cov) {
+        set_err("oa_set_traits before oa_set_covariates");
+        return OA_ERR_STATE;
+    }
+    if (t <= 0 || t > e->cfg.max_traits) {
+        set_err("trait block of %d traits (engine limit %d)", t, e->cfg.max_traits);
+        return OA_ERR_ARG;
+    }
+    const int n = e->n, l = e->l;
+    e->t = t;
+    const float* Y = y;
+    if (!device_ptr) {
+        OA_CHECK(e->Yraw.ensure((size_t)n * t));
+        OA_CU(cudaMemcpyAsync(e->Yraw.p, y, sizeof(float) * (size_t)n * t, cudaMemcpyHostToDevice, e->st));
+        Y = e->Yraw.p;
+    }
+    OA_CHECK(e->tsums.ensure((size_t)t * (2 + OA_MAX_L)));
+    OA_CHECK(e->tcounts.ensure((size_t)t * 2));
+    OA_CHECK(e->thash.ensure((size_t)t * 4));
+    TraitStatsOut tso{e->tsums.p, e->tcounts.p, e->thash.p};
+    k_trait_stats<<<t, OA_NTHREADS, 0, e->st>>>(Y, (size_t)n, n, l, e->Q64.p, tso);
+    ++e->launches;
+    OA_CU(cudaGetLastError());
+    std::vector<int> counts((size_t)t * 2);
+    std::vector<unsigned long long> hashes((size_t)t * 4);
+    OA_CU(cudaMemcpyAsync(counts.data(), e->tcounts.p, sizeof(int) * counts.size(), cudaMemcpyDeviceToHost, e->st));
+    OA_CU(cudaMemcpyAsync(hashes.data(), e->thash.p, sizeof(unsigned long long) * hashes.size(),
+                          cudaMemcpyDeviceToHost, e->st));
+    OA_CU(cudaStreamSynchronize(e->st));
+
+    // group traits: missingness patterns, then sets of observed exact zeros
+    std::map<std::tuple<int, unsigned long long, unsigned long long>, int> pmap, zmap;
+    std::vector<int> hpat(t), hz(t, -1), prep, zrep, pcnt, zcnt;
+    for (int j = 0; j < t; ++j) {
+        auto key = std::make_tuple(counts[j * 2], hashes[j * 4], hashes[j * 4 + 1]);
+        auto it = pmap.find(key);
+        if (it == pmap.end()) {
+            it = pmap.emplace(key, (int)prep.size()).first;
+            prep.push_back(j);
+            pcnt.push_back(counts[j * 2]);
+        }
+        hpat[j] = it->second;
+        if (counts[j * 2 + 1] > 0) {
+            auto zk = std::make_tuple(counts[j * 2 + 1], hashes[j * 4 + 2], hashes[j * 4 + 3]);
+            auto zt = zmap.find(zk);
+            if (zt == zmap.end()) {
+                zt = zmap.emplace(zk, (int)zrep.size()).first;
+                zrep.push_back(j);
+                zcnt.push_back(counts[j * 2 + 1]);
+            }
+            hz[j] = zt->second;
+        }
+    }
+    e->G = (int)prep.size();
+    e->Z = (int)zrep.size();
+    e->nsets = e->G + e->Z;
+    if (e->nsets > OA_SETS_MAX) {
+        set_err("%d distinct missingness/zero patterns in one trait block (limit %d)", e->nsets, OA_SETS_MAX);
+        return OA_ERR_UNSUPPORTED;
+    }
+    std::vector<int> off(e->nsets + 1, 0), rep(e->nsets), kind(e->nsets), slot(e->nsets);
+    for (int s = 0; s < e->nsets; ++s) {
+        const bool isz = s >= e->G;
+        rep[s] = isz ? zrep[s - e->G] : prep[s];
+        kind[s] = isz ? 1 : 0;
+        slot[s] = isz ? s - e->G : s;
+        off[s + 1] = off[s] + (isz ? zcnt[s - e->G] : pcnt[s]);
+    }
+    e->h_nobs.resize(t);
+    for (int j = 0; j < t; ++j) e->h_nobs[j] = n - counts[j * 2];
+    OA_CHECK(e->pat.ensure(t));
+    OA_CHECK(e->zset.ensure(t));
+    OA_CHECK(e->set_off.ensure(e->nsets + 1));
+    OA_CHECK(e->set_rep.ensure(e->nsets));
+    OA_CHECK(e->set_kind.ensure(e->nsets));
+    OA_CHECK(e->set_slot.ensure(e->nsets));
+    OA_CHECK(e->set_rows.ensure(std::max(off[e->nsets], 1)));
+    OA_CHECK(e->W.ensure((size_t)std::max(e->G, 1) * l * l));
+    OA_CHECK(e->zQ.ensure((size_t)std::max(e->Z, 1) * l * l));
+    OA_CHECK(e->pat_bad.ensure(std::max(e->G, 1)));
+    OA_CU(cudaMemcpyAsync(e->pat.p, hpat.data(), sizeof(int) * t, cudaMemcpyHostToDevice, e->st));
+    OA_CU(cudaMemcpyAsync(e->zset.p, hz.data(), sizeof(int) * t, cudaMemcpyHostToDevice, e->st));
+    OA_CU(cudaMemcpyAsync(e->set_off.p, off.data(), sizeof(int) * off.size(), cudaMemcpyHostToDevice, e->st));
+    OA_CU(cudaMemcpyAsync(e->set_rep.p, rep.data(), sizeof(int) * rep.size(), cudaMemcpyHostToDevice, e->st));
+    OA_CU(cudaMemcpyAsync(e->set_kind.p, kind.data(), sizeof(int) * kind.size(), cudaMemcpyHostToDevice, e->st));
+    OA_CU(cudaMemcpyAsync(e->set_slot.p, slot.data(), sizeof(int) * slot.size(), cudaMemcpyHostToDevice, e->st));
+    k_set_rows<<<e->nsets, OA_NTHREADS, 0, e->st>>>(Y, (size_t)n, n, e->set_rep.p, e->set_kind.p, e->set_off.p,
+                                                   e->set_rows.p);
+    k_set_gram<<<e->nsets, OA_NTHREADS, 0, e->st>>>(e->Q64.p, n, l, e->set_kind.p, e->set_off.p, e->set_rows.p,
+                                                   e->W.p, e->zQ.p, e->set_slot.p, e->pat_bad.p);
+    e->launches += 2;
+    OA_CU(cudaGetLastError());
+    OA_CHECK(e->Yt.ensure((size_t)t * e->n_pad));
+    if (e->cfg.precision == OA_MIXED_BF16X3) {
+        OA_CHECK(e->Yhi.ensure((size_t)t * e->n_pad));
+        OA_CHECK(e->Ylo.ensure((size_t)t * e->n_pad));
+    }
+    OA_CHECK(e->rss0.ensure(t));
+    OA_CHECK(e->sst.ensure(t));
+    OA_CHECK(e->nobs.ensure(t));
+    OA_CHECK(e->b0.ensure((size_t)t * l));
+    const bool mixed = e->cfg.precision == OA_MIXED_BF16X3;
+    k_trait_resid<<<t, OA_NTHREADS, 0, e->st>>>(Y, (size_t)n, n, e->n_pad, l, e->Q64.p, e->tsums.p, e->tcounts.p,
+                                               e->pat.p, e->W.p, e->Yt.p, mixed ? e->Yhi.p : nullptr,
+                                               mixed ? e->Ylo.p : nullptr, e->rss0.p, e->sst.p, e->nobs.p,
+                                               e->b0.p);
+    ++e->launches;
+    OA_CU(cudaGetLastError());
+    OA_CU(cudaStreamSynchronize(e->st));
+    return OA_OK;
+}
+
+StatsArgs stats_args(oa_engine* e, const float* X, int mbc, int LP, int spb, int spp) {
+    StatsArgs A{};
+    A.X = X;
+    A.ldx = (size_t)e->n;
+    A.n = e->n;
+    A.n_pad = e->n_pad;
+    A.l = e->l;
+    A.QS = LP;
+    A.mb = mbc;
+    A.spb = spb;
+    A.Qr = e->Qr.p;
+    A.nsets = e->nsets;
+    A.G = e->G;
+    A.Z = e->Z;
+    A.set_off = e->set_off.p;
+    A.rows = e->set_rows.p;
+    A.W = e->W.p;
+    A.pat_bad = e->pat_bad.p;
+    A.sets_per_pass = spp;
+    A.mean = e->mean.p;
+    A.has_nan = e->has_nan.p;
+    A.sinv = e->sinv.p;
+    A.sing = e->sing.p;
+    A.varx = e->varx.p;
+    const bool need_aobs = e->cfg.disp_cov || e->Z > 0;
+    A.aobs = need_aobs ? e->aobs.p : nullptr;
+    A.afull = e->cfg.disp_cov ? e->afull.p : nullptr;
+    A.sfinv = e->cfg.disp_cov ? e->sfinv.p : nullptr;
+    A.zA = e->zA.p;
+    A.zD = e->zD.p;
+    A.write_split = e->cfg.precision == OA_MIXED_BF16X3;
+    A.Xhi = e->Xhi.p;
+    A.Xlo = e->Xlo.p;
+    return A;
+}
+
+template <int R>
+oa_status stats_dispatch(oa_engine* e, const float* X, int mbc) {
+    // SNPs per CTA: as many as fit the register budget and ~160 KB of staged columns
+    const int nS = (e->n + 3) & ~3;
+    auto pick = [&](auto lp_tag) -> oa_status {
+        constexpr int LP = decltype(lp_tag)::value;
+        int spb = stats_spb_max(R, LP);
+        while (spb > 1 && (size_t)spb * R * nS * 4 > 160 * 1024) --spb;
+        const size_t base = stats_smem_bytes(R, LP, e->n, spb, 0);
+        const size_t limit = 227 * 1024 - 1024;
+        if (base + (size_t)spb * stats_na(R, LP) * 4 > limit) {
+            set_err("n = %d is too large for one SNP column in shared memory", e->n);
+            return OA_ERR_UNSUPPORTED;
+        }
+        int spp = (int)std::min<size_t>((size_t)std::max(e->nsets, 1),
+                                        (limit - base) / ((size_t)spb * stats_na(R, LP) * 4));
+        spp = std::max(spp, 1);
+        const size_t smem = stats_smem_bytes(R, LP, e->n, spb, spp);
+        StatsArgs A = stats_args(e, X, mbc, LP, spb, spp);
+        OA_CU(oa_launch_snp_stats(R, LP, A, (mbc + spb - 1) / spb, smem, e->st));
+        ++e->launches;
+        return OA_OK;
+    };
+    if (e->LP == 4) return pick(std::integral_constant<int, 4>{});
+    if (e->LP == 8) return pick(std::integral_constant<int, 8>{});
+    return pick(std::integral_constant<int, 16>{});
+}
+
+EpiArgs epi_args(oa_engine* e, int mbc, int snp_base) {
+    EpiArgs E{};
+    E.n = e->n;
+    E.l = e->l;
+    E.r = e->r;
+    E.p = e->p;
+    E.mb = mbc;
+    E.G = e->G;
+    E.pat = e->pat.p;
+    E.zset = e->zset.p;
+    E.rss0 = e->rss0.p;
+    E.sst = e->sst.p;
+    E.nobs = e->nobs.p;
+    E.b0 = e->b0.p;
+    E.sinv = e->sinv.p;
+    E.varx = e->varx.p;
+    E.sing = e->sing.p;
+    E.aobs = e->aobs.p;
+    E.zA = e->zA.p;
+    E.zD = e->zD.p;
+    E.zQ = e->zQ.p;
+    E.W = e->W.p;
+    E.min_r2 = e->cfg.min_r2_store;
+    E.min_t = e->cfg.min_t_store;
+    E.store_all = e->cfg.store_all;
+    E.rec = e->rec.p;
+    E.rec_count = e->counters.p;
+    E.cap = e->cap;
+    E.n_singular = e->counters.p + 1;
+    E.t = e->t;
+    E.snp_base = snp_base;
+    E.dense_ld = e->dense_ld;
+    if (e->dense_on || e->cfg.disp_cov) {
+        E.d_beta = e->d_beta.p;
+        E.d_se = e->d_se.p;
+        E.d_t = e->d_t.p;
+        E.d_r2 = e->d_r2.p;
+        E.d_sig = e->d_sig.p;
+    }
+    return E;
+}
+
+CovArgs cov_args(oa_engine* e, int mbc) {
+    CovArgs C{};
+    C.n = e->n;
+    C.l = e->l;
+    C.r = e->r;
+    C.p = e->p;
+    C.mb = mbc;
+    C.pat = e->pat.p;
+    C.b0 = e->b0.p;
+    C.W = e->W.p;
+    C.aobs = e->aobs.p;
+    C.afull = e->afull.p;
+    C.sfinv = e->sfinv.p;
+    C.Rinv = e->Rinv.p;
+    C.nobs = e->nobs.p;
+    C.min_t = e->cfg.min_t_store;
+    C.store_all = e->cfg.store_all;
+    C.min_p_disp = (double)e->cfg.min_p_disp;
+    return C;
+}
+
+template <int R>
+oa_status gemm_dispatch(oa_engine* e, const float* X, int mbc, int snp_base) {
+    EpiArgs E = epi_args(e, mbc, snp_base);
+    if (e->cfg.precision == OA_PLAIN_FP32) {
+        OA_CU(oa_launch_gemm_simt(R, X, (size_t)e->n, mbc * R, e->Yt.p, (size_t)e->n_pad, e->t, e->n, e->mean.p,
+                                  e->has_nan.p, E, e->st));
+        e->last_name = "k_gemm_simt";
+    } else {
+        OA_CU(oa_launch_gemm_tc(R, e->Xhi.p, e->Xlo.p, mbc * R, e->Yhi.p, e->Ylo.p, e->t, e->n_pad, E, e->st));
+        e->last_name = "k_gemm_tc";
+    }
+    ++e->launches;
+    OA_CU(cudaGetLastError());
+    return OA_OK;
+}
+
+oa_status ensure_chunk_buffers(oa_engine* e) {
+    const size_t mb = (size_t)e->chunk, r = e->r, l = e->l;
+    const size_t G = std::max(e->G, 1), Z = std::max(e->Z, 1);
+    OA_CHECK(e->mean.ensure(mb * r));
+    OA_CHECK(e->has_nan.ensure(1));
+    OA_CHECK(e->varx.ensure(mb * r));
+    OA_CHECK(e->sinv.ensure(G * mb * r * r));
+    OA_CHECK(e->sing.ensure(G * mb));
+    OA_CHECK(e->zA.ensure(Z * mb * l * r));
+    OA_CHECK(e->zD.ensure(Z * mb * r * r));
+    if (e->cfg.disp_cov || e->Z > 0) OA_CHECK(e->aobs.ensure(G * mb * l * r));
+    if (e->cfg.disp_cov) {
+        OA_CHECK(e->afull.ensure(mb * l * r));
+        OA_CHECK(e->sfinv.ensure(mb * r * r));
+    }
+    if (e->cfg.precision == OA_MIXED_BF16X3) {
+        OA_CHECK(e->Xhi.ensure(mb * r * e->n_pad));
+        OA_CHECK(e->Xlo.ensure(mb * r * e->n_pad));
+    }
+    return OA_OK;
+}
+
+oa_status ensure_cap(oa_engine* e, long long want) {
+    if (want <= e->cap) return OA_OK;
+    // keep what is already stored
+    DBuf<Rec> nr;
+    OA_CHECK(nr.ensure((size_t)want));
+    if (e->rec.p && e->cap > 0) OA_CU(cudaMemcpyAsync(nr.p, e->rec.p, sizeof(Rec) * e->cap, cudaMemcpyDeviceToDevice, e->st));
+    std::swap(e->rec, nr);
+    nr.release();
+    if (e->cfg.disp_cov) {
+        DBuf<float> nc;
+        OA_CHECK(nc.ensure((size_t)want * e->l * 3));
+        if (e->cov.p && e->cap > 0)
+            OA_CU(cudaMemcpyAsync(nc.p, e->cov.p, sizeof(float) * e->cap * e->l * 3, cudaMemcpyDeviceToDevice, e->st));
+        std::swap(e->cov, nc);
+        nc.release();
+    }
+    OA_CU(cudaStreamSynchronize(e->st));
+    e->cap = want;
+    return OA_OK;
+}
+
+// One SNP chunk already on the device.  Appends its stored rows.
+template <int R>
+oa_status run_chunk(oa_engine* e, const float* X, int mbc, int snp_base) {
+    OA_CU(cudaMemsetAsync(e->has_nan.p, 0, sizeof(int), e->st));
+    OA_CHECK(stats_dispatch<R>(e, X, mbc));
+    unsigned long long before[3];
+    OA_CU(cudaMemcpyAsync(before, e->counters.p, sizeof before, cudaMemcpyDeviceToHost, e->st));
+    OA_CU(cudaStreamSynchronize(e->st));
+    for (int attempt = 0; attempt < 3; ++attempt) {
+        OA_CU(cudaEventRecord(e->k0, e->st));
+        OA_CHECK(gemm_dispatch<R>(e, X, mbc, snp_base));
+        OA_CU(cudaEventRecord(e->k1, e->st));
+        unsigned long long after[3];
+        OA_CU(cudaMemcpyAsync(after, e->counters.p, sizeof after, cudaMemcpyDeviceToHost, e->st));
+        OA_CU(cudaStreamSynchronize(e->st));
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, e->k0, e->k1);
+        e->last_ms += ms;
+        if ((long long)after[0] <= e->cap) {
+            if (e->cfg.disp_cov) {
+                CovArgs C = cov_args(e, mbc);
+                const long long first = (long long)before[0], last = (long long)after[0];
+                if (last > first) {
+                    const long long nb = (last - first + 255) / 256;
+                    k_cov_terms<R><<<(unsigned)nb, 256, 0, e->st>>>(e->rec.p, first, last, snp_base, C, e->cov.p);
+                    ++e->launches;
+                }
+                k_cov_count<R><<<4 * 148, 256, 0, e->st>>>(e->d_beta.p, e->d_t.p, e->d_r2.p, e->d_sig.p, e->dense_ld,
+                                                          snp_base, mbc, e->t, e->cfg.min_r2_store, C,
+                                                          e->counters.p + 2);
+                ++e->launches;
+                OA_CU(cudaGetLastError());
+            }
+            return OA_OK;
+        }
+        // more rows than room: grow, roll the counters back and redo the GEMM
+        OA_CHECK(ensure_cap(e, (long long)(after[0] * 1.25) + 1024));
+        OA_CU(cudaMemcpyAsync(e->counters.p, before, sizeof before, cudaMemcpyHostToDevice, e->st));
+    }
+    set_err("stored-row buffer could not be grown");
+    return OA_ERR_NOMEM;
+}
+
+template <int R>
+oa_status run_snps_impl(oa_engine* e, const float* xr, int32_t mb, bool host_input, bool results_on_host,
+                        oa_rows* out) {
+    if (e->t <= 0) {
+        set_err("oa_run_snps before oa_set_traits");
+        return OA_ERR_STATE;
+    }
+    if (mb <= 0 || mb > e->cfg.max_snps) {
+        set_err("SNP block of %d SNPs (engine limit %d)", mb, e->cfg.max_snps);
+        return OA_ERR_ARG;
+    }
+    OA_CHECK(ensure_chunk_buffers(e));
+    const long long tests = (long long)mb * e->t;
+    if (e->cap == 0) OA_CHECK(ensure_cap(e, std::max<long long>(1 << 16, e->cfg.store_all ? tests : tests / 6)));
+    if (e->cfg.store_all) OA_CHECK(ensure_cap(e, tests));
+    OA_CU(cudaMemsetAsync(e->counters.p, 0, 3 * sizeof(unsigned long long), e->st));
+    if (e->dense_on || e->cfg.disp_cov) {
+        const size_t nd = (size_t)e->t * mb;
+        OA_CHECK(e->d_beta.ensure(nd * e->r));
+        OA_CHECK(e->d_se.ensure(nd * e->r));
+        OA_CHECK(e->d_t.ensure(nd * e->r));
+        OA_CHECK(e->d_r2.ensure(nd));
+        OA_CHECK(e->d_sig.ensure(nd));
+        e->dense_ld = mb;
+    }
+    e->last_ms = 0.f;
+    e->last_mb = mb;
+    const size_t colbytes = sizeof(float) * (size_t)e->n * e->r;
+    const int nch = (mb + e->chunk - 1) / e->chunk;
+    if (host_input) {
+        for (int b = 0; b < 2; ++b) OA_CHECK(e->Xstage[b].ensure((size_t)e->chunk * e->r * e->n));
+        // copy of chunk c+1 overlaps the compute of chunk c
+        auto issue_copy = [&](int c) -> oa_status {
+            const int b = c & 1;
+            const int c0 = c * e->chunk, mbc = std::min(e->chunk, mb - c0);
+            OA_CU(cudaStreamWaitEvent(e->cp, e->ev_used[b], 0));
+            OA_CU(cudaMemcpyAsync(e->Xstage[b].p, xr + (size_t)c0 * e->r * e->n, colbytes * mbc,
+                                  cudaMemcpyHostToDevice, e->cp));
+            OA_CU(cudaEventRecord(e->ev_copied[b], e->cp));
+            return OA_OK;
+        };
+        OA_CHECK(issue_copy(0));
+        for (int c = 0; c < nch; ++c) {
+            if (c + 1 < nch) OA_CHECK(issue_copy(c + 1));
+            const int b = c & 1;
+            const int c0 = c * e->chunk, mbc = std::min(e->chunk, mb - c0);
+            OA_CU(cudaStreamWaitEvent(e->st, e->ev_copied[b], 0));
+            OA_CHECK(run_chunk<R>(e, e->Xstage[b].p, mbc, c0));
+            OA_CU(cudaEventRecord(e->ev_used[b], e->st));
+        }
+    } else {
+        for (int c = 0; c < nch; ++c) {
+            const int c0 = c * e->chunk, mbc = std::min(e->chunk, mb - c0);
+            OA_CHECK(run_chunk<R>(e, xr + (size_t)c0 * e->r * e->n, mbc, c0));
+        }
+    }
+    unsigned long long cnt[3];
+    OA_CU(cudaMemcpyAsync(cnt, e->counters.p, sizeof cnt, cudaMemcpyDeviceToHost, e->st));
+    OA_CU(cudaStreamSynchronize(e->st));
+    std::memset(out, 0, sizeof *out);
+    out->count = (int64_t)cnt[0];
+    out->tests = tests;
+    out->singular = (int64_t)cnt[1];
+    out->sig_cov_unrowed = (int64_t)cnt[2];
+    if (!results_on_host) return OA_OK;
+
+    // sort the stored rows into reference order (trait, then SNP)
+    const long long N = (long long)cnt[0];
+    const int l = e->l, p = e->p;
+    e->h_rec.resize(N);
+    if (e->cfg.disp_cov) e->h_cov.resize((size_t)N * l * 3);
+    if (N > 0) {
+        OA_CHECK(e->keys.ensure(N));
+        OA_CHECK(e->keys2.ensure(N));
+        OA_CHECK(e->perm.ensure(N));
+        OA_CHECK(e->perm2.ensure(N));
+        OA_CHECK(e->rec2.ensure(N));
+        k_rec_keys<<<(unsigned)((N + 255) / 256), 256, 0, e->st>>>(e->rec.p, N, e->keys.p, e->perm.p);
+        ++e->launches;
+        size_t tmp = 0;
+        OA_CU(cub::DeviceRadixSort::SortPairs(nullptr, tmp, e->keys.p, e->keys2.p, e->perm.p, e->perm2.p, (int)N, 0,
+                                              64, e->st));
+        OA_CHECK(e->cub_tmp.ensure(tmp));
+        OA_CU(cub::DeviceRadixSort::SortPairs(e->cub_tmp.p, tmp, e->keys.p, e->keys2.p, e->perm.p, e->perm2.p, (int)N,
+                                              0, 64, e->st));
+        if (e->cfg.disp_cov) OA_CHECK(e->cov2.ensure((size_t)N * l * 3));
+        k_rec_gather<<<(unsigned)((N + 255) / 256), 256, 0, e->st>>>(e->rec.p, e->perm2.p, N, e->rec2.p,
+                                                                     e->cfg.disp_cov ? e->cov.p : nullptr,
+                                                                     e->cfg.disp_cov ? e->cov2.p : nullptr, l);
+        ++e->launches;
+        if (e->cfg.disp_cov)
+            OA_CU(cudaMemcpyAsync(e->h_cov.data(), e->cov2.p, sizeof(float) * N * l * 3, cudaMemcpyDeviceToHost,
+                                  e->st));
+        OA_CU(cudaGetLastError());
+        OA_CU(cudaMemcpyAsync(e->h_rec.data(), e->rec2.p, sizeof(Rec) * N, cudaMemcpyDeviceToHost, e->st));
+        OA_CU(cudaStreamSynchronize(e->st));
+    }
+    e->o_trait.resize(N);
+    e->o_snp.resize(N);
+    e->o_nused.resize(N);
+    e->o_r2.resize(N);
+    e->o_mask.resize(N);
+    e->o_b.assign((size_t)N * p, 0.f);
+    e->o_se.assign((size_t)N * p, 0.f);
+    e->o_t.assign((size_t)N * p, 0.f);
+    const float minT = e->cfg.min_t_store;
+    for (long long q = 0; q < N; ++q) {
+        const Rec& rc = e->h_rec[q];
+        e->o_trait[q] = rc.trait;
+        e->o_snp[q] = rc.snp;
+        e->o_nused[q] = e->h_nobs[rc.trait];
+        e->o_r2[q] = rc.r2;
+        uint32_t m = 0;
+        for (int a = 0; a < R; ++a) {
+            const int h = l + a;
+            e->o_b[(size_t)q * p + h] = rc.b[a];
+            e->o_se[(size_t)q * p + h] = rc.se[a];
+            e->o_t[(size_t)q * p + h] = rc.t[a];
+            if (rc.mask & (1u << a)) m |= 1u << h;
+        }
+        if (e->cfg.disp_cov) {
+            const float* cv = e->h_cov.data() + (size_t)q * l * 3;
+            for (int h = 1; h < l; ++h) {
+                e->o_b[(size_t)q * p + h] = cv[h * 3];
+                e->o_se[(size_t)q * p + h] = cv[h * 3 + 1];
+                e->o_t[(size_t)q * p + h] = cv[h * 3 + 2];
+                if (cv[h * 3 + 2] > minT || e->cfg.store_all) m |= 1u << h;
+            }
+        }
+        e->o_mask[q] = m;
+    }
+    out->trait = e->o_trait.data();
+    out->snp = e->o_snp.data();
+    out->r2 = e->o_r2.data();
+    out->n_used = e->o_nused.data();
+    out->coef_mask = e->o_mask.data();
+    out->coef_b = e->o_b.data();
+    out->coef_se = e->o_se.data();
+    out->coef_t = e->o_t.data();
+    return OA_OK;
+}
+
+oa_status run_snps_any(oa_engine* e, const float* xr, int32_t mb, bool host_input, bool results_on_host,
+                       oa_rows* out) {
+    if (!e || !xr || !out) {
+        set_err("null argument");
+        return OA_ERR_ARG;
+    }
+    OA_CU(cudaSetDevice(e->cfg.device));
+    switch (e->r) {
+        case 1: return run_snps_impl<1>(e, xr, mb, host_input, results_on_host, out);
+        case 2: return run_snps_impl<2>(e, xr, mb, host_input, results_on_host, out);
+        case 4: return run_snps_impl<4>(e, xr, mb, host_input, results_on_host, out);
+        default:
+            set_err("r = %d is not supported by this build (1, 2 or 4)", e->r);
+            return OA_ERR_UNSUPPORTED;
+    }
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// C ABI
+// ---------------------------------------------------------------------------
+extern "C" {
+
+const char* oa_last_error(void) { return g_err.c_str(); }
+void oa__set_error(const char* msg) { g_err = msg ? msg : ""; }
+int32_t oa_abi_version(void) { return OA_ABI_VERSION; }
+
+oa_status oa_engine_create(const oa_config* cfg, oa_engine** out) {
+    if (!cfg || !out) {
+        set_err("null argument");
+        return OA_ERR_ARG;
+    }
+    *out = nullptr;
+    if (cfg->l < 1 || cfg->l > OA_MAX_L || cfg->r < 1 || cfg->r > OA_MAX_R || cfg->n <= cfg->l + cfg->r ||
+        cfg->max_traits < 1 || cfg->max_snps < 1) {
+        set_err("invalid engine configuration (n=%d l=%d r=%d)", cfg->n, cfg->l, cfg->r);
+        return OA_ERR_ARG;
+    }
+    if (cfg->r == 3) {
+        set_err("r = 3 is not supported by this build (1, 2 or 4)");
+        return OA_ERR_UNSUPPORTED;
+    }
+    if (cfg->precision != OA_PLAIN_FP32 && cfg->precision != OA_MIXED_BF16X3) {
+        set_err("unknown precision %d", cfg->precision);
+        return OA_ERR_ARG;
+    }
+    if (cfg->quirk_r2 && cfg->r >= 2) {
+        set_err("the reference's r >= 2 downdate quirk is reproduced by the oracle only");
+        return OA_ERR_UNSUPPORTED;
+    }
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+        cudaGetLastError();
+        set_err("no CUDA device: the engine has no CPU path");
+        return OA_ERR_CUDA;
+    }
+    if (cfg->device < 0 || cfg->device >= ndev) {
+        set_err("device %d of %d", cfg->device, ndev);
+        return OA_ERR_ARG;
+    }
+    OA_CU(cudaSetDevice(cfg->device));
+    cudaDeviceProp prop;
+    OA_CU(cudaGetDeviceProperties(&prop, cfg->device));
+    if (prop.major < 10) {
+        set_err("device %s (sm_%d%d) is not a Blackwell sm_100 part", prop.name, prop.major, prop.minor);
+        return OA_ERR_UNSUPPORTED;
+    }
+    oa_engine* e = new oa_engine();
+    e->cfg = *cfg;
+    e->n = cfg->n;
+    e->l = cfg->l;
+    e->r = cfg->r;
+    e->p = cfg->l + cfg->r;
+    e->LP = pad_l(cfg->l);
+    e->n_pad = (cfg->n + 63) & ~63;
+    const char* ch = getenv("OA_CHUNK_SNPS");
+    e->chunk = std::min(cfg->max_snps, ch ? std::max(1, atoi(ch)) : 16384 / cfg->r);
+    if (cudaStreamCreateWithFlags(&e->st, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaStreamCreateWithFlags(&e->cp, cudaStreamNonBlocking) != cudaSuccess) {
+        set_err("stream creation failed");
+        delete e;
+        return OA_ERR_CUDA;
+    }
+    for (int b = 0; b < 2; ++b) {
+        cudaEventCreateWithFlags(&e->ev_copied[b], cudaEventDisableTiming);
+        cudaEventCreateWithFlags(&e->ev_used[b], cudaEventDisableTiming);
+        cudaEventRecord(e->ev_used[b], e->st);
+    }
+    cudaEventCreate(&e->k0);
+    cudaEventCreate(&e->k1);
+    if (e->counters.ensure(4) != OA_OK) {
+        delete e;
+        return OA_ERR_NOMEM;
+    }
+    *out = e;
+    return OA_OK;
+}
+
+oa_status oa_engine_destroy(oa_engine* e) {
+    if (!e) return OA_OK;
+    cudaSetDevice(e->cfg.device);
+    cudaStreamSynchronize(e->st);
+    cudaStreamSynchronize(e->cp);
+    for (auto* b : {&e->Q64, &e->Rinv, &e->tsums, &e->rss0, &e->b0, &e->W, &e->zQ, &e->sinv, &e->sfinv}) b->release();
+    for (auto* b : {&e->Qr, &e->Yraw, &e->Yt, &e->sst, &e->mean, &e->varx, &e->aobs, &e->afull, &e->zA, &e->zD,
+                    &e->cov, &e->cov2, &e->d_beta, &e->d_se, &e->d_t, &e->d_r2, &e->d_sig, &e->Xstage[0],
+                    &e->Xstage[1]})
+        b->release();
+    for (auto* b : {&e->tcounts, &e->pat, &e->zset, &e->nobs, &e->set_off, &e->set_rows, &e->set_rep, &e->set_kind,
+                    &e->set_slot, &e->has_nan, &e->perm, &e->perm2})
+        b->release();
+    e->Yhi.release();
+    e->Ylo.release();
+    e->Xhi.release();
+    e->Xlo.release();
+    e->thash.release();
+    e->counters.release();
+    e->keys.release();
+    e->keys2.release();
+    e->pat_bad.release();
+    e->sing.release();
+    e->rec.release();
+    e->rec2.release();
+    e->cub_tmp.release();
+    for (int b = 0; b < 2; ++b) {
+        cudaEventDestroy(e->ev_copied[b]);
+        cudaEventDestroy(e->ev_used[b]);
+    }
+    cudaEventDestroy(e->k0);
+    cudaEventDestroy(e->k1);
+    cudaStreamDestroy(e->st);
+    cudaStreamDestroy(e->cp);
+    delete e;
+    return OA_OK;
+}
+
+oa_status oa_set_covariates(oa_engine* e, const float* xl) {
+    if (!e || !xl) {
+        set_err("null argument");
+        return OA_ERR_ARG;
+    }
+    OA_CU(cudaSetDevice(e->cfg.device));
+    const int n = e->n, l = e->l;
+    std::vector<double> A((size_t)n * l), Q, R;
+    for (size_t q = 0; q < A.size(); ++q) {
+        if (std::isnan(xl[q])) {
+            set_err("covariate matrix contains NaN (the reader drops such individuals)");
+            return OA_ERR_ARG;
+        }
+        A[q] = xl[q];
+    }
+    householder_qr(A, n, l, Q, R);
+    // rank check: singular values of XL are those of R (src/Algorithm.cpp:508-522)
+    const std::vector<double> sv = singular_values(R, l);
+    for (double s : sv)
+        if (!(s >= 1e-6)) {
+            set_err("the covariate matrix contains linearly dependent columns (singular value %g)", s);
+            return OA_ERR_COLLINEAR;
+        }
+    // R^-1 (upper triangular)
+    std::vector<double> Ri((size_t)l * l, 0.0);
+    for (int i = l - 1; i >= 0; --i) {
+        Ri[(size_t)i * l + i] = 1.0 / R[(size_t)i * l + i];
+        for (int j = i + 1; j < l; ++j) {
+            double s = 0.0;
+            for (int k = i + 1; k <= j; ++k) s += R[(size_t)i * l + k] * Ri[(size_t)k * l + j];
+            Ri[(size_t)i * l + j] = -s / R[(size_t)i * l + i];
+        }
+    }
+    std::vector<float> Qr((size_t)n * e->LP, 0.f);
+    for (int k = 0; k < n; ++k)
+        for (int q = 0; q < l; ++q) Qr[(size_t)k * e->LP + q] = (float)Q[(size_t)q * n + k];
+    OA_CHECK(e->Q64.ensure((size_t)n * l));
+    OA_CHECK(e->Qr.ensure(Qr.size()));
+    OA_CHECK(e->Rinv.ensure((size_t)l * l));
+    OA_CU(cudaMemcpy(e->Q64.p, Q.data(), sizeof(double) * Q.size(), cudaMemcpyHostToDevice));
+    OA_CU(cudaMemcpy(e->Qr.p, Qr.data(), sizeof(float) * Qr.size(), cudaMemcpyHostToDevice));
+    OA_CU(cudaMemcpy(e->Rinv.p, Ri.data(), sizeof(double) * Ri.size(), cudaMemcpyHostToDevice));
+    e->have_cov = true;
+    e->t = 0;
+    return OA_OK;
+}
+
+oa_status oa_set_traits(oa_engine* e, const float* y, int32_t t) {
+    if (!e || !y) {
+        set_err("null argument");
+        return OA_ERR_ARG;
+    }
+    OA_CU(cudaSetDevice(e->cfg.device));
+    return set_traits_impl(e, y, t, false);
+}
+
+oa_status oa_set_traits_device(oa_engine* e, const float* y, int32_t t) {
+    if (!e || !y) {
+        set_err("null argument");
+        return OA_ERR_ARG;
+    }
+    OA_CU(cudaSetDevice(e->cfg.device));
+    return set_traits_impl(e, y, t, true);
+}
+
+oa_status oa_run_snps(oa_engine* e, const float* xr, int32_t mb, oa_rows* out) {
+    return run_snps_any(e, xr, mb, true, true, out);
+}
+
+oa_status oa_run_snps_device(oa_engine* e, const float* xr, int32_t mb, int32_t results_on_host, oa_rows* out) {
+    return run_snps_any(e, xr, mb, false, results_on_host != 0, out);
+}
+
+oa_status oa_enable_dense(oa_engine* e, int32_t on) {
+    if (!e) return OA_ERR_ARG;
+    e->dense_on = on != 0;
+    return OA_OK;
+}
+
+oa_status oa_dense_last(oa_engine* e, float* beta, float* se, float* tstat, float* r2) {
+    if (!e || !e->dense_on || e->last_mb == 0) {
+        set_err("dense output was not enabled for the last SNP block");
+        return OA_ERR_STATE;
+    }
+    OA_CU(cudaSetDevice(e->cfg.device));
+    const size_t nd = (size_t)e->t * e->last_mb;
+    if (beta) OA_CU(cudaMemcpy(beta, e->d_beta.p, sizeof(float) * nd * e->r, cudaMemcpyDeviceToHost));
+    if (se) OA_CU(cudaMemcpy(se, e->d_se.p, sizeof(float) * nd * e->r, cudaMemcpyDeviceToHost));
+    if (tstat) OA_CU(cudaMemcpy(tstat, e->d_t.p, sizeof(float) * nd * e->r, cudaMemcpyDeviceToHost));
+    if (r2) OA_CU(cudaMemcpy(r2, e->d_r2.p, sizeof(float) * nd, cudaMemcpyDeviceToHost));
+    return OA_OK;
+}
+
+int64_t oa_kernel_launches(const oa_engine* e) { return e ? e->launches : 0; }
+
+float oa_last_kernel_ms(const oa_engine* e, const char** name) {
+    if (!e) return 0.f;
+    if (name) *name = e->last_name;
+    return e->last_ms;
+}
+
+}  // extern "C"

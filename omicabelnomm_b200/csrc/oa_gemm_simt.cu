@@ -1,0 +1,30 @@
+// Instantiations of the FP32 SIMT GEMM with fused statistics (see oa_gemm_simt.cuh).
+#include "oa_gemm_simt.cuh"
+#include "oa_launch.h"
+
+namespace oa {
+
+template <int R>
+static cudaError_t go(const float* X, size_t ldx, int xrows, const float* Yt, size_t ldy, int t, int K,
+                      const float* colmean, const int* has_nan, const EpiArgs& E, cudaStream_t st) {
+    dim3 grid((t + SG_BN - 1) / SG_BN, (xrows + SG_BM - 1) / SG_BM);
+    const bool vec = (K % 4 == 0) && (ldx % 4 == 0) && (ldy % 4 == 0) &&
+                     ((reinterpret_cast<uintptr_t>(X) & 15) == 0) && ((reinterpret_cast<uintptr_t>(Yt) & 15) == 0);
+    if (vec)
+        k_gemm_simt<R, true><<<grid, 256, 0, st>>>(X, ldx, xrows, Yt, ldy, t, K, colmean, has_nan, E);
+    else
+        k_gemm_simt<R, false><<<grid, 256, 0, st>>>(X, ldx, xrows, Yt, ldy, t, K, colmean, has_nan, E);
+    return cudaGetLastError();
+}
+
+cudaError_t oa_launch_gemm_simt(int R, const float* X, size_t ldx, int xrows, const float* Yt, size_t ldy, int t,
+                                int K, const float* colmean, const int* has_nan, const EpiArgs& E, cudaStream_t st) {
+    switch (R) {
+        case 1: return go<1>(X, ldx, xrows, Yt, ldy, t, K, colmean, has_nan, E, st);
+        case 2: return go<2>(X, ldx, xrows, Yt, ldy, t, K, colmean, has_nan, E, st);
+        case 4: return go<4>(X, ldx, xrows, Yt, ldy, t, K, colmean, has_nan, E, st);
+        default: return cudaErrorInvalidValue;
+    }
+}
+
+}  // namespace oa

@@ -1,0 +1,123 @@
+// Plain-FP32 form of the dominant contraction, XR' Y~ (≙ the Ay_bot sgemm,
+// src/Algorithm.cpp:705-707), as a SIMT FFMA GEMM with the per-test
+// statistics fused into its epilogue: no SNP x trait matrix is ever written.
+//
+// C[c][j] = sum_k X[c][k] * Y~[j][k]: both operands are K-contiguous (the
+// individual index k is contiguous in a .fvd column).  Tile 128 (SNP
+// columns) x 128 (traits) x 16 (k), 256 threads, 8x8 accumulators per
+// thread, register-staged double buffering through shared memory.
+#pragma once
+#include "oa_epilogue.cuh"
+
+namespace oa {
+
+constexpr int SG_BM = 128, SG_BN = 128, SG_BK = 16, SG_PAD = 4;
+
+template <bool VEC>
+__device__ __forceinline__ void sg_load(const float* __restrict__ P, size_t ld, int nrow, int K,
+                                        int row, int k, const float* __restrict__ mean, bool fix_nan,
+                                        float (&v)[4]) {
+    if (row < nrow) {
+        const float* src = P + (size_t)row * ld + k;
+        if (VEC && k + 3 < K) {
+            const float4 q = __ldg(reinterpret_cast<const float4*>(src));
+            v[0] = q.x; v[1] = q.y; v[2] = q.z; v[3] = q.w;
+        } else {
+#pragma unroll
+            for (int u = 0; u < 4; ++u) v[u] = (k + u < K) ? __ldg(src + u) : 0.f;
+        }
+        if (fix_nan) {
+            const float mv = mean[row];
+#pragma unroll
+            for (int u = 0; u < 4; ++u) v[u] = isnan(v[u]) ? mv : v[u];
+        }
+    } else {
+#pragma unroll
+        for (int u = 0; u < 4; ++u) v[u] = 0.f;
+    }
+}
+
+template <int R, bool VEC>
+__global__ void __launch_bounds__(256, 2)
+k_gemm_simt(const float* __restrict__ X, size_t ldx, int xrows, const float* __restrict__ Yt, size_t ldy,
+            int t, int K, const float* __restrict__ colmean, const int* __restrict__ has_nan, EpiArgs E) {
+    __shared__ __align__(16) float As[2][SG_BK][SG_BM + SG_PAD];
+    __shared__ __align__(16) float Bs[2][SG_BK][SG_BN + SG_PAD];
+    const int tid = threadIdx.x;
+    const int tx = tid & 15, ty = tid >> 4;
+    const int m0 = blockIdx.y * SG_BM;  // first SNP column of the tile
+    const int n0 = blockIdx.x * SG_BN;  // first trait of the tile
+    const int lrow = tid >> 2, lk = (tid & 3) * 4;
+    const bool fix = *has_nan != 0;
+
+    float acc[8][8];
+#pragma unroll
+    for (int i = 0; i < 8; ++i)
+#pragma unroll
+        for (int j = 0; j < 8; ++j) acc[i][j] = 0.f;
+
+    float ra[2][4], rb[2][4];
+    auto gload = [&](int k0) {
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+            sg_load<VEC>(X, ldx, xrows, K, m0 + lrow + 64 * h, k0 + lk, colmean, fix, ra[h]);
+            sg_load<VEC>(Yt, ldy, t, K, n0 + lrow + 64 * h, k0 + lk, colmean, false, rb[h]);
+        }
+    };
+    auto sstore = [&](int buf) {
+#pragma unroll
+        for (int h = 0; h < 2; ++h)
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                As[buf][lk + u][lrow + 64 * h] = ra[h][u];
+                Bs[buf][lk + u][lrow + 64 * h] = rb[h][u];
+            }
+    };
+
+    const int nk = (K + SG_BK - 1) / SG_BK;
+    gload(0);
+    sstore(0);
+    __syncthreads();
+    for (int kt = 0; kt < nk; ++kt) {
+        const int buf = kt & 1;
+        if (kt + 1 < nk) gload((kt + 1) * SG_BK);
+#pragma unroll
+        for (int kk = 0; kk < SG_BK; ++kk) {
+            const float4 a0 = *reinterpret_cast<const float4*>(&As[buf][kk][ty * 4]);
+            const float4 a1 = *reinterpret_cast<const float4*>(&As[buf][kk][64 + ty * 4]);
+            const float4 b0 = *reinterpret_cast<const float4*>(&Bs[buf][kk][tx * 4]);
+            const float4 b1 = *reinterpret_cast<const float4*>(&Bs[buf][kk][64 + tx * 4]);
+            const float a[8] = {a0.x, a0.y, a0.z, a0.w, a1.x, a1.y, a1.z, a1.w};
+            const float b[8] = {b0.x, b0.y, b0.z, b0.w, b1.x, b1.y, b1.z, b1.w};
+#pragma unroll
+            for (int i = 0; i < 8; ++i)
+#pragma unroll
+                for (int j = 0; j < 8; ++j) acc[i][j] = fmaf(a[i], b[j], acc[i][j]);
+        }
+        if (kt + 1 < nk) sstore(buf ^ 1);
+        __syncthreads();
+    }
+
+    // fused epilogue: rows ty*4+{0..3} and 64+ty*4+{0..3}; a SNP's R columns
+    // are consecutive rows held by this thread (R divides 4)
+#pragma unroll
+    for (int half = 0; half < 2; ++half) {
+#pragma unroll
+        for (int sg = 0; sg < 4 / R; ++sg) {
+            const int row0 = m0 + 64 * half + ty * 4 + sg * R;
+            const int i = row0 / R;  // SNP within the block
+#pragma unroll
+            for (int jj = 0; jj < 8; ++jj) {
+                const int j = n0 + (jj < 4 ? tx * 4 + jj : 64 + tx * 4 + (jj - 4));
+                float z[R];
+#pragma unroll
+                for (int a = 0; a < R; ++a) z[a] = acc[half * 4 + sg * R + a][jj];
+                Rec rc;
+                const bool st = epi_eval<R>(E, i, j, z, (row0 < xrows) && (j < t), rc);
+                epi_emit(E, st, rc);
+            }
+        }
+    }
+}
+
+}  // namespace oa

@@ -1,0 +1,736 @@
+// Host side of the drop-in: .fvi/.fvd reading with the reference's row
+// selection, the whole-run driver (oa_solve ≙ Algorithm::solve), the
+// _dis.txt / _sto.ibin / _sto.dbin writers and the CLI (oa_cli_main ≙ main).
+//
+// Reference files followed: src/main.cpp (CLI), src/AIOwrapper.cpp
+// (initialize, exclusion list, removeALmissings, async_io writer),
+// src/Algorithm.cpp:322-886 (block loop, thresholds, hpc_statistics
+// filters), src/Utility.cpp:244-268 (getTvalue, float16 truncation).
+#include <getopt.h>
+#include <sys/stat.h>
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <fstream>
+#include <future>
+#include <sstream>
+#include <string>
+#include <vector>
+
+#include <cuda_runtime.h>
+
+#include "omicabel_b200.h"
+
+extern "C" void oa__set_error(const char* msg);  // oa_engine.cu: shared oa_last_error() text
+
+namespace {
+
+thread_local std::string h_err;
+
+void herr(const char* fmt, ...) {
+    char buf[2048];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof buf, fmt, ap);
+    va_end(ap);
+    h_err = buf;
+    oa__set_error(buf);
+}
+
+constexpr double ONE_OVER_SQRT2 = 0.7071067811865475244008443621048490392848359376884740;
+
+// ---------------------------------------------------------------------------
+// .fvi / .fvd (src/AIOwrapper.h:145-175, src/AIOwrapper.cpp:2294-2317)
+// ---------------------------------------------------------------------------
+struct Fvi {
+    uint16_t type = 0;
+    uint32_t nelements = 0, nobs = 0, nvar = 0, bytes_per_record = 0, bits_per_record = 0, namelength = 0;
+    std::vector<char> names;  // (nobs + nvar) * namelength raw bytes
+    std::string obs_name(size_t i) const { return cstr(i); }
+    std::string var_name(size_t i) const { return cstr(nobs + i); }
+    const char* raw(size_t i) const { return names.data() + i * namelength; }
+    std::string cstr(size_t i) const {
+        const char* p = names.data() + i * namelength;
+        size_t k = 0;
+        while (k < namelength && p[k]) ++k;
+        return std::string(p, k);
+    }
+};
+
+bool read_fvi(const std::string& path, Fvi& f) {
+    FILE* fp = fopen(path.c_str(), "rb");
+    if (!fp) {
+        herr("Error reading file: %s", path.c_str());
+        return false;
+    }
+    unsigned char hdr[48];
+    if (fread(hdr, 1, 48, fp) != 48) {
+        fclose(fp);
+        herr("%s: truncated header", path.c_str());
+        return false;
+    }
+    auto u32 = [&](int off) {
+        uint32_t v;
+        memcpy(&v, hdr + off, 4);
+        return v;
+    };
+    memcpy(&f.type, hdr, 2);
+    f.nelements = u32(4);
+    f.nobs = u32(8);
+    f.nvar = u32(12);
+    f.bytes_per_record = u32(16);
+    f.bits_per_record = u32(20);
+    f.namelength = u32(24);
+    const size_t nb = ((size_t)f.nobs + f.nvar) * f.namelength;
+    f.names.assign(nb, 0);
+    const size_t got = fread(f.names.data(), 1, nb, fp);
+    fclose(fp);
+    if (got != nb) {
+        herr("%s: %zu name bytes, header needs %zu", path.c_str(), got, nb);
+        return false;
+    }
+    // the reference reads every .fvd as float32 and never checks `type`
+    // (src/AIOwrapper.cpp:1103-1125); a non-float layout is refused here
+    if (f.type != 5 || f.bytes_per_record != 4) {
+        herr("%s: data type %u / %u bytes per record: only float32 (type 5) is supported", path.c_str(), f.type,
+             f.bytes_per_record);
+        return false;
+    }
+    return true;
+}
+
+// Kept rows as (start, length) runs, the reference's exclusion list.
+using Runs = std::vector<std::pair<int, int>>;
+
+// src/AIOwrapper.cpp:2146-2233 (read_excludeList): "first [second]" per line,
+// 1-based inclusive; a one-number line leaves `second` unchanged and is read
+// as a single index; reading stops once a range reaches n.
+bool exclusion_rows(const std::string& fname, int n, std::vector<char>& keep, int& excluded, bool verbose) {
+    std::ifstream f(fname.c_str());
+    if (!f) {
+        herr("Error reading exclude list file.");
+        return false;
+    }
+    std::string line;
+    int first = 0, second = 0, prev_second = -1;
+    excluded = 0;
+    if (verbose) printf("Excluding Ids: \n");
+    while (second < n && std::getline(f, line)) {
+        std::istringstream iss(line);
+        int a, b;
+        if (iss >> a) first = a;
+        if (iss >> b) second = b;
+        if (prev_second > first) {
+            herr("Please provide valid positive ordered indixes! %d > %d", prev_second, first);
+            return false;
+        }
+        if (second == prev_second) {
+            if (verbose) printf("%d, ", first);
+            second = first;
+        } else {
+            if (verbose) printf("%d-%d, ", first, second);
+            if (first > second) {
+                herr("Please provide ordered pairs!");
+                return false;
+            }
+            if (first < 1 || second < 1) {
+                herr("Please provide valid positive indixes!");
+                return false;
+            }
+        }
+        prev_second = second;
+        for (int i = first - 1; i <= second - 1; ++i)
+            if (i >= 0 && i < n && keep[i]) {
+                keep[i] = 0;
+                ++excluded;
+            }
+    }
+    if (excluded >= n) {
+        herr("Exclusion List excluded all data! Total Ids: %d Excluded Ids: %d", n, excluded);
+        return false;
+    }
+    if (verbose) printf("Excluded: %d Using: %d\n", excluded, n - excluded);
+    return true;
+}
+
+Runs keep_runs(const std::vector<char>& keep) {
+    Runs r;
+    const int n = (int)keep.size();
+    for (int i = 0; i < n;) {
+        if (!keep[i]) {
+            ++i;
+            continue;
+        }
+        int j = i;
+        while (j < n && keep[j]) ++j;
+        r.emplace_back(i, j - i);
+        i = j;
+    }
+    return r;
+}
+
+// Read variables [v0, v0+count) of a .fvd file, keeping only the rows in
+// `runs`, into dst (count columns of `kept` floats each).
+bool read_columns(FILE* fp, size_t fileN, size_t v0, size_t count, const Runs& runs, size_t kept, float* dst,
+                  std::vector<float>& scratch) {
+    const bool all = runs.size() == 1 && runs[0].first == 0 && (size_t)runs[0].second == fileN;
+    const size_t bytes = sizeof(float) * fileN * count;
+    if (fseeko(fp, (off_t)(sizeof(float) * fileN * v0), SEEK_SET) != 0) return false;
+    if (all) return fread(dst, 1, bytes, fp) == bytes;
+    scratch.resize(fileN * count);
+    if (fread(scratch.data(), 1, bytes, fp) != bytes) return false;
+    for (size_t c = 0; c < count; ++c) {
+        const float* src = scratch.data() + c * fileN;
+        float* out = dst + c * kept;
+        size_t pos = 0;
+        for (const auto& run : runs) {
+            memcpy(out + pos, src + run.first, sizeof(float) * run.second);
+            pos += run.second;
+        }
+    }
+    return true;
+}
+
+// ---------------------------------------------------------------------------
+// statistics helpers shared with the writer
+// ---------------------------------------------------------------------------
+long double pvalue_ld(float tf) {
+    // src/Algorithm.cpp:1159-1167: t is the float |b/SE| held in a long double
+    const long double t = (long double)tf;
+    if (t < 1.6) {
+        const float t1 = (float)(4.4 - t);
+        return 0.5 - (long double)(0.1 * (double)t1) * t;
+    }
+    return erfcl(t * (long double)ONE_OVER_SQRT2);
+}
+
+long double erf_inv_ld(long double z) {
+    // Newton's method on erfl(x) - z, started from Winitzki's closed form
+    if (z <= -1.0L) return -HUGE_VALL;
+    if (z >= 1.0L) return HUGE_VALL;
+    if (z == 0.0L) return 0.0L;
+    const long double a = 0.147L, pi = 3.141592653589793238462643383279502884L;
+    const long double ln = logl(1.0L - z * z);
+    const long double t1 = 2.0L / (pi * a) + ln / 2.0L;
+    long double x = sqrtl(sqrtl(t1 * t1 - ln / a) - t1);
+    if (z < 0) x = -x;
+    const long double c = 2.0L / sqrtl(pi);
+    for (int it = 0; it < 100; ++it) {
+        const long double step = (erfl(x) - z) / (c * expl(-x * x));
+        x -= step;
+        if (fabsl(step) <= 1e-19L * (1.0L + fabsl(x))) break;
+    }
+    return x;
+}
+
+uint16_t float16_trunc(float v) {
+    // top 16 bits of the IEEE bits (src/Utility.cpp:261-268)
+    uint32_t u;
+    memcpy(&u, &v, 4);
+    return (uint16_t)(u >> 16);
+}
+
+// ---------------------------------------------------------------------------
+// output writer (≙ async_io's write loop, src/AIOwrapper.cpp:1440-1558)
+// ---------------------------------------------------------------------------
+struct Writer {
+    FILE* dis = nullptr;
+    FILE* dbin = nullptr;
+    bool store_bin = false, store_all = false, disp_cov = false;
+    long double min_p_disp = 0;
+    float min_r2_disp = 0;
+    int l = 0, r = 0, p = 0, real_n = 0, mb_ref = 500;
+    const Fvi* fy = nullptr;
+    const Fvi* fl = nullptr;
+    const Fvi* fr = nullptr;
+    uint64_t total_sig = 0;
+    int64_t rows_written = 0;
+    std::string buf;
+
+    // One reference write block: rows of one trait block x one reference SNP
+    // block, in (trait, SNP) order; snp indices are global.
+    void write_block(const oa_rows& rr, const std::vector<int64_t>& idx, int trait_base, int ar_offset_snps) {
+        if (idx.empty()) return;
+        if (dbin && !store_all) {
+            const int32_t yname = trait_base + rr.trait[idx[0]];
+            const int32_t cnt = (int32_t)idx.size();
+            const int32_t aroff = ar_offset_snps * r;
+            fwrite(&yname, 4, 1, dbin);
+            fwrite(&cnt, 4, 1, dbin);
+            fwrite(&aroff, 4, 1, dbin);
+        }
+        const int start_h = disp_cov ? 1 : l;
+        char line[1024];
+        for (int64_t q : idx) {
+            const int ytr = trait_base + rr.trait[q];
+            const int snp = rr.snp[q];
+            const int ii = snp - ar_offset_snps;
+            const uint32_t mask = rr.coef_mask[q];
+            const int nused_i = rr.n_used[q];
+            const uint16_t nused = (uint16_t)nused_i;
+            const float npct = (float)nused_i / (float)real_n;
+            const float r2 = rr.r2[q];
+            if (dbin) {
+                const uint16_t r2h = float16_trunc(r2);
+                fwrite(&nused, 2, 1, dbin);
+                fwrite(&r2h, 2, 1, dbin);
+                if (!store_all) {
+                    uint8_t sz = 0;
+                    for (int h = p - 1; h >= start_h; --h) sz += (mask >> h) & 1u;
+                    fwrite(&sz, 1, 1, dbin);
+                }
+            }
+            for (int h = p - 1; h >= start_h; --h) {
+                if (!((mask >> h) & 1u)) continue;
+                const float B = rr.coef_b[(size_t)q * p + h];
+                const float SE = rr.coef_se[(size_t)q * p + h];
+                const float T = rr.coef_t[(size_t)q * p + h];
+                const long double P = pvalue_ld(T);
+                if (min_p_disp > P) ++total_sig;
+                const int ar_idx = ii * r + (h >= l ? h - l : 0);
+                const uint8_t al_idx = h >= l ? (uint8_t)255 : (uint8_t)h;
+                if ((P <= min_p_disp && r2 >= min_r2_disp) || store_all) {
+                    std::string aname = " ";
+                    if (h < l) aname = fl->var_name(h) + ":";
+                    aname += fr->var_name((size_t)ar_offset_snps * r + ar_idx);
+                    const int len = snprintf(line, sizeof line, "%s\t%s\t%u\t%.2f\t%.7f\t%.4f\t%.7f\t%.7f\t%.7Le\n",
+                                             fy->var_name(ytr).c_str(), aname.c_str(), (unsigned)nused,
+                                             (double)npct, (double)B, (double)r2, (double)SE, (double)T, P);
+                    buf.append(line, (size_t)len);
+                    ++rows_written;
+                }
+                if (dbin) {
+                    if (disp_cov && !store_all) fwrite(&al_idx, 1, 1, dbin);
+                    if (!store_all) {
+                        const uint16_t a16 = (uint16_t)ar_idx;
+                        fwrite(&a16, 2, 1, dbin);
+                    }
+                    fwrite(&B, 4, 1, dbin);
+                    fwrite(&SE, 4, 1, dbin);
+                }
+            }
+            if (buf.size() > (1u << 22)) flush();
+        }
+    }
+    void flush() {
+        if (!buf.empty()) fwrite(buf.data(), 1, buf.size(), dis);
+        buf.clear();
+    }
+};
+
+}  // namespace
+
+extern "C" {
+
+long double oa_pvalue(float t) { return pvalue_ld(t); }
+
+float oa_t_threshold(float p) {
+    // src/Utility.cpp:244-250: erf_inv(1 - p) * sqrt(2), evaluated in long double
+    return (float)(erf_inv_ld((long double)(1.0 - (double)p)) * sqrt(2.0));
+}
+
+void oa_default_settings(oa_settings* s) {
+    memset(s, 0, sizeof *s);
+    s->r = 1;
+    s->min_r2_store = 0.00001f;
+    s->min_r2_disp = 0.000001f;
+    s->min_p_store = 0.1f;
+    s->min_p_disp = 0.05f;
+    s->precision = OA_PLAIN_FP32;
+    s->device = 0;
+}
+
+oa_status oa_solve(const oa_settings* S, oa_outputs* out) {
+    if (!S || !out) {
+        herr("null argument");
+        return OA_ERR_ARG;
+    }
+    memset(out, 0, sizeof *out);
+    const auto t_start = std::chrono::steady_clock::now();
+    const bool verbose = S->verbose != 0;
+    // threshold coupling (src/Algorithm.cpp:338-342)
+    float min_r2_store = S->min_r2_store, min_p_store = S->min_p_store;
+    if (S->min_r2_disp < min_r2_store || S->store_bin) min_r2_store = S->min_r2_disp;
+    if (S->min_p_disp > min_p_store || S->store_bin) min_p_store = S->min_p_disp;
+    const float min_t_store = oa_t_threshold(min_p_store);
+
+    const std::string fxl = S->fname_xl ? S->fname_xl : "", fxr = S->fname_xr ? S->fname_xr : "",
+                      fy = S->fname_y ? S->fname_y : "", fout = S->fname_out ? S->fname_out : "";
+    Fvi FL, FR, FY;
+    if (!read_fvi(fy + ".fvi", FY) || !read_fvi(fxl + ".fvi", FL) || !read_fvi(fxr + ".fvi", FR)) return OA_ERR_IO;
+    if (FL.nobs != FR.nobs || FR.nobs != FY.nobs) {
+        // the reference only stops when all three differ (src/AIOwrapper.cpp:72-85); any mismatch is an error here
+        herr("The number of elements/individuals from the input files do not coincide with each other! %s:%u %s:%u "
+             "%s:%u",
+             fy.c_str(), FY.nobs, fxl.c_str(), FL.nobs, fxr.c_str(), FR.nobs);
+        return OA_ERR_IO;
+    }
+    const int r = std::max(1, S->r);
+    const int fileN = (int)FL.nobs;
+    if (FR.nvar % r != 0) {
+        herr("Number of elements in %s.fvi:%u is not consistent with the value of --ngpred (-n)%d provided",
+             fxr.c_str(), FR.nvar, r);
+        return OA_ERR_IO;
+    }
+    const int m = (int)(FR.nvar / r), t = (int)FY.nvar, l = (int)FL.nvar, p = l + r;
+    if (l < 1 || l > OA_MAX_L) {
+        herr("%d covariates: this build supports 1..%d", l, OA_MAX_L);
+        return OA_ERR_UNSUPPORTED;
+    }
+    // ID order checks (warnings only, as in the reference, src/AIOwrapper.cpp:148-191)
+    for (int i = 0; i < fileN; ++i) {
+        const std::string a = FY.obs_name(i), b = FL.obs_name(i), c = FR.obs_name(i);
+        if (a != b || a != c) {
+            if (verbose)
+                printf("Warning, ID names between input files do not coincide! The files must have the same "
+                       "meaningful order\n");
+            break;
+        }
+    }
+    // row selection: exclusion list, then rows with a NaN covariate (src/AIOwrapper.cpp:229-253, 1947-1991)
+    std::vector<char> keep(fileN, 1);
+    int excl = 0;
+    if (S->fname_exclude && S->fname_exclude[0])
+        if (!exclusion_rows(S->fname_exclude, fileN, keep, excl, verbose)) return OA_ERR_IO;
+    std::vector<float> xl_all((size_t)fileN * l);
+    {
+        FILE* fp = fopen((fxl + ".fvd").c_str(), "rb");
+        if (!fp) {
+            herr("Error Reading File %s", fxl.c_str());
+            return OA_ERR_IO;
+        }
+        const size_t got = fread(xl_all.data(), sizeof(float), xl_all.size(), fp);
+        fclose(fp);
+        if (got != xl_all.size()) {
+            herr("%s.fvd: short read", fxl.c_str());
+            return OA_ERR_IO;
+        }
+    }
+    int almiss = 0;
+    for (int h = 0; h < l; ++h)
+        for (int i = 0; i < fileN; ++i)
+            if (std::isnan(xl_all[(size_t)h * fileN + i]) && keep[i]) {
+                keep[i] = 0;
+                ++almiss;
+            }
+    if (almiss > 0 && verbose) printf("Excluding %d from covariate missings\n", almiss);
+    const Runs runs = keep_runs(keep);
+    const int n = fileN - excl - almiss;
+    if (p >= n) {
+        herr("Error! The amount of unknows (individuals|elements) must be greater than total of variables "
+             "(#covariates+#ind.variables)!");
+        return OA_ERR_ARG;
+    }
+    if ((l > 255 || p > 255 || n > 65535) && verbose)
+        printf("Warning, output binary format does not yet support current problem sizes for the provided p, l, r "
+               "and n.\n");
+    std::vector<float> XL((size_t)n * l);
+    for (int h = 0; h < l; ++h) {
+        size_t pos = 0;
+        for (const auto& run : runs) {
+            memcpy(&XL[(size_t)h * n + pos], &xl_all[(size_t)h * fileN + run.first], sizeof(float) * run.second);
+            pos += run.second;
+        }
+    }
+    xl_all.clear();
+    xl_all.shrink_to_fit();
+
+    // outputs
+    Writer W;
+    W.store_bin = S->store_bin;
+    W.store_all = S->store_all;
+    W.disp_cov = S->disp_cov;
+    W.min_p_disp = (long double)S->min_p_disp;
+    W.min_r2_disp = S->min_r2_disp;
+    W.l = l;
+    W.r = r;
+    W.p = p;
+    W.real_n = fileN;
+    W.fy = &FY;
+    W.fl = &FL;
+    W.fr = &FR;
+    W.dis = fopen((fout + "_dis.txt").c_str(), "wb");
+    if (!W.dis) {
+        herr("Error Creating File %s_dis.txt", fout.c_str());
+        return OA_ERR_IO;
+    }
+    fputs("Phe\tSNP\tn\tnPct\tB\tR2\tSE\tT\tP\n", W.dis);
+    if (S->store_bin) {
+        // _sto.ibin (src/AIOwrapper.cpp:679-733)
+        FILE* fi = fopen((fout + "_sto.ibin").c_str(), "wb");
+        if (!fi) {
+            herr("Error Creating File: %s_sto.ibin", fout.c_str());
+            fclose(W.dis);
+            return OA_ERR_IO;
+        }
+        const int32_t hdr[6] = {n, l, r, t, m, (int32_t)FR.namelength};
+        fwrite(hdr, 4, 6, fi);
+        const uint8_t flags[2] = {(uint8_t)(S->disp_cov ? 1 : 0), (uint8_t)(S->store_all ? 1 : 0)};
+        fwrite(flags, 1, 2, fi);
+        fwrite(FL.raw((size_t)FL.nobs + 1), 1, (size_t)FL.namelength * (l - 1), fi);
+        fwrite(FR.raw(FR.nobs), 1, (size_t)FR.namelength * r * m, fi);
+        fwrite(FY.raw(FY.nobs), 1, (size_t)FY.namelength * t, fi);
+        fclose(fi);
+        W.dbin = fopen((fout + "_sto.dbin").c_str(), "wb");
+        if (!W.dbin) {
+            herr("Error Creating File %s_sto.dbin", fout.c_str());
+            fclose(W.dis);
+            return OA_ERR_IO;
+        }
+    }
+
+    // engine: one trait block of the reference's size at a time (tb = min(t, 1000))
+    const int tb = std::min(t, 1000);
+    const int mb_ref = std::min(m, 500);
+    W.mb_ref = mb_ref;
+    // SNPs per engine call: a multiple of the reference block, about 1 GB of genotypes
+    int call_snps = (int)std::max<int64_t>(1, (int64_t)(1u << 28) / ((int64_t)n * r));
+    call_snps = std::max(mb_ref, call_snps / mb_ref * mb_ref);
+    call_snps = std::min(call_snps, m);
+    oa_config cfg{};
+    cfg.n = n;
+    cfg.l = l;
+    cfg.r = r;
+    cfg.max_traits = tb;
+    cfg.max_snps = call_snps;
+    cfg.precision = S->precision;
+    cfg.device = S->device;
+    cfg.disp_cov = S->disp_cov;
+    cfg.store_all = S->store_all;
+    cfg.quirk_r2 = S->quirk_r2;
+    cfg.min_r2_store = min_r2_store;
+    cfg.min_t_store = min_t_store;
+    cfg.min_p_disp = S->min_p_disp;
+    cfg.real_n = fileN;
+    oa_engine* eng = nullptr;
+    oa_status st = oa_engine_create(&cfg, &eng);
+    if (st != OA_OK) {
+        herr("%s", oa_last_error());
+        fclose(W.dis);
+        if (W.dbin) fclose(W.dbin);
+        return st;
+    }
+    auto fail = [&](oa_status s) {
+        herr("%s", oa_last_error());
+        oa_engine_destroy(eng);
+        W.flush();
+        fclose(W.dis);
+        if (W.dbin) fclose(W.dbin);
+        return s;
+    };
+    st = oa_set_covariates(eng, XL.data());
+    if (st != OA_OK) return fail(st);
+
+    FILE* fr = fopen((fxr + ".fvd").c_str(), "rb");
+    FILE* fyd = fopen((fy + ".fvd").c_str(), "rb");
+    if (!fr || !fyd) {
+        if (fr) fclose(fr);
+        if (fyd) fclose(fyd);
+        herr("Error opening File %s", !fr ? fxr.c_str() : fy.c_str());
+        oa_engine_destroy(eng);
+        fclose(W.dis);
+        if (W.dbin) fclose(W.dbin);
+        return OA_ERR_IO;
+    }
+    // pinned double buffers for the SNP blocks (copied with cudaMemcpyAsync by the engine)
+    float* pin[2] = {nullptr, nullptr};
+    const size_t pin_floats = (size_t)call_snps * r * n;
+    for (int b = 0; b < 2; ++b)
+        if (cudaMallocHost(&pin[b], sizeof(float) * pin_floats) != cudaSuccess) {
+            cudaGetLastError();
+            pin[b] = (float*)malloc(sizeof(float) * pin_floats);
+        }
+    std::vector<float> scratch[2];
+    std::vector<float> Yblk, yscratch;
+    int64_t tests = 0, singular = 0;
+    uint64_t sig_cov = 0;
+    bool io_ok = true;
+    const int ncalls = (m + call_snps - 1) / call_snps;
+    for (int y0 = 0; y0 < t && st == OA_OK && io_ok; y0 += tb) {
+        const int tcur = std::min(tb, t - y0);
+        Yblk.resize((size_t)tcur * n);
+        if (!read_columns(fyd, fileN, y0, tcur, runs, n, Yblk.data(), yscratch)) {
+            herr("Error reading file %s.fvd", fy.c_str());
+            io_ok = false;
+            break;
+        }
+        st = oa_set_traits(eng, Yblk.data(), tcur);
+        if (st != OA_OK) break;
+        auto read_call = [&](int c, int b) {
+            const int s0 = c * call_snps, cnt = std::min(call_snps, m - s0);
+            return read_columns(fr, fileN, (size_t)s0 * r, (size_t)cnt * r, runs, n, pin[b], scratch[b]);
+        };
+        std::future<bool> next = std::async(std::launch::async, read_call, 0, 0);
+        for (int c = 0; c < ncalls; ++c) {
+            if (!next.get()) {
+                herr("Error reading AR File %s.fvd", fxr.c_str());
+                io_ok = false;
+                break;
+            }
+            const int b = c & 1;
+            const int s0 = c * call_snps, cnt = std::min(call_snps, m - s0);
+            if (c + 1 < ncalls) next = std::async(std::launch::async, read_call, c + 1, b ^ 1);
+            oa_rows rows{};
+            st = oa_run_snps(eng, pin[b], cnt, &rows);
+            if (st != OA_OK) {
+                if (c + 1 < ncalls) next.wait();
+                break;
+            }
+            tests += rows.tests;
+            singular += rows.singular;
+            sig_cov += (uint64_t)rows.sig_cov_unrowed;
+            // split into the reference's SNP blocks (rows are in (trait, SNP) order)
+            const int nblk = (cnt + mb_ref - 1) / mb_ref;
+            std::vector<std::vector<int64_t>> blocks(nblk);
+            for (int64_t q = 0; q < rows.count; ++q) blocks[rows.snp[q] / mb_ref].push_back(q);
+            std::vector<int32_t> gsnp(rows.count);
+            for (int64_t q = 0; q < rows.count; ++q) gsnp[q] = rows.snp[q] + s0;
+            oa_rows g = rows;
+            g.snp = gsnp.data();
+            for (int k = 0; k < nblk; ++k) W.write_block(g, blocks[k], y0, s0 + k * mb_ref);
+            if (verbose) {
+                putchar('*');
+                fflush(stdout);
+            }
+        }
+    }
+    fclose(fr);
+    fclose(fyd);
+    for (int b = 0; b < 2; ++b) {
+        if (cudaFreeHost(pin[b]) != cudaSuccess) {
+            cudaGetLastError();
+            free(pin[b]);
+        }
+    }
+    W.flush();
+    fclose(W.dis);
+    if (W.dbin) fclose(W.dbin);
+    oa_engine_destroy(eng);
+    if (!io_ok) return OA_ERR_IO;
+    if (st != OA_OK) {
+        if (h_err.empty()) herr("%s", oa_last_error());
+        return st;
+    }
+    out->total_sig_results = W.total_sig + sig_cov;
+    out->tests = tests;
+    out->singular = singular;
+    out->rows_written = W.rows_written;
+    out->duration_s = std::chrono::duration<double>(std::chrono::steady_clock::now() - t_start).count();
+    return OA_OK;
+}
+
+// ---------------------------------------------------------------------------
+// CLI (src/main.cpp:102-437)
+// ---------------------------------------------------------------------------
+static const char* kHelp =
+    "usage: omicabelnomm -c <path/fname> --geno <path/fname> -p <path/fname> -o <path/fname> -x <path/fname> "
+    "-n <#SNPcols> -t <#CPUs> -d <0.0~1.0> -r <-10.0~1.0> -b -s <0.0~1.0> -e <-10.0~1.0> -i -f\n"
+    "  -p --phe     phenotypes (.fvi/.fvd)      -g --geno   genotypes\n"
+    "  -c --cov     covariates                  -o --out    output prefix\n"
+    "  -n --ngpred  columns per SNP             -t --thr    host threads (accepted, unused)\n"
+    "  -x --excl    exclusion list              -b --stobin also write _sto.ibin/_sto.dbin\n"
+    "  -d --pdisp   display P threshold         -s --psto   store P threshold\n"
+    "  -r --rdisp   display R2 threshold        -e --rsto   store R2 threshold\n"
+    "  -i --fdcov   include covariate terms      -f --fdgen  store every result\n"
+    "  --precision plain|mixed   --device <ordinal>   --quirk-r2\n";
+
+static std::string strip_ext(const char* a) {
+    std::string s(a);
+    const size_t pos = s.find_last_of('.');
+    if (pos != std::string::npos) s = s.substr(0, pos);
+    return s;
+}
+
+int oa_cli_main(int argc, char** argv) {
+    oa_settings S;
+    oa_default_settings(&S);
+    S.verbose = 1;
+    std::string fy, fr, fl, fo, fx;
+    bool phe = false, snp = false, cov = false, bout = false;
+    static struct option opts[] = {{"phe", required_argument, 0, 'p'},
+                                   {"geno", required_argument, 0, 'g'},
+                                   {"cov", required_argument, 0, 'c'},
+                                   {"out", required_argument, 0, 'o'},
+                                   {"ngpred", required_argument, 0, 'n'},
+                                   {"thr", required_argument, 0, 't'},
+                                   {"mem", required_argument, 0, 'm'},
+                                   {"excl", required_argument, 0, 'x'},
+                                   {"stobin", no_argument, 0, 'b'},
+                                   {"pdisp", required_argument, 0, 'd'},
+                                   {"psto", required_argument, 0, 's'},
+                                   {"rdisp", required_argument, 0, 'r'},
+                                   {"rsto", required_argument, 0, 'e'},
+                                   {"fdcov", no_argument, 0, 'i'},
+                                   {"fdgen", no_argument, 0, 'f'},
+                                   {"additive", no_argument, 0, 'j'},
+                                   {"dominant", no_argument, 0, 'k'},
+                                   {"recessive", no_argument, 0, 'l'},
+                                   {"mylinear", required_argument, 0, 'z'},
+                                   {"myaddit", required_argument, 0, 'y'},
+                                   {"simpleinter", required_argument, 0, 'v'},
+                                   {"multinter", required_argument, 0, 'w'},
+                                   {"keepinter", no_argument, 0, 'u'},
+                                   {"help", no_argument, 0, 'h'},
+                                   {"precision", required_argument, 0, 1000},
+                                   {"device", required_argument, 0, 1001},
+                                   {"quirk-r2", no_argument, 0, 1002},
+                                   {0, 0, 0, 0}};
+    optind = 1;
+    int c, idx = 0;
+    while ((c = getopt_long(argc, argv, "c:p:g:o:n:t:m:x:d:s:r:e:z:y:v:w:ufibhjkl", opts, &idx)) != -1) {
+        switch (c) {
+            case 'p': phe = !phe; fy = strip_ext(optarg); printf("-p Reading phenotypes from file %s\n", optarg); break;
+            case 'g': snp = !snp; fr = strip_ext(optarg); printf("-g Reading with genotype data from file %s\n", optarg); break;
+            case 'c': cov = !cov; fl = strip_ext(optarg); printf("-c Reading covariates from file %s\n", optarg); break;
+            case 'o': bout = !bout; fo = strip_ext(optarg); printf("-o Writing output files to %s\n", optarg); break;
+            case 'n': S.r = std::max(atoi(optarg), 1); printf("-n Using columns per snp as %d\n", S.r); break;
+            case 't': break;   // host threads: the GPU engine does not use them
+            case 'm': break;   // --mem: accepted (the reference has no handler for it)
+            case 'x': fx = optarg; printf("-x Excluding ids on %s\n", optarg); break;
+            case 'd': S.min_p_disp = (float)fabs(atof(optarg)); break;
+            case 's': S.min_p_store = (float)fabs(atof(optarg)); break;
+            case 'r': S.min_r2_disp = (float)atof(optarg); break;
+            case 'e': S.min_r2_store = (float)atof(optarg); break;
+            case 'i': S.disp_cov = 1; break;
+            case 'f': S.store_all = 1; break;
+            case 'b': S.store_bin = 1; break;
+            case 'j': case 'k': case 'l': case 'z': case 'y': case 'v': case 'w': case 'u':
+                fprintf(stdout, "option -%c (dosage models / interaction files) is not supported by this build\n", c);
+                return 1;
+            case 'h': fputs(kHelp, stdout); return 1;
+            case 1000:
+                if (!strcmp(optarg, "plain")) S.precision = OA_PLAIN_FP32;
+                else if (!strcmp(optarg, "mixed")) S.precision = OA_MIXED_BF16X3;
+                else { printf("--precision must be plain or mixed\n"); return 1; }
+                break;
+            case 1001: S.device = atoi(optarg); break;
+            case 1002: S.quirk_r2 = 1; break;
+            case '?': break;
+            default: return 1;
+        }
+    }
+    if (!bout || !phe || !cov || !snp) {
+        printf("Missing arguments! p:%d g:%d c:%d o:%d\n", phe, snp, cov, bout);
+        return 1;
+    }
+    S.fname_y = fy.c_str();
+    S.fname_xr = fr.c_str();
+    S.fname_xl = fl.c_str();
+    S.fname_out = fo.c_str();
+    S.fname_exclude = fx.empty() ? nullptr : fx.c_str();
+    printf("omicabelnomm-b200\n");
+    oa_outputs out;
+    const oa_status st = oa_solve(&S, &out);
+    if (st != OA_OK) {
+        printf("\n%s\n", h_err.c_str());
+        return 1;
+    }
+    printf("\nNumber of Significant Results: %llu\n\n", (unsigned long long)out.total_sig_results);
+    return 0;
+}
+
+}  // extern "C"

@@ -1,0 +1,30 @@
+// Instantiations of the per-SNP statistics kernel (see oa_kernels.cuh).
+#include "oa_stats.cuh"
+#include "oa_launch.h"
+
+namespace oa {
+
+template <int R, int LP>
+static cudaError_t go(const StatsArgs& A, int grid, size_t smem, cudaStream_t st) {
+    cudaError_t e = cudaFuncSetAttribute(k_snp_stats<R, LP>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    k_snp_stats<R, LP><<<grid, OA_NTHREADS, smem, st>>>(A);
+    return cudaGetLastError();
+}
+
+cudaError_t oa_launch_snp_stats(int R, int LP, const StatsArgs& A, int grid, size_t smem, cudaStream_t st) {
+    switch (R * 100 + LP) {
+        case 104: return go<1, 4>(A, grid, smem, st);
+        case 108: return go<1, 8>(A, grid, smem, st);
+        case 116: return go<1, 16>(A, grid, smem, st);
+        case 204: return go<2, 4>(A, grid, smem, st);
+        case 208: return go<2, 8>(A, grid, smem, st);
+        case 216: return go<2, 16>(A, grid, smem, st);
+        case 404: return go<4, 4>(A, grid, smem, st);
+        case 408: return go<4, 8>(A, grid, smem, st);
+        case 416: return go<4, 16>(A, grid, smem, st);
+        default: return cudaErrorInvalidValue;
+    }
+}
+
+}  // namespace oa

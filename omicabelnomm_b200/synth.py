@@ -214,3 +214,68 @@ def write_dataset(ds: Dataset, prefix: str) -> dict:
     fvformat.write_fv(paths["XR"], ds.XR, ds.obs, ds.xr_names)
     fvformat.write_fv(paths["Y"], ds.Y, ds.obs, ds.y_names)
     return paths
+
+
+def generate_device(w: Workload, device, seed_offset: int = 0, snp_chunk: int = 32768):
+    """Draw a workload directly in device memory with torch (for full-size runs).
+
+    Same distributions as ``generate`` (different random stream).  Returns
+    (XL (l, n), XR (m*r, n), Y (t, n)) float32 CUDA tensors, plus the pattern
+    of each trait.  Used by the benchmark, where numpy on the host would take
+    minutes for the 20 GB genotype matrix.
+    """
+    import torch
+    g = torch.Generator(device=device)
+    g.manual_seed(w.seed * 1000003 + seed_offset)
+    n, m, t, r = w.n, w.m, w.t, w.r
+    f32 = torch.float32
+    cols = [torch.ones(n, device=device), (torch.rand(n, generator=g, device=device) < 0.5).to(f32),
+            50.0 + 10.0 * torch.randn(n, generator=g, device=device)]
+    npc = w.l - 3 - (1 if w.collinear else 0)
+    for _ in range(max(0, npc)):
+        cols.append(torch.randn(n, generator=g, device=device))
+    if w.collinear:
+        cols.append(cols[2] + 1e-3 * torch.randn(n, generator=g, device=device))
+    XL = torch.stack(cols[: w.l]).contiguous()
+    maf = w.maf_lo + (w.maf_hi - w.maf_lo) * torch.rand(m, generator=g, device=device)
+    if w.low_maf_frac > 0:
+        k = int(round(w.low_maf_frac * m))
+        idx = torch.randperm(m, generator=g, device=device)[:k]
+        maf[idx] = 0.005 + 0.005 * torch.rand(k, generator=g, device=device)
+    XR = torch.empty((m * r, n), dtype=f32, device=device)
+    for c0 in range(0, m, snp_chunk):
+        c1 = min(m, c0 + snp_chunk)
+        p = maf[c0:c1, None]
+        x = (torch.rand((c1 - c0, n), generator=g, device=device) < p).to(f32)
+        x += (torch.rand((c1 - c0, n), generator=g, device=device) < p).to(f32)
+        x += 0.1 * torch.rand((c1 - c0, n), generator=g, device=device) - 0.05
+        x = torch.round(x.clamp_(0.0, 2.0) * 1000.0) / 1000.0
+        if r == 1:
+            XR[c0:c1] = x
+        else:
+            XR[2 * c0:2 * c1:2] = x * XL[1][None, :]
+            XR[2 * c0 + 1:2 * c1:2] = x
+        del x
+    causal = torch.arange(t, device=device) % m
+    b = torch.randn((t, w.l), generator=g, device=device)
+    noise = torch.sqrt(w.noise_lo + (w.noise_hi - w.noise_lo) * torch.rand(t, generator=g, device=device))
+    xc = XR[causal * r + (r - 1)]
+    Y = b @ XL + w.effect * xc + torch.randn((t, n), generator=g, device=device) * noise[:, None]
+    pattern = None
+    if w.miss_mode == "patterns":
+        G = w.n_patterns
+        if w.zipf > 0:
+            rng = np.random.Generator(np.random.PCG64(w.seed + seed_offset))
+            sizes = _zipf_sizes(rng, G, t, w.zipf, w.group_max or t)
+            pat = np.repeat(np.arange(G), sizes)
+            rng.shuffle(pat)
+            pattern = torch.as_tensor(pat, device=device)
+        else:
+            pattern = torch.randint(0, G, (t,), generator=g, device=device)
+        frac = w.miss_hi * torch.rand(G, generator=g, device=device)
+        miss = torch.rand((G, n), generator=g, device=device) < frac[:, None]
+        Y = torch.where(miss[pattern], torch.full_like(Y, float("nan")), Y)
+    elif w.miss_mode == "uniform":
+        miss = torch.rand((t, n), generator=g, device=device) < w.miss_frac
+        Y = torch.where(miss, torch.full_like(Y, float("nan")), Y)
+    return XL, XR, Y.contiguous(), pattern
