@@ -191,6 +191,13 @@ class Engine:
         _check(lib().oa_run_snps(self.h, _fptr(XR), XR.shape[0] // self.r, C.byref(rows)))
         return self._rows(rows)
 
+    def run_raw(self, XR: np.ndarray) -> Rows:
+        """Like run() but returns the C struct (host pointers owned by the engine, no copies)."""
+        assert XR.dtype == np.float32 and XR.flags.c_contiguous and XR.shape[1] == self.n
+        rows = Rows()
+        _check(lib().oa_run_snps(self.h, _fptr(XR), XR.shape[0] // self.r, C.byref(rows)))
+        return rows
+
     def run_device(self, ptr: int, mb: int, results_on_host: bool = False) -> Rows:
         rows = Rows()
         _check(lib().oa_run_snps_device(self.h, C.c_void_p(ptr), mb, int(results_on_host), C.byref(rows)))
