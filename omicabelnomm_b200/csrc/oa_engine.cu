@@ -14,6 +14,7 @@
 #include <cstring>
 #include <map>
 #include <string>
+#include <thread>
 #include <tuple>
 #include <vector>
 
@@ -79,6 +80,23 @@ struct DBuf {
 };
 
 int pad_l(int l) { return l <= 4 ? 4 : (l <= 8 ? 8 : 16); }
+
+// Grow a pinned host buffer (page-locked so the device-to-host copy runs at full speed).
+template <class T>
+oa_status ensure_pinned(T*& p, size_t& cap, size_t want) {
+    if (want <= cap && p) return OA_OK;
+    if (p) cudaFreeHost(p);
+    p = nullptr;
+    cap = 0;
+    const size_t n = std::max<size_t>(want + want / 4, 1024);
+    if (cudaMallocHost(reinterpret_cast<void**>(&p), n * sizeof(T)) != cudaSuccess) {
+        cudaGetLastError();
+        set_err("pinned host allocation of %zu bytes failed", n * sizeof(T));
+        return OA_ERR_NOMEM;
+    }
+    cap = n;
+    return OA_OK;
+}
 
 // Householder QR of the n x l column-major matrix A (FP64): Q (n x l,
 // column-major, orthonormal columns) and R (l x l, row-major upper
@@ -207,9 +225,11 @@ struct oa_engine {
     DBuf<float> d_beta, d_se, d_t, d_r2, d_sig;
     long long dense_ld = 0;
     int last_mb = 0;
-    // host results
-    std::vector<Rec> h_rec;
-    std::vector<float> h_cov;
+    // host results (pinned staging for the device-to-host copy)
+    Rec* h_rec = nullptr;
+    size_t h_rec_cap = 0;
+    float* h_cov = nullptr;
+    size_t h_cov_cap = 0;
     std::vector<int32_t> o_trait, o_snp, o_nused;
     std::vector<float> o_r2, o_b, o_se, o_t;
     std::vector<uint32_t> o_mask;
@@ -465,7 +485,8 @@ oa_status gemm_dispatch(oa_engine* e, const float* X, int mbc, int snp_base) {
                                   e->has_nan.p, E, e->st));
         e->last_name = "k_gemm_simt";
     } else {
-        OA_CU(oa_launch_gemm_tc(R, e->Xhi.p, e->Xlo.p, mbc * R, e->Yhi.p, e->Ylo.p, e->t, e->n_pad, E, e->st));
+        OA_CU(oa_launch_gemm_tc(R, e->Xhi.p, e->Xlo.p, mbc * R, e->Yhi.p, e->Ylo.p, e->t, e->n_pad, E,
+                                reinterpret_cast<int*>(e->counters.p + 3), e->st));
         e->last_name = "k_gemm_tc";
     }
     ++e->launches;
@@ -521,19 +542,23 @@ template <int R>
 oa_status run_chunk(oa_engine* e, const float* X, int mbc, int snp_base) {
     OA_CU(cudaMemsetAsync(e->has_nan.p, 0, sizeof(int), e->st));
     OA_CHECK(stats_dispatch<R>(e, X, mbc));
-    unsigned long long before[3];
+    unsigned long long before[4];
     OA_CU(cudaMemcpyAsync(before, e->counters.p, sizeof before, cudaMemcpyDeviceToHost, e->st));
     OA_CU(cudaStreamSynchronize(e->st));
     for (int attempt = 0; attempt < 3; ++attempt) {
         OA_CU(cudaEventRecord(e->k0, e->st));
         OA_CHECK(gemm_dispatch<R>(e, X, mbc, snp_base));
         OA_CU(cudaEventRecord(e->k1, e->st));
-        unsigned long long after[3];
+        unsigned long long after[4];
         OA_CU(cudaMemcpyAsync(after, e->counters.p, sizeof after, cudaMemcpyDeviceToHost, e->st));
         OA_CU(cudaStreamSynchronize(e->st));
         float ms = 0.f;
         cudaEventElapsedTime(&ms, e->k0, e->k1);
         e->last_ms += ms;
+        if (after[3]) {
+            set_err("tensor-core pipeline wait timed out (kernel aborted cleanly)");
+            return OA_ERR_CUDA;
+        }
         if ((long long)after[0] <= e->cap) {
             if (e->cfg.disp_cov) {
                 CovArgs C = cov_args(e, mbc);
@@ -574,7 +599,7 @@ oa_status run_snps_impl(oa_engine* e, const float* xr, int32_t mb, bool host_inp
     const long long tests = (long long)mb * e->t;
     if (e->cap == 0) OA_CHECK(ensure_cap(e, std::max<long long>(1 << 16, e->cfg.store_all ? tests : tests / 6)));
     if (e->cfg.store_all) OA_CHECK(ensure_cap(e, tests));
-    OA_CU(cudaMemsetAsync(e->counters.p, 0, 3 * sizeof(unsigned long long), e->st));
+    OA_CU(cudaMemsetAsync(e->counters.p, 0, 4 * sizeof(unsigned long long), e->st));
     if (e->dense_on || e->cfg.disp_cov) {
         const size_t nd = (size_t)e->t * mb;
         OA_CHECK(e->d_beta.ensure(nd * e->r));
@@ -628,8 +653,8 @@ oa_status run_snps_impl(oa_engine* e, const float* xr, int32_t mb, bool host_inp
     // sort the stored rows into reference order (trait, then SNP)
     const long long N = (long long)cnt[0];
     const int l = e->l, p = e->p;
-    e->h_rec.resize(N);
-    if (e->cfg.disp_cov) e->h_cov.resize((size_t)N * l * 3);
+    OA_CHECK(ensure_pinned(e->h_rec, e->h_rec_cap, (size_t)N));
+    if (e->cfg.disp_cov) OA_CHECK(ensure_pinned(e->h_cov, e->h_cov_cap, (size_t)N * l * 3));
     if (N > 0) {
         OA_CHECK(e->keys.ensure(N));
         OA_CHECK(e->keys2.ensure(N));
@@ -650,10 +675,9 @@ oa_status run_snps_impl(oa_engine* e, const float* xr, int32_t mb, bool host_inp
                                                                      e->cfg.disp_cov ? e->cov2.p : nullptr, l);
         ++e->launches;
         if (e->cfg.disp_cov)
-            OA_CU(cudaMemcpyAsync(e->h_cov.data(), e->cov2.p, sizeof(float) * N * l * 3, cudaMemcpyDeviceToHost,
-                                  e->st));
+            OA_CU(cudaMemcpyAsync(e->h_cov, e->cov2.p, sizeof(float) * N * l * 3, cudaMemcpyDeviceToHost, e->st));
         OA_CU(cudaGetLastError());
-        OA_CU(cudaMemcpyAsync(e->h_rec.data(), e->rec2.p, sizeof(Rec) * N, cudaMemcpyDeviceToHost, e->st));
+        OA_CU(cudaMemcpyAsync(e->h_rec, e->rec2.p, sizeof(Rec) * N, cudaMemcpyDeviceToHost, e->st));
         OA_CU(cudaStreamSynchronize(e->st));
     }
     e->o_trait.resize(N);
@@ -661,34 +685,48 @@ oa_status run_snps_impl(oa_engine* e, const float* xr, int32_t mb, bool host_inp
     e->o_nused.resize(N);
     e->o_r2.resize(N);
     e->o_mask.resize(N);
-    e->o_b.assign((size_t)N * p, 0.f);
-    e->o_se.assign((size_t)N * p, 0.f);
-    e->o_t.assign((size_t)N * p, 0.f);
+    e->o_b.resize((size_t)N * p);
+    e->o_se.resize((size_t)N * p);
+    e->o_t.resize((size_t)N * p);
     const float minT = e->cfg.min_t_store;
-    for (long long q = 0; q < N; ++q) {
-        const Rec& rc = e->h_rec[q];
-        e->o_trait[q] = rc.trait;
-        e->o_snp[q] = rc.snp;
-        e->o_nused[q] = e->h_nobs[rc.trait];
-        e->o_r2[q] = rc.r2;
-        uint32_t m = 0;
-        for (int a = 0; a < R; ++a) {
-            const int h = l + a;
-            e->o_b[(size_t)q * p + h] = rc.b[a];
-            e->o_se[(size_t)q * p + h] = rc.se[a];
-            e->o_t[(size_t)q * p + h] = rc.t[a];
-            if (rc.mask & (1u << a)) m |= 1u << h;
-        }
-        if (e->cfg.disp_cov) {
-            const float* cv = e->h_cov.data() + (size_t)q * l * 3;
-            for (int h = 1; h < l; ++h) {
-                e->o_b[(size_t)q * p + h] = cv[h * 3];
-                e->o_se[(size_t)q * p + h] = cv[h * 3 + 1];
-                e->o_t[(size_t)q * p + h] = cv[h * 3 + 2];
-                if (cv[h * 3 + 2] > minT || e->cfg.store_all) m |= 1u << h;
+    const bool disp_cov = e->cfg.disp_cov != 0, store_all = e->cfg.store_all != 0;
+    auto convert = [&](long long q0, long long q1) {
+        for (long long q = q0; q < q1; ++q) {
+            const Rec& rc = e->h_rec[q];
+            e->o_trait[q] = rc.trait;
+            e->o_snp[q] = rc.snp;
+            e->o_nused[q] = e->h_nobs[rc.trait];
+            e->o_r2[q] = rc.r2;
+            float* ob = &e->o_b[(size_t)q * p];
+            float* os = &e->o_se[(size_t)q * p];
+            float* ot = &e->o_t[(size_t)q * p];
+            for (int h = 0; h < l; ++h) ob[h] = os[h] = ot[h] = 0.f;
+            uint32_t m = 0;
+            for (int a = 0; a < R; ++a) {
+                ob[l + a] = rc.b[a];
+                os[l + a] = rc.se[a];
+                ot[l + a] = rc.t[a];
+                if (rc.mask & (1u << a)) m |= 1u << (l + a);
             }
+            if (disp_cov) {
+                const float* cv = e->h_cov + (size_t)q * l * 3;
+                for (int h = 1; h < l; ++h) {
+                    ob[h] = cv[h * 3];
+                    os[h] = cv[h * 3 + 1];
+                    ot[h] = cv[h * 3 + 2];
+                    if (cv[h * 3 + 2] > minT || store_all) m |= 1u << h;
+                }
+            }
+            e->o_mask[q] = m;
         }
-        e->o_mask[q] = m;
+    };
+    const int nthr = N > (1 << 18) ? (int)std::min<unsigned>(32u, std::max(1u, std::thread::hardware_concurrency())) : 1;
+    if (nthr <= 1) {
+        convert(0, N);
+    } else {
+        std::vector<std::thread> th;
+        for (int k = 0; k < nthr; ++k) th.emplace_back(convert, N * k / nthr, N * (k + 1) / nthr);
+        for (auto& x : th) x.join();
     }
     out->trait = e->o_trait.data();
     out->snp = e->o_snp.data();
@@ -826,6 +864,8 @@ oa_status oa_engine_destroy(oa_engine* e) {
     e->rec.release();
     e->rec2.release();
     e->cub_tmp.release();
+    if (e->h_rec) cudaFreeHost(e->h_rec);
+    if (e->h_cov) cudaFreeHost(e->h_cov);
     for (int b = 0; b < 2; ++b) {
         cudaEventDestroy(e->ev_copied[b]);
         cudaEventDestroy(e->ev_used[b]);

@@ -1,13 +1,375 @@
-// Mixed-precision XR'Y~ on tcgen05 tensor cores (BF16 hi/lo split, 3 products).
+// Mixed-precision form of XR'Y~ (≙ the Ay_bot sgemm, src/Algorithm.cpp:705-707)
+// on the 5th-generation tensor cores, with the per-test statistics fused
+// into the epilogue.
+//
+// Each FP32 operand is split into BF16 hi + lo (x = hi + lo to ~2^-17
+// relative) and the product is accumulated in FP32 TMEM as
+//     C = Xhi Yhi' + Xhi Ylo' + Xlo Yhi'        (the lo*lo term, ~2^-18, is dropped)
+//
+// Persistent, warp-specialised kernel, one CTA per SM:
+//   warp 0      TMA producer: 4 tiled loads per K-block (Xhi, Xlo, Yhi, Ylo),
+//               128B-swizzled, completing on the stage's full barrier
+//   warp 1      TMEM allocator and MMA issuer: 12 tcgen05.mma (kind::f16,
+//               M=128, N=256, K=16) per 64-wide K-block, tcgen05.commit frees
+//               the stage; a second commit hands the accumulator to the epilogue
+//   warps 2..5  epilogue: tcgen05.ld of the 128 x 256 FP32 accumulator, the
+//               statistics of epi_eval, warp-aggregated row emission
+// Two 256-column accumulators (512 TMEM columns) let the epilogue of one
+// tile overlap the main loop of the next.
+//
+// Every wait is bounded (2 s of %globaltimer); on a timeout the kernel sets
+// a flag, stops issuing, waits for its own copies and MMAs in flight, frees
+// its TMEM and returns.  The host turns the flag into an error.
+#include <cuda.h>
+
+#include "oa_epilogue.cuh"
 #include "oa_launch.h"
 
 namespace oa {
+namespace tc {
+
+constexpr int BM = 128, BN = 256, BK = 64, STAGES = 2;
+constexpr int A_BYTES = BM * BK * 2;                     // 16 KB per hi or lo tile
+constexpr int B_BYTES = BN * BK * 2;                     // 32 KB
+constexpr int STAGE_BYTES = 2 * A_BYTES + 2 * B_BYTES;   // 96 KB
+constexpr int EPI_WARPS = 4;
+constexpr int NUM_THREADS = 64 + 32 * EPI_WARPS;         // 192
+constexpr uint32_t TMEM_COLS = 512;
+constexpr int STG_STRIDE = 33;                           // epilogue staging row (conflict-free)
+constexpr size_t SMEM_BYTES = 1024 + (size_t)STAGES * STAGE_BYTES + (size_t)EPI_WARPS * 32 * STG_STRIDE * 4;
+constexpr unsigned long long WAIT_NS = 2000000000ull;
+
+// instruction descriptor, kind::f16: D FP32 (bits 4-5 = 1), A and B BF16
+// (bits 7-9 = 1, 10-12 = 1), both K-major (bits 15, 16 = 0), N >> 3 at
+// bits 17-22, M >> 4 at bits 24-28
+constexpr uint32_t IDESC = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(BN >> 3) << 17) |
+                           ((uint32_t)(BM >> 4) << 24);
+
+__device__ __forceinline__ uint32_t su32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ unsigned long long gtimer() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t* b, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(su32(b)), "r"(count));
+}
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* b, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(su32(b)), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ void mbar_arrive(uint64_t* b) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(su32(b)) : "memory");
+}
+__device__ __forceinline__ bool mbar_try(uint64_t* b, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\tselp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(ok)
+        : "r"(su32(b)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+// Wait for the phase of parity `parity` to complete; false on abort/timeout.
+__device__ __forceinline__ bool mbar_wait(uint64_t* b, uint32_t parity, volatile int* abort_flag) {
+    if (mbar_try(b, parity)) return true;
+    const unsigned long long t0 = gtimer();
+    while (true) {
+        if (mbar_try(b, parity)) return true;
+        if (*abort_flag) return false;
+        if (gtimer() - t0 > WAIT_NS) {
+            *abort_flag = 1;
+            return false;
+        }
+    }
+}
+// Bounded wait that ignores the abort flag (draining work in flight).
+__device__ __forceinline__ void mbar_drain(uint64_t* b, uint32_t parity) {
+    const unsigned long long t0 = gtimer();
+    while (!mbar_try(b, parity) && gtimer() - t0 < WAIT_NS) {
+    }
+}
+
+__device__ __forceinline__ void tma_load_2d(const CUtensorMap* map, uint64_t* bar, void* dst, int x, int y) {
+    asm volatile(
+        "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%3, %4}], [%2];" ::"r"(
+            su32(dst)),
+        "l"(reinterpret_cast<uint64_t>(map)), "r"(su32(bar)), "r"(x), "r"(y)
+        : "memory");
+}
+
+// UMMA shared-memory descriptor: K-major, 128-byte swizzle, 8-row groups
+// 1024 bytes apart (SBO), version 1 (sm_100), layout type 2 = SWIZZLE_128B.
+__device__ __forceinline__ uint64_t sw128_desc(uint32_t saddr) {
+    uint64_t d = (uint64_t)((saddr >> 4) & 0x3FFFu);
+    d |= (uint64_t)1u << 16;                 // leading byte offset (ignored for swizzled K-major)
+    d |= (uint64_t)(1024u >> 4) << 32;       // stride byte offset
+    d |= (uint64_t)1u << 46;                 // descriptor version
+    d |= (uint64_t)2u << 61;                 // SWIZZLE_128B
+    return d;
+}
+
+__device__ __forceinline__ void mma_bf16(uint32_t d_tmem, uint64_t a, uint64_t b, uint32_t accumulate) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n}\n" ::"r"(d_tmem),
+        "l"(a), "l"(b), "r"(IDESC), "r"(accumulate), "r"(0u), "r"(0u), "r"(0u), "r"(0u));
+}
+__device__ __forceinline__ void mma_commit(uint64_t* bar) {
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(su32(bar))
+                 : "memory");
+}
+__device__ __forceinline__ void fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+
+__device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&v)[32]) {
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
+        "%15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, [%32];\n"
+        : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
+          "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15]),
+          "=r"(v[16]), "=r"(v[17]), "=r"(v[18]), "=r"(v[19]), "=r"(v[20]), "=r"(v[21]), "=r"(v[22]), "=r"(v[23]),
+          "=r"(v[24]), "=r"(v[25]), "=r"(v[26]), "=r"(v[27]), "=r"(v[28]), "=r"(v[29]), "=r"(v[30]), "=r"(v[31])
+        : "r"(taddr));
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+}
+
+template <int R>
+__global__ void __launch_bounds__(NUM_THREADS, 1)
+k_gemm_tc(const __grid_constant__ CUtensorMap mAhi, const __grid_constant__ CUtensorMap mAlo,
+          const __grid_constant__ CUtensorMap mBhi, const __grid_constant__ CUtensorMap mBlo, int xrows, int t,
+          int nk, EpiArgs E, int* err) {
+    extern __shared__ uint8_t smem_raw[];
+    uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~(uintptr_t)1023);
+    float* stg = reinterpret_cast<float*>(smem + (size_t)STAGES * STAGE_BYTES);
+    __shared__ __align__(8) uint64_t full_bar[STAGES], empty_bar[STAGES], acc_full[2], acc_empty[2], done_bar;
+    __shared__ uint32_t tmem_base_sh;
+    __shared__ volatile int abort_sh;
+
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int m_tiles = (xrows + BM - 1) / BM, n_tiles = (t + BN - 1) / BN;
+    const int ntiles = m_tiles * n_tiles;
+
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < STAGES; ++s) {
+            mbar_init(&full_bar[s], 1);
+            mbar_init(&empty_bar[s], 1);
+        }
+        for (int a = 0; a < 2; ++a) {
+            mbar_init(&acc_full[a], 1);
+            mbar_init(&acc_empty[a], EPI_WARPS * 32);
+        }
+        mbar_init(&done_bar, 1);
+        abort_sh = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (warp == 1) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(su32(&tmem_base_sh)),
+                     "r"(TMEM_COLS));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+    }
+    fence_before();
+    __syncthreads();
+    fence_after();
+    const uint32_t tmem_base = tmem_base_sh;
+
+    auto stage_ptr = [&](int s, int which) -> uint8_t* {
+        // which: 0 Ahi, 1 Alo, 2 Bhi, 3 Blo
+        uint8_t* b = smem + (size_t)s * STAGE_BYTES;
+        return which < 2 ? b + which * A_BYTES : b + 2 * A_BYTES + (which - 2) * B_BYTES;
+    };
+
+    if (warp == 0) {
+        if (lane == 0) {
+            // ---------------- TMA producer ----------------
+            int s = 0;
+            uint32_t ph = 0;
+            uint32_t pend_par[STAGES];
+            bool pend[STAGES];
+            for (int q = 0; q < STAGES; ++q) pend[q] = false;
+            bool ok = true;
+            for (int tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x) {
+                const int m0 = (tile / n_tiles) * BM, n0 = (tile % n_tiles) * BN;
+                for (int kb = 0; kb < nk; ++kb) {
+                    if (!mbar_wait(&empty_bar[s], ph ^ 1u, &abort_sh)) {
+                        ok = false;
+                        break;
+                    }
+                    mbar_expect_tx(&full_bar[s], STAGE_BYTES);
+                    tma_load_2d(&mAhi, &full_bar[s], stage_ptr(s, 0), kb * BK, m0);
+                    tma_load_2d(&mAlo, &full_bar[s], stage_ptr(s, 1), kb * BK, m0);
+                    tma_load_2d(&mBhi, &full_bar[s], stage_ptr(s, 2), kb * BK, n0);
+                    tma_load_2d(&mBlo, &full_bar[s], stage_ptr(s, 3), kb * BK, n0);
+                    pend[s] = true;
+                    pend_par[s] = ph;
+                    if (++s == STAGES) {
+                        s = 0;
+                        ph ^= 1u;
+                    }
+                }
+            }
+            if (!ok)  // drain our own copies before the shared memory goes away
+                for (int q = 0; q < STAGES; ++q)
+                    if (pend[q]) mbar_drain(&full_bar[q], pend_par[q]);
+        }
+    } else if (warp == 1) {
+        if (lane == 0) {
+            // ---------------- MMA issuer ----------------
+            int s = 0, acc = 0;
+            uint32_t ph = 0, aph = 0;
+            bool ok = true, issued = false;
+            for (int tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x) {
+                if (!mbar_wait(&acc_empty[acc], aph ^ 1u, &abort_sh)) break;
+                fence_after();
+                const uint32_t d_tmem = tmem_base + (uint32_t)(acc * BN);
+                for (int kb = 0; kb < nk; ++kb) {
+                    if (!mbar_wait(&full_bar[s], ph, &abort_sh)) {
+                        ok = false;
+                        break;
+                    }
+                    fence_after();
+                    const uint32_t ahi = su32(stage_ptr(s, 0)), alo = su32(stage_ptr(s, 1));
+                    const uint32_t bhi = su32(stage_ptr(s, 2)), blo = su32(stage_ptr(s, 3));
+#pragma unroll
+                    for (int kk = 0; kk < BK / 16; ++kk) {
+                        const uint32_t off = (uint32_t)kk * 32u;   // 16 BF16 along K inside the swizzled row
+                        const uint64_t dah = sw128_desc(ahi + off), dal = sw128_desc(alo + off);
+                        const uint64_t dbh = sw128_desc(bhi + off), dbl = sw128_desc(blo + off);
+                        mma_bf16(d_tmem, dah, dbh, (kb > 0 || kk > 0) ? 1u : 0u);
+                        mma_bf16(d_tmem, dah, dbl, 1u);
+                        mma_bf16(d_tmem, dal, dbh, 1u);
+                    }
+                    issued = true;
+                    mma_commit(&empty_bar[s]);
+                    if (++s == STAGES) {
+                        s = 0;
+                        ph ^= 1u;
+                    }
+                }
+                if (!ok) break;
+                mma_commit(&acc_full[acc]);
+                if (++acc == 2) {
+                    acc = 0;
+                    aph ^= 1u;
+                }
+            }
+            if (issued) {  // all MMAs of this CTA complete before TMEM is freed
+                mma_commit(&done_bar);
+                mbar_drain(&done_bar, 0);
+            }
+        }
+    } else {
+        // ---------------- epilogue ----------------
+        const int ew = warp - 2;                 // 0..3
+        const int lg = warp & 3;                 // TMEM lane group this warp may access
+        float* my = stg + (size_t)ew * 32 * STG_STRIDE;
+        int acc = 0;
+        uint32_t aph = 0;
+        for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+            const int m0 = (tile / n_tiles) * BM, n0 = (tile % n_tiles) * BN;
+            if (!mbar_wait(&acc_full[acc], aph, &abort_sh)) break;
+            fence_after();
+            const int row = m0 + lg * 32 + lane;   // SNP column of this lane
+            for (int c0 = 0; c0 < BN && n0 + c0 < t; c0 += 32) {
+                uint32_t v[32];
+                tmem_ld32(tmem_base + ((uint32_t)(lg * 32) << 16) + (uint32_t)(acc * BN + c0), v);
+#pragma unroll
+                for (int q = 0; q < 32; ++q) my[lane * STG_STRIDE + q] = __uint_as_float(v[q]);
+                __syncwarp();
+                const int qmax = min(32, t - n0 - c0);
+                for (int q = 0; q < qmax; ++q) {
+                    const int j = n0 + c0 + q;
+                    const float zf = my[lane * STG_STRIDE + q];
+                    float z[R];
+#pragma unroll
+                    for (int a = 0; a < R; ++a) z[a] = __shfl_sync(0xffffffffu, zf, (lane & ~(R - 1)) + a);
+                    const bool valid = ((lane & (R - 1)) == 0) && (row < xrows);
+                    Rec rc;
+                    const bool st = epi_eval<R>(E, row / R, j, z, valid, rc);
+                    epi_emit(E, st, rc);
+                }
+                __syncwarp();
+            }
+            fence_before();
+            mbar_arrive(&acc_empty[acc]);
+            if (++acc == 2) {
+                acc = 0;
+                aph ^= 1u;
+            }
+        }
+    }
+
+    fence_before();
+    __syncthreads();
+    if (warp == 1) {
+        fence_after();
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem_base), "r"(TMEM_COLS));
+    }
+    if (threadIdx.x == 0 && abort_sh) atomicExch(err, 1);
+}
+
+typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                  const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                  CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+static EncodeTiledFn encode_fn() {
+    static EncodeTiledFn fn = nullptr;
+    if (!fn) {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<EncodeTiledFn>(p);
+    }
+    return fn;
+}
+
+// K-major BF16 matrix of `rows` rows and k_pad (multiple of 64) columns.
+static bool make_map(CUtensorMap* m, const __nv_bfloat16* ptr, int rows, int k_pad, int box_rows) {
+    EncodeTiledFn fn = encode_fn();
+    if (!fn || rows <= 0 || (k_pad % BK) != 0 || (reinterpret_cast<uintptr_t>(ptr) & 15) != 0) return false;
+    const cuuint64_t gdim[2] = {(cuuint64_t)k_pad, (cuuint64_t)rows};
+    const cuuint64_t gstride[1] = {(cuuint64_t)k_pad * 2};
+    const cuuint32_t box[2] = {(cuuint32_t)BK, (cuuint32_t)box_rows};
+    const cuuint32_t estride[2] = {1, 1};
+    return fn(m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<__nv_bfloat16*>(ptr), gdim, gstride, box, estride,
+              CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+              CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+template <int R>
+static cudaError_t go(const __nv_bfloat16* Xhi, const __nv_bfloat16* Xlo, int xrows, const __nv_bfloat16* Yhi,
+                      const __nv_bfloat16* Ylo, int t, int n_pad, const EpiArgs& E, int* err, cudaStream_t st) {
+    CUtensorMap a_hi, a_lo, b_hi, b_lo;
+    if (!make_map(&a_hi, Xhi, xrows, n_pad, BM) || !make_map(&a_lo, Xlo, xrows, n_pad, BM) ||
+        !make_map(&b_hi, Yhi, t, n_pad, BN) || !make_map(&b_lo, Ylo, t, n_pad, BN))
+        return cudaErrorInvalidValue;
+    static int sms = 0;
+    if (!sms) {
+        int dev = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    }
+    cudaError_t e = cudaFuncSetAttribute(k_gemm_tc<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM_BYTES);
+    if (e != cudaSuccess) return e;
+    const int ntiles = ((xrows + BM - 1) / BM) * ((t + BN - 1) / BN);
+    const int grid = ntiles < sms ? ntiles : sms;
+    k_gemm_tc<R><<<grid, NUM_THREADS, SMEM_BYTES, st>>>(a_hi, a_lo, b_hi, b_lo, xrows, t, n_pad / BK, E, err);
+    return cudaGetLastError();
+}
+
+}  // namespace tc
 
 cudaError_t oa_launch_gemm_tc(int R, const __nv_bfloat16* Xhi, const __nv_bfloat16* Xlo, int xrows,
                               const __nv_bfloat16* Yhi, const __nv_bfloat16* Ylo, int t, int n_pad,
-                              const EpiArgs& E, cudaStream_t st) {
-    (void)R; (void)Xhi; (void)Xlo; (void)xrows; (void)Yhi; (void)Ylo; (void)t; (void)n_pad; (void)E; (void)st;
-    return cudaErrorNotSupported;
+                              const EpiArgs& E, int* err, cudaStream_t st) {
+    switch (R) {
+        case 1: return tc::go<1>(Xhi, Xlo, xrows, Yhi, Ylo, t, n_pad, E, err, st);
+        case 2: return tc::go<2>(Xhi, Xlo, xrows, Yhi, Ylo, t, n_pad, E, err, st);
+        case 4: return tc::go<4>(Xhi, Xlo, xrows, Yhi, Ylo, t, n_pad, E, err, st);
+        default: return cudaErrorInvalidValue;
+    }
 }
 
 }  // namespace oa

@@ -10,5 +10,5 @@ cudaError_t oa_launch_gemm_simt(int R, const float* X, size_t ldx, int xrows, co
                                 int K, const float* colmean, const int* has_nan, const EpiArgs& E, cudaStream_t st);
 cudaError_t oa_launch_gemm_tc(int R, const __nv_bfloat16* Xhi, const __nv_bfloat16* Xlo, int xrows,
                               const __nv_bfloat16* Yhi, const __nv_bfloat16* Ylo, int t, int n_pad,
-                              const EpiArgs& E, cudaStream_t st);
+                              const EpiArgs& E, int* err, cudaStream_t st);
 }  // namespace oa

@@ -1,0 +1,47 @@
+"""GPU parity of the mixed-precision form (tcgen05 BF16 hi/lo, 3 products,
+FP32 accumulate) against the FP64 oracle.  Target: max |dt| <= 1e-3."""
+import numpy as np
+import pytest
+
+import oa_oracle as O
+from omicabelnomm_b200 import engine as E
+from omicabelnomm_b200 import synth
+from test_gpu_parity import CASES, engine_run, oracle_dense
+
+pytestmark = pytest.mark.gpu
+
+T_ABS_MIXED = 1e-3          # |t_mixed - t_fp64| <= 1e-3 (plus 1e-4 relative for very large t)
+T_REL_MIXED = 1e-4
+
+
+@pytest.mark.parametrize("case", ["r1_uniform", "r1_patterns", "r1_xrnan", "r1_collinear", "r2_complete",
+                                  "r2_missing"])
+def test_mixed_dense_matches_fp64_oracle(case):
+    w = synth.scaled(0, **CASES[case])
+    ds = synth.generate(w)
+    res, inp, s = oracle_dense(ds, w.r)
+    eng, rows, (b, se, tt, r2) = engine_run(ds, w.r, precision=E.MIXED)
+    D = res.dense
+    ok = ~D.singular
+    t_ref = D.tstat[:, :, res.l:][ok]
+    dt = np.abs(tt[ok] - t_ref)
+    lim = T_ABS_MIXED + T_REL_MIXED * np.abs(t_ref)
+    assert np.all(dt <= lim), f"max |dt| {dt.max():.3g}"
+    assert np.allclose(se[ok], D.se[:, :, res.l:][ok], rtol=1e-4, atol=0)
+
+
+def test_mixed_matches_plain_on_stored_rows():
+    ds = synth.generate(synth.scaled(0, n=1000, m=700, t=300, l=4, miss_mode="patterns", n_patterns=7, seed=51))
+    _, rp, (bp, sp, tp, r2p) = engine_run(ds, 1, precision=E.PLAIN)
+    _, rm, (bm, sm, tm, r2m) = engine_run(ds, 1, precision=E.MIXED)
+    assert np.nanmax(np.abs(tp - tm)) < 1e-3
+    assert rp.tests == rm.tests
+
+
+def test_mixed_multiple_tiles_and_ragged_edges():
+    """t and m not multiples of the 256 x 128 tile; several persistent tiles per CTA."""
+    ds = synth.generate(synth.scaled(0, n=333, m=1301, t=517, seed=52))
+    _, rp, (bp, sp, tp, _) = engine_run(ds, 1, precision=E.PLAIN)
+    _, rm, (bm, sm, tm, _) = engine_run(ds, 1, precision=E.MIXED)
+    assert np.nanmax(np.abs(tp - tm)) < 1e-3
+    np.testing.assert_array_equal(np.isnan(tp), np.isnan(tm))
