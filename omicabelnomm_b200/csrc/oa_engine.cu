@@ -183,7 +183,7 @@ std::vector<double> singular_values(std::vector<double> A /* row-major k x k */,
 
 struct oa_engine {
     oa_config cfg{};
-    int n = 0, l = 0, r = 0, p = 0, LP = 4, n_pad = 0;
+    int n = 0, l = 0, r = 0, p = 0, LP = 4, n_pad = 0, sm_count = 148;
     cudaStream_t st = nullptr, cp = nullptr;
     cudaEvent_t ev_copied[2]{}, ev_used[2]{}, k0 = nullptr, k1 = nullptr;
     long long launches = 0;
@@ -388,14 +388,17 @@ StatsArgs stats_args(oa_engine* e, const float* X, int mbc, int LP, int spb, int
 
 template <int R>
 oa_status stats_dispatch(oa_engine* e, const float* X, int mbc) {
-    // SNPs per CTA: as many as fit the register budget and ~160 KB of staged columns
+    // SNPs per group: as many as fit the register budget; two column buffers
+    // (double-buffered TMA staging) when they fit in ~170 KB, else one
     const int nS = (e->n + 3) & ~3;
+    const size_t limit = 227 * 1024 - 1024;
     auto pick = [&](auto lp_tag) -> oa_status {
         constexpr int LP = decltype(lp_tag)::value;
         int spb = stats_spb_max(R, LP);
-        while (spb > 1 && (size_t)spb * R * nS * 4 > 160 * 1024) --spb;
-        const size_t base = stats_smem_bytes(R, LP, e->n, spb, 0);
-        const size_t limit = 227 * 1024 - 1024;
+        int nbuf = 2;
+        while (spb > 1 && (size_t)nbuf * spb * R * nS * 4 > 170 * 1024) --spb;
+        if ((size_t)nbuf * spb * R * nS * 4 > 170 * 1024) nbuf = 1;
+        const size_t base = stats_smem_bytes(R, LP, e->n, spb, nbuf, 0);
         if (base + (size_t)spb * stats_na(R, LP) * 4 > limit) {
             set_err("n = %d is too large for one SNP column in shared memory", e->n);
             return OA_ERR_UNSUPPORTED;
@@ -403,9 +406,13 @@ oa_status stats_dispatch(oa_engine* e, const float* X, int mbc) {
         int spp = (int)std::min<size_t>((size_t)std::max(e->nsets, 1),
                                         (limit - base) / ((size_t)spb * stats_na(R, LP) * 4));
         spp = std::max(spp, 1);
-        const size_t smem = stats_smem_bytes(R, LP, e->n, spb, spp);
+        const size_t smem = stats_smem_bytes(R, LP, e->n, spb, nbuf, spp);
         StatsArgs A = stats_args(e, X, mbc, LP, spb, spp);
-        OA_CU(oa_launch_snp_stats(R, LP, A, (mbc + spb - 1) / spb, smem, e->st));
+        A.nbuf = nbuf;
+        A.err = reinterpret_cast<int*>(e->counters.p + 3);
+        const int groups = (mbc + spb - 1) / spb;
+        const int grid = std::min(groups, e->sm_count);
+        OA_CU(oa_launch_snp_stats(R, LP, A, grid, smem, e->st));
         ++e->launches;
         return OA_OK;
     };
@@ -556,7 +563,7 @@ oa_status run_chunk(oa_engine* e, const float* X, int mbc, int snp_base) {
         cudaEventElapsedTime(&ms, e->k0, e->k1);
         e->last_ms += ms;
         if (after[3]) {
-            set_err("tensor-core pipeline wait timed out (kernel aborted cleanly)");
+            set_err("a device pipeline wait timed out (the kernel stopped cleanly)");
             return OA_ERR_CUDA;
         }
         if ((long long)after[0] <= e->cap) {
@@ -809,6 +816,7 @@ oa_status oa_engine_create(const oa_config* cfg, oa_engine** out) {
     }
     oa_engine* e = new oa_engine();
     e->cfg = *cfg;
+    e->sm_count = prop.multiProcessorCount;
     e->n = cfg->n;
     e->l = cfg->l;
     e->r = cfg->r;

@@ -22,22 +22,34 @@
 // its TMEM and returns.  The host turns the flag into an error.
 #include <cuda.h>
 
+#include <cstdlib>
+
 #include "oa_epilogue.cuh"
 #include "oa_launch.h"
 
 namespace oa {
 namespace tc {
 
-constexpr int BM = 128, BN = 256, BK = 64, STAGES = 2;
-constexpr int A_BYTES = BM * BK * 2;                     // 16 KB per hi or lo tile
-constexpr int B_BYTES = BN * BK * 2;                     // 32 KB
-constexpr int STAGE_BYTES = 2 * A_BYTES + 2 * B_BYTES;   // 96 KB
+constexpr int BM = 128, BN = 256;
 constexpr int EPI_WARPS = 4;
 constexpr int NUM_THREADS = 64 + 32 * EPI_WARPS;         // 192
 constexpr uint32_t TMEM_COLS = 512;
 constexpr int STG_STRIDE = 33;                           // epilogue staging row (conflict-free)
-constexpr size_t SMEM_BYTES = 1024 + (size_t)STAGES * STAGE_BYTES + (size_t)EPI_WARPS * 32 * STG_STRIDE * 4;
 constexpr unsigned long long WAIT_NS = 2000000000ull;
+
+// Pipeline shape: K-block width BK (64 -> 128-byte swizzle, 32 -> 64-byte
+// swizzle) and the number of shared-memory stages.
+template <int BK_, int STAGES_>
+struct Shape {
+    static constexpr int BK = BK_, STAGES = STAGES_;
+    static constexpr int A_BYTES = BM * BK * 2;                     // one of hi / lo
+    static constexpr int B_BYTES = BN * BK * 2;
+    static constexpr int STAGE_BYTES = 2 * A_BYTES + 2 * B_BYTES;
+    static constexpr size_t SMEM_BYTES =
+        1024 + (size_t)STAGES * STAGE_BYTES + (size_t)EPI_WARPS * 32 * STG_STRIDE * 4;
+    static constexpr uint64_t LAYOUT = BK == 64 ? 2u : 4u;          // SWIZZLE_128B : SWIZZLE_64B
+    static constexpr uint32_t SBO = BK == 64 ? 1024u : 512u;        // bytes between 8-row groups
+};
 
 // instruction descriptor, kind::f16: D FP32 (bits 4-5 = 1), A and B BF16
 // (bits 7-9 = 1, 10-12 = 1), both K-major (bits 15, 16 = 0), N >> 3 at
@@ -99,14 +111,17 @@ __device__ __forceinline__ void tma_load_2d(const CUtensorMap* map, uint64_t* ba
         : "memory");
 }
 
-// UMMA shared-memory descriptor: K-major, 128-byte swizzle, 8-row groups
-// 1024 bytes apart (SBO), version 1 (sm_100), layout type 2 = SWIZZLE_128B.
-__device__ __forceinline__ uint64_t sw128_desc(uint32_t saddr) {
+// UMMA shared-memory descriptor, K-major swizzled operand: start address,
+// leading byte offset 1 (ignored for swizzled K-major), stride byte offset
+// = bytes between 8-row groups, version 1 (sm_100), layout type
+// (2 = SWIZZLE_128B, 4 = SWIZZLE_64B).
+template <class SH>
+__device__ __forceinline__ uint64_t smem_desc(uint32_t saddr) {
     uint64_t d = (uint64_t)((saddr >> 4) & 0x3FFFu);
-    d |= (uint64_t)1u << 16;                 // leading byte offset (ignored for swizzled K-major)
-    d |= (uint64_t)(1024u >> 4) << 32;       // stride byte offset
-    d |= (uint64_t)1u << 46;                 // descriptor version
-    d |= (uint64_t)2u << 61;                 // SWIZZLE_128B
+    d |= (uint64_t)1u << 16;
+    d |= (uint64_t)(SH::SBO >> 4) << 32;
+    d |= (uint64_t)1u << 46;
+    d |= SH::LAYOUT << 61;
     return d;
 }
 
@@ -135,11 +150,13 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&v)[32]) {
     asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 }
 
-template <int R>
+template <int R, class SH>
 __global__ void __launch_bounds__(NUM_THREADS, 1)
 k_gemm_tc(const __grid_constant__ CUtensorMap mAhi, const __grid_constant__ CUtensorMap mAlo,
           const __grid_constant__ CUtensorMap mBhi, const __grid_constant__ CUtensorMap mBlo, int xrows, int t,
           int nk, EpiArgs E, int* err) {
+    constexpr int BK = SH::BK, STAGES = SH::STAGES;
+    constexpr int A_BYTES = SH::A_BYTES, B_BYTES = SH::B_BYTES, STAGE_BYTES = SH::STAGE_BYTES;
     extern __shared__ uint8_t smem_raw[];
     uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~(uintptr_t)1023);
     float* stg = reinterpret_cast<float*>(smem + (size_t)STAGES * STAGE_BYTES);
@@ -234,8 +251,8 @@ k_gemm_tc(const __grid_constant__ CUtensorMap mAhi, const __grid_constant__ CUte
 #pragma unroll
                     for (int kk = 0; kk < BK / 16; ++kk) {
                         const uint32_t off = (uint32_t)kk * 32u;   // 16 BF16 along K inside the swizzled row
-                        const uint64_t dah = sw128_desc(ahi + off), dal = sw128_desc(alo + off);
-                        const uint64_t dbh = sw128_desc(bhi + off), dbl = sw128_desc(blo + off);
+                        const uint64_t dah = smem_desc<SH>(ahi + off), dal = smem_desc<SH>(alo + off);
+                        const uint64_t dbh = smem_desc<SH>(bhi + off), dbl = smem_desc<SH>(blo + off);
                         mma_bf16(d_tmem, dah, dbh, (kb > 0 || kk > 0) ? 1u : 0u);
                         mma_bf16(d_tmem, dah, dbl, 1u);
                         mma_bf16(d_tmem, dal, dbh, 1u);
@@ -325,25 +342,26 @@ static EncodeTiledFn encode_fn() {
     return fn;
 }
 
-// K-major BF16 matrix of `rows` rows and k_pad (multiple of 64) columns.
-static bool make_map(CUtensorMap* m, const __nv_bfloat16* ptr, int rows, int k_pad, int box_rows) {
+// K-major BF16 matrix of `rows` rows and k_pad (multiple of 64) columns,
+// boxes of bk x box_rows with the swizzle matching the UMMA descriptor.
+static bool make_map(CUtensorMap* m, const __nv_bfloat16* ptr, int rows, int k_pad, int box_rows, int bk) {
     EncodeTiledFn fn = encode_fn();
-    if (!fn || rows <= 0 || (k_pad % BK) != 0 || (reinterpret_cast<uintptr_t>(ptr) & 15) != 0) return false;
+    if (!fn || rows <= 0 || (k_pad % 64) != 0 || (reinterpret_cast<uintptr_t>(ptr) & 15) != 0) return false;
     const cuuint64_t gdim[2] = {(cuuint64_t)k_pad, (cuuint64_t)rows};
     const cuuint64_t gstride[1] = {(cuuint64_t)k_pad * 2};
-    const cuuint32_t box[2] = {(cuuint32_t)BK, (cuuint32_t)box_rows};
+    const cuuint32_t box[2] = {(cuuint32_t)bk, (cuuint32_t)box_rows};
     const cuuint32_t estride[2] = {1, 1};
     return fn(m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<__nv_bfloat16*>(ptr), gdim, gstride, box, estride,
-              CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
-              CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+              CU_TENSOR_MAP_INTERLEAVE_NONE, bk == 64 ? CU_TENSOR_MAP_SWIZZLE_128B : CU_TENSOR_MAP_SWIZZLE_64B,
+              CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
-template <int R>
+template <int R, class SH>
 static cudaError_t go(const __nv_bfloat16* Xhi, const __nv_bfloat16* Xlo, int xrows, const __nv_bfloat16* Yhi,
                       const __nv_bfloat16* Ylo, int t, int n_pad, const EpiArgs& E, int* err, cudaStream_t st) {
     CUtensorMap a_hi, a_lo, b_hi, b_lo;
-    if (!make_map(&a_hi, Xhi, xrows, n_pad, BM) || !make_map(&a_lo, Xlo, xrows, n_pad, BM) ||
-        !make_map(&b_hi, Yhi, t, n_pad, BN) || !make_map(&b_lo, Ylo, t, n_pad, BN))
+    if (!make_map(&a_hi, Xhi, xrows, n_pad, BM, SH::BK) || !make_map(&a_lo, Xlo, xrows, n_pad, BM, SH::BK) ||
+        !make_map(&b_hi, Yhi, t, n_pad, BN, SH::BK) || !make_map(&b_lo, Ylo, t, n_pad, BN, SH::BK))
         return cudaErrorInvalidValue;
     static int sms = 0;
     if (!sms) {
@@ -351,12 +369,31 @@ static cudaError_t go(const __nv_bfloat16* Xhi, const __nv_bfloat16* Xlo, int xr
         cudaGetDevice(&dev);
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     }
-    cudaError_t e = cudaFuncSetAttribute(k_gemm_tc<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM_BYTES);
+    cudaError_t e = cudaFuncSetAttribute(k_gemm_tc<R, SH>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)SH::SMEM_BYTES);
     if (e != cudaSuccess) return e;
     const int ntiles = ((xrows + BM - 1) / BM) * ((t + BN - 1) / BN);
     const int grid = ntiles < sms ? ntiles : sms;
-    k_gemm_tc<R><<<grid, NUM_THREADS, SMEM_BYTES, st>>>(a_hi, a_lo, b_hi, b_lo, xrows, t, n_pad / BK, E, err);
+    k_gemm_tc<R, SH><<<grid, NUM_THREADS, SH::SMEM_BYTES, st>>>(a_hi, a_lo, b_hi, b_lo, xrows, t, n_pad / SH::BK,
+                                                                 E, err);
     return cudaGetLastError();
+}
+
+// Pipeline variant: 0 = BK 32 x 4 stages (default), 1 = BK 64 x 2 stages.
+static int variant() {
+    static int v = -1;
+    if (v < 0) {
+        const char* s = getenv("OA_TC_VARIANT");
+        v = s ? atoi(s) : 0;
+    }
+    return v;
+}
+
+template <int R>
+static cudaError_t go_any(const __nv_bfloat16* Xhi, const __nv_bfloat16* Xlo, int xrows, const __nv_bfloat16* Yhi,
+                          const __nv_bfloat16* Ylo, int t, int n_pad, const EpiArgs& E, int* err, cudaStream_t st) {
+    if (variant() == 1) return go<R, Shape<64, 2>>(Xhi, Xlo, xrows, Yhi, Ylo, t, n_pad, E, err, st);
+    return go<R, Shape<32, 4>>(Xhi, Xlo, xrows, Yhi, Ylo, t, n_pad, E, err, st);
 }
 
 }  // namespace tc
@@ -365,9 +402,9 @@ cudaError_t oa_launch_gemm_tc(int R, const __nv_bfloat16* Xhi, const __nv_bfloat
                               const __nv_bfloat16* Yhi, const __nv_bfloat16* Ylo, int t, int n_pad,
                               const EpiArgs& E, int* err, cudaStream_t st) {
     switch (R) {
-        case 1: return tc::go<1>(Xhi, Xlo, xrows, Yhi, Ylo, t, n_pad, E, err, st);
-        case 2: return tc::go<2>(Xhi, Xlo, xrows, Yhi, Ylo, t, n_pad, E, err, st);
-        case 4: return tc::go<4>(Xhi, Xlo, xrows, Yhi, Ylo, t, n_pad, E, err, st);
+        case 1: return tc::go_any<1>(Xhi, Xlo, xrows, Yhi, Ylo, t, n_pad, E, err, st);
+        case 2: return tc::go_any<2>(Xhi, Xlo, xrows, Yhi, Ylo, t, n_pad, E, err, st);
+        case 4: return tc::go_any<4>(Xhi, Xlo, xrows, Yhi, Ylo, t, n_pad, E, err, st);
         default: return cudaErrorInvalidValue;
     }
 }

@@ -6,9 +6,19 @@ namespace oa {
 
 template <int R, int LP>
 static cudaError_t go(const StatsArgs& A, int grid, size_t smem, cudaStream_t st) {
-    cudaError_t e = cudaFuncSetAttribute(k_snp_stats<R, LP>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (e != cudaSuccess) return e;
-    k_snp_stats<R, LP><<<grid, OA_NTHREADS, smem, st>>>(A);
+    // TMA bulk staging needs 16-byte aligned columns whose size is a multiple of 16 bytes
+    const bool bulk = (A.n % 4 == 0) && (A.ldx % 4 == 0) && ((reinterpret_cast<uintptr_t>(A.X) & 15) == 0);
+    if (bulk) {
+        cudaError_t e = cudaFuncSetAttribute(k_snp_stats<R, LP, true>,
+                                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess) return e;
+        k_snp_stats<R, LP, true><<<grid, OA_NTHREADS, smem, st>>>(A);
+    } else {
+        cudaError_t e = cudaFuncSetAttribute(k_snp_stats<R, LP, false>,
+                                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess) return e;
+        k_snp_stats<R, LP, false><<<grid, OA_NTHREADS, smem, st>>>(A);
+    }
     return cudaGetLastError();
 }
 
