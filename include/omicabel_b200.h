@@ -132,6 +132,33 @@ oa_status oa_run_snps_device(oa_engine* e, const float* xr_dev, int32_t mb,
 oa_status oa_dense_last(oa_engine* e, float* beta, float* se, float* tstat, float* r2);
 oa_status oa_enable_dense(oa_engine* e, int32_t on);
 
+/* Size of the scratch array used by oa_scan_dense_noalloc (64 MiB).  Every
+ * GPU on which the library is loaded holds this much device memory until the
+ * process exits. */
+#define OA_NOALLOC_SCRATCH_BYTES (64u << 20)
+
+/* Plain-FP32 dense scan of one SNP block that allocates no memory.
+ *
+ * For callers that cannot call cudaMalloc: code recording a CUDA graph on
+ * `stream`, plug-ins whose host framework owns the device memory pool, and
+ * processes whose device memory was reserved up front.  All intermediates
+ * live in one static device array of OA_NOALLOC_SCRATCH_BYTES; inputs and
+ * outputs are the caller's device buffers (column-major, individual index
+ * contiguous): covariates n x l (NaN-free), traits n x t (NaN = missing),
+ * dosages n x (r*mb) (NaN = mean-imputed); outputs beta/se/|t| [t][mb][r]
+ * and R2 [t][mb] (NaN where the test is singular or has RSS <= 0), the same
+ * numbers as oa_run_snps_device + oa_dense_last of an engine with
+ * store_all.  Limits: r in {1, 2, 4}, l <= OA_MAX_L, t <= 2048, and all
+ * intermediates (about 4*n*t + 9*t*mb*r*r + 8*n*l bytes) within the array;
+ * larger inputs return OA_ERR_UNSUPPORTED.  Calls share the array: calls that
+ * overlap on the GPU (other streams or threads) race.  The first call on a
+ * device looks up the array's address and must come before any stream
+ * capture.  Synchronises `stream` (a cudaStream_t; NULL = default stream)
+ * before returning.  No counterpart in the reference. */
+oa_status oa_scan_dense_noalloc(const float* xl_dev, const float* y_dev, const float* xr_dev, int32_t n,
+                                int32_t l, int32_t r, int32_t t, int32_t mb, float* beta_dev, float* se_dev,
+                                float* t_dev, float* r2_dev, void* stream);
+
 /* Number of kernel launches this engine issued so far (instrumentation). */
 int64_t oa_kernel_launches(const oa_engine* e);
 /* Device time (ms) of the dominant kernel in the last SNP block and its name. */

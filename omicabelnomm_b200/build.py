@@ -24,7 +24,7 @@ OBJ = os.path.join(OUT, "obj")
 INCLUDE = os.path.join(ROOT, "include")
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
-CU_SOURCES = ["oa_engine.cu", "oa_stats.cu", "oa_gemm_simt.cu", "oa_gemm_tc.cu"]
+CU_SOURCES = ["oa_engine.cu", "oa_stats.cu", "oa_gemm_simt.cu", "oa_gemm_tc.cu", "oa_noalloc.cu"]
 CXX_SOURCES = ["oa_host.cpp"]
 LIB = os.path.join(OUT, "libomicabel_b200.so")
 CLI = os.path.join(OUT, "omicabelnomm")

@@ -23,7 +23,7 @@ struct TraitStatsOut {
     unsigned long long* hashes; // [t][4]: missing h1 h2, zero h1 h2
 };
 
-__global__ void __launch_bounds__(OA_NTHREADS)
+static __global__ void __launch_bounds__(OA_NTHREADS)
 k_trait_stats(const float* __restrict__ Y, size_t ldy, int n, int l, const double* __restrict__ Q64,
               TraitStatsOut out) {
     __shared__ double red[8 * (2 + OA_MAX_L)];
@@ -100,7 +100,7 @@ k_trait_stats(const float* __restrict__ Y, size_t ldy, int n, int l, const doubl
 // Ordered list of the rows of each row set.  kind 0: NaN rows of the
 // representative trait (a missingness pattern); kind 1: observed rows
 // whose value is exactly 0 (a zero set).
-__global__ void __launch_bounds__(OA_NTHREADS)
+static __global__ void __launch_bounds__(OA_NTHREADS)
 k_set_rows(const float* __restrict__ Y, size_t ldy, int n, const int* __restrict__ set_rep,
            const int* __restrict__ set_kind, const int* __restrict__ set_off, int* __restrict__ rows) {
     __shared__ int wcount[8];
@@ -140,7 +140,7 @@ k_set_rows(const float* __restrict__ Y, size_t ldy, int n, const int* __restrict
 // Per row set: G = sum over the set's rows of q q' (FP64).  Patterns store
 // W = (I - G)^-1 (Q orthonormal over all rows, so Q_obs'Q_obs = I - G);
 // zero sets store G.  sing_out[s] = 1 if I - G is not positive definite.
-__global__ void __launch_bounds__(OA_NTHREADS)
+static __global__ void __launch_bounds__(OA_NTHREADS)
 k_set_gram(const double* __restrict__ Q64, int n, int l, const int* __restrict__ set_kind,
            const int* __restrict__ set_off, const int* __restrict__ rows, double* __restrict__ W,
            double* __restrict__ zQ, const int* __restrict__ set_slot, uint8_t* __restrict__ pat_bad) {
@@ -178,7 +178,7 @@ k_set_gram(const double* __restrict__ Q64, int n, int l, const int* __restrict__
 
 // y~ = y - Q b0 on observed rows (0 on missing rows), b0 = W Q'y.
 // Writes Y~ (FP32, and BF16 hi/lo for the tensor-core form), RSS0 and SST.
-__global__ void __launch_bounds__(OA_NTHREADS)
+static __global__ void __launch_bounds__(OA_NTHREADS)
 k_trait_resid(const float* __restrict__ Y, size_t ldy, int n, int n_pad, int l,
               const double* __restrict__ Q64, const double* __restrict__ sums,
               const int* __restrict__ counts, const int* __restrict__ pat,
@@ -235,7 +235,7 @@ k_trait_resid(const float* __restrict__ Y, size_t ldy, int n, int n_pad, int l,
 }
 
 // Sort keys of the stored rows: (trait, SNP) -> reference output order.
-__global__ void k_rec_keys(const Rec* __restrict__ rec, long long N, unsigned long long* __restrict__ keys,
+static __global__ void k_rec_keys(const Rec* __restrict__ rec, long long N, unsigned long long* __restrict__ keys,
                            int* __restrict__ perm) {
     const long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x;
     if (q >= N) return;
@@ -243,7 +243,7 @@ __global__ void k_rec_keys(const Rec* __restrict__ rec, long long N, unsigned lo
     perm[q] = (int)q;
 }
 
-__global__ void k_rec_gather(const Rec* __restrict__ rec, const int* __restrict__ perm, long long N,
+static __global__ void k_rec_gather(const Rec* __restrict__ rec, const int* __restrict__ perm, long long N,
                              Rec* __restrict__ out, const float* __restrict__ cov, float* __restrict__ cov_out,
                              int l) {
     const long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x;

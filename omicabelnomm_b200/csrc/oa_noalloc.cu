@@ -1,0 +1,380 @@
+// oa_scan_dense_noalloc: the plain-FP32 scan of one SNP block for callers
+// that cannot allocate GPU memory.
+//
+// Some callers cannot call cudaMalloc: code running while a CUDA graph is
+// being captured on the caller's stream, plug-ins inside host frameworks
+// that own the device memory pool (and forbid raw allocations), and
+// processes under a hard device-memory cap that was reserved up front.
+// This entry point gives them the engine's plain-FP32 block scan (the SIMT
+// GEMM with fused statistics, plus the small kernels that prepare its
+// tables) with every intermediate buffer carved from one file-scope
+// `static __device__` array of OA_NOALLOC_SCRATCH_BYTES.  It calls no
+// cudaMalloc / cudaFree and no allocating library routine, and allocates
+// no host heap memory either.
+//
+// Differences from the block engine, all to avoid allocation: the
+// covariates are orthonormalised on the device (Cholesky QR, twice) instead
+// of a host Householder QR; every trait is its own missingness pattern (no
+// host-side grouping; the math is identical); results are dense arrays.
+// The scratch array is shared by every call in the process and keeps the
+// last call's contents; calls that overlap on the GPU (other streams or
+// host threads) race on it.  The first call on a device looks up the
+// array's device address (cudaGetSymbolAddress) and must therefore come
+// before any stream capture.
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+
+#include "oa_kernels.cuh"
+#include "oa_launch.h"
+
+namespace oa {
+namespace na {
+
+// The scratch every call shares (held by each GPU that loads the library until exit).
+static __device__ __align__(256) unsigned char g_scratch[OA_NOALLOC_SCRATCH_BYTES];
+
+constexpr int MAX_DEVICES = 64;
+static void* g_scratch_ptr[MAX_DEVICES];
+static std::mutex g_mu;
+
+// Device address of the scratch array on the current device (looked up once per device).
+static cudaError_t scratch_address(int dev, void** out) {
+    std::lock_guard<std::mutex> lock(g_mu);
+    if (dev < 0 || dev >= MAX_DEVICES) return cudaErrorInvalidDevice;
+    if (!g_scratch_ptr[dev]) {
+        void* p = nullptr;
+        const cudaError_t e = cudaGetSymbolAddress(&p, g_scratch);
+        if (e != cudaSuccess) return e;
+        g_scratch_ptr[dev] = p;
+    }
+    *out = g_scratch_ptr[dev];
+    return cudaSuccess;
+}
+
+// Gram matrix G[a][b] = sum_k X[a][k] X[b][k] of the l columns of X (FP64).
+template <class T>
+__global__ void __launch_bounds__(256) k_na_gram(const T* __restrict__ X, int n, int l, double* __restrict__ G) {
+    __shared__ double red[8];
+    const int a = blockIdx.x, b = blockIdx.y;
+    if (b > a) return;
+    double s = 0.0;
+    for (int k = threadIdx.x; k < n; k += blockDim.x) s += (double)X[(size_t)a * n + k] * (double)X[(size_t)b * n + k];
+    s = warp_sum(s);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double t = 0.0;
+        for (int w = 0; w < 8; ++w) t += red[w];
+        G[a * l + b] = t;
+        G[b * l + a] = t;
+    }
+}
+
+// Q = X R^-1 with R = chol(G) upper triangular: one Cholesky-QR pass.
+// Writes Q (FP64, column-major) and, if Qr is given, its FP32 row-major
+// copy padded to LP columns.  flag[0] = 1 if G is not positive definite or
+// R has a diagonal below 1e-6 (linearly dependent covariates).
+template <class T>
+__global__ void __launch_bounds__(256) k_na_cholq(const T* __restrict__ X, int n, int l, int LP,
+                                                 const double* __restrict__ G, double* __restrict__ Q,
+                                                 float* __restrict__ Qr, int* __restrict__ flag) {
+    __shared__ double Ri[OA_MAX_L * OA_MAX_L];
+    __shared__ int bad;
+    if (threadIdx.x == 0) {
+        double L[OA_MAX_L * OA_MAX_L];
+        bad = 0;
+        for (int i = 0; i < l * l; ++i) L[i] = 0.0;
+        for (int j = 0; j < l && !bad; ++j) {
+            double s = G[j * l + j];
+            for (int q = 0; q < j; ++q) s -= L[j * l + q] * L[j * l + q];
+            if (!(s > 0.0)) {
+                bad = 1;
+                break;
+            }
+            const double d = sqrt(s);
+            if (d < 1e-6) bad = 1;
+            L[j * l + j] = d;
+            for (int i = j + 1; i < l; ++i) {
+                double u = G[i * l + j];
+                for (int q = 0; q < j; ++q) u -= L[i * l + q] * L[j * l + q];
+                L[i * l + j] = u / d;
+            }
+        }
+        // R = L' (upper); R^-1 by back substitution
+        for (int i = 0; i < l * l; ++i) Ri[i] = 0.0;
+        if (!bad)
+            for (int i = l - 1; i >= 0; --i) {
+                Ri[i * l + i] = 1.0 / L[i * l + i];
+                for (int j = i + 1; j < l; ++j) {
+                    double s = 0.0;
+                    for (int k = i + 1; k <= j; ++k) s += L[k * l + i] * Ri[k * l + j];
+                    Ri[i * l + j] = -s / L[i * l + i];
+                }
+            }
+        if (bad) *flag = 1;
+    }
+    __syncthreads();
+    if (bad) return;
+    for (int k = threadIdx.x; k < n; k += blockDim.x) {
+        double x[OA_MAX_L];
+        for (int a = 0; a < l; ++a) x[a] = (double)X[(size_t)a * n + k];
+        for (int q = 0; q < l; ++q) {
+            double s = 0.0;
+            for (int a = 0; a <= q; ++a) s += x[a] * Ri[a * l + q];
+            Q[(size_t)q * n + k] = s;
+            if (Qr) Qr[(size_t)k * LP + q] = (float)s;
+        }
+        if (Qr)
+            for (int q = l; q < LP; ++q) Qr[(size_t)k * LP + q] = 0.f;
+    }
+}
+
+// Row sets with every trait its own missingness pattern, plus one zero set
+// per trait that has observed values exactly 0.  counts[j] = (missing, zeros).
+__global__ void k_na_sets(const int* __restrict__ counts, int t, int* __restrict__ pat, int* __restrict__ zset,
+                          int* __restrict__ set_off, int* __restrict__ set_rep, int* __restrict__ set_kind,
+                          int* __restrict__ set_slot, int* __restrict__ info /* [0] Z, [1] rows */) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    int z = 0, off = 0;
+    for (int j = 0; j < t; ++j) {
+        pat[j] = j;
+        set_off[j] = off;
+        set_rep[j] = j;
+        set_kind[j] = 0;
+        set_slot[j] = j;
+        off += counts[2 * j];
+    }
+    for (int j = 0; j < t; ++j) {
+        if (counts[2 * j + 1] > 0) {
+            const int s = t + z;
+            zset[j] = z;
+            set_off[s] = off;
+            set_rep[s] = j;
+            set_kind[s] = 1;
+            set_slot[s] = z;
+            off += counts[2 * j + 1];
+            ++z;
+        } else {
+            zset[j] = -1;
+        }
+    }
+    set_off[t + z] = off;
+    info[0] = z;
+    info[1] = off;
+}
+
+// Bump allocator over the scratch array (256-byte aligned pieces).
+struct Carve {
+    unsigned char* base;
+    size_t used = 0;
+    template <class T>
+    T* take(size_t count) {
+        used = (used + 255) & ~(size_t)255;
+        T* p = reinterpret_cast<T*>(base + used);
+        used += count * sizeof(T);
+        return p;
+    }
+};
+
+static int pad_l(int l) { return l <= 4 ? 4 : (l <= 8 ? 8 : 16); }
+
+}  // namespace na
+}  // namespace oa
+
+extern "C" void oa__set_error(const char* msg);
+
+namespace {
+oa_status fail(oa_status s, const char* fmt, ...) {
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof buf, fmt, ap);
+    va_end(ap);
+    oa__set_error(buf);
+    return s;
+}
+}  // namespace
+
+#define NA_CU(x)                                                                                 \
+    do {                                                                                         \
+        cudaError_t e_ = (x);                                                                    \
+        if (e_ != cudaSuccess) return fail(OA_ERR_CUDA, "%s: %s", #x, cudaGetErrorString(e_));   \
+    } while (0)
+
+extern "C" oa_status oa_scan_dense_noalloc(const float* xl, const float* y, const float* xr, int32_t n, int32_t l,
+                                           int32_t r, int32_t t, int32_t mb, float* beta, float* se, float* tstat,
+                                           float* r2, void* stream) {
+    using namespace oa;
+    using namespace oa::na;
+    if (!xl || !y || !xr || !beta || !se || !tstat || !r2) return fail(OA_ERR_ARG, "null argument");
+    if (l < 1 || l > OA_MAX_L || !(r == 1 || r == 2 || r == 4) || n <= l + r || t < 1 || mb < 1 || t > 2048)
+        return fail(OA_ERR_ARG, "invalid sizes n=%d l=%d r=%d t=%d mb=%d (r in {1,2,4}, t <= 2048)", n, l, r, t,
+                    mb);
+    int dev = 0;
+    NA_CU(cudaGetDevice(&dev));
+    void* sp = nullptr;
+    NA_CU(scratch_address(dev, &sp));
+    cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+    const int LP = pad_l(l), n_pad = (n + 63) & ~63;
+
+    // fixed part of the layout (sizes known before the data is looked at)
+    Carve cv{reinterpret_cast<unsigned char*>(sp)};
+    unsigned long long* counters = cv.take<unsigned long long>(4);
+    int* info = cv.take<int>(4);
+    double* G = cv.take<double>((size_t)OA_MAX_L * OA_MAX_L);
+    double* Q1 = cv.take<double>((size_t)n * l);
+    double* Q64 = cv.take<double>((size_t)n * l);
+    float* Qr = cv.take<float>((size_t)n * LP);
+    double* tsums = cv.take<double>((size_t)t * (2 + OA_MAX_L));
+    int* tcounts = cv.take<int>((size_t)t * 2);
+    unsigned long long* thash = cv.take<unsigned long long>((size_t)t * 4);
+    int* pat = cv.take<int>(t);
+    int* zset = cv.take<int>(t);
+    int* set_off = cv.take<int>((size_t)2 * t + 1);
+    int* set_rep = cv.take<int>((size_t)2 * t);
+    int* set_kind = cv.take<int>((size_t)2 * t);
+    int* set_slot = cv.take<int>((size_t)2 * t);
+    double* W = cv.take<double>((size_t)t * l * l);
+    double* zQ = cv.take<double>((size_t)t * l * l);
+    uint8_t* pat_bad = cv.take<uint8_t>(t);
+    float* Yt = cv.take<float>((size_t)t * n_pad);
+    double* rss0 = cv.take<double>(t);
+    float* sst = cv.take<float>(t);
+    int* nobs = cv.take<int>(t);
+    double* b0 = cv.take<double>((size_t)t * l);
+    float* mean = cv.take<float>((size_t)mb * r);
+    int* has_nan = cv.take<int>(1);
+    float* varx = cv.take<float>((size_t)mb * r);
+    double* sinv = cv.take<double>((size_t)t * mb * r * r);
+    uint8_t* sing = cv.take<uint8_t>((size_t)t * mb);
+    float* dsig = cv.take<float>((size_t)t * mb);
+    if (cv.used > OA_NOALLOC_SCRATCH_BYTES)
+        return fail(OA_ERR_UNSUPPORTED,
+                    "oa_scan_dense_noalloc: n=%d t=%d mb=%d r=%d needs more than the %u-byte scratch array", n, t, mb,
+                    r, (unsigned)OA_NOALLOC_SCRATCH_BYTES);
+
+    // everything that must start at zero
+    NA_CU(cudaMemsetAsync(counters, 0, 4 * sizeof(unsigned long long), st));
+    NA_CU(cudaMemsetAsync(info, 0, 4 * sizeof(int), st));
+    NA_CU(cudaMemsetAsync(has_nan, 0, sizeof(int), st));
+
+    // covariates: two Cholesky-QR passes give an orthonormal basis in FP64
+    k_na_gram<float><<<dim3(l, l), 256, 0, st>>>(xl, n, l, G);
+    k_na_cholq<float><<<1, 256, 0, st>>>(xl, n, l, LP, G, Q1, nullptr, info + 2);
+    k_na_gram<double><<<dim3(l, l), 256, 0, st>>>(Q1, n, l, G);
+    k_na_cholq<double><<<1, 256, 0, st>>>(Q1, n, l, LP, G, Q64, Qr, info + 3);
+    // traits: missing counts, sums, Q'y; one row set per trait
+    TraitStatsOut tso{tsums, tcounts, thash};
+    k_trait_stats<<<t, OA_NTHREADS, 0, st>>>(y, (size_t)n, n, l, Q64, tso);
+    k_na_sets<<<1, 1, 0, st>>>(tcounts, t, pat, zset, set_off, set_rep, set_kind, set_slot, info);
+    NA_CU(cudaGetLastError());
+    int hinfo[4] = {0, 0, 0, 0};
+    NA_CU(cudaMemcpyAsync(hinfo, info, sizeof hinfo, cudaMemcpyDeviceToHost, st));
+    NA_CU(cudaStreamSynchronize(st));
+    if (hinfo[2] || hinfo[3])
+        return fail(OA_ERR_COLLINEAR, "the covariate matrix contains linearly dependent columns");
+    const int Z = hinfo[0], nrows = hinfo[1], nsets = t + Z;
+    int* set_rows = cv.take<int>((size_t)(nrows > 0 ? nrows : 1));
+    float* zA = cv.take<float>((size_t)(Z > 0 ? Z : 1) * mb * l * r);
+    float* zD = cv.take<float>((size_t)(Z > 0 ? Z : 1) * mb * r * r);
+    float* aobs = Z > 0 ? cv.take<float>((size_t)t * mb * l * r) : nullptr;
+    if (cv.used > OA_NOALLOC_SCRATCH_BYTES)
+        return fail(OA_ERR_UNSUPPORTED,
+                    "oa_scan_dense_noalloc: these inputs need %zu bytes of scratch, the array holds %u", cv.used,
+                    (unsigned)OA_NOALLOC_SCRATCH_BYTES);
+    k_set_rows<<<nsets, OA_NTHREADS, 0, st>>>(y, (size_t)n, n, set_rep, set_kind, set_off, set_rows);
+    k_set_gram<<<nsets, OA_NTHREADS, 0, st>>>(Q64, n, l, set_kind, set_off, set_rows, W, zQ, set_slot, pat_bad);
+    k_trait_resid<<<t, OA_NTHREADS, 0, st>>>(y, (size_t)n, n, n_pad, l, Q64, tsums, tcounts, pat, W, Yt, nullptr,
+                                            nullptr, rss0, sst, nobs, b0);
+    NA_CU(cudaGetLastError());
+
+    // per-SNP statistics (same geometry rule as the block engine)
+    const int nS = (n + 3) & ~3;
+    const size_t limit = 227 * 1024 - 1024;
+    const int NA = r * r + LP * r;
+    int spb = 8 / r < 64 / NA ? 8 / r : (64 / NA > 0 ? 64 / NA : 1);
+    int nbuf = 2;
+    while (spb > 1 && (size_t)nbuf * spb * r * nS * 4 > 170 * 1024) --spb;
+    if ((size_t)nbuf * spb * r * nS * 4 > 170 * 1024) nbuf = 1;
+    const size_t base = stats_smem_bytes(r, LP, n, spb, nbuf, 0);
+    if (base + (size_t)spb * NA * 4 > limit) return fail(OA_ERR_UNSUPPORTED, "n = %d is too large", n);
+    int spp = (int)((limit - base) / ((size_t)spb * NA * 4));
+    if (spp > nsets) spp = nsets;
+    if (spp < 1) spp = 1;
+    StatsArgs A{};
+    A.X = xr;
+    A.ldx = (size_t)n;
+    A.n = n;
+    A.n_pad = n_pad;
+    A.l = l;
+    A.QS = LP;
+    A.mb = mb;
+    A.spb = spb;
+    A.Qr = Qr;
+    A.nsets = nsets;
+    A.G = t;
+    A.Z = Z;
+    A.set_off = set_off;
+    A.rows = set_rows;
+    A.W = W;
+    A.pat_bad = pat_bad;
+    A.sets_per_pass = spp;
+    A.mean = mean;
+    A.has_nan = has_nan;
+    A.sinv = sinv;
+    A.sing = sing;
+    A.varx = varx;
+    A.aobs = aobs;
+    A.zA = zA;
+    A.zD = zD;
+    A.nbuf = nbuf;
+    A.err = reinterpret_cast<int*>(counters + 3);
+    int sms = 148;
+    NA_CU(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    const int groups = (mb + spb - 1) / spb;
+    NA_CU(oa_launch_snp_stats(r, LP, A, groups < sms ? groups : sms, stats_smem_bytes(r, LP, n, spb, nbuf, spp), st));
+
+    // XR'Y~ with the fused statistics, dense outputs only
+    EpiArgs E{};
+    E.n = n;
+    E.l = l;
+    E.r = r;
+    E.p = l + r;
+    E.mb = mb;
+    E.G = t;
+    E.pat = pat;
+    E.zset = zset;
+    E.rss0 = rss0;
+    E.sst = sst;
+    E.nobs = nobs;
+    E.b0 = b0;
+    E.sinv = sinv;
+    E.varx = varx;
+    E.sing = sing;
+    E.aobs = aobs;
+    E.zA = zA;
+    E.zD = zD;
+    E.zQ = zQ;
+    E.W = W;
+    E.store_all = 1;
+    E.rec = nullptr;
+    E.rec_count = counters;
+    E.cap = 0;
+    E.n_singular = counters + 1;
+    E.d_beta = beta;
+    E.d_se = se;
+    E.d_t = tstat;
+    E.d_r2 = r2;
+    E.d_sig = dsig;
+    E.t = t;
+    E.snp_base = 0;
+    E.dense_ld = mb;
+    NA_CU(oa_launch_gemm_simt(r, xr, (size_t)n, mb * r, Yt, (size_t)n_pad, t, n, mean, has_nan, E, st));
+    unsigned long long hc[4];
+    NA_CU(cudaMemcpyAsync(hc, counters, sizeof hc, cudaMemcpyDeviceToHost, st));
+    NA_CU(cudaStreamSynchronize(st));
+    if (hc[3]) return fail(OA_ERR_CUDA, "a device staging wait timed out");
+    return OA_OK;
+}

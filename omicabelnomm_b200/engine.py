@@ -93,6 +93,8 @@ def lib() -> C.CDLL:
         "oa_t_threshold": ([C.c_float], C.c_float),
         "oa_last_error": ([], C.c_char_p),
         "oa_abi_version": ([], C.c_int32),
+        "oa_scan_dense_noalloc": ([P, P, P, C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_int32, P, P, P, P,
+                                   P], C.c_int),
     }
     for name, (args, res) in sig.items():
         f = getattr(L, name)
@@ -234,6 +236,14 @@ class Engine:
         name = C.c_char_p()
         ms = lib().oa_last_kernel_ms(self.h, C.byref(name))
         return float(ms), (name.value or b"").decode()
+
+
+def scan_dense_noalloc(xl_ptr: int, y_ptr: int, xr_ptr: int, n: int, l: int, r: int, t: int, mb: int,
+                       beta_ptr: int, se_ptr: int, t_ptr: int, r2_ptr: int, stream: int = 0) -> None:
+    """oa_scan_dense_noalloc on device pointers (see include/omicabel_b200.h)."""
+    V = C.c_void_p
+    _check(lib().oa_scan_dense_noalloc(V(xl_ptr), V(y_ptr), V(xr_ptr), n, l, r, t, mb, V(beta_ptr), V(se_ptr),
+                                       V(t_ptr), V(r2_ptr), V(stream)))
 
 
 def t_threshold(p: float) -> float:
