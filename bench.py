@@ -162,7 +162,7 @@ def reference_available():
     return os.path.exists(REF_BIN) and os.access(REF_BIN, os.X_OK)
 
 
-def cpu_baseline(snps_per_proc: int = 24, steps: int = 1):
+def cpu_baseline(snps_per_proc: int = 48, steps: int = 1):
     """The reference CPU build on a bounded sample of the workload (~10-30 s of CPU)."""
     if not reference_available():
         return None
@@ -183,7 +183,7 @@ def run_reference_arm(args):
         print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/omicabelnomm_ref was not built"}))
         return 0
     procs = max(1, min(cpu_cores(), 64))
-    snps = 12
+    snps = 48
     with tempfile.TemporaryDirectory(prefix="oa_ref_") as d:
         n, t = prepare_reference_sample(d, snps, procs)
         for _ in range(args.warmup):
@@ -280,11 +280,13 @@ def main():
         launches0 = eng.launches()
         t0 = time.perf_counter()
         gemm_ms = 0.0
+        stats_ms = 0.0
         rows = 0
         for _ in range(args.steps):
             r = eng.run_device(XR.data_ptr(), m)
             ms, kname = eng.last_kernel_ms()
             gemm_ms += ms
+            stats_ms += eng.last_stats_ms()
             rows = r.count
         torch.cuda.synchronize()
         elapsed = time.perf_counter() - t0
@@ -292,6 +294,7 @@ def main():
         clk = clocks.stop()
         elapsed = max_over_ranks(elapsed)
         results[name] = dict(engine=eng, step_s=elapsed / args.steps, gemm_ms=gemm_ms / args.steps,
+                             stats_ms=stats_ms / args.steps,
                              kernel=kname, launches=(eng.launches() - launches0) // args.steps,
                              rows=rows, clocks=clk)
 
@@ -392,7 +395,8 @@ def main():
         "cpu_baseline": cpu,
         "clocks": R["clocks"],
         "forms": {k: ({"tests_per_s": tests * world / v["step_s"], "ms_per_step": v["step_s"] * 1e3,
-                       "gemm_ms": v["gemm_ms"], "stored_rows": v["rows"]} if "error" not in v else v)
+                       "gemm_ms": v["gemm_ms"], "stats_ms": v["stats_ms"], "stored_rows": v["rows"]}
+                      if "error" not in v else v)
                   for k, v in results.items()},
     }
     print(json.dumps(line))

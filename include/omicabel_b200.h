@@ -163,6 +163,8 @@ oa_status oa_scan_dense_noalloc(const float* xl_dev, const float* y_dev, const f
 int64_t oa_kernel_launches(const oa_engine* e);
 /* Device time (ms) of the dominant kernel in the last SNP block and its name. */
 float oa_last_kernel_ms(const oa_engine* e, const char** name);
+/* Device time (ms) of the per-SNP statistics kernel in the last SNP block. */
+float oa_last_stats_ms(const oa_engine* e);
 
 /* ---------------------------------------------------------------------------
  * Whole-run entry points

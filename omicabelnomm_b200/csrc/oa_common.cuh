@@ -11,6 +11,13 @@
 
 namespace oa {
 
+// Per-trait constants of the epilogue, gathered once per tile.
+struct TraitP {
+    double rss0;
+    float a_r2, inv_ncorr, vf;
+    int g, zs, orig;
+};
+
 // One stored row (a (trait, SNP) test with at least one stored SNP term),
 // the device form of the reference's resultH (src/Definitions.h:271-280).
 struct alignas(16) Rec {
@@ -19,7 +26,8 @@ struct alignas(16) Rec {
     float r2;           // R2 (src/Algorithm.cpp:1092)
     uint32_t mask;      // bit a: SNP term a (coefficient h = l + a) stored
     float sig;          // sqrt(RSS / n_corrected) (src/Algorithm.cpp:1100)
-    float pad[3];
+    int32_t tint;       // trait index in the engine's internal (pattern-sorted) order
+    float pad[2];
     float b[OA_MAX_R];
     float se[OA_MAX_R];
     float t[OA_MAX_R];
@@ -27,14 +35,18 @@ struct alignas(16) Rec {
 static_assert(sizeof(Rec) == 80, "Rec layout");
 
 // Everything the fused statistics epilogue reads, per trait and per SNP.
+// Per-trait arrays are in the engine's internal trait order (traits sorted
+// by missingness pattern, so consecutive traits share their Schur tables).
 struct EpiArgs {
     int n, l, r, p, mb, G;
     // per trait
     const int* pat;          // missingness pattern of the trait
     const int* zset;         // zero set of the trait or -1
+    const int* tperm;        // internal -> original trait index
     const double* rss0;      // RSS of the covariate-only fit over observed rows
-    const float* sst;        // SST as the reference computes it (src/Algorithm.cpp:1222-1251)
-    const int* nobs;         // n - missing
+    const float* a_r2;       // (n-1) / ((n_corr-1) SST): R2 = 1 - RSS a_r2 (src/Algorithm.cpp:1092)
+    const float* inv_ncorr;  // 1 / n_corr (src/Algorithm.cpp:1100)
+    const float* vf;         // (n - miss) / n, the reference's varFactor (src/Algorithm.cpp:1052)
     const double* b0;        // covariate-only coefficients in the orthonormal basis [t][l]
     // per SNP (and pattern)
     const double* sinv;      // inverse Schur complement per (pattern, SNP): [G][mb][r*r]

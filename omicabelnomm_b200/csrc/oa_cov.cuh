@@ -13,6 +13,7 @@ namespace oa {
 
 struct CovArgs {
     int n, l, r, p, mb;
+    const int* tinv;       // original -> internal trait index
     const int* pat;
     const double* b0;      // [t][l]
     const double* W;       // [G][l][l]
@@ -20,7 +21,7 @@ struct CovArgs {
     const float* afull;    // [mb][l][r]
     const double* sfinv;   // [mb][r*r]
     const double* Rinv;    // [l][l] upper triangular, row-major
-    const int* nobs;       // [t]
+    const int* nobs;       // [t] (internal order)
     float min_t;
     int store_all;
     double min_p_disp;
@@ -34,7 +35,7 @@ __device__ __forceinline__ double dev_pvalue(double t) {
     return erfc(t * 0.70710678118654752440);
 }
 
-// beta, SE, |t| of covariate terms h = 1 .. l-1 of one test.
+// beta, SE, |t| of covariate terms h = 1 .. l-1 of one test (j: internal trait index).
 template <int R>
 __device__ __forceinline__ void cov_eval(const CovArgs& C, int i, int j, const float* bx, float sig,
                                          float* ob, float* ose, float* ot) {
@@ -89,7 +90,7 @@ k_cov_terms(const Rec* __restrict__ rec, long long first, long long last, int sn
     if (idx >= last) return;
     const Rec rc = rec[idx];
     float b[OA_MAX_L], se[OA_MAX_L], t[OA_MAX_L];
-    cov_eval<R>(C, rc.snp - snp_base, rc.trait, rc.b, rc.sig, b, se, t);
+    cov_eval<R>(C, rc.snp - snp_base, rc.tint, rc.b, rc.sig, b, se, t);
     float* o = cov + (size_t)idx * C.l * 3;
     o[0] = o[1] = o[2] = 0.f;
     for (int h = 1; h < C.l; ++h) {
@@ -125,7 +126,7 @@ k_cov_count(const float* __restrict__ d_beta, const float* __restrict__ d_t, con
         }
         if (row) continue;                                 // counted from the stored row
         float b[OA_MAX_L], se[OA_MAX_L], tt[OA_MAX_L];
-        cov_eval<R>(C, i, j, bx, d_sig[o], b, se, tt);
+        cov_eval<R>(C, i, C.tinv[j], bx, d_sig[o], b, se, tt);
         for (int h = 1; h < C.l; ++h)
             if ((tt[h] > C.min_t || C.store_all) && C.min_p_disp > dev_pvalue((double)tt[h])) ++mine;
     }

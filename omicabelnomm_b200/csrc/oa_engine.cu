@@ -48,6 +48,15 @@ void set_err(const char* fmt, ...) {
         }                                                                                     \
     } while (0)
 
+// Drop an error left by an earlier runtime call whose status was already
+// handled (or deliberately ignored), so that the launch checks of this entry
+// point report only their own launches.
+inline void clear_stale_error(const char* where) {
+    const cudaError_t s = cudaGetLastError();
+    if (s != cudaSuccess && getenv("OA_DEBUG")) fprintf(stderr, "[oa] stale CUDA error before %s: %s\n", where,
+                                                        cudaGetErrorString(s));
+}
+
 #define OA_CHECK(x)                    \
     do {                               \
         oa_status s_ = (x);            \
@@ -188,6 +197,8 @@ struct oa_engine {
     cudaEvent_t ev_copied[2]{}, ev_used[2]{}, k0 = nullptr, k1 = nullptr;
     long long launches = 0;
     float last_ms = 0.f;
+    float stats_ms = 0.f;
+    cudaEvent_t s0 = nullptr, s1 = nullptr;
     const char* last_name = "";
     // covariates
     DBuf<double> Q64, Rinv;
@@ -198,9 +209,10 @@ struct oa_engine {
     DBuf<float> Yraw, Yt;
     DBuf<__nv_bfloat16> Yhi, Ylo;
     DBuf<double> tsums, rss0, b0, W, zQ;
-    DBuf<int> tcounts, pat, zset, nobs, set_off, set_rows, set_rep, set_kind, set_slot;
+    DBuf<int> tcounts, pat, zset, nobs, set_off, set_rows, set_rep, set_kind, set_slot, tperm, tinv;
+    DBuf<float> a_r2, inv_ncorr, vf;
     DBuf<unsigned long long> thash;
-    DBuf<float> sst;
+    DBuf<float> sst, qrows;
     DBuf<uint8_t> pat_bad;
     int G = 0, Z = 0, nsets = 0;
     std::vector<int> h_nobs;
@@ -220,6 +232,23 @@ struct oa_engine {
     DBuf<unsigned long long> keys, keys2;
     DBuf<int> perm, perm2;
     DBuf<unsigned char> cub_tmp;
+    // whole-scan CUDA graph of the device-resident path
+    struct GraphKey {
+        const float* xr = nullptr;
+        int mb = 0, t = 0, dense = 0;
+        long long gen = 0, cap = 0;
+        const void* rec = nullptr;
+        bool operator==(const GraphKey& o) const {
+            return xr == o.xr && mb == o.mb && t == o.t && dense == o.dense && gen == o.gen && cap == o.cap &&
+                   rec == o.rec;
+        }
+    };
+    GraphKey gkey, warm_key;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t gexec = nullptr;
+    long long trait_gen = 0;
+    std::vector<cudaEvent_t> cev0, cev1, sev0, sev1;
+    bool use_graphs = true;
     // dense outputs
     bool dense_on = false;
     DBuf<float> d_beta, d_se, d_t, d_r2, d_sig;
@@ -248,6 +277,7 @@ oa_status set_traits_impl(oa_engine* e, const float* y, int32_t t, bool device_p
     }
     const int n = e->n, l = e->l;
     e->t = t;
+    ++e->trait_gen;
     const float* Y = y;
     if (!device_ptr) {
         OA_CHECK(e->Yraw.ensure((size_t)n * t));
@@ -308,8 +338,21 @@ oa_status set_traits_impl(oa_engine* e, const float* y, int32_t t, bool device_p
     }
     e->h_nobs.resize(t);
     for (int j = 0; j < t; ++j) e->h_nobs[j] = n - counts[j * 2];
+    // internal trait order: sorted by (pattern, zero set) so that consecutive
+    // traits of a GEMM tile share their per-(pattern, SNP) Schur inverses
+    std::vector<int> order(t), inv(t), ipat(t), iz(t);
+    for (int j = 0; j < t; ++j) order[j] = j;
+    std::stable_sort(order.begin(), order.end(),
+                     [&](int a, int b) { return hpat[a] != hpat[b] ? hpat[a] < hpat[b] : hz[a] < hz[b]; });
+    for (int jj = 0; jj < t; ++jj) {
+        inv[order[jj]] = jj;
+        ipat[jj] = hpat[order[jj]];
+        iz[jj] = hz[order[jj]];
+    }
     OA_CHECK(e->pat.ensure(t));
     OA_CHECK(e->zset.ensure(t));
+    OA_CHECK(e->tperm.ensure(t));
+    OA_CHECK(e->tinv.ensure(t));
     OA_CHECK(e->set_off.ensure(e->nsets + 1));
     OA_CHECK(e->set_rep.ensure(e->nsets));
     OA_CHECK(e->set_kind.ensure(e->nsets));
@@ -318,8 +361,10 @@ oa_status set_traits_impl(oa_engine* e, const float* y, int32_t t, bool device_p
     OA_CHECK(e->W.ensure((size_t)std::max(e->G, 1) * l * l));
     OA_CHECK(e->zQ.ensure((size_t)std::max(e->Z, 1) * l * l));
     OA_CHECK(e->pat_bad.ensure(std::max(e->G, 1)));
-    OA_CU(cudaMemcpyAsync(e->pat.p, hpat.data(), sizeof(int) * t, cudaMemcpyHostToDevice, e->st));
-    OA_CU(cudaMemcpyAsync(e->zset.p, hz.data(), sizeof(int) * t, cudaMemcpyHostToDevice, e->st));
+    OA_CU(cudaMemcpyAsync(e->pat.p, ipat.data(), sizeof(int) * t, cudaMemcpyHostToDevice, e->st));
+    OA_CU(cudaMemcpyAsync(e->zset.p, iz.data(), sizeof(int) * t, cudaMemcpyHostToDevice, e->st));
+    OA_CU(cudaMemcpyAsync(e->tperm.p, order.data(), sizeof(int) * t, cudaMemcpyHostToDevice, e->st));
+    OA_CU(cudaMemcpyAsync(e->tinv.p, inv.data(), sizeof(int) * t, cudaMemcpyHostToDevice, e->st));
     OA_CU(cudaMemcpyAsync(e->set_off.p, off.data(), sizeof(int) * off.size(), cudaMemcpyHostToDevice, e->st));
     OA_CU(cudaMemcpyAsync(e->set_rep.p, rep.data(), sizeof(int) * rep.size(), cudaMemcpyHostToDevice, e->st));
     OA_CU(cudaMemcpyAsync(e->set_kind.p, kind.data(), sizeof(int) * kind.size(), cudaMemcpyHostToDevice, e->st));
@@ -328,6 +373,14 @@ oa_status set_traits_impl(oa_engine* e, const float* y, int32_t t, bool device_p
                                                    e->set_rows.p);
     k_set_gram<<<e->nsets, OA_NTHREADS, 0, e->st>>>(e->Q64.p, n, l, e->set_kind.p, e->set_off.p, e->set_rows.p,
                                                    e->W.p, e->zQ.p, e->set_slot.p, e->pat_bad.p);
+    const int total_rows = off[e->nsets];
+    OA_CHECK(e->qrows.ensure((size_t)std::max(total_rows, 1) * e->LP));
+    if (total_rows > 0) {
+        const long long nq = (long long)total_rows * e->LP;
+        k_set_qrows<<<(unsigned)((nq + 255) / 256), 256, 0, e->st>>>(e->set_rows.p, total_rows, e->Qr.p, e->LP,
+                                                                      e->qrows.p);
+        ++e->launches;
+    }
     e->launches += 2;
     OA_CU(cudaGetLastError());
     OA_CHECK(e->Yt.ensure((size_t)t * e->n_pad));
@@ -339,11 +392,14 @@ oa_status set_traits_impl(oa_engine* e, const float* y, int32_t t, bool device_p
     OA_CHECK(e->sst.ensure(t));
     OA_CHECK(e->nobs.ensure(t));
     OA_CHECK(e->b0.ensure((size_t)t * l));
+    OA_CHECK(e->a_r2.ensure(t));
+    OA_CHECK(e->inv_ncorr.ensure(t));
+    OA_CHECK(e->vf.ensure(t));
     const bool mixed = e->cfg.precision == OA_MIXED_BF16X3;
-    k_trait_resid<<<t, OA_NTHREADS, 0, e->st>>>(Y, (size_t)n, n, e->n_pad, l, e->Q64.p, e->tsums.p, e->tcounts.p,
-                                               e->pat.p, e->W.p, e->Yt.p, mixed ? e->Yhi.p : nullptr,
-                                               mixed ? e->Ylo.p : nullptr, e->rss0.p, e->sst.p, e->nobs.p,
-                                               e->b0.p);
+    k_trait_resid<<<t, OA_NTHREADS, 0, e->st>>>(Y, (size_t)n, n, e->n_pad, l, e->p, e->Q64.p, e->tsums.p,
+                                               e->tcounts.p, e->pat.p, e->W.p, e->tperm.p, e->Yt.p,
+                                               mixed ? e->Yhi.p : nullptr, mixed ? e->Ylo.p : nullptr, e->rss0.p,
+                                               e->sst.p, e->nobs.p, e->b0.p, e->a_r2.p, e->inv_ncorr.p, e->vf.p);
     ++e->launches;
     OA_CU(cudaGetLastError());
     OA_CU(cudaStreamSynchronize(e->st));
@@ -366,6 +422,7 @@ StatsArgs stats_args(oa_engine* e, const float* X, int mbc, int LP, int spb, int
     A.Z = e->Z;
     A.set_off = e->set_off.p;
     A.rows = e->set_rows.p;
+    A.qrows = e->qrows.p;
     A.W = e->W.p;
     A.pat_bad = e->pat_bad.p;
     A.sets_per_pass = spp;
@@ -431,9 +488,11 @@ EpiArgs epi_args(oa_engine* e, int mbc, int snp_base) {
     E.G = e->G;
     E.pat = e->pat.p;
     E.zset = e->zset.p;
+    E.tperm = e->tperm.p;
     E.rss0 = e->rss0.p;
-    E.sst = e->sst.p;
-    E.nobs = e->nobs.p;
+    E.a_r2 = e->a_r2.p;
+    E.inv_ncorr = e->inv_ncorr.p;
+    E.vf = e->vf.p;
     E.b0 = e->b0.p;
     E.sinv = e->sinv.p;
     E.varx = e->varx.p;
@@ -470,6 +529,7 @@ CovArgs cov_args(oa_engine* e, int mbc) {
     C.r = e->r;
     C.p = e->p;
     C.mb = mbc;
+    C.tinv = e->tinv.p;
     C.pat = e->pat.p;
     C.b0 = e->b0.p;
     C.W = e->W.p;
@@ -548,7 +608,9 @@ oa_status ensure_cap(oa_engine* e, long long want) {
 template <int R>
 oa_status run_chunk(oa_engine* e, const float* X, int mbc, int snp_base) {
     OA_CU(cudaMemsetAsync(e->has_nan.p, 0, sizeof(int), e->st));
+    OA_CU(cudaEventRecord(e->s0, e->st));
     OA_CHECK(stats_dispatch<R>(e, X, mbc));
+    OA_CU(cudaEventRecord(e->s1, e->st));
     unsigned long long before[4];
     OA_CU(cudaMemcpyAsync(before, e->counters.p, sizeof before, cudaMemcpyDeviceToHost, e->st));
     OA_CU(cudaStreamSynchronize(e->st));
@@ -562,6 +624,10 @@ oa_status run_chunk(oa_engine* e, const float* X, int mbc, int snp_base) {
         float ms = 0.f;
         cudaEventElapsedTime(&ms, e->k0, e->k1);
         e->last_ms += ms;
+        if (attempt == 0) {
+            cudaEventElapsedTime(&ms, e->s0, e->s1);
+            e->stats_ms += ms;
+        }
         if (after[3]) {
             set_err("a device pipeline wait timed out (the kernel stopped cleanly)");
             return OA_ERR_CUDA;
@@ -591,6 +657,106 @@ oa_status run_chunk(oa_engine* e, const float* X, int mbc, int snp_base) {
     return OA_ERR_NOMEM;
 }
 
+// Every chunk of a device-resident SNP block, enqueued without host
+// synchronisation (the body of the captured graph).
+template <int R>
+oa_status enqueue_scan(oa_engine* e, const float* xr, int mb) {
+    const int nch = (mb + e->chunk - 1) / e->chunk;
+    while ((int)e->cev0.size() < nch) {
+        cudaEvent_t ev[4];
+        for (auto& x : ev) OA_CU(cudaEventCreate(&x));
+        e->cev0.push_back(ev[0]);
+        e->cev1.push_back(ev[1]);
+        e->sev0.push_back(ev[2]);
+        e->sev1.push_back(ev[3]);
+    }
+    for (int c = 0; c < nch; ++c) {
+        const int c0 = c * e->chunk, mbc = std::min(e->chunk, mb - c0);
+        const float* X = xr + (size_t)c0 * e->r * e->n;
+        OA_CU(cudaMemsetAsync(e->has_nan.p, 0, sizeof(int), e->st));
+        OA_CU(cudaEventRecord(e->sev0[c], e->st));
+        OA_CHECK(stats_dispatch<R>(e, X, mbc));
+        OA_CU(cudaEventRecord(e->sev1[c], e->st));
+        OA_CU(cudaEventRecord(e->cev0[c], e->st));
+        OA_CHECK(gemm_dispatch<R>(e, X, mbc, c0));
+        OA_CU(cudaEventRecord(e->cev1[c], e->st));
+    }
+    return OA_OK;
+}
+
+void drop_graph(oa_engine* e) {
+    if (e->gexec) cudaGraphExecDestroy(e->gexec);
+    if (e->graph) cudaGraphDestroy(e->graph);
+    e->gexec = nullptr;
+    e->graph = nullptr;
+    e->gkey = oa_engine::GraphKey{};
+}
+
+// Device-resident scan as one CUDA graph launch (captured on the second
+// call with the same inputs; the first call runs uncaptured).  Returns
+// false in *done when the caller must run the uncaptured path instead.
+template <int R>
+oa_status run_graph(oa_engine* e, const float* xr, int mb, bool* done) {
+    *done = false;
+    oa_engine::GraphKey key;
+    key.xr = xr;
+    key.mb = mb;
+    key.t = e->t;
+    key.dense = e->dense_on ? 1 : 0;
+    key.gen = e->trait_gen;
+    key.cap = e->cap;
+    key.rec = e->rec.p;
+    if (!(e->gexec && e->gkey == key)) {
+        drop_graph(e);
+        if (!(e->warm_key == key)) {
+            e->warm_key = key;       // first sight: uncaptured run (sets kernel attributes)
+            return OA_OK;
+        }
+        OA_CU(cudaStreamBeginCapture(e->st, cudaStreamCaptureModeThreadLocal));
+        const oa_status s = enqueue_scan<R>(e, xr, mb);
+        cudaGraph_t g = nullptr;
+        const cudaError_t ce = cudaStreamEndCapture(e->st, &g);
+        if (s != OA_OK) {
+            if (g) cudaGraphDestroy(g);
+            return s;
+        }
+        OA_CU(ce);
+        e->graph = g;
+        OA_CU(cudaGraphInstantiate(&e->gexec, g, 0));
+        e->gkey = key;
+    }
+    OA_CU(cudaGraphLaunch(e->gexec, e->st));
+    const int nch = (mb + e->chunk - 1) / e->chunk;
+    e->launches += 3 * nch;
+    unsigned long long cnt[4];
+    OA_CU(cudaMemcpyAsync(cnt, e->counters.p, sizeof cnt, cudaMemcpyDeviceToHost, e->st));
+    OA_CU(cudaStreamSynchronize(e->st));
+    if (cnt[3]) {
+        set_err("a device pipeline wait timed out (the kernel stopped cleanly)");
+        return OA_ERR_CUDA;
+    }
+    if ((long long)cnt[0] > e->cap) {
+        // more stored rows than room: grow and let the caller run the uncaptured path
+        OA_CHECK(ensure_cap(e, (long long)(cnt[0] * 1.25) + 1024));
+        OA_CU(cudaMemsetAsync(e->counters.p, 0, 4 * sizeof(unsigned long long), e->st));
+        drop_graph(e);
+        return OA_OK;
+    }
+    float total = 0.f, stotal = 0.f;
+    for (int c = 0; c < nch; ++c) {
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, e->cev0[c], e->cev1[c]);
+        total += ms;
+        cudaEventElapsedTime(&ms, e->sev0[c], e->sev1[c]);
+        stotal += ms;
+    }
+    e->last_ms = total;
+    e->stats_ms = stotal;
+    e->last_name = e->cfg.precision == OA_PLAIN_FP32 ? "k_gemm_simt" : "k_gemm_tc";
+    *done = true;
+    return OA_OK;
+}
+
 template <int R>
 oa_status run_snps_impl(oa_engine* e, const float* xr, int32_t mb, bool host_input, bool results_on_host,
                         oa_rows* out) {
@@ -617,6 +783,7 @@ oa_status run_snps_impl(oa_engine* e, const float* xr, int32_t mb, bool host_inp
         e->dense_ld = mb;
     }
     e->last_ms = 0.f;
+    e->stats_ms = 0.f;
     e->last_mb = mb;
     const size_t colbytes = sizeof(float) * (size_t)e->n * e->r;
     const int nch = (mb + e->chunk - 1) / e->chunk;
@@ -642,10 +809,13 @@ oa_status run_snps_impl(oa_engine* e, const float* xr, int32_t mb, bool host_inp
             OA_CU(cudaEventRecord(e->ev_used[b], e->st));
         }
     } else {
-        for (int c = 0; c < nch; ++c) {
-            const int c0 = c * e->chunk, mbc = std::min(e->chunk, mb - c0);
-            OA_CHECK(run_chunk<R>(e, xr + (size_t)c0 * e->r * e->n, mbc, c0));
-        }
+        bool done = false;
+        if (e->use_graphs && !e->cfg.disp_cov) OA_CHECK(run_graph<R>(e, xr, mb, &done));
+        if (!done)
+            for (int c = 0; c < nch; ++c) {
+                const int c0 = c * e->chunk, mbc = std::min(e->chunk, mb - c0);
+                OA_CHECK(run_chunk<R>(e, xr + (size_t)c0 * e->r * e->n, mbc, c0));
+            }
     }
     unsigned long long cnt[3];
     OA_CU(cudaMemcpyAsync(cnt, e->counters.p, sizeof cnt, cudaMemcpyDeviceToHost, e->st));
@@ -748,6 +918,7 @@ oa_status run_snps_impl(oa_engine* e, const float* xr, int32_t mb, bool host_inp
 
 oa_status run_snps_any(oa_engine* e, const float* xr, int32_t mb, bool host_input, bool results_on_host,
                        oa_rows* out) {
+    clear_stale_error("oa_run_snps");
     if (!e || !xr || !out) {
         set_err("null argument");
         return OA_ERR_ARG;
@@ -775,6 +946,7 @@ void oa__set_error(const char* msg) { g_err = msg ? msg : ""; }
 int32_t oa_abi_version(void) { return OA_ABI_VERSION; }
 
 oa_status oa_engine_create(const oa_config* cfg, oa_engine** out) {
+    clear_stale_error(__func__);
     if (!cfg || !out) {
         set_err("null argument");
         return OA_ERR_ARG;
@@ -825,6 +997,8 @@ oa_status oa_engine_create(const oa_config* cfg, oa_engine** out) {
     e->n_pad = (cfg->n + 63) & ~63;
     const char* ch = getenv("OA_CHUNK_SNPS");
     e->chunk = std::min(cfg->max_snps, ch ? std::max(1, atoi(ch)) : 16384 / cfg->r);
+    const char* gr = getenv("OA_GRAPHS");
+    e->use_graphs = !(gr && gr[0] == '0');
     if (cudaStreamCreateWithFlags(&e->st, cudaStreamNonBlocking) != cudaSuccess ||
         cudaStreamCreateWithFlags(&e->cp, cudaStreamNonBlocking) != cudaSuccess) {
         set_err("stream creation failed");
@@ -838,6 +1012,8 @@ oa_status oa_engine_create(const oa_config* cfg, oa_engine** out) {
     }
     cudaEventCreate(&e->k0);
     cudaEventCreate(&e->k1);
+    cudaEventCreate(&e->s0);
+    cudaEventCreate(&e->s1);
     if (e->counters.ensure(4) != OA_OK) {
         delete e;
         return OA_ERR_NOMEM;
@@ -857,8 +1033,9 @@ oa_status oa_engine_destroy(oa_engine* e) {
                     &e->Xstage[1]})
         b->release();
     for (auto* b : {&e->tcounts, &e->pat, &e->zset, &e->nobs, &e->set_off, &e->set_rows, &e->set_rep, &e->set_kind,
-                    &e->set_slot, &e->has_nan, &e->perm, &e->perm2})
+                    &e->set_slot, &e->has_nan, &e->perm, &e->perm2, &e->tperm, &e->tinv})
         b->release();
+    for (auto* b : {&e->a_r2, &e->inv_ncorr, &e->vf, &e->qrows}) b->release();
     e->Yhi.release();
     e->Ylo.release();
     e->Xhi.release();
@@ -880,6 +1057,11 @@ oa_status oa_engine_destroy(oa_engine* e) {
     }
     cudaEventDestroy(e->k0);
     cudaEventDestroy(e->k1);
+    cudaEventDestroy(e->s0);
+    cudaEventDestroy(e->s1);
+    drop_graph(e);
+    for (auto* v : {&e->cev0, &e->cev1, &e->sev0, &e->sev1})
+        for (auto ev : *v) cudaEventDestroy(ev);
     cudaStreamDestroy(e->st);
     cudaStreamDestroy(e->cp);
     delete e;
@@ -887,6 +1069,7 @@ oa_status oa_engine_destroy(oa_engine* e) {
 }
 
 oa_status oa_set_covariates(oa_engine* e, const float* xl) {
+    clear_stale_error(__func__);
     if (!e || !xl) {
         set_err("null argument");
         return OA_ERR_ARG;
@@ -934,6 +1117,7 @@ oa_status oa_set_covariates(oa_engine* e, const float* xl) {
 }
 
 oa_status oa_set_traits(oa_engine* e, const float* y, int32_t t) {
+    clear_stale_error(__func__);
     if (!e || !y) {
         set_err("null argument");
         return OA_ERR_ARG;
@@ -943,6 +1127,7 @@ oa_status oa_set_traits(oa_engine* e, const float* y, int32_t t) {
 }
 
 oa_status oa_set_traits_device(oa_engine* e, const float* y, int32_t t) {
+    clear_stale_error(__func__);
     if (!e || !y) {
         set_err("null argument");
         return OA_ERR_ARG;
@@ -966,6 +1151,7 @@ oa_status oa_enable_dense(oa_engine* e, int32_t on) {
 }
 
 oa_status oa_dense_last(oa_engine* e, float* beta, float* se, float* tstat, float* r2) {
+    clear_stale_error(__func__);
     if (!e || !e->dense_on || e->last_mb == 0) {
         set_err("dense output was not enabled for the last SNP block");
         return OA_ERR_STATE;
@@ -986,5 +1172,7 @@ float oa_last_kernel_ms(const oa_engine* e, const char** name) {
     if (name) *name = e->last_name;
     return e->last_ms;
 }
+
+float oa_last_stats_ms(const oa_engine* e) { return e ? e->stats_ms : 0.f; }
 
 }  // extern "C"

@@ -13,23 +13,78 @@
 //   t_h    = |beta_h / SE_h|                                           (:1137)
 //
 // and applies the store filters (RSS > 0, R2 > minR2store or -f, t >
-// minTstore or -f, at least one stored SNP term; :1119-1203).
+// minTstore or -f, at least one stored SNP term; :1119-1203).  The RSS
+// difference is formed in FP64 (it can cancel); the rest is FP32, the
+// precision the reference holds these values in, with the per-trait
+// constants folded so that a test needs one reciprocal square root and no
+// division.
 #pragma once
 #include "oa_common.cuh"
 
 namespace oa {
 
+__device__ __forceinline__ TraitP load_trait(const EpiArgs& E, int j) {
+    TraitP p;
+    p.rss0 = E.rss0[j];
+    p.a_r2 = E.a_r2[j];
+    p.inv_ncorr = E.inv_ncorr[j];
+    p.vf = E.vf[j];
+    p.g = E.pat[j];
+    p.zs = E.zset[j];
+    p.orig = E.tperm[j];
+    return p;
+}
+
+// Schur inverse of (pattern g, SNP i); false if the system is singular.
 template <int R>
-__device__ __forceinline__ bool epi_eval(const EpiArgs& E, int i, int j, const float* z, bool valid,
-                                         Rec& rc) {
-    if (!valid) return false;
-    const int g = E.pat[j];
+__device__ __forceinline__ bool load_schur(const EpiArgs& E, int g, int i, double* S) {
     const size_t gi = (size_t)g * E.mb + i;
-    if (E.sing[gi]) {
-        atomicAdd(E.n_singular, 1ull);
-        return false;
+    if (E.sing[gi]) return false;
+    const double* src = E.sinv + gi * (R * R);
+#pragma unroll
+    for (int q = 0; q < R * R; ++q) S[q] = src[q];
+    return true;
+}
+
+// Fitted values of the observed rows whose y is exactly 0 leave the RSS
+// (src/Algorithm.cpp:1013-1020).  Rare (continuous phenotypes have no exact
+// zeros); reads the zero set's sums directly.
+template <int R>
+__device__ __noinline__ double zero_rows_rss(const EpiArgs& E, int i, int j, const TraitP& tp, const double* bx) {
+    const int l = E.l;
+    const size_t gi = (size_t)tp.g * E.mb + i;
+    const float* ao = E.aobs + gi * (size_t)(l * R);
+    const double* W = E.W + (size_t)tp.g * l * l;
+    double bq[OA_MAX_L], aob[OA_MAX_L];
+    for (int q = 0; q < l; ++q) {
+        double s = 0.0;
+        for (int a = 0; a < R; ++a) s += (double)ao[q * R + a] * bx[a];
+        aob[q] = s;
     }
-    const double* S = E.sinv + gi * (R * R);
+    for (int q = 0; q < l; ++q) {
+        double s = 0.0;
+        for (int u = 0; u < l; ++u) s += W[q * l + u] * aob[u];
+        bq[q] = E.b0[(size_t)j * l + q] - s;
+    }
+    const double* zQ = E.zQ + (size_t)tp.zs * l * l;
+    const float* zA = E.zA + ((size_t)tp.zs * E.mb + i) * (l * R);
+    const float* zD = E.zD + ((size_t)tp.zs * E.mb + i) * (R * R);
+    double c = 0.0;
+    for (int q = 0; q < l; ++q) {
+        double s = 0.0;
+        for (int u = 0; u < l; ++u) s += zQ[q * l + u] * bq[u];
+        c += bq[q] * s;
+        for (int a = 0; a < R; ++a) c += 2.0 * bq[q] * (double)zA[q * R + a] * bx[a];
+    }
+    for (int a = 0; a < R; ++a)
+        for (int b = 0; b < R; ++b) c += bx[a] * (double)zD[a * R + b] * bx[b];
+    return c;
+}
+
+// One test given its trait constants, Schur inverse S and the SNP's var_x.
+template <int R>
+__device__ __forceinline__ bool epi_core(const EpiArgs& E, int i, int j, const float* z, const TraitP& tp,
+                                         const double* S, const float* vx, Rec& rc) {
     double bx[R];
     double zz = 0.0;
 #pragma unroll
@@ -40,80 +95,76 @@ __device__ __forceinline__ bool epi_eval(const EpiArgs& E, int i, int j, const f
         bx[a] = s;
         zz += (double)z[a] * s;
     }
-    double rss = E.rss0[j] - zz;
-    const int zs = E.zset[j];
-    if (zs >= 0) {
-        // fitted values on the observed zero-y rows leave the RSS (src/Algorithm.cpp:1013-1020)
-        const int l = E.l;
-        const float* ao = E.aobs + gi * (size_t)(l * R);
-        const double* W = E.W + (size_t)g * l * l;
-        double bq[OA_MAX_L];
-        double aob[OA_MAX_L];
-        for (int q = 0; q < l; ++q) {
-            double s = 0.0;
-#pragma unroll
-            for (int a = 0; a < R; ++a) s += (double)ao[q * R + a] * bx[a];
-            aob[q] = s;
-        }
-        for (int q = 0; q < l; ++q) {
-            double s = 0.0;
-            for (int u = 0; u < l; ++u) s += W[q * l + u] * aob[u];
-            bq[q] = E.b0[(size_t)j * l + q] - s;
-        }
-        const double* zQ = E.zQ + (size_t)zs * l * l;
-        const float* zA = E.zA + ((size_t)zs * E.mb + i) * (l * R);
-        const float* zD = E.zD + ((size_t)zs * E.mb + i) * (R * R);
-        double c = 0.0;
-        for (int q = 0; q < l; ++q) {
-            double s = 0.0;
-            for (int u = 0; u < l; ++u) s += zQ[q * l + u] * bq[u];
-            c += bq[q] * s;
-#pragma unroll
-            for (int a = 0; a < R; ++a) c += 2.0 * bq[q] * (double)zA[q * R + a] * bx[a];
-        }
-#pragma unroll
-        for (int a = 0; a < R; ++a)
-#pragma unroll
-            for (int b = 0; b < R; ++b) c += bx[a] * (double)zD[a * R + b] * bx[b];
-        rss -= c;
-    }
-    const int nobs = E.nobs[j];
-    const int ncorr = nobs - E.p;
-    const double R2 = 1.0 - (rss / (double)(ncorr - 1)) / ((double)E.sst[j] / (double)(E.n - 1));
-    const double sig = sqrt(fmax(rss, 0.0) / (double)ncorr);
-    const double vf = (double)nobs / (double)E.n;
-    rc.trait = j;
+    double rss = tp.rss0 - zz;
+    if (tp.zs >= 0) rss -= zero_rows_rss<R>(E, i, j, tp, bx);
+    const float rssf = (float)rss;
+    const float r2 = 1.f - rssf * tp.a_r2;
+    const float sig2 = rssf * tp.inv_ncorr;
+    rc.trait = tp.orig;
     rc.snp = E.snp_base + i;
-    rc.r2 = (float)R2;
-    rc.sig = (float)sig;
-    rc.pad[0] = rc.pad[1] = rc.pad[2] = 0.f;
+    rc.r2 = r2;
+    rc.sig = sqrtf(fmaxf(sig2, 0.f));
+    rc.tint = j;
+    rc.pad[0] = rc.pad[1] = 0.f;
     uint32_t mask = 0;
 #pragma unroll
     for (int a = 0; a < R; ++a) {
-        const double se = sig * sqrt((double)E.varx[(size_t)i * R + a] * vf);
-        const double t = fabs(bx[a] / se);
-        rc.b[a] = (float)bx[a];
-        rc.se[a] = (float)se;
-        rc.t[a] = (float)t;
-        if (t > (double)E.min_t || E.store_all) mask |= 1u << a;
+        const float w = sig2 * vx[a] * tp.vf;       // SE^2
+        const float rs = rsqrtf(w);
+        const float b = (float)bx[a];
+        const float t = fabsf(b) * rs;
+        rc.b[a] = b;
+        rc.se[a] = w * rs;
+        rc.t[a] = t;
+        if (t > E.min_t || E.store_all) mask |= 1u << a;
     }
 #pragma unroll
     for (int a = R; a < OA_MAX_R; ++a) rc.b[a] = rc.se[a] = rc.t[a] = 0.f;
     rc.mask = mask;
-    const bool live = (rss > 0.0) && (R2 > (double)E.min_r2 || E.store_all);
+    const bool live = (rss > 0.0) && (r2 > E.min_r2 || E.store_all);
     if (E.d_r2) {
-        const size_t o = (size_t)j * E.dense_ld + E.snp_base + i;
+        const size_t o = (size_t)tp.orig * E.dense_ld + E.snp_base + i;
         const float nanf_ = __int_as_float(0x7fc00000);
-        E.d_r2[o] = rss > 0.0 ? (float)R2 : nanf_;
-        E.d_sig[o] = rss > 0.0 ? (float)sig : nanf_;
+        const bool pos = rss > 0.0;
+        E.d_r2[o] = pos ? r2 : nanf_;
+        E.d_sig[o] = pos ? rc.sig : nanf_;
 #pragma unroll
         for (int a = 0; a < R; ++a) {
-            E.d_beta[o * R + a] = rss > 0.0 ? rc.b[a] : nanf_;
-            E.d_se[o * R + a] = rss > 0.0 ? rc.se[a] : nanf_;
-            E.d_t[o * R + a] = rss > 0.0 ? rc.t[a] : nanf_;
+            E.d_beta[o * R + a] = pos ? rc.b[a] : nanf_;
+            E.d_se[o * R + a] = pos ? rc.se[a] : nanf_;
+            E.d_t[o * R + a] = pos ? rc.t[a] : nanf_;
         }
     }
     return live && mask != 0u;
+}
+
+// Dense outputs of a singular test are NaN.
+template <int R>
+__device__ __forceinline__ void epi_dense_nan(const EpiArgs& E, int i, const TraitP& tp) {
+    if (!E.d_r2) return;
+    const size_t o = (size_t)tp.orig * E.dense_ld + E.snp_base + i;
+    const float nanf_ = __int_as_float(0x7fc00000);
+    E.d_r2[o] = nanf_;
+    E.d_sig[o] = nanf_;
+#pragma unroll
+    for (int a = 0; a < R; ++a) E.d_beta[o * R + a] = E.d_se[o * R + a] = E.d_t[o * R + a] = nanf_;
+}
+
+// Self-contained evaluation (loads its own constants): the SIMT GEMM epilogue.
+template <int R>
+__device__ __forceinline__ bool epi_eval(const EpiArgs& E, int i, int j, const float* z, bool valid, Rec& rc) {
+    if (!valid) return false;
+    const TraitP tp = load_trait(E, j);
+    double S[R * R];
+    if (!load_schur<R>(E, tp.g, i, S)) {
+        atomicAdd(E.n_singular, 1ull);
+        epi_dense_nan<R>(E, i, tp);
+        return false;
+    }
+    float vx[R];
+#pragma unroll
+    for (int a = 0; a < R; ++a) vx[a] = E.varx[(size_t)i * R + a];
+    return epi_core<R>(E, i, j, z, tp, S, vx, rc);
 }
 
 // Warp-aggregated append of the stored rows (one atomic per warp and slot).

@@ -45,8 +45,8 @@ struct Shape {
     static constexpr int A_BYTES = BM * BK * 2;                     // one of hi / lo
     static constexpr int B_BYTES = BN * BK * 2;
     static constexpr int STAGE_BYTES = 2 * A_BYTES + 2 * B_BYTES;
-    static constexpr size_t SMEM_BYTES =
-        1024 + (size_t)STAGES * STAGE_BYTES + (size_t)EPI_WARPS * 32 * STG_STRIDE * 4;
+    static constexpr size_t SMEM_BYTES = 1024 + (size_t)STAGES * STAGE_BYTES +
+                                         (size_t)EPI_WARPS * 32 * STG_STRIDE * 4 + (size_t)BN * sizeof(TraitP);
     static constexpr uint64_t LAYOUT = BK == 64 ? 2u : 4u;          // SWIZZLE_128B : SWIZZLE_64B
     static constexpr uint32_t SBO = BK == 64 ? 1024u : 512u;        // bytes between 8-row groups
 };
@@ -160,6 +160,7 @@ k_gemm_tc(const __grid_constant__ CUtensorMap mAhi, const __grid_constant__ CUte
     extern __shared__ uint8_t smem_raw[];
     uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~(uintptr_t)1023);
     float* stg = reinterpret_cast<float*>(smem + (size_t)STAGES * STAGE_BYTES);
+    TraitP* tps = reinterpret_cast<TraitP*>(stg + (size_t)EPI_WARPS * 32 * STG_STRIDE);   // this tile's traits
     __shared__ __align__(8) uint64_t full_bar[STAGES], empty_bar[STAGES], acc_full[2], acc_empty[2], done_bar;
     __shared__ uint32_t tmem_base_sh;
     __shared__ volatile int abort_sh;
@@ -278,38 +279,74 @@ k_gemm_tc(const __grid_constant__ CUtensorMap mAhi, const __grid_constant__ CUte
         }
     } else {
         // ---------------- epilogue ----------------
+        // The 128 epilogue threads synchronise among themselves with named
+        // barrier 1; every decision that ends the loop is taken right after
+        // it, so all of them leave together.
         const int ew = warp - 2;                 // 0..3
         const int lg = warp & 3;                 // TMEM lane group this warp may access
+        const int et = ew * 32 + lane;           // 0..127
         float* my = stg + (size_t)ew * 32 * STG_STRIDE;
         int acc = 0;
         uint32_t aph = 0;
         for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
             const int m0 = (tile / n_tiles) * BM, n0 = (tile % n_tiles) * BN;
-            if (!mbar_wait(&acc_full[acc], aph, &abort_sh)) break;
-            fence_after();
+            asm volatile("bar.sync 1, 128;" ::: "memory");     // previous tile's readers are done
+            if (abort_sh) break;
+            // trait constants of this tile (the main loop of the tile is still running)
+            for (int q = et; q < BN; q += 128)
+                if (n0 + q < t) tps[q] = load_trait(E, n0 + q);
             const int row = m0 + lg * 32 + lane;   // SNP column of this lane
-            for (int c0 = 0; c0 < BN && n0 + c0 < t; c0 += 32) {
-                uint32_t v[32];
-                tmem_ld32(tmem_base + ((uint32_t)(lg * 32) << 16) + (uint32_t)(acc * BN + c0), v);
+            const bool lead = ((lane & (R - 1)) == 0) && (row < xrows);
+            const int i = row / R;
+            float vx[R];
 #pragma unroll
-                for (int q = 0; q < 32; ++q) my[lane * STG_STRIDE + q] = __uint_as_float(v[q]);
-                __syncwarp();
-                const int qmax = min(32, t - n0 - c0);
-                for (int q = 0; q < qmax; ++q) {
-                    const int j = n0 + c0 + q;
-                    const float zf = my[lane * STG_STRIDE + q];
-                    float z[R];
+            for (int a = 0; a < R; ++a) vx[a] = lead ? E.varx[(size_t)i * R + a] : 1.f;
+            asm volatile("bar.sync 1, 128;" ::: "memory");
+            // accumulator ready (the wait is per warp: lane 0 waits, the warp follows)
+            int ok = 1;
+            if (lane == 0) ok = mbar_wait(&acc_full[acc], aph, &abort_sh) ? 1 : 0;
+            ok = __shfl_sync(0xffffffffu, ok, 0);
+            if (ok) {
+                mbar_try(&acc_full[acc], aph);
+                fence_after();
+                int cg = -1;            // pattern whose Schur inverse is cached
+                bool csing = true;
+                double S[R * R];
+                for (int c0 = 0; c0 < BN && n0 + c0 < t; c0 += 32) {
+                    uint32_t v[32];
+                    tmem_ld32(tmem_base + ((uint32_t)(lg * 32) << 16) + (uint32_t)(acc * BN + c0), v);
 #pragma unroll
-                    for (int a = 0; a < R; ++a) z[a] = __shfl_sync(0xffffffffu, zf, (lane & ~(R - 1)) + a);
-                    const bool valid = ((lane & (R - 1)) == 0) && (row < xrows);
-                    Rec rc;
-                    const bool st = epi_eval<R>(E, row / R, j, z, valid, rc);
-                    epi_emit(E, st, rc);
+                    for (int q = 0; q < 32; ++q) my[lane * STG_STRIDE + q] = __uint_as_float(v[q]);
+                    __syncwarp();
+                    const int qmax = min(32, t - n0 - c0);
+                    for (int q = 0; q < qmax; ++q) {
+                        const int j = n0 + c0 + q;
+                        const TraitP tp = tps[c0 + q];
+                        const float zf = my[lane * STG_STRIDE + q];
+                        float z[R];
+#pragma unroll
+                        for (int a = 0; a < R; ++a) z[a] = __shfl_sync(0xffffffffu, zf, (lane & ~(R - 1)) + a);
+                        if (tp.g != cg) {    // traits are sorted by pattern: reloads are rare
+                            cg = tp.g;
+                            csing = lead ? !load_schur<R>(E, cg, i, S) : true;
+                        }
+                        Rec rc;
+                        bool st = false;
+                        if (lead) {
+                            if (csing) {
+                                atomicAdd(E.n_singular, 1ull);
+                                epi_dense_nan<R>(E, i, tp);
+                            } else {
+                                st = epi_core<R>(E, i, j, z, tp, S, vx, rc);
+                            }
+                        }
+                        epi_emit(E, st, rc);
+                    }
+                    __syncwarp();
                 }
-                __syncwarp();
+                fence_before();
+                mbar_arrive(&acc_empty[acc]);
             }
-            fence_before();
-            mbar_arrive(&acc_empty[acc]);
             if (++acc == 2) {
                 acc = 0;
                 aph ^= 1u;
@@ -369,9 +406,15 @@ static cudaError_t go(const __nv_bfloat16* Xhi, const __nv_bfloat16* Xlo, int xr
         cudaGetDevice(&dev);
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     }
-    cudaError_t e = cudaFuncSetAttribute(k_gemm_tc<R, SH>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)SH::SMEM_BYTES);
-    if (e != cudaSuccess) return e;
+    static int attr_done[64];
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (!attr_done[dev & 63]) {   // once per device, never during a stream capture
+        cudaError_t e = cudaFuncSetAttribute(k_gemm_tc<R, SH>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             (int)SH::SMEM_BYTES);
+        if (e != cudaSuccess) return e;
+        attr_done[dev & 63] = 1;
+    }
     const int ntiles = ((xrows + BM - 1) / BM) * ((t + BN - 1) / BN);
     const int grid = ntiles < sms ? ntiles : sms;
     k_gemm_tc<R, SH><<<grid, NUM_THREADS, SH::SMEM_BYTES, st>>>(a_hi, a_lo, b_hi, b_lo, xrows, t, n_pad / SH::BK,

@@ -177,29 +177,34 @@ k_set_gram(const double* __restrict__ Q64, int n, int l, const int* __restrict__
 }
 
 // y~ = y - Q b0 on observed rows (0 on missing rows), b0 = W Q'y.
-// Writes Y~ (FP32, and BF16 hi/lo for the tensor-core form), RSS0 and SST.
+// Block jj builds internal trait jj = original trait tperm[jj] (traits are
+// kept sorted by missingness pattern inside the engine).  Writes Y~ (FP32,
+// and BF16 hi/lo for the tensor-core form), RSS0, SST and the constants the
+// epilogue folds: a_r2 = (n-1)/((n_corr-1) SST), 1/n_corr, (n-miss)/n.
 static __global__ void __launch_bounds__(OA_NTHREADS)
-k_trait_resid(const float* __restrict__ Y, size_t ldy, int n, int n_pad, int l,
+k_trait_resid(const float* __restrict__ Y, size_t ldy, int n, int n_pad, int l, int p,
               const double* __restrict__ Q64, const double* __restrict__ sums,
               const int* __restrict__ counts, const int* __restrict__ pat,
-              const double* __restrict__ W, float* __restrict__ Yt,
+              const double* __restrict__ W, const int* __restrict__ tperm, float* __restrict__ Yt,
               __nv_bfloat16* __restrict__ Yhi, __nv_bfloat16* __restrict__ Ylo,
               double* __restrict__ rss0, float* __restrict__ sst, int* __restrict__ nobs,
-              double* __restrict__ b0out) {
+              double* __restrict__ b0out, float* __restrict__ a_r2, float* __restrict__ inv_ncorr,
+              float* __restrict__ vf) {
     __shared__ double b0[OA_MAX_L];
     __shared__ double red[8];
-    const int j = blockIdx.x;
+    const int jj = blockIdx.x;
+    const int j = tperm[jj];
     const double* sj = sums + (size_t)j * (2 + OA_MAX_L);
     if (threadIdx.x < l) {
-        const double* Wg = W + (size_t)pat[j] * l * l;
+        const double* Wg = W + (size_t)pat[jj] * l * l;
         double acc = 0.0;
         for (int b = 0; b < l; ++b) acc += Wg[threadIdx.x * l + b] * sj[2 + b];
         b0[threadIdx.x] = acc;
-        b0out[(size_t)j * l + threadIdx.x] = acc;
+        b0out[(size_t)jj * l + threadIdx.x] = acc;
     }
     __syncthreads();
     const float* y = Y + (size_t)j * ldy;
-    float* out = Yt + (size_t)j * n_pad;
+    float* out = Yt + (size_t)jj * n_pad;
     double rss = 0.0;
     for (int k = threadIdx.x; k < n_pad; k += blockDim.x) {
         float e = 0.0f;
@@ -216,8 +221,8 @@ k_trait_resid(const float* __restrict__ Y, size_t ldy, int n, int n_pad, int l,
         out[k] = e;
         if (Yhi) {
             const __nv_bfloat16 hi = __float2bfloat16_rn(e);
-            Yhi[(size_t)j * n_pad + k] = hi;
-            Ylo[(size_t)j * n_pad + k] = __float2bfloat16_rn(e - __bfloat162float(hi));
+            Yhi[(size_t)jj * n_pad + k] = hi;
+            Ylo[(size_t)jj * n_pad + k] = __float2bfloat16_rn(e - __bfloat162float(hi));
         }
     }
     rss = warp_sum(rss);
@@ -226,12 +231,28 @@ k_trait_resid(const float* __restrict__ Y, size_t ldy, int n, int n_pad, int l,
     if (threadIdx.x == 0) {
         double s = 0.0;
         for (int w = 0; w < (int)(blockDim.x >> 5); ++w) s += red[w];
-        rss0[j] = s;
+        rss0[jj] = s;
         const int no = n - counts[j * 2];
-        nobs[j] = no;
+        nobs[jj] = no;
         // the reference holds SST in long double and stores it as float (src/Algorithm.cpp:1227-1240)
-        sst[j] = (float)(sj[1] - sj[0] * sj[0] / (double)no);
+        const float sstf = (float)(sj[1] - sj[0] * sj[0] / (double)no);
+        sst[jj] = sstf;
+        const int ncorr = no - p;
+        a_r2[jj] = (float)((double)(n - 1) / ((double)(ncorr - 1) * (double)sstf));
+        inv_ncorr[jj] = (float)(1.0 / (double)ncorr);
+        vf[jj] = (float)((double)no / (double)n);
     }
+}
+
+// Q rows of every row set's rows, stored contiguously in set order, so that
+// the per-SNP downdate gathers read them with independent coalesced loads.
+static __global__ void k_set_qrows(const int* __restrict__ rows, int total, const float* __restrict__ Qr, int LP,
+                                   float* __restrict__ qrows) {
+    const long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (q >= (long long)total * LP) return;
+    const long long kk = q / LP;
+    const int c = (int)(q % LP);
+    qrows[q] = Qr[(size_t)rows[kk] * LP + c];
 }
 
 // Sort keys of the stored rows: (trait, SNP) -> reference output order.

@@ -134,12 +134,14 @@ __global__ void __launch_bounds__(256) k_na_cholq(const T* __restrict__ X, int n
 // Row sets with every trait its own missingness pattern, plus one zero set
 // per trait that has observed values exactly 0.  counts[j] = (missing, zeros).
 __global__ void k_na_sets(const int* __restrict__ counts, int t, int* __restrict__ pat, int* __restrict__ zset,
-                          int* __restrict__ set_off, int* __restrict__ set_rep, int* __restrict__ set_kind,
-                          int* __restrict__ set_slot, int* __restrict__ info /* [0] Z, [1] rows */) {
+                          int* __restrict__ tperm, int* __restrict__ set_off, int* __restrict__ set_rep,
+                          int* __restrict__ set_kind, int* __restrict__ set_slot,
+                          int* __restrict__ info /* [0] Z, [1] rows */) {
     if (threadIdx.x != 0 || blockIdx.x != 0) return;
     int z = 0, off = 0;
     for (int j = 0; j < t; ++j) {
         pat[j] = j;
+        tperm[j] = j;
         set_off[j] = off;
         set_rep[j] = j;
         set_kind[j] = 0;
@@ -208,6 +210,7 @@ extern "C" oa_status oa_scan_dense_noalloc(const float* xl, const float* y, cons
                                            float* r2, void* stream) {
     using namespace oa;
     using namespace oa::na;
+    cudaGetLastError();   // an error left by an earlier, already-handled call is not ours
     if (!xl || !y || !xr || !beta || !se || !tstat || !r2) return fail(OA_ERR_ARG, "null argument");
     if (l < 1 || l > OA_MAX_L || !(r == 1 || r == 2 || r == 4) || n <= l + r || t < 1 || mb < 1 || t > 2048)
         return fail(OA_ERR_ARG, "invalid sizes n=%d l=%d r=%d t=%d mb=%d (r in {1,2,4}, t <= 2048)", n, l, r, t,
@@ -232,6 +235,10 @@ extern "C" oa_status oa_scan_dense_noalloc(const float* xl, const float* y, cons
     unsigned long long* thash = cv.take<unsigned long long>((size_t)t * 4);
     int* pat = cv.take<int>(t);
     int* zset = cv.take<int>(t);
+    int* tperm = cv.take<int>(t);
+    float* a_r2 = cv.take<float>(t);
+    float* inv_ncorr = cv.take<float>(t);
+    float* vf = cv.take<float>(t);
     int* set_off = cv.take<int>((size_t)2 * t + 1);
     int* set_rep = cv.take<int>((size_t)2 * t);
     int* set_kind = cv.take<int>((size_t)2 * t);
@@ -268,7 +275,7 @@ extern "C" oa_status oa_scan_dense_noalloc(const float* xl, const float* y, cons
     // traits: missing counts, sums, Q'y; one row set per trait
     TraitStatsOut tso{tsums, tcounts, thash};
     k_trait_stats<<<t, OA_NTHREADS, 0, st>>>(y, (size_t)n, n, l, Q64, tso);
-    k_na_sets<<<1, 1, 0, st>>>(tcounts, t, pat, zset, set_off, set_rep, set_kind, set_slot, info);
+    k_na_sets<<<1, 1, 0, st>>>(tcounts, t, pat, zset, tperm, set_off, set_rep, set_kind, set_slot, info);
     NA_CU(cudaGetLastError());
     int hinfo[4] = {0, 0, 0, 0};
     NA_CU(cudaMemcpyAsync(hinfo, info, sizeof hinfo, cudaMemcpyDeviceToHost, st));
@@ -277,6 +284,7 @@ extern "C" oa_status oa_scan_dense_noalloc(const float* xl, const float* y, cons
         return fail(OA_ERR_COLLINEAR, "the covariate matrix contains linearly dependent columns");
     const int Z = hinfo[0], nrows = hinfo[1], nsets = t + Z;
     int* set_rows = cv.take<int>((size_t)(nrows > 0 ? nrows : 1));
+    float* qrows = cv.take<float>((size_t)(nrows > 0 ? nrows : 1) * LP);
     float* zA = cv.take<float>((size_t)(Z > 0 ? Z : 1) * mb * l * r);
     float* zD = cv.take<float>((size_t)(Z > 0 ? Z : 1) * mb * r * r);
     float* aobs = Z > 0 ? cv.take<float>((size_t)t * mb * l * r) : nullptr;
@@ -286,8 +294,10 @@ extern "C" oa_status oa_scan_dense_noalloc(const float* xl, const float* y, cons
                     (unsigned)OA_NOALLOC_SCRATCH_BYTES);
     k_set_rows<<<nsets, OA_NTHREADS, 0, st>>>(y, (size_t)n, n, set_rep, set_kind, set_off, set_rows);
     k_set_gram<<<nsets, OA_NTHREADS, 0, st>>>(Q64, n, l, set_kind, set_off, set_rows, W, zQ, set_slot, pat_bad);
-    k_trait_resid<<<t, OA_NTHREADS, 0, st>>>(y, (size_t)n, n, n_pad, l, Q64, tsums, tcounts, pat, W, Yt, nullptr,
-                                            nullptr, rss0, sst, nobs, b0);
+    if (nrows > 0)
+        k_set_qrows<<<(unsigned)(((long long)nrows * LP + 255) / 256), 256, 0, st>>>(set_rows, nrows, Qr, LP, qrows);
+    k_trait_resid<<<t, OA_NTHREADS, 0, st>>>(y, (size_t)n, n, n_pad, l, l + r, Q64, tsums, tcounts, pat, W, tperm,
+                                            Yt, nullptr, nullptr, rss0, sst, nobs, b0, a_r2, inv_ncorr, vf);
     NA_CU(cudaGetLastError());
 
     // per-SNP statistics (same geometry rule as the block engine)
@@ -318,6 +328,7 @@ extern "C" oa_status oa_scan_dense_noalloc(const float* xl, const float* y, cons
     A.Z = Z;
     A.set_off = set_off;
     A.rows = set_rows;
+    A.qrows = qrows;
     A.W = W;
     A.pat_bad = pat_bad;
     A.sets_per_pass = spp;
@@ -346,9 +357,11 @@ extern "C" oa_status oa_scan_dense_noalloc(const float* xl, const float* y, cons
     E.G = t;
     E.pat = pat;
     E.zset = zset;
+    E.tperm = tperm;
     E.rss0 = rss0;
-    E.sst = sst;
-    E.nobs = nobs;
+    E.a_r2 = a_r2;
+    E.inv_ncorr = inv_ncorr;
+    E.vf = vf;
     E.b0 = b0;
     E.sinv = sinv;
     E.varx = varx;

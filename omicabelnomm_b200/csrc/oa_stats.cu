@@ -8,15 +8,27 @@ template <int R, int LP>
 static cudaError_t go(const StatsArgs& A, int grid, size_t smem, cudaStream_t st) {
     // TMA bulk staging needs 16-byte aligned columns whose size is a multiple of 16 bytes
     const bool bulk = (A.n % 4 == 0) && (A.ldx % 4 == 0) && ((reinterpret_cast<uintptr_t>(A.X) & 15) == 0);
+    // the opt-in shared-memory size is raised once per kernel and device (no
+    // attribute call while a stream is being captured into a graph)
+    static int set_bulk[64], set_plain[64];
+    int dev = 0;
+    cudaGetDevice(&dev);
+    const int d = dev & 63;
     if (bulk) {
-        cudaError_t e = cudaFuncSetAttribute(k_snp_stats<R, LP, true>,
-                                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        if (e != cudaSuccess) return e;
+        if (set_bulk[d] < (int)smem) {
+            cudaError_t e = cudaFuncSetAttribute(k_snp_stats<R, LP, true>,
+                                                 cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024 - 1024);
+            if (e != cudaSuccess) return e;
+            set_bulk[d] = 227 * 1024 - 1024;
+        }
         k_snp_stats<R, LP, true><<<grid, OA_NTHREADS, smem, st>>>(A);
     } else {
-        cudaError_t e = cudaFuncSetAttribute(k_snp_stats<R, LP, false>,
-                                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        if (e != cudaSuccess) return e;
+        if (set_plain[d] < (int)smem) {
+            cudaError_t e = cudaFuncSetAttribute(k_snp_stats<R, LP, false>,
+                                                 cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024 - 1024);
+            if (e != cudaSuccess) return e;
+            set_plain[d] = 227 * 1024 - 1024;
+        }
         k_snp_stats<R, LP, false><<<grid, OA_NTHREADS, smem, st>>>(A);
     }
     return cudaGetLastError();

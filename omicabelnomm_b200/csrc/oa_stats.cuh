@@ -42,6 +42,7 @@ struct StatsArgs {
     int nsets, G, Z;     // row sets: G patterns then Z zero sets
     const int* set_off;
     const int* rows;
+    const float* qrows;  // Q rows of each set's rows, gathered contiguous ([rows][QS], FP32)
     const double* W;     // [G][l][l]
     const uint8_t* pat_bad;
     int sets_per_pass;   // row sets whose sums fit in shared memory at once
@@ -256,7 +257,7 @@ k_snp_stats(StatsArgs A) {
         float acc[ACC];
 #pragma unroll
         for (int u = 0; u < ACC; ++u) acc[u] = 0.f;
-#pragma unroll 2
+#pragma unroll 4
         for (int k = threadIdx.x; k < n; k += blockDim.x) {
             float qk[LP];
 #pragma unroll
@@ -328,13 +329,13 @@ k_snp_stats(StatsArgs A) {
 #pragma unroll
                 for (int u = 0; u < ACC; ++u) acc[u] = 0.f;
                 const int r0 = A.set_off[set], r1 = A.set_off[set + 1];
-#pragma unroll 2
+#pragma unroll 4
                 for (int kk = r0 + lane; kk < r1; kk += 32) {
-                    const int k = A.rows[kk];
+                    const int k = __ldg(A.rows + kk);
                     float qk[LP];
 #pragma unroll
                     for (int q4 = 0; q4 < LP / 4; ++q4) {
-                        const float4 v = __ldg(reinterpret_cast<const float4*>(A.Qr + (size_t)k * LP + 4 * q4));
+                        const float4 v = __ldg(reinterpret_cast<const float4*>(A.qrows + (size_t)kk * LP + 4 * q4));
                         qk[4 * q4] = v.x; qk[4 * q4 + 1] = v.y; qk[4 * q4 + 2] = v.z; qk[4 * q4 + 3] = v.w;
                     }
 #pragma unroll

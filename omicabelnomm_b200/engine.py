@@ -86,6 +86,7 @@ def lib() -> C.CDLL:
         "oa_enable_dense": ([P, C.c_int32], C.c_int),
         "oa_kernel_launches": ([P], C.c_int64),
         "oa_last_kernel_ms": ([P, C.POINTER(C.c_char_p)], C.c_float),
+        "oa_last_stats_ms": ([P], C.c_float),
         "oa_default_settings": ([C.POINTER(Settings)], None),
         "oa_solve": ([C.POINTER(Settings), C.POINTER(Outputs)], C.c_int),
         "oa_cli_main": ([C.c_int, C.POINTER(C.c_char_p)], C.c_int),
@@ -231,6 +232,9 @@ class Engine:
 
     def launches(self) -> int:
         return int(lib().oa_kernel_launches(self.h))
+
+    def last_stats_ms(self) -> float:
+        return float(lib().oa_last_stats_ms(self.h))
 
     def last_kernel_ms(self):
         name = C.c_char_p()

@@ -153,3 +153,36 @@ def test_cli_matches_reference_outputs(case, tag, tmp_path):
         GU.compare_dbin(os.path.join(GU.GOLDEN, case, f"{tag}_sto.dbin"), out + "_sto.dbin", want,
                         exact_rows=(info["only_ref"] == 0 and info["only_our"] == 0
                                     and sig == run["significant"]))
+
+
+def test_device_path_graph_replay_matches_uncaptured(monkeypatch):
+    """The device-resident scan captured as a CUDA graph gives the uncaptured results, call after call."""
+    import torch
+    ds = synth.generate(synth.scaled(0, n=512, m=700, t=40, l=4, miss_mode="patterns", n_patterns=5, seed=71))
+    l, n = ds.XL.shape
+    m, t = ds.XR.shape[0], ds.Y.shape[0]
+    dev = torch.device("cuda", 0)
+    xr = torch.from_numpy(ds.XR).to(dev)
+    y = torch.from_numpy(ds.Y).to(dev)
+    monkeypatch.setenv("OA_CHUNK_SNPS", "256")       # several chunks in the graph
+    outs = {}
+    for graphs in ("0", "1"):
+        monkeypatch.setenv("OA_GRAPHS", graphs)
+        for prec in (E.PLAIN, E.MIXED):
+            eng = E.Engine(n, l, 1, t, m, precision=prec, min_t_store=E.t_threshold(0.1), min_r2_store=1e-6)
+            eng.set_covariates(ds.XL)
+            eng.set_traits_device(y.data_ptr(), t)
+            eng.enable_dense(True)
+            counts = []
+            for _ in range(3):                        # uncaptured, captured, replayed
+                r = eng.run_device(xr.data_ptr(), m)
+                counts.append((r.count, r.singular))
+                dense = eng.dense(m)
+            assert counts[0] == counts[1] == counts[2]
+            outs[(graphs, prec)] = (counts[0], dense)
+            eng.close()
+    for prec in (E.PLAIN, E.MIXED):
+        (c0, d0), (c1, d1) = outs[("0", prec)], outs[("1", prec)]
+        assert c0 == c1
+        for a, b in zip(d0, d1):
+            np.testing.assert_array_equal(a, b)
