@@ -210,6 +210,94 @@ def run_reference_arm(args):
 # ---------------------------------------------------------------------------
 # our engine
 # ---------------------------------------------------------------------------
+def time_scans(eng, xr_ptr, m, steps, warmup, local, barrier, max_over_ranks):
+    """Warm-up scans, then `steps` timed scans of the device-resident block."""
+    import torch
+    for _ in range(warmup):
+        eng.run_device(xr_ptr, m)
+    clocks = ClockSampler(local)
+    clocks.start()
+    barrier()
+    torch.cuda.synchronize()
+    launches0 = eng.launches()
+    t0 = time.perf_counter()
+    gemm_ms = stats_ms = 0.0
+    rows = 0
+    kname = ""
+    for _ in range(steps):
+        r = eng.run_device(xr_ptr, m)
+        ms, kname = eng.last_kernel_ms()
+        gemm_ms += ms
+        stats_ms += eng.last_stats_ms()
+        rows = r.count
+    torch.cuda.synchronize()
+    elapsed = time.perf_counter() - t0
+    barrier()
+    clk = clocks.stop()
+    elapsed = max_over_ranks(elapsed)
+    return dict(step_s=elapsed / steps, gemm_ms=gemm_ms / steps, stats_ms=stats_ms / steps, kernel=kname,
+                launches=(eng.launches() - launches0) // steps, rows=rows, clocks=clk)
+
+
+def max_dt(eng_a, eng_b, xr_ptr, mb):
+    """max |t_a - t_b| over the tests of the first mb SNPs (both finite)."""
+    import numpy as np
+    out = []
+    for eng in (eng_a, eng_b):
+        eng.enable_dense(True)
+        eng.run_device(xr_ptr, mb)
+        out.append(eng.dense(mb)[2])
+        eng.enable_dense(False)
+    a, b = out
+    ok = np.isfinite(a) & np.isfinite(b)
+    return float(np.max(np.abs(a[ok] - b[ok]))) if ok.any() else None
+
+
+def batched_section(args, dev, local, rank, barrier, max_over_ranks):
+    """Batched uneven systems with interactions: n = 8,000, l = 5, r = 2
+    (SNP x sex and SNP columns), t = 2,000 traits in 150 missingness-pattern
+    groups of Zipf(1.2) sizes, 4,096-SNP blocks; per block one launch of each
+    per-block kernel (the Schur solves of all SNP x pattern systems in one
+    persistent launch), the whole scan one CUDA graph, launch parameters
+    from the engine's autotuner."""
+    import torch
+    from omicabelnomm_b200 import engine as E
+    from omicabelnomm_b200 import synth
+    w = synth.scaled(3, m=args.batched_m)
+    XL, XR, Y, _ = synth.generate_device(w, dev, seed_offset=rank)
+    xl_host = XL.cpu().numpy()
+    n, l, r, m, t = w.n, w.l, w.r, w.m, w.t
+    forms = {}
+    engines = {}
+    for name, prec in (("mixed", E.MIXED), ("plain", E.PLAIN)):
+        eng = E.Engine(n, l, r, t, m, precision=prec, device=local, min_t_store=E.t_threshold(0.1),
+                       min_r2_store=1e-6)
+        eng.set_tuning(chunk_snps=4096)
+        eng.set_covariates(xl_host)
+        eng.set_traits_device(Y.data_ptr(), t)
+        t0 = time.perf_counter()
+        tuned = eng.autotune(XR.data_ptr(), min(m, 32768))
+        tune_s = time.perf_counter() - t0
+        eng.run_device(XR.data_ptr(), m)
+        R = time_scans(eng, XR.data_ptr(), m, args.steps, args.warmup, local, barrier, max_over_ranks)
+        forms[name] = {"tests_per_s": m * t * int(os.environ.get("WORLD_SIZE", "1")) / R["step_s"],
+                       "ms_per_step": R["step_s"] * 1e3, "gemm_ms": R["gemm_ms"], "stats_ms": R["stats_ms"],
+                       "stored_rows": R["rows"], "launches_per_scan": R["launches"], "tuning": tuned,
+                       "autotune_s": tune_s, "clocks": R["clocks"]}
+        engines[name] = eng
+    dt = max_dt(engines["mixed"], engines["plain"], XR.data_ptr(), min(m, 4096))
+    for eng in engines.values():
+        eng.close()
+    del XR, Y, XL
+    torch.cuda.empty_cache()
+    return {"workload": f"batched uneven systems: n={n}, l={l}, r={r} (SNP x sex, SNP), m={m} SNPs, t={t} traits "
+                        f"in {w.n_patterns} missingness-pattern groups (Zipf({w.zipf}) sizes 1-{w.group_max}), "
+                        f"4096-SNP blocks, whole scan one CUDA graph",
+            "forms": forms,
+            "mixed_over_plain": forms["mixed"]["tests_per_s"] / forms["plain"]["tests_per_s"],
+            "max_dt_mixed_vs_plain_first_4096_snps": dt}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -220,6 +308,7 @@ def main():
     ap.add_argument("--m", type=int, default=WORKLOAD["m"], help="SNPs per GPU (default: the full workload)")
     ap.add_argument("--e2e-steps", type=int, default=2)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--batched-m", type=int, default=200000, help="SNPs of the batched workload (0: skip it)")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference_arm(args)
@@ -271,32 +360,8 @@ def main():
         except E.OAError as ex:
             results[name] = {"error": str(ex)}
             continue
-        for _ in range(args.warmup):
-            eng.run_device(XR.data_ptr(), m)
-        clocks = ClockSampler(local)
-        clocks.start()
-        barrier()
-        torch.cuda.synchronize()
-        launches0 = eng.launches()
-        t0 = time.perf_counter()
-        gemm_ms = 0.0
-        stats_ms = 0.0
-        rows = 0
-        for _ in range(args.steps):
-            r = eng.run_device(XR.data_ptr(), m)
-            ms, kname = eng.last_kernel_ms()
-            gemm_ms += ms
-            stats_ms += eng.last_stats_ms()
-            rows = r.count
-        torch.cuda.synchronize()
-        elapsed = time.perf_counter() - t0
-        barrier()
-        clk = clocks.stop()
-        elapsed = max_over_ranks(elapsed)
-        results[name] = dict(engine=eng, step_s=elapsed / args.steps, gemm_ms=gemm_ms / args.steps,
-                             stats_ms=stats_ms / args.steps,
-                             kernel=kname, launches=(eng.launches() - launches0) // args.steps,
-                             rows=rows, clocks=clk)
+        results[name] = dict(engine=eng, **time_scans(eng, XR.data_ptr(), m, args.steps, args.warmup, local,
+                                                      barrier, max_over_ranks))
 
     valid = [k for k in order if "error" not in results[k]]
     if not valid:
@@ -305,16 +370,21 @@ def main():
         return 1
     head = valid[0]
     R = results[head]
+    dt_mp = None
+    if len(valid) == 2:
+        dt_mp = max_dt(results["mixed"]["engine"], results["plain"]["engine"], XR.data_ptr(), min(m, 16384))
+    for k in valid:
+        if k != head:
+            results[k]["engine"].close()
 
     # end to end through the C ABI with pinned host buffers
     xr_host = torch.empty(XR.shape, dtype=torch.float32, pin_memory=True)
     xr_host.copy_(XR)
     y_host = torch.empty(Y.shape, dtype=torch.float32, pin_memory=True)
     y_host.copy_(Y)
-    del XR
+    del XR, Y, XL
     torch.cuda.empty_cache()
     eng = R["engine"]
-    import numpy as np
     xr_np = xr_host.numpy()
     y_np = y_host.numpy()
     e2e_s = None
@@ -329,6 +399,17 @@ def main():
             out = eng.run_raw(xr_np)
             d2h += out.count * 80      # stored rows come back as 80-byte records
         e2e_s = max_over_ranks((time.perf_counter() - t0) / args.e2e_steps)
+    eng.close()
+    h2d = int(xr_np.nbytes + y_np.nbytes)
+    del xr_host, y_host, xr_np, y_np
+    torch.cuda.empty_cache()
+
+    batched = None
+    if args.batched_m > 0:
+        try:
+            batched = batched_section(args, dev, local, rank, barrier, max_over_ranks)
+        except E.OAError as ex:
+            batched = {"error": str(ex)}
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -384,8 +465,7 @@ def main():
         "config": {"workload": workload_desc(m), "form": head, "global_tests": tests * world,
                    "inputs": "genotypes resident in HBM (20 GB per GPU, larger than L2: no flush needed)",
                    "parallelism": f"independent SNP shards x{world}"},
-        "e2e": ({"value": tests * world / e2e_s, "unit": "tests/s",
-                 "h2d_bytes_per_step": int(xr_np.nbytes + y_np.nbytes),
+        "e2e": ({"value": tests * world / e2e_s, "unit": "tests/s", "h2d_bytes_per_step": h2d,
                  "d2h_bytes_per_step": int(d2h / args.e2e_steps)} if e2e_s else None),
         "gpu_launches": int(R["launches"] * args.steps),
         "roofline": {"bound": bound, "achieved": achieved_tflops, "peak": peak, "unit": "TFLOP/s",
@@ -398,6 +478,8 @@ def main():
                        "gemm_ms": v["gemm_ms"], "stats_ms": v["stats_ms"], "stored_rows": v["rows"]}
                       if "error" not in v else v)
                   for k, v in results.items()},
+        "max_dt_mixed_vs_plain_first_16384_snps": dt_mp,
+        "batched": batched,
     }
     print(json.dumps(line))
     if dist is not None:

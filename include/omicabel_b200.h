@@ -159,6 +159,30 @@ oa_status oa_scan_dense_noalloc(const float* xl_dev, const float* y_dev, const f
                                 int32_t l, int32_t r, int32_t t, int32_t mb, float* beta_dev, float* se_dev,
                                 float* t_dev, float* r2_dev, void* stream);
 
+/* Launch parameters of the per-block kernels.  0 in a field = the engine's
+ * own choice.  No counterpart in the reference (its block sizes mb/tb are
+ * fixed at src/Algorithm.cpp:361-372). */
+typedef struct oa_tuning {
+    int32_t chunk_snps;    /* SNPs per device chunk: one launch of each per-block kernel */
+    int32_t gemm_variant;  /* tensor-core pipeline: 1 = K-block 32 x 4 stages, 2 = K-block 64 x 2 stages */
+    int32_t gemm_raster;   /* GEMM tile order: 1 = trait tiles inner, 2 = SNP tiles inner */
+    int32_t stats_path;    /* per-SNP sums: 1 = pre-GEMM + batched Schur kernel, 2 = row gathers */
+    int32_t lean_spb;      /* SNPs per CTA group of the column-statistics kernel (1..8/r) */
+} oa_tuning;
+
+/* Set / read the tuning (oa_get_tuning reports the values in effect for
+ * the current trait block, zeros resolved). */
+oa_status oa_set_tuning(oa_engine* e, const oa_tuning* t);
+oa_status oa_get_tuning(const oa_engine* e, oa_tuning* t);
+
+/* Autotuner: times candidate tunings on the device SNP block xr_dev (mb
+ * SNPs, a sample of the real data; after oa_set_traits*) by coordinate
+ * descent over the fields of oa_tuning (device time of the per-block
+ * kernels, CUDA events), keeps the fastest in the engine and returns it in
+ * *best (may be NULL).  A chunk size set with oa_set_tuning before the call
+ * is kept fixed.  Results of the trial runs are discarded. */
+oa_status oa_autotune(oa_engine* e, const float* xr_dev, int32_t mb, oa_tuning* best);
+
 /* Number of kernel launches this engine issued so far (instrumentation). */
 int64_t oa_kernel_launches(const oa_engine* e);
 /* Device time (ms) of the dominant kernel in the last SNP block and its name. */

@@ -5,7 +5,9 @@
 //   k_trait_stats -> host groups traits by missingness pattern (and by the
 //   set of observed exact zeros) -> k_set_rows -> k_set_gram -> k_trait_resid
 // Per SNP chunk (≙ src/Algorithm.cpp:610-813):
-//   k_snp_stats -> XR'Y~ GEMM with fused statistics epilogue -> (covariate terms)
+//   k_snp_lean -> pre-GEMM [Q | Q o m_1 | ...]'X -> k_schur   (few row sets)
+//   or k_snp_stats (one kernel with row gathers; many row sets)
+//   -> XR'Y~ GEMM with fused statistics epilogue -> (covariate terms)
 // Per API call: sort of the stored rows into reference order (trait, SNP).
 #include <algorithm>
 #include <cmath>
@@ -23,6 +25,7 @@
 #include "oa_cov.cuh"
 #include "oa_kernels.cuh"
 #include "oa_launch.h"
+#include "oa_lean.cuh"
 
 using namespace oa;
 
@@ -215,12 +218,22 @@ struct oa_engine {
     DBuf<float> sst, qrows;
     DBuf<uint8_t> pat_bad;
     int G = 0, Z = 0, nsets = 0;
+    // pre-GEMM column matrix [Q | Q o m_1 | ... | Q o m_S] (c2 = l (1 + S) rows of n_pad)
+    bool use_pre = false, b2_ready = false;
+    int c2 = 0;
+    // tuning: requested (0 = automatic) and in effect
+    oa_tuning req{};
+    int variant = 1, raster = 1, lean_spb = 0;
+    long long tune_gen = 0;
+    DBuf<float> B2;
+    DBuf<__nv_bfloat16> B2hi, B2lo;
     std::vector<int> h_nobs;
     // SNP chunk buffers
     int chunk = 0;
     DBuf<float> Xstage[2];
     DBuf<__nv_bfloat16> Xhi, Xlo;
     DBuf<float> mean, varx, aobs, afull, zA, zD;
+    DBuf<float> D, Dset, C2T;   // pre-GEMM path: X'X, per-set X'X, pre-GEMM output
     DBuf<int> has_nan;
     DBuf<double> sinv, sfinv;
     DBuf<uint8_t> sing;
@@ -238,14 +251,16 @@ struct oa_engine {
         int mb = 0, t = 0, dense = 0;
         long long gen = 0, cap = 0;
         const void* rec = nullptr;
+        long long tune = 0;
         bool operator==(const GraphKey& o) const {
             return xr == o.xr && mb == o.mb && t == o.t && dense == o.dense && gen == o.gen && cap == o.cap &&
-                   rec == o.rec;
+                   rec == o.rec && tune == o.tune;
         }
     };
     GraphKey gkey, warm_key;
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t gexec = nullptr;
+    long long graph_launches = 0;
     long long trait_gen = 0;
     std::vector<cudaEvent_t> cev0, cev1, sev0, sev1;
     bool use_graphs = true;
@@ -383,6 +398,8 @@ oa_status set_traits_impl(oa_engine* e, const float* y, int32_t t, bool device_p
     }
     e->launches += 2;
     OA_CU(cudaGetLastError());
+    e->c2 = l * (1 + e->nsets);
+    e->b2_ready = false;
     OA_CHECK(e->Yt.ensure((size_t)t * e->n_pad));
     if (e->cfg.precision == OA_MIXED_BF16X3) {
         OA_CHECK(e->Yhi.ensure((size_t)t * e->n_pad));
@@ -403,6 +420,41 @@ oa_status set_traits_impl(oa_engine* e, const float* y, int32_t t, bool device_p
     ++e->launches;
     OA_CU(cudaGetLastError());
     OA_CU(cudaStreamSynchronize(e->st));
+    return OA_OK;
+}
+
+// Resolves the tuning for the current trait block.  Per-SNP covariate sums:
+// with few row sets one pre-GEMM of the SNP block with
+// [Q | Q o m_1 | ... | Q o m_S] (cost c2 / t of the main GEMM); with many,
+// row gathers inside k_snp_stats.  Builds the pre-GEMM's column matrix
+// the first time a trait block needs it.
+oa_status prepare_tuning(oa_engine* e) {
+    const int t = e->t, l = e->l, n = e->n;
+    e->chunk = std::min(e->cfg.max_snps, e->req.chunk_snps > 0 ? e->req.chunk_snps : 16384 / e->r);
+    e->variant = e->req.gemm_variant == 2 ? 2 : 1;
+    e->raster = e->req.gemm_raster == 2 ? 2 : 1;
+    e->lean_spb = e->req.lean_spb > 0 ? std::min(e->req.lean_spb, 8 / e->r) : 0;
+    e->use_pre = e->req.stats_path == 1 || (e->req.stats_path != 2 && e->c2 <= std::max(t, 256));
+    if (e->use_pre && !e->b2_ready) {
+        const size_t nb2 = (size_t)e->c2 * e->n_pad;
+        OA_CHECK(e->B2.ensure(nb2));
+        k_b2_init<<<(unsigned)((nb2 + 255) / 256), 256, 0, e->st>>>(e->Qr.p, e->LP, n, e->n_pad, l, e->c2, e->B2.p);
+        ++e->launches;
+        if (e->nsets > 0) {
+            k_b2_scatter<<<e->nsets, 256, 0, e->st>>>(e->Qr.p, e->LP, e->n_pad, l, e->set_off.p, e->set_rows.p,
+                                                      e->B2.p);
+            ++e->launches;
+        }
+        if (e->cfg.precision == OA_MIXED_BF16X3) {
+            OA_CHECK(e->B2hi.ensure(nb2));
+            OA_CHECK(e->B2lo.ensure(nb2));
+            k_split_bf16<<<(unsigned)((nb2 + 255) / 256), 256, 0, e->st>>>(e->B2.p, (long long)nb2, e->B2hi.p,
+                                                                          e->B2lo.p);
+            ++e->launches;
+        }
+        OA_CU(cudaGetLastError());
+        e->b2_ready = true;
+    }
     return OA_OK;
 }
 
@@ -444,7 +496,7 @@ StatsArgs stats_args(oa_engine* e, const float* X, int mbc, int LP, int spb, int
 }
 
 template <int R>
-oa_status stats_dispatch(oa_engine* e, const float* X, int mbc) {
+oa_status stats_gather(oa_engine* e, const float* X, int mbc) {
     // SNPs per group: as many as fit the register budget; two column buffers
     // (double-buffered TMA staging) when they fit in ~170 KB, else one
     const int nS = (e->n + 3) & ~3;
@@ -476,6 +528,101 @@ oa_status stats_dispatch(oa_engine* e, const float* X, int mbc) {
     if (e->LP == 4) return pick(std::integral_constant<int, 4>{});
     if (e->LP == 8) return pick(std::integral_constant<int, 8>{});
     return pick(std::integral_constant<int, 16>{});
+}
+
+// Lean path: k_snp_lean (imputation, BF16 split, X'X over all rows and over
+// each row set) -> pre-GEMM C2 = [Q | Q o m_1 | ...]'X -> k_schur.
+// SNPs per CTA group of k_snp_lean: requested, else two CTAs per SM where a
+// double-buffered group fits in half the shared memory (a power of two <= 8 / r)
+int lean_group(const oa_engine* e) {
+    if (e->lean_spb > 0) {
+        int s = 1;
+        while (s * 2 <= e->lean_spb) s *= 2;
+        return std::min(s, 8 / e->r);
+    }
+    const size_t colb = (size_t)e->r * e->n_pad * 4;
+    int s = 1;
+    while (s * 2 <= 8 / e->r && 2 * (size_t)(s * 2) * colb <= 100 * 1024) s *= 2;
+    return s;
+}
+
+template <int R>
+oa_status stats_pre(oa_engine* e, const float* X, int mbc) {
+    const size_t limit = 227 * 1024 - 1024;
+    const size_t colb = (size_t)R * e->n_pad * 4;
+    int spb = lean_group(e);
+    int nbuf = 2;
+    while (spb > 1 && nbuf * spb * colb > 200 * 1024) spb /= 2;
+    if (nbuf * spb * colb > 200 * 1024) nbuf = 1;
+    const size_t base = lean_smem_bytes(R, e->n_pad, spb, nbuf, 0);
+    const size_t per_set = (size_t)spb * R * R * 4;
+    if (base + per_set > limit) {
+        set_err("n = %d is too large for one SNP column in shared memory", e->n);
+        return OA_ERR_UNSUPPORTED;
+    }
+    const int sets_cap = (int)std::max<size_t>(1, std::min<size_t>(std::max(e->nsets, 1), (limit - base) / per_set));
+    const size_t smem = lean_smem_bytes(R, e->n_pad, spb, nbuf, sets_cap);
+    LeanArgs A{};
+    A.X = X;
+    A.ldx = (size_t)e->n;
+    A.n = e->n;
+    A.n_pad = e->n_pad;
+    A.mb = mbc;
+    A.nbuf = nbuf;
+    A.nsets = e->nsets;
+    A.sets_cap = sets_cap;
+    A.set_off = e->set_off.p;
+    A.rows = e->set_rows.p;
+    A.mean = e->mean.p;
+    A.has_nan = e->has_nan.p;
+    A.D = e->D.p;
+    A.Dset = e->Dset.p;
+    const bool mixed = e->cfg.precision == OA_MIXED_BF16X3;
+    A.write_split = mixed ? 1 : 0;
+    A.Xhi = e->Xhi.p;
+    A.Xlo = e->Xlo.p;
+    A.err = reinterpret_cast<int*>(e->counters.p + 3);
+    const int groups = (mbc + spb - 1) / spb;
+    const int per_sm = (int)std::max<size_t>(1, std::min<size_t>(4, (228 * 1024) / (smem + 1024)));
+    const int grid = std::min(groups, e->sm_count * per_sm);
+    OA_CU(oa_launch_snp_lean(R, spb, A, grid, smem, e->st));
+    ++e->launches;
+    const int ldc = e->chunk * R;
+    if (mixed)
+        OA_CU(oa_launch_pre_tc(e->Xhi.p, e->Xlo.p, mbc * R, e->B2hi.p, e->B2lo.p, e->c2, e->n_pad, e->C2T.p, ldc,
+                               reinterpret_cast<int*>(e->counters.p + 3), e->st));
+    else
+        OA_CU(oa_launch_pre_simt(X, (size_t)e->n, mbc * R, e->B2.p, (size_t)e->n_pad, e->c2, e->n, e->mean.p,
+                                 e->has_nan.p, e->C2T.p, ldc, e->st));
+    ++e->launches;
+    SchurArgs S{};
+    S.l = e->l;
+    S.mb = mbc;
+    S.G = e->G;
+    S.Z = e->Z;
+    S.ldc = ldc;
+    S.C2 = e->C2T.p;
+    S.D = e->D.p;
+    S.Dset = e->Dset.p;
+    S.W = e->W.p;
+    S.pat_bad = e->pat_bad.p;
+    S.sinv = e->sinv.p;
+    S.sing = e->sing.p;
+    S.varx = e->varx.p;
+    const bool need_aobs = e->cfg.disp_cov || e->Z > 0;
+    S.aobs = need_aobs ? e->aobs.p : nullptr;
+    S.afull = e->cfg.disp_cov ? e->afull.p : nullptr;
+    S.sfinv = e->cfg.disp_cov ? e->sfinv.p : nullptr;
+    S.zA = e->zA.p;
+    S.zD = e->zD.p;
+    OA_CU(oa_launch_schur(R, S, e->st));
+    ++e->launches;
+    return OA_OK;
+}
+
+template <int R>
+oa_status stats_dispatch(oa_engine* e, const float* X, int mbc) {
+    return e->use_pre ? stats_pre<R>(e, X, mbc) : stats_gather<R>(e, X, mbc);
 }
 
 EpiArgs epi_args(oa_engine* e, int mbc, int snp_base) {
@@ -552,8 +699,8 @@ oa_status gemm_dispatch(oa_engine* e, const float* X, int mbc, int snp_base) {
                                   e->has_nan.p, E, e->st));
         e->last_name = "k_gemm_simt";
     } else {
-        OA_CU(oa_launch_gemm_tc(R, e->Xhi.p, e->Xlo.p, mbc * R, e->Yhi.p, e->Ylo.p, e->t, e->n_pad, E,
-                                reinterpret_cast<int*>(e->counters.p + 3), e->st));
+        OA_CU(oa_launch_gemm_tc(R, e->variant, e->raster, e->Xhi.p, e->Xlo.p, mbc * R, e->Yhi.p, e->Ylo.p, e->t,
+                                e->n_pad, E, reinterpret_cast<int*>(e->counters.p + 3), e->st));
         e->last_name = "k_gemm_tc";
     }
     ++e->launches;
@@ -579,6 +726,11 @@ oa_status ensure_chunk_buffers(oa_engine* e) {
     if (e->cfg.precision == OA_MIXED_BF16X3) {
         OA_CHECK(e->Xhi.ensure(mb * r * e->n_pad));
         OA_CHECK(e->Xlo.ensure(mb * r * e->n_pad));
+    }
+    if (e->use_pre) {
+        OA_CHECK(e->D.ensure(mb * r * r));
+        OA_CHECK(e->Dset.ensure((size_t)std::max(e->nsets, 1) * mb * r * r));
+        OA_CHECK(e->C2T.ensure((size_t)e->c2 * mb * r));
     }
     return OA_OK;
 }
@@ -674,12 +826,12 @@ oa_status enqueue_scan(oa_engine* e, const float* xr, int mb) {
         const int c0 = c * e->chunk, mbc = std::min(e->chunk, mb - c0);
         const float* X = xr + (size_t)c0 * e->r * e->n;
         OA_CU(cudaMemsetAsync(e->has_nan.p, 0, sizeof(int), e->st));
-        OA_CU(cudaEventRecord(e->sev0[c], e->st));
+        OA_CU(cudaEventRecordWithFlags(e->sev0[c], e->st, cudaEventRecordExternal));
         OA_CHECK(stats_dispatch<R>(e, X, mbc));
-        OA_CU(cudaEventRecord(e->sev1[c], e->st));
-        OA_CU(cudaEventRecord(e->cev0[c], e->st));
+        OA_CU(cudaEventRecordWithFlags(e->sev1[c], e->st, cudaEventRecordExternal));
+        OA_CU(cudaEventRecordWithFlags(e->cev0[c], e->st, cudaEventRecordExternal));
         OA_CHECK(gemm_dispatch<R>(e, X, mbc, c0));
-        OA_CU(cudaEventRecord(e->cev1[c], e->st));
+        OA_CU(cudaEventRecordWithFlags(e->cev1[c], e->st, cudaEventRecordExternal));
     }
     return OA_OK;
 }
@@ -706,14 +858,18 @@ oa_status run_graph(oa_engine* e, const float* xr, int mb, bool* done) {
     key.gen = e->trait_gen;
     key.cap = e->cap;
     key.rec = e->rec.p;
+    key.tune = e->tune_gen;
     if (!(e->gexec && e->gkey == key)) {
         drop_graph(e);
         if (!(e->warm_key == key)) {
             e->warm_key = key;       // first sight: uncaptured run (sets kernel attributes)
             return OA_OK;
         }
+        const long long l0 = e->launches;
         OA_CU(cudaStreamBeginCapture(e->st, cudaStreamCaptureModeThreadLocal));
         const oa_status s = enqueue_scan<R>(e, xr, mb);
+        e->graph_launches = e->launches - l0;   // kernels in the graph (they run at each launch)
+        e->launches = l0;
         cudaGraph_t g = nullptr;
         const cudaError_t ce = cudaStreamEndCapture(e->st, &g);
         if (s != OA_OK) {
@@ -727,7 +883,7 @@ oa_status run_graph(oa_engine* e, const float* xr, int mb, bool* done) {
     }
     OA_CU(cudaGraphLaunch(e->gexec, e->st));
     const int nch = (mb + e->chunk - 1) / e->chunk;
-    e->launches += 3 * nch;
+    e->launches += e->graph_launches;
     unsigned long long cnt[4];
     OA_CU(cudaMemcpyAsync(cnt, e->counters.p, sizeof cnt, cudaMemcpyDeviceToHost, e->st));
     OA_CU(cudaStreamSynchronize(e->st));
@@ -768,6 +924,7 @@ oa_status run_snps_impl(oa_engine* e, const float* xr, int32_t mb, bool host_inp
         set_err("SNP block of %d SNPs (engine limit %d)", mb, e->cfg.max_snps);
         return OA_ERR_ARG;
     }
+    OA_CHECK(prepare_tuning(e));
     OA_CHECK(ensure_chunk_buffers(e));
     const long long tests = (long long)mb * e->t;
     if (e->cap == 0) OA_CHECK(ensure_cap(e, std::max<long long>(1 << 16, e->cfg.store_all ? tests : tests / 6)));
@@ -934,6 +1091,88 @@ oa_status run_snps_any(oa_engine* e, const float* xr, int32_t mb, bool host_inpu
     }
 }
 
+// Autotuner: coordinate descent over the tuning fields, each candidate
+// timed by the device time of its per-block kernels (statistics stage +
+// main GEMM, CUDA events per chunk) on the caller's sample block.
+oa_status autotune_impl(oa_engine* e, const float* xr, int mb, oa_tuning* best_out) {
+    if (e->t <= 0) {
+        set_err("oa_autotune before oa_set_traits");
+        return OA_ERR_STATE;
+    }
+    const int r = e->r;
+    const bool mixed = e->cfg.precision == OA_MIXED_BF16X3;
+    const bool graphs = e->use_graphs;
+    e->use_graphs = false;
+    oa_rows rows;
+    auto cost = [&](const oa_tuning& c, float* ms) -> oa_status {
+        e->req = c;
+        ++e->tune_gen;
+        float sum = 0.f;
+        for (int rep = 0; rep < 3; ++rep) {   // first run: allocations and kernel attributes
+            const oa_status s = run_snps_any(e, xr, mb, false, false, &rows);
+            if (s != OA_OK) return s;
+            if (rep > 0) sum += e->last_ms + e->stats_ms;
+        }
+        *ms = sum / 2.f;
+        return OA_OK;
+    };
+    // a chunk size set before the call is kept (the caller's block size)
+    const bool fixed_chunk = e->req.chunk_snps > 0;
+    oa_tuning best{};
+    best.chunk_snps = fixed_chunk ? std::min(mb, e->req.chunk_snps) : std::min(mb, 16384 / r);
+    best.gemm_variant = 1;
+    best.gemm_raster = 1;
+    OA_CHECK(prepare_tuning(e));
+    best.stats_path = e->use_pre ? 1 : 2;
+    best.lean_spb = 0;
+    float best_ms = 0.f;
+    oa_status s0 = cost(best, &best_ms);
+    if (s0 != OA_OK) {
+        e->use_graphs = graphs;
+        return s0;
+    }
+    auto try_field = [&](int32_t oa_tuning::*f, std::vector<int> vals) {
+        for (int v : vals) {
+            if (v == best.*f) continue;
+            oa_tuning c = best;
+            c.*f = v;
+            float ms = 0.f;
+            if (cost(c, &ms) != OA_OK) {   // an infeasible candidate (e.g. shared memory) is skipped
+                g_err.clear();
+                cudaGetLastError();
+                continue;
+            }
+            if (ms < best_ms * 0.98f) {
+                best_ms = ms;
+                best = c;
+            }
+        }
+    };
+    try_field(&oa_tuning::stats_path, {1, 2});
+    if (best.stats_path == 1) {
+        best.lean_spb = lean_group(e);
+        std::vector<int> spbs;
+        for (int v = 1; v <= 8 / r; v *= 2) spbs.push_back(v);
+        try_field(&oa_tuning::lean_spb, spbs);
+    }
+    if (mixed) {
+        try_field(&oa_tuning::gemm_variant, {1, 2});
+        try_field(&oa_tuning::gemm_raster, {1, 2});
+    }
+    if (!fixed_chunk) {
+        std::vector<int> chunks;
+        for (int c = 2048; c <= 32768; c *= 2)
+            if (c / r <= mb) chunks.push_back(c / r);
+        try_field(&oa_tuning::chunk_snps, chunks);
+    }
+    e->req = best;
+    ++e->tune_gen;
+    e->use_graphs = graphs;
+    OA_CHECK(prepare_tuning(e));
+    if (best_out) *best_out = best;
+    return OA_OK;
+}
+
 }  // namespace
 
 // ---------------------------------------------------------------------------
@@ -995,8 +1234,12 @@ oa_status oa_engine_create(const oa_config* cfg, oa_engine** out) {
     e->p = cfg->l + cfg->r;
     e->LP = pad_l(cfg->l);
     e->n_pad = (cfg->n + 63) & ~63;
-    const char* ch = getenv("OA_CHUNK_SNPS");
-    e->chunk = std::min(cfg->max_snps, ch ? std::max(1, atoi(ch)) : 16384 / cfg->r);
+    // environment defaults of the tuning (oa_set_tuning overrides them)
+    if (const char* v = getenv("OA_CHUNK_SNPS")) e->req.chunk_snps = std::max(1, atoi(v));
+    if (const char* v = getenv("OA_STATS_PATH")) e->req.stats_path = std::string(v) == "pre" ? 1 : (std::string(v) == "gather" ? 2 : 0);
+    if (const char* v = getenv("OA_TC_VARIANT")) e->req.gemm_variant = atoi(v) == 1 ? 2 : 1;
+    if (const char* v = getenv("OA_LEAN_SPB")) e->req.lean_spb = std::max(0, atoi(v));
+    e->chunk = std::min(cfg->max_snps, e->req.chunk_snps > 0 ? e->req.chunk_snps : 16384 / cfg->r);
     const char* gr = getenv("OA_GRAPHS");
     e->use_graphs = !(gr && gr[0] == '0');
     if (cudaStreamCreateWithFlags(&e->st, cudaStreamNonBlocking) != cudaSuccess ||
@@ -1035,7 +1278,9 @@ oa_status oa_engine_destroy(oa_engine* e) {
     for (auto* b : {&e->tcounts, &e->pat, &e->zset, &e->nobs, &e->set_off, &e->set_rows, &e->set_rep, &e->set_kind,
                     &e->set_slot, &e->has_nan, &e->perm, &e->perm2, &e->tperm, &e->tinv})
         b->release();
-    for (auto* b : {&e->a_r2, &e->inv_ncorr, &e->vf, &e->qrows}) b->release();
+    for (auto* b : {&e->a_r2, &e->inv_ncorr, &e->vf, &e->qrows, &e->B2, &e->D, &e->Dset, &e->C2T}) b->release();
+    e->B2hi.release();
+    e->B2lo.release();
     e->Yhi.release();
     e->Ylo.release();
     e->Xhi.release();
@@ -1142,6 +1387,45 @@ oa_status oa_run_snps(oa_engine* e, const float* xr, int32_t mb, oa_rows* out) {
 
 oa_status oa_run_snps_device(oa_engine* e, const float* xr, int32_t mb, int32_t results_on_host, oa_rows* out) {
     return run_snps_any(e, xr, mb, false, results_on_host != 0, out);
+}
+
+oa_status oa_set_tuning(oa_engine* e, const oa_tuning* t) {
+    clear_stale_error(__func__);
+    if (!e || !t) {
+        set_err("null argument");
+        return OA_ERR_ARG;
+    }
+    if (t->chunk_snps < 0 || t->gemm_variant < 0 || t->gemm_variant > 2 || t->gemm_raster < 0 ||
+        t->gemm_raster > 2 || t->stats_path < 0 || t->stats_path > 2 || t->lean_spb < 0 || t->lean_spb > 8) {
+        set_err("tuning field out of range");
+        return OA_ERR_ARG;
+    }
+    e->req = *t;
+    ++e->tune_gen;
+    return OA_OK;
+}
+
+oa_status oa_get_tuning(const oa_engine* e, oa_tuning* t) {
+    if (!e || !t) {
+        set_err("null argument");
+        return OA_ERR_ARG;
+    }
+    t->chunk_snps = e->chunk;
+    t->gemm_variant = e->variant;
+    t->gemm_raster = e->raster;
+    t->stats_path = e->t > 0 ? (e->use_pre ? 1 : 2) : e->req.stats_path;
+    t->lean_spb = lean_group(e);
+    return OA_OK;
+}
+
+oa_status oa_autotune(oa_engine* e, const float* xr_dev, int32_t mb, oa_tuning* best) {
+    clear_stale_error(__func__);
+    if (!e || !xr_dev || mb <= 0 || mb > e->cfg.max_snps) {
+        set_err("invalid autotune arguments");
+        return OA_ERR_ARG;
+    }
+    OA_CU(cudaSetDevice(e->cfg.device));
+    return autotune_impl(e, xr_dev, mb, best);
 }
 
 oa_status oa_enable_dense(oa_engine* e, int32_t on) {

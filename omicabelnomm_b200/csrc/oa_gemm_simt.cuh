@@ -37,10 +37,14 @@ __device__ __forceinline__ void sg_load(const float* __restrict__ P, size_t ld, 
     }
 }
 
-template <int R, bool VEC>
+// STORE = false: fused statistics epilogue.  STORE = true: the product is
+// written out transposed, C[col * ldc + row] (the pre-GEMM of the per-SNP
+// covariate sums).
+template <int R, bool VEC, bool STORE>
 __global__ void __launch_bounds__(256, 2)
 k_gemm_simt(const float* __restrict__ X, size_t ldx, int xrows, const float* __restrict__ Yt, size_t ldy,
-            int t, int K, const float* __restrict__ colmean, const int* __restrict__ has_nan, EpiArgs E) {
+            int t, int K, const float* __restrict__ colmean, const int* __restrict__ has_nan, EpiArgs E,
+            float* __restrict__ cout, int ldc) {
     __shared__ __align__(16) float As[2][SG_BK][SG_BM + SG_PAD];
     __shared__ __align__(16) float Bs[2][SG_BK][SG_BN + SG_PAD];
     const int tid = threadIdx.x;
@@ -98,23 +102,35 @@ k_gemm_simt(const float* __restrict__ X, size_t ldx, int xrows, const float* __r
         __syncthreads();
     }
 
-    // fused epilogue: rows ty*4+{0..3} and 64+ty*4+{0..3}; a SNP's R columns
-    // are consecutive rows held by this thread (R divides 4)
+    if constexpr (STORE) {
 #pragma unroll
-    for (int half = 0; half < 2; ++half) {
-#pragma unroll
-        for (int sg = 0; sg < 4 / R; ++sg) {
-            const int row0 = m0 + 64 * half + ty * 4 + sg * R;
-            const int i = row0 / R;  // SNP within the block
+        for (int ii = 0; ii < 8; ++ii) {
+            const int row = m0 + (ii < 4 ? ty * 4 + ii : 64 + ty * 4 + (ii - 4));
 #pragma unroll
             for (int jj = 0; jj < 8; ++jj) {
-                const int j = n0 + (jj < 4 ? tx * 4 + jj : 64 + tx * 4 + (jj - 4));
-                float z[R];
+                const int col = n0 + (jj < 4 ? tx * 4 + jj : 64 + tx * 4 + (jj - 4));
+                if (row < xrows && col < t) cout[(size_t)col * ldc + row] = acc[ii][jj];
+            }
+        }
+    } else {
+        // fused epilogue: rows ty*4+{0..3} and 64+ty*4+{0..3}; a SNP's R columns
+        // are consecutive rows held by this thread (R divides 4)
 #pragma unroll
-                for (int a = 0; a < R; ++a) z[a] = acc[half * 4 + sg * R + a][jj];
-                Rec rc;
-                const bool st = epi_eval<R>(E, i, j, z, (row0 < xrows) && (j < t), rc);
-                epi_emit(E, st, rc);
+        for (int half = 0; half < 2; ++half) {
+#pragma unroll
+            for (int sg = 0; sg < 4 / R; ++sg) {
+                const int row0 = m0 + 64 * half + ty * 4 + sg * R;
+                const int i = row0 / R;  // SNP within the block
+#pragma unroll
+                for (int jj = 0; jj < 8; ++jj) {
+                    const int j = n0 + (jj < 4 ? tx * 4 + jj : 64 + tx * 4 + (jj - 4));
+                    float z[R];
+#pragma unroll
+                    for (int a = 0; a < R; ++a) z[a] = acc[half * 4 + sg * R + a][jj];
+                    Rec rc;
+                    const bool st = epi_eval<R>(E, i, j, z, (row0 < xrows) && (j < t), rc);
+                    epi_emit(E, st, rc);
+                }
             }
         }
     }

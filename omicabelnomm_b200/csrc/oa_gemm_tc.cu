@@ -22,26 +22,23 @@
 // its TMEM and returns.  The host turns the flag into an error.
 #include <cuda.h>
 
-#include <cstdlib>
-
 #include "oa_epilogue.cuh"
 #include "oa_launch.h"
 
 namespace oa {
 namespace tc {
 
-constexpr int BM = 128, BN = 256;
+constexpr int BM = 128;
 constexpr int EPI_WARPS = 4;
 constexpr int NUM_THREADS = 64 + 32 * EPI_WARPS;         // 192
-constexpr uint32_t TMEM_COLS = 512;
 constexpr int STG_STRIDE = 33;                           // epilogue staging row (conflict-free)
 constexpr unsigned long long WAIT_NS = 2000000000ull;
 
 // Pipeline shape: K-block width BK (64 -> 128-byte swizzle, 32 -> 64-byte
-// swizzle) and the number of shared-memory stages.
-template <int BK_, int STAGES_>
+// swizzle), the number of shared-memory stages and the tile width BN.
+template <int BK_, int STAGES_, int BN_ = 256>
 struct Shape {
-    static constexpr int BK = BK_, STAGES = STAGES_;
+    static constexpr int BK = BK_, STAGES = STAGES_, BN = BN_;
     static constexpr int A_BYTES = BM * BK * 2;                     // one of hi / lo
     static constexpr int B_BYTES = BN * BK * 2;
     static constexpr int STAGE_BYTES = 2 * A_BYTES + 2 * B_BYTES;
@@ -49,13 +46,15 @@ struct Shape {
                                          (size_t)EPI_WARPS * 32 * STG_STRIDE * 4 + (size_t)BN * sizeof(TraitP);
     static constexpr uint64_t LAYOUT = BK == 64 ? 2u : 4u;          // SWIZZLE_128B : SWIZZLE_64B
     static constexpr uint32_t SBO = BK == 64 ? 1024u : 512u;        // bytes between 8-row groups
+    // two accumulators of BN FP32 columns (allocation: a power of two >= 32)
+    static constexpr uint32_t TMEM_COLS = 2 * BN <= 128 ? 128u : (2 * BN <= 256 ? 256u : 512u);
+    // instruction descriptor, kind::f16: D FP32 (bits 4-5 = 1), A and B BF16
+    // (bits 7-9 = 1, 10-12 = 1), both K-major (bits 15, 16 = 0), N >> 3 at
+    // bits 17-22, M >> 4 at bits 24-28
+    static constexpr uint32_t IDESC = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(BN >> 3) << 17) |
+                                      ((uint32_t)(BM >> 4) << 24);
+    static_assert(BN % 16 == 0 && BN >= 32 && BN <= 256, "UMMA N for M = 128");
 };
-
-// instruction descriptor, kind::f16: D FP32 (bits 4-5 = 1), A and B BF16
-// (bits 7-9 = 1, 10-12 = 1), both K-major (bits 15, 16 = 0), N >> 3 at
-// bits 17-22, M >> 4 at bits 24-28
-constexpr uint32_t IDESC = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(BN >> 3) << 17) |
-                           ((uint32_t)(BM >> 4) << 24);
 
 __device__ __forceinline__ uint32_t su32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
 
@@ -125,11 +124,12 @@ __device__ __forceinline__ uint64_t smem_desc(uint32_t saddr) {
     return d;
 }
 
-__device__ __forceinline__ void mma_bf16(uint32_t d_tmem, uint64_t a, uint64_t b, uint32_t accumulate) {
+__device__ __forceinline__ void mma_bf16(uint32_t d_tmem, uint64_t a, uint64_t b, uint32_t idesc,
+                                         uint32_t accumulate) {
     asm volatile(
         "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
         "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n}\n" ::"r"(d_tmem),
-        "l"(a), "l"(b), "r"(IDESC), "r"(accumulate), "r"(0u), "r"(0u), "r"(0u), "r"(0u));
+        "l"(a), "l"(b), "r"(idesc), "r"(accumulate), "r"(0u), "r"(0u), "r"(0u), "r"(0u));
 }
 __device__ __forceinline__ void mma_commit(uint64_t* bar) {
     asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(su32(bar))
@@ -150,12 +150,16 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&v)[32]) {
     asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 }
 
-template <int R, class SH>
+// STORE = false: fused statistics epilogue (t = traits).  STORE = true: the
+// FP32 product is written out transposed, C[col * ldc + row] (t = columns),
+// for the pre-GEMM of the per-SNP covariate sums.
+template <int R, class SH, bool STORE>
 __global__ void __launch_bounds__(NUM_THREADS, 1)
 k_gemm_tc(const __grid_constant__ CUtensorMap mAhi, const __grid_constant__ CUtensorMap mAlo,
           const __grid_constant__ CUtensorMap mBhi, const __grid_constant__ CUtensorMap mBlo, int xrows, int t,
-          int nk, EpiArgs E, int* err) {
-    constexpr int BK = SH::BK, STAGES = SH::STAGES;
+          int nk, EpiArgs E, float* __restrict__ cout, int ldc, int raster, int* err) {
+    constexpr int BK = SH::BK, STAGES = SH::STAGES, BN = SH::BN;
+    constexpr uint32_t TMEM_COLS = SH::TMEM_COLS;
     constexpr int A_BYTES = SH::A_BYTES, B_BYTES = SH::B_BYTES, STAGE_BYTES = SH::STAGE_BYTES;
     extern __shared__ uint8_t smem_raw[];
     uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~(uintptr_t)1023);
@@ -208,7 +212,8 @@ k_gemm_tc(const __grid_constant__ CUtensorMap mAhi, const __grid_constant__ CUte
             for (int q = 0; q < STAGES; ++q) pend[q] = false;
             bool ok = true;
             for (int tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x) {
-                const int m0 = (tile / n_tiles) * BM, n0 = (tile % n_tiles) * BN;
+                const int m0 = (raster == 2 ? tile % m_tiles : tile / n_tiles) * BM;
+                const int n0 = (raster == 2 ? tile / m_tiles : tile % n_tiles) * BN;
                 for (int kb = 0; kb < nk; ++kb) {
                     if (!mbar_wait(&empty_bar[s], ph ^ 1u, &abort_sh)) {
                         ok = false;
@@ -254,9 +259,9 @@ k_gemm_tc(const __grid_constant__ CUtensorMap mAhi, const __grid_constant__ CUte
                         const uint32_t off = (uint32_t)kk * 32u;   // 16 BF16 along K inside the swizzled row
                         const uint64_t dah = smem_desc<SH>(ahi + off), dal = smem_desc<SH>(alo + off);
                         const uint64_t dbh = smem_desc<SH>(bhi + off), dbl = smem_desc<SH>(blo + off);
-                        mma_bf16(d_tmem, dah, dbh, (kb > 0 || kk > 0) ? 1u : 0u);
-                        mma_bf16(d_tmem, dah, dbl, 1u);
-                        mma_bf16(d_tmem, dal, dbh, 1u);
+                        mma_bf16(d_tmem, dah, dbh, SH::IDESC, (kb > 0 || kk > 0) ? 1u : 0u);
+                        mma_bf16(d_tmem, dah, dbl, SH::IDESC, 1u);
+                        mma_bf16(d_tmem, dal, dbh, SH::IDESC, 1u);
                     }
                     issued = true;
                     mma_commit(&empty_bar[s]);
@@ -277,6 +282,40 @@ k_gemm_tc(const __grid_constant__ CUtensorMap mAhi, const __grid_constant__ CUte
                 mbar_drain(&done_bar, 0);
             }
         }
+    } else if constexpr (STORE) {
+        // ---------------- store epilogue ----------------
+        // lane = row of the tile: each tcgen05.ld column goes out as one
+        // coalesced 128-byte row segment of the transposed output
+        const int lg = warp & 3;
+        int acc = 0;
+        uint32_t aph = 0;
+        for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+            if (abort_sh) break;
+            const int m0 = (raster == 2 ? tile % m_tiles : tile / n_tiles) * BM;
+            const int n0 = (raster == 2 ? tile / m_tiles : tile % n_tiles) * BN;
+            int ok = 1;
+            if (lane == 0) ok = mbar_wait(&acc_full[acc], aph, &abort_sh) ? 1 : 0;
+            ok = __shfl_sync(0xffffffffu, ok, 0);
+            if (!ok) break;
+            mbar_try(&acc_full[acc], aph);
+            fence_after();
+            const int row = m0 + lg * 32 + lane;
+            for (int c0 = 0; c0 < BN && n0 + c0 < t; c0 += 32) {
+                uint32_t v[32];
+                tmem_ld32(tmem_base + ((uint32_t)(lg * 32) << 16) + (uint32_t)(acc * BN + c0), v);
+                const int qmax = min(32, t - n0 - c0);
+                if (row < xrows)
+#pragma unroll
+                    for (int q = 0; q < 32; ++q)
+                        if (q < qmax) cout[(size_t)(n0 + c0 + q) * ldc + row] = __uint_as_float(v[q]);
+            }
+            fence_before();
+            mbar_arrive(&acc_empty[acc]);
+            if (++acc == 2) {
+                acc = 0;
+                aph ^= 1u;
+            }
+        }
     } else {
         // ---------------- epilogue ----------------
         // The 128 epilogue threads synchronise among themselves with named
@@ -289,7 +328,8 @@ k_gemm_tc(const __grid_constant__ CUtensorMap mAhi, const __grid_constant__ CUte
         int acc = 0;
         uint32_t aph = 0;
         for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
-            const int m0 = (tile / n_tiles) * BM, n0 = (tile % n_tiles) * BN;
+            const int m0 = (raster == 2 ? tile % m_tiles : tile / n_tiles) * BM;
+            const int n0 = (raster == 2 ? tile / m_tiles : tile % n_tiles) * BN;
             asm volatile("bar.sync 1, 128;" ::: "memory");     // previous tile's readers are done
             if (abort_sh) break;
             // trait constants of this tile (the main loop of the tile is still running)
@@ -393,63 +433,71 @@ static bool make_map(CUtensorMap* m, const __nv_bfloat16* ptr, int rows, int k_p
               CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
-template <int R, class SH>
+static int sm_count() {
+    static int sms[64];
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (!sms[dev & 63]) cudaDeviceGetAttribute(&sms[dev & 63], cudaDevAttrMultiProcessorCount, dev);
+    return sms[dev & 63];
+}
+
+template <int R, class SH, bool STORE>
 static cudaError_t go(const __nv_bfloat16* Xhi, const __nv_bfloat16* Xlo, int xrows, const __nv_bfloat16* Yhi,
-                      const __nv_bfloat16* Ylo, int t, int n_pad, const EpiArgs& E, int* err, cudaStream_t st) {
+                      const __nv_bfloat16* Ylo, int t, int n_pad, const EpiArgs& E, float* cout, int ldc, int raster,
+                      int* err, cudaStream_t st) {
+    constexpr int BN = SH::BN;
     CUtensorMap a_hi, a_lo, b_hi, b_lo;
     if (!make_map(&a_hi, Xhi, xrows, n_pad, BM, SH::BK) || !make_map(&a_lo, Xlo, xrows, n_pad, BM, SH::BK) ||
         !make_map(&b_hi, Yhi, t, n_pad, BN, SH::BK) || !make_map(&b_lo, Ylo, t, n_pad, BN, SH::BK))
         return cudaErrorInvalidValue;
-    static int sms = 0;
-    if (!sms) {
-        int dev = 0;
-        cudaGetDevice(&dev);
-        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    }
     static int attr_done[64];
     int dev = 0;
     cudaGetDevice(&dev);
     if (!attr_done[dev & 63]) {   // once per device, never during a stream capture
-        cudaError_t e = cudaFuncSetAttribute(k_gemm_tc<R, SH>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        cudaError_t e = cudaFuncSetAttribute(k_gemm_tc<R, SH, STORE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                              (int)SH::SMEM_BYTES);
         if (e != cudaSuccess) return e;
         attr_done[dev & 63] = 1;
     }
     const int ntiles = ((xrows + BM - 1) / BM) * ((t + BN - 1) / BN);
+    const int sms = sm_count();
     const int grid = ntiles < sms ? ntiles : sms;
-    k_gemm_tc<R, SH><<<grid, NUM_THREADS, SH::SMEM_BYTES, st>>>(a_hi, a_lo, b_hi, b_lo, xrows, t, n_pad / SH::BK,
-                                                                 E, err);
+    k_gemm_tc<R, SH, STORE><<<grid, NUM_THREADS, SH::SMEM_BYTES, st>>>(a_hi, a_lo, b_hi, b_lo, xrows, t,
+                                                                        n_pad / SH::BK, E, cout, ldc, raster, err);
     return cudaGetLastError();
 }
 
-// Pipeline variant: 0 = BK 32 x 4 stages (default), 1 = BK 64 x 2 stages.
-static int variant() {
-    static int v = -1;
-    if (v < 0) {
-        const char* s = getenv("OA_TC_VARIANT");
-        v = s ? atoi(s) : 0;
-    }
-    return v;
-}
-
+// Pipeline variant: 1 = BK 32 x 4 stages, 2 = BK 64 x 2 stages.
 template <int R>
-static cudaError_t go_any(const __nv_bfloat16* Xhi, const __nv_bfloat16* Xlo, int xrows, const __nv_bfloat16* Yhi,
-                          const __nv_bfloat16* Ylo, int t, int n_pad, const EpiArgs& E, int* err, cudaStream_t st) {
-    if (variant() == 1) return go<R, Shape<64, 2>>(Xhi, Xlo, xrows, Yhi, Ylo, t, n_pad, E, err, st);
-    return go<R, Shape<32, 4>>(Xhi, Xlo, xrows, Yhi, Ylo, t, n_pad, E, err, st);
+static cudaError_t go_any(int variant, int raster, const __nv_bfloat16* Xhi, const __nv_bfloat16* Xlo, int xrows,
+                          const __nv_bfloat16* Yhi, const __nv_bfloat16* Ylo, int t, int n_pad, const EpiArgs& E,
+                          int* err, cudaStream_t st) {
+    if (variant == 2)
+        return go<R, Shape<64, 2>, false>(Xhi, Xlo, xrows, Yhi, Ylo, t, n_pad, E, nullptr, 0, raster, err, st);
+    return go<R, Shape<32, 4>, false>(Xhi, Xlo, xrows, Yhi, Ylo, t, n_pad, E, nullptr, 0, raster, err, st);
 }
 
 }  // namespace tc
 
-cudaError_t oa_launch_gemm_tc(int R, const __nv_bfloat16* Xhi, const __nv_bfloat16* Xlo, int xrows,
-                              const __nv_bfloat16* Yhi, const __nv_bfloat16* Ylo, int t, int n_pad,
+cudaError_t oa_launch_gemm_tc(int R, int variant, int raster, const __nv_bfloat16* Xhi, const __nv_bfloat16* Xlo,
+                              int xrows, const __nv_bfloat16* Yhi, const __nv_bfloat16* Ylo, int t, int n_pad,
                               const EpiArgs& E, int* err, cudaStream_t st) {
     switch (R) {
-        case 1: return tc::go_any<1>(Xhi, Xlo, xrows, Yhi, Ylo, t, n_pad, E, err, st);
-        case 2: return tc::go_any<2>(Xhi, Xlo, xrows, Yhi, Ylo, t, n_pad, E, err, st);
-        case 4: return tc::go_any<4>(Xhi, Xlo, xrows, Yhi, Ylo, t, n_pad, E, err, st);
+        case 1: return tc::go_any<1>(variant, raster, Xhi, Xlo, xrows, Yhi, Ylo, t, n_pad, E, err, st);
+        case 2: return tc::go_any<2>(variant, raster, Xhi, Xlo, xrows, Yhi, Ylo, t, n_pad, E, err, st);
+        case 4: return tc::go_any<4>(variant, raster, Xhi, Xlo, xrows, Yhi, Ylo, t, n_pad, E, err, st);
         default: return cudaErrorInvalidValue;
     }
+}
+
+cudaError_t oa_launch_pre_tc(const __nv_bfloat16* Xhi, const __nv_bfloat16* Xlo, int xrows,
+                             const __nv_bfloat16* Bhi, const __nv_bfloat16* Blo, int c2, int n_pad, float* C, int ldc,
+                             int* err, cudaStream_t st) {
+    const EpiArgs none{};
+    if (c2 <= 64) return tc::go<1, tc::Shape<32, 8, 64>, true>(Xhi, Xlo, xrows, Bhi, Blo, c2, n_pad, none, C, ldc, 1, err, st);
+    if (c2 <= 128)
+        return tc::go<1, tc::Shape<32, 6, 128>, true>(Xhi, Xlo, xrows, Bhi, Blo, c2, n_pad, none, C, ldc, 1, err, st);
+    return tc::go<1, tc::Shape<32, 4, 256>, true>(Xhi, Xlo, xrows, Bhi, Blo, c2, n_pad, none, C, ldc, 1, err, st);
 }
 
 }  // namespace oa

@@ -5,10 +5,22 @@
 
 namespace oa {
 struct StatsArgs;
+struct LeanArgs;
+struct SchurArgs;
 cudaError_t oa_launch_snp_stats(int R, int LP, const StatsArgs& A, int grid, size_t smem, cudaStream_t st);
+// spb: SNPs per CTA group, a power of two <= 8 / R
+cudaError_t oa_launch_snp_lean(int R, int spb, const LeanArgs& A, int grid, size_t smem, cudaStream_t st);
+cudaError_t oa_launch_schur(int R, const SchurArgs& S, cudaStream_t st);
+// pre-GEMM C[col * ldc + row] = sum_k X[row][k] B[col][k], col < c2 (tensor-core and SIMT forms)
+cudaError_t oa_launch_pre_tc(const __nv_bfloat16* Xhi, const __nv_bfloat16* Xlo, int xrows,
+                             const __nv_bfloat16* Bhi, const __nv_bfloat16* Blo, int c2, int n_pad, float* C, int ldc,
+                             int* err, cudaStream_t st);
+cudaError_t oa_launch_pre_simt(const float* X, size_t ldx, int xrows, const float* B, size_t ldb, int c2, int K,
+                               const float* colmean, const int* has_nan, float* C, int ldc, cudaStream_t st);
 cudaError_t oa_launch_gemm_simt(int R, const float* X, size_t ldx, int xrows, const float* Yt, size_t ldy, int t,
                                 int K, const float* colmean, const int* has_nan, const EpiArgs& E, cudaStream_t st);
-cudaError_t oa_launch_gemm_tc(int R, const __nv_bfloat16* Xhi, const __nv_bfloat16* Xlo, int xrows,
-                              const __nv_bfloat16* Yhi, const __nv_bfloat16* Ylo, int t, int n_pad,
+// variant: 1 = BK 32 x 4 stages, 2 = BK 64 x 2 stages; raster: 1 = trait tiles inner, 2 = SNP tiles inner
+cudaError_t oa_launch_gemm_tc(int R, int variant, int raster, const __nv_bfloat16* Xhi, const __nv_bfloat16* Xlo,
+                              int xrows, const __nv_bfloat16* Yhi, const __nv_bfloat16* Ylo, int t, int n_pad,
                               const EpiArgs& E, int* err, cudaStream_t st);
 }  // namespace oa

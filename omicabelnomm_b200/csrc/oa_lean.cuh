@@ -1,0 +1,475 @@
+// Per-SNP column statistics without covariates (k_snp_lean) and the FP64
+// Schur kernel (k_schur) that combines them with the pre-GEMM output.
+//
+// The per-SNP quantities of the reference's corrected systems
+// (Str/Sbr and their missing-row downdates, src/Algorithm.cpp:633-689,
+// 1260-1315) split into
+//   * X'X (r x r) over all rows and over each row set (missingness pattern
+//     or zero set): k_snp_lean, from the SNP columns staged in shared memory
+//     (x-only gathers, no covariate loads);
+//   * Q'X and (Q o m_s)'X for every row set s: a GEMM of the SNP block with
+//     the column matrix B2 = [Q | Q o m_1 | ... | Q o m_S] ("pre-GEMM", on
+//     the same tensor-core / SIMT kernels as the main contraction);
+// and k_schur forms, per (pattern, SNP), the FP64 Schur complement
+//     (D - D_g) - (A - A_g)' W_g (A - A_g)
+// and its inverse, plus var_x from the all-rows complement D - A'A.
+#pragma once
+#include "oa_stats.cuh"
+
+namespace oa {
+
+struct LeanArgs {
+    const float* X;       // SNP block, column c at X + c*ldx
+    size_t ldx;
+    int n, n_pad, mb, nbuf;
+    int nsets;
+    int sets_cap;         // row sets whose sums fit in shared memory at once
+    const int* set_off;
+    const int* rows;
+    float* mean;          // [mb*r] imputation means (0 if the column had no NaN)
+    int* has_nan;
+    float* D;             // [mb][r*r] X'X over all rows
+    float* Dset;          // [nsets][mb][r*r] X'X over each row set
+    __nv_bfloat16* Xhi;   // [mb*r][n_pad] (tensor-core form) or null
+    __nv_bfloat16* Xlo;
+    int write_split;
+    int* err;
+};
+
+// Shared memory of k_snp_lean: nbuf column buffers (stride n_pad floats, the
+// tail [n, n_pad) kept zero) | per-set sums | reduction scratch.
+__host__ __device__ inline size_t lean_smem_bytes(int R, int n_pad, int spb, int nbuf, int sets_cap) {
+    const int NQ = 2 * spb * R + spb * R * R;
+    return (size_t)nbuf * spb * R * n_pad * 4 + (size_t)sets_cap * spb * R * R * 4 + (size_t)8 * NQ * 8 + 64;
+}
+
+// Block-wide sum of NV floats per thread: FP32 within a warp, FP64 across
+// warps; the result is valid in v[] on every thread.
+template <int NV>
+__device__ __forceinline__ void block_sum_fd(float (&v)[NV], double (&out)[NV], double* red /* [8][NV] */) {
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+#pragma unroll
+    for (int q = 0; q < NV; ++q) v[q] = warp_sumf(v[q]);
+    if (lane == 0)
+#pragma unroll
+        for (int q = 0; q < NV; ++q) red[w * NV + q] = (double)v[q];
+    __syncthreads();
+#pragma unroll
+    for (int q = 0; q < NV; ++q) {
+        double s = 0.0;
+#pragma unroll
+        for (int ww = 0; ww < OA_NTHREADS / 32; ++ww) s += red[ww * NV + q];
+        out[q] = s;
+    }
+    __syncthreads();
+}
+
+// One CTA handles SPB SNPs (SPB*R columns) per group; a persistent loop over
+// groups with the next group's columns streaming into shared memory (TMA
+// bulk copies) while this one is processed:
+//   pass 1  column sums, NaN counts and X'X from float4 reads of the staged
+//           columns (one block reduction); a column with NaN is mean-imputed
+//           in place and X'X recomputed (src/Utility.cpp:302-326)
+//   pass 2  BF16 hi/lo split of the columns (tensor-core form only)
+//   pass 3  X'X over each row set: the flattened row lists split evenly
+//           over the warps, lanes accumulate while the set is unchanged and
+//           flush into per-set sums in shared memory at a set boundary
+template <int R, int SPB, bool BULK>
+__global__ void __launch_bounds__(OA_NTHREADS)
+k_snp_lean(LeanArgs A) {
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    constexpr int NC = SPB * R;                 // columns per group
+    constexpr int K2 = SPB * R * R;             // X'X entries per group
+    constexpr int NQ = 2 * NC + K2;
+    constexpr int NWARP = OA_NTHREADS / 32;
+    const int n = A.n, nS = A.n_pad;
+    const size_t buf_floats = (size_t)NC * nS;
+    float* bufs = reinterpret_cast<float*>(smem_raw);                                   // [nbuf][NC][nS]
+    float* setacc = bufs + (size_t)A.nbuf * buf_floats;                                 // [sets_cap][K2]
+    double* red = reinterpret_cast<double*>(
+        (reinterpret_cast<uintptr_t>(setacc + (size_t)A.sets_cap * K2) + 7) & ~(uintptr_t)7);   // [8][NQ]
+    __shared__ __align__(8) uint64_t mbar[2];
+    __shared__ int stop;
+    const int ngroups = (A.mb + SPB - 1) / SPB;
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+
+    auto issue = [&](int g, int b) {
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");   // earlier generic writes to the buffer
+        const int i0 = g * SPB;
+        const int ncol = min(SPB, A.mb - i0) * R;
+        const uint32_t bytes = (uint32_t)n * 4u;
+        asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(st_su32(&mbar[b])),
+                     "r"(bytes * (uint32_t)ncol)
+                     : "memory");
+        for (int c = 0; c < ncol; ++c) {
+            const float* src = A.X + (size_t)(i0 * R + c) * A.ldx;
+            float* dst = bufs + (size_t)b * buf_floats + (size_t)c * nS;
+            asm volatile(
+                "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                    st_su32(dst)),
+                "l"(reinterpret_cast<uint64_t>(src)), "r"(bytes), "r"(st_su32(&mbar[b]))
+                : "memory");
+        }
+    };
+
+    // zero the column tails [n, n_pad) once: copies write only [0, n)
+    for (int q = threadIdx.x; q < A.nbuf * NC * (nS - n); q += blockDim.x) {
+        const int c = q / (nS - n), k = n + q % (nS - n);
+        bufs[(size_t)c * nS + k] = 0.f;
+    }
+    if (threadIdx.x == 0) {
+        stop = 0;
+        if (BULK) {
+            for (int b = 0; b < 2; ++b) asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(st_su32(&mbar[b])));
+            asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+            if ((int)blockIdx.x < ngroups) issue(blockIdx.x, 0);
+        }
+    }
+    __syncthreads();
+
+    int q = 0;
+    for (int g = blockIdx.x; g < ngroups; g += gridDim.x, ++q) {
+        const int gn = g + gridDim.x;
+        const int b = A.nbuf == 2 ? (q & 1) : 0;
+        const uint32_t par = A.nbuf == 2 ? (uint32_t)((q >> 1) & 1) : (uint32_t)(q & 1);
+        float* xs = bufs + (size_t)b * buf_floats;
+        const int i0 = g * SPB;
+        const int nsnp = min(SPB, A.mb - i0);
+        const int ncol = nsnp * R;
+
+        if (BULK) {
+            if (threadIdx.x == 0) {
+                if (A.nbuf == 2 && gn < ngroups) issue(gn, b ^ 1);
+                if (!st_mbar_wait(&mbar[b], par)) {
+                    stop = 1;
+                    atomicExch(A.err, 1);
+                }
+            }
+            __syncthreads();
+            if (stop) break;
+            st_mbar_try(&mbar[b], par);
+        } else {
+            for (int c = 0; c < ncol; ++c) {
+                const float* src = A.X + (size_t)(i0 * R + c) * A.ldx;
+                float* dst = xs + (size_t)c * nS;
+#pragma unroll 4
+                for (int k = threadIdx.x; k < n; k += blockDim.x) dst[k] = src[k];
+            }
+            __syncthreads();
+        }
+        // columns past the block's end read as zero
+        const float4* x4 = reinterpret_cast<const float4*>(xs);
+        const int nS4 = nS / 4;
+
+        // ---- pass 1: sums, NaN counts, X'X
+        float acc[NQ];
+        double tot[NQ];
+#pragma unroll
+        for (int u = 0; u < NQ; ++u) acc[u] = 0.f;
+        for (int k4 = threadIdx.x; k4 < nS4; k4 += blockDim.x) {
+            float4 v[NC];
+#pragma unroll
+            for (int c = 0; c < NC; ++c) v[c] = c < ncol ? x4[(size_t)c * nS4 + k4] : make_float4(0.f, 0.f, 0.f, 0.f);
+#pragma unroll
+            for (int c = 0; c < NC; ++c) {
+                const float e[4] = {v[c].x, v[c].y, v[c].z, v[c].w};
+#pragma unroll
+                for (int u = 0; u < 4; ++u) {
+                    const bool nan = isnan(e[u]);
+                    acc[c] += nan ? 0.f : e[u];
+                    acc[NC + c] += nan ? 1.f : 0.f;
+                }
+            }
+#pragma unroll
+            for (int s = 0; s < SPB; ++s)
+#pragma unroll
+                for (int a = 0; a < R; ++a)
+#pragma unroll
+                    for (int bb = 0; bb < R; ++bb) {
+                        const float4 xa = v[s * R + a], xb = v[s * R + bb];
+                        acc[2 * NC + (s * R + a) * R + bb] += xa.x * xb.x + xa.y * xb.y + xa.z * xb.z + xa.w * xb.w;
+                    }
+        }
+        block_sum_fd<NQ>(acc, tot, red);
+        bool any_nan = false;
+#pragma unroll
+        for (int c = 0; c < NC; ++c) any_nan |= (c < ncol) && tot[NC + c] > 0.0;
+        if (any_nan) {   // mean-impute in place, then X'X again (block-uniform branch)
+#pragma unroll
+            for (int c = 0; c < NC; ++c) {
+                if (c < ncol && tot[NC + c] > 0.0) {
+                    const float mv = (float)(tot[c] / ((double)n - tot[NC + c]));
+                    float* col = xs + (size_t)c * nS;
+                    for (int k = threadIdx.x; k < n; k += blockDim.x)
+                        if (isnan(col[k])) col[k] = mv;
+                }
+            }
+            __syncthreads();
+            float acc2[K2];
+            double tot2[K2];
+#pragma unroll
+            for (int u = 0; u < K2; ++u) acc2[u] = 0.f;
+            for (int k4 = threadIdx.x; k4 < nS4; k4 += blockDim.x) {
+                float4 v[NC];
+#pragma unroll
+                for (int c = 0; c < NC; ++c)
+                    v[c] = c < ncol ? x4[(size_t)c * nS4 + k4] : make_float4(0.f, 0.f, 0.f, 0.f);
+#pragma unroll
+                for (int s = 0; s < SPB; ++s)
+#pragma unroll
+                    for (int a = 0; a < R; ++a)
+#pragma unroll
+                        for (int bb = 0; bb < R; ++bb) {
+                            const float4 xa = v[s * R + a], xb = v[s * R + bb];
+                            acc2[(s * R + a) * R + bb] += xa.x * xb.x + xa.y * xb.y + xa.z * xb.z + xa.w * xb.w;
+                        }
+            }
+            block_sum_fd<K2>(acc2, tot2, red);
+#pragma unroll
+            for (int u = 0; u < K2; ++u) tot[2 * NC + u] = tot2[u];
+        }
+        if (threadIdx.x == 0) {
+#pragma unroll
+            for (int c = 0; c < NC; ++c) {
+                if (c < ncol) {
+                    const bool has = tot[NC + c] > 0.0;
+                    A.mean[i0 * R + c] = has ? (float)(tot[c] / ((double)n - tot[NC + c])) : 0.0f;
+                    if (has) atomicOr(A.has_nan, 1);
+                }
+            }
+#pragma unroll
+            for (int u = 0; u < K2; ++u)
+                if (u < nsnp * R * R) A.D[(size_t)i0 * R * R + u] = (float)tot[2 * NC + u];
+        }
+
+        // ---- pass 2: BF16 hi/lo split, 8 elements per thread and step
+        if (A.write_split) {
+            const int np8 = nS / 8;
+            for (int c = 0; c < ncol; ++c) {
+                const float4* col = x4 + (size_t)c * nS4;
+                uint4* hi = reinterpret_cast<uint4*>(A.Xhi + (size_t)(i0 * R + c) * A.n_pad);
+                uint4* lo = reinterpret_cast<uint4*>(A.Xlo + (size_t)(i0 * R + c) * A.n_pad);
+                for (int k8 = threadIdx.x; k8 < np8; k8 += blockDim.x) {
+                    const float4 p0 = col[2 * k8], p1 = col[2 * k8 + 1];
+                    const float e[8] = {p0.x, p0.y, p0.z, p0.w, p1.x, p1.y, p1.z, p1.w};
+                    uint32_t h[4], o[4];
+#pragma unroll
+                    for (int u = 0; u < 4; ++u) {
+                        const __nv_bfloat16 h0 = __float2bfloat16_rn(e[2 * u]), h1 = __float2bfloat16_rn(e[2 * u + 1]);
+                        const __nv_bfloat16 l0 = __float2bfloat16_rn(e[2 * u] - __bfloat162float(h0));
+                        const __nv_bfloat16 l1 = __float2bfloat16_rn(e[2 * u + 1] - __bfloat162float(h1));
+                        h[u] = (uint32_t)__bfloat16_as_ushort(h0) | ((uint32_t)__bfloat16_as_ushort(h1) << 16);
+                        o[u] = (uint32_t)__bfloat16_as_ushort(l0) | ((uint32_t)__bfloat16_as_ushort(l1) << 16);
+                    }
+                    hi[k8] = make_uint4(h[0], h[1], h[2], h[3]);
+                    lo[k8] = make_uint4(o[0], o[1], o[2], o[3]);
+                }
+            }
+        }
+
+        // ---- pass 3: X'X over each row set
+        for (int s0 = 0; s0 < A.nsets; s0 += A.sets_cap) {
+            const int s1 = min(A.nsets, s0 + A.sets_cap);
+            for (int u = threadIdx.x; u < (s1 - s0) * K2; u += blockDim.x) setacc[u] = 0.f;
+            __syncthreads();
+            const int r0 = __ldg(A.set_off + s0), r1 = __ldg(A.set_off + s1);
+            const int per = (r1 - r0 + NWARP - 1) / NWARP;
+            const int w0 = r0 + w * per, w1 = min(r1, w0 + per);
+            if (w0 < w1) {
+                // set of row w0: last set s with set_off[s] <= w0
+                int lo_s = s0, hi_s = s1 - 1;
+                while (lo_s < hi_s) {
+                    const int mid = (lo_s + hi_s + 1) >> 1;
+                    if (__ldg(A.set_off + mid) <= w0) lo_s = mid;
+                    else hi_s = mid - 1;
+                }
+                int cur = lo_s;
+                int nextb = __ldg(A.set_off + cur + 1);
+                float sacc[K2];
+#pragma unroll
+                for (int u = 0; u < K2; ++u) sacc[u] = 0.f;
+                for (int kk = w0 + lane; kk < w1; kk += 32) {
+                    if (kk >= nextb) {
+#pragma unroll
+                        for (int u = 0; u < K2; ++u)
+                            if (sacc[u] != 0.f) atomicAdd(setacc + (cur - s0) * K2 + u, sacc[u]);
+#pragma unroll
+                        for (int u = 0; u < K2; ++u) sacc[u] = 0.f;
+                        do {
+                            ++cur;
+                            nextb = __ldg(A.set_off + cur + 1);
+                        } while (kk >= nextb);
+                    }
+                    const int k = __ldg(A.rows + kk);
+                    float x[NC];
+#pragma unroll
+                    for (int c = 0; c < NC; ++c) x[c] = xs[(size_t)c * nS + k];
+#pragma unroll
+                    for (int s = 0; s < SPB; ++s)
+#pragma unroll
+                        for (int a = 0; a < R; ++a)
+#pragma unroll
+                            for (int bb = 0; bb < R; ++bb) sacc[(s * R + a) * R + bb] += x[s * R + a] * x[s * R + bb];
+                }
+#pragma unroll
+                for (int u = 0; u < K2; ++u)
+                    if (sacc[u] != 0.f) atomicAdd(setacc + (cur - s0) * K2 + u, sacc[u]);
+            }
+            __syncthreads();
+            for (int u = threadIdx.x; u < (s1 - s0) * K2; u += blockDim.x) {
+                const int set = s0 + u / K2, e = u % K2;
+                const int s = e / (R * R), f = e % (R * R);
+                if (s < nsnp) A.Dset[((size_t)set * A.mb + i0 + s) * R * R + f] = setacc[u];
+            }
+            __syncthreads();
+        }
+        __syncthreads();   // every reader of this buffer is done before it is refilled
+        if (BULK && A.nbuf == 1 && threadIdx.x == 0 && gn < ngroups) issue(gn, 0);
+    }
+    if (BULK && threadIdx.x == 0 && stop) {
+        st_mbar_wait(&mbar[0], 0);
+        st_mbar_wait(&mbar[0], 1);
+        st_mbar_wait(&mbar[1], 0);
+        st_mbar_wait(&mbar[1], 1);
+    }
+}
+
+// The pre-GEMM's column matrix B2 = [Q | Q o m_1 | ... | Q o m_S] (K-major:
+// column c of B2 is row c of the c2 x n_pad array), FP32 and, for the
+// tensor-core form, BF16 hi/lo.  Step 1 writes Q and zeros; step 2 scatters
+// Q's rows into the columns of every row set that contains them.
+static __global__ void k_b2_init(const float* __restrict__ Qr, int LP, int n, int n_pad, int l, int c2,
+                          float* __restrict__ B2) {
+    const long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (q >= (long long)c2 * n_pad) return;
+    const int c = (int)(q / n_pad), k = (int)(q % n_pad);
+    B2[q] = (c < l && k < n) ? Qr[(size_t)k * LP + c] : 0.f;
+}
+
+static __global__ void k_b2_scatter(const float* __restrict__ Qr, int LP, int n_pad, int l, const int* __restrict__ set_off,
+                             const int* __restrict__ rows, float* __restrict__ B2) {
+    const int s = blockIdx.x;
+    const int r0 = set_off[s], r1 = set_off[s + 1];
+    float* dst = B2 + (size_t)(l + s * l) * n_pad;
+    for (int kk = r0 + threadIdx.x; kk < r1; kk += blockDim.x) {
+        const int k = rows[kk];
+        for (int a = 0; a < l; ++a) dst[(size_t)a * n_pad + k] = Qr[(size_t)k * LP + a];
+    }
+}
+
+static __global__ void k_split_bf16(const float* __restrict__ src, long long count, __nv_bfloat16* __restrict__ hi,
+                             __nv_bfloat16* __restrict__ lo) {
+    const long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (q >= count) return;
+    const float v = src[q];
+    const __nv_bfloat16 h = __float2bfloat16_rn(v);
+    hi[q] = h;
+    lo[q] = __float2bfloat16_rn(v - __bfloat162float(h));
+}
+
+struct SchurArgs {
+    int l, mb, G, Z, ldc;
+    const float* C2;         // pre-GEMM output, column c of SNP column x at C2[c * ldc + x]
+    const float* D;          // [mb][r*r]
+    const float* Dset;       // [G+Z][mb][r*r]
+    const double* W;         // [G][l][l]
+    const uint8_t* pat_bad;  // [G]
+    double* sinv;            // [G][mb][r*r]
+    uint8_t* sing;           // [G][mb]
+    float* varx;             // [mb][r]
+    float* aobs;             // [G][mb][l][r] or null
+    float* afull;            // [mb][l][r] or null
+    double* sfinv;           // [mb][r*r] or null
+    float* zA;               // [Z][mb][l][r]
+    float* zD;               // [Z][mb][r][r]
+};
+
+// All (SNP, pattern) systems of a SNP block in one persistent launch: a
+// thread per (SNP, slot) work item, grid-stride over the items.  Slot 0 is
+// the all-rows complement (var_x), slots 1..G the patterns, slots
+// G+1..G+Z copy the zero-set sums.
+template <int R>
+__device__ __forceinline__ void schur_item(const SchurArgs& S, int i, int slot) {
+    const int l = S.l;
+    double a_full[OA_MAX_L * R];
+    for (int qq = 0; qq < l; ++qq)
+#pragma unroll
+        for (int a = 0; a < R; ++a) a_full[qq * R + a] = (double)S.C2[(size_t)qq * S.ldc + i * R + a];
+    double Dm[R * R];
+#pragma unroll
+    for (int u = 0; u < R * R; ++u) Dm[u] = (double)S.D[(size_t)i * R * R + u];
+    // all-rows Schur complement D - A'A (Q orthonormal): var_x of the SNP terms (src/Algorithm.cpp:665-670)
+    double Sf[R * R];
+#pragma unroll
+    for (int a = 0; a < R; ++a)
+#pragma unroll
+        for (int b = 0; b < R; ++b) {
+            double v = Dm[a * R + b];
+            for (int qq = 0; qq < l; ++qq) v -= a_full[qq * R + a] * a_full[qq * R + b];
+            Sf[a * R + b] = v;
+        }
+    const bool full_ok = spd_inverse<R>(Sf, R, 1e-9);
+    if (slot == 0) {
+#pragma unroll
+        for (int a = 0; a < R; ++a) S.varx[(size_t)i * R + a] = full_ok ? (float)Sf[a * R + a] : 0.f;
+        if (S.sfinv)
+#pragma unroll
+            for (int u = 0; u < R * R; ++u) S.sfinv[(size_t)i * R * R + u] = full_ok ? Sf[u] : 0.0;
+        if (S.afull)
+            for (int u = 0; u < l * R; ++u) S.afull[(size_t)i * l * R + u] = (float)a_full[u];
+        return;
+    }
+    if (slot > S.G) {  // zero set z: its sums go to the epilogue unchanged
+        const int z = slot - 1 - S.G;
+        const size_t zi = (size_t)z * S.mb + i;
+        for (int qq = 0; qq < l; ++qq)
+#pragma unroll
+            for (int a = 0; a < R; ++a)
+                S.zA[zi * l * R + qq * R + a] = S.C2[(size_t)(l + (S.G + z) * l + qq) * S.ldc + i * R + a];
+#pragma unroll
+        for (int u = 0; u < R * R; ++u) S.zD[zi * R * R + u] = S.Dset[((size_t)(S.G + z) * S.mb + i) * R * R + u];
+        return;
+    }
+    const int g = slot - 1;
+    const size_t gi = (size_t)g * S.mb + i;
+    double ao[OA_MAX_L * R];
+    for (int qq = 0; qq < l; ++qq)
+#pragma unroll
+        for (int a = 0; a < R; ++a)
+            ao[qq * R + a] = a_full[qq * R + a] - (double)S.C2[(size_t)(l + g * l + qq) * S.ldc + i * R + a];
+    double Sg[R * R];
+#pragma unroll
+    for (int u = 0; u < R * R; ++u) Sg[u] = Dm[u] - (double)S.Dset[gi * R * R + u];
+    const double* Wg = S.W + (size_t)g * l * l;
+    for (int qq = 0; qq < l; ++qq) {
+        double wa[R];
+#pragma unroll
+        for (int b = 0; b < R; ++b) wa[b] = 0.0;
+        for (int u = 0; u < l; ++u) {
+            const double wq = Wg[qq * l + u];
+#pragma unroll
+            for (int b = 0; b < R; ++b) wa[b] += wq * ao[u * R + b];
+        }
+#pragma unroll
+        for (int a = 0; a < R; ++a)
+#pragma unroll
+            for (int b = 0; b < R; ++b) Sg[a * R + b] -= ao[qq * R + a] * wa[b];
+    }
+    const bool ok = full_ok && !S.pat_bad[g] && spd_inverse<R>(Sg, R, 1e-9);
+    S.sing[gi] = ok ? 0 : 1;
+#pragma unroll
+    for (int u = 0; u < R * R; ++u) S.sinv[gi * R * R + u] = ok ? Sg[u] : 0.0;
+    if (S.aobs)
+        for (int u = 0; u < l * R; ++u) S.aobs[gi * l * R + u] = (float)ao[u];
+}
+
+template <int R>
+__global__ void __launch_bounds__(256) k_schur(SchurArgs S) {
+    const int slots = 1 + S.G + S.Z;
+    const long long total = (long long)S.mb * slots;
+    for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < total;
+         q += (long long)gridDim.x * blockDim.x)
+        schur_item<R>(S, (int)(q / slots), (int)(q % slots));
+}
+
+}  // namespace oa

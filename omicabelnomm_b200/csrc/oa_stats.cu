@@ -1,5 +1,7 @@
-// Instantiations of the per-SNP statistics kernel (see oa_kernels.cuh).
-#include "oa_stats.cuh"
+// Instantiations of the per-SNP statistics kernels (oa_stats.cuh, oa_lean.cuh).
+#include <algorithm>
+
+#include "oa_lean.cuh"
 #include "oa_launch.h"
 
 namespace oa {
@@ -47,6 +49,62 @@ cudaError_t oa_launch_snp_stats(int R, int LP, const StatsArgs& A, int grid, siz
         case 416: return go<4, 16>(A, grid, smem, st);
         default: return cudaErrorInvalidValue;
     }
+}
+
+template <int R, int SPB>
+static cudaError_t go_lean(const LeanArgs& A, int grid, size_t smem, cudaStream_t st) {
+    const bool bulk = (A.n % 4 == 0) && (A.ldx % 4 == 0) && ((reinterpret_cast<uintptr_t>(A.X) & 15) == 0);
+    static int set_bulk[64], set_plain[64];
+    int dev = 0;
+    cudaGetDevice(&dev);
+    const int d = dev & 63;
+    int* done = bulk ? set_bulk : set_plain;
+    if (done[d] < (int)smem) {
+        cudaError_t e = bulk ? cudaFuncSetAttribute(k_snp_lean<R, SPB, true>,
+                                                    cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024 - 1024)
+                             : cudaFuncSetAttribute(k_snp_lean<R, SPB, false>,
+                                                    cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024 - 1024);
+        if (e != cudaSuccess) return e;
+        done[d] = 227 * 1024 - 1024;
+    }
+    if (bulk)
+        k_snp_lean<R, SPB, true><<<grid, OA_NTHREADS, smem, st>>>(A);
+    else
+        k_snp_lean<R, SPB, false><<<grid, OA_NTHREADS, smem, st>>>(A);
+    return cudaGetLastError();
+}
+
+cudaError_t oa_launch_snp_lean(int R, int spb, const LeanArgs& A, int grid, size_t smem, cudaStream_t st) {
+    switch (R * 100 + spb) {
+        case 101: return go_lean<1, 1>(A, grid, smem, st);
+        case 102: return go_lean<1, 2>(A, grid, smem, st);
+        case 104: return go_lean<1, 4>(A, grid, smem, st);
+        case 108: return go_lean<1, 8>(A, grid, smem, st);
+        case 201: return go_lean<2, 1>(A, grid, smem, st);
+        case 202: return go_lean<2, 2>(A, grid, smem, st);
+        case 204: return go_lean<2, 4>(A, grid, smem, st);
+        case 401: return go_lean<4, 1>(A, grid, smem, st);
+        case 402: return go_lean<4, 2>(A, grid, smem, st);
+        default: return cudaErrorInvalidValue;
+    }
+}
+
+cudaError_t oa_launch_schur(int R, const SchurArgs& S, cudaStream_t st) {
+    const long long total = (long long)S.mb * (1 + S.G + S.Z);
+    if (total <= 0) return cudaSuccess;
+    // persistent: at most 8 resident CTAs of 256 threads per SM
+    static int sms[64];
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (!sms[dev & 63]) cudaDeviceGetAttribute(&sms[dev & 63], cudaDevAttrMultiProcessorCount, dev);
+    const unsigned blocks = (unsigned)std::min<long long>((total + 255) / 256, 8LL * sms[dev & 63]);
+    switch (R) {
+        case 1: k_schur<1><<<blocks, 256, 0, st>>>(S); break;
+        case 2: k_schur<2><<<blocks, 256, 0, st>>>(S); break;
+        case 4: k_schur<4><<<blocks, 256, 0, st>>>(S); break;
+        default: return cudaErrorInvalidValue;
+    }
+    return cudaGetLastError();
 }
 
 }  // namespace oa

@@ -56,6 +56,14 @@ class Settings(C.Structure):
                 ("quirk_r2", C.c_int32), ("verbose", C.c_int32)]
 
 
+class Tuning(C.Structure):
+    _fields_ = [("chunk_snps", C.c_int32), ("gemm_variant", C.c_int32), ("gemm_raster", C.c_int32),
+                ("stats_path", C.c_int32), ("lean_spb", C.c_int32)]
+
+    def as_dict(self) -> dict:
+        return {k: int(getattr(self, k)) for k, _ in self._fields_}
+
+
 class Outputs(C.Structure):
     _fields_ = [("total_sig_results", C.c_uint64), ("duration_s", C.c_double), ("tests", C.c_int64),
                 ("rows_written", C.c_int64), ("singular", C.c_int64)]
@@ -96,6 +104,9 @@ def lib() -> C.CDLL:
         "oa_abi_version": ([], C.c_int32),
         "oa_scan_dense_noalloc": ([P, P, P, C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_int32, P, P, P, P,
                                    P], C.c_int),
+        "oa_set_tuning": ([P, C.POINTER(Tuning)], C.c_int),
+        "oa_get_tuning": ([P, C.POINTER(Tuning)], C.c_int),
+        "oa_autotune": ([P, P, C.c_int32, C.POINTER(Tuning)], C.c_int),
     }
     for name, (args, res) in sig.items():
         f = getattr(L, name)
@@ -229,6 +240,22 @@ class Engine:
         r2 = np.empty((t, mb), np.float32)
         _check(lib().oa_dense_last(self.h, _fptr(b), _fptr(se), _fptr(tt), _fptr(r2)))
         return b, se, tt, r2
+
+    def set_tuning(self, **fields):
+        """oa_set_tuning: chunk_snps, gemm_variant, gemm_raster, stats_path, lean_spb (0 = automatic)."""
+        t = Tuning(**{k: int(v) for k, v in fields.items()})
+        _check(lib().oa_set_tuning(self.h, C.byref(t)))
+
+    def tuning(self) -> dict:
+        t = Tuning()
+        _check(lib().oa_get_tuning(self.h, C.byref(t)))
+        return t.as_dict()
+
+    def autotune(self, ptr: int, mb: int) -> dict:
+        """oa_autotune on a device SNP block of mb SNPs; returns the tuning kept."""
+        t = Tuning()
+        _check(lib().oa_autotune(self.h, C.c_void_p(ptr), mb, C.byref(t)))
+        return t.as_dict()
 
     def launches(self) -> int:
         return int(lib().oa_kernel_launches(self.h))

@@ -26,6 +26,7 @@ def test_struct_sizes_match_header():
     assert C.sizeof(E.Config) == 14 * 4
     assert C.sizeof(E.Rows) == 8 + 8 * 8 + 3 * 8
     assert C.sizeof(E.Outputs) == 8 * 5
+    assert C.sizeof(E.Tuning) == 5 * 4
 
 
 @pytest.mark.parametrize("p", [0.1, 0.05, 0.01, 1e-5, 5e-8])

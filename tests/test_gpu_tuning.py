@@ -1,0 +1,80 @@
+"""Tuning parameters and the autotuner: every tuning gives the same results
+(the per-SNP work does not depend on tile order, chunking or SNPs per CTA
+group), and oa_autotune keeps a valid tuning."""
+import numpy as np
+import pytest
+
+from omicabelnomm_b200 import engine as E
+from omicabelnomm_b200 import synth
+
+pytestmark = pytest.mark.gpu
+
+
+def _data():
+    w = synth.scaled(0, n=1024, m=1500, t=300, l=5, r=2, miss_mode="patterns", n_patterns=12, miss_hi=0.15,
+                     seed=81)
+    return w, synth.generate(w)
+
+
+def _run(ds, w, prec, **tuning):
+    m = ds.XR.shape[0] // w.r
+    eng = E.Engine(w.n, w.l, w.r, w.t, m, precision=prec, min_t_store=E.t_threshold(0.1), min_r2_store=1e-6)
+    if tuning:
+        eng.set_tuning(**tuning)
+    eng.set_covariates(ds.XL)
+    eng.set_traits(ds.Y)
+    eng.enable_dense(True)
+    rows = eng.run(ds.XR)
+    return eng, rows, eng.dense(m)
+
+
+@pytest.mark.parametrize("prec", [E.PLAIN, E.MIXED])
+def test_tunings_give_identical_results(prec):
+    w, ds = _data()
+    _, rows0, d0 = _run(ds, w, prec)
+    variants = [dict(gemm_raster=2), dict(chunk_snps=256), dict(lean_spb=1), dict(lean_spb=4),
+                dict(stats_path=1, chunk_snps=700)]
+    if prec == E.MIXED:
+        variants.append(dict(gemm_variant=2))
+    for v in variants:
+        eng, rows, d = _run(ds, w, prec, **v)
+        for a, b in zip(d0, d):
+            np.testing.assert_array_equal(a, b, err_msg=str(v))
+        np.testing.assert_array_equal(rows0.trait, rows.trait)
+        np.testing.assert_array_equal(rows0.snp, rows.snp)
+        got = eng.tuning()
+        for k, val in v.items():
+            if k != "lean_spb":
+                assert got[k] == val, (k, got)
+    # the row-gather path: same numbers within FP32 summation-order differences
+    _, rows_g, dg = _run(ds, w, prec, stats_path=2)
+    np.testing.assert_allclose(dg[2], d0[2], rtol=1e-4, atol=1e-4)
+
+
+def test_autotune_keeps_a_valid_tuning():
+    import torch
+    w, ds = _data()
+    m = ds.XR.shape[0] // w.r
+    dev = torch.device("cuda", 0)
+    xr = torch.from_numpy(ds.XR).to(dev)
+    y = torch.from_numpy(ds.Y).to(dev)
+    eng = E.Engine(w.n, w.l, w.r, w.t, m, precision=E.MIXED, min_t_store=E.t_threshold(0.1), min_r2_store=1e-6)
+    eng.set_covariates(ds.XL)
+    eng.set_traits_device(y.data_ptr(), w.t)
+    eng.enable_dense(True)
+    eng.run_device(xr.data_ptr(), m)
+    before = [a.copy() for a in eng.dense(m)]
+    best = eng.autotune(xr.data_ptr(), m)
+    assert best["gemm_variant"] in (1, 2) and best["gemm_raster"] in (1, 2) and best["stats_path"] in (1, 2)
+    assert 0 < best["chunk_snps"] <= m
+    eng.run_device(xr.data_ptr(), m)
+    after = eng.dense(m)
+    np.testing.assert_allclose(after[2], before[2], rtol=1e-4, atol=1e-4)
+
+
+def test_set_tuning_rejects_out_of_range():
+    eng = E.Engine(256, 3, 1, 4, 16)
+    with pytest.raises(E.OAError):
+        eng.set_tuning(gemm_variant=3)
+    with pytest.raises(E.OAError):
+        eng.set_tuning(stats_path=-1)
