@@ -298,6 +298,47 @@ def batched_section(args, dev, local, rank, barrier, max_over_ranks):
             "max_dt_mixed_vs_plain_first_4096_snps": dt}
 
 
+def serve_section(args, dev, local):
+    """Serving loop: Poisson arrivals (20/s) of scan requests against a
+    genotype matrix resident in HBM (n = 20,000 x 1,000,000 SNPs, 80 GB);
+    each request: a cohort of n ~ U(2,000, 20,000) individuals with l ~ U{3..6}
+    covariates (12 cohorts), t ~ LogUniform(1, 500) traits with 0-10 %
+    missingness, a contiguous range of LogUniform(10k, 1M) SNPs; mixed form,
+    stored rows P < 1e-3 returned to the host; admission by device-memory
+    footprint, up to 8 requests on the GPU at once."""
+    import torch
+    from omicabelnomm_b200 import serve as S
+    w = S.ServeWorkload(m_total=args.serve_m, requests=args.serve_requests)
+    G = S.resident_genotypes(w, dev)
+    cohorts = S.make_cohorts(w)
+    keep = []
+    reqs = S.make_requests(w, cohorts, dev, keep)
+    torch.cuda.synchronize()
+    free, _ = torch.cuda.mem_get_info(dev)
+    budget = int(free - (6 << 30))
+    srv = S.Server(G.data_ptr(), w.n_total, w.m_total, cohorts, device=local, budget_bytes=budget, max_slots=8,
+                   chunk_snps=8192, min_p_store=1e-3)
+    # warm-up (kernel attributes, first engine), not timed: one trait of the first request
+    srv.run([S.Request(rid=-1, cohort=reqs[0].cohort, snp0=0, nsnp=20000, y_ptr=reqs[0].y_ptr, t=1)],
+            realtime=False)
+    clocks = ClockSampler(local)
+    clocks.start()
+    res = srv.run(reqs, realtime=True)
+    clk = clocks.stop()
+    out = S.summarize(res)
+    out.update({"workload": f"serving: resident genotypes n={w.n_total} x m={w.m_total} SNPs (float32 in HBM), "
+                            f"{w.requests} requests at Poisson rate {w.rate}/s, {w.cohorts} cohorts, "
+                            f"n_req~U({w.n_lo},{w.n_hi}), t~LogU({w.t_lo:g},{w.t_hi:g}), "
+                            f"SNP range~LogU({w.len_lo:g},{w.len_hi:g}), l~U{{{w.l_lo}..{w.l_hi}}}, "
+                            f"missing 0-{w.miss_hi:g}",
+                "form": "mixed", "max_concurrent": srv.max_slots, "budget_bytes": budget,
+                "peak_admitted_bytes": srv.peak_bytes, "evictions": srv.evictions, "clocks": clk})
+    srv.close()
+    del G, keep
+    torch.cuda.empty_cache()
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -309,6 +350,8 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=2)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--batched-m", type=int, default=200000, help="SNPs of the batched workload (0: skip it)")
+    ap.add_argument("--serve-requests", type=int, default=120, help="requests of the serving run (0: skip it)")
+    ap.add_argument("--serve-m", type=int, default=1_000_000, help="SNPs of the resident serving matrix")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference_arm(args)
@@ -411,6 +454,13 @@ def main():
         except E.OAError as ex:
             batched = {"error": str(ex)}
 
+    serve = None
+    if args.serve_requests > 0 and world == 1:
+        try:
+            serve = serve_section(args, dev, local)
+        except E.OAError as ex:
+            serve = {"error": str(ex)}
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
@@ -480,6 +530,7 @@ def main():
                   for k, v in results.items()},
         "max_dt_mixed_vs_plain_first_16384_snps": dt_mp,
         "batched": batched,
+        "serve": serve,
     }
     print(json.dumps(line))
     if dist is not None:

@@ -132,6 +132,19 @@ oa_status oa_run_snps_device(oa_engine* e, const float* xr_dev, int32_t mb,
 oa_status oa_dense_last(oa_engine* e, float* beta, float* se, float* tstat, float* r2);
 oa_status oa_enable_dense(oa_engine* e, int32_t on);
 
+/* Row subset of device SNP blocks: after this call oa_run_snps_device reads
+ * SNP columns of ld floats (e.g. a genotype matrix kept resident across
+ * calls) and takes rows[0..n_rows) of each (ascending, n_rows = the
+ * engine's n) as its individuals, gathered on the device chunk by chunk.
+ * rows = NULL restores contiguous columns of n.  Not for host blocks
+ * (oa_run_snps returns OA_ERR_STATE).  No counterpart in the reference
+ * (its reader keeps the rows of the exclusion list's kept runs while loading a
+ * SNP block, src/AIOwrapper.cpp:1098-1130). */
+oa_status oa_set_snp_rows(oa_engine* e, const int32_t* rows, int32_t n_rows, int64_t ld);
+
+/* Device memory held by the engine's buffers, in bytes. */
+int64_t oa_device_bytes(const oa_engine* e);
+
 /* Size of the scratch array used by oa_scan_dense_noalloc (64 MiB).  Every
  * GPU on which the library is loaded holds this much device memory until the
  * process exits. */
@@ -211,6 +224,11 @@ typedef struct oa_settings {
     int32_t device;
     int32_t quirk_r2;
     int32_t verbose;             /* progress characters and messages on stdout */
+    int32_t shard;               /* this process's SNP shard, 0..shards-1 (≙ mpi_id) */
+    int32_t shards;              /* SNP shards (≙ mpi_num_threads, src/AIOwrapper.cpp:95-117): with
+                                    shards > 1 and m >= shards, shard k scans SNPs [k*m/shards, ...)
+                                    (the last shard also the remainder) and writes
+                                    <out>_mpi<k+1>__dis.txt etc. with shard-local SNP indices */
 } oa_settings;
 
 typedef struct oa_outputs {
@@ -227,6 +245,11 @@ void oa_default_settings(oa_settings* s);
 oa_status oa_solve(const oa_settings* s, oa_outputs* out);
 /* ≙ main of the reference CLI: same flags, exit status 0 / 1. */
 int oa_cli_main(int argc, char** argv);
+
+/* SNP range [*first, *first + *count) of shard `shard` of `shards` over m
+ * SNPs: the reference's MPI split (src/AIOwrapper.cpp:95-117): m / shards
+ * each, the last shard also the remainder; no split when m < shards. */
+oa_status oa_shard_range(int32_t m, int32_t shard, int32_t shards, int32_t* first, int32_t* count);
 
 /* |t| -> P exactly as the reference (long double, src/Algorithm.cpp:1159-1167). */
 long double oa_pvalue(float t);

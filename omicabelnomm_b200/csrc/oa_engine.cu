@@ -224,6 +224,13 @@ struct oa_engine {
     // tuning: requested (0 = automatic) and in effect
     oa_tuning req{};
     int variant = 1, raster = 1, lean_spb = 0;
+    // work items of the lean kernel's set pass (per trait block) and its launch plan
+    DBuf<int> item_start, set_item_off, pass_off;
+    std::vector<int> h_set_item_off;
+    struct LeanPlan {
+        int spb = 0, nbuf = 0, items_cap = 0, npass = 0;
+        size_t smem = 0;
+    } lp;
     long long tune_gen = 0;
     DBuf<float> B2;
     DBuf<__nv_bfloat16> B2hi, B2lo;
@@ -267,6 +274,10 @@ struct oa_engine {
     // dense outputs
     bool dense_on = false;
     DBuf<float> d_beta, d_se, d_t, d_r2, d_sig;
+    // row subset of device SNP blocks: columns of x_ld floats, rows xrows[0..n)
+    DBuf<int> xrows;
+    long long x_ld = 0;
+    bool subset = false;
     long long dense_ld = 0;
     int last_mb = 0;
     // host results (pinned staging for the device-to-host copy)
@@ -280,6 +291,48 @@ struct oa_engine {
 };
 
 namespace {
+
+// Every device buffer of an engine (release, footprint).
+template <class F>
+void for_each_buf(oa_engine* e, F&& f) {
+    f(e->Q64); f(e->Rinv); f(e->Qr);
+    f(e->Yraw); f(e->Yt); f(e->Yhi); f(e->Ylo);
+    f(e->tsums); f(e->rss0); f(e->b0); f(e->W); f(e->zQ);
+    f(e->tcounts); f(e->pat); f(e->zset); f(e->nobs); f(e->set_off); f(e->set_rows); f(e->set_rep);
+    f(e->set_kind); f(e->set_slot); f(e->tperm); f(e->tinv);
+    f(e->a_r2); f(e->inv_ncorr); f(e->vf); f(e->thash); f(e->sst); f(e->qrows); f(e->pat_bad);
+    f(e->B2); f(e->B2hi); f(e->B2lo);
+    f(e->Xstage[0]); f(e->Xstage[1]); f(e->Xhi); f(e->Xlo);
+    f(e->mean); f(e->varx); f(e->aobs); f(e->afull); f(e->zA); f(e->zD); f(e->D); f(e->Dset); f(e->C2T);
+    f(e->has_nan); f(e->sinv); f(e->sfinv); f(e->sing);
+    f(e->rec); f(e->rec2); f(e->cov); f(e->cov2); f(e->counters); f(e->keys); f(e->keys2); f(e->perm);
+    f(e->perm2); f(e->cub_tmp);
+    f(e->d_beta); f(e->d_se); f(e->d_t); f(e->d_r2); f(e->d_sig); f(e->xrows);
+    f(e->item_start); f(e->set_item_off); f(e->pass_off);
+}
+
+// Columns [c0, c0 + ncol) of a strided block gathered to the engine's rows.
+static __global__ void k_gather_rows(const float* __restrict__ in, long long ld, const int* __restrict__ rows, int n,
+                                     float* __restrict__ out) {
+    const int c = blockIdx.y;
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j < n) out[(size_t)c * n + j] = __ldg(in + (size_t)c * ld + __ldg(rows + j));
+}
+
+// Device input of one chunk: the block itself, or its row-subset gather.
+template <int R>
+oa_status chunk_input(oa_engine* e, const float* xr, int c0, int mbc, const float** X) {
+    if (!e->subset) {
+        *X = xr + (size_t)c0 * R * e->n;
+        return OA_OK;
+    }
+    dim3 grid((unsigned)((e->n + 255) / 256), (unsigned)(mbc * R));
+    k_gather_rows<<<grid, 256, 0, e->st>>>(xr + (size_t)c0 * R * e->x_ld, e->x_ld, e->xrows.p, e->n, e->Xstage[0].p);
+    ++e->launches;
+    OA_CU(cudaGetLastError());
+    *X = e->Xstage[0].p;
+    return OA_OK;
+}
 
 oa_status set_traits_impl(oa_engine* e, const float* y, int32_t t, bool device_ptr) {
     if (!e->have_cov) {
@@ -400,6 +453,23 @@ oa_status set_traits_impl(oa_engine* e, const float* y, int32_t t, bool device_p
     OA_CU(cudaGetLastError());
     e->c2 = l * (1 + e->nsets);
     e->b2_ready = false;
+    {   // work items of at most LEAN_ITEM_ROWS rows of one set, tiling the flattened row lists
+        std::vector<int> istart;
+        e->h_set_item_off.assign(e->nsets + 1, 0);
+        for (int s2 = 0; s2 < e->nsets; ++s2) {
+            e->h_set_item_off[s2] = (int)istart.size();
+            for (int r0 = off[s2]; r0 < off[s2 + 1]; r0 += LEAN_ITEM_ROWS) istart.push_back(r0);
+        }
+        e->h_set_item_off[e->nsets] = (int)istart.size();
+        istart.push_back(off[e->nsets]);
+        OA_CHECK(e->item_start.ensure(istart.size()));
+        OA_CHECK(e->set_item_off.ensure(e->h_set_item_off.size()));
+        OA_CU(cudaMemcpyAsync(e->item_start.p, istart.data(), sizeof(int) * istart.size(), cudaMemcpyHostToDevice,
+                              e->st));
+        OA_CU(cudaMemcpyAsync(e->set_item_off.p, e->h_set_item_off.data(), sizeof(int) * e->h_set_item_off.size(),
+                              cudaMemcpyHostToDevice, e->st));
+        e->lp = oa_engine::LeanPlan{};
+    }
     OA_CHECK(e->Yt.ensure((size_t)t * e->n_pad));
     if (e->cfg.precision == OA_MIXED_BF16X3) {
         OA_CHECK(e->Yhi.ensure((size_t)t * e->n_pad));
@@ -428,6 +498,8 @@ oa_status set_traits_impl(oa_engine* e, const float* y, int32_t t, bool device_p
 // [Q | Q o m_1 | ... | Q o m_S] (cost c2 / t of the main GEMM); with many,
 // row gathers inside k_snp_stats.  Builds the pre-GEMM's column matrix
 // the first time a trait block needs it.
+oa_status lean_plan(oa_engine* e);
+
 oa_status prepare_tuning(oa_engine* e) {
     const int t = e->t, l = e->l, n = e->n;
     e->chunk = std::min(e->cfg.max_snps, e->req.chunk_snps > 0 ? e->req.chunk_snps : 16384 / e->r);
@@ -455,6 +527,7 @@ oa_status prepare_tuning(oa_engine* e) {
         OA_CU(cudaGetLastError());
         e->b2_ready = true;
     }
+    if (e->use_pre) OA_CHECK(lean_plan(e));
     return OA_OK;
 }
 
@@ -546,8 +619,11 @@ int lean_group(const oa_engine* e) {
     return s;
 }
 
-template <int R>
-oa_status stats_pre(oa_engine* e, const float* X, int mbc) {
+// Launch plan of k_snp_lean for the current trait block and tuning: SNPs per
+// group, column buffers, shared memory, and passes over the row sets whose
+// work items fit in shared memory.  Host-only (runs before any capture).
+oa_status lean_plan(oa_engine* e) {
+    const int R = e->r;
     const size_t limit = 227 * 1024 - 1024;
     const size_t colb = (size_t)R * e->n_pad * 4;
     int spb = lean_group(e);
@@ -555,24 +631,53 @@ oa_status stats_pre(oa_engine* e, const float* X, int mbc) {
     while (spb > 1 && nbuf * spb * colb > 200 * 1024) spb /= 2;
     if (nbuf * spb * colb > 200 * 1024) nbuf = 1;
     const size_t base = lean_smem_bytes(R, e->n_pad, spb, nbuf, 0);
-    const size_t per_set = (size_t)spb * R * R * 4;
-    if (base + per_set > limit) {
-        set_err("n = %d is too large for one SNP column in shared memory", e->n);
+    const size_t per_item = (size_t)spb * R * R * 4;
+    int max_items = 1;
+    for (int s2 = 0; s2 < e->nsets; ++s2)
+        max_items = std::max(max_items, e->h_set_item_off[s2 + 1] - e->h_set_item_off[s2]);
+    if (base + per_item * max_items > limit) {
+        set_err("n = %d is too large for the column-statistics kernel's shared memory", e->n);
         return OA_ERR_UNSUPPORTED;
     }
-    const int sets_cap = (int)std::max<size_t>(1, std::min<size_t>(std::max(e->nsets, 1), (limit - base) / per_set));
-    const size_t smem = lean_smem_bytes(R, e->n_pad, spb, nbuf, sets_cap);
+    const int total_items = std::max(1, e->h_set_item_off.empty() ? 1 : e->h_set_item_off.back());
+    const int cap = (int)std::min<size_t>((size_t)total_items, (limit - base) / per_item);
+    if (e->lp.spb == spb && e->lp.nbuf == nbuf && e->lp.items_cap == cap) return OA_OK;
+    std::vector<int> passes{0};
+    for (int s0 = 0; s0 < e->nsets;) {
+        int s1 = s0 + 1;
+        while (s1 < e->nsets && e->h_set_item_off[s1 + 1] - e->h_set_item_off[s0] <= cap) ++s1;
+        passes.push_back(s1);
+        s0 = s1;
+    }
+    OA_CHECK(e->pass_off.ensure(passes.size()));
+    OA_CU(cudaMemcpyAsync(e->pass_off.p, passes.data(), sizeof(int) * passes.size(), cudaMemcpyHostToDevice, e->st));
+    OA_CU(cudaStreamSynchronize(e->st));
+    e->lp.spb = spb;
+    e->lp.nbuf = nbuf;
+    e->lp.items_cap = cap;
+    e->lp.npass = e->nsets > 0 ? (int)passes.size() - 1 : 0;
+    e->lp.smem = lean_smem_bytes(R, e->n_pad, spb, nbuf, cap);
+    return OA_OK;
+}
+
+template <int R>
+oa_status stats_pre(oa_engine* e, const float* X, int mbc) {
+    const int spb = e->lp.spb;
+    const size_t smem = e->lp.smem;
     LeanArgs A{};
     A.X = X;
     A.ldx = (size_t)e->n;
     A.n = e->n;
     A.n_pad = e->n_pad;
     A.mb = mbc;
-    A.nbuf = nbuf;
+    A.nbuf = e->lp.nbuf;
     A.nsets = e->nsets;
-    A.sets_cap = sets_cap;
-    A.set_off = e->set_off.p;
     A.rows = e->set_rows.p;
+    A.item_start = e->item_start.p;
+    A.set_item_off = e->set_item_off.p;
+    A.pass_off = e->pass_off.p;
+    A.npass = e->lp.npass;
+    A.items_cap = e->lp.items_cap;
     A.mean = e->mean.p;
     A.has_nan = e->has_nan.p;
     A.D = e->D.p;
@@ -583,7 +688,7 @@ oa_status stats_pre(oa_engine* e, const float* X, int mbc) {
     A.Xlo = e->Xlo.p;
     A.err = reinterpret_cast<int*>(e->counters.p + 3);
     const int groups = (mbc + spb - 1) / spb;
-    const int per_sm = (int)std::max<size_t>(1, std::min<size_t>(4, (228 * 1024) / (smem + 1024)));
+    const int per_sm = std::max(1, oa_lean_ctas_per_sm(R, spb, smem));
     const int grid = std::min(groups, e->sm_count * per_sm);
     OA_CU(oa_launch_snp_lean(R, spb, A, grid, smem, e->st));
     ++e->launches;
@@ -824,7 +929,8 @@ oa_status enqueue_scan(oa_engine* e, const float* xr, int mb) {
     }
     for (int c = 0; c < nch; ++c) {
         const int c0 = c * e->chunk, mbc = std::min(e->chunk, mb - c0);
-        const float* X = xr + (size_t)c0 * e->r * e->n;
+        const float* X = nullptr;
+        OA_CHECK(chunk_input<R>(e, xr, c0, mbc, &X));
         OA_CU(cudaMemsetAsync(e->has_nan.p, 0, sizeof(int), e->st));
         OA_CU(cudaEventRecordWithFlags(e->sev0[c], e->st, cudaEventRecordExternal));
         OA_CHECK(stats_dispatch<R>(e, X, mbc));
@@ -944,6 +1050,13 @@ oa_status run_snps_impl(oa_engine* e, const float* xr, int32_t mb, bool host_inp
     e->last_mb = mb;
     const size_t colbytes = sizeof(float) * (size_t)e->n * e->r;
     const int nch = (mb + e->chunk - 1) / e->chunk;
+    if (e->subset) {
+        if (host_input) {
+            set_err("a row subset applies to device SNP blocks only (oa_run_snps_device)");
+            return OA_ERR_STATE;
+        }
+        OA_CHECK(e->Xstage[0].ensure((size_t)e->chunk * e->r * e->n));
+    }
     if (host_input) {
         for (int b = 0; b < 2; ++b) OA_CHECK(e->Xstage[b].ensure((size_t)e->chunk * e->r * e->n));
         // copy of chunk c+1 overlaps the compute of chunk c
@@ -971,7 +1084,9 @@ oa_status run_snps_impl(oa_engine* e, const float* xr, int32_t mb, bool host_inp
         if (!done)
             for (int c = 0; c < nch; ++c) {
                 const int c0 = c * e->chunk, mbc = std::min(e->chunk, mb - c0);
-                OA_CHECK(run_chunk<R>(e, xr + (size_t)c0 * e->r * e->n, mbc, c0));
+                const float* X = nullptr;
+                OA_CHECK(chunk_input<R>(e, xr, c0, mbc, &X));
+                OA_CHECK(run_chunk<R>(e, X, mbc, c0));
             }
     }
     unsigned long long cnt[3];
@@ -1270,30 +1385,7 @@ oa_status oa_engine_destroy(oa_engine* e) {
     cudaSetDevice(e->cfg.device);
     cudaStreamSynchronize(e->st);
     cudaStreamSynchronize(e->cp);
-    for (auto* b : {&e->Q64, &e->Rinv, &e->tsums, &e->rss0, &e->b0, &e->W, &e->zQ, &e->sinv, &e->sfinv}) b->release();
-    for (auto* b : {&e->Qr, &e->Yraw, &e->Yt, &e->sst, &e->mean, &e->varx, &e->aobs, &e->afull, &e->zA, &e->zD,
-                    &e->cov, &e->cov2, &e->d_beta, &e->d_se, &e->d_t, &e->d_r2, &e->d_sig, &e->Xstage[0],
-                    &e->Xstage[1]})
-        b->release();
-    for (auto* b : {&e->tcounts, &e->pat, &e->zset, &e->nobs, &e->set_off, &e->set_rows, &e->set_rep, &e->set_kind,
-                    &e->set_slot, &e->has_nan, &e->perm, &e->perm2, &e->tperm, &e->tinv})
-        b->release();
-    for (auto* b : {&e->a_r2, &e->inv_ncorr, &e->vf, &e->qrows, &e->B2, &e->D, &e->Dset, &e->C2T}) b->release();
-    e->B2hi.release();
-    e->B2lo.release();
-    e->Yhi.release();
-    e->Ylo.release();
-    e->Xhi.release();
-    e->Xlo.release();
-    e->thash.release();
-    e->counters.release();
-    e->keys.release();
-    e->keys2.release();
-    e->pat_bad.release();
-    e->sing.release();
-    e->rec.release();
-    e->rec2.release();
-    e->cub_tmp.release();
+    for_each_buf(e, [](auto& b) { b.release(); });
     if (e->h_rec) cudaFreeHost(e->h_rec);
     if (e->h_cov) cudaFreeHost(e->h_cov);
     for (int b = 0; b < 2; ++b) {
@@ -1426,6 +1518,44 @@ oa_status oa_autotune(oa_engine* e, const float* xr_dev, int32_t mb, oa_tuning* 
     }
     OA_CU(cudaSetDevice(e->cfg.device));
     return autotune_impl(e, xr_dev, mb, best);
+}
+
+oa_status oa_set_snp_rows(oa_engine* e, const int32_t* rows, int32_t n_rows, int64_t ld) {
+    clear_stale_error(__func__);
+    if (!e) {
+        set_err("null engine");
+        return OA_ERR_ARG;
+    }
+    OA_CU(cudaSetDevice(e->cfg.device));
+    drop_graph(e);
+    ++e->tune_gen;
+    if (!rows) {
+        e->subset = false;
+        e->x_ld = 0;
+        return OA_OK;
+    }
+    if (n_rows != e->n || ld < n_rows) {
+        set_err("row subset of %d rows (engine n = %d) from columns of %lld", n_rows, e->n, (long long)ld);
+        return OA_ERR_ARG;
+    }
+    for (int j = 0; j < n_rows; ++j)
+        if (rows[j] < 0 || rows[j] >= ld || (j > 0 && rows[j] <= rows[j - 1])) {
+            set_err("row subset: rows must be ascending and within [0, %lld)", (long long)ld);
+            return OA_ERR_ARG;
+        }
+    OA_CHECK(e->xrows.ensure(n_rows));
+    OA_CU(cudaMemcpyAsync(e->xrows.p, rows, sizeof(int32_t) * n_rows, cudaMemcpyHostToDevice, e->st));
+    OA_CU(cudaStreamSynchronize(e->st));
+    e->x_ld = ld;
+    e->subset = true;
+    return OA_OK;
+}
+
+int64_t oa_device_bytes(const oa_engine* e) {
+    if (!e) return 0;
+    int64_t total = 0;
+    for_each_buf(const_cast<oa_engine*>(e), [&](auto& b) { total += (int64_t)(b.n * sizeof(*b.p)); });
+    return total;
 }
 
 oa_status oa_enable_dense(oa_engine* e, int32_t on) {

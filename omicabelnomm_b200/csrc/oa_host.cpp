@@ -244,6 +244,7 @@ struct Writer {
     long double min_p_disp = 0;
     float min_r2_disp = 0;
     int l = 0, r = 0, p = 0, real_n = 0, mb_ref = 500;
+    int name_base = 0;   // first SNP of this shard in the genotype file (names only; indices are shard-local)
     const Fvi* fy = nullptr;
     const Fvi* fl = nullptr;
     const Fvi* fr = nullptr;
@@ -296,7 +297,7 @@ struct Writer {
                 if ((P <= min_p_disp && r2 >= min_r2_disp) || store_all) {
                     std::string aname = " ";
                     if (h < l) aname = fl->var_name(h) + ":";
-                    aname += fr->var_name((size_t)ar_offset_snps * r + ar_idx);
+                    aname += fr->var_name((size_t)(name_base + ar_offset_snps) * r + ar_idx);
                     const int len = snprintf(line, sizeof line, "%s\t%s\t%u\t%.2f\t%.7f\t%.4f\t%.7f\t%.7f\t%.7Le\n",
                                              fy->var_name(ytr).c_str(), aname.c_str(), (unsigned)nused,
                                              (double)npct, (double)B, (double)r2, (double)SE, (double)T, P);
@@ -328,6 +329,21 @@ extern "C" {
 
 long double oa_pvalue(float t) { return pvalue_ld(t); }
 
+oa_status oa_shard_range(int32_t m, int32_t shard, int32_t shards, int32_t* first, int32_t* count) {
+    if (!first || !count || m < 0 || shards < 1 || shard < 0 || shard >= shards) {
+        herr("shard %d of %d", shard, shards);
+        return OA_ERR_ARG;
+    }
+    *first = 0;
+    *count = m;
+    if (shards > 1 && m >= shards) {
+        const int m_sh = m / shards;
+        *first = m_sh * shard;
+        *count = shard == shards - 1 ? m_sh + (m - shards * m_sh) : m_sh;
+    }
+    return OA_OK;
+}
+
 float oa_t_threshold(float p) {
     // src/Utility.cpp:244-250: erf_inv(1 - p) * sqrt(2), evaluated in long double
     return (float)(erf_inv_ld((long double)(1.0 - (double)p)) * sqrt(2.0));
@@ -342,6 +358,8 @@ void oa_default_settings(oa_settings* s) {
     s->min_p_disp = 0.05f;
     s->precision = OA_PLAIN_FP32;
     s->device = 0;
+    s->shard = 0;
+    s->shards = 1;
 }
 
 oa_status oa_solve(const oa_settings* S, oa_outputs* out) {
@@ -376,7 +394,17 @@ oa_status oa_solve(const oa_settings* S, oa_outputs* out) {
              fxr.c_str(), FR.nvar, r);
         return OA_ERR_IO;
     }
-    const int m = (int)(FR.nvar / r), t = (int)FY.nvar, l = (int)FL.nvar, p = l + r;
+    const int m_file = (int)(FR.nvar / r), t = (int)FY.nvar, l = (int)FL.nvar, p = l + r;
+    // SNP shard of this process (the reference's MPI split, src/AIOwrapper.cpp:95-117)
+    const int shards = std::max(1, S->shards);
+    if (S->shard < 0 || S->shard >= shards) {
+        herr("shard %d of %d", S->shard, shards);
+        return OA_ERR_ARG;
+    }
+    int first = 0, m = m_file;
+    oa_shard_range(m_file, S->shard, shards, &first, &m);
+    const std::string fout_eff =
+        (shards > 1 && m_file >= shards) ? fout + "_mpi" + std::to_string(S->shard + 1) + "_" : fout;
     if (l < 1 || l > OA_MAX_L) {
         herr("%d covariates: this build supports 1..%d", l, OA_MAX_L);
         return OA_ERR_UNSUPPORTED;
@@ -453,17 +481,18 @@ oa_status oa_solve(const oa_settings* S, oa_outputs* out) {
     W.fy = &FY;
     W.fl = &FL;
     W.fr = &FR;
-    W.dis = fopen((fout + "_dis.txt").c_str(), "wb");
+    W.name_base = first;
+    W.dis = fopen((fout_eff + "_dis.txt").c_str(), "wb");
     if (!W.dis) {
-        herr("Error Creating File %s_dis.txt", fout.c_str());
+        herr("Error Creating File %s_dis.txt", fout_eff.c_str());
         return OA_ERR_IO;
     }
     fputs("Phe\tSNP\tn\tnPct\tB\tR2\tSE\tT\tP\n", W.dis);
     if (S->store_bin) {
         // _sto.ibin (src/AIOwrapper.cpp:679-733)
-        FILE* fi = fopen((fout + "_sto.ibin").c_str(), "wb");
+        FILE* fi = fopen((fout_eff + "_sto.ibin").c_str(), "wb");
         if (!fi) {
-            herr("Error Creating File: %s_sto.ibin", fout.c_str());
+            herr("Error Creating File: %s_sto.ibin", fout_eff.c_str());
             fclose(W.dis);
             return OA_ERR_IO;
         }
@@ -472,12 +501,12 @@ oa_status oa_solve(const oa_settings* S, oa_outputs* out) {
         const uint8_t flags[2] = {(uint8_t)(S->disp_cov ? 1 : 0), (uint8_t)(S->store_all ? 1 : 0)};
         fwrite(flags, 1, 2, fi);
         fwrite(FL.raw((size_t)FL.nobs + 1), 1, (size_t)FL.namelength * (l - 1), fi);
-        fwrite(FR.raw(FR.nobs), 1, (size_t)FR.namelength * r * m, fi);
+        fwrite(FR.raw((size_t)FR.nobs + (size_t)first * r), 1, (size_t)FR.namelength * r * m, fi);
         fwrite(FY.raw(FY.nobs), 1, (size_t)FY.namelength * t, fi);
         fclose(fi);
-        W.dbin = fopen((fout + "_sto.dbin").c_str(), "wb");
+        W.dbin = fopen((fout_eff + "_sto.dbin").c_str(), "wb");
         if (!W.dbin) {
-            herr("Error Creating File %s_sto.dbin", fout.c_str());
+            herr("Error Creating File %s_sto.dbin", fout_eff.c_str());
             fclose(W.dis);
             return OA_ERR_IO;
         }
@@ -562,7 +591,7 @@ oa_status oa_solve(const oa_settings* S, oa_outputs* out) {
         if (st != OA_OK) break;
         auto read_call = [&](int c, int b) {
             const int s0 = c * call_snps, cnt = std::min(call_snps, m - s0);
-            return read_columns(fr, fileN, (size_t)s0 * r, (size_t)cnt * r, runs, n, pin[b], scratch[b]);
+            return read_columns(fr, fileN, (size_t)(first + s0) * r, (size_t)cnt * r, runs, n, pin[b], scratch[b]);
         };
         std::future<bool> next = std::async(std::launch::async, read_call, 0, 0);
         for (int c = 0; c < ncalls; ++c) {
@@ -650,7 +679,7 @@ int oa_cli_main(int argc, char** argv) {
     oa_default_settings(&S);
     S.verbose = 1;
     std::string fy, fr, fl, fo, fx;
-    bool phe = false, snp = false, cov = false, bout = false;
+    bool phe = false, snp = false, cov = false, bout = false, shard_set = false, device_set = false;
     static struct option opts[] = {{"phe", required_argument, 0, 'p'},
                                    {"geno", required_argument, 0, 'g'},
                                    {"cov", required_argument, 0, 'c'},
@@ -678,6 +707,7 @@ int oa_cli_main(int argc, char** argv) {
                                    {"precision", required_argument, 0, 1000},
                                    {"device", required_argument, 0, 1001},
                                    {"quirk-r2", no_argument, 0, 1002},
+                                   {"shard", required_argument, 0, 1003},
                                    {0, 0, 0, 0}};
     optind = 1;
     int c, idx = 0;
@@ -707,8 +737,16 @@ int oa_cli_main(int argc, char** argv) {
                 else if (!strcmp(optarg, "mixed")) S.precision = OA_MIXED_BF16X3;
                 else { printf("--precision must be plain or mixed\n"); return 1; }
                 break;
-            case 1001: S.device = atoi(optarg); break;
+            case 1001: S.device = atoi(optarg); device_set = true; break;
             case 1002: S.quirk_r2 = 1; break;
+            case 1003:
+                if (sscanf(optarg, "%d/%d", &S.shard, &S.shards) != 2 || S.shards < 1 || S.shard < 0 ||
+                    S.shard >= S.shards) {
+                    printf("--shard must be k/N with 0 <= k < N\n");
+                    return 1;
+                }
+                shard_set = true;
+                break;
             case '?': break;
             default: return 1;
         }
@@ -716,6 +754,24 @@ int oa_cli_main(int argc, char** argv) {
     if (!bout || !phe || !cov || !snp) {
         printf("Missing arguments! p:%d g:%d c:%d o:%d\n", phe, snp, cov, bout);
         return 1;
+    }
+    // launched as one process per GPU (mpirun or torchrun): shard and device from the launcher
+    if (!shard_set) {
+        const char* rk = getenv("OMPI_COMM_WORLD_RANK");
+        const char* sz = getenv("OMPI_COMM_WORLD_SIZE");
+        if (!rk || !sz) {
+            rk = getenv("RANK");
+            sz = getenv("WORLD_SIZE");
+        }
+        if (rk && sz && atoi(sz) > 1) {
+            S.shard = atoi(rk);
+            S.shards = atoi(sz);
+        }
+    }
+    if (!device_set) {
+        const char* lr = getenv("OMPI_COMM_WORLD_LOCAL_RANK");
+        if (!lr) lr = getenv("LOCAL_RANK");
+        if (lr) S.device = atoi(lr);
     }
     S.fname_y = fy.c_str();
     S.fname_xr = fr.c_str();

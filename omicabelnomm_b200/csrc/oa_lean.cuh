@@ -23,9 +23,12 @@ struct LeanArgs {
     size_t ldx;
     int n, n_pad, mb, nbuf;
     int nsets;
-    int sets_cap;         // row sets whose sums fit in shared memory at once
-    const int* set_off;
-    const int* rows;
+    const int* rows;          // flattened row lists of the row sets
+    const int* item_start;    // work items: rows [item_start[i], item_start[i+1]) of one set
+    const int* set_item_off;  // items of set s: [set_item_off[s], set_item_off[s+1])
+    const int* pass_off;      // passes over sets [pass_off[p], pass_off[p+1]) whose items fit in shared memory
+    int npass;
+    int items_cap;
     float* mean;          // [mb*r] imputation means (0 if the column had no NaN)
     int* has_nan;
     float* D;             // [mb][r*r] X'X over all rows
@@ -36,17 +39,22 @@ struct LeanArgs {
     int* err;
 };
 
+constexpr int LEAN_THREADS = 512;
+constexpr int LEAN_WARPS = LEAN_THREADS / 32;
+constexpr int LEAN_ITEM_ROWS = 256;     // rows per work item of the set pass
+
 // Shared memory of k_snp_lean: nbuf column buffers (stride n_pad floats, the
-// tail [n, n_pad) kept zero) | per-set sums | reduction scratch.
-__host__ __device__ inline size_t lean_smem_bytes(int R, int n_pad, int spb, int nbuf, int sets_cap) {
+// tail [n, n_pad) kept zero) | per-item partial sums | reduction scratch.
+__host__ __device__ inline size_t lean_smem_bytes(int R, int n_pad, int spb, int nbuf, int items_cap) {
     const int NQ = 2 * spb * R + spb * R * R;
-    return (size_t)nbuf * spb * R * n_pad * 4 + (size_t)sets_cap * spb * R * R * 4 + (size_t)8 * NQ * 8 + 64;
+    return (size_t)nbuf * spb * R * n_pad * 4 + (size_t)items_cap * spb * R * R * 4 +
+           (size_t)(LEAN_WARPS + 1) * NQ * 8 + 64;
 }
 
 // Block-wide sum of NV floats per thread: FP32 within a warp, FP64 across
-// warps; the result is valid in v[] on every thread.
+// warps (warp 0, fixed order); the result is valid in out[] on every thread.
 template <int NV>
-__device__ __forceinline__ void block_sum_fd(float (&v)[NV], double (&out)[NV], double* red /* [8][NV] */) {
+__device__ __forceinline__ void block_sum_fd(float (&v)[NV], double (&out)[NV], double* red /* [warps + 1][NV] */) {
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
 #pragma unroll
     for (int q = 0; q < NV; ++q) v[q] = warp_sumf(v[q]);
@@ -54,40 +62,61 @@ __device__ __forceinline__ void block_sum_fd(float (&v)[NV], double (&out)[NV], 
 #pragma unroll
         for (int q = 0; q < NV; ++q) red[w * NV + q] = (double)v[q];
     __syncthreads();
+    double* bc = red + LEAN_WARPS * NV;
+    if (w == 0) {
 #pragma unroll
-    for (int q = 0; q < NV; ++q) {
-        double s = 0.0;
-#pragma unroll
-        for (int ww = 0; ww < OA_NTHREADS / 32; ++ww) s += red[ww * NV + q];
-        out[q] = s;
+        for (int q = 0; q < NV; ++q) {
+            const double s = warp_sum(lane < LEAN_WARPS ? red[lane * NV + q] : 0.0);
+            if (lane == 0) bc[q] = s;
+        }
     }
     __syncthreads();
+#pragma unroll
+    for (int q = 0; q < NV; ++q) out[q] = bc[q];
+}
+
+// BF16 hi/lo of 8 floats (x = hi + lo to ~2^-17 relative), packed
+__device__ __forceinline__ void split8(const float4 p0, const float4 p1, uint4& hi, uint4& lo) {
+    const float e[8] = {p0.x, p0.y, p0.z, p0.w, p1.x, p1.y, p1.z, p1.w};
+    uint32_t h[4], o[4];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+        const __nv_bfloat162 hb = __floats2bfloat162_rn(e[2 * u], e[2 * u + 1]);
+        const float2 hf = __bfloat1622float2(hb);
+        const __nv_bfloat162 lb = __floats2bfloat162_rn(e[2 * u] - hf.x, e[2 * u + 1] - hf.y);
+        h[u] = *reinterpret_cast<const uint32_t*>(&hb);
+        o[u] = *reinterpret_cast<const uint32_t*>(&lb);
+    }
+    hi = make_uint4(h[0], h[1], h[2], h[3]);
+    lo = make_uint4(o[0], o[1], o[2], o[3]);
 }
 
 // One CTA handles SPB SNPs (SPB*R columns) per group; a persistent loop over
 // groups with the next group's columns streaming into shared memory (TMA
 // bulk copies) while this one is processed:
-//   pass 1  column sums, NaN counts and X'X from float4 reads of the staged
-//           columns (one block reduction); a column with NaN is mean-imputed
-//           in place and X'X recomputed (src/Utility.cpp:302-326)
+//   pass 1  column sums and X'X from float4 reads of the staged columns (one
+//           block reduction); NaN propagates, so a column whose sum is NaN
+//           is counted, mean-imputed in place and X'X recomputed
+//           (src/Utility.cpp:302-326) - rare, dosage files seldom hold NaN
 //   pass 2  BF16 hi/lo split of the columns (tensor-core form only)
-//   pass 3  X'X over each row set: the flattened row lists split evenly
-//           over the warps, lanes accumulate while the set is unchanged and
-//           flush into per-set sums in shared memory at a set boundary
+//   pass 3  X'X over each row set: work items of at most 256 rows of one set
+//           (fixed on the host per trait block) go round-robin to the warps;
+//           a warp's item sum (row indices prefetched, shuffle reduction)
+//           lands in its own shared-memory slot, and a set's sum adds its
+//           items in order.  No atomics: the sums are bit-reproducible.
 template <int R, int SPB, bool BULK>
-__global__ void __launch_bounds__(OA_NTHREADS)
+__global__ void __launch_bounds__(LEAN_THREADS)
 k_snp_lean(LeanArgs A) {
     extern __shared__ __align__(128) unsigned char smem_raw[];
     constexpr int NC = SPB * R;                 // columns per group
     constexpr int K2 = SPB * R * R;             // X'X entries per group
-    constexpr int NQ = 2 * NC + K2;
-    constexpr int NWARP = OA_NTHREADS / 32;
+    constexpr int NWARP = LEAN_WARPS;
     const int n = A.n, nS = A.n_pad;
     const size_t buf_floats = (size_t)NC * nS;
     float* bufs = reinterpret_cast<float*>(smem_raw);                                   // [nbuf][NC][nS]
-    float* setacc = bufs + (size_t)A.nbuf * buf_floats;                                 // [sets_cap][K2]
+    float* part = bufs + (size_t)A.nbuf * buf_floats;                                   // [items_cap][K2]
     double* red = reinterpret_cast<double*>(
-        (reinterpret_cast<uintptr_t>(setacc + (size_t)A.sets_cap * K2) + 7) & ~(uintptr_t)7);   // [8][NQ]
+        (reinterpret_cast<uintptr_t>(part + (size_t)A.items_cap * K2) + 7) & ~(uintptr_t)7);   // [NWARP + 1][NQ]
     __shared__ __align__(8) uint64_t mbar[2];
     __shared__ int stop;
     const int ngroups = (A.mb + SPB - 1) / SPB;
@@ -157,29 +186,20 @@ k_snp_lean(LeanArgs A) {
             }
             __syncthreads();
         }
-        // columns past the block's end read as zero
         const float4* x4 = reinterpret_cast<const float4*>(xs);
         const int nS4 = nS / 4;
 
-        // ---- pass 1: sums, NaN counts, X'X
-        float acc[NQ];
-        double tot[NQ];
+        // ---- pass 1: sums and X'X (NaN propagates)
+        float acc[NC + K2];
+        double tot[NC + K2];
 #pragma unroll
-        for (int u = 0; u < NQ; ++u) acc[u] = 0.f;
+        for (int u = 0; u < NC + K2; ++u) acc[u] = 0.f;
         for (int k4 = threadIdx.x; k4 < nS4; k4 += blockDim.x) {
             float4 v[NC];
 #pragma unroll
             for (int c = 0; c < NC; ++c) v[c] = c < ncol ? x4[(size_t)c * nS4 + k4] : make_float4(0.f, 0.f, 0.f, 0.f);
 #pragma unroll
-            for (int c = 0; c < NC; ++c) {
-                const float e[4] = {v[c].x, v[c].y, v[c].z, v[c].w};
-#pragma unroll
-                for (int u = 0; u < 4; ++u) {
-                    const bool nan = isnan(e[u]);
-                    acc[c] += nan ? 0.f : e[u];
-                    acc[NC + c] += nan ? 1.f : 0.f;
-                }
-            }
+            for (int c = 0; c < NC; ++c) acc[c] += (v[c].x + v[c].y) + (v[c].z + v[c].w);
 #pragma unroll
             for (int s = 0; s < SPB; ++s)
 #pragma unroll
@@ -187,21 +207,47 @@ k_snp_lean(LeanArgs A) {
 #pragma unroll
                     for (int bb = 0; bb < R; ++bb) {
                         const float4 xa = v[s * R + a], xb = v[s * R + bb];
-                        acc[2 * NC + (s * R + a) * R + bb] += xa.x * xb.x + xa.y * xb.y + xa.z * xb.z + xa.w * xb.w;
+                        float& d = acc[NC + (s * R + a) * R + bb];
+                        d = fmaf(xa.x, xb.x, d);
+                        d = fmaf(xa.y, xb.y, d);
+                        d = fmaf(xa.z, xb.z, d);
+                        d = fmaf(xa.w, xb.w, d);
                     }
         }
-        block_sum_fd<NQ>(acc, tot, red);
+        block_sum_fd<NC + K2>(acc, tot, red);
         bool any_nan = false;
+        float cmean[NC];
+        bool cnan[NC];
 #pragma unroll
-        for (int c = 0; c < NC; ++c) any_nan |= (c < ncol) && tot[NC + c] > 0.0;
-        if (any_nan) {   // mean-impute in place, then X'X again (block-uniform branch)
+        for (int c = 0; c < NC; ++c) {
+            cnan[c] = (c < ncol) && isnan(tot[c]);
+            any_nan |= cnan[c];
+            cmean[c] = 0.f;
+        }
+        if (any_nan) {   // block-uniform: count, impute in place, recompute X'X
+            float cs[2 * NC];
+            double ct[2 * NC];
+#pragma unroll
+            for (int u = 0; u < 2 * NC; ++u) cs[u] = 0.f;
 #pragma unroll
             for (int c = 0; c < NC; ++c) {
-                if (c < ncol && tot[NC + c] > 0.0) {
-                    const float mv = (float)(tot[c] / ((double)n - tot[NC + c]));
+                if (cnan[c]) {
+                    const float* col = xs + (size_t)c * nS;
+                    for (int k = threadIdx.x; k < n; k += blockDim.x) {
+                        const float v = col[k];
+                        if (isnan(v)) cs[NC + c] += 1.f;
+                        else cs[c] += v;
+                    }
+                }
+            }
+            block_sum_fd<2 * NC>(cs, ct, red);
+#pragma unroll
+            for (int c = 0; c < NC; ++c) {
+                if (cnan[c]) {
+                    cmean[c] = (float)(ct[c] / ((double)n - ct[NC + c]));
                     float* col = xs + (size_t)c * nS;
                     for (int k = threadIdx.x; k < n; k += blockDim.x)
-                        if (isnan(col[k])) col[k] = mv;
+                        if (isnan(col[k])) col[k] = cmean[c];
                 }
             }
             __syncthreads();
@@ -221,25 +267,28 @@ k_snp_lean(LeanArgs A) {
 #pragma unroll
                         for (int bb = 0; bb < R; ++bb) {
                             const float4 xa = v[s * R + a], xb = v[s * R + bb];
-                            acc2[(s * R + a) * R + bb] += xa.x * xb.x + xa.y * xb.y + xa.z * xb.z + xa.w * xb.w;
+                            float& d = acc2[(s * R + a) * R + bb];
+                            d = fmaf(xa.x, xb.x, d);
+                            d = fmaf(xa.y, xb.y, d);
+                            d = fmaf(xa.z, xb.z, d);
+                            d = fmaf(xa.w, xb.w, d);
                         }
             }
             block_sum_fd<K2>(acc2, tot2, red);
 #pragma unroll
-            for (int u = 0; u < K2; ++u) tot[2 * NC + u] = tot2[u];
+            for (int u = 0; u < K2; ++u) tot[NC + u] = tot2[u];
         }
         if (threadIdx.x == 0) {
 #pragma unroll
             for (int c = 0; c < NC; ++c) {
                 if (c < ncol) {
-                    const bool has = tot[NC + c] > 0.0;
-                    A.mean[i0 * R + c] = has ? (float)(tot[c] / ((double)n - tot[NC + c])) : 0.0f;
-                    if (has) atomicOr(A.has_nan, 1);
+                    A.mean[i0 * R + c] = cmean[c];
+                    if (cnan[c]) atomicOr(A.has_nan, 1);
                 }
             }
 #pragma unroll
             for (int u = 0; u < K2; ++u)
-                if (u < nsnp * R * R) A.D[(size_t)i0 * R * R + u] = (float)tot[2 * NC + u];
+                if (u < nsnp * R * R) A.D[(size_t)i0 * R * R + u] = (float)tot[NC + u];
         }
 
         // ---- pass 2: BF16 hi/lo split, 8 elements per thread and step
@@ -250,76 +299,59 @@ k_snp_lean(LeanArgs A) {
                 uint4* hi = reinterpret_cast<uint4*>(A.Xhi + (size_t)(i0 * R + c) * A.n_pad);
                 uint4* lo = reinterpret_cast<uint4*>(A.Xlo + (size_t)(i0 * R + c) * A.n_pad);
                 for (int k8 = threadIdx.x; k8 < np8; k8 += blockDim.x) {
-                    const float4 p0 = col[2 * k8], p1 = col[2 * k8 + 1];
-                    const float e[8] = {p0.x, p0.y, p0.z, p0.w, p1.x, p1.y, p1.z, p1.w};
-                    uint32_t h[4], o[4];
-#pragma unroll
-                    for (int u = 0; u < 4; ++u) {
-                        const __nv_bfloat16 h0 = __float2bfloat16_rn(e[2 * u]), h1 = __float2bfloat16_rn(e[2 * u + 1]);
-                        const __nv_bfloat16 l0 = __float2bfloat16_rn(e[2 * u] - __bfloat162float(h0));
-                        const __nv_bfloat16 l1 = __float2bfloat16_rn(e[2 * u + 1] - __bfloat162float(h1));
-                        h[u] = (uint32_t)__bfloat16_as_ushort(h0) | ((uint32_t)__bfloat16_as_ushort(h1) << 16);
-                        o[u] = (uint32_t)__bfloat16_as_ushort(l0) | ((uint32_t)__bfloat16_as_ushort(l1) << 16);
-                    }
-                    hi[k8] = make_uint4(h[0], h[1], h[2], h[3]);
-                    lo[k8] = make_uint4(o[0], o[1], o[2], o[3]);
+                    uint4 h, o;
+                    split8(col[2 * k8], col[2 * k8 + 1], h, o);
+                    hi[k8] = h;
+                    lo[k8] = o;
                 }
             }
         }
 
-        // ---- pass 3: X'X over each row set
-        for (int s0 = 0; s0 < A.nsets; s0 += A.sets_cap) {
-            const int s1 = min(A.nsets, s0 + A.sets_cap);
-            for (int u = threadIdx.x; u < (s1 - s0) * K2; u += blockDim.x) setacc[u] = 0.f;
-            __syncthreads();
-            const int r0 = __ldg(A.set_off + s0), r1 = __ldg(A.set_off + s1);
-            const int per = (r1 - r0 + NWARP - 1) / NWARP;
-            const int w0 = r0 + w * per, w1 = min(r1, w0 + per);
-            if (w0 < w1) {
-                // set of row w0: last set s with set_off[s] <= w0
-                int lo_s = s0, hi_s = s1 - 1;
-                while (lo_s < hi_s) {
-                    const int mid = (lo_s + hi_s + 1) >> 1;
-                    if (__ldg(A.set_off + mid) <= w0) lo_s = mid;
-                    else hi_s = mid - 1;
-                }
-                int cur = lo_s;
-                int nextb = __ldg(A.set_off + cur + 1);
+        // ---- pass 3: X'X over each row set, by work items
+        for (int ps = 0; ps < A.npass; ++ps) {
+            const int s0 = __ldg(A.pass_off + ps), s1 = __ldg(A.pass_off + ps + 1);
+            const int it0 = __ldg(A.set_item_off + s0), it1 = __ldg(A.set_item_off + s1);
+            for (int item = it0 + w; item < it1; item += NWARP) {
+                const int ra = __ldg(A.item_start + item), rb = __ldg(A.item_start + item + 1);
                 float sacc[K2];
 #pragma unroll
                 for (int u = 0; u < K2; ++u) sacc[u] = 0.f;
-                for (int kk = w0 + lane; kk < w1; kk += 32) {
-                    if (kk >= nextb) {
+                constexpr int U = LEAN_ITEM_ROWS / 32;
+                int kid[U];
 #pragma unroll
-                        for (int u = 0; u < K2; ++u)
-                            if (sacc[u] != 0.f) atomicAdd(setacc + (cur - s0) * K2 + u, sacc[u]);
-#pragma unroll
-                        for (int u = 0; u < K2; ++u) sacc[u] = 0.f;
-                        do {
-                            ++cur;
-                            nextb = __ldg(A.set_off + cur + 1);
-                        } while (kk >= nextb);
-                    }
-                    const int k = __ldg(A.rows + kk);
-                    float x[NC];
-#pragma unroll
-                    for (int c = 0; c < NC; ++c) x[c] = xs[(size_t)c * nS + k];
-#pragma unroll
-                    for (int s = 0; s < SPB; ++s)
-#pragma unroll
-                        for (int a = 0; a < R; ++a)
-#pragma unroll
-                            for (int bb = 0; bb < R; ++bb) sacc[(s * R + a) * R + bb] += x[s * R + a] * x[s * R + bb];
+                for (int u = 0; u < U; ++u) {
+                    const int kk = ra + 32 * u + lane;
+                    kid[u] = kk < rb ? __ldg(A.rows + kk) : -1;
                 }
 #pragma unroll
-                for (int u = 0; u < K2; ++u)
-                    if (sacc[u] != 0.f) atomicAdd(setacc + (cur - s0) * K2 + u, sacc[u]);
+                for (int u = 0; u < U; ++u) {
+                    if (kid[u] >= 0) {
+                        float x[NC];
+#pragma unroll
+                        for (int c = 0; c < NC; ++c) x[c] = xs[(size_t)c * nS + kid[u]];
+#pragma unroll
+                        for (int s = 0; s < SPB; ++s)
+#pragma unroll
+                            for (int a = 0; a < R; ++a)
+#pragma unroll
+                                for (int bb = 0; bb < R; ++bb)
+                                    sacc[(s * R + a) * R + bb] = fmaf(x[s * R + a], x[s * R + bb], sacc[(s * R + a) * R + bb]);
+                    }
+                }
+#pragma unroll
+                for (int u = 0; u < K2; ++u) {
+                    const float v = warp_sumf(sacc[u]);
+                    if (lane == 0) part[(size_t)(item - it0) * K2 + u] = v;
+                }
             }
             __syncthreads();
             for (int u = threadIdx.x; u < (s1 - s0) * K2; u += blockDim.x) {
                 const int set = s0 + u / K2, e = u % K2;
                 const int s = e / (R * R), f = e % (R * R);
-                if (s < nsnp) A.Dset[((size_t)set * A.mb + i0 + s) * R * R + f] = setacc[u];
+                const int a0 = __ldg(A.set_item_off + set), a1 = __ldg(A.set_item_off + set + 1);
+                float sum = 0.f;
+                for (int it = a0; it < a1; ++it) sum += part[(size_t)(it - it0) * K2 + e];
+                if (s < nsnp) A.Dset[((size_t)set * A.mb + i0 + s) * R * R + f] = sum;
             }
             __syncthreads();
         }

@@ -1,5 +1,8 @@
 // Instantiations of the per-SNP statistics kernels (oa_stats.cuh, oa_lean.cuh).
 #include <algorithm>
+#include <map>
+#include <mutex>
+#include <tuple>
 
 #include "oa_lean.cuh"
 #include "oa_launch.h"
@@ -68,10 +71,52 @@ static cudaError_t go_lean(const LeanArgs& A, int grid, size_t smem, cudaStream_
         done[d] = 227 * 1024 - 1024;
     }
     if (bulk)
-        k_snp_lean<R, SPB, true><<<grid, OA_NTHREADS, smem, st>>>(A);
+        k_snp_lean<R, SPB, true><<<grid, LEAN_THREADS, smem, st>>>(A);
     else
-        k_snp_lean<R, SPB, false><<<grid, OA_NTHREADS, smem, st>>>(A);
+        k_snp_lean<R, SPB, false><<<grid, LEAN_THREADS, smem, st>>>(A);
     return cudaGetLastError();
+}
+
+template <int R, int SPB>
+static int lean_occ(size_t smem) {
+    int nb = 0;
+    if (cudaFuncSetAttribute(k_snp_lean<R, SPB, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024 - 1024) !=
+            cudaSuccess ||
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_snp_lean<R, SPB, true>, LEAN_THREADS, smem) != cudaSuccess) {
+        cudaGetLastError();
+        return 0;
+    }
+    return nb;
+}
+
+int oa_lean_ctas_per_sm(int R, int spb, size_t smem) {
+    // cached per (device, R, spb, smem): no runtime calls while a stream is captured
+    static std::map<std::tuple<int, int, int, size_t>, int> cache;
+    static std::mutex mu;
+    int dev = 0;
+    cudaGetDevice(&dev);
+    const auto key = std::make_tuple(dev, R, spb, smem);
+    {
+        std::lock_guard<std::mutex> g(mu);
+        auto it = cache.find(key);
+        if (it != cache.end()) return it->second;
+    }
+    int v = 0;
+    switch (R * 100 + spb) {
+        case 101: v = lean_occ<1, 1>(smem); break;
+        case 102: v = lean_occ<1, 2>(smem); break;
+        case 104: v = lean_occ<1, 4>(smem); break;
+        case 108: v = lean_occ<1, 8>(smem); break;
+        case 201: v = lean_occ<2, 1>(smem); break;
+        case 202: v = lean_occ<2, 2>(smem); break;
+        case 204: v = lean_occ<2, 4>(smem); break;
+        case 401: v = lean_occ<4, 1>(smem); break;
+        case 402: v = lean_occ<4, 2>(smem); break;
+        default: v = 0;
+    }
+    std::lock_guard<std::mutex> g(mu);
+    cache[key] = v;
+    return v;
 }
 
 cudaError_t oa_launch_snp_lean(int R, int spb, const LeanArgs& A, int grid, size_t smem, cudaStream_t st) {

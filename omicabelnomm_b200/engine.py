@@ -53,7 +53,7 @@ class Settings(C.Structure):
                 ("min_p_disp", C.c_float), ("min_p_store", C.c_float), ("min_r2_disp", C.c_float),
                 ("min_r2_store", C.c_float), ("store_bin", C.c_int32), ("disp_cov", C.c_int32),
                 ("store_all", C.c_int32), ("precision", C.c_int32), ("device", C.c_int32),
-                ("quirk_r2", C.c_int32), ("verbose", C.c_int32)]
+                ("quirk_r2", C.c_int32), ("verbose", C.c_int32), ("shard", C.c_int32), ("shards", C.c_int32)]
 
 
 class Tuning(C.Structure):
@@ -105,6 +105,9 @@ def lib() -> C.CDLL:
         "oa_scan_dense_noalloc": ([P, P, P, C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_int32, P, P, P, P,
                                    P], C.c_int),
         "oa_set_tuning": ([P, C.POINTER(Tuning)], C.c_int),
+        "oa_shard_range": ([C.c_int32, C.c_int32, C.c_int32, C.POINTER(C.c_int32), C.POINTER(C.c_int32)], C.c_int),
+        "oa_set_snp_rows": ([P, C.POINTER(C.c_int32), C.c_int32, C.c_int64], C.c_int),
+        "oa_device_bytes": ([P], C.c_int64),
         "oa_get_tuning": ([P, C.POINTER(Tuning)], C.c_int),
         "oa_autotune": ([P, P, C.c_int32, C.POINTER(Tuning)], C.c_int),
     }
@@ -217,6 +220,10 @@ class Engine:
         _check(lib().oa_run_snps_device(self.h, C.c_void_p(ptr), mb, int(results_on_host), C.byref(rows)))
         return rows
 
+    def scan(self, ptr: int, mb: int) -> StoredRows:
+        """Device SNP block -> stored rows on the host, in (trait, SNP) order (copied)."""
+        return self._rows(self.run_device(ptr, mb, results_on_host=True))
+
     def _rows(self, rows: Rows) -> StoredRows:
         N, p = rows.count, self.p
 
@@ -257,6 +264,17 @@ class Engine:
         _check(lib().oa_autotune(self.h, C.c_void_p(ptr), mb, C.byref(t)))
         return t.as_dict()
 
+    def set_snp_rows(self, rows: Optional[np.ndarray], ld: int = 0):
+        """Read device SNP columns of ``ld`` floats and use rows ``rows`` (ascending, n of them)."""
+        if rows is None:
+            _check(lib().oa_set_snp_rows(self.h, None, 0, 0))
+            return
+        rows = np.ascontiguousarray(rows, dtype=np.int32)
+        _check(lib().oa_set_snp_rows(self.h, rows.ctypes.data_as(C.POINTER(C.c_int32)), rows.size, ld))
+
+    def device_bytes(self) -> int:
+        return int(lib().oa_device_bytes(self.h))
+
     def launches(self) -> int:
         return int(lib().oa_kernel_launches(self.h))
 
@@ -277,6 +295,13 @@ def scan_dense_noalloc(xl_ptr: int, y_ptr: int, xr_ptr: int, n: int, l: int, r: 
                                        V(t_ptr), V(r2_ptr), V(stream)))
 
 
+def shard_range(m: int, shard: int, shards: int) -> tuple[int, int]:
+    """(first SNP, SNP count) of a shard: the reference's MPI split of m SNPs."""
+    first, count = C.c_int32(), C.c_int32()
+    _check(lib().oa_shard_range(m, shard, shards, C.byref(first), C.byref(count)))
+    return first.value, count.value
+
+
 def t_threshold(p: float) -> float:
     return float(lib().oa_t_threshold(C.c_float(p)))
 
@@ -287,7 +312,7 @@ def pvalue(t: float) -> float:
 
 def solve(xl: str, xr: str, y: str, out: str, *, r: int = 1, exclude: str = "", store_bin=False,
           disp_cov=False, store_all=False, precision=PLAIN, device=0, min_p_disp=None, min_p_store=None,
-          min_r2_disp=None, min_r2_store=None, verbose=False) -> Outputs:
+          min_r2_disp=None, min_r2_store=None, verbose=False, shard=0, shards=1) -> Outputs:
     """≙ Algorithm::solve on files: writes out_dis.txt (+ _sto.ibin/.dbin)."""
     L = lib()
     s = Settings()
@@ -298,6 +323,7 @@ def solve(xl: str, xr: str, y: str, out: str, *, r: int = 1, exclude: str = "", 
     s.r = r
     s.store_bin, s.disp_cov, s.store_all = int(store_bin), int(disp_cov), int(store_all)
     s.precision, s.device, s.verbose = precision, device, int(verbose)
+    s.shard, s.shards = shard, shards
     if min_p_disp is not None:
         s.min_p_disp = min_p_disp
     if min_p_store is not None:
