@@ -1,0 +1,74 @@
+"""Precision of both forms against the FP64 oracle on samples of the
+benchmark workloads (full n, t, l, r and pattern structure; a slice of the
+SNPs):
+  * omics scale (n = 10,000, t = 1,000, 20 patterns, r = 1);
+  * the same with a near-collinear covariate (age2 = age + N(0, 1e-3)) and
+    1 % of SNPs with MAF in [0.005, 0.01];
+  * batched interactions (n = 8,000, l = 5, r = 2: SNP x sex and SNP,
+    t = 2,000 in 150 Zipf-sized patterns).
+Bars: plain |dt| <= 1e-4 |t| + 1e-4; mixed |dt| <= 1e-3 for r = 1 and
+|dt| <= 1e-3 + 1e-4 |t| for r = 2 (the two correlated SNP columns amplify the
+BF16x3 rounding of X'y by the conditioning of their 2 x 2 Schur system).
+With OA_PRECISION_REPORT set, the measured errors are written there as JSON."""
+import json
+import os
+
+import numpy as np
+import pytest
+
+from omicabelnomm_b200 import engine as E
+from omicabelnomm_b200 import synth
+from test_gpu_parity import engine_run, oracle_dense
+
+pytestmark = pytest.mark.gpu
+
+SAMPLES = {
+    "omics_n10000_t1000_g20": (1, dict(m=128)),
+    "collinear_lowmaf_n10000_t1000": (2, dict(m=128)),
+    "interaction_r2_n8000_t2000_g150": (3, dict(m=48)),
+}
+REPORT = {}
+
+
+@pytest.mark.parametrize("name", sorted(SAMPLES))
+def test_forms_against_fp64_oracle(name):
+    cfg, over = SAMPLES[name]
+    w = synth.scaled(cfg, **over)
+    ds = synth.generate(w)
+    res, _, _ = oracle_dense(ds, w.r)
+    D = res.dense
+    ok = ~D.singular
+    t_ref = D.tstat[:, :, res.l:][ok]
+    out = {"tests": int(ok.sum()) * w.r, "max_abs_t": float(np.abs(t_ref).max())}
+    for label, prec in (("plain", E.PLAIN), ("mixed", E.MIXED)):
+        _, _, (b, se, tt, r2) = engine_run(ds, w.r, precision=prec)
+        dt = np.abs(tt[ok] - t_ref)
+        if prec == E.PLAIN:
+            lim = 1e-4 * np.abs(t_ref) + 1e-4
+        elif w.r == 1:
+            lim = np.full_like(t_ref, 1e-3)
+        else:
+            lim = 1e-3 + 1e-4 * np.abs(t_ref)
+        # the worst test relative to its bar, with what it depends on
+        q = int(np.argmax((dt / lim).ravel()))
+        row, a = q // w.r, q % w.r
+        j, i = (int(v) for v in np.argwhere(ok)[row])
+        b_ref = D.beta[:, :, res.l:][ok][row, a]
+        se_ref = D.se[:, :, res.l:][ok][row, a]
+        out[label] = {"max_dt": float(dt.max()), "p9999_dt": float(np.quantile(dt, 0.9999)),
+                      "max_rel_dt": float((dt / np.maximum(np.abs(t_ref), 1.0)).max()),
+                      "max_rel_se": float((np.abs(se[ok] - D.se[:, :, res.l:][ok]) /
+                                           np.abs(D.se[:, :, res.l:][ok])).max()),
+                      "worst": {"trait": j, "snp": i, "coef": a, "t_ref": float(t_ref[row, a]),
+                                "t": float(tt[ok][row, a]), "b_ref": float(b_ref), "b": float(b[ok][row, a]),
+                                "se_ref": float(se_ref), "se": float(se[ok][row, a]),
+                                "r2_ref": float(D.r2[j, i]), "r2": float(r2[j, i]),
+                                "missing": int(np.isnan(ds.Y[j]).sum()),
+                                "x_mean": float(np.nanmean(ds.XR[i * w.r + a])),
+                                "ratio_to_bar": float(dt[row, a] / lim[row, a])}}
+        REPORT[name] = out
+        path = os.environ.get("OA_PRECISION_REPORT")
+        if path:
+            with open(path, "w") as f:
+                json.dump(REPORT, f, indent=1)
+        assert np.all(dt <= lim), f"{name} {label}: max |dt| {dt.max():.3g}"
