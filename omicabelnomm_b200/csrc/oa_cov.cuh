@@ -81,22 +81,27 @@ __device__ __forceinline__ void cov_eval(const CovArgs& C, int i, int j, const f
     }
 }
 
-// Fill covariate terms of the records [first, last) of one SNP block.
+// Fill covariate terms of one chunk's records: [*first, counters[0]) (capped
+// at the record buffer), read on the device after the chunk's GEMM.
 template <int R>
 __global__ void __launch_bounds__(256)
-k_cov_terms(const Rec* __restrict__ rec, long long first, long long last, int snp_base, CovArgs C,
+k_cov_terms(const Rec* __restrict__ rec, const unsigned long long* __restrict__ first_p,
+            const unsigned long long* __restrict__ counters, long long cap, int snp_base, CovArgs C,
             float* __restrict__ cov /* [rec][l][3] */) {
-    const long long idx = first + blockIdx.x * (long long)blockDim.x + threadIdx.x;
-    if (idx >= last) return;
-    const Rec rc = rec[idx];
-    float b[OA_MAX_L], se[OA_MAX_L], t[OA_MAX_L];
-    cov_eval<R>(C, rc.snp - snp_base, rc.tint, rc.b, rc.sig, b, se, t);
-    float* o = cov + (size_t)idx * C.l * 3;
-    o[0] = o[1] = o[2] = 0.f;
-    for (int h = 1; h < C.l; ++h) {
-        o[h * 3] = b[h];
-        o[h * 3 + 1] = se[h];
-        o[h * 3 + 2] = t[h];
+    const long long first = (long long)*first_p;
+    const long long last = min((long long)counters[0], cap);
+    for (long long idx = first + blockIdx.x * (long long)blockDim.x + threadIdx.x; idx < last;
+         idx += (long long)gridDim.x * blockDim.x) {
+        const Rec rc = rec[idx];
+        float b[OA_MAX_L], se[OA_MAX_L], t[OA_MAX_L];
+        cov_eval<R>(C, rc.snp - snp_base, rc.tint, rc.b, rc.sig, b, se, t);
+        float* o = cov + (size_t)idx * C.l * 3;
+        o[0] = o[1] = o[2] = 0.f;
+        for (int h = 1; h < C.l; ++h) {
+            o[h * 3] = b[h];
+            o[h * 3 + 1] = se[h];
+            o[h * 3 + 2] = t[h];
+        }
     }
 }
 

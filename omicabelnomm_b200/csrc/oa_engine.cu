@@ -207,6 +207,7 @@ struct oa_engine {
     DBuf<double> Q64, Rinv;
     DBuf<float> Qr;
     bool have_cov = false;
+    bool center = false;   // the first covariate is constant: SNP columns are taken relative to their means
     // traits
     int t = 0;
     DBuf<float> Yraw, Yt;
@@ -249,6 +250,7 @@ struct oa_engine {
     DBuf<float> cov, cov2;
     long long cap = 0;
     DBuf<unsigned long long> counters;  // [0] rows, [1] singular, [2] significant covariate terms
+    DBuf<unsigned long long> marks;     // stored-row count at the start of each chunk's GEMM
     DBuf<unsigned long long> keys, keys2;
     DBuf<int> perm, perm2;
     DBuf<unsigned char> cub_tmp;
@@ -308,7 +310,7 @@ void for_each_buf(oa_engine* e, F&& f) {
     f(e->rec); f(e->rec2); f(e->cov); f(e->cov2); f(e->counters); f(e->keys); f(e->keys2); f(e->perm);
     f(e->perm2); f(e->cub_tmp);
     f(e->d_beta); f(e->d_se); f(e->d_t); f(e->d_r2); f(e->d_sig); f(e->xrows);
-    f(e->item_start); f(e->set_item_off); f(e->pass_off);
+    f(e->item_start); f(e->set_item_off); f(e->pass_off); f(e->marks);
 }
 
 // Columns [c0, c0 + ncol) of a strided block gathered to the engine's rows.
@@ -563,6 +565,7 @@ StatsArgs stats_args(oa_engine* e, const float* X, int mbc, int LP, int spb, int
     A.zA = e->zA.p;
     A.zD = e->zD.p;
     A.write_split = e->cfg.precision == OA_MIXED_BF16X3;
+    A.center = e->center ? 1 : 0;
     A.Xhi = e->Xhi.p;
     A.Xlo = e->Xlo.p;
     return A;
@@ -684,6 +687,7 @@ oa_status stats_pre(oa_engine* e, const float* X, int mbc) {
     A.Dset = e->Dset.p;
     const bool mixed = e->cfg.precision == OA_MIXED_BF16X3;
     A.write_split = mixed ? 1 : 0;
+    A.center = e->center ? 1 : 0;
     A.Xhi = e->Xhi.p;
     A.Xlo = e->Xlo.p;
     A.err = reinterpret_cast<int*>(e->counters.p + 3);
@@ -698,7 +702,7 @@ oa_status stats_pre(oa_engine* e, const float* X, int mbc) {
                                reinterpret_cast<int*>(e->counters.p + 3), e->st));
     else
         OA_CU(oa_launch_pre_simt(X, (size_t)e->n, mbc * R, e->B2.p, (size_t)e->n_pad, e->c2, e->n, e->mean.p,
-                                 e->has_nan.p, e->C2T.p, ldc, e->st));
+                                 e->has_nan.p, e->center ? 1 : 0, e->C2T.p, ldc, e->st));
     ++e->launches;
     SchurArgs S{};
     S.l = e->l;
@@ -801,7 +805,7 @@ oa_status gemm_dispatch(oa_engine* e, const float* X, int mbc, int snp_base) {
     EpiArgs E = epi_args(e, mbc, snp_base);
     if (e->cfg.precision == OA_PLAIN_FP32) {
         OA_CU(oa_launch_gemm_simt(R, X, (size_t)e->n, mbc * R, e->Yt.p, (size_t)e->n_pad, e->t, e->n, e->mean.p,
-                                  e->has_nan.p, E, e->st));
+                                  e->has_nan.p, e->center ? 1 : 0, E, e->st));
         e->last_name = "k_gemm_simt";
     } else {
         OA_CU(oa_launch_gemm_tc(R, e->variant, e->raster, e->Xhi.p, e->Xlo.p, mbc * R, e->Yhi.p, e->Ylo.p, e->t,
@@ -861,63 +865,18 @@ oa_status ensure_cap(oa_engine* e, long long want) {
     return OA_OK;
 }
 
-// One SNP chunk already on the device.  Appends its stored rows.
-template <int R>
-oa_status run_chunk(oa_engine* e, const float* X, int mbc, int snp_base) {
-    OA_CU(cudaMemsetAsync(e->has_nan.p, 0, sizeof(int), e->st));
-    OA_CU(cudaEventRecord(e->s0, e->st));
-    OA_CHECK(stats_dispatch<R>(e, X, mbc));
-    OA_CU(cudaEventRecord(e->s1, e->st));
-    unsigned long long before[4];
-    OA_CU(cudaMemcpyAsync(before, e->counters.p, sizeof before, cudaMemcpyDeviceToHost, e->st));
-    OA_CU(cudaStreamSynchronize(e->st));
-    for (int attempt = 0; attempt < 3; ++attempt) {
-        OA_CU(cudaEventRecord(e->k0, e->st));
-        OA_CHECK(gemm_dispatch<R>(e, X, mbc, snp_base));
-        OA_CU(cudaEventRecord(e->k1, e->st));
-        unsigned long long after[4];
-        OA_CU(cudaMemcpyAsync(after, e->counters.p, sizeof after, cudaMemcpyDeviceToHost, e->st));
-        OA_CU(cudaStreamSynchronize(e->st));
-        float ms = 0.f;
-        cudaEventElapsedTime(&ms, e->k0, e->k1);
-        e->last_ms += ms;
-        if (attempt == 0) {
-            cudaEventElapsedTime(&ms, e->s0, e->s1);
-            e->stats_ms += ms;
-        }
-        if (after[3]) {
-            set_err("a device pipeline wait timed out (the kernel stopped cleanly)");
-            return OA_ERR_CUDA;
-        }
-        if ((long long)after[0] <= e->cap) {
-            if (e->cfg.disp_cov) {
-                CovArgs C = cov_args(e, mbc);
-                const long long first = (long long)before[0], last = (long long)after[0];
-                if (last > first) {
-                    const long long nb = (last - first + 255) / 256;
-                    k_cov_terms<R><<<(unsigned)nb, 256, 0, e->st>>>(e->rec.p, first, last, snp_base, C, e->cov.p);
-                    ++e->launches;
-                }
-                k_cov_count<R><<<4 * 148, 256, 0, e->st>>>(e->d_beta.p, e->d_t.p, e->d_r2.p, e->d_sig.p, e->dense_ld,
-                                                          snp_base, mbc, e->t, e->cfg.min_r2_store, C,
-                                                          e->counters.p + 2);
-                ++e->launches;
-                OA_CU(cudaGetLastError());
-            }
-            return OA_OK;
-        }
-        // more rows than room: grow, roll the counters back and redo the GEMM
-        OA_CHECK(ensure_cap(e, (long long)(after[0] * 1.25) + 1024));
-        OA_CU(cudaMemcpyAsync(e->counters.p, before, sizeof before, cudaMemcpyHostToDevice, e->st));
-    }
-    set_err("stored-row buffer could not be grown");
-    return OA_ERR_NOMEM;
+// Stored-row count at the start of a chunk's GEMM (the covariate-term
+// kernel of that chunk reads its record range from here and the counter).
+static __global__ void k_mark(const unsigned long long* __restrict__ counters, unsigned long long* __restrict__ mark) {
+    *mark = counters[0];
 }
 
-// Every chunk of a device-resident SNP block, enqueued without host
-// synchronisation (the body of the captured graph).
+// Every chunk of a SNP block enqueued on the engine's stream with no host
+// synchronisation: host blocks stream through two staging buffers on the
+// copy stream, device blocks are read in place (or gathered for a row
+// subset).  `capture`: the events become graph nodes.
 template <int R>
-oa_status enqueue_scan(oa_engine* e, const float* xr, int mb) {
+oa_status enqueue_block(oa_engine* e, const float* xr, int mb, bool host_input, bool capture) {
     const int nch = (mb + e->chunk - 1) / e->chunk;
     while ((int)e->cev0.size() < nch) {
         cudaEvent_t ev[4];
@@ -927,17 +886,54 @@ oa_status enqueue_scan(oa_engine* e, const float* xr, int mb) {
         e->sev0.push_back(ev[2]);
         e->sev1.push_back(ev[3]);
     }
+    auto rec = [&](cudaEvent_t ev) -> cudaError_t {
+        return capture ? cudaEventRecordWithFlags(ev, e->st, cudaEventRecordExternal) : cudaEventRecord(ev, e->st);
+    };
+    const size_t colbytes = sizeof(float) * (size_t)e->n * R;
+    auto issue_copy = [&](int c) -> oa_status {   // host chunk c -> staging buffer c & 1 (copy stream)
+        const int b = c & 1;
+        const int c0 = c * e->chunk, mbc = std::min(e->chunk, mb - c0);
+        OA_CU(cudaStreamWaitEvent(e->cp, e->ev_used[b], 0));
+        OA_CU(cudaMemcpyAsync(e->Xstage[b].p, xr + (size_t)c0 * R * e->n, colbytes * mbc, cudaMemcpyHostToDevice,
+                              e->cp));
+        OA_CU(cudaEventRecord(e->ev_copied[b], e->cp));
+        return OA_OK;
+    };
+    if (host_input) OA_CHECK(issue_copy(0));
+    const bool cov = e->cfg.disp_cov != 0;
+    if (cov) OA_CHECK(e->marks.ensure(nch));
     for (int c = 0; c < nch; ++c) {
         const int c0 = c * e->chunk, mbc = std::min(e->chunk, mb - c0);
         const float* X = nullptr;
-        OA_CHECK(chunk_input<R>(e, xr, c0, mbc, &X));
+        if (host_input) {
+            if (c + 1 < nch) OA_CHECK(issue_copy(c + 1));
+            OA_CU(cudaStreamWaitEvent(e->st, e->ev_copied[c & 1], 0));
+            X = e->Xstage[c & 1].p;
+        } else {
+            OA_CHECK(chunk_input<R>(e, xr, c0, mbc, &X));
+        }
         OA_CU(cudaMemsetAsync(e->has_nan.p, 0, sizeof(int), e->st));
-        OA_CU(cudaEventRecordWithFlags(e->sev0[c], e->st, cudaEventRecordExternal));
+        OA_CU(rec(e->sev0[c]));
         OA_CHECK(stats_dispatch<R>(e, X, mbc));
-        OA_CU(cudaEventRecordWithFlags(e->sev1[c], e->st, cudaEventRecordExternal));
-        OA_CU(cudaEventRecordWithFlags(e->cev0[c], e->st, cudaEventRecordExternal));
+        OA_CU(rec(e->sev1[c]));
+        if (cov) {
+            k_mark<<<1, 1, 0, e->st>>>(e->counters.p, e->marks.p + c);
+            ++e->launches;
+        }
+        OA_CU(rec(e->cev0[c]));
         OA_CHECK(gemm_dispatch<R>(e, X, mbc, c0));
-        OA_CU(cudaEventRecordWithFlags(e->cev1[c], e->st, cudaEventRecordExternal));
+        OA_CU(rec(e->cev1[c]));
+        if (host_input) OA_CU(cudaEventRecord(e->ev_used[c & 1], e->st));
+        if (cov) {
+            CovArgs C = cov_args(e, mbc);
+            k_cov_terms<R><<<4 * e->sm_count, 256, 0, e->st>>>(e->rec.p, e->marks.p + c, e->counters.p, e->cap, c0, C,
+                                                             e->cov.p);
+            k_cov_count<R><<<4 * e->sm_count, 256, 0, e->st>>>(e->d_beta.p, e->d_t.p, e->d_r2.p, e->d_sig.p,
+                                                             e->dense_ld, c0, mbc, e->t, e->cfg.min_r2_store, C,
+                                                             e->counters.p + 2);
+            e->launches += 2;
+            OA_CU(cudaGetLastError());
+        }
     }
     return OA_OK;
 }
@@ -950,73 +946,82 @@ void drop_graph(oa_engine* e) {
     e->gkey = oa_engine::GraphKey{};
 }
 
-// Device-resident scan as one CUDA graph launch (captured on the second
-// call with the same inputs; the first call runs uncaptured).  Returns
-// false in *done when the caller must run the uncaptured path instead.
+// One SNP block, host or device, with one host synchronisation at its end.
+// A device block seen twice with the same inputs is captured as one CUDA
+// graph and replayed afterwards (the first sight runs uncaptured, which also
+// sets the kernels' attributes).  If the stored rows outgrow their buffer,
+// the buffer grows and the block runs again.
 template <int R>
-oa_status run_graph(oa_engine* e, const float* xr, int mb, bool* done) {
-    *done = false;
-    oa_engine::GraphKey key;
-    key.xr = xr;
-    key.mb = mb;
-    key.t = e->t;
-    key.dense = e->dense_on ? 1 : 0;
-    key.gen = e->trait_gen;
-    key.cap = e->cap;
-    key.rec = e->rec.p;
-    key.tune = e->tune_gen;
-    if (!(e->gexec && e->gkey == key)) {
-        drop_graph(e);
-        if (!(e->warm_key == key)) {
-            e->warm_key = key;       // first sight: uncaptured run (sets kernel attributes)
-            return OA_OK;
-        }
-        const long long l0 = e->launches;
-        OA_CU(cudaStreamBeginCapture(e->st, cudaStreamCaptureModeThreadLocal));
-        const oa_status s = enqueue_scan<R>(e, xr, mb);
-        e->graph_launches = e->launches - l0;   // kernels in the graph (they run at each launch)
-        e->launches = l0;
-        cudaGraph_t g = nullptr;
-        const cudaError_t ce = cudaStreamEndCapture(e->st, &g);
-        if (s != OA_OK) {
-            if (g) cudaGraphDestroy(g);
-            return s;
-        }
-        OA_CU(ce);
-        e->graph = g;
-        OA_CU(cudaGraphInstantiate(&e->gexec, g, 0));
-        e->gkey = key;
-    }
-    OA_CU(cudaGraphLaunch(e->gexec, e->st));
+oa_status run_block(oa_engine* e, const float* xr, int mb, bool host_input) {
     const int nch = (mb + e->chunk - 1) / e->chunk;
-    e->launches += e->graph_launches;
-    unsigned long long cnt[4];
-    OA_CU(cudaMemcpyAsync(cnt, e->counters.p, sizeof cnt, cudaMemcpyDeviceToHost, e->st));
-    OA_CU(cudaStreamSynchronize(e->st));
-    if (cnt[3]) {
-        set_err("a device pipeline wait timed out (the kernel stopped cleanly)");
-        return OA_ERR_CUDA;
-    }
-    if ((long long)cnt[0] > e->cap) {
-        // more stored rows than room: grow and let the caller run the uncaptured path
-        OA_CHECK(ensure_cap(e, (long long)(cnt[0] * 1.25) + 1024));
+    for (int attempt = 0; attempt < 3; ++attempt) {
         OA_CU(cudaMemsetAsync(e->counters.p, 0, 4 * sizeof(unsigned long long), e->st));
-        drop_graph(e);
+        bool launched = false;
+        if (!host_input && e->use_graphs) {
+            oa_engine::GraphKey key;
+            key.xr = xr;
+            key.mb = mb;
+            key.t = e->t;
+            key.dense = e->dense_on ? 1 : 0;
+            key.gen = e->trait_gen;
+            key.cap = e->cap;
+            key.rec = e->rec.p;
+            key.tune = e->tune_gen;
+            if (!(e->gexec && e->gkey == key)) {
+                drop_graph(e);
+                if (e->warm_key == key) {
+                    const long long l0 = e->launches;
+                    OA_CU(cudaStreamBeginCapture(e->st, cudaStreamCaptureModeThreadLocal));
+                    const oa_status s = enqueue_block<R>(e, xr, mb, false, true);
+                    e->graph_launches = e->launches - l0;   // kernels in the graph (they run at each launch)
+                    e->launches = l0;
+                    cudaGraph_t g = nullptr;
+                    const cudaError_t ce = cudaStreamEndCapture(e->st, &g);
+                    if (s != OA_OK) {
+                        if (g) cudaGraphDestroy(g);
+                        return s;
+                    }
+                    OA_CU(ce);
+                    e->graph = g;
+                    OA_CU(cudaGraphInstantiate(&e->gexec, g, 0));
+                    e->gkey = key;
+                } else {
+                    e->warm_key = key;
+                }
+            }
+            if (e->gexec && e->gkey == key) {
+                OA_CU(cudaGraphLaunch(e->gexec, e->st));
+                e->launches += e->graph_launches;
+                launched = true;
+            }
+        }
+        if (!launched) OA_CHECK(enqueue_block<R>(e, xr, mb, host_input, false));
+        unsigned long long cnt[4];
+        OA_CU(cudaMemcpyAsync(cnt, e->counters.p, sizeof cnt, cudaMemcpyDeviceToHost, e->st));
+        OA_CU(cudaStreamSynchronize(e->st));
+        if (cnt[3]) {
+            set_err("a device pipeline wait timed out (the kernel stopped cleanly)");
+            return OA_ERR_CUDA;
+        }
+        if ((long long)cnt[0] > e->cap) {   // more stored rows than room: grow, run the block again
+            OA_CHECK(ensure_cap(e, (long long)(cnt[0] * 1.25) + 1024));
+            drop_graph(e);
+            continue;
+        }
+        float total = 0.f, stotal = 0.f;
+        for (int c = 0; c < nch; ++c) {
+            float ms = 0.f;
+            if (cudaEventElapsedTime(&ms, e->cev0[c], e->cev1[c]) == cudaSuccess) total += ms;
+            if (cudaEventElapsedTime(&ms, e->sev0[c], e->sev1[c]) == cudaSuccess) stotal += ms;
+        }
+        cudaGetLastError();
+        e->last_ms = total;
+        e->stats_ms = stotal;
+        e->last_name = e->cfg.precision == OA_PLAIN_FP32 ? "k_gemm_simt" : "k_gemm_tc";
         return OA_OK;
     }
-    float total = 0.f, stotal = 0.f;
-    for (int c = 0; c < nch; ++c) {
-        float ms = 0.f;
-        cudaEventElapsedTime(&ms, e->cev0[c], e->cev1[c]);
-        total += ms;
-        cudaEventElapsedTime(&ms, e->sev0[c], e->sev1[c]);
-        stotal += ms;
-    }
-    e->last_ms = total;
-    e->stats_ms = stotal;
-    e->last_name = e->cfg.precision == OA_PLAIN_FP32 ? "k_gemm_simt" : "k_gemm_tc";
-    *done = true;
-    return OA_OK;
+    set_err("stored-row buffer could not be grown");
+    return OA_ERR_NOMEM;
 }
 
 template <int R>
@@ -1033,7 +1038,12 @@ oa_status run_snps_impl(oa_engine* e, const float* xr, int32_t mb, bool host_inp
     OA_CHECK(prepare_tuning(e));
     OA_CHECK(ensure_chunk_buffers(e));
     const long long tests = (long long)mb * e->t;
-    if (e->cap == 0) OA_CHECK(ensure_cap(e, std::max<long long>(1 << 16, e->cfg.store_all ? tests : tests / 6)));
+    if (e->cap == 0) {
+        // expected stored share: the two-sided normal tail beyond the |t| threshold, with headroom
+        const double tail = std::erfc((double)e->cfg.min_t_store / std::sqrt(2.0));
+        const double share = std::min(1.0, 1.5 * tail + 1e-3);
+        OA_CHECK(ensure_cap(e, std::max<long long>(1 << 16, e->cfg.store_all ? tests : (long long)(tests * share))));
+    }
     if (e->cfg.store_all) OA_CHECK(ensure_cap(e, tests));
     OA_CU(cudaMemsetAsync(e->counters.p, 0, 4 * sizeof(unsigned long long), e->st));
     if (e->dense_on || e->cfg.disp_cov) {
@@ -1048,8 +1058,6 @@ oa_status run_snps_impl(oa_engine* e, const float* xr, int32_t mb, bool host_inp
     e->last_ms = 0.f;
     e->stats_ms = 0.f;
     e->last_mb = mb;
-    const size_t colbytes = sizeof(float) * (size_t)e->n * e->r;
-    const int nch = (mb + e->chunk - 1) / e->chunk;
     if (e->subset) {
         if (host_input) {
             set_err("a row subset applies to device SNP blocks only (oa_run_snps_device)");
@@ -1057,38 +1065,9 @@ oa_status run_snps_impl(oa_engine* e, const float* xr, int32_t mb, bool host_inp
         }
         OA_CHECK(e->Xstage[0].ensure((size_t)e->chunk * e->r * e->n));
     }
-    if (host_input) {
+    if (host_input)
         for (int b = 0; b < 2; ++b) OA_CHECK(e->Xstage[b].ensure((size_t)e->chunk * e->r * e->n));
-        // copy of chunk c+1 overlaps the compute of chunk c
-        auto issue_copy = [&](int c) -> oa_status {
-            const int b = c & 1;
-            const int c0 = c * e->chunk, mbc = std::min(e->chunk, mb - c0);
-            OA_CU(cudaStreamWaitEvent(e->cp, e->ev_used[b], 0));
-            OA_CU(cudaMemcpyAsync(e->Xstage[b].p, xr + (size_t)c0 * e->r * e->n, colbytes * mbc,
-                                  cudaMemcpyHostToDevice, e->cp));
-            OA_CU(cudaEventRecord(e->ev_copied[b], e->cp));
-            return OA_OK;
-        };
-        OA_CHECK(issue_copy(0));
-        for (int c = 0; c < nch; ++c) {
-            if (c + 1 < nch) OA_CHECK(issue_copy(c + 1));
-            const int b = c & 1;
-            const int c0 = c * e->chunk, mbc = std::min(e->chunk, mb - c0);
-            OA_CU(cudaStreamWaitEvent(e->st, e->ev_copied[b], 0));
-            OA_CHECK(run_chunk<R>(e, e->Xstage[b].p, mbc, c0));
-            OA_CU(cudaEventRecord(e->ev_used[b], e->st));
-        }
-    } else {
-        bool done = false;
-        if (e->use_graphs && !e->cfg.disp_cov) OA_CHECK(run_graph<R>(e, xr, mb, &done));
-        if (!done)
-            for (int c = 0; c < nch; ++c) {
-                const int c0 = c * e->chunk, mbc = std::min(e->chunk, mb - c0);
-                const float* X = nullptr;
-                OA_CHECK(chunk_input<R>(e, xr, c0, mbc, &X));
-                OA_CHECK(run_chunk<R>(e, X, mbc, c0));
-            }
-    }
+    OA_CHECK(run_block<R>(e, xr, mb, host_input));
     unsigned long long cnt[3];
     OA_CU(cudaMemcpyAsync(cnt, e->counters.p, sizeof cnt, cudaMemcpyDeviceToHost, e->st));
     OA_CU(cudaStreamSynchronize(e->st));
@@ -1448,6 +1427,12 @@ oa_status oa_set_covariates(oa_engine* e, const float* xl) {
     OA_CU(cudaMemcpy(e->Q64.p, Q.data(), sizeof(double) * Q.size(), cudaMemcpyHostToDevice));
     OA_CU(cudaMemcpy(e->Qr.p, Qr.data(), sizeof(float) * Qr.size(), cudaMemcpyHostToDevice));
     OA_CU(cudaMemcpy(e->Rinv.p, Ri.data(), sizeof(double) * Ri.size(), cudaMemcpyHostToDevice));
+    // An intercept as the first covariate makes every quantity of the scan
+    // invariant to shifting a SNP column by a constant (its Q column is
+    // proportional to 1 and the other Q columns are orthogonal to 1); the
+    // kernels then work with x - mean, whose sums cancel far less.
+    e->center = xl[0] != 0.f;
+    for (int k = 1; k < n && e->center; ++k) e->center = xl[k] == xl[0];
     e->have_cov = true;
     e->t = 0;
     return OA_OK;

@@ -13,9 +13,12 @@ namespace oa {
 
 constexpr int SG_BM = 128, SG_BN = 128, SG_BK = 16, SG_PAD = 4;
 
+// Four consecutive k of row `row`.  fix: dosage columns, where NaN is the
+// column mean (center = 0: NaN -> mean[row]) or every value is taken
+// relative to the column mean (center = 1: x -> x - mean[row], NaN -> 0).
 template <bool VEC>
 __device__ __forceinline__ void sg_load(const float* __restrict__ P, size_t ld, int nrow, int K,
-                                        int row, int k, const float* __restrict__ mean, bool fix_nan,
+                                        int row, int k, const float* __restrict__ mean, bool fix, bool center,
                                         float (&v)[4]) {
     if (row < nrow) {
         const float* src = P + (size_t)row * ld + k;
@@ -26,10 +29,13 @@ __device__ __forceinline__ void sg_load(const float* __restrict__ P, size_t ld, 
 #pragma unroll
             for (int u = 0; u < 4; ++u) v[u] = (k + u < K) ? __ldg(src + u) : 0.f;
         }
-        if (fix_nan) {
+        if (fix) {
             const float mv = mean[row];
 #pragma unroll
-            for (int u = 0; u < 4; ++u) v[u] = isnan(v[u]) ? mv : v[u];
+            for (int u = 0; u < 4; ++u) {
+                const float c = center ? (isnan(v[u]) ? 0.f : v[u] - mv) : (isnan(v[u]) ? mv : v[u]);
+                v[u] = (k + u < K) ? c : 0.f;
+            }
         }
     } else {
 #pragma unroll
@@ -43,7 +49,7 @@ __device__ __forceinline__ void sg_load(const float* __restrict__ P, size_t ld, 
 template <int R, bool VEC, bool STORE>
 __global__ void __launch_bounds__(256, 2)
 k_gemm_simt(const float* __restrict__ X, size_t ldx, int xrows, const float* __restrict__ Yt, size_t ldy,
-            int t, int K, const float* __restrict__ colmean, const int* __restrict__ has_nan, EpiArgs E,
+            int t, int K, const float* __restrict__ colmean, const int* __restrict__ has_nan, int center, EpiArgs E,
             float* __restrict__ cout, int ldc) {
     __shared__ __align__(16) float As[2][SG_BK][SG_BM + SG_PAD];
     __shared__ __align__(16) float Bs[2][SG_BK][SG_BN + SG_PAD];
@@ -52,7 +58,7 @@ k_gemm_simt(const float* __restrict__ X, size_t ldx, int xrows, const float* __r
     const int m0 = blockIdx.y * SG_BM;  // first SNP column of the tile
     const int n0 = blockIdx.x * SG_BN;  // first trait of the tile
     const int lrow = tid >> 2, lk = (tid & 3) * 4;
-    const bool fix = *has_nan != 0;
+    const bool fix = center || *has_nan != 0;
 
     float acc[8][8];
 #pragma unroll
@@ -64,8 +70,8 @@ k_gemm_simt(const float* __restrict__ X, size_t ldx, int xrows, const float* __r
     auto gload = [&](int k0) {
 #pragma unroll
         for (int h = 0; h < 2; ++h) {
-            sg_load<VEC>(X, ldx, xrows, K, m0 + lrow + 64 * h, k0 + lk, colmean, fix, ra[h]);
-            sg_load<VEC>(Yt, ldy, t, K, n0 + lrow + 64 * h, k0 + lk, colmean, false, rb[h]);
+            sg_load<VEC>(X, ldx, xrows, K, m0 + lrow + 64 * h, k0 + lk, colmean, fix, center != 0, ra[h]);
+            sg_load<VEC>(Yt, ldy, t, K, n0 + lrow + 64 * h, k0 + lk, colmean, false, false, rb[h]);
         }
     };
     auto sstore = [&](int buf) {

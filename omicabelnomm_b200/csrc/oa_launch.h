@@ -18,9 +18,12 @@ cudaError_t oa_launch_pre_tc(const __nv_bfloat16* Xhi, const __nv_bfloat16* Xlo,
                              const __nv_bfloat16* Bhi, const __nv_bfloat16* Blo, int c2, int n_pad, float* C, int ldc,
                              int* err, cudaStream_t st);
 cudaError_t oa_launch_pre_simt(const float* X, size_t ldx, int xrows, const float* B, size_t ldb, int c2, int K,
-                               const float* colmean, const int* has_nan, float* C, int ldc, cudaStream_t st);
+                               const float* colmean, const int* has_nan, int center, float* C, int ldc,
+                               cudaStream_t st);
+// center: dosages taken relative to colmean (NaN -> 0); else NaN -> colmean
 cudaError_t oa_launch_gemm_simt(int R, const float* X, size_t ldx, int xrows, const float* Yt, size_t ldy, int t,
-                                int K, const float* colmean, const int* has_nan, const EpiArgs& E, cudaStream_t st);
+                                int K, const float* colmean, const int* has_nan, int center, const EpiArgs& E,
+                                cudaStream_t st);
 // variant: 1 = BK 32 x 4 stages, 2 = BK 64 x 2 stages; raster: 1 = trait tiles inner, 2 = SNP tiles inner
 cudaError_t oa_launch_gemm_tc(int R, int variant, int raster, const __nv_bfloat16* Xhi, const __nv_bfloat16* Xlo,
                               int xrows, const __nv_bfloat16* Yhi, const __nv_bfloat16* Ylo, int t, int n_pad,

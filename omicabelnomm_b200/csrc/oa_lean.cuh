@@ -29,13 +29,14 @@ struct LeanArgs {
     const int* pass_off;      // passes over sets [pass_off[p], pass_off[p+1]) whose items fit in shared memory
     int npass;
     int items_cap;
-    float* mean;          // [mb*r] imputation means (0 if the column had no NaN)
+    float* mean;          // [mb*r] column means if center, else imputation means (0 if the column had no NaN)
     int* has_nan;
     float* D;             // [mb][r*r] X'X over all rows
     float* Dset;          // [nsets][mb][r*r] X'X over each row set
     __nv_bfloat16* Xhi;   // [mb*r][n_pad] (tensor-core form) or null
     __nv_bfloat16* Xlo;
     int write_split;
+    int center;           // take each column relative to its mean (valid when XL holds an intercept)
     int* err;
 };
 
@@ -94,10 +95,13 @@ __device__ __forceinline__ void split8(const float4 p0, const float4 p1, uint4& 
 // One CTA handles SPB SNPs (SPB*R columns) per group; a persistent loop over
 // groups with the next group's columns streaming into shared memory (TMA
 // bulk copies) while this one is processed:
-//   pass 1  column sums and X'X from float4 reads of the staged columns (one
-//           block reduction); NaN propagates, so a column whose sum is NaN
-//           is counted, mean-imputed in place and X'X recomputed
-//           (src/Utility.cpp:302-326) - rare, dosage files seldom hold NaN
+//   pass 1  column sums from float4 reads of the staged columns; NaN
+//           propagates, so a column whose sum is NaN is counted and
+//           mean-imputed in place (src/Utility.cpp:302-326) - rare, dosage
+//           files seldom hold NaN.  With an intercept among the covariates
+//           every later sum uses x - mean (the Schur complements, X'y~ and
+//           var_x do not change; the sums lose their large common part)
+//   pass 1b X'X over all rows
 //   pass 2  BF16 hi/lo split of the columns (tensor-core form only)
 //   pass 3  X'X over each row set: work items of at most 256 rows of one set
 //           (fixed on the host per trait block) go round-robin to the warps;
@@ -189,77 +193,91 @@ k_snp_lean(LeanArgs A) {
         const float4* x4 = reinterpret_cast<const float4*>(xs);
         const int nS4 = nS / 4;
 
-        // ---- pass 1: sums and X'X (NaN propagates)
-        float acc[NC + K2];
-        double tot[NC + K2];
-#pragma unroll
-        for (int u = 0; u < NC + K2; ++u) acc[u] = 0.f;
-        for (int k4 = threadIdx.x; k4 < nS4; k4 += blockDim.x) {
-            float4 v[NC];
-#pragma unroll
-            for (int c = 0; c < NC; ++c) v[c] = c < ncol ? x4[(size_t)c * nS4 + k4] : make_float4(0.f, 0.f, 0.f, 0.f);
-#pragma unroll
-            for (int c = 0; c < NC; ++c) acc[c] += (v[c].x + v[c].y) + (v[c].z + v[c].w);
-#pragma unroll
-            for (int s = 0; s < SPB; ++s)
-#pragma unroll
-                for (int a = 0; a < R; ++a)
-#pragma unroll
-                    for (int bb = 0; bb < R; ++bb) {
-                        const float4 xa = v[s * R + a], xb = v[s * R + bb];
-                        float& d = acc[NC + (s * R + a) * R + bb];
-                        d = fmaf(xa.x, xb.x, d);
-                        d = fmaf(xa.y, xb.y, d);
-                        d = fmaf(xa.z, xb.z, d);
-                        d = fmaf(xa.w, xb.w, d);
-                    }
-        }
-        block_sum_fd<NC + K2>(acc, tot, red);
-        bool any_nan = false;
-        float cmean[NC];
+        // ---- pass 1: column sums (NaN propagates), then the mean of every
+        // column; a column whose sum is NaN is counted and mean-imputed in place
+        float sh[NC];                          // subtracted from every value (centring), 0 without
         bool cnan[NC];
+        {
+            float acc[NC];
+            double tot[NC];
 #pragma unroll
-        for (int c = 0; c < NC; ++c) {
-            cnan[c] = (c < ncol) && isnan(tot[c]);
-            any_nan |= cnan[c];
-            cmean[c] = 0.f;
-        }
-        if (any_nan) {   // block-uniform: count, impute in place, recompute X'X
-            float cs[2 * NC];
-            double ct[2 * NC];
+            for (int c = 0; c < NC; ++c) acc[c] = 0.f;
+            for (int k4 = threadIdx.x; k4 < nS4; k4 += blockDim.x) {
 #pragma unroll
-            for (int u = 0; u < 2 * NC; ++u) cs[u] = 0.f;
+                for (int c = 0; c < NC; ++c) {
+                    const float4 v = c < ncol ? x4[(size_t)c * nS4 + k4] : make_float4(0.f, 0.f, 0.f, 0.f);
+                    acc[c] += (v.x + v.y) + (v.z + v.w);
+                }
+            }
+            block_sum_fd<NC>(acc, tot, red);
+            bool any_nan = false;
+            float cmean[NC];
 #pragma unroll
             for (int c = 0; c < NC; ++c) {
-                if (cnan[c]) {
-                    const float* col = xs + (size_t)c * nS;
-                    for (int k = threadIdx.x; k < n; k += blockDim.x) {
-                        const float v = col[k];
-                        if (isnan(v)) cs[NC + c] += 1.f;
-                        else cs[c] += v;
+                cnan[c] = (c < ncol) && isnan(tot[c]);
+                any_nan |= cnan[c];
+                cmean[c] = (float)(tot[c] / (double)n);
+            }
+            if (any_nan) {   // block-uniform: count and sum the observed values, impute in place
+                float cs[2 * NC];
+                double ct[2 * NC];
+#pragma unroll
+                for (int u = 0; u < 2 * NC; ++u) cs[u] = 0.f;
+#pragma unroll
+                for (int c = 0; c < NC; ++c) {
+                    if (cnan[c]) {
+                        const float* col = xs + (size_t)c * nS;
+                        for (int k = threadIdx.x; k < n; k += blockDim.x) {
+                            const float v = col[k];
+                            if (isnan(v)) cs[NC + c] += 1.f;
+                            else cs[c] += v;
+                        }
+                    }
+                }
+                block_sum_fd<2 * NC>(cs, ct, red);
+#pragma unroll
+                for (int c = 0; c < NC; ++c) {
+                    if (cnan[c]) {
+                        cmean[c] = (float)(ct[c] / ((double)n - ct[NC + c]));
+                        float* col = xs + (size_t)c * nS;
+                        for (int k = threadIdx.x; k < n; k += blockDim.x)
+                            if (isnan(col[k])) col[k] = cmean[c];
+                    }
+                }
+                __syncthreads();
+            }
+#pragma unroll
+            for (int c = 0; c < NC; ++c) sh[c] = A.center ? cmean[c] : 0.f;
+            if (threadIdx.x == 0) {
+#pragma unroll
+                for (int c = 0; c < NC; ++c) {
+                    if (c < ncol) {
+                        A.mean[i0 * R + c] = A.center ? cmean[c] : (cnan[c] ? cmean[c] : 0.f);
+                        if (cnan[c]) atomicOr(A.has_nan, 1);
                     }
                 }
             }
-            block_sum_fd<2 * NC>(cs, ct, red);
+        }
+
+        // ---- pass 1b: X'X of the (centred) columns over all rows
+        {
+            float acc[K2];
+            double tot[K2];
 #pragma unroll
-            for (int c = 0; c < NC; ++c) {
-                if (cnan[c]) {
-                    cmean[c] = (float)(ct[c] / ((double)n - ct[NC + c]));
-                    float* col = xs + (size_t)c * nS;
-                    for (int k = threadIdx.x; k < n; k += blockDim.x)
-                        if (isnan(col[k])) col[k] = cmean[c];
-                }
-            }
-            __syncthreads();
-            float acc2[K2];
-            double tot2[K2];
-#pragma unroll
-            for (int u = 0; u < K2; ++u) acc2[u] = 0.f;
+            for (int u = 0; u < K2; ++u) acc[u] = 0.f;
             for (int k4 = threadIdx.x; k4 < nS4; k4 += blockDim.x) {
                 float4 v[NC];
+                const int k0 = 4 * k4;
 #pragma unroll
-                for (int c = 0; c < NC; ++c)
-                    v[c] = c < ncol ? x4[(size_t)c * nS4 + k4] : make_float4(0.f, 0.f, 0.f, 0.f);
+                for (int c = 0; c < NC; ++c) {
+                    float4 q = c < ncol ? x4[(size_t)c * nS4 + k4] : make_float4(0.f, 0.f, 0.f, 0.f);
+                    const float s0 = sh[c];
+                    q.x = k0 < n ? q.x - s0 : 0.f;          // the zero tail stays zero
+                    q.y = k0 + 1 < n ? q.y - s0 : 0.f;
+                    q.z = k0 + 2 < n ? q.z - s0 : 0.f;
+                    q.w = k0 + 3 < n ? q.w - s0 : 0.f;
+                    v[c] = q;
+                }
 #pragma unroll
                 for (int s = 0; s < SPB; ++s)
 #pragma unroll
@@ -267,40 +285,45 @@ k_snp_lean(LeanArgs A) {
 #pragma unroll
                         for (int bb = 0; bb < R; ++bb) {
                             const float4 xa = v[s * R + a], xb = v[s * R + bb];
-                            float& d = acc2[(s * R + a) * R + bb];
+                            float& d = acc[(s * R + a) * R + bb];
                             d = fmaf(xa.x, xb.x, d);
                             d = fmaf(xa.y, xb.y, d);
                             d = fmaf(xa.z, xb.z, d);
                             d = fmaf(xa.w, xb.w, d);
                         }
             }
-            block_sum_fd<K2>(acc2, tot2, red);
+            block_sum_fd<K2>(acc, tot, red);
+            if (threadIdx.x == 0)
 #pragma unroll
-            for (int u = 0; u < K2; ++u) tot[NC + u] = tot2[u];
-        }
-        if (threadIdx.x == 0) {
-#pragma unroll
-            for (int c = 0; c < NC; ++c) {
-                if (c < ncol) {
-                    A.mean[i0 * R + c] = cmean[c];
-                    if (cnan[c]) atomicOr(A.has_nan, 1);
-                }
-            }
-#pragma unroll
-            for (int u = 0; u < K2; ++u)
-                if (u < nsnp * R * R) A.D[(size_t)i0 * R * R + u] = (float)tot[NC + u];
+                for (int u = 0; u < K2; ++u)
+                    if (u < nsnp * R * R) A.D[(size_t)i0 * R * R + u] = (float)tot[u];
         }
 
         // ---- pass 2: BF16 hi/lo split, 8 elements per thread and step
         if (A.write_split) {
             const int np8 = nS / 8;
-            for (int c = 0; c < ncol; ++c) {
+#pragma unroll
+            for (int c = 0; c < NC; ++c) {
+                if (c >= ncol) break;
                 const float4* col = x4 + (size_t)c * nS4;
                 uint4* hi = reinterpret_cast<uint4*>(A.Xhi + (size_t)(i0 * R + c) * A.n_pad);
                 uint4* lo = reinterpret_cast<uint4*>(A.Xlo + (size_t)(i0 * R + c) * A.n_pad);
+                const float s0 = sh[c];
                 for (int k8 = threadIdx.x; k8 < np8; k8 += blockDim.x) {
+                    float4 p0 = col[2 * k8], p1 = col[2 * k8 + 1];
+                    if (s0 != 0.f) {
+                        const int k0 = 8 * k8;
+                        p0.x = k0 < n ? p0.x - s0 : 0.f;
+                        p0.y = k0 + 1 < n ? p0.y - s0 : 0.f;
+                        p0.z = k0 + 2 < n ? p0.z - s0 : 0.f;
+                        p0.w = k0 + 3 < n ? p0.w - s0 : 0.f;
+                        p1.x = k0 + 4 < n ? p1.x - s0 : 0.f;
+                        p1.y = k0 + 5 < n ? p1.y - s0 : 0.f;
+                        p1.z = k0 + 6 < n ? p1.z - s0 : 0.f;
+                        p1.w = k0 + 7 < n ? p1.w - s0 : 0.f;
+                    }
                     uint4 h, o;
-                    split8(col[2 * k8], col[2 * k8 + 1], h, o);
+                    split8(p0, p1, h, o);
                     hi[k8] = h;
                     lo[k8] = o;
                 }
@@ -328,7 +351,7 @@ k_snp_lean(LeanArgs A) {
                     if (kid[u] >= 0) {
                         float x[NC];
 #pragma unroll
-                        for (int c = 0; c < NC; ++c) x[c] = xs[(size_t)c * nS + kid[u]];
+                        for (int c = 0; c < NC; ++c) x[c] = xs[(size_t)c * nS + kid[u]] - sh[c];
 #pragma unroll
                         for (int s = 0; s < SPB; ++s)
 #pragma unroll

@@ -384,7 +384,7 @@ extern "C" oa_status oa_scan_dense_noalloc(const float* xl, const float* y, cons
     E.t = t;
     E.snp_base = 0;
     E.dense_ld = mb;
-    NA_CU(oa_launch_gemm_simt(r, xr, (size_t)n, mb * r, Yt, (size_t)n_pad, t, n, mean, has_nan, E, st));
+    NA_CU(oa_launch_gemm_simt(r, xr, (size_t)n, mb * r, Yt, (size_t)n_pad, t, n, mean, has_nan, 0, E, st));
     unsigned long long hc[4];
     NA_CU(cudaMemcpyAsync(hc, counters, sizeof hc, cudaMemcpyDeviceToHost, st));
     NA_CU(cudaStreamSynchronize(st));

@@ -60,6 +60,7 @@ struct StatsArgs {
     __nv_bfloat16* Xhi;  // [mb*r][n_pad] or null (tensor-core form)
     __nv_bfloat16* Xlo;
     int write_split;
+    int center;          // take each column relative to its mean (valid when XL holds an intercept)
     int nbuf;            // column buffers (2: the next group streams in during this one)
     int* err;            // set if a staging copy did not complete in time
 };
@@ -121,6 +122,7 @@ k_snp_stats(StatsArgs A) {
     __shared__ __align__(8) uint64_t mbar[2];
     __shared__ int fsing[8];
     __shared__ float cmean[8];
+    __shared__ float cshift[8];
     __shared__ int cnan[8];
     __shared__ int stop;
 
@@ -213,8 +215,9 @@ k_snp_stats(StatsArgs A) {
             const double cnt = vs[8 + c];
             const float mean = (float)(vs[c] / ((double)n - cnt));
             cmean[c] = mean;
+            cshift[c] = A.center ? mean : 0.f;
             cnan[c] = cnt > 0.0 ? 1 : 0;
-            A.mean[i0 * R + c] = cnt > 0.0 ? mean : 0.0f;
+            A.mean[i0 * R + c] = (A.center || cnt > 0.0) ? mean : 0.0f;
             if (cnt > 0.0) atomicOr(A.has_nan, 1);
         }
         __syncthreads();
@@ -233,6 +236,7 @@ k_snp_stats(StatsArgs A) {
             const int np8 = A.n_pad / 8;
             for (int c = 0; c < ncol; ++c) {
                 const float* col = xs + (size_t)c * nS;
+                const float s0 = cshift[c];
                 uint4* hi = reinterpret_cast<uint4*>(A.Xhi + (size_t)(i0 * R + c) * A.n_pad);
                 uint4* lo = reinterpret_cast<uint4*>(A.Xlo + (size_t)(i0 * R + c) * A.n_pad);
                 for (int k8 = threadIdx.x; k8 < np8; k8 += blockDim.x) {
@@ -240,7 +244,7 @@ k_snp_stats(StatsArgs A) {
 #pragma unroll
                     for (int u = 0; u < 4; ++u) {
                         const int k = k8 * 8 + 2 * u;
-                        const float v0 = k < n ? col[k] : 0.f, v1 = k + 1 < n ? col[k + 1] : 0.f;
+                        const float v0 = k < n ? col[k] - s0 : 0.f, v1 = k + 1 < n ? col[k + 1] - s0 : 0.f;
                         const __nv_bfloat16 h0 = __float2bfloat16_rn(v0), h1 = __float2bfloat16_rn(v1);
                         const __nv_bfloat16 l0 = __float2bfloat16_rn(v0 - __bfloat162float(h0));
                         const __nv_bfloat16 l1 = __float2bfloat16_rn(v1 - __bfloat162float(h1));
@@ -270,7 +274,7 @@ k_snp_stats(StatsArgs A) {
                 if (s < nsnp) {
                     float x[R];
 #pragma unroll
-                    for (int a = 0; a < R; ++a) x[a] = xs[(size_t)(s * R + a) * nS + k];
+                    for (int a = 0; a < R; ++a) x[a] = xs[(size_t)(s * R + a) * nS + k] - cshift[s * R + a];
                     float* ac = acc + s * NA;
 #pragma unroll
                     for (int a = 0; a < R; ++a)
@@ -343,7 +347,7 @@ k_snp_stats(StatsArgs A) {
                         if (s < nsnp) {
                             float x[R];
 #pragma unroll
-                            for (int a = 0; a < R; ++a) x[a] = xs[(size_t)(s * R + a) * nS + k];
+                            for (int a = 0; a < R; ++a) x[a] = xs[(size_t)(s * R + a) * nS + k] - cshift[s * R + a];
                             float* ac = acc + s * NA;
 #pragma unroll
                             for (int a = 0; a < R; ++a)
