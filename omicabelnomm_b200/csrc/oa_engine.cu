@@ -15,6 +15,7 @@
 #include <cstdio>
 #include <cstring>
 #include <map>
+#include <mutex>
 #include <string>
 #include <thread>
 #include <tuple>
@@ -66,18 +67,31 @@ inline void clear_stale_error(const char* where) {
         if (s_ != OA_OK) return s_;    \
     } while (0)
 
+// Stream on which the calling thread's engine allocates: device buffers use
+// the stream-ordered allocator (cudaMallocAsync / cudaFreeAsync on the
+// engine's stream), so one engine growing a buffer never waits for, or
+// stalls, the work of other engines on the same GPU.
+thread_local cudaStream_t g_alloc_stream = nullptr;
+
+struct AllocOn {   // scope in which an entry point allocates on its engine's stream
+    cudaStream_t prev;
+    explicit AllocOn(cudaStream_t s) : prev(g_alloc_stream) { g_alloc_stream = s; }
+    ~AllocOn() { g_alloc_stream = prev; }
+};
+
 template <class T>
 struct DBuf {
     T* p = nullptr;
     size_t n = 0;
     oa_status ensure(size_t cnt) {
         if (cnt <= n && p) return OA_OK;
-        if (p) cudaFree(p);
+        if (p) cudaFreeAsync(p, g_alloc_stream);
         p = nullptr;
         n = 0;
         if (cnt == 0) cnt = 1;
-        if (cudaMalloc(&p, cnt * sizeof(T)) != cudaSuccess) {
+        if (cudaMallocAsync(reinterpret_cast<void**>(&p), cnt * sizeof(T), g_alloc_stream) != cudaSuccess) {
             cudaGetLastError();
+            p = nullptr;
             set_err("device allocation of %zu bytes failed", cnt * sizeof(T));
             return OA_ERR_NOMEM;
         }
@@ -85,7 +99,7 @@ struct DBuf {
         return OA_OK;
     }
     void release() {
-        if (p) cudaFree(p);
+        if (p) cudaFreeAsync(p, g_alloc_stream);
         p = nullptr;
         n = 0;
     }
@@ -502,9 +516,26 @@ oa_status set_traits_impl(oa_engine* e, const float* y, int32_t t, bool device_p
 // the first time a trait block needs it.
 oa_status lean_plan(oa_engine* e);
 
+// Default SNPs per chunk: about 16,384/r, rounded so that the tensor-core
+// GEMM's 128 x 256 tiles fill whole waves of the persistent grid (one CTA
+// per SM): the M-tile count is a multiple of sm_count / gcd(sm_count, N-tiles).
+int wave_chunk(const oa_engine* e) {
+    const int r = e->r;
+    const int n_tiles = std::max(1, (std::max(e->t, 1) + 255) / 256);
+    int a = e->sm_count, b = n_tiles;
+    while (b) {
+        const int q = a % b;
+        a = b;
+        b = q;
+    }
+    const int unit = e->sm_count / a;                       // M-tiles per whole number of waves
+    const int mt = std::max(unit, (16384 / r * r / 128 + unit - 1) / unit * unit);
+    return mt * 128 / r;
+}
+
 oa_status prepare_tuning(oa_engine* e) {
     const int t = e->t, l = e->l, n = e->n;
-    e->chunk = std::min(e->cfg.max_snps, e->req.chunk_snps > 0 ? e->req.chunk_snps : 16384 / e->r);
+    e->chunk = std::min(e->cfg.max_snps, e->req.chunk_snps > 0 ? e->req.chunk_snps : wave_chunk(e));
     e->variant = e->req.gemm_variant == 2 ? 2 : 1;
     e->raster = e->req.gemm_raster == 2 ? 2 : 1;
     e->lean_spb = e->req.lean_spb > 0 ? std::min(e->req.lean_spb, 8 / e->r) : 0;
@@ -804,8 +835,10 @@ template <int R>
 oa_status gemm_dispatch(oa_engine* e, const float* X, int mbc, int snp_base) {
     EpiArgs E = epi_args(e, mbc, snp_base);
     if (e->cfg.precision == OA_PLAIN_FP32) {
+        // X'y~ does not change when a column is shifted (y~ is orthogonal to the intercept on the
+        // observed rows): the main GEMM reads the dosages as they are, imputing NaN only
         OA_CU(oa_launch_gemm_simt(R, X, (size_t)e->n, mbc * R, e->Yt.p, (size_t)e->n_pad, e->t, e->n, e->mean.p,
-                                  e->has_nan.p, e->center ? 1 : 0, E, e->st));
+                                  e->has_nan.p, 0, E, e->st));
         e->last_name = "k_gemm_simt";
     } else {
         OA_CU(oa_launch_gemm_tc(R, e->variant, e->raster, e->Xhi.p, e->Xlo.p, mbc * R, e->Yhi.p, e->Ylo.p, e->t,
@@ -900,8 +933,7 @@ oa_status enqueue_block(oa_engine* e, const float* xr, int mb, bool host_input, 
         return OA_OK;
     };
     if (host_input) OA_CHECK(issue_copy(0));
-    const bool cov = e->cfg.disp_cov != 0;
-    if (cov) OA_CHECK(e->marks.ensure(nch));
+    const bool cov = e->cfg.disp_cov != 0;   // e->marks holds nch entries (allocated before any capture)
     for (int c = 0; c < nch; ++c) {
         const int c0 = c * e->chunk, mbc = std::min(e->chunk, mb - c0);
         const float* X = nullptr;
@@ -1065,8 +1097,13 @@ oa_status run_snps_impl(oa_engine* e, const float* xr, int32_t mb, bool host_inp
         }
         OA_CHECK(e->Xstage[0].ensure((size_t)e->chunk * e->r * e->n));
     }
-    if (host_input)
-        for (int b = 0; b < 2; ++b) OA_CHECK(e->Xstage[b].ensure((size_t)e->chunk * e->r * e->n));
+    if (host_input) {
+        for (int b = 0; b < 2; ++b) {
+            OA_CHECK(e->Xstage[b].ensure((size_t)e->chunk * e->r * e->n));
+            OA_CU(cudaEventRecord(e->ev_used[b], e->st));   // the copy stream starts after the allocation
+        }
+    }
+    if (e->cfg.disp_cov) OA_CHECK(e->marks.ensure((mb + e->chunk - 1) / e->chunk));
     OA_CHECK(run_block<R>(e, xr, mb, host_input));
     unsigned long long cnt[3];
     OA_CU(cudaMemcpyAsync(cnt, e->counters.p, sizeof cnt, cudaMemcpyDeviceToHost, e->st));
@@ -1175,6 +1212,7 @@ oa_status run_snps_any(oa_engine* e, const float* xr, int32_t mb, bool host_inpu
         return OA_ERR_ARG;
     }
     OA_CU(cudaSetDevice(e->cfg.device));
+    AllocOn alloc_on(e->st);
     switch (e->r) {
         case 1: return run_snps_impl<1>(e, xr, mb, host_input, results_on_host, out);
         case 2: return run_snps_impl<2>(e, xr, mb, host_input, results_on_host, out);
@@ -1213,7 +1251,7 @@ oa_status autotune_impl(oa_engine* e, const float* xr, int mb, oa_tuning* best_o
     // a chunk size set before the call is kept (the caller's block size)
     const bool fixed_chunk = e->req.chunk_snps > 0;
     oa_tuning best{};
-    best.chunk_snps = fixed_chunk ? std::min(mb, e->req.chunk_snps) : std::min(mb, 16384 / r);
+    best.chunk_snps = fixed_chunk ? std::min(mb, e->req.chunk_snps) : std::min(mb, wave_chunk(e));
     best.gemm_variant = 1;
     best.gemm_raster = 1;
     OA_CHECK(prepare_tuning(e));
@@ -1255,6 +1293,9 @@ oa_status autotune_impl(oa_engine* e, const float* xr, int mb, oa_tuning* best_o
     }
     if (!fixed_chunk) {
         std::vector<int> chunks;
+        const int w = wave_chunk(e);
+        for (int c : {w / 2, w, 2 * w})
+            if (c > 0 && c <= mb) chunks.push_back(c);
         for (int c = 2048; c <= 32768; c *= 2)
             if (c / r <= mb) chunks.push_back(c / r);
         try_field(&oa_tuning::chunk_snps, chunks);
@@ -1351,9 +1392,25 @@ oa_status oa_engine_create(const oa_config* cfg, oa_engine** out) {
     cudaEventCreate(&e->k1);
     cudaEventCreate(&e->s0);
     cudaEventCreate(&e->s1);
-    if (e->counters.ensure(4) != OA_OK) {
-        delete e;
-        return OA_ERR_NOMEM;
+    {   // freed engine memory stays in the device's pool for the next allocation (no device-wide sync)
+        static std::mutex mu;
+        static bool done[64];
+        std::lock_guard<std::mutex> g(mu);
+        if (!done[cfg->device & 63]) {
+            cudaMemPool_t pool;
+            uint64_t keep = ~0ull;
+            if (cudaDeviceGetDefaultMemPool(&pool, cfg->device) == cudaSuccess)
+                cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+            cudaGetLastError();
+            done[cfg->device & 63] = true;
+        }
+    }
+    {
+        AllocOn alloc_on(e->st);
+        if (e->counters.ensure(4) != OA_OK) {
+            delete e;
+            return OA_ERR_NOMEM;
+        }
     }
     *out = e;
     return OA_OK;
@@ -1362,9 +1419,17 @@ oa_status oa_engine_create(const oa_config* cfg, oa_engine** out) {
 oa_status oa_engine_destroy(oa_engine* e) {
     if (!e) return OA_OK;
     cudaSetDevice(e->cfg.device);
-    cudaStreamSynchronize(e->st);
     cudaStreamSynchronize(e->cp);
-    for_each_buf(e, [](auto& b) { b.release(); });
+    {
+        AllocOn alloc_on(e->st);
+        for_each_buf(e, [](auto& b) { b.release(); });
+    }
+    cudaStreamSynchronize(e->st);
+    {   // return the pool's unused memory to the device
+        cudaMemPool_t pool;
+        if (cudaDeviceGetDefaultMemPool(&pool, e->cfg.device) == cudaSuccess) cudaMemPoolTrimTo(pool, 0);
+        cudaGetLastError();
+    }
     if (e->h_rec) cudaFreeHost(e->h_rec);
     if (e->h_cov) cudaFreeHost(e->h_cov);
     for (int b = 0; b < 2; ++b) {
@@ -1391,6 +1456,7 @@ oa_status oa_set_covariates(oa_engine* e, const float* xl) {
         return OA_ERR_ARG;
     }
     OA_CU(cudaSetDevice(e->cfg.device));
+    AllocOn alloc_on(e->st);
     const int n = e->n, l = e->l;
     std::vector<double> A((size_t)n * l), Q, R;
     for (size_t q = 0; q < A.size(); ++q) {
@@ -1424,14 +1490,16 @@ oa_status oa_set_covariates(oa_engine* e, const float* xl) {
     OA_CHECK(e->Q64.ensure((size_t)n * l));
     OA_CHECK(e->Qr.ensure(Qr.size()));
     OA_CHECK(e->Rinv.ensure((size_t)l * l));
-    OA_CU(cudaMemcpy(e->Q64.p, Q.data(), sizeof(double) * Q.size(), cudaMemcpyHostToDevice));
-    OA_CU(cudaMemcpy(e->Qr.p, Qr.data(), sizeof(float) * Qr.size(), cudaMemcpyHostToDevice));
-    OA_CU(cudaMemcpy(e->Rinv.p, Ri.data(), sizeof(double) * Ri.size(), cudaMemcpyHostToDevice));
+    OA_CU(cudaMemcpyAsync(e->Q64.p, Q.data(), sizeof(double) * Q.size(), cudaMemcpyHostToDevice, e->st));
+    OA_CU(cudaMemcpyAsync(e->Qr.p, Qr.data(), sizeof(float) * Qr.size(), cudaMemcpyHostToDevice, e->st));
+    OA_CU(cudaMemcpyAsync(e->Rinv.p, Ri.data(), sizeof(double) * Ri.size(), cudaMemcpyHostToDevice, e->st));
+    OA_CU(cudaStreamSynchronize(e->st));
     // An intercept as the first covariate makes every quantity of the scan
     // invariant to shifting a SNP column by a constant (its Q column is
     // proportional to 1 and the other Q columns are orthogonal to 1); the
     // kernels then work with x - mean, whose sums cancel far less.
-    e->center = xl[0] != 0.f;
+    const char* ce = getenv("OA_CENTER");
+    e->center = xl[0] != 0.f && !(ce && ce[0] == '0');
     for (int k = 1; k < n && e->center; ++k) e->center = xl[k] == xl[0];
     e->have_cov = true;
     e->t = 0;
@@ -1445,6 +1513,7 @@ oa_status oa_set_traits(oa_engine* e, const float* y, int32_t t) {
         return OA_ERR_ARG;
     }
     OA_CU(cudaSetDevice(e->cfg.device));
+    AllocOn alloc_on(e->st);
     return set_traits_impl(e, y, t, false);
 }
 
@@ -1455,6 +1524,7 @@ oa_status oa_set_traits_device(oa_engine* e, const float* y, int32_t t) {
         return OA_ERR_ARG;
     }
     OA_CU(cudaSetDevice(e->cfg.device));
+    AllocOn alloc_on(e->st);
     return set_traits_impl(e, y, t, true);
 }
 
@@ -1502,6 +1572,7 @@ oa_status oa_autotune(oa_engine* e, const float* xr_dev, int32_t mb, oa_tuning* 
         return OA_ERR_ARG;
     }
     OA_CU(cudaSetDevice(e->cfg.device));
+    AllocOn alloc_on(e->st);
     return autotune_impl(e, xr_dev, mb, best);
 }
 
@@ -1512,6 +1583,7 @@ oa_status oa_set_snp_rows(oa_engine* e, const int32_t* rows, int32_t n_rows, int
         return OA_ERR_ARG;
     }
     OA_CU(cudaSetDevice(e->cfg.device));
+    AllocOn alloc_on(e->st);
     drop_graph(e);
     ++e->tune_gen;
     if (!rows) {
@@ -1557,10 +1629,11 @@ oa_status oa_dense_last(oa_engine* e, float* beta, float* se, float* tstat, floa
     }
     OA_CU(cudaSetDevice(e->cfg.device));
     const size_t nd = (size_t)e->t * e->last_mb;
-    if (beta) OA_CU(cudaMemcpy(beta, e->d_beta.p, sizeof(float) * nd * e->r, cudaMemcpyDeviceToHost));
-    if (se) OA_CU(cudaMemcpy(se, e->d_se.p, sizeof(float) * nd * e->r, cudaMemcpyDeviceToHost));
-    if (tstat) OA_CU(cudaMemcpy(tstat, e->d_t.p, sizeof(float) * nd * e->r, cudaMemcpyDeviceToHost));
-    if (r2) OA_CU(cudaMemcpy(r2, e->d_r2.p, sizeof(float) * nd, cudaMemcpyDeviceToHost));
+    if (beta) OA_CU(cudaMemcpyAsync(beta, e->d_beta.p, sizeof(float) * nd * e->r, cudaMemcpyDeviceToHost, e->st));
+    if (se) OA_CU(cudaMemcpyAsync(se, e->d_se.p, sizeof(float) * nd * e->r, cudaMemcpyDeviceToHost, e->st));
+    if (tstat) OA_CU(cudaMemcpyAsync(tstat, e->d_t.p, sizeof(float) * nd * e->r, cudaMemcpyDeviceToHost, e->st));
+    if (r2) OA_CU(cudaMemcpyAsync(r2, e->d_r2.p, sizeof(float) * nd, cudaMemcpyDeviceToHost, e->st));
+    OA_CU(cudaStreamSynchronize(e->st));
     return OA_OK;
 }
 

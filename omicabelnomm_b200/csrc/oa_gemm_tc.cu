@@ -32,6 +32,7 @@ constexpr int BM = 128;
 constexpr int EPI_WARPS = 4;
 constexpr int NUM_THREADS = 64 + 32 * EPI_WARPS;         // 192
 constexpr int STG_STRIDE = 33;                           // epilogue staging row (conflict-free)
+constexpr int PF_BLOCKS = 16;                            // A-operand K-blocks prefetched into L2 ahead
 constexpr unsigned long long WAIT_NS = 2000000000ull;
 
 // Pipeline shape: K-block width BK (64 -> 128-byte swizzle, 32 -> 64-byte
@@ -100,6 +101,16 @@ __device__ __forceinline__ void mbar_drain(uint64_t* b, uint32_t parity) {
     const unsigned long long t0 = gtimer();
     while (!mbar_try(b, parity) && gtimer() - t0 < WAIT_NS) {
     }
+}
+
+// L2 prefetch of one tile box (no shared memory, no barrier): the A operand
+// streams from DRAM, and prefetching it well ahead of the stage loads keeps
+// DRAM latency off the pipeline without more shared-memory stages.
+__device__ __forceinline__ void tma_prefetch_2d(const CUtensorMap* map, int x, int y) {
+    asm volatile("cp.async.bulk.prefetch.tensor.2d.L2.global.tile [%0, {%1, %2}];" ::"l"(
+                     reinterpret_cast<uint64_t>(map)),
+                 "r"(x), "r"(y)
+                 : "memory");
 }
 
 __device__ __forceinline__ void tma_load_2d(const CUtensorMap* map, uint64_t* bar, void* dst, int x, int y) {
@@ -211,6 +222,19 @@ k_gemm_tc(const __grid_constant__ CUtensorMap mAhi, const __grid_constant__ CUte
             bool pend[STAGES];
             for (int q = 0; q < STAGES; ++q) pend[q] = false;
             bool ok = true;
+            // L2 prefetch cursor, PF_BLOCKS K-blocks ahead of the stage loads (across tiles)
+            int pt = blockIdx.x, pkb = 0;
+            auto prefetch_next = [&]() {
+                if (pt >= ntiles) return;
+                const int pm0 = (raster == 2 ? pt % m_tiles : pt / n_tiles) * BM;
+                tma_prefetch_2d(&mAhi, pkb * BK, pm0);
+                tma_prefetch_2d(&mAlo, pkb * BK, pm0);
+                if (++pkb == nk) {
+                    pkb = 0;
+                    pt += gridDim.x;
+                }
+            };
+            for (int q = 0; q < PF_BLOCKS; ++q) prefetch_next();
             for (int tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x) {
                 const int m0 = (raster == 2 ? tile % m_tiles : tile / n_tiles) * BM;
                 const int n0 = (raster == 2 ? tile / m_tiles : tile % n_tiles) * BN;
@@ -224,6 +248,7 @@ k_gemm_tc(const __grid_constant__ CUtensorMap mAhi, const __grid_constant__ CUte
                     tma_load_2d(&mAlo, &full_bar[s], stage_ptr(s, 1), kb * BK, m0);
                     tma_load_2d(&mBhi, &full_bar[s], stage_ptr(s, 2), kb * BK, n0);
                     tma_load_2d(&mBlo, &full_bar[s], stage_ptr(s, 3), kb * BK, n0);
+                    prefetch_next();
                     pend[s] = true;
                     pend_par[s] = ph;
                     if (++s == STAGES) {

@@ -91,7 +91,7 @@ class Server:
     def __init__(self, geno_ptr: int, n_total: int, m_total: int, cohorts: Dict[int, Cohort], *,
                  device: int = 0, budget_bytes: int, max_slots: int = 8, precision: int = E.MIXED,
                  chunk_snps: int = 8192, min_p_store: float = 1e-3, max_snps: Optional[int] = None,
-                 engine_factory=None):
+                 engine_factory=None, t_cap_min: int = 64):
         self.geno_ptr = geno_ptr
         self.n_total = n_total
         self.m_total = m_total
@@ -107,6 +107,7 @@ class Server:
         self.peak_bytes = 0             # largest admitted + idle footprint seen
         self.evictions = 0
         self.max_bypass_s = 2.0         # later requests may pass a waiting one for this long
+        self.t_cap_min = t_cap_min      # trait capacity of a new engine (larger ones are reused more)
         self._lock = threading.Condition()
         self._idle: "OrderedDict[int, _Slot]" = OrderedDict()   # cohort -> idle engine (LRU order)
         self._active_bytes = 0
@@ -155,7 +156,7 @@ class Server:
 
     def _new_engine(self, req: Request) -> _Slot:
         c = self.cohorts[req.cohort]
-        t_cap = max(req.t, 64)
+        t_cap = max(req.t, self.t_cap_min)
         eng = self.engine_factory(c, t_cap)
         return _Slot(engine=eng, cohort=req.cohort, l=c.XL.shape[0], t_cap=t_cap)
 
@@ -252,6 +253,19 @@ class Server:
         if errors:
             raise errors[0]
         return sorted(results, key=lambda r: r.rid)
+
+    def warm(self, device=None):
+        """Create and keep an engine for every cohort (covariate factorisation,
+        buffers) by serving one 1-trait, 1000-SNP request per cohort."""
+        import torch
+        keep, reqs = [], []
+        for cid, c in self.cohorts.items():
+            y = torch.randn((1, c.rows.size), device=device if device is not None else f"cuda:{self.device}")
+            keep.append(y)
+            reqs.append(Request(rid=-1 - cid, cohort=cid, snp0=0, nsnp=min(1000, self.m_total), y_ptr=y.data_ptr(),
+                                t=1))
+        self.run(reqs, realtime=False)
+        torch.cuda.synchronize()
 
     def close(self):
         with self._lock:
