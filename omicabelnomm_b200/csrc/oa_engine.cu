@@ -308,6 +308,15 @@ struct oa_engine {
 
 namespace {
 
+// Engines alive per device (their memory stays pooled while any is alive).
+int live_engines(int device, int delta) {
+    static std::mutex mu;
+    static int count[64];
+    std::lock_guard<std::mutex> g(mu);
+    count[device & 63] += delta;
+    return count[device & 63];
+}
+
 // Every device buffer of an engine (release, footprint).
 template <class F>
 void for_each_buf(oa_engine* e, F&& f) {
@@ -536,7 +545,7 @@ int wave_chunk(const oa_engine* e) {
 oa_status prepare_tuning(oa_engine* e) {
     const int t = e->t, l = e->l, n = e->n;
     e->chunk = std::min(e->cfg.max_snps, e->req.chunk_snps > 0 ? e->req.chunk_snps : wave_chunk(e));
-    e->variant = e->req.gemm_variant == 2 ? 2 : 1;
+    e->variant = (e->req.gemm_variant >= 1 && e->req.gemm_variant <= 3) ? e->req.gemm_variant : 1;
     e->raster = e->req.gemm_raster == 2 ? 2 : 1;
     e->lean_spb = e->req.lean_spb > 0 ? std::min(e->req.lean_spb, 8 / e->r) : 0;
     e->use_pre = e->req.stats_path == 1 || (e->req.stats_path != 2 && e->c2 <= std::max(t, 256));
@@ -647,9 +656,8 @@ int lean_group(const oa_engine* e) {
         while (s * 2 <= e->lean_spb) s *= 2;
         return std::min(s, 8 / e->r);
     }
-    const size_t colb = (size_t)e->r * e->n_pad * 4;
     int s = 1;
-    while (s * 2 <= 8 / e->r && 2 * (size_t)(s * 2) * colb <= 100 * 1024) s *= 2;
+    while (s * 2 <= 8 / e->r && lean_smem_bytes(e->r, e->n_pad, s * 2, 2, 0) <= 100 * 1024) s *= 2;
     return s;
 }
 
@@ -659,11 +667,10 @@ int lean_group(const oa_engine* e) {
 oa_status lean_plan(oa_engine* e) {
     const int R = e->r;
     const size_t limit = 227 * 1024 - 1024;
-    const size_t colb = (size_t)R * e->n_pad * 4;
     int spb = lean_group(e);
     int nbuf = 2;
-    while (spb > 1 && nbuf * spb * colb > 200 * 1024) spb /= 2;
-    if (nbuf * spb * colb > 200 * 1024) nbuf = 1;
+    while (spb > 1 && lean_smem_bytes(R, e->n_pad, spb, nbuf, 0) > 200 * 1024) spb /= 2;
+    if (lean_smem_bytes(R, e->n_pad, spb, nbuf, 0) > 200 * 1024) nbuf = 1;
     const size_t base = lean_smem_bytes(R, e->n_pad, spb, nbuf, 0);
     const size_t per_item = (size_t)spb * R * R * 4;
     int max_items = 1;
@@ -1372,7 +1379,7 @@ oa_status oa_engine_create(const oa_config* cfg, oa_engine** out) {
     // environment defaults of the tuning (oa_set_tuning overrides them)
     if (const char* v = getenv("OA_CHUNK_SNPS")) e->req.chunk_snps = std::max(1, atoi(v));
     if (const char* v = getenv("OA_STATS_PATH")) e->req.stats_path = std::string(v) == "pre" ? 1 : (std::string(v) == "gather" ? 2 : 0);
-    if (const char* v = getenv("OA_TC_VARIANT")) e->req.gemm_variant = atoi(v) == 1 ? 2 : 1;
+    if (const char* v = getenv("OA_TC_VARIANT")) e->req.gemm_variant = std::min(3, std::max(0, atoi(v)));
     if (const char* v = getenv("OA_LEAN_SPB")) e->req.lean_spb = std::max(0, atoi(v));
     e->chunk = std::min(cfg->max_snps, e->req.chunk_snps > 0 ? e->req.chunk_snps : 16384 / cfg->r);
     const char* gr = getenv("OA_GRAPHS");
@@ -1412,6 +1419,7 @@ oa_status oa_engine_create(const oa_config* cfg, oa_engine** out) {
             return OA_ERR_NOMEM;
         }
     }
+    live_engines(cfg->device, +1);
     *out = e;
     return OA_OK;
 }
@@ -1425,7 +1433,7 @@ oa_status oa_engine_destroy(oa_engine* e) {
         for_each_buf(e, [](auto& b) { b.release(); });
     }
     cudaStreamSynchronize(e->st);
-    {   // return the pool's unused memory to the device
+    if (live_engines(e->cfg.device, -1) == 0) {   // the last engine on the device returns the pool's memory
         cudaMemPool_t pool;
         if (cudaDeviceGetDefaultMemPool(&pool, e->cfg.device) == cudaSuccess) cudaMemPoolTrimTo(pool, 0);
         cudaGetLastError();
@@ -1542,7 +1550,7 @@ oa_status oa_set_tuning(oa_engine* e, const oa_tuning* t) {
         set_err("null argument");
         return OA_ERR_ARG;
     }
-    if (t->chunk_snps < 0 || t->gemm_variant < 0 || t->gemm_variant > 2 || t->gemm_raster < 0 ||
+    if (t->chunk_snps < 0 || t->gemm_variant < 0 || t->gemm_variant > 3 || t->gemm_raster < 0 ||
         t->gemm_raster > 2 || t->stats_path < 0 || t->stats_path > 2 || t->lean_spb < 0 || t->lean_spb > 8) {
         set_err("tuning field out of range");
         return OA_ERR_ARG;

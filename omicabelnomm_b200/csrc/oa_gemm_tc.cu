@@ -22,6 +22,8 @@
 // its TMEM and returns.  The host turns the flag into an error.
 #include <cuda.h>
 
+#include <algorithm>
+
 #include "oa_epilogue.cuh"
 #include "oa_launch.h"
 
@@ -159,6 +161,49 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&v)[32]) {
           "=r"(v[24]), "=r"(v[25]), "=r"(v[26]), "=r"(v[27]), "=r"(v[28]), "=r"(v[29]), "=r"(v[30]), "=r"(v[31])
         : "r"(taddr));
     asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+}
+
+// Statistics epilogue of one accumulator tile for one warp: lane = row
+// (SNP column i of the block, `lead` on its first column), BN traits from
+// TMEM at taddr (32 columns per tcgen05.ld), trait constants from tps.
+template <int R, int BN>
+__device__ __forceinline__ void epi_columns(const EpiArgs& E, uint32_t taddr, int n0, int t, int lane, int i,
+                                            bool lead, const float* vx, const TraitP* tps, float* my) {
+    int cg = -1;            // pattern whose Schur inverse is cached
+    bool csing = true;
+    double S[R * R];
+    for (int c0 = 0; c0 < BN && n0 + c0 < t; c0 += 32) {
+        uint32_t v[32];
+        tmem_ld32(taddr + (uint32_t)c0, v);
+#pragma unroll
+        for (int q = 0; q < 32; ++q) my[lane * STG_STRIDE + q] = __uint_as_float(v[q]);
+        __syncwarp();
+        const int qmax = min(32, t - n0 - c0);
+        for (int q = 0; q < qmax; ++q) {
+            const int j = n0 + c0 + q;
+            const TraitP tp = tps[c0 + q];
+            const float zf = my[lane * STG_STRIDE + q];
+            float z[R];
+#pragma unroll
+            for (int a = 0; a < R; ++a) z[a] = __shfl_sync(0xffffffffu, zf, (lane & ~(R - 1)) + a);
+            if (tp.g != cg) {    // traits are sorted by pattern: reloads are rare
+                cg = tp.g;
+                csing = lead ? !load_schur<R>(E, cg, i, S) : true;
+            }
+            Rec rc;
+            bool st = false;
+            if (lead) {
+                if (csing) {
+                    atomicAdd(E.n_singular, 1ull);
+                    epi_dense_nan<R>(E, i, tp);
+                } else {
+                    st = epi_core<R>(E, i, j, z, tp, S, vx, rc);
+                }
+            }
+            epi_emit(E, st, rc);
+        }
+        __syncwarp();
+    }
 }
 
 // STORE = false: fused statistics epilogue (t = traits).  STORE = true: the
@@ -374,41 +419,8 @@ k_gemm_tc(const __grid_constant__ CUtensorMap mAhi, const __grid_constant__ CUte
             if (ok) {
                 mbar_try(&acc_full[acc], aph);
                 fence_after();
-                int cg = -1;            // pattern whose Schur inverse is cached
-                bool csing = true;
-                double S[R * R];
-                for (int c0 = 0; c0 < BN && n0 + c0 < t; c0 += 32) {
-                    uint32_t v[32];
-                    tmem_ld32(tmem_base + ((uint32_t)(lg * 32) << 16) + (uint32_t)(acc * BN + c0), v);
-#pragma unroll
-                    for (int q = 0; q < 32; ++q) my[lane * STG_STRIDE + q] = __uint_as_float(v[q]);
-                    __syncwarp();
-                    const int qmax = min(32, t - n0 - c0);
-                    for (int q = 0; q < qmax; ++q) {
-                        const int j = n0 + c0 + q;
-                        const TraitP tp = tps[c0 + q];
-                        const float zf = my[lane * STG_STRIDE + q];
-                        float z[R];
-#pragma unroll
-                        for (int a = 0; a < R; ++a) z[a] = __shfl_sync(0xffffffffu, zf, (lane & ~(R - 1)) + a);
-                        if (tp.g != cg) {    // traits are sorted by pattern: reloads are rare
-                            cg = tp.g;
-                            csing = lead ? !load_schur<R>(E, cg, i, S) : true;
-                        }
-                        Rec rc;
-                        bool st = false;
-                        if (lead) {
-                            if (csing) {
-                                atomicAdd(E.n_singular, 1ull);
-                                epi_dense_nan<R>(E, i, tp);
-                            } else {
-                                st = epi_core<R>(E, i, j, z, tp, S, vx, rc);
-                            }
-                        }
-                        epi_emit(E, st, rc);
-                    }
-                    __syncwarp();
-                }
+                epi_columns<R, BN>(E, tmem_base + ((uint32_t)(lg * 32) << 16) + (uint32_t)(acc * BN), n0, t, lane,
+                                   i, lead, vx, tps, my);
                 fence_before();
                 mbar_arrive(&acc_empty[acc]);
             }
@@ -424,6 +436,276 @@ k_gemm_tc(const __grid_constant__ CUtensorMap mAhi, const __grid_constant__ CUte
     if (warp == 1) {
         fence_after();
         asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem_base), "r"(TMEM_COLS));
+    }
+    if (threadIdx.x == 0 && abort_sh) atomicExch(err, 1);
+}
+
+// ---------------------------------------------------------------------------
+// 2-SM form of the statistics GEMM: a cluster of two CTAs on neighbouring SMs
+// computes a 256 x 256 tile with tcgen05.mma.cta_group::2 (M = 256: each CTA
+// holds 128 rows of A and of the accumulator; B is split along N, each CTA
+// staging 128 of its 256 rows).  Per SM this stages a third fewer bytes for
+// the same MMA work, so six 32-K stages fit where the 1-SM form has four.
+//   * both CTAs' producers load their halves with cp.async.bulk.tensor
+//     .cta_group::2 into their own shared memory; the bytes complete on the
+//     leader CTA's full barrier, which expects both CTAs' bytes (no
+//     multicast loads);
+//   * the leader's MMA thread issues the MMAs and commits with
+//     .multicast::cluster to both CTAs' empty / accumulator-full barriers;
+//   * each CTA's epilogue reads its own TMEM rows and releases the
+//     accumulator by arriving on the leader's accumulator-empty barrier.
+// Every wait is bounded as in the 1-SM form.
+// ---------------------------------------------------------------------------
+template <int BK_, int STAGES_>
+struct Shape2 {
+    static constexpr int BK = BK_, STAGES = STAGES_, BN = 256;
+    static constexpr int A_BYTES = BM * BK * 2;                     // this CTA's 128 rows, one of hi / lo
+    static constexpr int B_BYTES = (BN / 2) * BK * 2;               // this CTA's half of B
+    static constexpr int STAGE_BYTES = 2 * A_BYTES + 2 * B_BYTES;
+    static constexpr size_t SMEM_BYTES = 1024 + (size_t)STAGES * STAGE_BYTES +
+                                         (size_t)EPI_WARPS * 32 * STG_STRIDE * 4 + (size_t)BN * sizeof(TraitP);
+    static constexpr uint64_t LAYOUT = BK == 64 ? 2u : 4u;
+    static constexpr uint32_t SBO = BK == 64 ? 1024u : 512u;
+    static constexpr uint32_t TMEM_COLS = 512;
+    // kind::f16, D FP32, A/B BF16, K-major, N = 256, M = 256 (the CTA pair)
+    static constexpr uint32_t IDESC = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(BN >> 3) << 17) |
+                                      ((uint32_t)(256 >> 4) << 24);
+};
+
+__device__ __forceinline__ uint32_t cluster_rank() {
+    uint32_t r;
+    asm volatile("mov.u32 %0, %%cluster_ctarank;" : "=r"(r));
+    return r;
+}
+// shared::cluster address of the same shared variable in CTA `rank` of the cluster
+__device__ __forceinline__ uint32_t map_to_rank(const void* p, uint32_t rank) {
+    uint32_t out;
+    asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(out) : "r"(su32(p)), "r"(rank));
+    return out;
+}
+__device__ __forceinline__ void cluster_sync() {
+    asm volatile("barrier.cluster.arrive.release.aligned;\n\tbarrier.cluster.wait.acquire.aligned;" ::: "memory");
+}
+__device__ __forceinline__ void tma_load_2d_pair(const CUtensorMap* map, uint32_t bar_cluster, void* dst, int x, int y) {
+    asm volatile(
+        "cp.async.bulk.tensor.2d.cta_group::2.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%3, "
+        "%4}], [%2];" ::"r"(su32(dst)),
+        "l"(reinterpret_cast<uint64_t>(map)), "r"(bar_cluster), "r"(x), "r"(y)
+        : "memory");
+}
+__device__ __forceinline__ void mma_bf16_pair(uint32_t d_tmem, uint64_t a, uint64_t b, uint32_t idesc,
+                                              uint32_t accumulate) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::2.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8, %9, %10, %11, %12}, p;\n}\n" ::"r"(
+            d_tmem),
+        "l"(a), "l"(b), "r"(idesc), "r"(accumulate), "r"(0u), "r"(0u), "r"(0u), "r"(0u), "r"(0u), "r"(0u), "r"(0u),
+        "r"(0u));
+}
+// commit the leader's MMAs so far to the barrier at the same offset in both CTAs
+__device__ __forceinline__ void mma_commit_pair(uint64_t* bar) {
+    asm volatile(
+        "tcgen05.commit.cta_group::2.mbarrier::arrive::one.shared::cluster.multicast::cluster.b64 [%0], %1;" ::"r"(
+            su32(bar)),
+        "h"((uint16_t)3)
+        : "memory");
+}
+__device__ __forceinline__ void mbar_arrive_cluster(uint32_t bar_cluster) {
+    asm volatile("mbarrier.arrive.release.cluster.shared::cluster.b64 _, [%0];" ::"r"(bar_cluster) : "memory");
+}
+
+template <int R, class SH>
+__global__ void __launch_bounds__(NUM_THREADS, 1)
+k_gemm_tc2(const __grid_constant__ CUtensorMap mAhi, const __grid_constant__ CUtensorMap mAlo,
+           const __grid_constant__ CUtensorMap mBhi, const __grid_constant__ CUtensorMap mBlo, int xrows, int t,
+           int nk, EpiArgs E, int raster, int* err) {
+    constexpr int BK = SH::BK, STAGES = SH::STAGES, BN = SH::BN;
+    constexpr uint32_t TMEM_COLS = SH::TMEM_COLS;
+    constexpr int A_BYTES = SH::A_BYTES, B_BYTES = SH::B_BYTES, STAGE_BYTES = SH::STAGE_BYTES;
+    extern __shared__ uint8_t smem_raw[];
+    uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~(uintptr_t)1023);
+    float* stg = reinterpret_cast<float*>(smem + (size_t)STAGES * STAGE_BYTES);
+    TraitP* tps = reinterpret_cast<TraitP*>(stg + (size_t)EPI_WARPS * 32 * STG_STRIDE);
+    __shared__ __align__(8) uint64_t full_bar[STAGES], empty_bar[STAGES], acc_full[2], acc_empty[2], done_bar;
+    __shared__ uint32_t tmem_base_sh;
+    __shared__ volatile int abort_sh;
+
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const uint32_t rank = cluster_rank();
+    const bool leader = rank == 0;
+    const int pair = blockIdx.x >> 1, npairs = gridDim.x >> 1;
+    const int m_tiles = (xrows + 2 * BM - 1) / (2 * BM), n_tiles = (t + BN - 1) / BN;
+    const int ntiles = m_tiles * n_tiles;
+
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < STAGES; ++s) {
+            mbar_init(&full_bar[s], 1);
+            mbar_init(&empty_bar[s], 1);
+        }
+        for (int a = 0; a < 2; ++a) {
+            mbar_init(&acc_full[a], 1);
+            mbar_init(&acc_empty[a], 2 * EPI_WARPS);   // one arrival per epilogue warp of both CTAs (leader's copy)
+        }
+        mbar_init(&done_bar, 1);
+        abort_sh = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (warp == 1) {
+        asm volatile("tcgen05.alloc.cta_group::2.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(su32(&tmem_base_sh)),
+                     "r"(TMEM_COLS));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::2.sync.aligned;");
+    }
+    fence_before();
+    __syncthreads();
+    cluster_sync();       // both CTAs' barriers and TMEM exist before any remote use
+    fence_after();
+    const uint32_t tmem_base = tmem_base_sh;
+
+    auto stage_ptr = [&](int s, int which) -> uint8_t* {
+        uint8_t* b = smem + (size_t)s * STAGE_BYTES;
+        return which < 2 ? b + which * A_BYTES : b + 2 * A_BYTES + (which - 2) * B_BYTES;
+    };
+    auto tile_mn = [&](int tile, int& m0, int& n0) {
+        m0 = (raster == 2 ? tile % m_tiles : tile / n_tiles) * 2 * BM;
+        n0 = (raster == 2 ? tile / m_tiles : tile % n_tiles) * BN;
+    };
+
+    if (warp == 0) {
+        if (lane == 0) {
+            // ---------------- TMA producer (both CTAs) ----------------
+            int s = 0;
+            uint32_t ph = 0;
+            bool ok = true;
+            int pt = pair, pkb = 0;          // L2 prefetch cursor, PF_BLOCKS K-blocks ahead
+            auto prefetch_next = [&]() {
+                if (pt >= ntiles) return;
+                int pm0, pn0;
+                tile_mn(pt, pm0, pn0);
+                tma_prefetch_2d(&mAhi, pkb * BK, pm0 + (int)rank * BM);
+                tma_prefetch_2d(&mAlo, pkb * BK, pm0 + (int)rank * BM);
+                if (++pkb == nk) {
+                    pkb = 0;
+                    pt += npairs;
+                }
+            };
+            for (int q = 0; q < PF_BLOCKS; ++q) prefetch_next();
+            for (int tile = pair; tile < ntiles && ok; tile += npairs) {
+                int m0, n0;
+                tile_mn(tile, m0, n0);
+                const int ma = m0 + (int)rank * BM, nb = n0 + (int)rank * (BN / 2);
+                for (int kb = 0; kb < nk; ++kb) {
+                    if (!mbar_wait(&empty_bar[s], ph ^ 1u, &abort_sh)) {
+                        ok = false;
+                        break;
+                    }
+                    const uint32_t fb = map_to_rank(&full_bar[s], 0);
+                    if (leader) mbar_expect_tx(&full_bar[s], 2 * STAGE_BYTES);
+                    tma_load_2d_pair(&mAhi, fb, stage_ptr(s, 0), kb * BK, ma);
+                    tma_load_2d_pair(&mAlo, fb, stage_ptr(s, 1), kb * BK, ma);
+                    tma_load_2d_pair(&mBhi, fb, stage_ptr(s, 2), kb * BK, nb);
+                    tma_load_2d_pair(&mBlo, fb, stage_ptr(s, 3), kb * BK, nb);
+                    prefetch_next();
+                    if (++s == STAGES) {
+                        s = 0;
+                        ph ^= 1u;
+                    }
+                }
+            }
+            if (!ok && leader)   // the leader's full barriers see both CTAs' copies: drain them
+                for (int q = 0; q < STAGES; ++q) mbar_drain(&full_bar[q], 0), mbar_drain(&full_bar[q], 1);
+        }
+    } else if (warp == 1) {
+        if (lane == 0 && leader) {
+            // ---------------- MMA issuer (leader CTA) ----------------
+            int s = 0, acc = 0;
+            uint32_t ph = 0, aph = 0;
+            bool ok = true, issued = false;
+            for (int tile = pair; tile < ntiles && ok; tile += npairs) {
+                if (!mbar_wait(&acc_empty[acc], aph ^ 1u, &abort_sh)) break;
+                fence_after();
+                const uint32_t d_tmem = tmem_base + (uint32_t)(acc * BN);
+                for (int kb = 0; kb < nk; ++kb) {
+                    if (!mbar_wait(&full_bar[s], ph, &abort_sh)) {
+                        ok = false;
+                        break;
+                    }
+                    fence_after();
+                    const uint32_t ahi = su32(stage_ptr(s, 0)), alo = su32(stage_ptr(s, 1));
+                    const uint32_t bhi = su32(stage_ptr(s, 2)), blo = su32(stage_ptr(s, 3));
+#pragma unroll
+                    for (int kk = 0; kk < BK / 16; ++kk) {
+                        const uint32_t off = (uint32_t)kk * 32u;
+                        const uint64_t dah = smem_desc<SH>(ahi + off), dal = smem_desc<SH>(alo + off);
+                        const uint64_t dbh = smem_desc<SH>(bhi + off), dbl = smem_desc<SH>(blo + off);
+                        mma_bf16_pair(d_tmem, dah, dbh, SH::IDESC, (kb > 0 || kk > 0) ? 1u : 0u);
+                        mma_bf16_pair(d_tmem, dah, dbl, SH::IDESC, 1u);
+                        mma_bf16_pair(d_tmem, dal, dbh, SH::IDESC, 1u);
+                    }
+                    issued = true;
+                    mma_commit_pair(&empty_bar[s]);
+                    if (++s == STAGES) {
+                        s = 0;
+                        ph ^= 1u;
+                    }
+                }
+                if (!ok) break;
+                mma_commit_pair(&acc_full[acc]);
+                if (++acc == 2) {
+                    acc = 0;
+                    aph ^= 1u;
+                }
+            }
+            if (issued) mma_commit_pair(&done_bar);   // both CTAs learn when the last MMA has completed
+        }
+        if (lane == 0) mbar_drain(&done_bar, 0);      // (a CTA pair that issued nothing waits out the bound once)
+    } else {
+        // ---------------- epilogue (both CTAs, own 128 rows) ----------------
+        const int ew = warp - 2;
+        const int lg = warp & 3;
+        const int et = ew * 32 + lane;
+        float* my = stg + (size_t)ew * 32 * STG_STRIDE;
+        int acc = 0;
+        uint32_t aph = 0;
+        for (int tile = pair; tile < ntiles; tile += npairs) {
+            int m0, n0;
+            tile_mn(tile, m0, n0);
+            m0 += (int)rank * BM;
+            asm volatile("bar.sync 1, 128;" ::: "memory");
+            if (abort_sh) break;
+            for (int q = et; q < BN; q += 128)
+                if (n0 + q < t) tps[q] = load_trait(E, n0 + q);
+            const int row = m0 + lg * 32 + lane;
+            const bool lead = ((lane & (R - 1)) == 0) && (row < xrows);
+            const int i = row / R;
+            float vx[R];
+#pragma unroll
+            for (int a = 0; a < R; ++a) vx[a] = lead ? E.varx[(size_t)i * R + a] : 1.f;
+            asm volatile("bar.sync 1, 128;" ::: "memory");
+            int ok = 1;
+            if (lane == 0) ok = mbar_wait(&acc_full[acc], aph, &abort_sh) ? 1 : 0;
+            ok = __shfl_sync(0xffffffffu, ok, 0);
+            if (ok) {
+                mbar_try(&acc_full[acc], aph);
+                fence_after();
+                epi_columns<R, BN>(E, tmem_base + ((uint32_t)(lg * 32) << 16) + (uint32_t)(acc * BN), n0, t, lane,
+                                   i, lead, vx, tps, my);
+                fence_before();
+                __syncwarp();
+                if (lane == 0) mbar_arrive_cluster(map_to_rank(&acc_empty[acc], 0));
+            }
+            if (++acc == 2) {
+                acc = 0;
+                aph ^= 1u;
+            }
+        }
+    }
+
+    fence_before();
+    __syncthreads();
+    cluster_sync();       // no CTA frees TMEM or leaves while its pair may still touch it
+    if (warp == 1) {
+        fence_after();
+        asm volatile("tcgen05.dealloc.cta_group::2.sync.aligned.b32 %0, %1;" ::"r"(tmem_base), "r"(TMEM_COLS));
     }
     if (threadIdx.x == 0 && abort_sh) atomicExch(err, 1);
 }
@@ -492,13 +774,49 @@ static cudaError_t go(const __nv_bfloat16* Xhi, const __nv_bfloat16* Xlo, int xr
     return cudaGetLastError();
 }
 
-// Pipeline variant: 1 = BK 32 x 4 stages, 2 = BK 64 x 2 stages.
+template <int R, class SH>
+static cudaError_t go2(const __nv_bfloat16* Xhi, const __nv_bfloat16* Xlo, int xrows, const __nv_bfloat16* Yhi,
+                       const __nv_bfloat16* Ylo, int t, int n_pad, const EpiArgs& E, int raster, int* err,
+                       cudaStream_t st) {
+    CUtensorMap a_hi, a_lo, b_hi, b_lo;
+    if (!make_map(&a_hi, Xhi, xrows, n_pad, BM, SH::BK) || !make_map(&a_lo, Xlo, xrows, n_pad, BM, SH::BK) ||
+        !make_map(&b_hi, Yhi, t, n_pad, SH::BN / 2, SH::BK) || !make_map(&b_lo, Ylo, t, n_pad, SH::BN / 2, SH::BK))
+        return cudaErrorInvalidValue;
+    static int attr_done[64];
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (!attr_done[dev & 63]) {   // once per device, never during a stream capture
+        cudaError_t e = cudaFuncSetAttribute(k_gemm_tc2<R, SH>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             (int)SH::SMEM_BYTES);
+        if (e != cudaSuccess) return e;
+        attr_done[dev & 63] = 1;
+    }
+    const int ntiles = ((xrows + 2 * BM - 1) / (2 * BM)) * ((t + SH::BN - 1) / SH::BN);
+    const int pairs = std::min(ntiles, sm_count() / 2);
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(2 * pairs, 1, 1);
+    cfg.blockDim = dim3(NUM_THREADS, 1, 1);
+    cfg.dynamicSmemBytes = SH::SMEM_BYTES;
+    cfg.stream = st;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = 2;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, k_gemm_tc2<R, SH>, a_hi, a_lo, b_hi, b_lo, xrows, t, n_pad / SH::BK, E, raster,
+                              err);
+}
+
+// Pipeline variant: 1 = BK 32 x 4 stages, 2 = BK 64 x 2 stages, 3 = CTA pairs (2-SM MMA), BK 32 x 6 stages.
 template <int R>
 static cudaError_t go_any(int variant, int raster, const __nv_bfloat16* Xhi, const __nv_bfloat16* Xlo, int xrows,
                           const __nv_bfloat16* Yhi, const __nv_bfloat16* Ylo, int t, int n_pad, const EpiArgs& E,
                           int* err, cudaStream_t st) {
     if (variant == 2)
         return go<R, Shape<64, 2>, false>(Xhi, Xlo, xrows, Yhi, Ylo, t, n_pad, E, nullptr, 0, raster, err, st);
+    if (variant == 3) return go2<R, Shape2<32, 6>>(Xhi, Xlo, xrows, Yhi, Ylo, t, n_pad, E, raster, err, st);
     return go<R, Shape<32, 4>, false>(Xhi, Xlo, xrows, Yhi, Ylo, t, n_pad, E, nullptr, 0, raster, err, st);
 }
 

@@ -45,10 +45,13 @@ constexpr int LEAN_WARPS = LEAN_THREADS / 32;
 constexpr int LEAN_ITEM_ROWS = 256;     // rows per work item of the set pass
 
 // Shared memory of k_snp_lean: nbuf column buffers (stride n_pad floats, the
-// tail [n, n_pad) kept zero) | per-item partial sums | reduction scratch.
+// tail [n, n_pad) kept zero) | with several columns per group, the centred
+// columns interleaved by row ([n_pad][spb*R], one vector load per row in the
+// set pass) | per-item partial sums | reduction scratch.
 __host__ __device__ inline size_t lean_smem_bytes(int R, int n_pad, int spb, int nbuf, int items_cap) {
-    const int NQ = 2 * spb * R + spb * R * R;
-    return (size_t)nbuf * spb * R * n_pad * 4 + (size_t)items_cap * spb * R * R * 4 +
+    const int NC = spb * R;
+    const int NQ = 2 * NC + spb * R * R;
+    return (size_t)(nbuf + (NC > 1 ? 1 : 0)) * NC * n_pad * 4 + (size_t)items_cap * spb * R * R * 4 +
            (size_t)(LEAN_WARPS + 1) * NQ * 8 + 64;
 }
 
@@ -105,7 +108,8 @@ __device__ __forceinline__ void split8(const float4 p0, const float4 p1, uint4& 
 //   pass 2  BF16 hi/lo split of the columns (tensor-core form only)
 //   pass 3  X'X over each row set: work items of at most 256 rows of one set
 //           (fixed on the host per trait block) go round-robin to the warps;
-//           a warp's item sum (row indices prefetched, shuffle reduction)
+//           a warp's item sum (row indices prefetched, one vector load of
+//           the interleaved centred columns per row, shuffle reduction)
 //           lands in its own shared-memory slot, and a set's sum adds its
 //           items in order.  No atomics: the sums are bit-reproducible.
 template <int R, int SPB, bool BULK>
@@ -118,7 +122,8 @@ k_snp_lean(LeanArgs A) {
     const int n = A.n, nS = A.n_pad;
     const size_t buf_floats = (size_t)NC * nS;
     float* bufs = reinterpret_cast<float*>(smem_raw);                                   // [nbuf][NC][nS]
-    float* part = bufs + (size_t)A.nbuf * buf_floats;                                   // [items_cap][K2]
+    float* xi = bufs + (size_t)A.nbuf * buf_floats;                                     // [nS][NC] if NC > 1
+    float* part = xi + (NC > 1 ? (size_t)NC * nS : 0);                                   // [items_cap][K2]
     double* red = reinterpret_cast<double*>(
         (reinterpret_cast<uintptr_t>(part + (size_t)A.items_cap * K2) + 7) & ~(uintptr_t)7);   // [NWARP + 1][NQ]
     __shared__ __align__(8) uint64_t mbar[2];
@@ -278,6 +283,19 @@ k_snp_lean(LeanArgs A) {
                     q.w = k0 + 3 < n ? q.w - s0 : 0.f;
                     v[c] = q;
                 }
+                if constexpr (NC == 2) {
+                    float4* d = reinterpret_cast<float4*>(xi + (size_t)k0 * 2);   // rows k0..k0+3 x 2 columns
+                    d[0] = make_float4(v[0].x, v[1].x, v[0].y, v[1].y);
+                    d[1] = make_float4(v[0].z, v[1].z, v[0].w, v[1].w);
+                } else if constexpr (NC > 2) {
+#pragma unroll
+                    for (int c = 0; c < NC; ++c) {
+                        xi[(size_t)(k0 + 0) * NC + c] = v[c].x;
+                        xi[(size_t)(k0 + 1) * NC + c] = v[c].y;
+                        xi[(size_t)(k0 + 2) * NC + c] = v[c].z;
+                        xi[(size_t)(k0 + 3) * NC + c] = v[c].w;
+                    }
+                }
 #pragma unroll
                 for (int s = 0; s < SPB; ++s)
 #pragma unroll
@@ -351,7 +369,25 @@ k_snp_lean(LeanArgs A) {
                     if (kid[u] >= 0) {
                         float x[NC];
 #pragma unroll
-                        for (int c = 0; c < NC; ++c) x[c] = xs[(size_t)c * nS + kid[u]] - sh[c];
+                        for (int c = 0; c < NC; ++c) {
+                            if constexpr (NC == 1) {
+                                x[c] = xs[kid[u]] - sh[c];
+                            } else if constexpr (NC % 4 == 0) {
+                                if (c % 4 == 0) {
+                                    const float4 q4 = reinterpret_cast<const float4*>(xi + (size_t)kid[u] * NC)[c / 4];
+                                    x[c] = q4.x;
+                                    x[c + 1] = q4.y;
+                                    x[c + 2] = q4.z;
+                                    x[c + 3] = q4.w;
+                                }
+                            } else {
+                                if (c % 2 == 0) {
+                                    const float2 q2 = reinterpret_cast<const float2*>(xi + (size_t)kid[u] * NC)[c / 2];
+                                    x[c] = q2.x;
+                                    x[c + 1] = q2.y;
+                                }
+                            }
+                        }
 #pragma unroll
                         for (int s = 0; s < SPB; ++s)
 #pragma unroll

@@ -12,10 +12,11 @@ contiguous SNP range.  The loop
 * runs every admitted request on its own host thread and its own engine
   (own CUDA streams), so the kernels of concurrent requests overlap on the
   device; the ctypes calls release the GIL;
-* keeps one engine per cohort after its request ends (covariate
-  factorisation, row-set tables and buffers stay resident) and reuses it
-  for the next request of that cohort; idle engines are evicted, least
-  recently used first, when an admission needs their memory;
+* keeps every engine after its request ends (covariate factorisation,
+  row-set tables and buffers stay resident) and reuses it for the next
+  request of that cohort (several engines per cohort when its requests
+  overlap); idle engines are evicted, least recently used first, when an
+  admission needs their memory;
 * reports per-request latency (arrival to results on the host), queueing
   and run time, and the aggregate tests/s.
 
@@ -27,7 +28,6 @@ from __future__ import annotations
 
 import threading
 import time
-from collections import OrderedDict
 from dataclasses import dataclass, field
 from typing import Dict, List, Optional
 
@@ -109,7 +109,7 @@ class Server:
         self.max_bypass_s = 2.0         # later requests may pass a waiting one for this long
         self.t_cap_min = t_cap_min      # trait capacity of a new engine (larger ones are reused more)
         self._lock = threading.Condition()
-        self._idle: "OrderedDict[int, _Slot]" = OrderedDict()   # cohort -> idle engine (LRU order)
+        self._idle: List[_Slot] = []    # idle engines, least recently used first (several per cohort allowed)
         self._active_bytes = 0
         self._active = 0
 
@@ -132,16 +132,15 @@ class Server:
         return int(traits + sets + chunks + rows + (32 << 20))
 
     def _idle_bytes(self) -> int:
-        return sum(s.bytes for s in self._idle.values())
+        return sum(s.bytes for s in self._idle)
 
     # -- engines --------------------------------------------------------------
-    def _take_engine(self, req: Request) -> _Slot:
-        c = self.cohorts[req.cohort]
-        slot = self._idle.pop(req.cohort, None)   # caller holds the lock
-        if slot is not None and slot.t_cap >= req.t:
-            return slot
-        if slot is not None:
-            slot.engine.close()
+    def _take_engine(self, req: Request) -> Optional[_Slot]:
+        """The most recently used idle engine of the request's cohort that holds its traits (caller holds the lock)."""
+        for q in range(len(self._idle) - 1, -1, -1):
+            slot = self._idle[q]
+            if slot.cohort == req.cohort and slot.t_cap >= req.t:
+                return self._idle.pop(q)
         return None
 
     def _engine(self, cohort: Cohort, t_cap: int):
@@ -183,10 +182,7 @@ class Server:
             self._active -= 1
             self._active_bytes -= need
             if slot is not None:
-                old = self._idle.pop(slot.cohort, None)
-                if old is not None:
-                    old.engine.close()
-                self._idle[slot.cohort] = slot
+                self._idle.append(slot)
             self._lock.notify_all()
 
     # -- the loop -------------------------------------------------------------
@@ -219,12 +215,12 @@ class Server:
                         need = max(need, slot.bytes)            # the engine's memory moves from idle to active
                     # evict idle engines (least recently used first) until the request fits
                     while self._active_bytes + self._idle_bytes() + need > self.budget and self._idle:
-                        _, victim = self._idle.popitem(last=False)
+                        victim = self._idle.pop(0)
                         victim.engine.close()
                         self.evictions += 1
                     if self._active_bytes + self._idle_bytes() + need > self.budget:
                         if slot is not None:
-                            self._idle[req.cohort] = slot
+                            self._idle.append(slot)
                         if self._active == 0 and not self._idle:
                             raise E.OAError(6, f"request {req.rid} needs {need} bytes, budget {self.budget}")
                         continue
@@ -269,7 +265,7 @@ class Server:
 
     def close(self):
         with self._lock:
-            for s in self._idle.values():
+            for s in self._idle:
                 s.engine.close()
             self._idle.clear()
 

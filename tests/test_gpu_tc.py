@@ -45,3 +45,35 @@ def test_mixed_multiple_tiles_and_ragged_edges():
     _, rm, (bm, sm, tm, _) = engine_run(ds, 1, precision=E.MIXED)
     assert np.nanmax(np.abs(tp - tm)) < 1e-3
     np.testing.assert_array_equal(np.isnan(tp), np.isnan(tm))
+
+
+@pytest.mark.parametrize("case", ["r1_patterns", "r2_missing", "r1_xrnan"])
+def test_cta_pair_gemm_matches_fp64_oracle(case, monkeypatch):
+    """The 2-SM (CTA pair) form of the statistics GEMM: same bars as the 1-SM form,
+    and the same numbers as the 1-SM form to FP32 rounding."""
+    w = synth.scaled(0, **CASES[case])
+    ds = synth.generate(w)
+    res, inp, s = oracle_dense(ds, w.r)
+    monkeypatch.setenv("OA_TC_VARIANT", "3")
+    _, rows3, (b3, se3, t3, r23) = engine_run(ds, w.r, precision=E.MIXED)
+    monkeypatch.setenv("OA_TC_VARIANT", "1")
+    _, rows1, (b1, se1, t1, r21) = engine_run(ds, w.r, precision=E.MIXED)
+    D = res.dense
+    ok = ~D.singular
+    t_ref = D.tstat[:, :, res.l:][ok]
+    dt = np.abs(t3[ok] - t_ref)
+    assert np.all(dt <= T_ABS_MIXED + T_REL_MIXED * np.abs(t_ref)), f"max |dt| {dt.max():.3g}"
+    np.testing.assert_allclose(t3, t1, rtol=1e-5, atol=1e-5)
+    assert rows3.singular == rows1.singular
+
+
+def test_cta_pair_gemm_multiple_tiles_and_ragged_edges(monkeypatch):
+    """Several 256 x 256 pair tiles per cluster, t and m not multiples of 256."""
+    ds = synth.generate(synth.scaled(0, n=333, m=1301, t=517, seed=52))
+    monkeypatch.setenv("OA_TC_VARIANT", "3")
+    _, r3, (b3, s3, t3, _) = engine_run(ds, 1, precision=E.MIXED)
+    monkeypatch.setenv("OA_TC_VARIANT", "1")
+    _, r1, (b1, s1, t1, _) = engine_run(ds, 1, precision=E.MIXED)
+    np.testing.assert_allclose(t3, t1, rtol=1e-5, atol=1e-5)
+    np.testing.assert_array_equal(np.isnan(t3), np.isnan(t1))
+    np.testing.assert_array_equal(r3.trait, r1.trait)
