@@ -7,6 +7,10 @@
 #include "omicabel_b200.h"
 
 #define OA_NTHREADS 256
+
+namespace oa {
+constexpr int EMIT_BLOCK = 128;   // record slots a tensor-core epilogue warp reserves at a time
+}
 #define OA_SETS_MAX 4096   // row sets (missingness patterns + zero sets) per trait block
 
 namespace oa {
@@ -62,7 +66,8 @@ struct EpiArgs {
     int store_all;
     // outputs
     Rec* rec;
-    unsigned long long* rec_count;
+    unsigned long long* rec_count;   // record slots handed out (written rows and unused slots of reserved blocks)
+    unsigned long long* rec_valid;   // rows written (null: not counted)
     long long cap;
     unsigned long long* n_singular;
     // dense outputs (optional): beta/se/t [t][mb][r], r2 [t][mb], sig [t][mb]

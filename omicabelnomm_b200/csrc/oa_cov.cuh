@@ -93,6 +93,7 @@ k_cov_terms(const Rec* __restrict__ rec, const unsigned long long* __restrict__ 
     for (long long idx = first + blockIdx.x * (long long)blockDim.x + threadIdx.x; idx < last;
          idx += (long long)gridDim.x * blockDim.x) {
         const Rec rc = rec[idx];
+        if (rc.trait < 0) continue;   // an unused slot of a reserved block
         float b[OA_MAX_L], se[OA_MAX_L], t[OA_MAX_L];
         cov_eval<R>(C, rc.snp - snp_base, rc.tint, rc.b, rc.sig, b, se, t);
         float* o = cov + (size_t)idx * C.l * 3;

@@ -263,7 +263,8 @@ struct oa_engine {
     DBuf<Rec> rec, rec2;
     DBuf<float> cov, cov2;
     long long cap = 0;
-    DBuf<unsigned long long> counters;  // [0] rows, [1] singular, [2] significant covariate terms
+    DBuf<unsigned long long> counters;  // [0] record slots, [1] singular, [2] significant covariate terms,
+                                        // [3] pipeline error, [4] rows written
     DBuf<unsigned long long> marks;     // stored-row count at the start of each chunk's GEMM
     DBuf<unsigned long long> keys, keys2;
     DBuf<int> perm, perm2;
@@ -545,7 +546,7 @@ int wave_chunk(const oa_engine* e) {
 oa_status prepare_tuning(oa_engine* e) {
     const int t = e->t, l = e->l, n = e->n;
     e->chunk = std::min(e->cfg.max_snps, e->req.chunk_snps > 0 ? e->req.chunk_snps : wave_chunk(e));
-    e->variant = (e->req.gemm_variant >= 1 && e->req.gemm_variant <= 3) ? e->req.gemm_variant : 1;
+    e->variant = (e->req.gemm_variant >= 1 && e->req.gemm_variant <= 4) ? e->req.gemm_variant : 1;
     e->raster = e->req.gemm_raster == 2 ? 2 : 1;
     e->lean_spb = e->req.lean_spb > 0 ? std::min(e->req.lean_spb, 8 / e->r) : 0;
     e->use_pre = e->req.stats_path == 1 || (e->req.stats_path != 2 && e->c2 <= std::max(t, 256));
@@ -801,6 +802,7 @@ EpiArgs epi_args(oa_engine* e, int mbc, int snp_base) {
     E.store_all = e->cfg.store_all;
     E.rec = e->rec.p;
     E.rec_count = e->counters.p;
+    E.rec_valid = e->counters.p + 4;
     E.cap = e->cap;
     E.n_singular = e->counters.p + 1;
     E.t = e->t;
@@ -994,7 +996,7 @@ template <int R>
 oa_status run_block(oa_engine* e, const float* xr, int mb, bool host_input) {
     const int nch = (mb + e->chunk - 1) / e->chunk;
     for (int attempt = 0; attempt < 3; ++attempt) {
-        OA_CU(cudaMemsetAsync(e->counters.p, 0, 4 * sizeof(unsigned long long), e->st));
+        OA_CU(cudaMemsetAsync(e->counters.p, 0, 8 * sizeof(unsigned long long), e->st));
         bool launched = false;
         if (!host_input && e->use_graphs) {
             oa_engine::GraphKey key;
@@ -1081,10 +1083,14 @@ oa_status run_snps_impl(oa_engine* e, const float* xr, int32_t mb, bool host_inp
         // expected stored share: the two-sided normal tail beyond the |t| threshold, with headroom
         const double tail = std::erfc((double)e->cfg.min_t_store / std::sqrt(2.0));
         const double share = std::min(1.0, 1.5 * tail + 1e-3);
-        OA_CHECK(ensure_cap(e, std::max<long long>(1 << 16, e->cfg.store_all ? tests : (long long)(tests * share))));
+        // + the unused tails of the epilogue warps' reserved blocks (at most one block per warp and launch)
+        const long long nch = (mb + e->chunk - 1) / e->chunk;
+        const long long slack = nch * (long long)e->sm_count * 4 * EMIT_BLOCK;
+        OA_CHECK(ensure_cap(e, std::max<long long>(1 << 16, (e->cfg.store_all ? tests : (long long)(tests * share)) + slack)));
     }
-    if (e->cfg.store_all) OA_CHECK(ensure_cap(e, tests));
-    OA_CU(cudaMemsetAsync(e->counters.p, 0, 4 * sizeof(unsigned long long), e->st));
+    if (e->cfg.store_all)
+        OA_CHECK(ensure_cap(e, tests + (long long)((mb + e->chunk - 1) / e->chunk) * e->sm_count * 4 * EMIT_BLOCK));
+    OA_CU(cudaMemsetAsync(e->counters.p, 0, 8 * sizeof(unsigned long long), e->st));
     if (e->dense_on || e->cfg.disp_cov) {
         const size_t nd = (size_t)e->t * mb;
         OA_CHECK(e->d_beta.ensure(nd * e->r));
@@ -1112,34 +1118,36 @@ oa_status run_snps_impl(oa_engine* e, const float* xr, int32_t mb, bool host_inp
     }
     if (e->cfg.disp_cov) OA_CHECK(e->marks.ensure((mb + e->chunk - 1) / e->chunk));
     OA_CHECK(run_block<R>(e, xr, mb, host_input));
-    unsigned long long cnt[3];
+    unsigned long long cnt[5];
     OA_CU(cudaMemcpyAsync(cnt, e->counters.p, sizeof cnt, cudaMemcpyDeviceToHost, e->st));
     OA_CU(cudaStreamSynchronize(e->st));
     std::memset(out, 0, sizeof *out);
-    out->count = (int64_t)cnt[0];
+    out->count = (int64_t)cnt[4];
     out->tests = tests;
     out->singular = (int64_t)cnt[1];
     out->sig_cov_unrowed = (int64_t)cnt[2];
     if (!results_on_host) return OA_OK;
 
-    // sort the stored rows into reference order (trait, then SNP)
-    const long long N = (long long)cnt[0];
+    // sort the stored rows into reference order (trait, then SNP); unused
+    // slots of the warps' reserved blocks sort last and are dropped
+    const long long NS = (long long)cnt[0];   // slots handed out
+    const long long N = (long long)cnt[4];    // rows written
     const int l = e->l, p = e->p;
     OA_CHECK(ensure_pinned(e->h_rec, e->h_rec_cap, (size_t)N));
     if (e->cfg.disp_cov) OA_CHECK(ensure_pinned(e->h_cov, e->h_cov_cap, (size_t)N * l * 3));
     if (N > 0) {
-        OA_CHECK(e->keys.ensure(N));
-        OA_CHECK(e->keys2.ensure(N));
-        OA_CHECK(e->perm.ensure(N));
-        OA_CHECK(e->perm2.ensure(N));
+        OA_CHECK(e->keys.ensure(NS));
+        OA_CHECK(e->keys2.ensure(NS));
+        OA_CHECK(e->perm.ensure(NS));
+        OA_CHECK(e->perm2.ensure(NS));
         OA_CHECK(e->rec2.ensure(N));
-        k_rec_keys<<<(unsigned)((N + 255) / 256), 256, 0, e->st>>>(e->rec.p, N, e->keys.p, e->perm.p);
+        k_rec_keys<<<(unsigned)((NS + 255) / 256), 256, 0, e->st>>>(e->rec.p, NS, e->keys.p, e->perm.p);
         ++e->launches;
         size_t tmp = 0;
-        OA_CU(cub::DeviceRadixSort::SortPairs(nullptr, tmp, e->keys.p, e->keys2.p, e->perm.p, e->perm2.p, (int)N, 0,
+        OA_CU(cub::DeviceRadixSort::SortPairs(nullptr, tmp, e->keys.p, e->keys2.p, e->perm.p, e->perm2.p, (int)NS, 0,
                                               64, e->st));
         OA_CHECK(e->cub_tmp.ensure(tmp));
-        OA_CU(cub::DeviceRadixSort::SortPairs(e->cub_tmp.p, tmp, e->keys.p, e->keys2.p, e->perm.p, e->perm2.p, (int)N,
+        OA_CU(cub::DeviceRadixSort::SortPairs(e->cub_tmp.p, tmp, e->keys.p, e->keys2.p, e->perm.p, e->perm2.p, (int)NS,
                                               0, 64, e->st));
         if (e->cfg.disp_cov) OA_CHECK(e->cov2.ensure((size_t)N * l * 3));
         k_rec_gather<<<(unsigned)((N + 255) / 256), 256, 0, e->st>>>(e->rec.p, e->perm2.p, N, e->rec2.p,
@@ -1295,7 +1303,7 @@ oa_status autotune_impl(oa_engine* e, const float* xr, int mb, oa_tuning* best_o
         try_field(&oa_tuning::lean_spb, spbs);
     }
     if (mixed) {
-        try_field(&oa_tuning::gemm_variant, {1, 2});
+        try_field(&oa_tuning::gemm_variant, {1, 2, 3, 4});
         try_field(&oa_tuning::gemm_raster, {1, 2});
     }
     if (!fixed_chunk) {
@@ -1379,7 +1387,7 @@ oa_status oa_engine_create(const oa_config* cfg, oa_engine** out) {
     // environment defaults of the tuning (oa_set_tuning overrides them)
     if (const char* v = getenv("OA_CHUNK_SNPS")) e->req.chunk_snps = std::max(1, atoi(v));
     if (const char* v = getenv("OA_STATS_PATH")) e->req.stats_path = std::string(v) == "pre" ? 1 : (std::string(v) == "gather" ? 2 : 0);
-    if (const char* v = getenv("OA_TC_VARIANT")) e->req.gemm_variant = std::min(3, std::max(0, atoi(v)));
+    if (const char* v = getenv("OA_TC_VARIANT")) e->req.gemm_variant = std::min(4, std::max(0, atoi(v)));
     if (const char* v = getenv("OA_LEAN_SPB")) e->req.lean_spb = std::max(0, atoi(v));
     e->chunk = std::min(cfg->max_snps, e->req.chunk_snps > 0 ? e->req.chunk_snps : 16384 / cfg->r);
     const char* gr = getenv("OA_GRAPHS");
@@ -1414,7 +1422,7 @@ oa_status oa_engine_create(const oa_config* cfg, oa_engine** out) {
     }
     {
         AllocOn alloc_on(e->st);
-        if (e->counters.ensure(4) != OA_OK) {
+        if (e->counters.ensure(8) != OA_OK) {
             delete e;
             return OA_ERR_NOMEM;
         }
@@ -1550,7 +1558,7 @@ oa_status oa_set_tuning(oa_engine* e, const oa_tuning* t) {
         set_err("null argument");
         return OA_ERR_ARG;
     }
-    if (t->chunk_snps < 0 || t->gemm_variant < 0 || t->gemm_variant > 3 || t->gemm_raster < 0 ||
+    if (t->chunk_snps < 0 || t->gemm_variant < 0 || t->gemm_variant > 4 || t->gemm_raster < 0 ||
         t->gemm_raster > 2 || t->stats_path < 0 || t->stats_path > 2 || t->lean_spb < 0 || t->lean_spb > 8) {
         set_err("tuning field out of range");
         return OA_ERR_ARG;

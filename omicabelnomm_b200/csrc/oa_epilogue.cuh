@@ -167,14 +167,18 @@ __device__ __forceinline__ bool epi_eval(const EpiArgs& E, int i, int j, const f
     return epi_core<R>(E, i, j, z, tp, S, vx, rc);
 }
 
-// Warp-aggregated append of the stored rows (one atomic per warp and slot).
+// Warp-aggregated append of the stored rows: one atomic on the slot counter
+// per warp and step (the SIMT GEMM, whose epilogue runs a few steps per tile).
 __device__ __forceinline__ void epi_emit(const EpiArgs& E, bool st, const Rec& rc) {
     const unsigned m = __ballot_sync(0xffffffffu, st);
     if (!m) return;
     const int lane = threadIdx.x & 31;
     const int lead = __ffs(m) - 1;
     unsigned long long base = 0;
-    if (lane == lead) base = atomicAdd(E.rec_count, (unsigned long long)__popc(m));
+    if (lane == lead) {
+        base = atomicAdd(E.rec_count, (unsigned long long)__popc(m));
+        if (E.rec_valid) atomicAdd(E.rec_valid, (unsigned long long)__popc(m));
+    }
     base = __shfl_sync(0xffffffffu, base, lead);
     if (st) {
         const unsigned long long idx = base + __popc(m & ((1u << lane) - 1u));
@@ -185,6 +189,54 @@ __device__ __forceinline__ void epi_emit(const EpiArgs& E, bool st, const Rec& r
             for (int q = 0; q < (int)(sizeof(Rec) / 16); ++q) dst[q] = src[q];
         }
     }
+}
+
+// Record slots reserved by one warp: the tensor-core epilogues emit a few rows
+// at nearly every step, and one shared counter taking an atomic per warp and
+// step serialises them; a warp instead reserves EMIT_BLOCK slots at a time
+// (oa_common.cuh).
+struct Emitter {
+    unsigned long long base = 0;
+    int used = 0, cap = 0;
+};
+
+// Close a warp's reserved block: unused slots are marked invalid (trait -1)
+// and the rows written are counted.  All lanes of the warp take part.
+__device__ __forceinline__ void epi_retire(const EpiArgs& E, Emitter& em) {
+    if (em.cap == 0) return;
+    const int lane = threadIdx.x & 31;
+    for (int q = em.used + lane; q < em.cap; q += 32) {
+        const unsigned long long idx = em.base + (unsigned long long)q;
+        if ((long long)idx < E.cap) E.rec[idx].trait = -1;
+    }
+    if (lane == 0 && E.rec_valid && em.used > 0) atomicAdd(E.rec_valid, (unsigned long long)em.used);
+    em.used = em.cap = 0;
+}
+
+__device__ __forceinline__ void epi_emit_blocked(const EpiArgs& E, bool st, const Rec& rc, Emitter& em) {
+    if (!E.rec) return;
+    const unsigned m = __ballot_sync(0xffffffffu, st);
+    if (!m) return;
+    const int lane = threadIdx.x & 31;
+    const int k = __popc(m);
+    if (em.used + k > em.cap) {   // warp-uniform
+        epi_retire(E, em);
+        unsigned long long b = 0;
+        if (lane == 0) b = atomicAdd(E.rec_count, (unsigned long long)EMIT_BLOCK);
+        em.base = __shfl_sync(0xffffffffu, b, 0);
+        em.used = 0;
+        em.cap = EMIT_BLOCK;
+    }
+    if (st) {
+        const unsigned long long idx = em.base + (unsigned long long)(em.used + __popc(m & ((1u << lane) - 1u)));
+        if ((long long)idx < E.cap) {
+            float4* dst = reinterpret_cast<float4*>(E.rec + idx);
+            const float4* src = reinterpret_cast<const float4*>(&rc);
+#pragma unroll
+            for (int q = 0; q < (int)(sizeof(Rec) / 16); ++q) dst[q] = src[q];
+        }
+    }
+    em.used += k;
 }
 
 }  // namespace oa

@@ -168,7 +168,7 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&v)[32]) {
 // TMEM at taddr (32 columns per tcgen05.ld), trait constants from tps.
 template <int R, int BN>
 __device__ __forceinline__ void epi_columns(const EpiArgs& E, uint32_t taddr, int n0, int t, int lane, int i,
-                                            bool lead, const float* vx, const TraitP* tps, float* my) {
+                                            bool lead, const float* vx, const TraitP* tps, float* my, Emitter& em) {
     int cg = -1;            // pattern whose Schur inverse is cached
     bool csing = true;
     double S[R * R];
@@ -200,7 +200,7 @@ __device__ __forceinline__ void epi_columns(const EpiArgs& E, uint32_t taddr, in
                     st = epi_core<R>(E, i, j, z, tp, S, vx, rc);
                 }
             }
-            epi_emit(E, st, rc);
+            epi_emit_blocked(E, st, rc, em);
         }
         __syncwarp();
     }
@@ -395,6 +395,7 @@ k_gemm_tc(const __grid_constant__ CUtensorMap mAhi, const __grid_constant__ CUte
         const int lg = warp & 3;                 // TMEM lane group this warp may access
         const int et = ew * 32 + lane;           // 0..127
         float* my = stg + (size_t)ew * 32 * STG_STRIDE;
+        Emitter em;
         int acc = 0;
         uint32_t aph = 0;
         for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
@@ -420,7 +421,7 @@ k_gemm_tc(const __grid_constant__ CUtensorMap mAhi, const __grid_constant__ CUte
                 mbar_try(&acc_full[acc], aph);
                 fence_after();
                 epi_columns<R, BN>(E, tmem_base + ((uint32_t)(lg * 32) << 16) + (uint32_t)(acc * BN), n0, t, lane,
-                                   i, lead, vx, tps, my);
+                                   i, lead, vx, tps, my, em);
                 fence_before();
                 mbar_arrive(&acc_empty[acc]);
             }
@@ -429,6 +430,7 @@ k_gemm_tc(const __grid_constant__ CUtensorMap mAhi, const __grid_constant__ CUte
                 aph ^= 1u;
             }
         }
+        epi_retire(E, em);
     }
 
     fence_before();
@@ -664,6 +666,7 @@ k_gemm_tc2(const __grid_constant__ CUtensorMap mAhi, const __grid_constant__ CUt
         const int lg = warp & 3;
         const int et = ew * 32 + lane;
         float* my = stg + (size_t)ew * 32 * STG_STRIDE;
+        Emitter em;
         int acc = 0;
         uint32_t aph = 0;
         for (int tile = pair; tile < ntiles; tile += npairs) {
@@ -688,7 +691,7 @@ k_gemm_tc2(const __grid_constant__ CUtensorMap mAhi, const __grid_constant__ CUt
                 mbar_try(&acc_full[acc], aph);
                 fence_after();
                 epi_columns<R, BN>(E, tmem_base + ((uint32_t)(lg * 32) << 16) + (uint32_t)(acc * BN), n0, t, lane,
-                                   i, lead, vx, tps, my);
+                                   i, lead, vx, tps, my, em);
                 fence_before();
                 __syncwarp();
                 if (lane == 0) mbar_arrive_cluster(map_to_rank(&acc_empty[acc], 0));
@@ -698,6 +701,7 @@ k_gemm_tc2(const __grid_constant__ CUtensorMap mAhi, const __grid_constant__ CUt
                 aph ^= 1u;
             }
         }
+        epi_retire(E, em);
     }
 
     fence_before();
@@ -809,7 +813,8 @@ static cudaError_t go2(const __nv_bfloat16* Xhi, const __nv_bfloat16* Xlo, int x
                               err);
 }
 
-// Pipeline variant: 1 = BK 32 x 4 stages, 2 = BK 64 x 2 stages, 3 = CTA pairs (2-SM MMA), BK 32 x 6 stages.
+// Pipeline variant: 1 = BK 32 x 4 stages, 2 = BK 64 x 2 stages, 3 = CTA pairs (2-SM MMA), BK 32 x 6 stages,
+// 4 = CTA pairs, BK 64 x 3 stages (128-byte rows: half the TMA requests per byte).
 template <int R>
 static cudaError_t go_any(int variant, int raster, const __nv_bfloat16* Xhi, const __nv_bfloat16* Xlo, int xrows,
                           const __nv_bfloat16* Yhi, const __nv_bfloat16* Ylo, int t, int n_pad, const EpiArgs& E,
@@ -817,6 +822,7 @@ static cudaError_t go_any(int variant, int raster, const __nv_bfloat16* Xhi, con
     if (variant == 2)
         return go<R, Shape<64, 2>, false>(Xhi, Xlo, xrows, Yhi, Ylo, t, n_pad, E, nullptr, 0, raster, err, st);
     if (variant == 3) return go2<R, Shape2<32, 6>>(Xhi, Xlo, xrows, Yhi, Ylo, t, n_pad, E, raster, err, st);
+    if (variant == 4) return go2<R, Shape2<64, 3>>(Xhi, Xlo, xrows, Yhi, Ylo, t, n_pad, E, raster, err, st);
     return go<R, Shape<32, 4>, false>(Xhi, Xlo, xrows, Yhi, Ylo, t, n_pad, E, nullptr, 0, raster, err, st);
 }
 

@@ -260,7 +260,8 @@ static __global__ void k_rec_keys(const Rec* __restrict__ rec, long long N, unsi
                            int* __restrict__ perm) {
     const long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x;
     if (q >= N) return;
-    keys[q] = ((unsigned long long)(unsigned)rec[q].trait << 32) | (unsigned)rec[q].snp;
+    const int tr = rec[q].trait;   // -1: an unused slot (sorts last)
+    keys[q] = tr < 0 ? ~0ull : (((unsigned long long)(unsigned)tr << 32) | (unsigned)rec[q].snp);
     perm[q] = (int)q;
 }
 

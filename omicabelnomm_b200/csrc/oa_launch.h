@@ -24,7 +24,7 @@ cudaError_t oa_launch_pre_simt(const float* X, size_t ldx, int xrows, const floa
 cudaError_t oa_launch_gemm_simt(int R, const float* X, size_t ldx, int xrows, const float* Yt, size_t ldy, int t,
                                 int K, const float* colmean, const int* has_nan, int center, const EpiArgs& E,
                                 cudaStream_t st);
-// variant: 1 = BK 32 x 4 stages, 2 = BK 64 x 2 stages, 3 = CTA pairs (2-SM MMA) BK 32 x 6;
+// variant: 1 = BK 32 x 4 stages, 2 = BK 64 x 2 stages, 3 = CTA pairs (2-SM MMA) BK 32 x 6, 4 = pairs BK 64 x 3;
 // raster: 1 = trait tiles inner, 2 = SNP tiles inner
 cudaError_t oa_launch_gemm_tc(int R, int variant, int raster, const __nv_bfloat16* Xhi, const __nv_bfloat16* Xlo,
                               int xrows, const __nv_bfloat16* Yhi, const __nv_bfloat16* Ylo, int t, int n_pad,

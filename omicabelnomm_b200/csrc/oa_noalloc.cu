@@ -374,6 +374,7 @@ extern "C" oa_status oa_scan_dense_noalloc(const float* xl, const float* y, cons
     E.store_all = 1;
     E.rec = nullptr;
     E.rec_count = counters;
+    E.rec_valid = nullptr;
     E.cap = 0;
     E.n_singular = counters + 1;
     E.d_beta = beta;

@@ -47,14 +47,15 @@ def test_mixed_multiple_tiles_and_ragged_edges():
     np.testing.assert_array_equal(np.isnan(tp), np.isnan(tm))
 
 
+@pytest.mark.parametrize("variant", ["3", "4"])
 @pytest.mark.parametrize("case", ["r1_patterns", "r2_missing", "r1_xrnan"])
-def test_cta_pair_gemm_matches_fp64_oracle(case, monkeypatch):
+def test_cta_pair_gemm_matches_fp64_oracle(case, variant, monkeypatch):
     """The 2-SM (CTA pair) form of the statistics GEMM: same bars as the 1-SM form,
     and the same numbers as the 1-SM form to FP32 rounding."""
     w = synth.scaled(0, **CASES[case])
     ds = synth.generate(w)
     res, inp, s = oracle_dense(ds, w.r)
-    monkeypatch.setenv("OA_TC_VARIANT", "3")
+    monkeypatch.setenv("OA_TC_VARIANT", variant)
     _, rows3, (b3, se3, t3, r23) = engine_run(ds, w.r, precision=E.MIXED)
     monkeypatch.setenv("OA_TC_VARIANT", "1")
     _, rows1, (b1, se1, t1, r21) = engine_run(ds, w.r, precision=E.MIXED)
@@ -67,10 +68,11 @@ def test_cta_pair_gemm_matches_fp64_oracle(case, monkeypatch):
     assert rows3.singular == rows1.singular
 
 
-def test_cta_pair_gemm_multiple_tiles_and_ragged_edges(monkeypatch):
+@pytest.mark.parametrize("variant", ["3", "4"])
+def test_cta_pair_gemm_multiple_tiles_and_ragged_edges(variant, monkeypatch):
     """Several 256 x 256 pair tiles per cluster, t and m not multiples of 256."""
     ds = synth.generate(synth.scaled(0, n=333, m=1301, t=517, seed=52))
-    monkeypatch.setenv("OA_TC_VARIANT", "3")
+    monkeypatch.setenv("OA_TC_VARIANT", variant)
     _, r3, (b3, s3, t3, _) = engine_run(ds, 1, precision=E.MIXED)
     monkeypatch.setenv("OA_TC_VARIANT", "1")
     _, r1, (b1, s1, t1, _) = engine_run(ds, 1, precision=E.MIXED)
