@@ -107,14 +107,18 @@ struct DBuf {
 
 int pad_l(int l) { return l <= 4 ? 4 : (l <= 8 ? 8 : 16); }
 
-// Grow a pinned host buffer (page-locked so the device-to-host copy runs at full speed).
+// Pinned host buffers an engine has outgrown: freed when the engine is
+// destroyed, because cudaFreeHost waits for the whole device (every other
+// engine's work) and would stall concurrent scans if called while growing.
+// Grow a pinned host buffer (page-locked so the device-to-host copy runs at
+// full speed), doubling so that growth is rare.
 template <class T>
-oa_status ensure_pinned(T*& p, size_t& cap, size_t want) {
+oa_status ensure_pinned(T*& p, size_t& cap, size_t want, std::vector<void*>& retired) {
     if (want <= cap && p) return OA_OK;
-    if (p) cudaFreeHost(p);
+    if (p) retired.push_back(p);
     p = nullptr;
+    const size_t n = std::max<size_t>({want + want / 4, 2 * cap, 1024});
     cap = 0;
-    const size_t n = std::max<size_t>(want + want / 4, 1024);
     if (cudaMallocHost(reinterpret_cast<void**>(&p), n * sizeof(T)) != cudaSuccess) {
         cudaGetLastError();
         set_err("pinned host allocation of %zu bytes failed", n * sizeof(T));
@@ -302,6 +306,7 @@ struct oa_engine {
     size_t h_rec_cap = 0;
     float* h_cov = nullptr;
     size_t h_cov_cap = 0;
+    std::vector<void*> retired_pinned;   // outgrown pinned buffers, freed at destroy
     std::vector<int32_t> o_trait, o_snp, o_nused;
     std::vector<float> o_r2, o_b, o_se, o_t;
     std::vector<uint32_t> o_mask;
@@ -1133,8 +1138,8 @@ oa_status run_snps_impl(oa_engine* e, const float* xr, int32_t mb, bool host_inp
     const long long NS = (long long)cnt[0];   // slots handed out
     const long long N = (long long)cnt[4];    // rows written
     const int l = e->l, p = e->p;
-    OA_CHECK(ensure_pinned(e->h_rec, e->h_rec_cap, (size_t)N));
-    if (e->cfg.disp_cov) OA_CHECK(ensure_pinned(e->h_cov, e->h_cov_cap, (size_t)N * l * 3));
+    OA_CHECK(ensure_pinned(e->h_rec, e->h_rec_cap, (size_t)N, e->retired_pinned));
+    if (e->cfg.disp_cov) OA_CHECK(ensure_pinned(e->h_cov, e->h_cov_cap, (size_t)N * l * 3, e->retired_pinned));
     if (N > 0) {
         OA_CHECK(e->keys.ensure(NS));
         OA_CHECK(e->keys2.ensure(NS));
@@ -1448,6 +1453,7 @@ oa_status oa_engine_destroy(oa_engine* e) {
     }
     if (e->h_rec) cudaFreeHost(e->h_rec);
     if (e->h_cov) cudaFreeHost(e->h_cov);
+    for (void* q : e->retired_pinned) cudaFreeHost(q);
     for (int b = 0; b < 2; ++b) {
         cudaEventDestroy(e->ev_copied[b]);
         cudaEventDestroy(e->ev_used[b]);

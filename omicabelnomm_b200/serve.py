@@ -62,6 +62,7 @@ class Result:
     arrival: float
     admitted: float
     finished: float
+    phases: dict = field(default_factory=dict)   # seconds: engine (creation), traits, scan (incl. results to host)
 
     @property
     def latency(self) -> float:
@@ -163,15 +164,21 @@ class Server:
     def _serve_one(self, req: Request, need: int, slot: Optional[_Slot], t_start: float, arrival: float,
                    admitted: float, results: List[Result], errors: List[BaseException]):
         try:
+            ph = {}
+            t0 = time.perf_counter()
             if slot is None:
                 slot = self._new_engine(req)
+            t1 = time.perf_counter()
             eng = slot.engine
             eng.set_traits_device(req.y_ptr, req.t)
+            t2 = time.perf_counter()
             ptr = self.geno_ptr + 4 * req.snp0 * self.n_total
             out = eng.scan(ptr, req.nsnp)
-            finished = time.perf_counter() - t_start
+            t3 = time.perf_counter()
+            ph = {"engine": t1 - t0, "traits": t2 - t1, "scan": t3 - t2}
+            finished = t3 - t_start
             results.append(Result(rid=req.rid, rows=out, tests=req.t * req.nsnp, arrival=arrival,
-                                  admitted=admitted, finished=finished))
+                                  admitted=admitted, finished=finished, phases=ph))
             slot.bytes = eng.device_bytes()
         except BaseException as ex:  # reported to the caller of run()
             errors.append(ex)
@@ -277,7 +284,12 @@ def summarize(results: List[Result]) -> dict:
     tests = sum(r.tests for r in results)
     t0 = min(r.arrival for r in results)
     t1 = max(r.finished for r in results)
-    return {"requests": len(results), "tests": int(tests), "wall_s": t1 - t0,
+    phases = {}
+    for k in ("engine", "traits", "scan"):
+        v = np.array([r.phases.get(k, 0.0) for r in results])
+        phases[k + "_p50_ms"] = float(np.percentile(v, 50) * 1e3)
+        phases[k + "_p99_ms"] = float(np.percentile(v, 99) * 1e3)
+    return {"requests": len(results), "tests": int(tests), "wall_s": t1 - t0, "phases": phases,
             "tests_per_s": tests / (t1 - t0) if t1 > t0 else None,
             "latency_p50_ms": float(np.percentile(lat, 50) * 1e3),
             "latency_p99_ms": float(np.percentile(lat, 99) * 1e3),

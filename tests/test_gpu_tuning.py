@@ -75,6 +75,6 @@ def test_autotune_keeps_a_valid_tuning():
 def test_set_tuning_rejects_out_of_range():
     eng = E.Engine(256, 3, 1, 4, 16)
     with pytest.raises(E.OAError):
-        eng.set_tuning(gemm_variant=3)
+        eng.set_tuning(gemm_variant=5)
     with pytest.raises(E.OAError):
         eng.set_tuning(stats_path=-1)
