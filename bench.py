@@ -318,7 +318,7 @@ def serve_section(args, dev, local):
     free, _ = torch.cuda.mem_get_info(dev)
     budget = int(free - (6 << 30))
     srv = S.Server(G.data_ptr(), w.n_total, w.m_total, cohorts, device=local, budget_bytes=budget, max_slots=8,
-                   chunk_snps=8192, min_p_store=1e-3, t_cap_min=512)
+                   min_p_store=1e-3, t_cap_min=512)
     # start-up, not timed: one engine per cohort (as a server does when it loads its cohorts)
     srv.warm(dev)
     clocks = ClockSampler(local)

@@ -892,22 +892,14 @@ oa_status ensure_chunk_buffers(oa_engine* e) {
 }
 
 oa_status ensure_cap(oa_engine* e, long long want) {
+    // contents are not kept: callers grow before a block starts or before it runs again
     if (want <= e->cap) return OA_OK;
-    // keep what is already stored
-    DBuf<Rec> nr;
-    OA_CHECK(nr.ensure((size_t)want));
-    if (e->rec.p && e->cap > 0) OA_CU(cudaMemcpyAsync(nr.p, e->rec.p, sizeof(Rec) * e->cap, cudaMemcpyDeviceToDevice, e->st));
-    std::swap(e->rec, nr);
-    nr.release();
-    if (e->cfg.disp_cov) {
-        DBuf<float> nc;
-        OA_CHECK(nc.ensure((size_t)want * e->l * 3));
-        if (e->cov.p && e->cap > 0)
-            OA_CU(cudaMemcpyAsync(nc.p, e->cov.p, sizeof(float) * e->cap * e->l * 3, cudaMemcpyDeviceToDevice, e->st));
-        std::swap(e->cov, nc);
-        nc.release();
-    }
-    OA_CU(cudaStreamSynchronize(e->st));
+    want += want / 4;   // headroom, so that slightly larger requests reuse the buffer
+    e->rec.release();
+    e->cov.release();
+    e->cap = 0;
+    OA_CHECK(e->rec.ensure((size_t)want));
+    if (e->cfg.disp_cov) OA_CHECK(e->cov.ensure((size_t)want * e->l * 3));
     e->cap = want;
     return OA_OK;
 }
@@ -1084,17 +1076,17 @@ oa_status run_snps_impl(oa_engine* e, const float* xr, int32_t mb, bool host_inp
     OA_CHECK(prepare_tuning(e));
     OA_CHECK(ensure_chunk_buffers(e));
     const long long tests = (long long)mb * e->t;
-    if (e->cap == 0) {
-        // expected stored share: the two-sided normal tail beyond the |t| threshold, with headroom
+    {
+        // room for the expected stored rows (the two-sided normal tail beyond the |t| threshold, with
+        // headroom) + the unused tails of the epilogue warps' reserved blocks (at most one block per
+        // warp and launch); a block that still overflows grows the buffer and runs again
         const double tail = std::erfc((double)e->cfg.min_t_store / std::sqrt(2.0));
         const double share = std::min(1.0, 1.5 * tail + 1e-3);
-        // + the unused tails of the epilogue warps' reserved blocks (at most one block per warp and launch)
         const long long nch = (mb + e->chunk - 1) / e->chunk;
         const long long slack = nch * (long long)e->sm_count * 4 * EMIT_BLOCK;
-        OA_CHECK(ensure_cap(e, std::max<long long>(1 << 16, (e->cfg.store_all ? tests : (long long)(tests * share)) + slack)));
+        const long long rows = e->cfg.store_all ? tests : (long long)(tests * share);
+        OA_CHECK(ensure_cap(e, std::max<long long>(1 << 16, rows + slack)));
     }
-    if (e->cfg.store_all)
-        OA_CHECK(ensure_cap(e, tests + (long long)((mb + e->chunk - 1) / e->chunk) * e->sm_count * 4 * EMIT_BLOCK));
     OA_CU(cudaMemsetAsync(e->counters.p, 0, 8 * sizeof(unsigned long long), e->st));
     if (e->dense_on || e->cfg.disp_cov) {
         const size_t nd = (size_t)e->t * mb;

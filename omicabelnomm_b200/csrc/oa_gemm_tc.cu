@@ -814,11 +814,17 @@ static cudaError_t go2(const __nv_bfloat16* Xhi, const __nv_bfloat16* Xlo, int x
 }
 
 // Pipeline variant: 1 = BK 32 x 4 stages, 2 = BK 64 x 2 stages, 3 = CTA pairs (2-SM MMA), BK 32 x 6 stages,
-// 4 = CTA pairs, BK 64 x 3 stages (128-byte rows: half the TMA requests per byte).
+// 4 = CTA pairs, BK 64 x 3 stages (128-byte rows: half the TMA requests per byte).  Trait blocks of at most
+// 128 traits take a narrower N tile (64 or 128 columns, more stages) whatever the variant: a 256-column tile
+// would spend most of its MMA work on absent traits.
 template <int R>
 static cudaError_t go_any(int variant, int raster, const __nv_bfloat16* Xhi, const __nv_bfloat16* Xlo, int xrows,
                           const __nv_bfloat16* Yhi, const __nv_bfloat16* Ylo, int t, int n_pad, const EpiArgs& E,
                           int* err, cudaStream_t st) {
+    if (t <= 64)
+        return go<R, Shape<32, 8, 64>, false>(Xhi, Xlo, xrows, Yhi, Ylo, t, n_pad, E, nullptr, 0, raster, err, st);
+    if (t <= 128)
+        return go<R, Shape<32, 6, 128>, false>(Xhi, Xlo, xrows, Yhi, Ylo, t, n_pad, E, nullptr, 0, raster, err, st);
     if (variant == 2)
         return go<R, Shape<64, 2>, false>(Xhi, Xlo, xrows, Yhi, Ylo, t, n_pad, E, nullptr, 0, raster, err, st);
     if (variant == 3) return go2<R, Shape2<32, 6>>(Xhi, Xlo, xrows, Yhi, Ylo, t, n_pad, E, raster, err, st);

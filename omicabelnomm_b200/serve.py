@@ -91,7 +91,7 @@ class Server:
 
     def __init__(self, geno_ptr: int, n_total: int, m_total: int, cohorts: Dict[int, Cohort], *,
                  device: int = 0, budget_bytes: int, max_slots: int = 8, precision: int = E.MIXED,
-                 chunk_snps: int = 8192, min_p_store: float = 1e-3, max_snps: Optional[int] = None,
+                 chunk_snps: int = 0, min_p_store: float = 1e-3, max_snps: Optional[int] = None,
                  engine_factory=None, t_cap_min: int = 64):
         self.geno_ptr = geno_ptr
         self.n_total = n_total
@@ -114,6 +114,9 @@ class Server:
         self._active_bytes = 0
         self._active = 0
 
+    # largest SNP chunk an engine picks by itself (whole waves of 128-SNP tiles, about 16,384 SNPs)
+    AUTO_CHUNK_BOUND = 32768
+
     # -- memory ---------------------------------------------------------------
     def footprint(self, req: Request) -> int:
         """Upper estimate of the device bytes an engine needs for this request."""
@@ -122,7 +125,7 @@ class Server:
         l = c.XL.shape[0]
         n_pad = (n + 63) // 64 * 64
         t = req.t
-        chunk = min(self.chunk, req.nsnp)
+        chunk = min(self.chunk if self.chunk > 0 else self.AUTO_CHUNK_BOUND, req.nsnp)
         traits = t * n * 4 + t * n_pad * 8 + t * (64 + 8 * l)
         sets = l * (1 + 2 * t) * n_pad * 8 + n * 8 * 2           # B2 (+BF16) for the worst case of set counts
         chunks = chunk * n * 4 + chunk * n_pad * 4 + chunk * (l * (1 + 2 * t) + 2 * t + 16) * 8
@@ -149,7 +152,8 @@ class Server:
         n, l = cohort.rows.size, cohort.XL.shape[0]
         eng = E.Engine(n, l, 1, t_cap, self.max_snps, precision=self.precision, device=self.device,
                        min_t_store=E.t_threshold(self.min_p_store), min_r2_store=1e-6)
-        eng.set_tuning(chunk_snps=self.chunk)
+        if self.chunk > 0:
+            eng.set_tuning(chunk_snps=self.chunk)
         eng.set_covariates(cohort.XL)
         eng.set_snp_rows(cohort.rows, self.n_total)
         return eng

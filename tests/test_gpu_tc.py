@@ -51,8 +51,9 @@ def test_mixed_multiple_tiles_and_ragged_edges():
 @pytest.mark.parametrize("case", ["r1_patterns", "r2_missing", "r1_xrnan"])
 def test_cta_pair_gemm_matches_fp64_oracle(case, variant, monkeypatch):
     """The 2-SM (CTA pair) form of the statistics GEMM: same bars as the 1-SM form,
-    and the same numbers as the 1-SM form to FP32 rounding."""
-    w = synth.scaled(0, **CASES[case])
+    and the same numbers as the 1-SM form to FP32 rounding (t > 128: narrower trait
+    blocks take the 1-SM narrow tiles whatever the variant)."""
+    w = synth.scaled(0, **dict(CASES[case], t=150))
     ds = synth.generate(w)
     res, inp, s = oracle_dense(ds, w.r)
     monkeypatch.setenv("OA_TC_VARIANT", variant)
@@ -79,3 +80,16 @@ def test_cta_pair_gemm_multiple_tiles_and_ragged_edges(variant, monkeypatch):
     np.testing.assert_allclose(t3, t1, rtol=1e-5, atol=1e-5)
     np.testing.assert_array_equal(np.isnan(t3), np.isnan(t1))
     np.testing.assert_array_equal(r3.trait, r1.trait)
+
+
+@pytest.mark.parametrize("t", [1, 37, 64, 65, 128, 129])
+def test_mixed_narrow_trait_tiles(t):
+    """Trait blocks of at most 64 / 128 traits run on 64- / 128-column tiles, wider
+    ones on 256-column tiles: the same statistics as the FP32 form either side of
+    each boundary, several M tiles per CTA, ragged SNP edge."""
+    ds = synth.generate(synth.scaled(0, n=517, m=2333, t=t, l=4, miss_mode="patterns", n_patterns=3, seed=60 + t))
+    _, rp, (bp, sp, tp, _) = engine_run(ds, 1, precision=E.PLAIN)
+    _, rm, (bm, sm, tm, _) = engine_run(ds, 1, precision=E.MIXED)
+    assert np.nanmax(np.abs(tp - tm)) < 1e-3
+    np.testing.assert_array_equal(np.isnan(tp), np.isnan(tm))
+    assert rp.tests == rm.tests == t * 2333
