@@ -351,6 +351,13 @@ static __global__ void k_gather_rows(const float* __restrict__ in, long long ld,
 }
 
 // Device input of one chunk: the block itself, or its row-subset gather.
+// Mixed form with the pre-GEMM statistics path: nothing after the column
+// statistics reads the FP32 chunk (the GEMMs read its BF16 split), so a row
+// subset is gathered by the statistics kernel as it stages the columns.
+bool lean_gathers(const oa_engine* e) {
+    return e->subset && e->use_pre && e->cfg.precision == OA_MIXED_BF16X3;
+}
+
 template <int R>
 oa_status chunk_input(oa_engine* e, const float* xr, int c0, int mbc, const float** X) {
     if (!e->subset) {
@@ -708,12 +715,13 @@ oa_status lean_plan(oa_engine* e) {
 }
 
 template <int R>
-oa_status stats_pre(oa_engine* e, const float* X, int mbc) {
+oa_status stats_pre(oa_engine* e, const float* X, size_t ldx, const int* xrows, int mbc) {
     const int spb = e->lp.spb;
     const size_t smem = e->lp.smem;
     LeanArgs A{};
     A.X = X;
-    A.ldx = (size_t)e->n;
+    A.ldx = ldx;
+    A.xrows = xrows;
     A.n = e->n;
     A.n_pad = e->n_pad;
     A.mb = mbc;
@@ -774,8 +782,13 @@ oa_status stats_pre(oa_engine* e, const float* X, int mbc) {
 }
 
 template <int R>
-oa_status stats_dispatch(oa_engine* e, const float* X, int mbc) {
-    return e->use_pre ? stats_pre<R>(e, X, mbc) : stats_gather<R>(e, X, mbc);
+oa_status stats_dispatch(oa_engine* e, const float* X, size_t ldx, const int* xrows, int mbc) {
+    if (e->use_pre) return stats_pre<R>(e, X, ldx, xrows, mbc);
+    if (xrows || ldx != (size_t)e->n) {
+        set_err("internal: the gather-path statistics kernel reads gathered chunks only");
+        return OA_ERR_STATE;
+    }
+    return stats_gather<R>(e, X, mbc);
 }
 
 EpiArgs epi_args(oa_engine* e, int mbc, int snp_base) {
@@ -943,16 +956,22 @@ oa_status enqueue_block(oa_engine* e, const float* xr, int mb, bool host_input, 
     for (int c = 0; c < nch; ++c) {
         const int c0 = c * e->chunk, mbc = std::min(e->chunk, mb - c0);
         const float* X = nullptr;
+        size_t ldx = (size_t)e->n;
+        const int* xrows = nullptr;
         if (host_input) {
             if (c + 1 < nch) OA_CHECK(issue_copy(c + 1));
             OA_CU(cudaStreamWaitEvent(e->st, e->ev_copied[c & 1], 0));
             X = e->Xstage[c & 1].p;
+        } else if (lean_gathers(e)) {   // the column-statistics kernel reads the subset rows itself
+            X = xr + (size_t)c0 * R * e->x_ld;
+            ldx = e->x_ld;
+            xrows = e->xrows.p;
         } else {
             OA_CHECK(chunk_input<R>(e, xr, c0, mbc, &X));
         }
         OA_CU(cudaMemsetAsync(e->has_nan.p, 0, sizeof(int), e->st));
         OA_CU(rec(e->sev0[c]));
-        OA_CHECK(stats_dispatch<R>(e, X, mbc));
+        OA_CHECK(stats_dispatch<R>(e, X, ldx, xrows, mbc));
         OA_CU(rec(e->sev1[c]));
         if (cov) {
             k_mark<<<1, 1, 0, e->st>>>(e->counters.p, e->marks.p + c);
@@ -1105,7 +1124,7 @@ oa_status run_snps_impl(oa_engine* e, const float* xr, int32_t mb, bool host_inp
             set_err("a row subset applies to device SNP blocks only (oa_run_snps_device)");
             return OA_ERR_STATE;
         }
-        OA_CHECK(e->Xstage[0].ensure((size_t)e->chunk * e->r * e->n));
+        if (!lean_gathers(e)) OA_CHECK(e->Xstage[0].ensure((size_t)e->chunk * e->r * e->n));
     }
     if (host_input) {
         for (int b = 0; b < 2; ++b) {

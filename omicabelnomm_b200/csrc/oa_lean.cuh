@@ -21,6 +21,7 @@ namespace oa {
 struct LeanArgs {
     const float* X;       // SNP block, column c at X + c*ldx
     size_t ldx;
+    const int* xrows;     // row k of a column is X[c*ldx + xrows[k]] (a row subset), or null: X[c*ldx + k]
     int n, n_pad, mb, nbuf;
     int nsets;
     const int* rows;          // flattened row lists of the row sets
@@ -43,6 +44,7 @@ struct LeanArgs {
 constexpr int LEAN_THREADS = 512;
 constexpr int LEAN_WARPS = LEAN_THREADS / 32;
 constexpr int LEAN_ITEM_ROWS = 256;     // rows per work item of the set pass
+constexpr int LEAN_STAGE_U = 8;         // elements per thread and step of the element-wise staging
 
 // Shared memory of k_snp_lean: nbuf column buffers (stride n_pad floats, the
 // tail [n, n_pad) kept zero) | with several columns per group, the centred
@@ -97,7 +99,9 @@ __device__ __forceinline__ void split8(const float4 p0, const float4 p1, uint4& 
 
 // One CTA handles SPB SNPs (SPB*R columns) per group; a persistent loop over
 // groups with the next group's columns streaming into shared memory (TMA
-// bulk copies) while this one is processed:
+// bulk copies of aligned columns; 4-byte cp.async copies otherwise, which also
+// gather a row subset of a resident genotype matrix) while this one is
+// processed:
 //   pass 1  column sums from float4 reads of the staged columns; NaN
 //           propagates, so a column whose sum is NaN is counted and
 //           mean-imputed in place (src/Utility.cpp:302-326) - rare, dosage
@@ -150,6 +154,36 @@ k_snp_lean(LeanArgs A) {
         }
     };
 
+    // element-wise staging (columns not 16-byte aligned, or a row subset): 4-byte
+    // cp.async copies, one commit group per group of columns and thread
+    auto stage = [&](int g, int b) {
+        const int i0 = g * SPB;
+        const int ncol = min(SPB, A.mb - i0) * R;
+        for (int c = 0; c < ncol; ++c) {
+            const float* src = A.X + (size_t)(i0 * R + c) * A.ldx;
+            const uint32_t dst = st_su32(bufs + (size_t)b * buf_floats + (size_t)c * nS);
+            // LEAN_STAGE_U elements per thread and step: the row indices of a step
+            // are loaded together, so their latencies overlap
+            for (int k0 = threadIdx.x; k0 < n; k0 += LEAN_STAGE_U * LEAN_THREADS) {
+                int kk[LEAN_STAGE_U];
+#pragma unroll
+                for (int u = 0; u < LEAN_STAGE_U; ++u) {
+                    const int k = k0 + u * LEAN_THREADS;
+                    kk[u] = k < n ? (A.xrows ? __ldg(A.xrows + k) : k) : -1;
+                }
+#pragma unroll
+                for (int u = 0; u < LEAN_STAGE_U; ++u)
+                    if (kk[u] >= 0)
+                        asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(
+                                         dst + 4u * (uint32_t)(k0 + u * LEAN_THREADS)),
+                                     "l"(src + kk[u])
+                                     : "memory");
+            }
+        }
+        asm volatile("cp.async.commit_group;" ::: "memory");
+    };
+    if (!BULK && (int)blockIdx.x < ngroups) stage(blockIdx.x, 0);
+
     // zero the column tails [n, n_pad) once: copies write only [0, n)
     for (int q = threadIdx.x; q < A.nbuf * NC * (nS - n); q += blockDim.x) {
         const int c = q / (nS - n), k = n + q % (nS - n);
@@ -187,11 +221,12 @@ k_snp_lean(LeanArgs A) {
             if (stop) break;
             st_mbar_try(&mbar[b], par);
         } else {
-            for (int c = 0; c < ncol; ++c) {
-                const float* src = A.X + (size_t)(i0 * R + c) * A.ldx;
-                float* dst = xs + (size_t)c * nS;
-#pragma unroll 4
-                for (int k = threadIdx.x; k < n; k += blockDim.x) dst[k] = src[k];
+            // the next group goes into the other buffer (read completely in the previous round)
+            if (A.nbuf == 2 && gn < ngroups) {
+                stage(gn, b ^ 1);
+                asm volatile("cp.async.wait_group 1;" ::: "memory");
+            } else {
+                asm volatile("cp.async.wait_group 0;" ::: "memory");
             }
             __syncthreads();
         }
@@ -416,7 +451,9 @@ k_snp_lean(LeanArgs A) {
         }
         __syncthreads();   // every reader of this buffer is done before it is refilled
         if (BULK && A.nbuf == 1 && threadIdx.x == 0 && gn < ngroups) issue(gn, 0);
+        if (!BULK && A.nbuf == 1 && gn < ngroups) stage(gn, 0);
     }
+    if (!BULK) asm volatile("cp.async.wait_group 0;" ::: "memory");   // nothing in flight at exit
     if (BULK && threadIdx.x == 0 && stop) {
         st_mbar_wait(&mbar[0], 0);
         st_mbar_wait(&mbar[0], 1);

@@ -56,7 +56,8 @@ cudaError_t oa_launch_snp_stats(int R, int LP, const StatsArgs& A, int grid, siz
 
 template <int R, int SPB>
 static cudaError_t go_lean(const LeanArgs& A, int grid, size_t smem, cudaStream_t st) {
-    const bool bulk = (A.n % 4 == 0) && (A.ldx % 4 == 0) && ((reinterpret_cast<uintptr_t>(A.X) & 15) == 0);
+    const bool bulk = !A.xrows && (A.n % 4 == 0) && (A.ldx % 4 == 0) &&
+                      ((reinterpret_cast<uintptr_t>(A.X) & 15) == 0);
     static int set_bulk[64], set_plain[64];
     int dev = 0;
     cudaGetDevice(&dev);

@@ -98,3 +98,63 @@ def test_each_request_same_alone_and_in_the_mix(resident):
             np.testing.assert_array_equal(getattr(a, f), getattr(b, f), err_msg=f"request {res.rid} field {f}")
     s = S.summarize(mix)
     assert s["tests"] == sum(q.t * q.nsnp for q in reqs)
+
+
+@pytest.mark.parametrize("prec", [E.PLAIN, E.MIXED])
+def test_row_subset_gives_the_numbers_of_the_gathered_block(resident, prec):
+    """A scan over a row subset of the resident matrix (gathered by the
+    column-statistics kernel in the mixed form, by a gather kernel in the
+    FP32 form) returns bit-identical statistics to a scan of the gathered
+    block as a contiguous device array."""
+    import torch
+    X, Xd = resident
+    _, coh = _cohorts()
+    c = coh[2]
+    n, l = c.rows.size, c.XL.shape[0]
+    rng = np.random.Generator(np.random.PCG64(94))
+    t, s0, ln = 21, 7001, 777
+    Y = rng.normal(0, 1, (t, n)).astype(np.float32)
+    Y[rng.random((t, n)) < 0.05] = np.nan
+    y = torch.from_numpy(Y).cuda()
+    out = []
+    for subset in (True, False):
+        eng = E.Engine(n, l, 1, t, 1000, precision=prec, store_all=True, min_t_store=E.t_threshold(0.1),
+                       min_r2_store=1e-6)
+        eng.set_tuning(chunk_snps=256)
+        eng.set_covariates(c.XL)
+        eng.set_traits_device(y.data_ptr(), t)
+        eng.enable_dense(True)
+        if subset:
+            eng.set_snp_rows(c.rows, N_TOTAL)
+            eng.run_device(Xd.data_ptr() + 4 * s0 * N_TOTAL, ln)
+        else:
+            blk = torch.from_numpy(np.ascontiguousarray(X[s0:s0 + ln][:, c.rows])).cuda()
+            eng.run_device(blk.data_ptr(), ln)
+        out.append(eng.dense(ln))
+        eng.close()
+    for a, b in zip(*out):
+        np.testing.assert_array_equal(a, b)
+
+
+@pytest.mark.parametrize("prec", [E.PLAIN, E.MIXED])
+def test_single_buffered_unaligned_columns_match_oracle(prec):
+    """n = 26,003: one column buffer per CTA (two do not fit in shared memory)
+    and columns that are not 16-byte aligned (element-wise staging)."""
+    ds = synth.generate(synth.scaled(0, n=26003, m=40, t=3, seed=95))
+    l, n = ds.XL.shape
+    eng = E.Engine(n, l, 1, 3, 40, precision=prec, store_all=True, min_t_store=E.t_threshold(0.1),
+                   min_r2_store=1e-6)
+    eng.set_covariates(ds.XL)
+    eng.set_traits(ds.Y)
+    eng.enable_dense(True)
+    eng.run(ds.XR)
+    b, se, tt, r2 = eng.dense(40)
+    inp = O.Inputs(XL=ds.XL, XR=ds.XR, Y=ds.Y, xl_names=ds.xl_names, xr_names=ds.xr_names, y_names=ds.y_names,
+                   realN=n, kept=np.arange(n))
+    res = O.solve(inp, O.Settings(r=1, storePInd=True), keep_dense=True)
+    D = res.dense
+    ok = ~D.singular
+    t_ref = D.tstat[:, :, l:][ok]
+    dt = np.abs(tt[ok] - t_ref)
+    lim = (T_REL * np.abs(t_ref) + T_ABS) if prec == E.PLAIN else (1e-3 + 1e-4 * np.abs(t_ref))
+    assert np.all(dt <= lim), f"max |dt| {dt.max():.3g}"
