@@ -305,7 +305,7 @@ def serve_section(args, dev, local):
     covariates (12 cohorts), t ~ LogUniform(1, 500) traits with 0-10 %
     missingness, a contiguous range of LogUniform(10k, 1M) SNPs; mixed form,
     stored rows P < 1e-3 returned to the host; admission by device-memory
-    footprint, up to 8 requests on the GPU at once; the cohorts' engines are
+    footprint, up to 8 requests on the GPU at once; two engines per cohort are
     created at start-up (untimed)."""
     import torch
     from omicabelnomm_b200 import serve as S
@@ -319,8 +319,8 @@ def serve_section(args, dev, local):
     budget = int(free - (6 << 30))
     srv = S.Server(G.data_ptr(), w.n_total, w.m_total, cohorts, device=local, budget_bytes=budget, max_slots=8,
                    min_p_store=1e-3, t_cap_min=512)
-    # start-up, not timed: one engine per cohort (as a server does when it loads its cohorts)
-    srv.warm(dev)
+    # start-up, not timed: two engines per cohort (as a server does when it loads its cohorts)
+    srv.warm(dev, per_cohort=2)
     clocks = ClockSampler(local)
     clocks.start()
     res = srv.run(reqs, realtime=True)

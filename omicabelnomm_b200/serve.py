@@ -261,18 +261,25 @@ class Server:
             raise errors[0]
         return sorted(results, key=lambda r: r.rid)
 
-    def warm(self, device=None):
-        """Create and keep an engine for every cohort (covariate factorisation,
-        buffers) by serving one 1-trait, 1000-SNP request per cohort."""
+    def warm(self, device=None, per_cohort: int = 1):
+        """Create and keep `per_cohort` engines for every cohort (covariate
+        factorisation, buffers) by serving 1-trait, 1000-SNP requests, the
+        engines of a cohort at the same time (so that each gets its own)."""
         import torch
         keep, reqs = [], []
-        for cid, c in self.cohorts.items():
-            y = torch.randn((1, c.rows.size), device=device if device is not None else f"cuda:{self.device}")
-            keep.append(y)
-            reqs.append(Request(rid=-1 - cid, cohort=cid, snp0=0, nsnp=min(1000, self.m_total), y_ptr=y.data_ptr(),
-                                t=1))
-        self.run(reqs, realtime=False)
-        torch.cuda.synchronize()
+        for k in range(per_cohort):
+            for cid, c in self.cohorts.items():
+                y = torch.randn((1, c.rows.size), device=device if device is not None else f"cuda:{self.device}")
+                keep.append(y)
+                reqs.append(Request(rid=-1 - len(reqs), cohort=cid, snp0=0, nsnp=min(1000, self.m_total),
+                                    y_ptr=y.data_ptr(), t=1))
+        saved, self.max_slots = self.max_slots, max(self.max_slots, len(reqs))
+        try:
+            self.run(sorted(reqs, key=lambda q: q.cohort), realtime=False)
+        finally:
+            self.max_slots = saved
+        if torch.cuda.is_available():
+            torch.cuda.synchronize()
 
     def close(self):
         with self._lock:

@@ -100,3 +100,12 @@ def test_footprint_grows_with_the_request():
     small = S.Request(rid=0, cohort=0, snp0=0, nsnp=100, y_ptr=0, t=2)
     big = S.Request(rid=1, cohort=0, snp0=0, nsnp=100000, y_ptr=0, t=400)
     assert srv.footprint(big) > srv.footprint(small) > 0
+
+
+def test_warm_creates_the_engines_of_every_cohort():
+    coh, _ = _setup(cohorts=3)
+    srv = _server(coh, budget=1 << 30, slots=2)
+    srv.warm("cpu", per_cohort=2)
+    assert FakeEngine.created == 6
+    assert sorted(s.cohort for s in srv._idle) == [0, 0, 1, 1, 2, 2]
+    assert srv.max_slots == 2
