@@ -446,6 +446,7 @@ def main():
     h2d = int(xr_np.nbytes + y_np.nbytes)
     del xr_host, y_host, xr_np, y_np
     torch.cuda.empty_cache()
+    torch._C._host_emptyCache()   # unpin the 20 GB of host input (torch caches pinned blocks)
 
     batched = None
     if args.batched_m > 0:

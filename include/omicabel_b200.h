@@ -145,6 +145,16 @@ oa_status oa_set_snp_rows(oa_engine* e, const int32_t* rows, int32_t n_rows, int
 /* Device memory held by the engine's buffers, in bytes. */
 int64_t oa_device_bytes(const oa_engine* e);
 
+/* Allocates now what a trait block of up to `traits` traits and an SNP
+ * block of up to `snps` SNPs need at the engine's store thresholds
+ * (trait-sized device buffers, the stored-row buffers and their sort space
+ * on the device, the pinned host buffer the rows come back in), so that
+ * later calls within those sizes seldom allocate.  Pinned host allocations
+ * are slow while other engines keep the GPU busy: a server reserves its
+ * engines' buffers when it creates them.  No counterpart in the reference
+ * (one scan per process). */
+oa_status oa_reserve(oa_engine* e, int32_t traits, int32_t snps);
+
 /* Size of the scratch array used by oa_scan_dense_noalloc (64 MiB).  Every
  * GPU on which the library is loaded holds this much device memory until the
  * process exits. */

@@ -107,11 +107,12 @@ struct DBuf {
 
 int pad_l(int l) { return l <= 4 ? 4 : (l <= 8 ? 8 : 16); }
 
-// Pinned host buffers an engine has outgrown: freed when the engine is
-// destroyed, because cudaFreeHost waits for the whole device (every other
-// engine's work) and would stall concurrent scans if called while growing.
 // Grow a pinned host buffer (page-locked so the device-to-host copy runs at
-// full speed), doubling so that growth is rare.
+// full speed), doubling so that growth is rare.  Outgrown buffers go to
+// `retired` and are freed when the engine is destroyed: cudaFreeHost waits
+// for the whole device (every other engine's work).  Allocating pinned
+// memory is itself slow while other engines keep the GPU busy, so serving
+// engines reserve their buffers up front (oa_reserve).
 template <class T>
 oa_status ensure_pinned(T*& p, size_t& cap, size_t want, std::vector<void*>& retired) {
     if (want <= cap && p) return OA_OK;
@@ -127,6 +128,14 @@ oa_status ensure_pinned(T*& p, size_t& cap, size_t want, std::vector<void*>& ret
     cap = n;
     return OA_OK;
 }
+
+// Host-to-device copies of int tables, issued from the engine's pinned
+// staging area in one batch (the area is reused only after the stream has
+// been synchronised).
+struct H2DBatch {
+    std::vector<std::pair<int*, const std::vector<int>*>> items;
+    void add(int* dst, const std::vector<int>& v) { items.emplace_back(dst, &v); }
+};
 
 // Householder QR of the n x l column-major matrix A (FP64): Q (n x l,
 // column-major, orthonormal columns) and R (l x l, row-major upper
@@ -307,6 +316,11 @@ struct oa_engine {
     float* h_cov = nullptr;
     size_t h_cov_cap = 0;
     std::vector<void*> retired_pinned;   // outgrown pinned buffers, freed at destroy
+    // pinned staging of the small host <-> device transfers (trait grouping,
+    // row-set tables, counters): asynchronous copies that need no driver staging
+    unsigned char* stage = nullptr;
+    size_t stage_cap = 0;
+    unsigned long long* h_cnt = nullptr;   // 8 counters read back after each block
     std::vector<int32_t> o_trait, o_snp, o_nused;
     std::vector<float> o_r2, o_b, o_se, o_t;
     std::vector<uint32_t> o_mask;
@@ -372,6 +386,25 @@ oa_status chunk_input(oa_engine* e, const float* xr, int c0, int mbc, const floa
     return OA_OK;
 }
 
+oa_status stage_reserve(oa_engine* e, size_t bytes) {
+    return ensure_pinned(e->stage, e->stage_cap, bytes, e->retired_pinned);
+}
+
+oa_status flush_h2d(oa_engine* e, const H2DBatch& b) {
+    size_t total = 0;
+    for (const auto& it : b.items) total += (it.second->size() + 3) & ~size_t(3);
+    OA_CHECK(stage_reserve(e, total * sizeof(int)));
+    int* h = reinterpret_cast<int*>(e->stage);
+    for (const auto& it : b.items) {
+        const size_t k = it.second->size();
+        if (k == 0) continue;
+        std::memcpy(h, it.second->data(), k * sizeof(int));
+        OA_CU(cudaMemcpyAsync(it.first, h, k * sizeof(int), cudaMemcpyHostToDevice, e->st));
+        h += (k + 3) & ~size_t(3);
+    }
+    return OA_OK;
+}
+
 oa_status set_traits_impl(oa_engine* e, const float* y, int32_t t, bool device_ptr) {
     if (!e->have_cov) {
         set_err("oa_set_traits before oa_set_covariates");
@@ -399,10 +432,15 @@ oa_status set_traits_impl(oa_engine* e, const float* y, int32_t t, bool device_p
     OA_CU(cudaGetLastError());
     std::vector<int> counts((size_t)t * 2);
     std::vector<unsigned long long> hashes((size_t)t * 4);
-    OA_CU(cudaMemcpyAsync(counts.data(), e->tcounts.p, sizeof(int) * counts.size(), cudaMemcpyDeviceToHost, e->st));
-    OA_CU(cudaMemcpyAsync(hashes.data(), e->thash.p, sizeof(unsigned long long) * hashes.size(),
-                          cudaMemcpyDeviceToHost, e->st));
-    OA_CU(cudaStreamSynchronize(e->st));
+    {
+        const size_t hb = sizeof(unsigned long long) * hashes.size(), cb = sizeof(int) * counts.size();
+        OA_CHECK(stage_reserve(e, hb + cb));
+        OA_CU(cudaMemcpyAsync(e->stage, e->thash.p, hb, cudaMemcpyDeviceToHost, e->st));
+        OA_CU(cudaMemcpyAsync(e->stage + hb, e->tcounts.p, cb, cudaMemcpyDeviceToHost, e->st));
+        OA_CU(cudaStreamSynchronize(e->st));
+        std::memcpy(hashes.data(), e->stage, hb);
+        std::memcpy(counts.data(), e->stage + hb, cb);
+    }
 
     // group traits: missingness patterns, then sets of observed exact zeros
     std::map<std::tuple<int, unsigned long long, unsigned long long>, int> pmap, zmap;
@@ -467,14 +505,29 @@ oa_status set_traits_impl(oa_engine* e, const float* y, int32_t t, bool device_p
     OA_CHECK(e->W.ensure((size_t)std::max(e->G, 1) * l * l));
     OA_CHECK(e->zQ.ensure((size_t)std::max(e->Z, 1) * l * l));
     OA_CHECK(e->pat_bad.ensure(std::max(e->G, 1)));
-    OA_CU(cudaMemcpyAsync(e->pat.p, ipat.data(), sizeof(int) * t, cudaMemcpyHostToDevice, e->st));
-    OA_CU(cudaMemcpyAsync(e->zset.p, iz.data(), sizeof(int) * t, cudaMemcpyHostToDevice, e->st));
-    OA_CU(cudaMemcpyAsync(e->tperm.p, order.data(), sizeof(int) * t, cudaMemcpyHostToDevice, e->st));
-    OA_CU(cudaMemcpyAsync(e->tinv.p, inv.data(), sizeof(int) * t, cudaMemcpyHostToDevice, e->st));
-    OA_CU(cudaMemcpyAsync(e->set_off.p, off.data(), sizeof(int) * off.size(), cudaMemcpyHostToDevice, e->st));
-    OA_CU(cudaMemcpyAsync(e->set_rep.p, rep.data(), sizeof(int) * rep.size(), cudaMemcpyHostToDevice, e->st));
-    OA_CU(cudaMemcpyAsync(e->set_kind.p, kind.data(), sizeof(int) * kind.size(), cudaMemcpyHostToDevice, e->st));
-    OA_CU(cudaMemcpyAsync(e->set_slot.p, slot.data(), sizeof(int) * slot.size(), cudaMemcpyHostToDevice, e->st));
+    // work items of at most LEAN_ITEM_ROWS rows of one set, tiling the flattened row lists
+    std::vector<int> istart;
+    e->h_set_item_off.assign(e->nsets + 1, 0);
+    for (int s2 = 0; s2 < e->nsets; ++s2) {
+        e->h_set_item_off[s2] = (int)istart.size();
+        for (int r0 = off[s2]; r0 < off[s2 + 1]; r0 += LEAN_ITEM_ROWS) istart.push_back(r0);
+    }
+    e->h_set_item_off[e->nsets] = (int)istart.size();
+    istart.push_back(off[e->nsets]);
+    OA_CHECK(e->item_start.ensure(istart.size()));
+    OA_CHECK(e->set_item_off.ensure(e->h_set_item_off.size()));
+    H2DBatch h2d;
+    h2d.add(e->pat.p, ipat);
+    h2d.add(e->zset.p, iz);
+    h2d.add(e->tperm.p, order);
+    h2d.add(e->tinv.p, inv);
+    h2d.add(e->set_off.p, off);
+    h2d.add(e->set_rep.p, rep);
+    h2d.add(e->set_kind.p, kind);
+    h2d.add(e->set_slot.p, slot);
+    h2d.add(e->item_start.p, istart);
+    h2d.add(e->set_item_off.p, e->h_set_item_off);
+    OA_CHECK(flush_h2d(e, h2d));
     k_set_rows<<<e->nsets, OA_NTHREADS, 0, e->st>>>(Y, (size_t)n, n, e->set_rep.p, e->set_kind.p, e->set_off.p,
                                                    e->set_rows.p);
     k_set_gram<<<e->nsets, OA_NTHREADS, 0, e->st>>>(e->Q64.p, n, l, e->set_kind.p, e->set_off.p, e->set_rows.p,
@@ -491,23 +544,7 @@ oa_status set_traits_impl(oa_engine* e, const float* y, int32_t t, bool device_p
     OA_CU(cudaGetLastError());
     e->c2 = l * (1 + e->nsets);
     e->b2_ready = false;
-    {   // work items of at most LEAN_ITEM_ROWS rows of one set, tiling the flattened row lists
-        std::vector<int> istart;
-        e->h_set_item_off.assign(e->nsets + 1, 0);
-        for (int s2 = 0; s2 < e->nsets; ++s2) {
-            e->h_set_item_off[s2] = (int)istart.size();
-            for (int r0 = off[s2]; r0 < off[s2 + 1]; r0 += LEAN_ITEM_ROWS) istart.push_back(r0);
-        }
-        e->h_set_item_off[e->nsets] = (int)istart.size();
-        istart.push_back(off[e->nsets]);
-        OA_CHECK(e->item_start.ensure(istart.size()));
-        OA_CHECK(e->set_item_off.ensure(e->h_set_item_off.size()));
-        OA_CU(cudaMemcpyAsync(e->item_start.p, istart.data(), sizeof(int) * istart.size(), cudaMemcpyHostToDevice,
-                              e->st));
-        OA_CU(cudaMemcpyAsync(e->set_item_off.p, e->h_set_item_off.data(), sizeof(int) * e->h_set_item_off.size(),
-                              cudaMemcpyHostToDevice, e->st));
-        e->lp = oa_engine::LeanPlan{};
-    }
+    e->lp = oa_engine::LeanPlan{};
     OA_CHECK(e->Yt.ensure((size_t)t * e->n_pad));
     if (e->cfg.precision == OA_MIXED_BF16X3) {
         OA_CHECK(e->Yhi.ensure((size_t)t * e->n_pad));
@@ -541,9 +578,9 @@ oa_status lean_plan(oa_engine* e);
 // Default SNPs per chunk: about 16,384/r, rounded so that the tensor-core
 // GEMM's 128 x 256 tiles fill whole waves of the persistent grid (one CTA
 // per SM): the M-tile count is a multiple of sm_count / gcd(sm_count, N-tiles).
-int wave_chunk(const oa_engine* e) {
+int wave_chunk(const oa_engine* e, int t) {
     const int r = e->r;
-    const int n_tiles = std::max(1, (std::max(e->t, 1) + 255) / 256);
+    const int n_tiles = std::max(1, (std::max(t, 1) + 255) / 256);
     int a = e->sm_count, b = n_tiles;
     while (b) {
         const int q = a % b;
@@ -557,7 +594,7 @@ int wave_chunk(const oa_engine* e) {
 
 oa_status prepare_tuning(oa_engine* e) {
     const int t = e->t, l = e->l, n = e->n;
-    e->chunk = std::min(e->cfg.max_snps, e->req.chunk_snps > 0 ? e->req.chunk_snps : wave_chunk(e));
+    e->chunk = std::min(e->cfg.max_snps, e->req.chunk_snps > 0 ? e->req.chunk_snps : wave_chunk(e, e->t));
     e->variant = (e->req.gemm_variant >= 1 && e->req.gemm_variant <= 4) ? e->req.gemm_variant : 1;
     e->raster = e->req.gemm_raster == 2 ? 2 : 1;
     e->lean_spb = e->req.lean_spb > 0 ? std::min(e->req.lean_spb, 8 / e->r) : 0;
@@ -704,7 +741,9 @@ oa_status lean_plan(oa_engine* e) {
         s0 = s1;
     }
     OA_CHECK(e->pass_off.ensure(passes.size()));
-    OA_CU(cudaMemcpyAsync(e->pass_off.p, passes.data(), sizeof(int) * passes.size(), cudaMemcpyHostToDevice, e->st));
+    H2DBatch h2d;
+    h2d.add(e->pass_off.p, passes);
+    OA_CHECK(flush_h2d(e, h2d));
     OA_CU(cudaStreamSynchronize(e->st));
     e->lp.spb = spb;
     e->lp.nbuf = nbuf;
@@ -1053,8 +1092,8 @@ oa_status run_block(oa_engine* e, const float* xr, int mb, bool host_input) {
             }
         }
         if (!launched) OA_CHECK(enqueue_block<R>(e, xr, mb, host_input, false));
-        unsigned long long cnt[4];
-        OA_CU(cudaMemcpyAsync(cnt, e->counters.p, sizeof cnt, cudaMemcpyDeviceToHost, e->st));
+        const unsigned long long* cnt = e->h_cnt;
+        OA_CU(cudaMemcpyAsync(e->h_cnt, e->counters.p, 4 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, e->st));
         OA_CU(cudaStreamSynchronize(e->st));
         if (cnt[3]) {
             set_err("a device pipeline wait timed out (the kernel stopped cleanly)");
@@ -1081,6 +1120,21 @@ oa_status run_block(oa_engine* e, const float* xr, int mb, bool host_input) {
     return OA_ERR_NOMEM;
 }
 
+// Stored-row slots for a block of mb SNPs x t traits in chunks of `chunk`
+// SNPs: the expected stored rows (the two-sided normal tail beyond the |t|
+// threshold, with headroom; every test with store_all) + the unused tails
+// of the epilogue warps' reserved blocks (at most one block per warp and
+// launch).  A block that still overflows grows the buffer and runs again.
+long long slots_needed(const oa_engine* e, long long mb, long long t, long long chunk) {
+    const long long tests = mb * t;
+    const double tail = std::erfc((double)e->cfg.min_t_store / std::sqrt(2.0));
+    const double share = std::min(1.0, 1.5 * tail + 1e-3);
+    const long long nch = (mb + chunk - 1) / chunk;
+    const long long slack = nch * (long long)e->sm_count * 4 * EMIT_BLOCK;
+    const long long rows = e->cfg.store_all ? tests : (long long)(tests * share);
+    return std::max<long long>(1 << 16, rows + slack);
+}
+
 template <int R>
 oa_status run_snps_impl(oa_engine* e, const float* xr, int32_t mb, bool host_input, bool results_on_host,
                         oa_rows* out) {
@@ -1095,17 +1149,7 @@ oa_status run_snps_impl(oa_engine* e, const float* xr, int32_t mb, bool host_inp
     OA_CHECK(prepare_tuning(e));
     OA_CHECK(ensure_chunk_buffers(e));
     const long long tests = (long long)mb * e->t;
-    {
-        // room for the expected stored rows (the two-sided normal tail beyond the |t| threshold, with
-        // headroom) + the unused tails of the epilogue warps' reserved blocks (at most one block per
-        // warp and launch); a block that still overflows grows the buffer and runs again
-        const double tail = std::erfc((double)e->cfg.min_t_store / std::sqrt(2.0));
-        const double share = std::min(1.0, 1.5 * tail + 1e-3);
-        const long long nch = (mb + e->chunk - 1) / e->chunk;
-        const long long slack = nch * (long long)e->sm_count * 4 * EMIT_BLOCK;
-        const long long rows = e->cfg.store_all ? tests : (long long)(tests * share);
-        OA_CHECK(ensure_cap(e, std::max<long long>(1 << 16, rows + slack)));
-    }
+    OA_CHECK(ensure_cap(e, slots_needed(e, mb, e->t, e->chunk)));
     OA_CU(cudaMemsetAsync(e->counters.p, 0, 8 * sizeof(unsigned long long), e->st));
     if (e->dense_on || e->cfg.disp_cov) {
         const size_t nd = (size_t)e->t * mb;
@@ -1135,8 +1179,9 @@ oa_status run_snps_impl(oa_engine* e, const float* xr, int32_t mb, bool host_inp
     if (e->cfg.disp_cov) OA_CHECK(e->marks.ensure((mb + e->chunk - 1) / e->chunk));
     OA_CHECK(run_block<R>(e, xr, mb, host_input));
     unsigned long long cnt[5];
-    OA_CU(cudaMemcpyAsync(cnt, e->counters.p, sizeof cnt, cudaMemcpyDeviceToHost, e->st));
+    OA_CU(cudaMemcpyAsync(e->h_cnt, e->counters.p, sizeof cnt, cudaMemcpyDeviceToHost, e->st));
     OA_CU(cudaStreamSynchronize(e->st));
+    std::memcpy(cnt, e->h_cnt, sizeof cnt);
     std::memset(out, 0, sizeof *out);
     out->count = (int64_t)cnt[4];
     out->tests = tests;
@@ -1282,7 +1327,7 @@ oa_status autotune_impl(oa_engine* e, const float* xr, int mb, oa_tuning* best_o
     // a chunk size set before the call is kept (the caller's block size)
     const bool fixed_chunk = e->req.chunk_snps > 0;
     oa_tuning best{};
-    best.chunk_snps = fixed_chunk ? std::min(mb, e->req.chunk_snps) : std::min(mb, wave_chunk(e));
+    best.chunk_snps = fixed_chunk ? std::min(mb, e->req.chunk_snps) : std::min(mb, wave_chunk(e, e->t));
     best.gemm_variant = 1;
     best.gemm_raster = 1;
     OA_CHECK(prepare_tuning(e));
@@ -1324,7 +1369,7 @@ oa_status autotune_impl(oa_engine* e, const float* xr, int mb, oa_tuning* best_o
     }
     if (!fixed_chunk) {
         std::vector<int> chunks;
-        const int w = wave_chunk(e);
+        const int w = wave_chunk(e, e->t);
         for (int c : {w / 2, w, 2 * w})
             if (c > 0 && c <= mb) chunks.push_back(c);
         for (int c = 2048; c <= 32768; c *= 2)
@@ -1444,6 +1489,14 @@ oa_status oa_engine_create(const oa_config* cfg, oa_engine** out) {
         }
     }
     live_engines(cfg->device, +1);
+    // pinned counters and a first staging area (trait grouping of max_traits traits)
+    if (cudaMallocHost(reinterpret_cast<void**>(&e->h_cnt), 8 * sizeof(unsigned long long)) != cudaSuccess ||
+        stage_reserve(e, (size_t)48 * cfg->max_traits + 65536) != OA_OK) {
+        cudaGetLastError();
+        set_err("pinned host allocation failed");
+        oa_engine_destroy(e);
+        return OA_ERR_NOMEM;
+    }
     *out = e;
     return OA_OK;
 }
@@ -1465,6 +1518,8 @@ oa_status oa_engine_destroy(oa_engine* e) {
     if (e->h_rec) cudaFreeHost(e->h_rec);
     if (e->h_cov) cudaFreeHost(e->h_cov);
     for (void* q : e->retired_pinned) cudaFreeHost(q);
+    if (e->stage) cudaFreeHost(e->stage);
+    if (e->h_cnt) cudaFreeHost(e->h_cnt);
     for (int b = 0; b < 2; ++b) {
         cudaEventDestroy(e->ev_copied[b]);
         cudaEventDestroy(e->ev_used[b]);
@@ -1646,6 +1701,68 @@ int64_t oa_device_bytes(const oa_engine* e) {
     int64_t total = 0;
     for_each_buf(const_cast<oa_engine*>(e), [&](auto& b) { total += (int64_t)(b.n * sizeof(*b.p)); });
     return total;
+}
+
+oa_status oa_reserve(oa_engine* e, int32_t traits, int32_t snps) {
+    clear_stale_error(__func__);
+    if (!e) {
+        set_err("null argument");
+        return OA_ERR_ARG;
+    }
+    if (traits < 1 || traits > e->cfg.max_traits || snps < 1 || snps > e->cfg.max_snps) {
+        set_err("reservation of %d traits x %d SNPs (engine limits %d, %d)", traits, snps, e->cfg.max_traits,
+                e->cfg.max_snps);
+        return OA_ERR_ARG;
+    }
+    OA_CU(cudaSetDevice(e->cfg.device));
+    AllocOn alloc_on(e->st);
+    const size_t t = (size_t)std::max(traits, 1), n = (size_t)e->n, l = (size_t)e->l;
+    {
+        OA_CHECK(e->tsums.ensure(t * (2 + OA_MAX_L)));
+        OA_CHECK(e->tcounts.ensure(t * 2));
+        OA_CHECK(e->thash.ensure(t * 4));
+        for (auto* b : {&e->pat, &e->zset, &e->tperm, &e->tinv}) OA_CHECK(b->ensure(t));
+        OA_CHECK(e->Yt.ensure(t * e->n_pad));
+        if (e->cfg.precision == OA_MIXED_BF16X3) {
+            OA_CHECK(e->Yhi.ensure(t * e->n_pad));
+            OA_CHECK(e->Ylo.ensure(t * e->n_pad));
+        }
+        OA_CHECK(e->rss0.ensure(t));
+        for (auto* b : {&e->sst, &e->a_r2, &e->inv_ncorr, &e->vf}) OA_CHECK(b->ensure(t));
+        OA_CHECK(e->nobs.ensure(t));
+        OA_CHECK(e->b0.ensure(t * l));
+        OA_CHECK(stage_reserve(e, 48 * t + 65536 + 16 * n / LEAN_ITEM_ROWS));
+    }
+    {
+        // the smallest chunk the tuning picks by itself (narrow trait blocks give the most chunks)
+        const int chunk = std::min(e->cfg.max_snps, e->req.chunk_snps > 0 ? e->req.chunk_snps : wave_chunk(e, 1));
+        const long long slots = slots_needed(e, snps, traits, chunk);
+        if (slots > (long long)INT32_MAX) {
+            set_err("%lld stored-row slots exceed the sort's 2^31 limit", slots);
+            return OA_ERR_ARG;
+        }
+        OA_CHECK(ensure_cap(e, slots));
+        const size_t cap = (size_t)e->cap;   // slots, with the headroom ensure_cap adds
+        // rows written: all slots but the block tails
+        const long long tails = ((snps + chunk - 1) / chunk) * (long long)e->sm_count * 4 * EMIT_BLOCK;
+        const size_t R = (size_t)std::max<long long>(1, slots - tails);
+        OA_CHECK(e->keys.ensure(cap));
+        OA_CHECK(e->keys2.ensure(cap));
+        OA_CHECK(e->perm.ensure(cap));
+        OA_CHECK(e->perm2.ensure(cap));
+        OA_CHECK(e->rec2.ensure(R));
+        size_t tmp = 0;
+        OA_CU(cub::DeviceRadixSort::SortPairs(nullptr, tmp, e->keys.p, e->keys2.p, e->perm.p, e->perm2.p, (int)cap, 0,
+                                              64, e->st));
+        OA_CHECK(e->cub_tmp.ensure(tmp));
+        OA_CHECK(ensure_pinned(e->h_rec, e->h_rec_cap, R, e->retired_pinned));
+        if (e->cfg.disp_cov) {
+            OA_CHECK(e->cov2.ensure(R * l * 3));
+            OA_CHECK(ensure_pinned(e->h_cov, e->h_cov_cap, R * l * 3, e->retired_pinned));
+        }
+    }
+    OA_CU(cudaStreamSynchronize(e->st));
+    return OA_OK;
 }
 
 oa_status oa_enable_dense(oa_engine* e, int32_t on) {

@@ -108,6 +108,7 @@ def lib() -> C.CDLL:
         "oa_shard_range": ([C.c_int32, C.c_int32, C.c_int32, C.POINTER(C.c_int32), C.POINTER(C.c_int32)], C.c_int),
         "oa_set_snp_rows": ([P, C.POINTER(C.c_int32), C.c_int32, C.c_int64], C.c_int),
         "oa_device_bytes": ([P], C.c_int64),
+        "oa_reserve": ([P, C.c_int32, C.c_int32], C.c_int),
         "oa_get_tuning": ([P, C.POINTER(Tuning)], C.c_int),
         "oa_autotune": ([P, P, C.c_int32, C.POINTER(Tuning)], C.c_int),
     }
@@ -274,6 +275,10 @@ class Engine:
 
     def device_bytes(self) -> int:
         return int(lib().oa_device_bytes(self.h))
+
+    def reserve(self, traits: int, snps: int) -> None:
+        """oa_reserve: allocate now what blocks of up to `traits` traits x `snps` SNPs need."""
+        _check(lib().oa_reserve(self.h, int(traits), int(snps)))
 
     def launches(self) -> int:
         return int(lib().oa_kernel_launches(self.h))

@@ -156,6 +156,7 @@ class Server:
             eng.set_tuning(chunk_snps=self.chunk)
         eng.set_covariates(cohort.XL)
         eng.set_snp_rows(cohort.rows, self.n_total)
+        eng.reserve(t_cap, self.max_snps)     # no pinned allocations once it serves
         return eng
 
     def _new_engine(self, req: Request) -> _Slot:

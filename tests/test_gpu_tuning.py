@@ -78,3 +78,27 @@ def test_set_tuning_rejects_out_of_range():
         eng.set_tuning(gemm_variant=5)
     with pytest.raises(E.OAError):
         eng.set_tuning(stats_path=-1)
+
+
+def test_reserve_allocates_up_front_and_changes_no_result():
+    ds = synth.generate(synth.scaled(0, n=900, m=3000, t=40, seed=71))
+    l, n = ds.XL.shape
+    out = []
+    for reserve in (True, False):
+        eng = E.Engine(n, l, 1, 64, 4000, precision=E.MIXED, min_t_store=E.t_threshold(0.05), min_r2_store=1e-6)
+        eng.set_covariates(ds.XL)
+        if reserve:
+            before = eng.device_bytes()
+            eng.reserve(64, 4000)
+            assert eng.device_bytes() > before
+            with pytest.raises(E.OAError):
+                eng.reserve(65, 10)
+            with pytest.raises(E.OAError):
+                eng.reserve(1, 4001)
+        eng.set_traits(ds.Y)
+        out.append(eng.run(ds.XR))
+        eng.close()
+    a, b = out
+    np.testing.assert_array_equal(a.trait, b.trait)
+    np.testing.assert_array_equal(a.snp, b.snp)
+    np.testing.assert_array_equal(a.T, b.T)
