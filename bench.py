@@ -43,6 +43,9 @@ import time
 
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
+# the serving section runs up to 8 engines' streams at once: give the device as
+# many hardware work queues as it has (must be set before CUDA starts)
+os.environ.setdefault("CUDA_DEVICE_MAX_CONNECTIONS", "32")
 
 METRIC = "SNP×trait tests/s: plain FP32 vs mixed @ |Δt|≤1e-3 vs FP64; serve p50/p99"
 REF_BIN = os.path.join(ROOT, "oracle", "_ref", "omicabelnomm_ref")

@@ -1171,6 +1171,7 @@ oa_status run_snps_impl(oa_engine* e, const float* xr, int32_t mb, bool host_inp
         if (!lean_gathers(e)) OA_CHECK(e->Xstage[0].ensure((size_t)e->chunk * e->r * e->n));
     }
     if (host_input) {
+        if (!e->cp) OA_CU(cudaStreamCreateWithFlags(&e->cp, cudaStreamNonBlocking));
         for (int b = 0; b < 2; ++b) {
             OA_CHECK(e->Xstage[b].ensure((size_t)e->chunk * e->r * e->n));
             OA_CU(cudaEventRecord(e->ev_used[b], e->st));   // the copy stream starts after the allocation
@@ -1453,8 +1454,10 @@ oa_status oa_engine_create(const oa_config* cfg, oa_engine** out) {
     e->chunk = std::min(cfg->max_snps, e->req.chunk_snps > 0 ? e->req.chunk_snps : 16384 / cfg->r);
     const char* gr = getenv("OA_GRAPHS");
     e->use_graphs = !(gr && gr[0] == '0');
-    if (cudaStreamCreateWithFlags(&e->st, cudaStreamNonBlocking) != cudaSuccess ||
-        cudaStreamCreateWithFlags(&e->cp, cudaStreamNonBlocking) != cudaSuccess) {
+    // the copy stream of host SNP blocks is created on first use: a device-resident
+    // scan (serving) holds one stream, so concurrent engines spread over the
+    // device's hardware work queues
+    if (cudaStreamCreateWithFlags(&e->st, cudaStreamNonBlocking) != cudaSuccess) {
         set_err("stream creation failed");
         delete e;
         return OA_ERR_CUDA;
@@ -1504,7 +1507,7 @@ oa_status oa_engine_create(const oa_config* cfg, oa_engine** out) {
 oa_status oa_engine_destroy(oa_engine* e) {
     if (!e) return OA_OK;
     cudaSetDevice(e->cfg.device);
-    cudaStreamSynchronize(e->cp);
+    if (e->cp) cudaStreamSynchronize(e->cp);
     {
         AllocOn alloc_on(e->st);
         for_each_buf(e, [](auto& b) { b.release(); });
@@ -1532,7 +1535,7 @@ oa_status oa_engine_destroy(oa_engine* e) {
     for (auto* v : {&e->cev0, &e->cev1, &e->sev0, &e->sev1})
         for (auto ev : *v) cudaEventDestroy(ev);
     cudaStreamDestroy(e->st);
-    cudaStreamDestroy(e->cp);
+    if (e->cp) cudaStreamDestroy(e->cp);
     delete e;
     return OA_OK;
 }

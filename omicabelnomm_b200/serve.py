@@ -26,6 +26,7 @@ request gives the same result alone and in a mix.
 """
 from __future__ import annotations
 
+import os
 import threading
 import time
 from dataclasses import dataclass, field
@@ -34,6 +35,11 @@ from typing import Dict, List, Optional
 import numpy as np
 
 from . import engine as E
+
+# Concurrent requests run on separate streams; with the default 8 hardware
+# work queues, streams share queues and one request's queued chunks hold up
+# another's kernels.  Effective only when set before the process starts CUDA.
+os.environ.setdefault("CUDA_DEVICE_MAX_CONNECTIONS", "32")
 
 
 @dataclass
