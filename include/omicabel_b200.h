@@ -189,7 +189,8 @@ typedef struct oa_tuning {
     int32_t chunk_snps;    /* SNPs per device chunk: one launch of each per-block kernel */
     int32_t gemm_variant;  /* tensor-core pipeline: 1 = K-block 32 x 4 stages, 2 = K-block 64 x 2 stages,
                               3 = CTA pairs on neighbouring SMs (2-SM MMA, 256 x 256 tiles), K-block 32 x 6,
-                              4 = CTA pairs, K-block 64 x 3 */
+                              4 = CTA pairs, K-block 64 x 3 (the default); trait blocks of at most 128
+                              traits use 1-SM tiles of 64 or 128 columns whatever the variant */
     int32_t gemm_raster;   /* GEMM tile order: 1 = trait tiles inner, 2 = SNP tiles inner */
     int32_t stats_path;    /* per-SNP sums: 1 = pre-GEMM + batched Schur kernel, 2 = row gathers */
     int32_t lean_spb;      /* SNPs per CTA group of the column-statistics kernel (1..8/r) */

@@ -10,6 +10,7 @@
 
 namespace oa {
 constexpr int EMIT_BLOCK = 128;   // record slots a tensor-core epilogue warp reserves at a time
+constexpr int EPI_WARPS_TC = 8;   // epilogue warps per tensor-core GEMM CTA (each holds one reserved block)
 }
 #define OA_SETS_MAX 4096   // row sets (missingness patterns + zero sets) per trait block
 

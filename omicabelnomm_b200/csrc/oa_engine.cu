@@ -595,7 +595,9 @@ int wave_chunk(const oa_engine* e, int t) {
 oa_status prepare_tuning(oa_engine* e) {
     const int t = e->t, l = e->l, n = e->n;
     e->chunk = std::min(e->cfg.max_snps, e->req.chunk_snps > 0 ? e->req.chunk_snps : wave_chunk(e, e->t));
-    e->variant = (e->req.gemm_variant >= 1 && e->req.gemm_variant <= 4) ? e->req.gemm_variant : 1;
+    // default pipeline: CTA pairs with 64-wide K-blocks (the fastest at wide trait blocks; blocks of
+    // at most 128 traits take the 1-SM narrow tiles whatever the variant)
+    e->variant = (e->req.gemm_variant >= 1 && e->req.gemm_variant <= 4) ? e->req.gemm_variant : 4;
     e->raster = e->req.gemm_raster == 2 ? 2 : 1;
     e->lean_spb = e->req.lean_spb > 0 ? std::min(e->req.lean_spb, 8 / e->r) : 0;
     e->use_pre = e->req.stats_path == 1 || (e->req.stats_path != 2 && e->c2 <= std::max(t, 256));
@@ -1130,7 +1132,7 @@ long long slots_needed(const oa_engine* e, long long mb, long long t, long long 
     const double tail = std::erfc((double)e->cfg.min_t_store / std::sqrt(2.0));
     const double share = std::min(1.0, 1.5 * tail + 1e-3);
     const long long nch = (mb + chunk - 1) / chunk;
-    const long long slack = nch * (long long)e->sm_count * 4 * EMIT_BLOCK;
+    const long long slack = nch * (long long)e->sm_count * EPI_WARPS_TC * EMIT_BLOCK;
     const long long rows = e->cfg.store_all ? tests : (long long)(tests * share);
     return std::max<long long>(1 << 16, rows + slack);
 }
@@ -1329,7 +1331,7 @@ oa_status autotune_impl(oa_engine* e, const float* xr, int mb, oa_tuning* best_o
     const bool fixed_chunk = e->req.chunk_snps > 0;
     oa_tuning best{};
     best.chunk_snps = fixed_chunk ? std::min(mb, e->req.chunk_snps) : std::min(mb, wave_chunk(e, e->t));
-    best.gemm_variant = 1;
+    best.gemm_variant = 4;
     best.gemm_raster = 1;
     OA_CHECK(prepare_tuning(e));
     best.stats_path = e->use_pre ? 1 : 2;
@@ -1747,7 +1749,7 @@ oa_status oa_reserve(oa_engine* e, int32_t traits, int32_t snps) {
         OA_CHECK(ensure_cap(e, slots));
         const size_t cap = (size_t)e->cap;   // slots, with the headroom ensure_cap adds
         // rows written: all slots but the block tails
-        const long long tails = ((snps + chunk - 1) / chunk) * (long long)e->sm_count * 4 * EMIT_BLOCK;
+        const long long tails = ((snps + chunk - 1) / chunk) * (long long)e->sm_count * EPI_WARPS_TC * EMIT_BLOCK;
         const size_t R = (size_t)std::max<long long>(1, slots - tails);
         OA_CHECK(e->keys.ensure(cap));
         OA_CHECK(e->keys2.ensure(cap));

@@ -138,6 +138,89 @@ __device__ __forceinline__ bool epi_core(const EpiArgs& E, int i, int j, const f
     return live && mask != 0u;
 }
 
+// The statistics of one test, kept in registers until the warp knows which
+// of its lanes store a row (the tensor-core epilogues build a record only
+// for those).  Same arithmetic as epi_core.
+template <int R>
+struct EpiTest {
+    double rss;
+    float r2, sig2;
+    float b[R], se[R], t[R];
+    uint32_t mask;
+};
+
+template <int R>
+__device__ __forceinline__ bool epi_decide(const EpiArgs& E, int i, int j, const float* z, const TraitP& tp,
+                                           const double* S, const float* vx, EpiTest<R>& o) {
+    double bx[R];
+    double zz = 0.0;
+#pragma unroll
+    for (int a = 0; a < R; ++a) {
+        double s = 0.0;
+#pragma unroll
+        for (int b = 0; b < R; ++b) s += S[a * R + b] * (double)z[b];
+        bx[a] = s;
+        zz += (double)z[a] * s;
+    }
+    double rss = tp.rss0 - zz;
+    if (tp.zs >= 0) rss -= zero_rows_rss<R>(E, i, j, tp, bx);
+    const float rssf = (float)rss;
+    o.rss = rss;
+    o.r2 = 1.f - rssf * tp.a_r2;
+    o.sig2 = rssf * tp.inv_ncorr;
+    uint32_t mask = 0;
+#pragma unroll
+    for (int a = 0; a < R; ++a) {
+        const float w = o.sig2 * vx[a] * tp.vf;     // SE^2
+        const float rs = rsqrtf(w);
+        const float b = (float)bx[a];
+        o.b[a] = b;
+        o.se[a] = w * rs;
+        o.t[a] = fabsf(b) * rs;
+        if (o.t[a] > E.min_t || E.store_all) mask |= 1u << a;
+    }
+    o.mask = mask;
+    if (E.d_r2) {
+        const size_t off = (size_t)tp.orig * E.dense_ld + E.snp_base + i;
+        const float nanf_ = __int_as_float(0x7fc00000);
+        const bool pos = rss > 0.0;
+        E.d_r2[off] = pos ? o.r2 : nanf_;
+        E.d_sig[off] = pos ? sqrtf(fmaxf(o.sig2, 0.f)) : nanf_;
+#pragma unroll
+        for (int a = 0; a < R; ++a) {
+            E.d_beta[off * R + a] = pos ? o.b[a] : nanf_;
+            E.d_se[off * R + a] = pos ? o.se[a] : nanf_;
+            E.d_t[off * R + a] = pos ? o.t[a] : nanf_;
+        }
+    }
+    const bool live = (rss > 0.0) && (o.r2 > E.min_r2 || E.store_all);
+    return live && mask != 0u;
+}
+
+// The record of a stored test (the fields epi_core fills).
+template <int R>
+__device__ __forceinline__ void epi_write(const EpiArgs& E, int i, int j, const TraitP& tp, const EpiTest<R>& o,
+                                          Rec* dst) {
+    Rec rc;
+    rc.trait = tp.orig;
+    rc.snp = E.snp_base + i;
+    rc.r2 = o.r2;
+    rc.mask = o.mask;
+    rc.sig = sqrtf(fmaxf(o.sig2, 0.f));
+    rc.tint = j;
+    rc.pad[0] = rc.pad[1] = 0.f;
+#pragma unroll
+    for (int a = 0; a < OA_MAX_R; ++a) {
+        rc.b[a] = a < R ? o.b[a] : 0.f;
+        rc.se[a] = a < R ? o.se[a] : 0.f;
+        rc.t[a] = a < R ? o.t[a] : 0.f;
+    }
+    float4* d = reinterpret_cast<float4*>(dst);
+    const float4* src = reinterpret_cast<const float4*>(&rc);
+#pragma unroll
+    for (int q = 0; q < (int)(sizeof(Rec) / 16); ++q) d[q] = src[q];
+}
+
 // Dense outputs of a singular test are NaN.
 template <int R>
 __device__ __forceinline__ void epi_dense_nan(const EpiArgs& E, int i, const TraitP& tp) {
@@ -235,6 +318,30 @@ __device__ __forceinline__ void epi_emit_blocked(const EpiArgs& E, bool st, cons
 #pragma unroll
             for (int q = 0; q < (int)(sizeof(Rec) / 16); ++q) dst[q] = src[q];
         }
+    }
+    em.used += k;
+}
+
+// epi_emit_blocked for records built only by the lanes that store: `write`
+// receives the slot of the calling lane's row.
+template <class W>
+__device__ __forceinline__ void epi_emit_lazy(const EpiArgs& E, bool st, Emitter& em, W&& write) {
+    if (!E.rec) return;
+    const unsigned m = __ballot_sync(0xffffffffu, st);
+    if (!m) return;
+    const int lane = threadIdx.x & 31;
+    const int k = __popc(m);
+    if (em.used + k > em.cap) {   // warp-uniform
+        epi_retire(E, em);
+        unsigned long long b = 0;
+        if (lane == 0) b = atomicAdd(E.rec_count, (unsigned long long)EMIT_BLOCK);
+        em.base = __shfl_sync(0xffffffffu, b, 0);
+        em.used = 0;
+        em.cap = EMIT_BLOCK;
+    }
+    if (st) {
+        const unsigned long long idx = em.base + (unsigned long long)(em.used + __popc(m & ((1u << lane) - 1u)));
+        if ((long long)idx < E.cap) write(E.rec + idx);
     }
     em.used += k;
 }

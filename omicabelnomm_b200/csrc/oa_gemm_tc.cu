@@ -12,8 +12,13 @@
 //   warp 1      TMEM allocator and MMA issuer: 12 tcgen05.mma (kind::f16,
 //               M=128, N=256, K=16) per 64-wide K-block, tcgen05.commit frees
 //               the stage; a second commit hands the accumulator to the epilogue
-//   warps 2..5  epilogue: tcgen05.ld of the 128 x 256 FP32 accumulator, the
-//               statistics of epi_eval, warp-aggregated row emission
+//   warps 2..9  epilogue, two warps per TMEM lane group (32 rows), each
+//               taking half of the tile's columns: tcgen05.ld of 8 columns
+//               at a time, the statistics of epi_core in registers, a record
+//               built only by the lanes that store one, block-reserved row
+//               emission.  The epilogue of a tile must keep pace with the
+//               main loop of the next; with one warp per lane group it
+//               did not.
 // Two 256-column accumulators (512 TMEM columns) let the epilogue of one
 // tile overlap the main loop of the next.
 //
@@ -31,9 +36,9 @@ namespace oa {
 namespace tc {
 
 constexpr int BM = 128;
-constexpr int EPI_WARPS = 4;
-constexpr int NUM_THREADS = 64 + 32 * EPI_WARPS;         // 192
-constexpr int STG_STRIDE = 33;                           // epilogue staging row (conflict-free)
+constexpr int EPI_WARPS = EPI_WARPS_TC;                  // two per TMEM lane group, half of the columns each
+constexpr int NUM_THREADS = 64 + 32 * EPI_WARPS;         // 320
+constexpr int EPI_COLS = 8;                              // accumulator columns per tcgen05.ld of the epilogue
 constexpr int PF_BLOCKS = 16;                            // A-operand K-blocks prefetched into L2 ahead
 constexpr unsigned long long WAIT_NS = 2000000000ull;
 
@@ -45,8 +50,7 @@ struct Shape {
     static constexpr int A_BYTES = BM * BK * 2;                     // one of hi / lo
     static constexpr int B_BYTES = BN * BK * 2;
     static constexpr int STAGE_BYTES = 2 * A_BYTES + 2 * B_BYTES;
-    static constexpr size_t SMEM_BYTES = 1024 + (size_t)STAGES * STAGE_BYTES +
-                                         (size_t)EPI_WARPS * 32 * STG_STRIDE * 4 + (size_t)BN * sizeof(TraitP);
+    static constexpr size_t SMEM_BYTES = 1024 + (size_t)STAGES * STAGE_BYTES + (size_t)BN * sizeof(TraitP);
     static constexpr uint64_t LAYOUT = BK == 64 ? 2u : 4u;          // SWIZZLE_128B : SWIZZLE_64B
     static constexpr uint32_t SBO = BK == 64 ? 1024u : 512u;        // bytes between 8-row groups
     // two accumulators of BN FP32 columns (allocation: a power of two >= 32)
@@ -163,46 +167,55 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&v)[32]) {
     asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 }
 
+__device__ __forceinline__ void tmem_ld8(uint32_t taddr, uint32_t (&v)[8]) {
+    asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];\n"
+                 : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7])
+                 : "r"(taddr));
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+}
+
 // Statistics epilogue of one accumulator tile for one warp: lane = row
 // (SNP column i of the block, `lead` on its first column), BN traits from
 // TMEM at taddr (32 columns per tcgen05.ld), trait constants from tps.
 template <int R, int BN>
 __device__ __forceinline__ void epi_columns(const EpiArgs& E, uint32_t taddr, int n0, int t, int lane, int i,
-                                            bool lead, const float* vx, const TraitP* tps, float* my, Emitter& em) {
+                                            bool lead, const float* vx, const TraitP* tps, int cb, int ce,
+                                            Emitter& em) {
     int cg = -1;            // pattern whose Schur inverse is cached
     bool csing = true;
     double S[R * R];
-    for (int c0 = 0; c0 < BN && n0 + c0 < t; c0 += 32) {
-        uint32_t v[32];
-        tmem_ld32(taddr + (uint32_t)c0, v);
+    for (int c0 = cb; c0 < ce && n0 + c0 < t; c0 += EPI_COLS) {
+        uint32_t v[EPI_COLS];
+        tmem_ld8(taddr + (uint32_t)c0, v);
 #pragma unroll
-        for (int q = 0; q < 32; ++q) my[lane * STG_STRIDE + q] = __uint_as_float(v[q]);
-        __syncwarp();
-        const int qmax = min(32, t - n0 - c0);
-        for (int q = 0; q < qmax; ++q) {
+        for (int q = 0; q < EPI_COLS; ++q) {
             const int j = n0 + c0 + q;
+            if (j >= t) break;   // warp-uniform
             const TraitP tp = tps[c0 + q];
-            const float zf = my[lane * STG_STRIDE + q];
             float z[R];
+            if constexpr (R == 1) {
+                z[0] = __uint_as_float(v[q]);
+            } else {
 #pragma unroll
-            for (int a = 0; a < R; ++a) z[a] = __shfl_sync(0xffffffffu, zf, (lane & ~(R - 1)) + a);
+                for (int a = 0; a < R; ++a)
+                    z[a] = __shfl_sync(0xffffffffu, __uint_as_float(v[q]), (lane & ~(R - 1)) + a);
+            }
             if (tp.g != cg) {    // traits are sorted by pattern: reloads are rare
                 cg = tp.g;
                 csing = lead ? !load_schur<R>(E, cg, i, S) : true;
             }
-            Rec rc;
+            EpiTest<R> o;
             bool st = false;
             if (lead) {
                 if (csing) {
                     atomicAdd(E.n_singular, 1ull);
                     epi_dense_nan<R>(E, i, tp);
                 } else {
-                    st = epi_core<R>(E, i, j, z, tp, S, vx, rc);
+                    st = epi_decide<R>(E, i, j, z, tp, S, vx, o);
                 }
             }
-            epi_emit_blocked(E, st, rc, em);
+            epi_emit_lazy(E, st, em, [&](Rec* dst) { epi_write<R>(E, i, j, tp, o, dst); });
         }
-        __syncwarp();
     }
 }
 
@@ -219,8 +232,7 @@ k_gemm_tc(const __grid_constant__ CUtensorMap mAhi, const __grid_constant__ CUte
     constexpr int A_BYTES = SH::A_BYTES, B_BYTES = SH::B_BYTES, STAGE_BYTES = SH::STAGE_BYTES;
     extern __shared__ uint8_t smem_raw[];
     uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~(uintptr_t)1023);
-    float* stg = reinterpret_cast<float*>(smem + (size_t)STAGES * STAGE_BYTES);
-    TraitP* tps = reinterpret_cast<TraitP*>(stg + (size_t)EPI_WARPS * 32 * STG_STRIDE);   // this tile's traits
+    TraitP* tps = reinterpret_cast<TraitP*>(smem + (size_t)STAGES * STAGE_BYTES);   // this tile's traits
     __shared__ __align__(8) uint64_t full_bar[STAGES], empty_bar[STAGES], acc_full[2], acc_empty[2], done_bar;
     __shared__ uint32_t tmem_base_sh;
     __shared__ volatile int abort_sh;
@@ -357,6 +369,7 @@ k_gemm_tc(const __grid_constant__ CUtensorMap mAhi, const __grid_constant__ CUte
         // lane = row of the tile: each tcgen05.ld column goes out as one
         // coalesced 128-byte row segment of the transposed output
         const int lg = warp & 3;
+        const int cb = ((warp - 2) >> 2) * (BN / 2);   // this warp's half of the columns
         int acc = 0;
         uint32_t aph = 0;
         for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
@@ -370,7 +383,7 @@ k_gemm_tc(const __grid_constant__ CUtensorMap mAhi, const __grid_constant__ CUte
             mbar_try(&acc_full[acc], aph);
             fence_after();
             const int row = m0 + lg * 32 + lane;
-            for (int c0 = 0; c0 < BN && n0 + c0 < t; c0 += 32) {
+            for (int c0 = cb; c0 < cb + BN / 2 && n0 + c0 < t; c0 += 32) {
                 uint32_t v[32];
                 tmem_ld32(tmem_base + ((uint32_t)(lg * 32) << 16) + (uint32_t)(acc * BN + c0), v);
                 const int qmax = min(32, t - n0 - c0);
@@ -388,23 +401,24 @@ k_gemm_tc(const __grid_constant__ CUtensorMap mAhi, const __grid_constant__ CUte
         }
     } else {
         // ---------------- epilogue ----------------
-        // The 128 epilogue threads synchronise among themselves with named
+        // The epilogue threads synchronise among themselves with named
         // barrier 1; every decision that ends the loop is taken right after
-        // it, so all of them leave together.
-        const int ew = warp - 2;                 // 0..3
+        // it, so all of them leave together.  Two warps share each TMEM lane
+        // group (32 rows), one per half of the tile's columns.
+        const int ew = warp - 2;                 // 0..EPI_WARPS-1
         const int lg = warp & 3;                 // TMEM lane group this warp may access
-        const int et = ew * 32 + lane;           // 0..127
-        float* my = stg + (size_t)ew * 32 * STG_STRIDE;
+        const int et = ew * 32 + lane;
+        const int cb = (ew >> 2) * (BN / 2);
         Emitter em;
         int acc = 0;
         uint32_t aph = 0;
         for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
             const int m0 = (raster == 2 ? tile % m_tiles : tile / n_tiles) * BM;
             const int n0 = (raster == 2 ? tile / m_tiles : tile % n_tiles) * BN;
-            asm volatile("bar.sync 1, 128;" ::: "memory");     // previous tile's readers are done
+            asm volatile("bar.sync 1, %0;" ::"n"(EPI_WARPS * 32) : "memory");   // previous tile's readers are done
             if (abort_sh) break;
             // trait constants of this tile (the main loop of the tile is still running)
-            for (int q = et; q < BN; q += 128)
+            for (int q = et; q < BN; q += EPI_WARPS * 32)
                 if (n0 + q < t) tps[q] = load_trait(E, n0 + q);
             const int row = m0 + lg * 32 + lane;   // SNP column of this lane
             const bool lead = ((lane & (R - 1)) == 0) && (row < xrows);
@@ -412,7 +426,7 @@ k_gemm_tc(const __grid_constant__ CUtensorMap mAhi, const __grid_constant__ CUte
             float vx[R];
 #pragma unroll
             for (int a = 0; a < R; ++a) vx[a] = lead ? E.varx[(size_t)i * R + a] : 1.f;
-            asm volatile("bar.sync 1, 128;" ::: "memory");
+            asm volatile("bar.sync 1, %0;" ::"n"(EPI_WARPS * 32) : "memory");
             // accumulator ready (the wait is per warp: lane 0 waits, the warp follows)
             int ok = 1;
             if (lane == 0) ok = mbar_wait(&acc_full[acc], aph, &abort_sh) ? 1 : 0;
@@ -421,7 +435,7 @@ k_gemm_tc(const __grid_constant__ CUtensorMap mAhi, const __grid_constant__ CUte
                 mbar_try(&acc_full[acc], aph);
                 fence_after();
                 epi_columns<R, BN>(E, tmem_base + ((uint32_t)(lg * 32) << 16) + (uint32_t)(acc * BN), n0, t, lane,
-                                   i, lead, vx, tps, my, em);
+                                   i, lead, vx, tps, cb, cb + BN / 2, em);
                 fence_before();
                 mbar_arrive(&acc_empty[acc]);
             }
@@ -464,8 +478,7 @@ struct Shape2 {
     static constexpr int A_BYTES = BM * BK * 2;                     // this CTA's 128 rows, one of hi / lo
     static constexpr int B_BYTES = (BN / 2) * BK * 2;               // this CTA's half of B
     static constexpr int STAGE_BYTES = 2 * A_BYTES + 2 * B_BYTES;
-    static constexpr size_t SMEM_BYTES = 1024 + (size_t)STAGES * STAGE_BYTES +
-                                         (size_t)EPI_WARPS * 32 * STG_STRIDE * 4 + (size_t)BN * sizeof(TraitP);
+    static constexpr size_t SMEM_BYTES = 1024 + (size_t)STAGES * STAGE_BYTES + (size_t)BN * sizeof(TraitP);
     static constexpr uint64_t LAYOUT = BK == 64 ? 2u : 4u;
     static constexpr uint32_t SBO = BK == 64 ? 1024u : 512u;
     static constexpr uint32_t TMEM_COLS = 512;
@@ -526,8 +539,7 @@ k_gemm_tc2(const __grid_constant__ CUtensorMap mAhi, const __grid_constant__ CUt
     constexpr int A_BYTES = SH::A_BYTES, B_BYTES = SH::B_BYTES, STAGE_BYTES = SH::STAGE_BYTES;
     extern __shared__ uint8_t smem_raw[];
     uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~(uintptr_t)1023);
-    float* stg = reinterpret_cast<float*>(smem + (size_t)STAGES * STAGE_BYTES);
-    TraitP* tps = reinterpret_cast<TraitP*>(stg + (size_t)EPI_WARPS * 32 * STG_STRIDE);
+    TraitP* tps = reinterpret_cast<TraitP*>(smem + (size_t)STAGES * STAGE_BYTES);
     __shared__ __align__(8) uint64_t full_bar[STAGES], empty_bar[STAGES], acc_full[2], acc_empty[2], done_bar;
     __shared__ uint32_t tmem_base_sh;
     __shared__ volatile int abort_sh;
@@ -665,7 +677,7 @@ k_gemm_tc2(const __grid_constant__ CUtensorMap mAhi, const __grid_constant__ CUt
         const int ew = warp - 2;
         const int lg = warp & 3;
         const int et = ew * 32 + lane;
-        float* my = stg + (size_t)ew * 32 * STG_STRIDE;
+        const int cb = (ew >> 2) * (BN / 2);
         Emitter em;
         int acc = 0;
         uint32_t aph = 0;
@@ -673,9 +685,9 @@ k_gemm_tc2(const __grid_constant__ CUtensorMap mAhi, const __grid_constant__ CUt
             int m0, n0;
             tile_mn(tile, m0, n0);
             m0 += (int)rank * BM;
-            asm volatile("bar.sync 1, 128;" ::: "memory");
+            asm volatile("bar.sync 1, %0;" ::"n"(EPI_WARPS * 32) : "memory");
             if (abort_sh) break;
-            for (int q = et; q < BN; q += 128)
+            for (int q = et; q < BN; q += EPI_WARPS * 32)
                 if (n0 + q < t) tps[q] = load_trait(E, n0 + q);
             const int row = m0 + lg * 32 + lane;
             const bool lead = ((lane & (R - 1)) == 0) && (row < xrows);
@@ -683,7 +695,7 @@ k_gemm_tc2(const __grid_constant__ CUtensorMap mAhi, const __grid_constant__ CUt
             float vx[R];
 #pragma unroll
             for (int a = 0; a < R; ++a) vx[a] = lead ? E.varx[(size_t)i * R + a] : 1.f;
-            asm volatile("bar.sync 1, 128;" ::: "memory");
+            asm volatile("bar.sync 1, %0;" ::"n"(EPI_WARPS * 32) : "memory");
             int ok = 1;
             if (lane == 0) ok = mbar_wait(&acc_full[acc], aph, &abort_sh) ? 1 : 0;
             ok = __shfl_sync(0xffffffffu, ok, 0);
@@ -691,7 +703,7 @@ k_gemm_tc2(const __grid_constant__ CUtensorMap mAhi, const __grid_constant__ CUt
                 mbar_try(&acc_full[acc], aph);
                 fence_after();
                 epi_columns<R, BN>(E, tmem_base + ((uint32_t)(lg * 32) << 16) + (uint32_t)(acc * BN), n0, t, lane,
-                                   i, lead, vx, tps, my, em);
+                                   i, lead, vx, tps, cb, cb + BN / 2, em);
                 fence_before();
                 __syncwarp();
                 if (lane == 0) mbar_arrive_cluster(map_to_rank(&acc_empty[acc], 0));

@@ -65,7 +65,7 @@ def test_autotune_keeps_a_valid_tuning():
     eng.run_device(xr.data_ptr(), m)
     before = [a.copy() for a in eng.dense(m)]
     best = eng.autotune(xr.data_ptr(), m)
-    assert best["gemm_variant"] in (1, 2) and best["gemm_raster"] in (1, 2) and best["stats_path"] in (1, 2)
+    assert best["gemm_variant"] in (1, 2, 3, 4) and best["gemm_raster"] in (1, 2) and best["stats_path"] in (1, 2)
     assert 0 < best["chunk_snps"] <= m
     eng.run_device(xr.data_ptr(), m)
     after = eng.dense(m)
