@@ -911,7 +911,7 @@ oa_status gemm_dispatch(oa_engine* e, const float* X, int mbc, int snp_base) {
     } else {
         OA_CU(oa_launch_gemm_tc(R, e->variant, e->raster, e->Xhi.p, e->Xlo.p, mbc * R, e->Yhi.p, e->Ylo.p, e->t,
                                 e->n_pad, E, reinterpret_cast<int*>(e->counters.p + 3), e->st));
-        e->last_name = "k_gemm_tc";
+        e->last_name = (e->t > 128 && e->variant >= 3) ? "k_gemm_tc2" : "k_gemm_tc";
     }
     ++e->launches;
     OA_CU(cudaGetLastError());
@@ -1115,7 +1115,9 @@ oa_status run_block(oa_engine* e, const float* xr, int mb, bool host_input) {
         cudaGetLastError();
         e->last_ms = total;
         e->stats_ms = stotal;
-        e->last_name = e->cfg.precision == OA_PLAIN_FP32 ? "k_gemm_simt" : "k_gemm_tc";
+        e->last_name = e->cfg.precision == OA_PLAIN_FP32                ? "k_gemm_simt"
+                       : (e->t > 128 && e->variant >= 3) ? "k_gemm_tc2"
+                                                          : "k_gemm_tc";
         return OA_OK;
     }
     set_err("stored-row buffer could not be grown");
