@@ -252,6 +252,7 @@ struct oa_engine {
     // tuning: requested (0 = automatic) and in effect
     oa_tuning req{};
     int variant = 1, raster = 1, lean_spb = 0;
+    int lean_nbuf = 0;   // column buffers of the statistics kernel: 0 = two where they fit, 1 = one (more CTAs per SM)
     // work items of the lean kernel's set pass (per trait block) and its launch plan
     DBuf<int> item_start, set_item_off, pass_off;
     std::vector<int> h_set_item_off;
@@ -720,7 +721,7 @@ oa_status lean_plan(oa_engine* e) {
     const int R = e->r;
     const size_t limit = 227 * 1024 - 1024;
     int spb = lean_group(e);
-    int nbuf = 2;
+    int nbuf = e->lean_nbuf == 1 ? 1 : 2;
     while (spb > 1 && lean_smem_bytes(R, e->n_pad, spb, nbuf, 0) > 200 * 1024) spb /= 2;
     if (lean_smem_bytes(R, e->n_pad, spb, nbuf, 0) > 200 * 1024) nbuf = 1;
     const size_t base = lean_smem_bytes(R, e->n_pad, spb, nbuf, 0);
@@ -1455,6 +1456,7 @@ oa_status oa_engine_create(const oa_config* cfg, oa_engine** out) {
     if (const char* v = getenv("OA_STATS_PATH")) e->req.stats_path = std::string(v) == "pre" ? 1 : (std::string(v) == "gather" ? 2 : 0);
     if (const char* v = getenv("OA_TC_VARIANT")) e->req.gemm_variant = std::min(4, std::max(0, atoi(v)));
     if (const char* v = getenv("OA_LEAN_SPB")) e->req.lean_spb = std::max(0, atoi(v));
+    if (const char* v = getenv("OA_LEAN_NBUF")) e->lean_nbuf = atoi(v) == 1 ? 1 : 0;
     e->chunk = std::min(cfg->max_snps, e->req.chunk_snps > 0 ? e->req.chunk_snps : 16384 / cfg->r);
     const char* gr = getenv("OA_GRAPHS");
     e->use_graphs = !(gr && gr[0] == '0');

@@ -102,14 +102,17 @@ __device__ __forceinline__ void split8(const float4 p0, const float4 p1, uint4& 
 // bulk copies of aligned columns; 4-byte cp.async copies otherwise, which also
 // gather a row subset of a resident genotype matrix) while this one is
 // processed:
-//   pass 1  column sums from float4 reads of the staged columns; NaN
+//   pass 1  column sums and raw cross products from float4 reads of the
+//           staged columns, one block reduction (FP64 across warps); NaN
 //           propagates, so a column whose sum is NaN is counted and
-//           mean-imputed in place (src/Utility.cpp:302-326) - rare, dosage
-//           files seldom hold NaN.  With an intercept among the covariates
-//           every later sum uses x - mean (the Schur complements, X'y~ and
-//           var_x do not change; the sums lose their large common part)
-//   pass 1b X'X over all rows
-//   pass 2  BF16 hi/lo split of the columns (tensor-core form only)
+//           mean-imputed in place (src/Utility.cpp:302-326) and the sweep
+//           repeated - rare, dosage files seldom hold NaN.  With an
+//           intercept among the covariates every later sum uses x - mean
+//           (the Schur complements, X'y~ and var_x do not change; the sums
+//           lose their large common part); X'X of the shifted columns
+//           follows from the raw sums in FP64
+//   pass 2  BF16 hi/lo split of the shifted columns (tensor-core form) and,
+//           with several columns per group, their row-interleaved copy
 //   pass 3  X'X over each row set: work items of at most 256 rows of one set
 //           (fixed on the host per trait block) go round-robin to the warps;
 //           a warp's item sum (row indices prefetched, one vector load of
@@ -233,23 +236,43 @@ k_snp_lean(LeanArgs A) {
         const float4* x4 = reinterpret_cast<const float4*>(xs);
         const int nS4 = nS / 4;
 
-        // ---- pass 1: column sums (NaN propagates), then the mean of every
-        // column; a column whose sum is NaN is counted and mean-imputed in place
+        // ---- pass 1: column sums and raw cross products in one sweep (the
+        // zero tail adds nothing); NaN propagates, so a column whose sum is
+        // NaN is counted and mean-imputed in place (src/Utility.cpp:302-326)
+        // and the sweep is repeated - rare, dosage files seldom hold NaN
         float sh[NC];                          // subtracted from every value (centring), 0 without
         bool cnan[NC];
         {
-            float acc[NC];
-            double tot[NC];
+            constexpr int NV = NC + K2;        // [column sums | cross products]
+            float acc[NV];
+            double tot[NV];
+            auto sweep = [&]() {
 #pragma unroll
-            for (int c = 0; c < NC; ++c) acc[c] = 0.f;
-            for (int k4 = threadIdx.x; k4 < nS4; k4 += blockDim.x) {
+                for (int u = 0; u < NV; ++u) acc[u] = 0.f;
+                for (int k4 = threadIdx.x; k4 < nS4; k4 += blockDim.x) {
+                    float4 v[NC];
 #pragma unroll
-                for (int c = 0; c < NC; ++c) {
-                    const float4 v = c < ncol ? x4[(size_t)c * nS4 + k4] : make_float4(0.f, 0.f, 0.f, 0.f);
-                    acc[c] += (v.x + v.y) + (v.z + v.w);
+                    for (int c = 0; c < NC; ++c) {
+                        v[c] = c < ncol ? x4[(size_t)c * nS4 + k4] : make_float4(0.f, 0.f, 0.f, 0.f);
+                        acc[c] += (v[c].x + v[c].y) + (v[c].z + v[c].w);
+                    }
+#pragma unroll
+                    for (int s2 = 0; s2 < SPB; ++s2)
+#pragma unroll
+                        for (int a = 0; a < R; ++a)
+#pragma unroll
+                            for (int bb = 0; bb < R; ++bb) {
+                                const float4 xa = v[s2 * R + a], xb = v[s2 * R + bb];
+                                float& d = acc[NC + (s2 * R + a) * R + bb];
+                                d = fmaf(xa.x, xb.x, d);
+                                d = fmaf(xa.y, xb.y, d);
+                                d = fmaf(xa.z, xb.z, d);
+                                d = fmaf(xa.w, xb.w, d);
+                            }
                 }
-            }
-            block_sum_fd<NC>(acc, tot, red);
+                block_sum_fd<NV>(acc, tot, red);
+            };
+            sweep();
             bool any_nan = false;
             float cmean[NC];
 #pragma unroll
@@ -259,6 +282,7 @@ k_snp_lean(LeanArgs A) {
                 cmean[c] = (float)(tot[c] / (double)n);
             }
             if (any_nan) {   // block-uniform: count and sum the observed values, impute in place
+                __syncthreads();   // every thread has read the sums before the scratch is reused
                 float cs[2 * NC];
                 double ct[2 * NC];
 #pragma unroll
@@ -285,6 +309,7 @@ k_snp_lean(LeanArgs A) {
                     }
                 }
                 __syncthreads();
+                sweep();
             }
 #pragma unroll
             for (int c = 0; c < NC; ++c) sh[c] = A.center ? cmean[c] : 0.f;
@@ -296,91 +321,72 @@ k_snp_lean(LeanArgs A) {
                         if (cnan[c]) atomicOr(A.has_nan, 1);
                     }
                 }
-            }
-        }
-
-        // ---- pass 1b: X'X of the (centred) columns over all rows
-        {
-            float acc[K2];
-            double tot[K2];
+                // X'X of the columns taken relative to sh over the n rows:
+                // sum x_a x_b - s_a sum x_b - s_b sum x_a + n s_a s_b
 #pragma unroll
-            for (int u = 0; u < K2; ++u) acc[u] = 0.f;
-            for (int k4 = threadIdx.x; k4 < nS4; k4 += blockDim.x) {
-                float4 v[NC];
-                const int k0 = 4 * k4;
-#pragma unroll
-                for (int c = 0; c < NC; ++c) {
-                    float4 q = c < ncol ? x4[(size_t)c * nS4 + k4] : make_float4(0.f, 0.f, 0.f, 0.f);
-                    const float s0 = sh[c];
-                    q.x = k0 < n ? q.x - s0 : 0.f;          // the zero tail stays zero
-                    q.y = k0 + 1 < n ? q.y - s0 : 0.f;
-                    q.z = k0 + 2 < n ? q.z - s0 : 0.f;
-                    q.w = k0 + 3 < n ? q.w - s0 : 0.f;
-                    v[c] = q;
-                }
-                if constexpr (NC == 2) {
-                    float4* d = reinterpret_cast<float4*>(xi + (size_t)k0 * 2);   // rows k0..k0+3 x 2 columns
-                    d[0] = make_float4(v[0].x, v[1].x, v[0].y, v[1].y);
-                    d[1] = make_float4(v[0].z, v[1].z, v[0].w, v[1].w);
-                } else if constexpr (NC > 2) {
-#pragma unroll
-                    for (int c = 0; c < NC; ++c) {
-                        xi[(size_t)(k0 + 0) * NC + c] = v[c].x;
-                        xi[(size_t)(k0 + 1) * NC + c] = v[c].y;
-                        xi[(size_t)(k0 + 2) * NC + c] = v[c].z;
-                        xi[(size_t)(k0 + 3) * NC + c] = v[c].w;
-                    }
-                }
-#pragma unroll
-                for (int s = 0; s < SPB; ++s)
+                for (int s2 = 0; s2 < SPB; ++s2)
 #pragma unroll
                     for (int a = 0; a < R; ++a)
 #pragma unroll
                         for (int bb = 0; bb < R; ++bb) {
-                            const float4 xa = v[s * R + a], xb = v[s * R + bb];
-                            float& d = acc[(s * R + a) * R + bb];
-                            d = fmaf(xa.x, xb.x, d);
-                            d = fmaf(xa.y, xb.y, d);
-                            d = fmaf(xa.z, xb.z, d);
-                            d = fmaf(xa.w, xb.w, d);
+                            const int ca = s2 * R + a, cb = s2 * R + bb, u = (s2 * R + a) * R + bb;
+                            const double sa = sh[ca], sb = sh[cb];
+                            const double d = tot[NC + u] - sa * tot[cb] - sb * tot[ca] + (double)n * sa * sb;
+                            if (s2 < nsnp) A.D[(size_t)i0 * R * R + u] = (float)d;
                         }
             }
-            block_sum_fd<K2>(acc, tot, red);
-            if (threadIdx.x == 0)
-#pragma unroll
-                for (int u = 0; u < K2; ++u)
-                    if (u < nsnp * R * R) A.D[(size_t)i0 * R * R + u] = (float)tot[u];
         }
 
-        // ---- pass 2: BF16 hi/lo split, 8 elements per thread and step
-        if (A.write_split) {
+        // ---- pass 2: BF16 hi/lo split of the centred columns (tensor-core
+        // form) and, with several columns per group, the centred columns
+        // interleaved by row for the set pass; 8 rows per thread and step.
+        // The tail rows [n, n_pad) get -sh: the other operands of the GEMMs
+        // are zero there.
+        if (A.write_split || NC > 1) {
             const int np8 = nS / 8;
+            for (int k8 = threadIdx.x; k8 < np8; k8 += blockDim.x) {
+                float e[NC][8];
 #pragma unroll
-            for (int c = 0; c < NC; ++c) {
-                if (c >= ncol) break;
-                const float4* col = x4 + (size_t)c * nS4;
-                uint4* hi = reinterpret_cast<uint4*>(A.Xhi + (size_t)(i0 * R + c) * A.n_pad);
-                uint4* lo = reinterpret_cast<uint4*>(A.Xlo + (size_t)(i0 * R + c) * A.n_pad);
-                const float s0 = sh[c];
-                for (int k8 = threadIdx.x; k8 < np8; k8 += blockDim.x) {
-                    float4 p0 = col[2 * k8], p1 = col[2 * k8 + 1];
-                    if (s0 != 0.f) {
-                        const int k0 = 8 * k8;
-                        p0.x = k0 < n ? p0.x - s0 : 0.f;
-                        p0.y = k0 + 1 < n ? p0.y - s0 : 0.f;
-                        p0.z = k0 + 2 < n ? p0.z - s0 : 0.f;
-                        p0.w = k0 + 3 < n ? p0.w - s0 : 0.f;
-                        p1.x = k0 + 4 < n ? p1.x - s0 : 0.f;
-                        p1.y = k0 + 5 < n ? p1.y - s0 : 0.f;
-                        p1.z = k0 + 6 < n ? p1.z - s0 : 0.f;
-                        p1.w = k0 + 7 < n ? p1.w - s0 : 0.f;
+                for (int c = 0; c < NC; ++c) {
+                    float4 p0 = make_float4(0.f, 0.f, 0.f, 0.f), p1 = p0;
+                    if (c < ncol) {
+                        p0 = x4[(size_t)c * nS4 + 2 * k8];
+                        p1 = x4[(size_t)c * nS4 + 2 * k8 + 1];
                     }
-                    uint4 h, o;
-                    split8(p0, p1, h, o);
-                    hi[k8] = h;
-                    lo[k8] = o;
+                    const float s0 = sh[c];
+                    e[c][0] = p0.x - s0;
+                    e[c][1] = p0.y - s0;
+                    e[c][2] = p0.z - s0;
+                    e[c][3] = p0.w - s0;
+                    e[c][4] = p1.x - s0;
+                    e[c][5] = p1.y - s0;
+                    e[c][6] = p1.z - s0;
+                    e[c][7] = p1.w - s0;
+                    if (A.write_split && c < ncol) {
+                        uint4 h, o;
+                        split8(make_float4(e[c][0], e[c][1], e[c][2], e[c][3]),
+                               make_float4(e[c][4], e[c][5], e[c][6], e[c][7]), h, o);
+                        reinterpret_cast<uint4*>(A.Xhi + (size_t)(i0 * R + c) * A.n_pad)[k8] = h;
+                        reinterpret_cast<uint4*>(A.Xlo + (size_t)(i0 * R + c) * A.n_pad)[k8] = o;
+                    }
+                }
+                if constexpr (NC == 2) {
+                    float4* d = reinterpret_cast<float4*>(xi + (size_t)k8 * 16);
+#pragma unroll
+                    for (int u = 0; u < 4; ++u)
+                        d[u] = make_float4(e[0][2 * u], e[1][2 * u], e[0][2 * u + 1], e[1][2 * u + 1]);
+                } else if constexpr (NC == 4) {
+                    float4* d = reinterpret_cast<float4*>(xi + (size_t)k8 * 32);
+#pragma unroll
+                    for (int u = 0; u < 8; ++u) d[u] = make_float4(e[0][u], e[1][u], e[2][u], e[3][u]);
+                } else if constexpr (NC > 1) {
+#pragma unroll
+                    for (int u = 0; u < 8; ++u)
+#pragma unroll
+                        for (int c = 0; c < NC; ++c) xi[(size_t)(8 * k8 + u) * NC + c] = e[c][u];
                 }
             }
+            if (NC > 1) __syncthreads();   // xi is read by other warps in the set pass
         }
 
         // ---- pass 3: X'X over each row set, by work items
