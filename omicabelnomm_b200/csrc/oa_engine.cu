@@ -252,12 +252,15 @@ struct oa_engine {
     // tuning: requested (0 = automatic) and in effect
     oa_tuning req{};
     int variant = 1, raster = 1, lean_spb = 0;
-    int lean_nbuf = 0;   // column buffers of the statistics kernel: 0 = two where they fit, 1 = one (more CTAs per SM)
+    // statistics-kernel layout requests (environment; 0 / -1 = the plan's choice): column buffers (1, 2)
+    // and the row-interleaved column copy of the set pass (0, 1)
+    int lean_nbuf = 0, lean_xi = -1;
     // work items of the lean kernel's set pass (per trait block) and its launch plan
     DBuf<int> item_start, set_item_off, pass_off;
     std::vector<int> h_set_item_off;
     struct LeanPlan {
         int spb = 0, nbuf = 0, items_cap = 0, npass = 0;
+        bool xi = true;   // row-interleaved column copy for the set pass
         size_t smem = 0;
     } lp;
     long long tune_gen = 0;
@@ -721,10 +724,16 @@ oa_status lean_plan(oa_engine* e) {
     const int R = e->r;
     const size_t limit = 227 * 1024 - 1024;
     int spb = lean_group(e);
-    int nbuf = e->lean_nbuf == 1 ? 1 : 2;
-    while (spb > 1 && lean_smem_bytes(R, e->n_pad, spb, nbuf, 0) > 200 * 1024) spb /= 2;
-    if (lean_smem_bytes(R, e->n_pad, spb, nbuf, 0) > 200 * 1024) nbuf = 1;
-    const size_t base = lean_smem_bytes(R, e->n_pad, spb, nbuf, 0);
+    // A set pass heavier than the column passes (more rows in the row sets than in a column) is
+    // latency-bound: it runs faster with more CTAs per SM (one column buffer, no interleaved copy)
+    // than with a prefetched second buffer.
+    const long long set_rows = e->h_set_item_off.empty() ? 0 : (long long)e->h_set_item_off.back() * LEAN_ITEM_ROWS;
+    const bool heavy_sets = set_rows > e->n;
+    int nbuf = e->lean_nbuf ? e->lean_nbuf : (heavy_sets ? 1 : 2);
+    const bool xi = e->lean_xi >= 0 ? e->lean_xi == 1 : !heavy_sets;
+    while (spb > 1 && lean_smem_bytes(R, e->n_pad, spb, nbuf, 0, xi) > 200 * 1024) spb /= 2;
+    if (lean_smem_bytes(R, e->n_pad, spb, nbuf, 0, xi) > 200 * 1024) nbuf = 1;
+    const size_t base = lean_smem_bytes(R, e->n_pad, spb, nbuf, 0, xi);
     const size_t per_item = (size_t)spb * R * R * 4;
     int max_items = 1;
     for (int s2 = 0; s2 < e->nsets; ++s2)
@@ -735,7 +744,7 @@ oa_status lean_plan(oa_engine* e) {
     }
     const int total_items = std::max(1, e->h_set_item_off.empty() ? 1 : e->h_set_item_off.back());
     const int cap = (int)std::min<size_t>((size_t)total_items, (limit - base) / per_item);
-    if (e->lp.spb == spb && e->lp.nbuf == nbuf && e->lp.items_cap == cap) return OA_OK;
+    if (e->lp.spb == spb && e->lp.nbuf == nbuf && e->lp.items_cap == cap && e->lp.xi == xi) return OA_OK;
     std::vector<int> passes{0};
     for (int s0 = 0; s0 < e->nsets;) {
         int s1 = s0 + 1;
@@ -752,7 +761,8 @@ oa_status lean_plan(oa_engine* e) {
     e->lp.nbuf = nbuf;
     e->lp.items_cap = cap;
     e->lp.npass = e->nsets > 0 ? (int)passes.size() - 1 : 0;
-    e->lp.smem = lean_smem_bytes(R, e->n_pad, spb, nbuf, cap);
+    e->lp.xi = xi;
+    e->lp.smem = lean_smem_bytes(R, e->n_pad, spb, nbuf, cap, xi);
     return OA_OK;
 }
 
@@ -781,6 +791,7 @@ oa_status stats_pre(oa_engine* e, const float* X, size_t ldx, const int* xrows, 
     A.Dset = e->Dset.p;
     const bool mixed = e->cfg.precision == OA_MIXED_BF16X3;
     A.write_split = mixed ? 1 : 0;
+    A.use_xi = e->lp.xi ? 1 : 0;
     A.center = e->center ? 1 : 0;
     A.Xhi = e->Xhi.p;
     A.Xlo = e->Xlo.p;
@@ -1456,7 +1467,8 @@ oa_status oa_engine_create(const oa_config* cfg, oa_engine** out) {
     if (const char* v = getenv("OA_STATS_PATH")) e->req.stats_path = std::string(v) == "pre" ? 1 : (std::string(v) == "gather" ? 2 : 0);
     if (const char* v = getenv("OA_TC_VARIANT")) e->req.gemm_variant = std::min(4, std::max(0, atoi(v)));
     if (const char* v = getenv("OA_LEAN_SPB")) e->req.lean_spb = std::max(0, atoi(v));
-    if (const char* v = getenv("OA_LEAN_NBUF")) e->lean_nbuf = atoi(v) == 1 ? 1 : 0;
+    if (const char* v = getenv("OA_LEAN_NBUF")) e->lean_nbuf = atoi(v) == 1 ? 1 : (atoi(v) == 2 ? 2 : 0);
+    if (const char* v = getenv("OA_LEAN_XI")) e->lean_xi = atoi(v) == 0 ? 0 : (atoi(v) == 1 ? 1 : -1);
     e->chunk = std::min(cfg->max_snps, e->req.chunk_snps > 0 ? e->req.chunk_snps : 16384 / cfg->r);
     const char* gr = getenv("OA_GRAPHS");
     e->use_graphs = !(gr && gr[0] == '0');

@@ -37,6 +37,7 @@ struct LeanArgs {
     __nv_bfloat16* Xhi;   // [mb*r][n_pad] (tensor-core form) or null
     __nv_bfloat16* Xlo;
     int write_split;
+    int use_xi;           // with several columns per group: keep the row-interleaved copy for the set pass
     int center;           // take each column relative to its mean (valid when XL holds an intercept)
     int* err;
 };
@@ -50,10 +51,11 @@ constexpr int LEAN_STAGE_U = 8;         // elements per thread and step of the e
 // tail [n, n_pad) kept zero) | with several columns per group, the centred
 // columns interleaved by row ([n_pad][spb*R], one vector load per row in the
 // set pass) | per-item partial sums | reduction scratch.
-__host__ __device__ inline size_t lean_smem_bytes(int R, int n_pad, int spb, int nbuf, int items_cap) {
+__host__ __device__ inline size_t lean_smem_bytes(int R, int n_pad, int spb, int nbuf, int items_cap,
+                                                  bool use_xi = true) {
     const int NC = spb * R;
     const int NQ = 2 * NC + spb * R * R;
-    return (size_t)(nbuf + (NC > 1 ? 1 : 0)) * NC * n_pad * 4 + (size_t)items_cap * spb * R * R * 4 +
+    return (size_t)(nbuf + (NC > 1 && use_xi ? 1 : 0)) * NC * n_pad * 4 + (size_t)items_cap * spb * R * R * 4 +
            (size_t)(LEAN_WARPS + 1) * NQ * 8 + 64;
 }
 
@@ -130,7 +132,8 @@ k_snp_lean(LeanArgs A) {
     const size_t buf_floats = (size_t)NC * nS;
     float* bufs = reinterpret_cast<float*>(smem_raw);                                   // [nbuf][NC][nS]
     float* xi = bufs + (size_t)A.nbuf * buf_floats;                                     // [nS][NC] if NC > 1
-    float* part = xi + (NC > 1 ? (size_t)NC * nS : 0);                                   // [items_cap][K2]
+    const bool use_xi = NC > 1 && A.use_xi;
+    float* part = xi + (use_xi ? (size_t)NC * nS : 0);                                   // [items_cap][K2]
     double* red = reinterpret_cast<double*>(
         (reinterpret_cast<uintptr_t>(part + (size_t)A.items_cap * K2) + 7) & ~(uintptr_t)7);   // [NWARP + 1][NQ]
     __shared__ __align__(8) uint64_t mbar[2];
@@ -342,7 +345,7 @@ k_snp_lean(LeanArgs A) {
         // interleaved by row for the set pass; 8 rows per thread and step.
         // The tail rows [n, n_pad) get -sh: the other operands of the GEMMs
         // are zero there.
-        if (A.write_split || NC > 1) {
+        if (A.write_split || use_xi) {
             const int np8 = nS / 8;
             for (int k8 = threadIdx.x; k8 < np8; k8 += blockDim.x) {
                 float e[NC][8];
@@ -370,7 +373,8 @@ k_snp_lean(LeanArgs A) {
                         reinterpret_cast<uint4*>(A.Xlo + (size_t)(i0 * R + c) * A.n_pad)[k8] = o;
                     }
                 }
-                if constexpr (NC == 2) {
+                if (!use_xi) {
+                } else if constexpr (NC == 2) {
                     float4* d = reinterpret_cast<float4*>(xi + (size_t)k8 * 16);
 #pragma unroll
                     for (int u = 0; u < 4; ++u)
@@ -386,7 +390,7 @@ k_snp_lean(LeanArgs A) {
                         for (int c = 0; c < NC; ++c) xi[(size_t)(8 * k8 + u) * NC + c] = e[c][u];
                 }
             }
-            if (NC > 1) __syncthreads();   // xi is read by other warps in the set pass
+            if (use_xi) __syncthreads();   // xi is read by other warps in the set pass
         }
 
         // ---- pass 3: X'X over each row set, by work items
@@ -411,8 +415,8 @@ k_snp_lean(LeanArgs A) {
                         float x[NC];
 #pragma unroll
                         for (int c = 0; c < NC; ++c) {
-                            if constexpr (NC == 1) {
-                                x[c] = xs[kid[u]] - sh[c];
+                            if (NC == 1 || !use_xi) {
+                                x[c] = xs[(size_t)c * nS + kid[u]] - sh[c];
                             } else if constexpr (NC % 4 == 0) {
                                 if (c % 4 == 0) {
                                     const float4 q4 = reinterpret_cast<const float4*>(xi + (size_t)kid[u] * NC)[c / 4];

@@ -51,6 +51,22 @@ def test_tunings_give_identical_results(prec):
     np.testing.assert_allclose(dg[2], d0[2], rtol=1e-4, atol=1e-4)
 
 
+@pytest.mark.parametrize("prec", [E.PLAIN, E.MIXED])
+@pytest.mark.parametrize("spb", [1, 2])
+def test_statistics_kernel_layouts_give_identical_results(prec, spb, monkeypatch):
+    """One or two column buffers, with or without the row-interleaved copy of
+    the set pass (the plan picks them by the weight of the set pass): same bits."""
+    w, ds = _data()
+    out = []
+    for nbuf, xi in ((2, 1), (1, 0), (2, 0), (1, 1)):
+        monkeypatch.setenv("OA_LEAN_NBUF", str(nbuf))
+        monkeypatch.setenv("OA_LEAN_XI", str(xi))
+        out.append(_run(ds, w, prec, lean_spb=spb, stats_path=1)[2])
+    for d in out[1:]:
+        for a, b in zip(out[0], d):
+            np.testing.assert_array_equal(a, b)
+
+
 def test_autotune_keeps_a_valid_tuning():
     import torch
     w, ds = _data()
