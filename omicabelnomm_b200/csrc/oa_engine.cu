@@ -10,6 +10,7 @@
 //   -> XR'Y~ GEMM with fused statistics epilogue -> (covariate terms)
 // Per API call: sort of the stored rows into reference order (trait, SNP).
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
@@ -220,6 +221,9 @@ std::vector<double> singular_values(std::vector<double> A /* row-major k x k */,
 
 }  // namespace
 
+// Pieces in which the stored rows come back to the host (converted while the next piece copies).
+constexpr int RESULT_PIECES = 8;
+
 struct oa_engine {
     oa_config cfg{};
     int n = 0, l = 0, r = 0, p = 0, LP = 4, n_pad = 0, sm_count = 148;
@@ -325,6 +329,7 @@ struct oa_engine {
     unsigned char* stage = nullptr;
     size_t stage_cap = 0;
     unsigned long long* h_cnt = nullptr;   // 8 counters read back after each block
+    cudaEvent_t ev_piece[RESULT_PIECES] = {};  // the stored rows' pieces have reached the host
     std::vector<int32_t> o_trait, o_snp, o_nused;
     std::vector<float> o_r2, o_b, o_se, o_t;
     std::vector<uint32_t> o_mask;
@@ -1219,14 +1224,17 @@ oa_status run_snps_impl(oa_engine* e, const float* xr, int32_t mb, bool host_inp
         OA_CHECK(e->perm.ensure(NS));
         OA_CHECK(e->perm2.ensure(NS));
         OA_CHECK(e->rec2.ensure(N));
-        k_rec_keys<<<(unsigned)((NS + 255) / 256), 256, 0, e->st>>>(e->rec.p, NS, e->keys.p, e->perm.p);
+        // key bits: enough for t * mb with the all-ones invalid key above every valid one
+        int bits = 1;
+        while (bits < 64 && (1ull << bits) <= (unsigned long long)e->t * (unsigned long long)mb) ++bits;
+        k_rec_keys<<<(unsigned)((NS + 255) / 256), 256, 0, e->st>>>(e->rec.p, NS, mb, bits, e->keys.p, e->perm.p);
         ++e->launches;
         size_t tmp = 0;
         OA_CU(cub::DeviceRadixSort::SortPairs(nullptr, tmp, e->keys.p, e->keys2.p, e->perm.p, e->perm2.p, (int)NS, 0,
-                                              64, e->st));
+                                              bits, e->st));
         OA_CHECK(e->cub_tmp.ensure(tmp));
         OA_CU(cub::DeviceRadixSort::SortPairs(e->cub_tmp.p, tmp, e->keys.p, e->keys2.p, e->perm.p, e->perm2.p, (int)NS,
-                                              0, 64, e->st));
+                                              0, bits, e->st));
         if (e->cfg.disp_cov) OA_CHECK(e->cov2.ensure((size_t)N * l * 3));
         k_rec_gather<<<(unsigned)((N + 255) / 256), 256, 0, e->st>>>(e->rec.p, e->perm2.p, N, e->rec2.p,
                                                                      e->cfg.disp_cov ? e->cov.p : nullptr,
@@ -1235,8 +1243,14 @@ oa_status run_snps_impl(oa_engine* e, const float* xr, int32_t mb, bool host_inp
         if (e->cfg.disp_cov)
             OA_CU(cudaMemcpyAsync(e->h_cov, e->cov2.p, sizeof(float) * N * l * 3, cudaMemcpyDeviceToHost, e->st));
         OA_CU(cudaGetLastError());
-        OA_CU(cudaMemcpyAsync(e->h_rec, e->rec2.p, sizeof(Rec) * N, cudaMemcpyDeviceToHost, e->st));
-        OA_CU(cudaStreamSynchronize(e->st));
+        // the rows come back in pieces, each converted on the host while the next is in flight
+        for (int k = 0; k < RESULT_PIECES; ++k) {
+            const long long q0 = N * k / RESULT_PIECES, q1 = N * (k + 1) / RESULT_PIECES;
+            if (q1 > q0)
+                OA_CU(cudaMemcpyAsync(e->h_rec + q0, e->rec2.p + q0, sizeof(Rec) * (q1 - q0), cudaMemcpyDeviceToHost,
+                                      e->st));
+            OA_CU(cudaEventRecord(e->ev_piece[k], e->st));
+        }
     }
     e->o_trait.resize(N);
     e->o_snp.resize(N);
@@ -1279,12 +1293,28 @@ oa_status run_snps_impl(oa_engine* e, const float* xr, int32_t mb, bool host_inp
         }
     };
     const int nthr = N > (1 << 18) ? (int)std::min<unsigned>(32u, std::max(1u, std::thread::hardware_concurrency())) : 1;
+    std::atomic<int> piece_err{0};
+    auto convert_pieces = [&](int k0, int nk) {   // thread k0 of nk: its share of every piece, in piece order
+        for (int k = 0; k < RESULT_PIECES; ++k) {
+            if (N > 0 && cudaEventSynchronize(e->ev_piece[k]) != cudaSuccess) {
+                piece_err = 1;
+                return;
+            }
+            const long long q0 = N * k / RESULT_PIECES, q1 = N * (k + 1) / RESULT_PIECES;
+            convert(q0 + (q1 - q0) * k0 / nk, q0 + (q1 - q0) * (k0 + 1) / nk);
+        }
+    };
     if (nthr <= 1) {
-        convert(0, N);
+        convert_pieces(0, 1);
     } else {
         std::vector<std::thread> th;
-        for (int k = 0; k < nthr; ++k) th.emplace_back(convert, N * k / nthr, N * (k + 1) / nthr);
+        for (int k = 0; k < nthr; ++k) th.emplace_back(convert_pieces, k, nthr);
         for (auto& x : th) x.join();
+    }
+    if (piece_err) {
+        cudaGetLastError();
+        set_err("waiting for the stored rows failed");
+        return OA_ERR_CUDA;
     }
     out->trait = e->o_trait.data();
     out->snp = e->o_snp.data();
@@ -1485,6 +1515,7 @@ oa_status oa_engine_create(const oa_config* cfg, oa_engine** out) {
         cudaEventCreateWithFlags(&e->ev_used[b], cudaEventDisableTiming);
         cudaEventRecord(e->ev_used[b], e->st);
     }
+    for (auto& ev : e->ev_piece) cudaEventCreateWithFlags(&ev, cudaEventDisableTiming);
     cudaEventCreate(&e->k0);
     cudaEventCreate(&e->k1);
     cudaEventCreate(&e->s0);
@@ -1545,6 +1576,8 @@ oa_status oa_engine_destroy(oa_engine* e) {
         cudaEventDestroy(e->ev_copied[b]);
         cudaEventDestroy(e->ev_used[b]);
     }
+    for (auto ev : e->ev_piece)
+        if (ev) cudaEventDestroy(ev);
     cudaEventDestroy(e->k0);
     cudaEventDestroy(e->k1);
     cudaEventDestroy(e->s0);

@@ -256,12 +256,16 @@ static __global__ void k_set_qrows(const int* __restrict__ rows, int total, cons
 }
 
 // Sort keys of the stored rows: (trait, SNP) -> reference output order.
-static __global__ void k_rec_keys(const Rec* __restrict__ rec, long long N, unsigned long long* __restrict__ keys,
-                           int* __restrict__ perm) {
+// Sort keys of the stored-row slots: trait * mb + SNP, an unused slot (trait
+// -1) all ones in the low `bits` bits, so that it sorts last (the sort looks
+// at those bits only; 2^bits > t * mb).
+static __global__ void k_rec_keys(const Rec* __restrict__ rec, long long N, long long mb, int bits,
+                                  unsigned long long* __restrict__ keys, int* __restrict__ perm) {
     const long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x;
     if (q >= N) return;
-    const int tr = rec[q].trait;   // -1: an unused slot (sorts last)
-    keys[q] = tr < 0 ? ~0ull : (((unsigned long long)(unsigned)tr << 32) | (unsigned)rec[q].snp);
+    const int tr = rec[q].trait;
+    keys[q] = tr < 0 ? (bits >= 64 ? ~0ull : ((1ull << bits) - 1ull))
+                     : (unsigned long long)tr * (unsigned long long)mb + (unsigned)rec[q].snp;
     perm[q] = (int)q;
 }
 
