@@ -259,6 +259,19 @@ oa_status oa_solve(const oa_settings* s, oa_outputs* out);
 /* ≙ main of the reference CLI: same flags, exit status 0 / 1. */
 int oa_cli_main(int argc, char** argv);
 
+/* Re-thresholds the binary outputs <source>.ibin / <source>.dbin (written
+ * with store_bin / -b) into <dest>.txt: rows whose P is below min_p_disp and
+ * whose R2 is above min_r2 (force_all: every stored term), covariate terms
+ * only with include_cov and when the files hold them; the reference's
+ * column formats.  ≙ the reference's OmicOUT tool (OmicOUT/main.cpp:227-483),
+ * including its reading of at most t blocks and its 16-bit SNP indices.
+ * *rows_printed (may be NULL) receives the number of rows written. */
+oa_status oa_omicout(const char* source, const char* dest, float min_p_disp, float min_r2, int32_t force_all,
+                     int32_t include_cov, int64_t* rows_printed);
+/* ≙ main of the reference's omicout (-b <base> -o <base> -d <P> [-r <R2>]
+ * [-i] [-f]; OmicOUT/main.cpp:86-227): exit status 0 / 1. */
+int oa_omicout_main(int argc, char** argv);
+
 /* SNP range [*first, *first + *count) of shard `shard` of `shards` over m
  * SNPs: the reference's MPI split (src/AIOwrapper.cpp:95-117): m / shards
  * each, the last shard also the remainder; no split when m < shards. */

@@ -5,6 +5,7 @@
 Products (git-ignored, they travel with the tree):
     omicabelnomm_b200/lib/libomicabel_b200.so   the C-ABI library (include/omicabel_b200.h)
     omicabelnomm_b200/lib/omicabelnomm          the CLI
+    omicabelnomm_b200/lib/omicout               the re-thresholding tool for the binary outputs
 """
 from __future__ import annotations
 
@@ -25,9 +26,10 @@ INCLUDE = os.path.join(ROOT, "include")
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 CU_SOURCES = ["oa_engine.cu", "oa_stats.cu", "oa_gemm_simt.cu", "oa_gemm_tc.cu", "oa_noalloc.cu"]
-CXX_SOURCES = ["oa_host.cpp"]
+CXX_SOURCES = ["oa_host.cpp", "oa_omicout.cpp"]
 LIB = os.path.join(OUT, "libomicabel_b200.so")
 CLI = os.path.join(OUT, "omicabelnomm")
+OMICOUT = os.path.join(OUT, "omicout")
 
 
 def nvcc() -> str:
@@ -89,12 +91,15 @@ def build(jobs: int = 0, verbose: bool = False, force: bool = False) -> str:
             "-L" + cudalib, "-lcudart", "-Xlinker", "-rpath," + cudalib]
     subprocess.run(link, check=True)
     os.replace(LIB + ".tmp", LIB)
-    cli_obj = _compile("oa_cli.cpp", verbose)
-    subprocess.run([host_cxx(), "-o", CLI + ".tmp", cli_obj, "-L" + OUT, "-lomicabel_b200",
-                    "-Wl,-rpath,$ORIGIN", "-Wl,-rpath," + cudalib, "-L" + cudalib, "-lcudart"], check=True)
-    os.replace(CLI + ".tmp", CLI)
+    mains = []
+    for src, exe in (("oa_cli.cpp", CLI), ("oa_omicout_cli.cpp", OMICOUT)):
+        obj = _compile(src, verbose)
+        subprocess.run([host_cxx(), "-o", exe + ".tmp", obj, "-L" + OUT, "-lomicabel_b200",
+                        "-Wl,-rpath,$ORIGIN", "-Wl,-rpath," + cudalib, "-L" + cudalib, "-lcudart"], check=True)
+        os.replace(exe + ".tmp", exe)
+        mains.append(obj)
     # drop stale objects of older source versions
-    keep = set(os.path.basename(o) for o in objs + [cli_obj])
+    keep = set(os.path.basename(o) for o in objs + mains)
     for f in os.listdir(OBJ):
         if f not in keep:
             os.unlink(os.path.join(OBJ, f))

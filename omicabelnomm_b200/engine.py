@@ -17,6 +17,7 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "lib", "libomicabel_b200.so")
 CLI_PATH = os.path.join(HERE, "lib", "omicabelnomm")
+OMICOUT_PATH = os.path.join(HERE, "lib", "omicout")
 HEADER = os.path.join(os.path.dirname(HERE), "include", "omicabel_b200.h")
 
 OA_OK = 0
@@ -109,6 +110,9 @@ def lib() -> C.CDLL:
         "oa_set_snp_rows": ([P, C.POINTER(C.c_int32), C.c_int32, C.c_int64], C.c_int),
         "oa_device_bytes": ([P], C.c_int64),
         "oa_reserve": ([P, C.c_int32, C.c_int32], C.c_int),
+        "oa_omicout": ([C.c_char_p, C.c_char_p, C.c_float, C.c_float, C.c_int32, C.c_int32,
+                        C.POINTER(C.c_int64)], C.c_int),
+        "oa_omicout_main": ([C.c_int, C.POINTER(C.c_char_p)], C.c_int),
         "oa_get_tuning": ([P, C.POINTER(Tuning)], C.c_int),
         "oa_autotune": ([P, P, C.c_int32, C.POINTER(Tuning)], C.c_int),
     }
@@ -298,6 +302,15 @@ def scan_dense_noalloc(xl_ptr: int, y_ptr: int, xr_ptr: int, n: int, l: int, r: 
     V = C.c_void_p
     _check(lib().oa_scan_dense_noalloc(V(xl_ptr), V(y_ptr), V(xr_ptr), n, l, r, t, mb, V(beta_ptr), V(se_ptr),
                                        V(t_ptr), V(r2_ptr), V(stream)))
+
+
+def omicout(source: str, dest: str, min_p_disp: float, min_r2: float = -100.0, force_all: bool = False,
+            include_cov: bool = False) -> int:
+    """oa_omicout: <source>.ibin/.dbin -> <dest>.txt re-thresholded; returns the rows written."""
+    rows = C.c_int64()
+    _check(lib().oa_omicout(source.encode(), dest.encode(), C.c_float(min_p_disp), C.c_float(min_r2),
+                            int(force_all), int(include_cov), C.byref(rows)))
+    return rows.value
 
 
 def shard_range(m: int, shard: int, shards: int) -> tuple[int, int]:
