@@ -142,6 +142,18 @@ oa_status oa_enable_dense(oa_engine* e, int32_t on);
  * SNP block, src/AIOwrapper.cpp:1098-1130). */
 oa_status oa_set_snp_rows(oa_engine* e, const int32_t* rows, int32_t n_rows, int64_t ld);
 
+/* Column model of the SNP blocks (the reference's dosage models, applied by
+ * its reader, src/AIOwrapper.cpp:257-340, 1213-1275): after this call every
+ * SNP of a block passed to oa_run_snps(_device) is in_cols file columns
+ * (1..8), and the engine forms its r columns on the device:
+ *   combine != 0: r = 1 column sum_c weights[c] * x_c  (additive: {2,1,0},
+ *                 dominant: {1,1,0}, recessive: {1,0,0} on genotype
+ *                 probabilities AA, AB[, BB]; custom additive: the factors file)
+ *   combine == 0: r = in_cols columns weights[c] * x_c (custom linear model).
+ * in_cols = 0 restores plain blocks of r columns per SNP.  Not with row subsets. */
+#define OA_MODEL_MAX_COLS 8
+oa_status oa_set_column_model(oa_engine* e, int32_t in_cols, const float* weights, int32_t combine);
+
 /* Device memory held by the engine's buffers, in bytes. */
 int64_t oa_device_bytes(const oa_engine* e);
 
@@ -242,6 +254,11 @@ typedef struct oa_settings {
                                     shards > 1 and m >= shards, shard k scans SNPs [k*m/shards, ...)
                                     (the last shard also the remainder) and writes
                                     <out>_mpi<k+1>__dis.txt etc. with shard-local SNP indices */
+    int32_t dosage_model;        /* 0 none; 1 additive (-j), 2 dominant (-k), 3 recessive (-l) on r = 2
+                                    or 3 genotype-probability columns per SNP (AA, AB[, BB]);
+                                    4 custom linear (-z), 5 custom additive (-y) with the factors of
+                                    fname_factors (src/AIOwrapper.cpp:257-340) */
+    const char* fname_factors;   /* -z / -y: whitespace-separated factors, one per file column of a SNP */
 } oa_settings;
 
 typedef struct oa_outputs {

@@ -274,6 +274,11 @@ struct oa_engine {
     // SNP chunk buffers
     int chunk = 0;
     DBuf<float> Xstage[2];
+    // column model (dosage models): each SNP arrives as in_cols file columns and its r columns are
+    // formed on the device; in_cols = 0: the input already holds r columns per SNP
+    int in_cols = 0, model_combine = 0;
+    float model_w[OA_MODEL_MAX_COLS] = {};
+    DBuf<float> Xmodel;
     DBuf<__nv_bfloat16> Xhi, Xlo;
     DBuf<float> mean, varx, aobs, afull, zA, zD;
     DBuf<float> D, Dset, C2T;   // pre-GEMM path: X'X, per-set X'X, pre-GEMM output
@@ -356,7 +361,7 @@ void for_each_buf(oa_engine* e, F&& f) {
     f(e->set_kind); f(e->set_slot); f(e->tperm); f(e->tinv);
     f(e->a_r2); f(e->inv_ncorr); f(e->vf); f(e->thash); f(e->sst); f(e->qrows); f(e->pat_bad);
     f(e->B2); f(e->B2hi); f(e->B2lo);
-    f(e->Xstage[0]); f(e->Xstage[1]); f(e->Xhi); f(e->Xlo);
+    f(e->Xstage[0]); f(e->Xstage[1]); f(e->Xmodel); f(e->Xhi); f(e->Xlo);
     f(e->mean); f(e->varx); f(e->aobs); f(e->afull); f(e->zA); f(e->zD); f(e->D); f(e->Dset); f(e->C2T);
     f(e->has_nan); f(e->sinv); f(e->sfinv); f(e->sing);
     f(e->rec); f(e->rec2); f(e->cov); f(e->cov2); f(e->counters); f(e->keys); f(e->keys2); f(e->perm);
@@ -374,6 +379,38 @@ static __global__ void k_gather_rows(const float* __restrict__ in, long long ld,
 }
 
 // Device input of one chunk: the block itself, or its row-subset gather.
+// The column model of one chunk (the reference's dosage models,
+// src/AIOwrapper.cpp:257-340, 1213-1275): SNP i's in_cols file columns ->
+// combine: one column sum_c w[c] * x_c (additive, dominant, recessive and
+// custom additive models); otherwise in_cols columns w[c] * x_c (custom
+// linear model).  NaN propagates (mean imputation follows, as in the reference).
+struct ModelW {
+    float w[OA_MODEL_MAX_COLS];
+};
+static __global__ void k_column_model(const float* __restrict__ in, int n, int in_cols, ModelW W, int combine,
+                                      float* __restrict__ out) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    const int i = blockIdx.y;
+    if (k >= n) return;
+    const float* src = in + (size_t)i * in_cols * n + k;
+    if (combine) {   // a zero factor drops its column (the reference does not read it)
+        float acc = 0.f;
+        bool any = false;
+        for (int c = 0; c < in_cols; ++c) {
+            if (W.w[c] == 0.f) continue;
+            const float x = src[(size_t)c * n];
+            acc = any ? fmaf(W.w[c], x, acc) : W.w[c] * x;
+            any = true;
+        }
+        out[(size_t)i * n + k] = acc;
+    } else {
+        for (int c = 0; c < in_cols; ++c) out[((size_t)i * in_cols + c) * n + k] = W.w[c] * src[(size_t)c * n];
+    }
+}
+
+// Columns per SNP of the caller's SNP blocks.
+int input_cols(const oa_engine* e) { return e->in_cols > 0 ? e->in_cols : e->r; }
+
 // Mixed form with the pre-GEMM statistics path: nothing after the column
 // statistics reads the FP32 chunk (the GEMMs read its BF16 split), so a row
 // subset is gathered by the statistics kernel as it stages the columns.
@@ -999,12 +1036,13 @@ oa_status enqueue_block(oa_engine* e, const float* xr, int mb, bool host_input, 
     auto rec = [&](cudaEvent_t ev) -> cudaError_t {
         return capture ? cudaEventRecordWithFlags(ev, e->st, cudaEventRecordExternal) : cudaEventRecord(ev, e->st);
     };
-    const size_t colbytes = sizeof(float) * (size_t)e->n * R;
+    const int IC = input_cols(e);
+    const size_t colbytes = sizeof(float) * (size_t)e->n * IC;
     auto issue_copy = [&](int c) -> oa_status {   // host chunk c -> staging buffer c & 1 (copy stream)
         const int b = c & 1;
         const int c0 = c * e->chunk, mbc = std::min(e->chunk, mb - c0);
         OA_CU(cudaStreamWaitEvent(e->cp, e->ev_used[b], 0));
-        OA_CU(cudaMemcpyAsync(e->Xstage[b].p, xr + (size_t)c0 * R * e->n, colbytes * mbc, cudaMemcpyHostToDevice,
+        OA_CU(cudaMemcpyAsync(e->Xstage[b].p, xr + (size_t)c0 * IC * e->n, colbytes * mbc, cudaMemcpyHostToDevice,
                               e->cp));
         OA_CU(cudaEventRecord(e->ev_copied[b], e->cp));
         return OA_OK;
@@ -1024,8 +1062,19 @@ oa_status enqueue_block(oa_engine* e, const float* xr, int mb, bool host_input, 
             X = xr + (size_t)c0 * R * e->x_ld;
             ldx = e->x_ld;
             xrows = e->xrows.p;
+        } else if (e->in_cols > 0) {
+            X = xr + (size_t)c0 * IC * e->n;
         } else {
             OA_CHECK(chunk_input<R>(e, xr, c0, mbc, &X));
+        }
+        if (e->in_cols > 0) {   // file columns -> model columns
+            ModelW W;
+            for (int c = 0; c < OA_MODEL_MAX_COLS; ++c) W.w[c] = e->model_w[c];
+            k_column_model<<<dim3((unsigned)((e->n + 255) / 256), (unsigned)mbc), 256, 0, e->st>>>(
+                X, e->n, e->in_cols, W, e->model_combine, e->Xmodel.p);
+            ++e->launches;
+            OA_CU(cudaGetLastError());
+            X = e->Xmodel.p;
         }
         OA_CU(cudaMemsetAsync(e->has_nan.p, 0, sizeof(int), e->st));
         OA_CU(rec(e->sev0[c]));
@@ -1191,10 +1240,11 @@ oa_status run_snps_impl(oa_engine* e, const float* xr, int32_t mb, bool host_inp
         }
         if (!lean_gathers(e)) OA_CHECK(e->Xstage[0].ensure((size_t)e->chunk * e->r * e->n));
     }
+    if (e->in_cols > 0) OA_CHECK(e->Xmodel.ensure((size_t)e->chunk * e->r * e->n));
     if (host_input) {
         if (!e->cp) OA_CU(cudaStreamCreateWithFlags(&e->cp, cudaStreamNonBlocking));
         for (int b = 0; b < 2; ++b) {
-            OA_CHECK(e->Xstage[b].ensure((size_t)e->chunk * e->r * e->n));
+            OA_CHECK(e->Xstage[b].ensure((size_t)e->chunk * input_cols(e) * e->n));
             OA_CU(cudaEventRecord(e->ev_used[b], e->st));   // the copy stream starts after the allocation
         }
     }
@@ -1718,11 +1768,48 @@ oa_status oa_autotune(oa_engine* e, const float* xr_dev, int32_t mb, oa_tuning* 
     return autotune_impl(e, xr_dev, mb, best);
 }
 
+oa_status oa_set_column_model(oa_engine* e, int32_t in_cols, const float* weights, int32_t combine) {
+    clear_stale_error(__func__);
+    if (!e) {
+        set_err("null engine");
+        return OA_ERR_ARG;
+    }
+    if (in_cols == 0) {   // plain input
+        e->in_cols = 0;
+        drop_graph(e);
+        ++e->tune_gen;
+        return OA_OK;
+    }
+    if (in_cols < 1 || in_cols > OA_MODEL_MAX_COLS || !weights) {
+        set_err("column model of %d file columns per SNP (1..%d, with weights)", in_cols, OA_MODEL_MAX_COLS);
+        return OA_ERR_ARG;
+    }
+    if ((combine && e->r != 1) || (!combine && e->r != in_cols)) {
+        set_err("column model: %s needs r = %d, the engine has r = %d", combine ? "a combined column" : "scaled columns",
+                combine ? 1 : in_cols, e->r);
+        return OA_ERR_ARG;
+    }
+    if (e->subset) {
+        set_err("a column model does not apply to row subsets of a resident matrix");
+        return OA_ERR_STATE;
+    }
+    e->in_cols = in_cols;
+    e->model_combine = combine ? 1 : 0;
+    for (int c = 0; c < OA_MODEL_MAX_COLS; ++c) e->model_w[c] = c < in_cols ? weights[c] : 0.f;
+    drop_graph(e);
+    ++e->tune_gen;
+    return OA_OK;
+}
+
 oa_status oa_set_snp_rows(oa_engine* e, const int32_t* rows, int32_t n_rows, int64_t ld) {
     clear_stale_error(__func__);
     if (!e) {
         set_err("null engine");
         return OA_ERR_ARG;
+    }
+    if (rows && e->in_cols > 0) {
+        set_err("a row subset does not apply with a column model");
+        return OA_ERR_STATE;
     }
     OA_CU(cudaSetDevice(e->cfg.device));
     AllocOn alloc_on(e->st);

@@ -245,6 +245,8 @@ struct Writer {
     float min_r2_disp = 0;
     int l = 0, r = 0, p = 0, real_n = 0, mb_ref = 500;
     int name_base = 0;   // first SNP of this shard in the genotype file (names only; indices are shard-local)
+    int name_stride = 1;           // file columns per SNP
+    bool name_first_only = false;  // a combined dosage model names a SNP by its first file column
     const Fvi* fy = nullptr;
     const Fvi* fl = nullptr;
     const Fvi* fr = nullptr;
@@ -297,7 +299,8 @@ struct Writer {
                 if ((P <= min_p_disp && r2 >= min_r2_disp) || store_all) {
                     std::string aname = " ";
                     if (h < l) aname = fl->var_name(h) + ":";
-                    aname += fr->var_name((size_t)(name_base + ar_offset_snps) * r + ar_idx);
+                    const size_t snp_g = (size_t)(name_base + snp);
+                    aname += fr->var_name(snp_g * name_stride + (name_first_only ? 0 : (size_t)(h >= l ? h - l : 0)));
                     const int len = snprintf(line, sizeof line, "%s\t%s\t%u\t%.2f\t%.7f\t%.4f\t%.7f\t%.7f\t%.7Le\n",
                                              fy->var_name(ytr).c_str(), aname.c_str(), (unsigned)nused,
                                              (double)npct, (double)B, (double)r2, (double)SE, (double)T, P);
@@ -387,14 +390,56 @@ oa_status oa_solve(const oa_settings* S, oa_outputs* out) {
              fy.c_str(), FY.nobs, fxl.c_str(), FL.nobs, fxr.c_str(), FR.nobs);
         return OA_ERR_IO;
     }
-    const int r = std::max(1, S->r);
+    // file columns per SNP (-n) and the model's columns per SNP (src/AIOwrapper.cpp:257-340)
+    const int file_r = std::max(1, S->r);
     const int fileN = (int)FL.nobs;
-    if (FR.nvar % r != 0) {
+    if (FR.nvar % file_r != 0) {
         herr("Number of elements in %s.fvi:%u is not consistent with the value of --ngpred (-n)%d provided",
-             fxr.c_str(), FR.nvar, r);
+             fxr.c_str(), FR.nvar, file_r);
         return OA_ERR_IO;
     }
-    const int m_file = (int)(FR.nvar / r), t = (int)FY.nvar, l = (int)FL.nvar, p = l + r;
+    float model_w[OA_MODEL_MAX_COLS] = {};
+    bool combine = false;
+    int r = file_r;
+    if (S->dosage_model < 0 || S->dosage_model > 5) {
+        herr("Requested dosages model wihtout a valid model!");
+        return OA_ERR_ARG;
+    }
+    if (S->dosage_model >= 1 && S->dosage_model <= 3) {
+        static const char* kName[] = {"", "Additive", "Dominant", "Recessive"};
+        static const float kW[4][3] = {{0, 0, 0}, {2, 1, 0}, {1, 1, 0}, {1, 0, 0}};
+        if (file_r != 2 && file_r != 3) {
+            herr("The amount of columns per Independent Variable (--ngpred) is not 2 or 3 for a valid %s Model!",
+                 kName[S->dosage_model]);
+            return OA_ERR_ARG;
+        }
+        for (int c = 0; c < file_r; ++c) model_w[c] = kW[S->dosage_model][c];
+        combine = true;
+        r = 1;
+    } else if (S->dosage_model == 4 || S->dosage_model == 5) {
+        if (file_r > OA_MODEL_MAX_COLS) {
+            herr("a dosage model takes at most %d columns per SNP", OA_MODEL_MAX_COLS);
+            return OA_ERR_UNSUPPORTED;
+        }
+        FILE* ff = S->fname_factors ? fopen(S->fname_factors, "r") : nullptr;
+        if (!ff) {
+            herr("Error reading dosages file.");
+            return OA_ERR_IO;
+        }
+        int got = 0;
+        while (got < file_r && fscanf(ff, "%f", &model_w[got]) == 1) ++got;
+        fclose(ff);
+        if (got != file_r) {
+            herr("The number of factors for the dosage model! does not coincide with the source data #facctors:%d, "
+                 "expected:%d",
+                 got, file_r);
+            return OA_ERR_IO;
+        }
+        combine = S->dosage_model == 5;
+        r = combine ? 1 : file_r;
+    }
+    const bool model = S->dosage_model != 0;
+    const int m_file = (int)(FR.nvar / file_r), t = (int)FY.nvar, l = (int)FL.nvar, p = l + r;
     // SNP shard of this process (the reference's MPI split, src/AIOwrapper.cpp:95-117)
     const int shards = std::max(1, S->shards);
     if (S->shard < 0 || S->shard >= shards) {
@@ -482,6 +527,8 @@ oa_status oa_solve(const oa_settings* S, oa_outputs* out) {
     W.fl = &FL;
     W.fr = &FR;
     W.name_base = first;
+    W.name_stride = file_r;
+    W.name_first_only = combine;
     W.dis = fopen((fout_eff + "_dis.txt").c_str(), "wb");
     if (!W.dis) {
         herr("Error Creating File %s_dis.txt", fout_eff.c_str());
@@ -501,7 +548,12 @@ oa_status oa_solve(const oa_settings* S, oa_outputs* out) {
         const uint8_t flags[2] = {(uint8_t)(S->disp_cov ? 1 : 0), (uint8_t)(S->store_all ? 1 : 0)};
         fwrite(flags, 1, 2, fi);
         fwrite(FL.raw((size_t)FL.nobs + 1), 1, (size_t)FL.namelength * (l - 1), fi);
-        fwrite(FR.raw((size_t)FR.nobs + (size_t)first * r), 1, (size_t)FR.namelength * r * m, fi);
+        if (combine) {   // one name per SNP: its first file column (src/AIOwrapper.cpp:711-721)
+            for (int i = 0; i < m; ++i)
+                fwrite(FR.raw((size_t)FR.nobs + (size_t)(first + i) * file_r), 1, (size_t)FR.namelength, fi);
+        } else {
+            fwrite(FR.raw((size_t)FR.nobs + (size_t)first * r), 1, (size_t)FR.namelength * r * m, fi);
+        }
         fwrite(FY.raw(FY.nobs), 1, (size_t)FY.namelength * t, fi);
         fclose(fi);
         W.dbin = fopen((fout_eff + "_sto.dbin").c_str(), "wb");
@@ -517,7 +569,7 @@ oa_status oa_solve(const oa_settings* S, oa_outputs* out) {
     const int mb_ref = std::min(m, 500);
     W.mb_ref = mb_ref;
     // SNPs per engine call: a multiple of the reference block, about 1 GB of genotypes
-    int call_snps = (int)std::max<int64_t>(1, (int64_t)(1u << 28) / ((int64_t)n * r));
+    int call_snps = (int)std::max<int64_t>(1, (int64_t)(1u << 28) / ((int64_t)n * file_r));
     call_snps = std::max(mb_ref, call_snps / mb_ref * mb_ref);
     call_snps = std::min(call_snps, m);
     oa_config cfg{};
@@ -553,6 +605,10 @@ oa_status oa_solve(const oa_settings* S, oa_outputs* out) {
     };
     st = oa_set_covariates(eng, XL.data());
     if (st != OA_OK) return fail(st);
+    if (model) {
+        st = oa_set_column_model(eng, file_r, model_w, combine ? 1 : 0);
+        if (st != OA_OK) return fail(st);
+    }
 
     FILE* fr = fopen((fxr + ".fvd").c_str(), "rb");
     FILE* fyd = fopen((fy + ".fvd").c_str(), "rb");
@@ -567,7 +623,7 @@ oa_status oa_solve(const oa_settings* S, oa_outputs* out) {
     }
     // pinned double buffers for the SNP blocks (copied with cudaMemcpyAsync by the engine)
     float* pin[2] = {nullptr, nullptr};
-    const size_t pin_floats = (size_t)call_snps * r * n;
+    const size_t pin_floats = (size_t)call_snps * file_r * n;
     for (int b = 0; b < 2; ++b)
         if (cudaMallocHost(&pin[b], sizeof(float) * pin_floats) != cudaSuccess) {
             cudaGetLastError();
@@ -591,7 +647,8 @@ oa_status oa_solve(const oa_settings* S, oa_outputs* out) {
         if (st != OA_OK) break;
         auto read_call = [&](int c, int b) {
             const int s0 = c * call_snps, cnt = std::min(call_snps, m - s0);
-            return read_columns(fr, fileN, (size_t)(first + s0) * r, (size_t)cnt * r, runs, n, pin[b], scratch[b]);
+            return read_columns(fr, fileN, (size_t)(first + s0) * file_r, (size_t)cnt * file_r, runs, n, pin[b],
+                                scratch[b]);
         };
         std::future<bool> next = std::async(std::launch::async, read_call, 0, 0);
         for (int c = 0; c < ncalls; ++c) {
@@ -678,7 +735,7 @@ int oa_cli_main(int argc, char** argv) {
     oa_settings S;
     oa_default_settings(&S);
     S.verbose = 1;
-    std::string fy, fr, fl, fo, fx;
+    std::string fy, fr, fl, fo, fx, ffac;
     bool phe = false, snp = false, cov = false, bout = false, shard_set = false, device_set = false;
     static struct option opts[] = {{"phe", required_argument, 0, 'p'},
                                    {"geno", required_argument, 0, 'g'},
@@ -728,8 +785,30 @@ int oa_cli_main(int argc, char** argv) {
             case 'i': S.disp_cov = 1; break;
             case 'f': S.store_all = 1; break;
             case 'b': S.store_bin = 1; break;
-            case 'j': case 'k': case 'l': case 'z': case 'y': case 'v': case 'w': case 'u':
-                fprintf(stdout, "option -%c (dosage models / interaction files) is not supported by this build\n", c);
+            case 'j':
+                S.dosage_model = 1;
+                printf("-j Using Additive Model with (2*AA, 1*AB, 0*BB) effects\n");
+                break;
+            case 'k':
+                S.dosage_model = 2;
+                printf("-k Using Dominant Model with (1*AA, 1*AB, 0*BB) effects\n");
+                break;
+            case 'l':
+                S.dosage_model = 3;
+                printf("-j Using Recessive Model with (1*AA, 0*AB, 0*BB) effects\n");
+                break;
+            case 'z':
+                S.dosage_model = 4;
+                ffac = optarg;
+                printf("-z Using Custom Linear Model with parameters read from the file %s\n", optarg);
+                break;
+            case 'y':
+                S.dosage_model = 5;
+                ffac = optarg;
+                printf("-z Using Custom Additive Model with parameters read from the file %s\n", optarg);
+                break;
+            case 'v': case 'w': case 'u':
+                fprintf(stdout, "option -%c (interaction files) is not supported by this build\n", c);
                 return 1;
             case 'h': fputs(kHelp, stdout); return 1;
             case 1000:
@@ -778,6 +857,7 @@ int oa_cli_main(int argc, char** argv) {
     S.fname_xl = fl.c_str();
     S.fname_out = fo.c_str();
     S.fname_exclude = fx.empty() ? nullptr : fx.c_str();
+    S.fname_factors = ffac.empty() ? nullptr : ffac.c_str();
     printf("omicabelnomm-b200\n");
     oa_outputs out;
     const oa_status st = oa_solve(&S, &out);

@@ -54,7 +54,8 @@ class Settings(C.Structure):
                 ("min_p_disp", C.c_float), ("min_p_store", C.c_float), ("min_r2_disp", C.c_float),
                 ("min_r2_store", C.c_float), ("store_bin", C.c_int32), ("disp_cov", C.c_int32),
                 ("store_all", C.c_int32), ("precision", C.c_int32), ("device", C.c_int32),
-                ("quirk_r2", C.c_int32), ("verbose", C.c_int32), ("shard", C.c_int32), ("shards", C.c_int32)]
+                ("quirk_r2", C.c_int32), ("verbose", C.c_int32), ("shard", C.c_int32), ("shards", C.c_int32),
+                ("dosage_model", C.c_int32), ("fname_factors", C.c_char_p)]
 
 
 class Tuning(C.Structure):
@@ -110,6 +111,7 @@ def lib() -> C.CDLL:
         "oa_set_snp_rows": ([P, C.POINTER(C.c_int32), C.c_int32, C.c_int64], C.c_int),
         "oa_device_bytes": ([P], C.c_int64),
         "oa_reserve": ([P, C.c_int32, C.c_int32], C.c_int),
+        "oa_set_column_model": ([P, C.c_int32, fp, C.c_int32], C.c_int),
         "oa_omicout": ([C.c_char_p, C.c_char_p, C.c_float, C.c_float, C.c_int32, C.c_int32,
                         C.POINTER(C.c_int64)], C.c_int),
         "oa_omicout_main": ([C.c_int, C.POINTER(C.c_char_p)], C.c_int),
@@ -208,9 +210,10 @@ class Engine:
     def run(self, XR: np.ndarray) -> StoredRows:
         """XR as a (mb*r, n) float32 array; returns the stored rows in (trait, SNP) order."""
         XR = np.ascontiguousarray(XR, dtype=np.float32)
-        assert XR.shape[1] == self.n and XR.shape[0] % self.r == 0
+        cols = getattr(self, "in_cols", 0) or self.r
+        assert XR.shape[1] == self.n and XR.shape[0] % cols == 0
         rows = Rows()
-        _check(lib().oa_run_snps(self.h, _fptr(XR), XR.shape[0] // self.r, C.byref(rows)))
+        _check(lib().oa_run_snps(self.h, _fptr(XR), XR.shape[0] // cols, C.byref(rows)))
         return self._rows(rows)
 
     def run_raw(self, XR: np.ndarray) -> Rows:
@@ -280,6 +283,12 @@ class Engine:
     def device_bytes(self) -> int:
         return int(lib().oa_device_bytes(self.h))
 
+    def set_column_model(self, in_cols: int, weights=None, combine: bool = True) -> None:
+        """oa_set_column_model: SNPs arrive as in_cols file columns combined (or scaled) on the device."""
+        w = np.ascontiguousarray(weights if weights is not None else np.ones(max(in_cols, 1)), dtype=np.float32)
+        _check(lib().oa_set_column_model(self.h, int(in_cols), _fptr(w), int(combine)))
+        self.in_cols = int(in_cols)
+
     def reserve(self, traits: int, snps: int) -> None:
         """oa_reserve: allocate now what blocks of up to `traits` traits x `snps` SNPs need."""
         _check(lib().oa_reserve(self.h, int(traits), int(snps)))
@@ -330,12 +339,15 @@ def pvalue(t: float) -> float:
 
 def solve(xl: str, xr: str, y: str, out: str, *, r: int = 1, exclude: str = "", store_bin=False,
           disp_cov=False, store_all=False, precision=PLAIN, device=0, min_p_disp=None, min_p_store=None,
-          min_r2_disp=None, min_r2_store=None, verbose=False, shard=0, shards=1) -> Outputs:
+          min_r2_disp=None, min_r2_store=None, verbose=False, shard=0, shards=1, dosage_model=0,
+          factors: str = "") -> Outputs:
     """≙ Algorithm::solve on files: writes out_dis.txt (+ _sto.ibin/.dbin)."""
     L = lib()
     s = Settings()
     L.oa_default_settings(C.byref(s))
-    keep = [v.encode() for v in (xl, xr, y, out, exclude)]
+    keep = [v.encode() for v in (xl, xr, y, out, exclude, factors)]
+    s.dosage_model = int(dosage_model)
+    s.fname_factors = keep[5] if factors else None
     s.fname_xl, s.fname_xr, s.fname_y, s.fname_out = keep[:4]
     s.fname_exclude = keep[4] if exclude else None
     s.r = r

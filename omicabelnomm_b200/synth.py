@@ -49,6 +49,8 @@ class Workload:
     group_max: int = 0                 # patterns mode: largest group size with Zipf sizes
     xr_nan_frac: float = 0.0           # fraction of NaN dosages (mean-imputed by the engine)
     xl_nan_rows: int = 0               # rows with a NaN covariate (dropped by the reader)
+    prob_cols: int = 0                 # 2 or 3: genotype-probability columns per SNP (AA, AB[, BB])
+                                       # instead of one dosage column (input of the dosage models)
     seed: int = 0
     name: str = "custom"
 
@@ -142,13 +144,46 @@ def dosages(rng, n: int, m: int, maf_lo: float, maf_hi: float,
     return np.round(np.clip(g, 0.0, 2.0), 3).astype(np.float32)
 
 
+def genotype_probabilities(rng, n: int, m: int, maf_lo: float, maf_hi: float, cols: int):
+    """Imputed genotype probabilities: genotype g ~ Binomial(2, maf) (copies of
+    the counted allele), its class AA (g = 2), AB (g = 1) or BB (g = 0) gets
+    1 - e with e ~ U(0, 0.3), the other two classes share e; rounded to 0.001.
+    Returns the (m*cols, n) file columns [P(AA), P(AB)(, P(BB))] per SNP, the
+    additive dosage 2 P(AA) + P(AB) (m, n) and the column names."""
+    if cols not in (2, 3):
+        raise ValueError("genotype probabilities come as 2 or 3 columns per SNP")
+    maf = rng.uniform(maf_lo, maf_hi, m)
+    g = rng.binomial(2, maf[:, None], (m, n))
+    e = rng.uniform(0.0, 0.3, (m, n))
+    split = rng.uniform(0.0, 1.0, (m, n))
+    P = np.empty((m, 3, n))
+    for cls, gval in enumerate((2, 1, 0)):
+        hit = g == gval
+        others = [c for c in range(3) if c != cls]
+        P[:, cls][hit] = 1.0 - e[hit]
+        P[:, others[0]][hit] = e[hit] * split[hit]
+        P[:, others[1]][hit] = e[hit] * (1.0 - split[hit])
+    P = np.round(P, 3).astype(np.float32)
+    XR = np.ascontiguousarray(P[:, :cols].reshape(m * cols, n))
+    X = (2.0 * P[:, 0] + P[:, 1]).astype(np.float32)
+    names = []
+    for i in range(m):
+        names += [f"snp{i + 1}_{c}" for c in ("AA", "AB", "BB")[:cols]]
+    return XR, X, names
+
+
 def generate(w: Workload) -> Dataset:
     """Draw one workload in memory.  Meant for n*m up to a few 1e8."""
     rng = np.random.Generator(np.random.PCG64(w.seed))
     n, m, t, r = w.n, w.m, w.t, w.r
     XL, xl_names = covariates(rng, w)
-    X = dosages(rng, n, m, w.maf_lo, w.maf_hi, w.low_maf_frac)
-    if r == 1:
+    if w.prob_cols:
+        XR, X, xr_names = genotype_probabilities(rng, n, m, w.maf_lo, w.maf_hi, w.prob_cols)
+    else:
+        X = dosages(rng, n, m, w.maf_lo, w.maf_hi, w.low_maf_frac)
+    if w.prob_cols:
+        pass
+    elif r == 1:
         XR = X
         xr_names = [f"snp{i + 1}" for i in range(m)]
     elif r == 2:

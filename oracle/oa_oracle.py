@@ -68,6 +68,43 @@ class Settings:
     disp_cov: bool = False       # -i
     fname_excludelist: str = ""  # -x
     quirk_r2: bool = False
+    model: int = 0               # dosage model: 0 none, 1 additive (-j), 2 dominant (-k), 3 recessive (-l),
+                                 # 4 custom linear (-z), 5 custom additive (-y); r is then the file's
+                                 # columns per SNP (-n)
+    factors: tuple = ()          # -z / -y factors, one per file column of a SNP
+
+
+# Factors of the fixed dosage models on genotype probabilities (AA, AB, BB)
+# (src/AIOwrapper.cpp:268-321); a zero factor drops its column, which the
+# reference does not read.
+MODEL_FACTORS = {1: (2.0, 1.0, 0.0), 2: (1.0, 1.0, 0.0), 3: (1.0, 0.0, 0.0)}
+
+
+def column_model(XR: np.ndarray, names: List[str], s: "Settings"):
+    """The reference's dosage models (src/AIOwrapper.cpp:257-340, 1213-1275):
+    (m*fileR, n) file columns -> (m*r, n) model columns, their names and r.
+    Combined models give one column per SNP, named after its first file column."""
+    fr = s.r
+    m = XR.shape[0] // fr
+    if s.model in MODEL_FACTORS:
+        if fr not in (2, 3):
+            raise ValueError("the fixed dosage models take 2 or 3 columns per SNP")
+        w, combine = MODEL_FACTORS[s.model][:fr], True
+    elif s.model in (4, 5):
+        if len(s.factors) != fr:
+            raise ValueError("one factor per file column")
+        w, combine = tuple(float(f) for f in s.factors), s.model == 5
+    else:
+        raise ValueError(f"dosage model {s.model}")
+    cols = XR.reshape(m, fr, -1).astype(np.float64)
+    if combine:
+        out = np.zeros((m, cols.shape[2]))
+        for c, wc in enumerate(w):
+            if wc != 0.0:
+                out += wc * cols[:, c]
+        return out.astype(np.float32), [names[i * fr] for i in range(m)], 1
+    out = cols * np.asarray(w)[None, :, None]
+    return out.reshape(m * fr, -1).astype(np.float32), list(names), fr
 
 
 def erf_inv(z: float) -> float:
@@ -192,6 +229,7 @@ class Inputs:
     y_names: List[str]
     realN: int
     kept: np.ndarray
+    r: int = 0          # columns per SNP of XR after a dosage model (0: Settings.r)
 
 
 def load(xl_prefix: str, xr_prefix: str, y_prefix: str, s: Settings) -> Inputs:
@@ -213,9 +251,12 @@ def load(xl_prefix: str, xr_prefix: str, y_prefix: str, s: Settings) -> Inputs:
         keep[exclusion_rows(s.fname_excludelist, n)] = False
     keep &= ~np.isnan(XL).any(axis=0)
     kept = np.nonzero(keep)[0]
+    xr_names, r_eff = fr["var"], 0
+    if s.model:
+        XR, xr_names, r_eff = column_model(XR, xr_names, s)
     return Inputs(XL=XL[:, kept], XR=XR[:, kept], Y=Y[:, kept],
-                  xl_names=fl["var"], xr_names=fr["var"], y_names=fy["var"],
-                  realN=n, kept=kept)
+                  xl_names=fl["var"], xr_names=xr_names, y_names=fy["var"],
+                  realN=n, kept=kept, r=r_eff)
 
 
 # ----------------------------------------------------------------------------
@@ -261,7 +302,7 @@ def _pair_products(XRc: np.ndarray, r: int):
 
 
 def solve(inp: Inputs, s: Settings, snp_chunk: int = 2048, keep_dense: bool = False) -> Results:
-    r = s.r
+    r = inp.r or s.r
     XL = inp.XL.astype(np.float64)
     l, n = XL.shape
     p = l + r

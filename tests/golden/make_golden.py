@@ -9,7 +9,9 @@ For every case in CASES this script
 
 1. draws the inputs with ``omicabelnomm_b200.synth`` (seeded, so the test
    suite regenerates them byte for byte; the manifest keeps their sha256),
-2. runs ``oracle/_ref/omicabelnomm_ref`` with the case's flags,
+2. runs ``oracle/_ref/omicabelnomm_ref`` with the case's flags (for the
+   dosage models -j/-k/-l, which the reference's command line rejects,
+   ``oracle/_ref/ref_model_driver``: its solver with the model set in-process),
 3. stores the reference's ``_dis.txt`` (gzip) and, with ``-b``, its
    ``_sto.ibin`` / ``_sto.dbin`` plus the printed "Number of Significant
    Results" in ``tests/golden/<case>/``.
@@ -34,6 +36,9 @@ sys.path.insert(0, ROOT)
 from omicabelnomm_b200 import synth  # noqa: E402
 
 REF_BIN = os.path.join(ROOT, "oracle", "_ref", "omicabelnomm_ref")
+# the reference's solver with a dosage model set in-process (its CLI cannot reach the models)
+REF_MODEL = os.path.join(ROOT, "oracle", "_ref", "ref_model_driver")
+MODEL_FLAGS = {"-j": 0, "-k": 1, "-l": 2, "-z": 3, "-y": 4}   # the reference's Settings::model values
 
 # name -> (workload overrides on config 0, post-processing, [flag sets])
 CASES = {
@@ -59,7 +64,20 @@ CASES = {
                     [["-n", "2", "-f"], ["-n", "2", "-i"], ["-n", "2", "-b"]]),
     # r = 2 with missingness (the reference's downdate bug applies)
     "r2_missing": (dict(n=400, m=60, t=6, l=4, r=2, seed=19), None, [["-n", "2", "-f"]]),
+    # dosage models on genotype probabilities: three columns (AA, AB, BB) per SNP
+    "r1_dos3": (dict(n=400, m=60, t=8, prob_cols=3, seed=31), None,
+                [["-n", "3", "-j"], ["-n", "3", "-k"], ["-n", "3", "-l"], ["-n", "3", "-j", "-b"],
+                 ["-n", "3", "-k", "-f"]]),
+    # ... and two columns (AA, AB)
+    "r1_dos2": (dict(n=300, m=50, t=6, prob_cols=2, seed=32), None,
+                [["-n", "2", "-j"], ["-n", "2", "-k", "-b"]]),
+    # custom models with a factors file on (AA, AB): linear (each column scaled, r = 2; with all
+    # three columns, which sum to 1, the model would be collinear with the intercept) and additive
+    "r1_dosf": (dict(n=400, m=40, t=6, prob_cols=2, seed=33), "factors",
+                [["-n", "2", "-z", "{fac}"], ["-n", "2", "-y", "{fac}"], ["-n", "2", "-y", "{fac}", "-b"]]),
 }
+
+FACTORS = "0.5 1.5\n"
 
 EXCLUDE_LIST = "1 2\n5\n7\n9 11\n13\n40 44\n"
 
@@ -83,6 +101,11 @@ def build_inputs(case: str, where: str):
         with open(p, "w") as f:
             f.write(EXCLUDE_LIST)
         extra["excl"] = p
+    if post == "factors":
+        p = os.path.join(where, case + "_factors.txt")
+        with open(p, "w") as f:
+            f.write(FACTORS)
+        extra["fac"] = p
     return pre, extra
 
 
@@ -105,13 +128,19 @@ def flag_tag(flags) -> str:
     return t or "default"
 
 
-def main():
+def main(only=None):
+    """Run every case, or only the named ones (merged into the existing manifest)."""
     if not os.path.exists(REF_BIN):
         sys.exit("build the reference first: make -C oracle")
     manifest = {}
+    if only:
+        with open(os.path.join(HERE, "manifest.json")) as f:
+            manifest = json.load(f)["cases"]
     tmp = tempfile.mkdtemp(prefix="oa_golden_")
     try:
         for case, (over, post, flagsets) in CASES.items():
+            if only and case not in only:
+                continue
             pre, extra = build_inputs(case, tmp)
             cdir = os.path.join(HERE, case)
             os.makedirs(cdir, exist_ok=True)
@@ -120,7 +149,15 @@ def main():
                 tag = flag_tag(flags)
                 args = [f.format(**extra) for f in flags]
                 out = os.path.join(tmp, f"{case}_{tag}")
-                cmd = [REF_BIN, "-c", pre + "XL", "-g", pre + "XR", "-p", pre + "Y", "-o", out] + args
+                model = [f for f in args if f in MODEL_FLAGS]
+                if model:
+                    ngpred = args[args.index("-n") + 1]
+                    rest = [f for f in args if f in ("-b", "-f", "-i")]
+                    fac = args[args.index(model[0]) + 1] if model[0] in ("-z", "-y") else "-"
+                    cmd = [REF_MODEL, pre + "XL", pre + "XR", pre + "Y", out, ngpred, str(MODEL_FLAGS[model[0]]),
+                           fac] + rest
+                else:
+                    cmd = [REF_BIN, "-c", pre + "XL", "-g", pre + "XR", "-p", pre + "Y", "-o", out] + args
                 p = subprocess.run(cmd, capture_output=True, text=True, timeout=600)
                 if p.returncode != 0:
                     raise RuntimeError(f"{case} {flags}: exit {p.returncode}\n{p.stdout[-2000:]}")
@@ -144,4 +181,4 @@ def main():
 
 
 if __name__ == "__main__":
-    main()
+    main(sys.argv[1:])

@@ -61,6 +61,12 @@ def settings_for(flags, extra) -> O.Settings:
             s.r = int(next(it))
         elif f == "-x":
             s.fname_excludelist = next(it).format(**extra)
+        elif f in ("-j", "-k", "-l"):
+            s.model = {"-j": 1, "-k": 2, "-l": 3}[f]
+        elif f in ("-z", "-y"):
+            s.model = 4 if f == "-z" else 5
+            with open(next(it).format(**extra)) as fh:
+                s.factors = tuple(float(v) for v in fh.read().split())
         else:
             raise ValueError(f)
     return s
