@@ -154,6 +154,14 @@ oa_status oa_set_snp_rows(oa_engine* e, const int32_t* rows, int32_t n_rows, int
 #define OA_MODEL_MAX_COLS 8
 oa_status oa_set_column_model(oa_engine* e, int32_t in_cols, const float* weights, int32_t combine);
 
+/* Interaction columns (the reference's single-set interactions,
+ * src/AIOwrapper.cpp:808-840): inter holds k columns of n values (the
+ * engine's rows, column-major, no NaN); each SNP's model column x becomes the
+ * r = k (+1 with keep) columns [I_1 x, ..., I_k x (, x)].  Needs one model
+ * column per SNP (plain single-column SNPs or a combined dosage model) and
+ * r = k + keep.  oa_set_column_model(e, 0, ...) clears them. */
+oa_status oa_set_interactions(oa_engine* e, const float* inter, int32_t k, int32_t keep);
+
 /* Device memory held by the engine's buffers, in bytes. */
 int64_t oa_device_bytes(const oa_engine* e);
 
@@ -259,6 +267,9 @@ typedef struct oa_settings {
                                     4 custom linear (-z), 5 custom additive (-y) with the factors of
                                     fname_factors (src/AIOwrapper.cpp:257-340) */
     const char* fname_factors;   /* -z / -y: whitespace-separated factors, one per file column of a SNP */
+    const char* fname_interactions; /* -v: .fvi/.fvd with k interaction columns; each SNP column x
+                                       becomes [I_1 x, ..., I_k x, x] (r = k + 1) and rows with a NaN
+                                       interaction value are excluded (src/AIOwrapper.cpp:371-540) */
 } oa_settings;
 
 typedef struct oa_outputs {

@@ -279,6 +279,10 @@ struct oa_engine {
     int in_cols = 0, model_combine = 0;
     float model_w[OA_MODEL_MAX_COLS] = {};
     DBuf<float> Xmodel;
+    // interaction columns (n x n_inter, the engine's rows): the model column x becomes
+    // [I_1 x, ..., I_k x (, x)] (src/AIOwrapper.cpp:808-840)
+    DBuf<float> inter;
+    int n_inter = 0, inter_keep = 0;
     DBuf<__nv_bfloat16> Xhi, Xlo;
     DBuf<float> mean, varx, aobs, afull, zA, zD;
     DBuf<float> D, Dset, C2T;   // pre-GEMM path: X'X, per-set X'X, pre-GEMM output
@@ -361,7 +365,7 @@ void for_each_buf(oa_engine* e, F&& f) {
     f(e->set_kind); f(e->set_slot); f(e->tperm); f(e->tinv);
     f(e->a_r2); f(e->inv_ncorr); f(e->vf); f(e->thash); f(e->sst); f(e->qrows); f(e->pat_bad);
     f(e->B2); f(e->B2hi); f(e->B2lo);
-    f(e->Xstage[0]); f(e->Xstage[1]); f(e->Xmodel); f(e->Xhi); f(e->Xlo);
+    f(e->Xstage[0]); f(e->Xstage[1]); f(e->Xmodel); f(e->inter); f(e->Xhi); f(e->Xlo);
     f(e->mean); f(e->varx); f(e->aobs); f(e->afull); f(e->zA); f(e->zD); f(e->D); f(e->Dset); f(e->C2T);
     f(e->has_nan); f(e->sinv); f(e->sfinv); f(e->sing);
     f(e->rec); f(e->rec2); f(e->cov); f(e->cov2); f(e->counters); f(e->keys); f(e->keys2); f(e->perm);
@@ -388,6 +392,7 @@ struct ModelW {
     float w[OA_MODEL_MAX_COLS];
 };
 static __global__ void k_column_model(const float* __restrict__ in, int n, int in_cols, ModelW W, int combine,
+                                      const float* __restrict__ inter, int n_inter, int keep,
                                       float* __restrict__ out) {
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
     const int i = blockIdx.y;
@@ -402,7 +407,13 @@ static __global__ void k_column_model(const float* __restrict__ in, int n, int i
             acc = any ? fmaf(W.w[c], x, acc) : W.w[c] * x;
             any = true;
         }
-        out[(size_t)i * n + k] = acc;
+        if (n_inter == 0) {
+            out[(size_t)i * n + k] = acc;
+        } else {   // [I_1 x, ..., I_k x (, x)] (src/AIOwrapper.cpp:808-840)
+            const int r = n_inter + keep;
+            for (int h = 0; h < n_inter; ++h) out[((size_t)i * r + h) * n + k] = inter[(size_t)h * n + k] * acc;
+            if (keep) out[((size_t)i * r + n_inter) * n + k] = acc;
+        }
     } else {
         for (int c = 0; c < in_cols; ++c) out[((size_t)i * in_cols + c) * n + k] = W.w[c] * src[(size_t)c * n];
     }
@@ -1071,7 +1082,7 @@ oa_status enqueue_block(oa_engine* e, const float* xr, int mb, bool host_input, 
             ModelW W;
             for (int c = 0; c < OA_MODEL_MAX_COLS; ++c) W.w[c] = e->model_w[c];
             k_column_model<<<dim3((unsigned)((e->n + 255) / 256), (unsigned)mbc), 256, 0, e->st>>>(
-                X, e->n, e->in_cols, W, e->model_combine, e->Xmodel.p);
+                X, e->n, e->in_cols, W, e->model_combine, e->inter.p, e->n_inter, e->inter_keep, e->Xmodel.p);
             ++e->launches;
             OA_CU(cudaGetLastError());
             X = e->Xmodel.p;
@@ -1774,8 +1785,9 @@ oa_status oa_set_column_model(oa_engine* e, int32_t in_cols, const float* weight
         set_err("null engine");
         return OA_ERR_ARG;
     }
-    if (in_cols == 0) {   // plain input
+    if (in_cols == 0) {   // plain input (and no interactions)
         e->in_cols = 0;
+        e->n_inter = e->inter_keep = 0;
         drop_graph(e);
         ++e->tune_gen;
         return OA_OK;
@@ -1784,9 +1796,10 @@ oa_status oa_set_column_model(oa_engine* e, int32_t in_cols, const float* weight
         set_err("column model of %d file columns per SNP (1..%d, with weights)", in_cols, OA_MODEL_MAX_COLS);
         return OA_ERR_ARG;
     }
-    if ((combine && e->r != 1) || (!combine && e->r != in_cols)) {
-        set_err("column model: %s needs r = %d, the engine has r = %d", combine ? "a combined column" : "scaled columns",
-                combine ? 1 : in_cols, e->r);
+    const int want_r = combine ? (e->n_inter > 0 ? e->n_inter + e->inter_keep : 1) : in_cols;
+    if (want_r != e->r || (!combine && e->n_inter > 0)) {
+        set_err("column model: %s needs r = %d, the engine has r = %d",
+                combine ? "a combined column" : "scaled columns (no interactions)", want_r, e->r);
         return OA_ERR_ARG;
     }
     if (e->subset) {
@@ -1796,6 +1809,42 @@ oa_status oa_set_column_model(oa_engine* e, int32_t in_cols, const float* weight
     e->in_cols = in_cols;
     e->model_combine = combine ? 1 : 0;
     for (int c = 0; c < OA_MODEL_MAX_COLS; ++c) e->model_w[c] = c < in_cols ? weights[c] : 0.f;
+    drop_graph(e);
+    ++e->tune_gen;
+    return OA_OK;
+}
+
+oa_status oa_set_interactions(oa_engine* e, const float* inter, int32_t k, int32_t keep) {
+    clear_stale_error(__func__);
+    if (!e || (k > 0 && !inter)) {
+        set_err("null argument");
+        return OA_ERR_ARG;
+    }
+    if (k < 1 || k + (keep ? 1 : 0) != e->r) {
+        set_err("%d interaction columns%s need r = %d, the engine has r = %d", k, keep ? " + the SNP" : "",
+                k + (keep ? 1 : 0), e->r);
+        return OA_ERR_ARG;
+    }
+    if (e->in_cols > 0 && !e->model_combine) {
+        set_err("interactions apply to one model column per SNP (not the custom linear model)");
+        return OA_ERR_ARG;
+    }
+    if (e->subset) {
+        set_err("interactions do not apply to row subsets of a resident matrix");
+        return OA_ERR_STATE;
+    }
+    OA_CU(cudaSetDevice(e->cfg.device));
+    AllocOn alloc_on(e->st);
+    OA_CHECK(e->inter.ensure((size_t)e->n * k));
+    OA_CU(cudaMemcpyAsync(e->inter.p, inter, sizeof(float) * (size_t)e->n * k, cudaMemcpyHostToDevice, e->st));
+    OA_CU(cudaStreamSynchronize(e->st));
+    if (e->in_cols == 0) {   // plain single-column SNPs: the identity model
+        e->in_cols = 1;
+        e->model_combine = 1;
+        for (int c = 0; c < OA_MODEL_MAX_COLS; ++c) e->model_w[c] = c == 0 ? 1.f : 0.f;
+    }
+    e->n_inter = k;
+    e->inter_keep = keep ? 1 : 0;
     drop_graph(e);
     ++e->tune_gen;
     return OA_OK;

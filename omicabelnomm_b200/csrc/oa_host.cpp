@@ -247,6 +247,7 @@ struct Writer {
     int name_base = 0;   // first SNP of this shard in the genotype file (names only; indices are shard-local)
     int name_stride = 1;           // file columns per SNP
     bool name_first_only = false;  // a combined dosage model names a SNP by its first file column
+    int n_inter = 0;               // interaction columns: SNP term a < n_inter is named "I<a+1>x<SNP>"
     const Fvi* fy = nullptr;
     const Fvi* fl = nullptr;
     const Fvi* fr = nullptr;
@@ -300,7 +301,13 @@ struct Writer {
                     std::string aname = " ";
                     if (h < l) aname = fl->var_name(h) + ":";
                     const size_t snp_g = (size_t)(name_base + snp);
-                    aname += fr->var_name(snp_g * name_stride + (name_first_only ? 0 : (size_t)(h >= l ? h - l : 0)));
+                    const int term = h >= l ? h - l : 0;
+                    if (n_inter > 0) {   // src/AIOwrapper.cpp:566-612
+                        if (term < n_inter) aname += "I" + std::to_string(term + 1) + "x";
+                        aname += fr->var_name(snp_g * name_stride);
+                    } else {
+                        aname += fr->var_name(snp_g * name_stride + (name_first_only ? 0 : (size_t)term));
+                    }
                     const int len = snprintf(line, sizeof line, "%s\t%s\t%u\t%.2f\t%.7f\t%.4f\t%.7f\t%.7f\t%.7Le\n",
                                              fy->var_name(ytr).c_str(), aname.c_str(), (unsigned)nused,
                                              (double)npct, (double)B, (double)r2, (double)SE, (double)T, P);
@@ -439,6 +446,30 @@ oa_status oa_solve(const oa_settings* S, oa_outputs* out) {
         r = combine ? 1 : file_r;
     }
     const bool model = S->dosage_model != 0;
+    // single-set interactions: k columns, each SNP column x -> [I_1 x, ..., I_k x, x] (src/AIOwrapper.cpp:371-480)
+    Fvi FI;
+    const bool use_inter = S->fname_interactions && S->fname_interactions[0];
+    int n_inter = 0;
+    if (use_inter) {
+        if (r != 1) {
+            herr("Cannot use Interactions with --ngpred set to: %d. Required is 1!\nInteractions can be only of the "
+                 "form y~cov+V1*X+...+Vi*X, (only with --ngpred=1 or models excluding(--mylinear)) !",
+                 file_r);
+            return OA_ERR_ARG;
+        }
+        if (!read_fvi(std::string(S->fname_interactions) + ".fvi", FI)) return OA_ERR_IO;
+        if (FI.nobs != FR.nobs) {
+            herr("The number of elements/individuals from the input files do not coincide with each other! %s:%u %s:%u",
+                 S->fname_interactions, FI.nobs, fxr.c_str(), FR.nobs);
+            return OA_ERR_IO;
+        }
+        n_inter = (int)FI.nvar;
+        if (n_inter < 1 || n_inter + 1 > OA_MAX_R) {
+            herr("%d interaction columns: this build supports 1..%d", n_inter, OA_MAX_R - 1);
+            return OA_ERR_UNSUPPORTED;
+        }
+        r = n_inter + 1;
+    }
     const int m_file = (int)(FR.nvar / file_r), t = (int)FY.nvar, l = (int)FL.nvar, p = l + r;
     // SNP shard of this process (the reference's MPI split, src/AIOwrapper.cpp:95-117)
     const int shards = std::max(1, S->shards);
@@ -491,8 +522,34 @@ oa_status oa_solve(const oa_settings* S, oa_outputs* out) {
                 ++almiss;
             }
     if (almiss > 0 && verbose) printf("Excluding %d from covariate missings\n", almiss);
+    std::vector<float> inter_all;
+    int intermiss = 0;
+    if (use_inter) {
+        for (int i = 0; i < fileN; ++i)
+            if (FI.obs_name(i) != FR.obs_name(i)) {
+                if (verbose)
+                    printf("Warning, ID names between -g file and interactions file do not coincide! The files must "
+                           "have the same meaningful order!\n");
+                break;
+            }
+        inter_all.resize((size_t)n_inter * fileN);
+        FILE* fp = fopen((std::string(S->fname_interactions) + ".fvd").c_str(), "rb");
+        const size_t got = fp ? fread(inter_all.data(), sizeof(float), inter_all.size(), fp) : 0;
+        if (fp) fclose(fp);
+        if (got != inter_all.size()) {
+            herr("Error opening Interactions File %s", S->fname_interactions);
+            return OA_ERR_IO;
+        }
+        for (int h = 0; h < n_inter; ++h)   // rows with a NaN interaction value (src/AIOwrapper.cpp:519-533)
+            for (int i = 0; i < fileN; ++i)
+                if (std::isnan(inter_all[(size_t)h * fileN + i]) && keep[i]) {
+                    keep[i] = 0;
+                    ++intermiss;
+                }
+        if (intermiss > 0 && verbose) printf("Excluding %d from Interaction missings\n", intermiss);
+    }
     const Runs runs = keep_runs(keep);
-    const int n = fileN - excl - almiss;
+    const int n = fileN - excl - almiss - intermiss;
     if (p >= n) {
         herr("Error! The amount of unknows (individuals|elements) must be greater than total of variables "
              "(#covariates+#ind.variables)!");
@@ -529,6 +586,7 @@ oa_status oa_solve(const oa_settings* S, oa_outputs* out) {
     W.name_base = first;
     W.name_stride = file_r;
     W.name_first_only = combine;
+    W.n_inter = n_inter;
     W.dis = fopen((fout_eff + "_dis.txt").c_str(), "wb");
     if (!W.dis) {
         herr("Error Creating File %s_dis.txt", fout_eff.c_str());
@@ -552,7 +610,8 @@ oa_status oa_solve(const oa_settings* S, oa_outputs* out) {
             for (int i = 0; i < m; ++i)
                 fwrite(FR.raw((size_t)FR.nobs + (size_t)(first + i) * file_r), 1, (size_t)FR.namelength, fi);
         } else {
-            fwrite(FR.raw((size_t)FR.nobs + (size_t)first * r), 1, (size_t)FR.namelength * r * m, fi);
+            // the file's names, fileR per SNP, also with interactions (src/AIOwrapper.cpp:722-728)
+            fwrite(FR.raw((size_t)FR.nobs + (size_t)first * file_r), 1, (size_t)FR.namelength * file_r * m, fi);
         }
         fwrite(FY.raw(FY.nobs), 1, (size_t)FY.namelength * t, fi);
         fclose(fi);
@@ -607,6 +666,18 @@ oa_status oa_solve(const oa_settings* S, oa_outputs* out) {
     if (st != OA_OK) return fail(st);
     if (model) {
         st = oa_set_column_model(eng, file_r, model_w, combine ? 1 : 0);
+        if (st != OA_OK) return fail(st);
+    }
+    if (use_inter) {   // the kept rows of each interaction column
+        std::vector<float> I((size_t)n_inter * n);
+        for (int h = 0; h < n_inter; ++h) {
+            size_t pos = 0;
+            for (const auto& run : runs) {
+                memcpy(&I[(size_t)h * n + pos], &inter_all[(size_t)h * fileN + run.first], sizeof(float) * run.second);
+                pos += run.second;
+            }
+        }
+        st = oa_set_interactions(eng, I.data(), n_inter, 1);
         if (st != OA_OK) return fail(st);
     }
 
@@ -735,7 +806,7 @@ int oa_cli_main(int argc, char** argv) {
     oa_settings S;
     oa_default_settings(&S);
     S.verbose = 1;
-    std::string fy, fr, fl, fo, fx, ffac;
+    std::string fy, fr, fl, fo, fx, ffac, finter;
     bool phe = false, snp = false, cov = false, bout = false, shard_set = false, device_set = false;
     static struct option opts[] = {{"phe", required_argument, 0, 'p'},
                                    {"geno", required_argument, 0, 'g'},
@@ -807,8 +878,15 @@ int oa_cli_main(int argc, char** argv) {
                 ffac = optarg;
                 printf("-z Using Custom Additive Model with parameters read from the file %s\n", optarg);
                 break;
-            case 'v': case 'w': case 'u':
-                fprintf(stdout, "option -%c (interaction files) is not supported by this build\n", c);
+            case 'v':
+                finter = optarg;
+                printf("-v File containing single interactions %s\n", optarg);
+                break;
+            case 'u':
+                printf("-u Keeping independent variable for interaction analysis \n");
+                break;
+            case 'w':
+                fprintf(stdout, "option -w (one analysis per interaction) is not supported by this build\n");
                 return 1;
             case 'h': fputs(kHelp, stdout); return 1;
             case 1000:
@@ -858,6 +936,7 @@ int oa_cli_main(int argc, char** argv) {
     S.fname_out = fo.c_str();
     S.fname_exclude = fx.empty() ? nullptr : fx.c_str();
     S.fname_factors = ffac.empty() ? nullptr : ffac.c_str();
+    S.fname_interactions = finter.empty() ? nullptr : finter.c_str();
     printf("omicabelnomm-b200\n");
     oa_outputs out;
     const oa_status st = oa_solve(&S, &out);

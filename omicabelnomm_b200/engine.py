@@ -55,7 +55,7 @@ class Settings(C.Structure):
                 ("min_r2_store", C.c_float), ("store_bin", C.c_int32), ("disp_cov", C.c_int32),
                 ("store_all", C.c_int32), ("precision", C.c_int32), ("device", C.c_int32),
                 ("quirk_r2", C.c_int32), ("verbose", C.c_int32), ("shard", C.c_int32), ("shards", C.c_int32),
-                ("dosage_model", C.c_int32), ("fname_factors", C.c_char_p)]
+                ("dosage_model", C.c_int32), ("fname_factors", C.c_char_p), ("fname_interactions", C.c_char_p)]
 
 
 class Tuning(C.Structure):
@@ -112,6 +112,7 @@ def lib() -> C.CDLL:
         "oa_device_bytes": ([P], C.c_int64),
         "oa_reserve": ([P, C.c_int32, C.c_int32], C.c_int),
         "oa_set_column_model": ([P, C.c_int32, fp, C.c_int32], C.c_int),
+        "oa_set_interactions": ([P, fp, C.c_int32, C.c_int32], C.c_int),
         "oa_omicout": ([C.c_char_p, C.c_char_p, C.c_float, C.c_float, C.c_int32, C.c_int32,
                         C.POINTER(C.c_int64)], C.c_int),
         "oa_omicout_main": ([C.c_int, C.POINTER(C.c_char_p)], C.c_int),
@@ -289,6 +290,13 @@ class Engine:
         _check(lib().oa_set_column_model(self.h, int(in_cols), _fptr(w), int(combine)))
         self.in_cols = int(in_cols)
 
+    def set_interactions(self, inter: np.ndarray, keep: bool = True) -> None:
+        """oa_set_interactions: inter (k, n) float32; SNP column x -> [I_1 x, ..., I_k x (, x)]."""
+        inter = np.ascontiguousarray(inter, dtype=np.float32)
+        _check(lib().oa_set_interactions(self.h, _fptr(inter), inter.shape[0], int(keep)))
+        if not getattr(self, "in_cols", 0):
+            self.in_cols = 1
+
     def reserve(self, traits: int, snps: int) -> None:
         """oa_reserve: allocate now what blocks of up to `traits` traits x `snps` SNPs need."""
         _check(lib().oa_reserve(self.h, int(traits), int(snps)))
@@ -340,14 +348,15 @@ def pvalue(t: float) -> float:
 def solve(xl: str, xr: str, y: str, out: str, *, r: int = 1, exclude: str = "", store_bin=False,
           disp_cov=False, store_all=False, precision=PLAIN, device=0, min_p_disp=None, min_p_store=None,
           min_r2_disp=None, min_r2_store=None, verbose=False, shard=0, shards=1, dosage_model=0,
-          factors: str = "") -> Outputs:
+          factors: str = "", interactions: str = "") -> Outputs:
     """≙ Algorithm::solve on files: writes out_dis.txt (+ _sto.ibin/.dbin)."""
     L = lib()
     s = Settings()
     L.oa_default_settings(C.byref(s))
-    keep = [v.encode() for v in (xl, xr, y, out, exclude, factors)]
+    keep = [v.encode() for v in (xl, xr, y, out, exclude, factors, interactions)]
     s.dosage_model = int(dosage_model)
     s.fname_factors = keep[5] if factors else None
+    s.fname_interactions = keep[6] if interactions else None
     s.fname_xl, s.fname_xr, s.fname_y, s.fname_out = keep[:4]
     s.fname_exclude = keep[4] if exclude else None
     s.r = r

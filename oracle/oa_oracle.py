@@ -72,6 +72,7 @@ class Settings:
                                  # 4 custom linear (-z), 5 custom additive (-y); r is then the file's
                                  # columns per SNP (-n)
     factors: tuple = ()          # -z / -y factors, one per file column of a SNP
+    fname_interactions: str = "" # -v: single-set interactions (the SNP column is kept)
 
 
 # Factors of the fixed dosage models on genotype probabilities (AA, AB, BB)
@@ -105,6 +106,23 @@ def column_model(XR: np.ndarray, names: List[str], s: "Settings"):
         return out.astype(np.float32), [names[i * fr] for i in range(m)], 1
     out = cols * np.asarray(w)[None, :, None]
     return out.reshape(m * fr, -1).astype(np.float32), list(names), fr
+
+
+def interaction_columns(XR: np.ndarray, names: List[str], r: int, inter: np.ndarray):
+    """Single-set interactions (src/AIOwrapper.cpp:808-840, names :566-612): each
+    SNP column x -> [I_1 x, ..., I_k x, x], named "I<h>x<name>" and <name>."""
+    if r != 1:
+        raise ValueError("interactions need one column per SNP")
+    k, m = inter.shape[0], XR.shape[0]
+    out = np.empty((m * (k + 1), XR.shape[1]), dtype=np.float32)
+    out_names = []
+    for i in range(m):
+        for h in range(k):
+            out[i * (k + 1) + h] = inter[h] * XR[i]
+            out_names.append(f"I{h + 1}x{names[i]}")
+        out[i * (k + 1) + k] = XR[i]
+        out_names.append(names[i])
+    return out, out_names, k + 1
 
 
 def erf_inv(z: float) -> float:
@@ -250,10 +268,18 @@ def load(xl_prefix: str, xr_prefix: str, y_prefix: str, s: Settings) -> Inputs:
     if s.fname_excludelist:
         keep[exclusion_rows(s.fname_excludelist, n)] = False
     keep &= ~np.isnan(XL).any(axis=0)
+    inter = None
+    if s.fname_interactions:
+        # rows with a NaN interaction value leave the analysis (src/AIOwrapper.cpp:519-533)
+        fi = read_fvi(s.fname_interactions)
+        inter = read_fvd(s.fname_interactions, fi["n"], fi["v"])
+        keep &= ~np.isnan(inter).any(axis=0)
     kept = np.nonzero(keep)[0]
     xr_names, r_eff = fr["var"], 0
     if s.model:
         XR, xr_names, r_eff = column_model(XR, xr_names, s)
+    if inter is not None:
+        XR, xr_names, r_eff = interaction_columns(XR, xr_names, r_eff or s.r, inter)
     return Inputs(XL=XL[:, kept], XR=XR[:, kept], Y=Y[:, kept],
                   xl_names=fl["var"], xr_names=xr_names, y_names=fy["var"],
                   realN=n, kept=kept, r=r_eff)

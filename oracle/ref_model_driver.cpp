@@ -6,10 +6,13 @@
 // src/main.cpp:341-358), while its reader implements the models
 // (src/AIOwrapper.cpp:257-340, 1213-1275).
 //
-//   ref_model_driver XL XR Y OUT NGPRED MODEL [FACTORS|-] [-b] [-f] [-i]
+//   ref_model_driver XL XR Y OUT NGPRED MODEL [FACTORS|-] [-b] [-f] [-i] [-v INTER]
 //
 // MODEL is the reference's Settings::model: 0 additive, 1 dominant,
-// 2 recessive, 3 custom linear, 4 custom additive.
+// 2 recessive, 3 custom linear, 4 custom additive, -1 none.  -v sets the
+// single-set interactions with the file INTER (keeping the SNP column, as
+// the reference's -v does, src/main.cpp:369-378), whose command-line form
+// stores atof(optarg) as the file name (src/main.cpp:370).
 #include <cstdlib>
 #include <cstring>
 #include <iostream>
@@ -30,7 +33,7 @@ int main(int argc, char** argv) {
     params.fnameOutFiles = argv[4];
     params.r = std::atoi(argv[5]);
     params.model = std::atoi(argv[6]);
-    params.dosages = true;
+    params.dosages = params.model >= 0;
     int a = 7;
     if (a < argc && argv[a][0] != '-') params.fname_dosages = argv[a++];
     else if (a < argc && std::strcmp(argv[a], "-") == 0) ++a;
@@ -38,6 +41,12 @@ int main(int argc, char** argv) {
         if (!std::strcmp(argv[a], "-b")) params.storeBin = true;
         else if (!std::strcmp(argv[a], "-f")) params.storePInd = true;
         else if (!std::strcmp(argv[a], "-i")) params.disp_cov = true;
+        else if (!std::strcmp(argv[a], "-v") && a + 1 < argc) {
+            params.fname_interactions = argv[++a];
+            params.use_interactions = true;
+            params.keep_depVar = true;
+            params.use_multiple_interaction_sets = false;
+        }
     }
     blas_set_num_threads(params.threads);
     Outputs out = {0};

@@ -75,9 +75,28 @@ CASES = {
     # three columns, which sum to 1, the model would be collinear with the intercept) and additive
     "r1_dosf": (dict(n=400, m=40, t=6, prob_cols=2, seed=33), "factors",
                 [["-n", "2", "-z", "{fac}"], ["-n", "2", "-y", "{fac}"], ["-n", "2", "-y", "{fac}", "-b"]]),
+    # single-set interactions (-v): SNP x I and the SNP itself (r = 2); no phenotype missingness, so
+    # the reference's r >= 2 downdate quirk does not enter; a few NaN interaction values drop rows
+    "r1_inter": (dict(n=400, m=50, t=6, l=4, miss_mode="none", seed=34), "inter",
+                 [["-v", "{inter}"], ["-v", "{inter}", "-b"], ["-v", "{inter}", "-f", "-i"]]),
+    # three interaction columns (r = 4)
+    "r1_inter3": (dict(n=400, m=30, t=5, l=3, miss_mode="none", seed=35), "inter3",
+                  [["-v", "{inter}"], ["-v", "{inter}", "-f"]]),
 }
 
 FACTORS = "0.5 1.5\n"
+
+
+def interaction_file(n: int, seed: int, prefix: str, k: int):
+    """k interaction columns of n individuals: N(0, 1), then Bernoulli(0.5), then U(0, 2);
+    the first column holds 3 NaN values."""
+    import numpy as np
+    from omicabelnomm_b200 import fvformat
+    rng = np.random.Generator(np.random.PCG64(seed))
+    cols = [rng.normal(0.0, 1.0, n), rng.binomial(1, 0.5, n).astype(np.float64), rng.uniform(0.0, 2.0, n)]
+    I = np.stack(cols[:k]).astype(np.float32)
+    I[0, rng.choice(n, 3, replace=False)] = np.nan
+    fvformat.write_fv(prefix, I, fvformat.obs_names(n), ["inter_env", "inter_sex", "inter_dose"][:k])
 
 EXCLUDE_LIST = "1 2\n5\n7\n9 11\n13\n40 44\n"
 
@@ -101,6 +120,10 @@ def build_inputs(case: str, where: str):
         with open(p, "w") as f:
             f.write(EXCLUDE_LIST)
         extra["excl"] = p
+    if post in ("inter", "inter3"):
+        p = os.path.join(where, case + "_INT")
+        interaction_file(over["n"], over["seed"] + 7, p, 1 if post == "inter" else 3)
+        extra["inter"] = p
     if post == "factors":
         p = os.path.join(where, case + "_factors.txt")
         with open(p, "w") as f:
@@ -150,12 +173,14 @@ def main(only=None):
                 args = [f.format(**extra) for f in flags]
                 out = os.path.join(tmp, f"{case}_{tag}")
                 model = [f for f in args if f in MODEL_FLAGS]
-                if model:
-                    ngpred = args[args.index("-n") + 1]
+                if model or "-v" in args:
+                    ngpred = args[args.index("-n") + 1] if "-n" in args else "1"
                     rest = [f for f in args if f in ("-b", "-f", "-i")]
-                    fac = args[args.index(model[0]) + 1] if model[0] in ("-z", "-y") else "-"
-                    cmd = [REF_MODEL, pre + "XL", pre + "XR", pre + "Y", out, ngpred, str(MODEL_FLAGS[model[0]]),
-                           fac] + rest
+                    fac = args[args.index(model[0]) + 1] if model and model[0] in ("-z", "-y") else "-"
+                    code = str(MODEL_FLAGS[model[0]]) if model else "-1"
+                    if "-v" in args:
+                        rest += ["-v", args[args.index("-v") + 1]]
+                    cmd = [REF_MODEL, pre + "XL", pre + "XR", pre + "Y", out, ngpred, code, fac] + rest
                 else:
                     cmd = [REF_BIN, "-c", pre + "XL", "-g", pre + "XR", "-p", pre + "Y", "-o", out] + args
                 p = subprocess.run(cmd, capture_output=True, text=True, timeout=600)

@@ -63,6 +63,8 @@ def settings_for(flags, extra) -> O.Settings:
             s.fname_excludelist = next(it).format(**extra)
         elif f in ("-j", "-k", "-l"):
             s.model = {"-j": 1, "-k": 2, "-l": 3}[f]
+        elif f == "-v":
+            s.fname_interactions = next(it).format(**extra)
         elif f in ("-z", "-y"):
             s.model = 4 if f == "-z" else 5
             with open(next(it).format(**extra)) as fh:
