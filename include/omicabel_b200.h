@@ -270,6 +270,11 @@ typedef struct oa_settings {
     const char* fname_interactions; /* -v: .fvi/.fvd with k interaction columns; each SNP column x
                                        becomes [I_1 x, ..., I_k x, x] (r = k + 1) and rows with a NaN
                                        interaction value are excluded (src/AIOwrapper.cpp:371-540) */
+    int32_t multi_interactions;  /* -w: with fname_interactions, one analysis per interaction column h:
+                                    each SNP column x becomes the r = 2 columns [I_h x, x] of its own
+                                    test, k tests per SNP, output in blocks of max(1, mb/k) SNPs x k
+                                    columns with the names I<h>_<SNP> and I<h>_o_<SNP>
+                                    (src/AIOwrapper.cpp:441-452, 618-660, 1208-1241) */
 } oa_settings;
 
 typedef struct oa_outputs {

@@ -248,6 +248,9 @@ struct Writer {
     int name_stride = 1;           // file columns per SNP
     bool name_first_only = false;  // a combined dosage model names a SNP by its first file column
     int n_inter = 0;               // interaction columns: SNP term a < n_inter is named "I<a+1>x<SNP>"
+    // one analysis per interaction column (-w): SNP indices count (SNP, column) pairs in blocks of
+    // multi_fmb file SNPs x multi_k columns; term 0 is "I<h>_<SNP>", term 1 "I<h>_o_<SNP>"
+    int multi_k = 0, multi_fmb = 1, multi_m = 0;
     const Fvi* fy = nullptr;
     const Fvi* fl = nullptr;
     const Fvi* fr = nullptr;
@@ -302,7 +305,9 @@ struct Writer {
                     if (h < l) aname = fl->var_name(h) + ":";
                     const size_t snp_g = (size_t)(name_base + snp);
                     const int term = h >= l ? h - l : 0;
-                    if (n_inter > 0) {   // src/AIOwrapper.cpp:566-612
+                    if (multi_k > 0) {   // src/AIOwrapper.cpp:618-660
+                        aname += multi_name(snp, term);
+                    } else if (n_inter > 0) {   // src/AIOwrapper.cpp:566-612
                         if (term < n_inter) aname += "I" + std::to_string(term + 1) + "x";
                         aname += fr->var_name(snp_g * name_stride);
                     } else {
@@ -327,11 +332,108 @@ struct Writer {
             if (buf.size() > (1u << 22)) flush();
         }
     }
+    // File SNP (shard-local) and interaction column of a (SNP, column) pair of -w: blocks of
+    // multi_fmb file SNPs, each listed once per column (src/AIOwrapper.cpp:441-452, 1208-1241).
+    void multi_pair(int v, int& file_snp, int& col) const {
+        const int mbv = multi_fmb * multi_k;
+        const int b = v / mbv, rem = v - b * mbv;
+        const int fb = std::min(multi_fmb, multi_m - b * multi_fmb);
+        col = rem / fb;
+        file_snp = b * multi_fmb + rem % fb;
+    }
+    std::string multi_name(int v, int term) const {
+        int i, col;
+        multi_pair(v, i, col);
+        return "I" + std::to_string(col + 1) + (term == 0 ? "_" : "_o_") +
+               fr->var_name((size_t)(name_base + i) * name_stride);
+    }
     void flush() {
         if (!buf.empty()) fwrite(buf.data(), 1, buf.size(), dis);
         buf.clear();
     }
 };
+
+// One engine call of -w: the call's cnt file SNPs (starting at shard SNP s0, a multiple of the
+// reference's file block) go to the device once, then one scan per interaction column h with the
+// columns [I_h x, x]; the stored rows of all columns are merged into the reference's order (block
+// of file SNPs -> trait -> column -> SNP, src/AIOwrapper.cpp:1208-1241) and written.
+oa_status multi_call(oa_engine* eng, const float* xr_pinned, float* xr_dev, int cnt, int s0, int file_r, int n,
+                     const std::vector<float>& inter, Writer& W, int trait_base, int64_t& tests, int64_t& singular,
+                     uint64_t& sig_cov) {
+    if (cudaMemcpy(xr_dev, xr_pinned, sizeof(float) * (size_t)cnt * file_r * n, cudaMemcpyHostToDevice) !=
+        cudaSuccess) {
+        herr("copy of a SNP block: %s", cudaGetErrorString(cudaGetLastError()));
+        return OA_ERR_CUDA;
+    }
+    const int k = W.multi_k, fmb = W.multi_fmb, p = W.p;
+    struct Row {
+        int32_t trait, pair;
+        float r2;
+        int32_t n_used;
+        uint32_t mask;
+        size_t coef;   // offset into the coefficient arrays
+    };
+    std::vector<Row> rows;
+    std::vector<float> cb, cs, ct;
+    for (int h = 0; h < k; ++h) {
+        oa_status st = oa_set_interactions(eng, inter.data() + (size_t)h * n, 1, 1);
+        if (st != OA_OK) return st;
+        oa_rows rr{};
+        st = oa_run_snps_device(eng, xr_dev, cnt, 1, &rr);
+        if (st != OA_OK) return st;
+        tests += rr.tests;
+        singular += rr.singular;
+        sig_cov += (uint64_t)rr.sig_cov_unrowed;
+        for (int64_t q = 0; q < rr.count; ++q) {
+            const int s = s0 + rr.snp[q];           // shard-local file SNP
+            const int b = s / fmb;
+            const int fb = std::min(fmb, W.multi_m - b * fmb);
+            const int pair = b * fmb * k + h * fb + (s - b * fmb);
+            rows.push_back(Row{rr.trait[q], pair, rr.r2[q], rr.n_used[q], rr.coef_mask[q], cb.size()});
+            cb.insert(cb.end(), rr.coef_b + (size_t)q * p, rr.coef_b + (size_t)(q + 1) * p);
+            cs.insert(cs.end(), rr.coef_se + (size_t)q * p, rr.coef_se + (size_t)(q + 1) * p);
+            ct.insert(ct.end(), rr.coef_t + (size_t)q * p, rr.coef_t + (size_t)(q + 1) * p);
+        }
+    }
+    const int mbv = fmb * k;
+    std::sort(rows.begin(), rows.end(), [mbv](const Row& a, const Row& b) {
+        const int ba = a.pair / mbv, bb = b.pair / mbv;
+        if (ba != bb) return ba < bb;
+        if (a.trait != b.trait) return a.trait < b.trait;
+        return a.pair < b.pair;
+    });
+    const size_t cnt_rows = rows.size();
+    std::vector<int32_t> tr(cnt_rows), pr(cnt_rows), nu(cnt_rows);
+    std::vector<float> r2(cnt_rows), B(cnt_rows * p), SE(cnt_rows * p), T(cnt_rows * p);
+    std::vector<uint32_t> mk(cnt_rows);
+    for (size_t q = 0; q < cnt_rows; ++q) {
+        const Row& x = rows[q];
+        tr[q] = x.trait;
+        pr[q] = x.pair;
+        nu[q] = x.n_used;
+        r2[q] = x.r2;
+        mk[q] = x.mask;
+        std::copy(cb.begin() + x.coef, cb.begin() + x.coef + p, B.begin() + q * p);
+        std::copy(cs.begin() + x.coef, cs.begin() + x.coef + p, SE.begin() + q * p);
+        std::copy(ct.begin() + x.coef, ct.begin() + x.coef + p, T.begin() + q * p);
+    }
+    oa_rows g{};
+    g.count = (int64_t)cnt_rows;
+    g.trait = tr.data();
+    g.snp = pr.data();
+    g.r2 = r2.data();
+    g.n_used = nu.data();
+    g.coef_mask = mk.data();
+    g.coef_b = B.data();
+    g.coef_se = SE.data();
+    g.coef_t = T.data();
+    // the call covers whole reference blocks: s0 / fmb .. (s0 + cnt - 1) / fmb
+    const int b_first = s0 / fmb, b_last = (s0 + cnt - 1) / fmb;
+    std::vector<std::vector<int64_t>> blocks(b_last - b_first + 1);
+    for (size_t q = 0; q < cnt_rows; ++q) blocks[pr[q] / mbv - b_first].push_back((int64_t)q);
+    for (int b = b_first; b <= b_last; ++b) W.write_block(g, blocks[b - b_first], trait_base, b * mbv);
+    return OA_OK;
+}
 
 }  // namespace
 
@@ -464,12 +566,15 @@ oa_status oa_solve(const oa_settings* S, oa_outputs* out) {
             return OA_ERR_IO;
         }
         n_inter = (int)FI.nvar;
-        if (n_inter < 1 || n_inter + 1 > OA_MAX_R) {
+        if (n_inter < 1 || (n_inter + 1 > OA_MAX_R && !S->multi_interactions)) {
             herr("%d interaction columns: this build supports 1..%d", n_inter, OA_MAX_R - 1);
             return OA_ERR_UNSUPPORTED;
         }
         r = n_inter + 1;
     }
+    // one analysis per interaction column (-w): k columns, r = 2 ([I_h x, x]) for each
+    const bool multi = use_inter && S->multi_interactions;
+    if (multi) r = 2;
     const int m_file = (int)(FR.nvar / file_r), t = (int)FY.nvar, l = (int)FL.nvar, p = l + r;
     // SNP shard of this process (the reference's MPI split, src/AIOwrapper.cpp:95-117)
     const int shards = std::max(1, S->shards);
@@ -586,7 +691,15 @@ oa_status oa_solve(const oa_settings* S, oa_outputs* out) {
     W.name_base = first;
     W.name_stride = file_r;
     W.name_first_only = combine;
-    W.n_inter = n_inter;
+    W.n_inter = multi ? 0 : n_inter;
+    // -w: reference blocks of fmb file SNPs x k columns (src/AIOwrapper.cpp:441-452)
+    const int multi_fmb = multi ? std::max(1, std::min(m, 500) / n_inter) : 1;
+    if (multi) {
+        W.multi_k = n_inter;
+        W.multi_fmb = multi_fmb;
+        W.multi_m = m;
+    }
+    const int m_out = multi ? m * n_inter : m;   // SNPs of the outputs: (SNP, column) pairs with -w
     W.dis = fopen((fout_eff + "_dis.txt").c_str(), "wb");
     if (!W.dis) {
         herr("Error Creating File %s_dis.txt", fout_eff.c_str());
@@ -601,12 +714,25 @@ oa_status oa_solve(const oa_settings* S, oa_outputs* out) {
             fclose(W.dis);
             return OA_ERR_IO;
         }
-        const int32_t hdr[6] = {n, l, r, t, m, (int32_t)FR.namelength};
+        const int32_t hdr[6] = {n, l, r, t, m_out, (int32_t)FR.namelength};
         fwrite(hdr, 4, 6, fi);
         const uint8_t flags[2] = {(uint8_t)(S->disp_cov ? 1 : 0), (uint8_t)(S->store_all ? 1 : 0)};
         fwrite(flags, 1, 2, fi);
         fwrite(FL.raw((size_t)FL.nobs + 1), 1, (size_t)FL.namelength * (l - 1), fi);
-        if (combine) {   // one name per SNP: its first file column (src/AIOwrapper.cpp:711-721)
+        if (multi) {
+            // r names per (SNP, column) pair in output order, as the text output names them.  The
+            // reference writes fileR * m file names here with m already multiplied by the column
+            // count (src/AIOwrapper.cpp:444, 722-728), i.e. past the end of its name table; the
+            // list written here matches the header's r * m instead.
+            std::vector<char> nm((size_t)FR.namelength);
+            for (int v = 0; v < m_out; ++v)
+                for (int term = 0; term < 2; ++term) {
+                    const std::string a = W.multi_name(v, term);
+                    std::fill(nm.begin(), nm.end(), 0);
+                    memcpy(nm.data(), a.data(), std::min(a.size(), nm.size() - 1));
+                    fwrite(nm.data(), 1, nm.size(), fi);
+                }
+        } else if (combine) {   // one name per SNP: its first file column (src/AIOwrapper.cpp:711-721)
             for (int i = 0; i < m; ++i)
                 fwrite(FR.raw((size_t)FR.nobs + (size_t)(first + i) * file_r), 1, (size_t)FR.namelength, fi);
         } else {
@@ -625,11 +751,13 @@ oa_status oa_solve(const oa_settings* S, oa_outputs* out) {
 
     // engine: one trait block of the reference's size at a time (tb = min(t, 1000))
     const int tb = std::min(t, 1000);
-    const int mb_ref = std::min(m, 500);
+    const int mb_ref = multi ? multi_fmb * n_inter : std::min(m, 500);
     W.mb_ref = mb_ref;
-    // SNPs per engine call: a multiple of the reference block, about 1 GB of genotypes
+    // SNPs per engine call: a multiple of the reference block (of its file SNPs with -w), about
+    // 1 GB of genotypes
+    const int mb_file = multi ? multi_fmb : mb_ref;
     int call_snps = (int)std::max<int64_t>(1, (int64_t)(1u << 28) / ((int64_t)n * file_r));
-    call_snps = std::max(mb_ref, call_snps / mb_ref * mb_ref);
+    call_snps = std::max(mb_file, call_snps / mb_file * mb_file);
     call_snps = std::min(call_snps, m);
     oa_config cfg{};
     cfg.n = n;
@@ -664,21 +792,36 @@ oa_status oa_solve(const oa_settings* S, oa_outputs* out) {
     };
     st = oa_set_covariates(eng, XL.data());
     if (st != OA_OK) return fail(st);
+    std::vector<float> inter_kept;
+    if (use_inter) {   // the kept rows of each interaction column
+        inter_kept.resize((size_t)n_inter * n);
+        for (int h = 0; h < n_inter; ++h) {
+            size_t pos = 0;
+            for (const auto& run : runs) {
+                memcpy(&inter_kept[(size_t)h * n + pos], &inter_all[(size_t)h * fileN + run.first],
+                       sizeof(float) * run.second);
+                pos += run.second;
+            }
+        }
+        // the interactions first: a combined dosage model then keeps them (r = columns + 1)
+        st = multi ? oa_set_interactions(eng, inter_kept.data(), 1, 1)
+                   : oa_set_interactions(eng, inter_kept.data(), n_inter, 1);
+        if (st != OA_OK) return fail(st);
+    }
     if (model) {
         st = oa_set_column_model(eng, file_r, model_w, combine ? 1 : 0);
         if (st != OA_OK) return fail(st);
     }
-    if (use_inter) {   // the kept rows of each interaction column
-        std::vector<float> I((size_t)n_inter * n);
-        for (int h = 0; h < n_inter; ++h) {
-            size_t pos = 0;
-            for (const auto& run : runs) {
-                memcpy(&I[(size_t)h * n + pos], &inter_all[(size_t)h * fileN + run.first], sizeof(float) * run.second);
-                pos += run.second;
-            }
-        }
-        st = oa_set_interactions(eng, I.data(), n_inter, 1);
-        if (st != OA_OK) return fail(st);
+    // -w: each call's SNP block is copied to the device once and scanned once per interaction column
+    float* xr_dev = nullptr;
+    if (multi && (cudaSetDevice(S->device) != cudaSuccess ||
+                  cudaMalloc(&xr_dev, sizeof(float) * (size_t)call_snps * file_r * n) != cudaSuccess)) {
+        cudaGetLastError();
+        herr("device buffer for the SNP blocks of -w: out of memory");
+        oa_engine_destroy(eng);
+        fclose(W.dis);
+        if (W.dbin) fclose(W.dbin);
+        return OA_ERR_NOMEM;
     }
 
     FILE* fr = fopen((fxr + ".fvd").c_str(), "rb");
@@ -731,6 +874,18 @@ oa_status oa_solve(const oa_settings* S, oa_outputs* out) {
             const int b = c & 1;
             const int s0 = c * call_snps, cnt = std::min(call_snps, m - s0);
             if (c + 1 < ncalls) next = std::async(std::launch::async, read_call, c + 1, b ^ 1);
+            if (multi) {
+                st = multi_call(eng, pin[b], xr_dev, cnt, s0, file_r, n, inter_kept, W, y0, tests, singular, sig_cov);
+                if (st != OA_OK) {
+                    if (c + 1 < ncalls) next.wait();
+                    break;
+                }
+                if (verbose) {
+                    putchar('*');
+                    fflush(stdout);
+                }
+                continue;
+            }
             oa_rows rows{};
             st = oa_run_snps(eng, pin[b], cnt, &rows);
             if (st != OA_OK) {
@@ -757,6 +912,7 @@ oa_status oa_solve(const oa_settings* S, oa_outputs* out) {
     }
     fclose(fr);
     fclose(fyd);
+    if (xr_dev) cudaFree(xr_dev);
     for (int b = 0; b < 2; ++b) {
         if (cudaFreeHost(pin[b]) != cudaSuccess) {
             cudaGetLastError();
@@ -880,14 +1036,17 @@ int oa_cli_main(int argc, char** argv) {
                 break;
             case 'v':
                 finter = optarg;
+                S.multi_interactions = 0;
                 printf("-v File containing single interactions %s\n", optarg);
                 break;
             case 'u':
                 printf("-u Keeping independent variable for interaction analysis \n");
                 break;
             case 'w':
-                fprintf(stdout, "option -w (one analysis per interaction) is not supported by this build\n");
-                return 1;
+                finter = optarg;
+                S.multi_interactions = 1;
+                printf("-w File containing multiple interactions %s\n", optarg);
+                break;
             case 'h': fputs(kHelp, stdout); return 1;
             case 1000:
                 if (!strcmp(optarg, "plain")) S.precision = OA_PLAIN_FP32;

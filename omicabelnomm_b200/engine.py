@@ -55,7 +55,8 @@ class Settings(C.Structure):
                 ("min_r2_store", C.c_float), ("store_bin", C.c_int32), ("disp_cov", C.c_int32),
                 ("store_all", C.c_int32), ("precision", C.c_int32), ("device", C.c_int32),
                 ("quirk_r2", C.c_int32), ("verbose", C.c_int32), ("shard", C.c_int32), ("shards", C.c_int32),
-                ("dosage_model", C.c_int32), ("fname_factors", C.c_char_p), ("fname_interactions", C.c_char_p)]
+                ("dosage_model", C.c_int32), ("fname_factors", C.c_char_p), ("fname_interactions", C.c_char_p),
+                ("multi_interactions", C.c_int32)]
 
 
 class Tuning(C.Structure):
@@ -348,7 +349,7 @@ def pvalue(t: float) -> float:
 def solve(xl: str, xr: str, y: str, out: str, *, r: int = 1, exclude: str = "", store_bin=False,
           disp_cov=False, store_all=False, precision=PLAIN, device=0, min_p_disp=None, min_p_store=None,
           min_r2_disp=None, min_r2_store=None, verbose=False, shard=0, shards=1, dosage_model=0,
-          factors: str = "", interactions: str = "") -> Outputs:
+          factors: str = "", interactions: str = "", multi_interactions=False) -> Outputs:
     """≙ Algorithm::solve on files: writes out_dis.txt (+ _sto.ibin/.dbin)."""
     L = lib()
     s = Settings()
@@ -357,6 +358,7 @@ def solve(xl: str, xr: str, y: str, out: str, *, r: int = 1, exclude: str = "", 
     s.dosage_model = int(dosage_model)
     s.fname_factors = keep[5] if factors else None
     s.fname_interactions = keep[6] if interactions else None
+    s.multi_interactions = int(bool(multi_interactions))
     s.fname_xl, s.fname_xr, s.fname_y, s.fname_out = keep[:4]
     s.fname_exclude = keep[4] if exclude else None
     s.r = r

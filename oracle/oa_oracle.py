@@ -30,7 +30,9 @@ Reference semantics reproduced on purpose:
 * thresholds, loop order h = p-1 .. start_h and the result/row filters
   (src/Algorithm.cpp:338-342, 359, 1119-1203; src/AIOwrapper.cpp:1494);
 * output order Y block -> SNP block -> trait -> SNP -> h descending, with
-  tb = min(t, 1000), mb = min(m, 500) (src/AIOwrapper.cpp:212-216).
+  tb = min(t, 1000), mb = min(m, 500) (src/AIOwrapper.cpp:212-216); with one
+  analysis per interaction column (-w) the blocks are max(1, mb // k) * k
+  (SNP, column) pairs (src/AIOwrapper.cpp:441-452).
 
 ``quirk_r2=True`` additionally reproduces the reference's r >= 2 downdate
 bug (src/Algorithm.cpp:1300 and 1390-1396); the default computes the
@@ -73,6 +75,7 @@ class Settings:
                                  # columns per SNP (-n)
     factors: tuple = ()          # -z / -y factors, one per file column of a SNP
     fname_interactions: str = "" # -v: single-set interactions (the SNP column is kept)
+    multi_interactions: bool = False  # -w: one analysis per interaction column (with fname_interactions)
 
 
 # Factors of the fixed dosage models on genotype probabilities (AA, AB, BB)
@@ -123,6 +126,30 @@ def interaction_columns(XR: np.ndarray, names: List[str], r: int, inter: np.ndar
         out[i * (k + 1) + k] = XR[i]
         out_names.append(names[i])
     return out, out_names, k + 1
+
+
+def multi_interaction_columns(XR: np.ndarray, names: List[str], r: int, inter: np.ndarray):
+    """One analysis per interaction column (-w; src/AIOwrapper.cpp:441-452, 1208-1241,
+    names :618-660).  The reference reads file blocks of fmb = max(1, mb // k) SNPs
+    (mb = min(m, 500)) and hands the solver, per block, k groups of that block's SNPs:
+    group h holds, per SNP x, the r = 2 columns [I_h x, x], named "I<h>_<name>" and
+    "I<h>_o_<name>".  Returns the columns in that order, their names, r = 2 and the
+    solver's SNP block size fmb * k (its output blocks)."""
+    if r != 1:
+        raise ValueError("interactions need one column per SNP")
+    k, m = inter.shape[0], XR.shape[0]
+    fmb = max(1, min(m, 500) // k)
+    out = np.empty((m * k * 2, XR.shape[1]), dtype=np.float32)
+    out_names = []
+    v = 0
+    for b0 in range(0, m, fmb):
+        for h in range(k):
+            for i in range(b0, min(m, b0 + fmb)):
+                out[2 * v] = inter[h] * XR[i]
+                out[2 * v + 1] = XR[i]
+                out_names += [f"I{h + 1}_{names[i]}", f"I{h + 1}_o_{names[i]}"]
+                v += 1
+    return out, out_names, 2, fmb * k
 
 
 def erf_inv(z: float) -> float:
@@ -248,6 +275,7 @@ class Inputs:
     realN: int
     kept: np.ndarray
     r: int = 0          # columns per SNP of XR after a dosage model (0: Settings.r)
+    mb: int = 0         # SNPs per output block (0: min(m, 500))
 
 
 def load(xl_prefix: str, xr_prefix: str, y_prefix: str, s: Settings) -> Inputs:
@@ -278,11 +306,14 @@ def load(xl_prefix: str, xr_prefix: str, y_prefix: str, s: Settings) -> Inputs:
     xr_names, r_eff = fr["var"], 0
     if s.model:
         XR, xr_names, r_eff = column_model(XR, xr_names, s)
-    if inter is not None:
+    mb = 0
+    if inter is not None and s.multi_interactions:
+        XR, xr_names, r_eff, mb = multi_interaction_columns(XR, xr_names, r_eff or s.r, inter)
+    elif inter is not None:
         XR, xr_names, r_eff = interaction_columns(XR, xr_names, r_eff or s.r, inter)
     return Inputs(XL=XL[:, kept], XR=XR[:, kept], Y=Y[:, kept],
                   xl_names=fl["var"], xr_names=xr_names, y_names=fy["var"],
-                  realN=n, kept=kept, r=r_eff)
+                  realN=n, kept=kept, r=r_eff, mb=mb)
 
 
 # ----------------------------------------------------------------------------
@@ -493,7 +524,7 @@ def solve(inp: Inputs, s: Settings, snp_chunk: int = 2048, keep_dense: bool = Fa
     trait, snp, h, B, SEa, Ta, R2a = (a[keep] for a in (trait, snp, h, B, SEa, Ta, R2a))
 
     # reference order: Y block, SNP block, trait, SNP, h descending
-    tb, mb = min(t, 1000), min(m, 500)
+    tb, mb = min(t, 1000), (inp.mb or min(m, 500))
     order = np.lexsort((-h, snp, trait, snp // mb, trait // tb))
     trait, snp, h, B, SEa, Ta, R2a = (a[order] for a in (trait, snp, h, B, SEa, Ta, R2a))
     P = np.array([pvalue(float(np.float32(x))) for x in Ta])

@@ -6,13 +6,14 @@
 // src/main.cpp:341-358), while its reader implements the models
 // (src/AIOwrapper.cpp:257-340, 1213-1275).
 //
-//   ref_model_driver XL XR Y OUT NGPRED MODEL [FACTORS|-] [-b] [-f] [-i] [-v INTER]
+//   ref_model_driver XL XR Y OUT NGPRED MODEL [FACTORS|-] [-b] [-f] [-i] [-v INTER | -w INTER]
 //
 // MODEL is the reference's Settings::model: 0 additive, 1 dominant,
 // 2 recessive, 3 custom linear, 4 custom additive, -1 none.  -v sets the
 // single-set interactions with the file INTER (keeping the SNP column, as
-// the reference's -v does, src/main.cpp:369-378), whose command-line form
-// stores atof(optarg) as the file name (src/main.cpp:370).
+// the reference's -v does, src/main.cpp:369-378), -w one analysis per
+// interaction column (src/main.cpp:380-389); the command-line forms of both
+// store atof(optarg) as the file name (src/main.cpp:370, 381).
 #include <cstdlib>
 #include <cstring>
 #include <iostream>
@@ -46,6 +47,11 @@ int main(int argc, char** argv) {
             params.use_interactions = true;
             params.keep_depVar = true;
             params.use_multiple_interaction_sets = false;
+        } else if (!std::strcmp(argv[a], "-w") && a + 1 < argc) {
+            params.fname_interactions = argv[++a];
+            params.use_interactions = true;
+            params.keep_depVar = true;
+            params.use_multiple_interaction_sets = true;
         }
     }
     blas_set_num_threads(params.threads);

@@ -82,6 +82,13 @@ CASES = {
     # three interaction columns (r = 4)
     "r1_inter3": (dict(n=400, m=30, t=5, l=3, miss_mode="none", seed=35), "inter3",
                   [["-v", "{inter}"], ["-v", "{inter}", "-f"]]),
+    # one analysis per interaction column (-w, three columns): r = 2 ([I_h x, x]) per (SNP, column);
+    # 230 SNPs make reference blocks of 76 file SNPs x 3 columns and a ragged last block of 2.
+    # With -b only the .dbin is kept: the reference's .ibin name list reads past its name table
+    # here (it writes fileR * m names with m already multiplied by the column count)
+    "r1_multinter": (dict(n=300, m=230, t=5, l=3, miss_mode="none", seed=36), "inter3",
+                     [["-w", "{inter}"], ["-w", "{inter}", "-f"], ["-w", "{inter}", "-f", "-i"],
+                      ["-w", "{inter}", "-b"]]),
 }
 
 FACTORS = "0.5 1.5\n"
@@ -173,13 +180,14 @@ def main(only=None):
                 args = [f.format(**extra) for f in flags]
                 out = os.path.join(tmp, f"{case}_{tag}")
                 model = [f for f in args if f in MODEL_FLAGS]
-                if model or "-v" in args:
+                inter_flag = [f for f in args if f in ("-v", "-w")]
+                if model or inter_flag:
                     ngpred = args[args.index("-n") + 1] if "-n" in args else "1"
                     rest = [f for f in args if f in ("-b", "-f", "-i")]
                     fac = args[args.index(model[0]) + 1] if model and model[0] in ("-z", "-y") else "-"
                     code = str(MODEL_FLAGS[model[0]]) if model else "-1"
-                    if "-v" in args:
-                        rest += ["-v", args[args.index("-v") + 1]]
+                    if inter_flag:
+                        rest += [inter_flag[0], args[args.index(inter_flag[0]) + 1]]
                     cmd = [REF_MODEL, pre + "XL", pre + "XR", pre + "Y", out, ngpred, code, fac] + rest
                 else:
                     cmd = [REF_BIN, "-c", pre + "XL", "-g", pre + "XR", "-p", pre + "Y", "-o", out] + args
@@ -193,7 +201,7 @@ def main(only=None):
                     shutil.copyfileobj(f, g)
                 files = ["dis.txt.gz"]
                 if "-b" in flags:
-                    for ext in ("ibin", "dbin"):
+                    for ext in (("dbin",) if "-w" in flags else ("ibin", "dbin")):
                         shutil.copy(out + f"_sto.{ext}", os.path.join(cdir, f"{tag}_sto.{ext}"))
                         files.append(f"sto.{ext}")
                 entry["runs"][tag] = {"flags": flags, "significant": sig, "files": files}

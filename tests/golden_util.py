@@ -63,8 +63,9 @@ def settings_for(flags, extra) -> O.Settings:
             s.fname_excludelist = next(it).format(**extra)
         elif f in ("-j", "-k", "-l"):
             s.model = {"-j": 1, "-k": 2, "-l": 3}[f]
-        elif f == "-v":
+        elif f in ("-v", "-w"):
             s.fname_interactions = next(it).format(**extra)
+            s.multi_interactions = f == "-w"
         elif f in ("-z", "-y"):
             s.model = 4 if f == "-z" else 5
             with open(next(it).format(**extra)) as fh:
@@ -205,6 +206,18 @@ def parse_ibin(raw: bytes):
     n, l, r, t, m, nl = struct.unpack_from("<6i", raw, 0)
     disp_cov, store_all = raw[24], raw[25]
     return dict(n=n, l=l, r=r, t=t, m=m, namelength=nl, disp_cov=bool(disp_cov), store_all=bool(store_all))
+
+
+def ibin_ar_names(raw: bytes):
+    """The SNP-term names of a _sto.ibin file (r * m of them, src/AIOwrapper.cpp:693-732)."""
+    info = parse_ibin(raw)
+    nl = info["namelength"]
+    pos = 26 + (info["l"] - 1) * nl
+    out = []
+    for _ in range(info["r"] * info["m"]):
+        out.append(raw[pos:pos + nl].split(b"\0")[0].decode())
+        pos += nl
+    return out
 
 
 def parse_dbin(path: str, info: dict):

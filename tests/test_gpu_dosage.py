@@ -145,3 +145,32 @@ def test_interaction_argument_checks():
         eng.set_interactions(np.ones((2, 100), np.float32), keep=True)   # 2 + 1 != r = 2
     eng.set_interactions(np.ones((1, 100), np.float32), keep=True)
     eng.set_column_model(0)                                              # clears them
+
+
+@pytest.mark.parametrize("prec", [E.PLAIN, E.MIXED])
+def test_multi_interactions_match_oracle(prec, tmp_path):
+    """One analysis per interaction column (-w) through oa_solve: each SNP block goes to the
+    device once and is scanned once per column with [I_h x, x]; the rows of all columns are
+    merged into the reference's order (blocks of 166 SNPs x 3 columns, a ragged last block).
+    With phenotype missingness (the correct downdate) against the oracle's restatement."""
+    import golden_util as GU
+    from golden import make_golden as MG
+    w = synth.scaled(0, n=500, m=700, t=7, l=4, miss_mode="patterns", n_patterns=3, seed=61)
+    ds = synth.generate(w)
+    pre = str(tmp_path / "c_")
+    synth.write_dataset(ds, pre)
+    MG.interaction_file(w.n, 62, pre + "INT", 3)
+    s = O.Settings(storePInd=True, fname_interactions=pre + "INT", multi_interactions=True)
+    res, inp = O.run_files(pre + "XL", pre + "XR", pre + "Y", s, keep_dense=True)
+    out = str(tmp_path / "o")
+    o = E.solve(pre + "XL", pre + "XR", pre + "Y", out, store_all=True, precision=prec,
+                interactions=pre + "INT", multi_interactions=True)
+    assert o.tests == 700 * 3 * w.t
+    want = GU.oracle_rows(res, inp, s)
+    ours = O.parse_dis(out + "_dis.txt")
+    assert [(r["Phe"], r["SNP"]) for r in ours] == [(r["Phe"], r["SNP"]) for r in want]
+    assert [r["n"] for r in ours] == [r["n"] for r in want]
+    t_ref = np.array([r["T"] for r in want])
+    dt = np.abs(np.array([r["T"] for r in ours]) - t_ref)
+    lim = (T_REL * np.abs(t_ref) + T_ABS + 1e-6) if prec == E.PLAIN else (1e-3 + 2e-4 * np.abs(t_ref))
+    assert np.all(dt <= lim), f"max |dt| {dt.max():.3g}"

@@ -144,7 +144,20 @@ def test_cli_matches_reference_outputs(case, tag, tmp_path):
     ours = O.parse_dis(out + "_dis.txt")
     info = GU.compare_rows(ref, ours, GU.REF_TOL, near)
     assert abs(sig - run["significant"]) <= max(2, 0.01 * run["significant"])
-    if "-b" in run["flags"]:
+    if "-b" in run["flags"] and "-w" in run["flags"]:
+        # the reference's .ibin name list for -w reads past its name table (not kept as a
+        # fixture): the header must give the run's shape and the names those of the text output
+        with open(out + "_sto.ibin", "rb") as f:
+            got = f.read()
+        hdr = GU.parse_ibin(got)
+        pairs = inp.XR.shape[0] // 2
+        assert (hdr["n"], hdr["l"], hdr["r"], hdr["t"], hdr["m"]) == (
+            inp.XL.shape[1], inp.XL.shape[0], 2, inp.Y.shape[0], pairs)
+        assert GU.ibin_ar_names(got) == inp.xr_names
+        GU.compare_dbin(os.path.join(GU.GOLDEN, case, f"{tag}_sto.dbin"), out + "_sto.dbin", got,
+                        exact_rows=(info["only_ref"] == 0 and info["only_our"] == 0
+                                    and sig == run["significant"]))
+    elif "-b" in run["flags"]:
         with open(os.path.join(GU.GOLDEN, case, f"{tag}_sto.ibin"), "rb") as f:
             want = f.read()
         with open(out + "_sto.ibin", "rb") as f:
