@@ -224,7 +224,7 @@ def time_scans(eng, xr_ptr, m, steps, warmup, local, barrier, max_over_ranks):
     torch.cuda.synchronize()
     launches0 = eng.launches()
     t0 = time.perf_counter()
-    gemm_ms = stats_ms = 0.0
+    gemm_ms = stats_ms = block_ms = 0.0
     rows = 0
     kname = ""
     for _ in range(steps):
@@ -232,14 +232,17 @@ def time_scans(eng, xr_ptr, m, steps, warmup, local, barrier, max_over_ranks):
         ms, kname = eng.last_kernel_ms()
         gemm_ms += ms
         stats_ms += eng.last_stats_ms()
+        block_ms += eng.last_block_ms()   # CUDA events on the engine's stream around the whole scan
         rows = r.count
     torch.cuda.synchronize()
     elapsed = time.perf_counter() - t0
     barrier()
     clk = clocks.stop()
-    elapsed = max_over_ranks(elapsed)
-    return dict(step_s=elapsed / steps, gemm_ms=gemm_ms / steps, stats_ms=stats_ms / steps, kernel=kname,
-                launches=(eng.launches() - launches0) // steps, rows=rows, clocks=clk)
+    step_s = max_over_ranks(block_ms / 1000.0 / steps)
+    host_step_s = max_over_ranks(elapsed / steps)
+    return dict(step_s=step_s, host_step_s=host_step_s, gemm_ms=gemm_ms / steps, stats_ms=stats_ms / steps,
+                kernel=kname, launches=(eng.launches() - launches0) // steps, rows=rows, clocks=clk,
+                tuning=eng.tuning())
 
 
 def max_dt(eng_a, eng_b, xr_ptr, mb):
@@ -533,8 +536,11 @@ def main():
                      else None},
         "cpu_baseline": cpu,
         "clocks": R["clocks"],
+        "timing": "device: CUDA events on the engine's stream before the first and after the last launch "
+                  "of each scan, summed over the timed scans, max over ranks",
         "forms": {k: ({"tests_per_s": tests * world / v["step_s"], "ms_per_step": v["step_s"] * 1e3,
-                       "gemm_ms": v["gemm_ms"], "stats_ms": v["stats_ms"], "stored_rows": v["rows"]}
+                       "host_ms_per_step": v["host_step_s"] * 1e3, "gemm_ms": v["gemm_ms"],
+                       "stats_ms": v["stats_ms"], "stored_rows": v["rows"], "tuning": v["tuning"]}
                       if "error" not in v else v)
                   for k, v in results.items()},
         "max_dt_mixed_vs_plain_first_16384_snps": dt_mp,

@@ -150,7 +150,9 @@ oa_status oa_set_snp_rows(oa_engine* e, const int32_t* rows, int32_t n_rows, int
  *                 dominant: {1,1,0}, recessive: {1,0,0} on genotype
  *                 probabilities AA, AB[, BB]; custom additive: the factors file)
  *   combine == 0: r = in_cols columns weights[c] * x_c (custom linear model).
- * in_cols = 0 restores plain blocks of r columns per SNP.  Not with row subsets. */
+ * With interactions (oa_set_interactions, before or after this call) a
+ * combined column becomes r = k (+1) columns.  in_cols = 0 restores plain
+ * blocks of r columns per SNP.  Not with row subsets. */
 #define OA_MODEL_MAX_COLS 8
 oa_status oa_set_column_model(oa_engine* e, int32_t in_cols, const float* weights, int32_t combine);
 
@@ -235,6 +237,10 @@ int64_t oa_kernel_launches(const oa_engine* e);
 float oa_last_kernel_ms(const oa_engine* e, const char** name);
 /* Device time (ms) of the per-SNP statistics kernel in the last SNP block. */
 float oa_last_stats_ms(const oa_engine* e);
+/* Device time (ms) of the whole last SNP block: CUDA events on the engine's
+ * stream before its first launch and after its last (the stored-row count
+ * read-back and, for host results, the sort and copy not included). */
+float oa_last_block_ms(const oa_engine* e);
 
 /* ---------------------------------------------------------------------------
  * Whole-run entry points

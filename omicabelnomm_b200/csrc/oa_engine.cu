@@ -232,6 +232,7 @@ struct oa_engine {
     long long launches = 0;
     float last_ms = 0.f;
     float stats_ms = 0.f;
+    float block_ms = 0.f;   // device time of the last SNP block on the engine's stream (events k0, k1)
     cudaEvent_t s0 = nullptr, s1 = nullptr;
     const char* last_name = "";
     // covariates
@@ -1131,6 +1132,7 @@ oa_status run_block(oa_engine* e, const float* xr, int mb, bool host_input) {
     const int nch = (mb + e->chunk - 1) / e->chunk;
     for (int attempt = 0; attempt < 3; ++attempt) {
         OA_CU(cudaMemsetAsync(e->counters.p, 0, 8 * sizeof(unsigned long long), e->st));
+        OA_CU(cudaEventRecord(e->k0, e->st));
         bool launched = false;
         if (!host_input && e->use_graphs) {
             oa_engine::GraphKey key;
@@ -1171,6 +1173,7 @@ oa_status run_block(oa_engine* e, const float* xr, int mb, bool host_input) {
             }
         }
         if (!launched) OA_CHECK(enqueue_block<R>(e, xr, mb, host_input, false));
+        OA_CU(cudaEventRecord(e->k1, e->st));
         const unsigned long long* cnt = e->h_cnt;
         OA_CU(cudaMemcpyAsync(e->h_cnt, e->counters.p, 4 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, e->st));
         OA_CU(cudaStreamSynchronize(e->st));
@@ -1192,6 +1195,9 @@ oa_status run_block(oa_engine* e, const float* xr, int mb, bool host_input) {
         cudaGetLastError();
         e->last_ms = total;
         e->stats_ms = stotal;
+        float bms = 0.f;
+        e->block_ms = cudaEventElapsedTime(&bms, e->k0, e->k1) == cudaSuccess ? bms : 0.f;
+        cudaGetLastError();
         e->last_name = e->cfg.precision == OA_PLAIN_FP32                ? "k_gemm_simt"
                        : (e->t > 128 && e->variant >= 3) ? "k_gemm_tc2"
                                                           : "k_gemm_tc";
@@ -1226,6 +1232,12 @@ oa_status run_snps_impl(oa_engine* e, const float* xr, int32_t mb, bool host_inp
     if (mb <= 0 || mb > e->cfg.max_snps) {
         set_err("SNP block of %d SNPs (engine limit %d)", mb, e->cfg.max_snps);
         return OA_ERR_ARG;
+    }
+    if (e->in_cols > 0 && e->model_combine && (e->n_inter > 0 ? e->n_inter + e->inter_keep : 1) != e->r) {
+        set_err("a combined column model gives r = %d columns per SNP%s, the engine has r = %d",
+                e->n_inter > 0 ? e->n_inter + e->inter_keep : 1, e->n_inter > 0 ? " with its interactions" : "",
+                e->r);
+        return OA_ERR_STATE;
     }
     OA_CHECK(prepare_tuning(e));
     OA_CHECK(ensure_chunk_buffers(e));
@@ -1427,7 +1439,7 @@ oa_status autotune_impl(oa_engine* e, const float* xr, int mb, oa_tuning* best_o
         for (int rep = 0; rep < 3; ++rep) {   // first run: allocations and kernel attributes
             const oa_status s = run_snps_any(e, xr, mb, false, false, &rows);
             if (s != OA_OK) return s;
-            if (rep > 0) sum += e->last_ms + e->stats_ms;
+            if (rep > 0) sum += e->block_ms;   // the whole block on the device
         }
         *ms = sum / 2.f;
         return OA_OK;
@@ -1796,8 +1808,10 @@ oa_status oa_set_column_model(oa_engine* e, int32_t in_cols, const float* weight
         set_err("column model of %d file columns per SNP (1..%d, with weights)", in_cols, OA_MODEL_MAX_COLS);
         return OA_ERR_ARG;
     }
+    // a combined column without interactions yet: r = 1, or interaction columns follow (checked when a
+    // block runs, so that the model and the interactions may be set in either order)
     const int want_r = combine ? (e->n_inter > 0 ? e->n_inter + e->inter_keep : 1) : in_cols;
-    if (want_r != e->r || (!combine && e->n_inter > 0)) {
+    if ((!combine && (want_r != e->r || e->n_inter > 0)) || (combine && e->n_inter > 0 && want_r != e->r)) {
         set_err("column model: %s needs r = %d, the engine has r = %d",
                 combine ? "a combined column" : "scaled columns (no interactions)", want_r, e->r);
         return OA_ERR_ARG;
@@ -1986,5 +2000,6 @@ float oa_last_kernel_ms(const oa_engine* e, const char** name) {
 }
 
 float oa_last_stats_ms(const oa_engine* e) { return e ? e->stats_ms : 0.f; }
+float oa_last_block_ms(const oa_engine* e) { return e ? e->block_ms : 0.f; }
 
 }  // extern "C"

@@ -98,6 +98,7 @@ def lib() -> C.CDLL:
         "oa_kernel_launches": ([P], C.c_int64),
         "oa_last_kernel_ms": ([P, C.POINTER(C.c_char_p)], C.c_float),
         "oa_last_stats_ms": ([P], C.c_float),
+        "oa_last_block_ms": ([P], C.c_float),
         "oa_default_settings": ([C.POINTER(Settings)], None),
         "oa_solve": ([C.POINTER(Settings), C.POINTER(Outputs)], C.c_int),
         "oa_cli_main": ([C.c_int, C.POINTER(C.c_char_p)], C.c_int),
@@ -307,6 +308,10 @@ class Engine:
 
     def last_stats_ms(self) -> float:
         return float(lib().oa_last_stats_ms(self.h))
+
+    def last_block_ms(self) -> float:
+        """Device time of the last SNP block (CUDA events on the engine's stream)."""
+        return float(lib().oa_last_block_ms(self.h))
 
     def last_kernel_ms(self):
         name = C.c_char_p()

@@ -145,6 +145,17 @@ def test_interaction_argument_checks():
         eng.set_interactions(np.ones((2, 100), np.float32), keep=True)   # 2 + 1 != r = 2
     eng.set_interactions(np.ones((1, 100), np.float32), keep=True)
     eng.set_column_model(0)                                              # clears them
+    # a combined model may come before its interactions; a block without them is refused
+    w = synth.scaled(0, n=100, m=50, t=4, prob_cols=3, seed=5)
+    ds = synth.generate(w)
+    eng2 = E.Engine(100, w.l, 2, 4, 50)
+    eng2.set_covariates(ds.XL)
+    eng2.set_column_model(3, (2.0, 1.0, 0.0), True)
+    eng2.set_traits(ds.Y)
+    with pytest.raises(E.OAError):
+        eng2.run(ds.XR)                                                  # r = 2 needs one interaction column
+    eng2.set_interactions(np.ones((1, 100), np.float32), keep=True)
+    assert eng2.run(ds.XR).tests == 4 * 50
 
 
 @pytest.mark.parametrize("prec", [E.PLAIN, E.MIXED])
