@@ -77,7 +77,7 @@ class ClockSampler:
         os.close(fd)
         self.out = open(self.path, "w")
         self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.QUERY}",
-                                      "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.out,
+                                      "--format=csv,noheader,nounits", "-lms", "100"], stdout=self.out,
                                      stderr=subprocess.DEVNULL)
 
     def stop(self):
@@ -311,7 +311,7 @@ def serve_section(args, dev, local):
     covariates (12 cohorts), t ~ LogUniform(1, 500) traits with 0-10 %
     missingness, a contiguous range of LogUniform(10k, 1M) SNPs; mixed form,
     stored rows P < 1e-3 returned to the host; admission by device-memory
-    footprint, up to 8 requests on the GPU at once; two engines per cohort are
+    footprint, up to 8 requests on the GPU at once; three engines per cohort are
     created at start-up (untimed)."""
     import torch
     from omicabelnomm_b200 import serve as S
@@ -325,8 +325,8 @@ def serve_section(args, dev, local):
     budget = int(free - (6 << 30))
     srv = S.Server(G.data_ptr(), w.n_total, w.m_total, cohorts, device=local, budget_bytes=budget, max_slots=8,
                    min_p_store=1e-3, t_cap_min=512)
-    # start-up, not timed: two engines per cohort (as a server does when it loads its cohorts)
-    srv.warm(dev, per_cohort=2)
+    # start-up, not timed: three engines per cohort (as a server does when it loads its cohorts)
+    srv.warm(dev, per_cohort=3)
     clocks = ClockSampler(local)
     clocks.start()
     res = srv.run(reqs, realtime=True)
@@ -348,7 +348,7 @@ def serve_section(args, dev, local):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--form", default="auto", choices=["auto", "mixed", "plain"])
