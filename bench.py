@@ -405,12 +405,17 @@ def main():
                            min_r2_store=1e-6)
             eng.set_covariates(xl_host)
             eng.set_traits_device(Y.data_ptr(), t)
+            # launch parameters from the engine's autotuner on a sample of three default chunks (untimed)
+            t0 = time.perf_counter()
+            eng.autotune(XR.data_ptr(), min(m, 3 * 18944))
+            tune_s = time.perf_counter() - t0
             eng.run_device(XR.data_ptr(), m)     # probe once before timing
         except E.OAError as ex:
             results[name] = {"error": str(ex)}
             continue
-        results[name] = dict(engine=eng, **time_scans(eng, XR.data_ptr(), m, args.steps, args.warmup, local,
-                                                      barrier, max_over_ranks))
+        results[name] = dict(engine=eng, autotune_s=tune_s,
+                             **time_scans(eng, XR.data_ptr(), m, args.steps, args.warmup, local, barrier,
+                                          max_over_ranks))
 
     valid = [k for k in order if "error" not in results[k]]
     if not valid:
@@ -540,7 +545,8 @@ def main():
                   "of each scan, summed over the timed scans, max over ranks",
         "forms": {k: ({"tests_per_s": tests * world / v["step_s"], "ms_per_step": v["step_s"] * 1e3,
                        "host_ms_per_step": v["host_step_s"] * 1e3, "gemm_ms": v["gemm_ms"],
-                       "stats_ms": v["stats_ms"], "stored_rows": v["rows"], "tuning": v["tuning"]}
+                       "stats_ms": v["stats_ms"], "stored_rows": v["rows"], "tuning": v["tuning"],
+                       "autotune_s": v["autotune_s"]}
                       if "error" not in v else v)
                   for k, v in results.items()},
         "max_dt_mixed_vs_plain_first_16384_snps": dt_mp,

@@ -159,14 +159,16 @@ def test_interaction_argument_checks():
 
 
 @pytest.mark.parametrize("prec", [E.PLAIN, E.MIXED])
-def test_multi_interactions_match_oracle(prec, tmp_path):
+@pytest.mark.parametrize("m", [700, 2])
+def test_multi_interactions_match_oracle(prec, m, tmp_path):
     """One analysis per interaction column (-w) through oa_solve: each SNP block goes to the
     device once and is scanned once per column with [I_h x, x]; the rows of all columns are
-    merged into the reference's order (blocks of 166 SNPs x 3 columns, a ragged last block).
-    With phenotype missingness (the correct downdate) against the oracle's restatement."""
+    merged into the reference's order (700 SNPs: blocks of 166 SNPs x 3 columns and a ragged
+    last block; 2 SNPs: fewer SNPs than columns, blocks of one SNP x 3 columns).  With
+    phenotype missingness (the correct downdate) against the oracle's restatement."""
     import golden_util as GU
     from golden import make_golden as MG
-    w = synth.scaled(0, n=500, m=700, t=7, l=4, miss_mode="patterns", n_patterns=3, seed=61)
+    w = synth.scaled(0, n=500, m=m, t=7, l=4, miss_mode="patterns", n_patterns=3, seed=61)
     ds = synth.generate(w)
     pre = str(tmp_path / "c_")
     synth.write_dataset(ds, pre)
@@ -176,7 +178,7 @@ def test_multi_interactions_match_oracle(prec, tmp_path):
     out = str(tmp_path / "o")
     o = E.solve(pre + "XL", pre + "XR", pre + "Y", out, store_all=True, precision=prec,
                 interactions=pre + "INT", multi_interactions=True)
-    assert o.tests == 700 * 3 * w.t
+    assert o.tests == m * 3 * w.t
     want = GU.oracle_rows(res, inp, s)
     ours = O.parse_dis(out + "_dis.txt")
     assert [(r["Phe"], r["SNP"]) for r in ours] == [(r["Phe"], r["SNP"]) for r in want]
