@@ -1309,19 +1309,30 @@ oa_status run_snps_impl(oa_engine* e, const float* xr, int32_t mb, bool host_inp
         OA_CU(cub::DeviceRadixSort::SortPairs(e->cub_tmp.p, tmp, e->keys.p, e->keys2.p, e->perm.p, e->perm2.p, (int)NS,
                                               0, bits, e->st));
         if (e->cfg.disp_cov) OA_CHECK(e->cov2.ensure((size_t)N * l * 3));
-        k_rec_gather<<<(unsigned)((N + 255) / 256), 256, 0, e->st>>>(e->rec.p, e->perm2.p, N, e->rec2.p,
-                                                                     e->cfg.disp_cov ? e->cov.p : nullptr,
-                                                                     e->cfg.disp_cov ? e->cov2.p : nullptr, l);
+        const RowsSoA dsoa = rows_soa(e->rec2.p, N, R);   // the record buffer holds the packed fields
+        k_rec_gather<R><<<(unsigned)((N + 255) / 256), 256, 0, e->st>>>(e->rec.p, e->perm2.p, N, dsoa,
+                                                                        e->cfg.disp_cov ? e->cov.p : nullptr,
+                                                                        e->cfg.disp_cov ? e->cov2.p : nullptr, l);
         ++e->launches;
         if (e->cfg.disp_cov)
             OA_CU(cudaMemcpyAsync(e->h_cov, e->cov2.p, sizeof(float) * N * l * 3, cudaMemcpyDeviceToHost, e->st));
         OA_CU(cudaGetLastError());
         // the rows come back in pieces, each converted on the host while the next is in flight
+        const RowsSoA hsoa = rows_soa(e->h_rec, N, R);
         for (int k = 0; k < RESULT_PIECES; ++k) {
-            const long long q0 = N * k / RESULT_PIECES, q1 = N * (k + 1) / RESULT_PIECES;
-            if (q1 > q0)
-                OA_CU(cudaMemcpyAsync(e->h_rec + q0, e->rec2.p + q0, sizeof(Rec) * (q1 - q0), cudaMemcpyDeviceToHost,
-                                      e->st));
+            const long long q0 = N * k / RESULT_PIECES, q1 = N * (k + 1) / RESULT_PIECES, nq = q1 - q0;
+            if (nq > 0) {
+                auto d2h = [&](void* dst, const void* src, size_t bytes) {
+                    return cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, e->st);
+                };
+                OA_CU(d2h(hsoa.trait + q0, dsoa.trait + q0, 4 * nq));
+                OA_CU(d2h(hsoa.snp + q0, dsoa.snp + q0, 4 * nq));
+                OA_CU(d2h(hsoa.r2 + q0, dsoa.r2 + q0, 4 * nq));
+                OA_CU(d2h(hsoa.mask + q0, dsoa.mask + q0, 4 * nq));
+                OA_CU(d2h(hsoa.b + q0 * R, dsoa.b + q0 * R, 4 * R * nq));
+                OA_CU(d2h(hsoa.se + q0 * R, dsoa.se + q0 * R, 4 * R * nq));
+                OA_CU(d2h(hsoa.t + q0 * R, dsoa.t + q0 * R, 4 * R * nq));
+            }
             OA_CU(cudaEventRecord(e->ev_piece[k], e->st));
         }
     }
@@ -1335,23 +1346,25 @@ oa_status run_snps_impl(oa_engine* e, const float* xr, int32_t mb, bool host_inp
     e->o_t.resize((size_t)N * p);
     const float minT = e->cfg.min_t_store;
     const bool disp_cov = e->cfg.disp_cov != 0, store_all = e->cfg.store_all != 0;
+    const RowsSoA hs = rows_soa(e->h_rec, N, R);
     auto convert = [&](long long q0, long long q1) {
         for (long long q = q0; q < q1; ++q) {
-            const Rec& rc = e->h_rec[q];
-            e->o_trait[q] = rc.trait;
-            e->o_snp[q] = rc.snp;
-            e->o_nused[q] = e->h_nobs[rc.trait];
-            e->o_r2[q] = rc.r2;
+            const int32_t tr = hs.trait[q];
+            e->o_trait[q] = tr;
+            e->o_snp[q] = hs.snp[q];
+            e->o_nused[q] = e->h_nobs[tr];
+            e->o_r2[q] = hs.r2[q];
             float* ob = &e->o_b[(size_t)q * p];
             float* os = &e->o_se[(size_t)q * p];
             float* ot = &e->o_t[(size_t)q * p];
             for (int h = 0; h < l; ++h) ob[h] = os[h] = ot[h] = 0.f;
             uint32_t m = 0;
+            const uint32_t rm = hs.mask[q];
             for (int a = 0; a < R; ++a) {
-                ob[l + a] = rc.b[a];
-                os[l + a] = rc.se[a];
-                ot[l + a] = rc.t[a];
-                if (rc.mask & (1u << a)) m |= 1u << (l + a);
+                ob[l + a] = hs.b[(size_t)q * R + a];
+                os[l + a] = hs.se[(size_t)q * R + a];
+                ot[l + a] = hs.t[(size_t)q * R + a];
+                if (rm & (1u << a)) m |= 1u << (l + a);
             }
             if (disp_cov) {
                 const float* cv = e->h_cov + (size_t)q * l * 3;

@@ -269,13 +269,50 @@ static __global__ void k_rec_keys(const Rec* __restrict__ rec, long long N, long
     perm[q] = (int)q;
 }
 
+// The stored rows that go back to the host, in sorted order and packed by
+// field: N x {trait, snp, r2, mask} then N x R each of b, se, t (16 + 12 R
+// bytes per row instead of the 80-byte record).
+struct RowsSoA {
+    int32_t* trait;
+    int32_t* snp;
+    float* r2;
+    uint32_t* mask;
+    float* b;
+    float* se;
+    float* t;
+};
+// Field arrays of N rows carved from `base` (at least rows_soa_bytes(N, R) bytes).
+__host__ __device__ inline size_t rows_soa_bytes(long long N, int R) { return (size_t)N * (16 + 12 * (size_t)R); }
+__host__ __device__ inline RowsSoA rows_soa(void* base, long long N, int R) {
+    uint8_t* p = static_cast<uint8_t*>(base);
+    RowsSoA s;
+    s.trait = reinterpret_cast<int32_t*>(p);
+    s.snp = reinterpret_cast<int32_t*>(p + 4 * (size_t)N);
+    s.r2 = reinterpret_cast<float*>(p + 8 * (size_t)N);
+    s.mask = reinterpret_cast<uint32_t*>(p + 12 * (size_t)N);
+    s.b = reinterpret_cast<float*>(p + 16 * (size_t)N);
+    s.se = s.b + (size_t)N * R;
+    s.t = s.se + (size_t)N * R;
+    return s;
+}
+
+template <int R>
 static __global__ void k_rec_gather(const Rec* __restrict__ rec, const int* __restrict__ perm, long long N,
-                             Rec* __restrict__ out, const float* __restrict__ cov, float* __restrict__ cov_out,
-                             int l) {
+                                    RowsSoA out, const float* __restrict__ cov, float* __restrict__ cov_out, int l) {
     const long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x;
     if (q >= N) return;
     const int src = perm[q];
-    out[q] = rec[src];
+    const Rec& rc = rec[src];
+    out.trait[q] = rc.trait;
+    out.snp[q] = rc.snp;
+    out.r2[q] = rc.r2;
+    out.mask[q] = rc.mask;
+#pragma unroll
+    for (int a = 0; a < R; ++a) {
+        out.b[(size_t)q * R + a] = rc.b[a];
+        out.se[(size_t)q * R + a] = rc.se[a];
+        out.t[(size_t)q * R + a] = rc.t[a];
+    }
     if (cov)
         for (int u = 0; u < l * 3; ++u) cov_out[(size_t)q * l * 3 + u] = cov[(size_t)src * l * 3 + u];
 }
