@@ -159,25 +159,28 @@ def test_interaction_argument_checks():
 
 
 @pytest.mark.parametrize("prec", [E.PLAIN, E.MIXED])
-@pytest.mark.parametrize("m", [700, 2])
-def test_multi_interactions_match_oracle(prec, m, tmp_path):
+@pytest.mark.parametrize("m,model", [(700, 0), (2, 0), (300, 1)])
+def test_multi_interactions_match_oracle(prec, m, model, tmp_path):
     """One analysis per interaction column (-w) through oa_solve: each SNP block goes to the
     device once and is scanned once per column with [I_h x, x]; the rows of all columns are
     merged into the reference's order (700 SNPs: blocks of 166 SNPs x 3 columns and a ragged
     last block; 2 SNPs: fewer SNPs than columns, blocks of one SNP x 3 columns).  With
-    phenotype missingness (the correct downdate) against the oracle's restatement."""
+    phenotype missingness (the correct downdate) against the oracle's restatement.  model = 1:
+    three genotype-probability columns per SNP through the additive dosage model first."""
     import golden_util as GU
     from golden import make_golden as MG
-    w = synth.scaled(0, n=500, m=m, t=7, l=4, miss_mode="patterns", n_patterns=3, seed=61)
+    cols = 3 if model else 0
+    w = synth.scaled(0, n=500, m=m, t=7, l=4, prob_cols=cols, miss_mode="patterns", n_patterns=3, seed=61)
     ds = synth.generate(w)
     pre = str(tmp_path / "c_")
     synth.write_dataset(ds, pre)
     MG.interaction_file(w.n, 62, pre + "INT", 3)
-    s = O.Settings(storePInd=True, fname_interactions=pre + "INT", multi_interactions=True)
+    s = O.Settings(r=cols or 1, model=model, storePInd=True, fname_interactions=pre + "INT",
+                   multi_interactions=True)
     res, inp = O.run_files(pre + "XL", pre + "XR", pre + "Y", s, keep_dense=True)
     out = str(tmp_path / "o")
-    o = E.solve(pre + "XL", pre + "XR", pre + "Y", out, store_all=True, precision=prec,
-                interactions=pre + "INT", multi_interactions=True)
+    o = E.solve(pre + "XL", pre + "XR", pre + "Y", out, r=cols or 1, dosage_model=model, store_all=True,
+                precision=prec, interactions=pre + "INT", multi_interactions=True)
     assert o.tests == m * 3 * w.t
     want = GU.oracle_rows(res, inp, s)
     ours = O.parse_dis(out + "_dis.txt")
