@@ -834,9 +834,9 @@ static cudaError_t go_any(int variant, int raster, const __nv_bfloat16* Xhi, con
                           const __nv_bfloat16* Yhi, const __nv_bfloat16* Ylo, int t, int n_pad, const EpiArgs& E,
                           int* err, cudaStream_t st) {
     if (t <= 64)
-        return go<R, Shape<32, 8, 64>, false>(Xhi, Xlo, xrows, Yhi, Ylo, t, n_pad, E, nullptr, 0, raster, err, st);
+        return go<R, Shape<64, 4, 64>, false>(Xhi, Xlo, xrows, Yhi, Ylo, t, n_pad, E, nullptr, 0, raster, err, st);
     if (t <= 128)
-        return go<R, Shape<32, 6, 128>, false>(Xhi, Xlo, xrows, Yhi, Ylo, t, n_pad, E, nullptr, 0, raster, err, st);
+        return go<R, Shape<64, 3, 128>, false>(Xhi, Xlo, xrows, Yhi, Ylo, t, n_pad, E, nullptr, 0, raster, err, st);
     if (variant == 2)
         return go<R, Shape<64, 2>, false>(Xhi, Xlo, xrows, Yhi, Ylo, t, n_pad, E, nullptr, 0, raster, err, st);
     if (variant == 3) return go2<R, Shape2<32, 6>>(Xhi, Xlo, xrows, Yhi, Ylo, t, n_pad, E, raster, err, st);
@@ -861,9 +861,9 @@ cudaError_t oa_launch_pre_tc(const __nv_bfloat16* Xhi, const __nv_bfloat16* Xlo,
                              const __nv_bfloat16* Bhi, const __nv_bfloat16* Blo, int c2, int n_pad, float* C, int ldc,
                              int* err, cudaStream_t st) {
     const EpiArgs none{};
-    if (c2 <= 64) return tc::go<1, tc::Shape<32, 8, 64>, true>(Xhi, Xlo, xrows, Bhi, Blo, c2, n_pad, none, C, ldc, 1, err, st);
+    if (c2 <= 64) return tc::go<1, tc::Shape<64, 4, 64>, true>(Xhi, Xlo, xrows, Bhi, Blo, c2, n_pad, none, C, ldc, 1, err, st);
     if (c2 <= 128)
-        return tc::go<1, tc::Shape<32, 6, 128>, true>(Xhi, Xlo, xrows, Bhi, Blo, c2, n_pad, none, C, ldc, 1, err, st);
+        return tc::go<1, tc::Shape<64, 3, 128>, true>(Xhi, Xlo, xrows, Bhi, Blo, c2, n_pad, none, C, ldc, 1, err, st);
     return tc::go<1, tc::Shape<32, 4, 256>, true>(Xhi, Xlo, xrows, Bhi, Blo, c2, n_pad, none, C, ldc, 1, err, st);
 }
 
