@@ -355,6 +355,9 @@ def main():
     ap.add_argument("--m", type=int, default=WORKLOAD["m"], help="SNPs per GPU (default: the full workload)")
     ap.add_argument("--e2e-steps", type=int, default=2)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-autotune", action="store_true",
+                    help="keep the engines' default tuning (profiling runs: timings under a profiler would steer "
+                         "the autotuner elsewhere)")
     ap.add_argument("--batched-m", type=int, default=200000, help="SNPs of the batched workload (0: skip it)")
     ap.add_argument("--serve-requests", type=int, default=120, help="requests of the serving run (0: skip it)")
     ap.add_argument("--serve-m", type=int, default=1_000_000, help="SNPs of the resident serving matrix")
@@ -407,7 +410,8 @@ def main():
             eng.set_traits_device(Y.data_ptr(), t)
             # launch parameters from the engine's autotuner on a sample of three default chunks (untimed)
             t0 = time.perf_counter()
-            eng.autotune(XR.data_ptr(), min(m, 3 * 18944))
+            if not args.no_autotune:
+                eng.autotune(XR.data_ptr(), min(m, 3 * 18944))
             tune_s = time.perf_counter() - t0
             eng.run_device(XR.data_ptr(), m)     # probe once before timing
         except E.OAError as ex:
