@@ -39,7 +39,13 @@ constexpr int BM = 128;
 constexpr int EPI_WARPS = EPI_WARPS_TC;                  // two per TMEM lane group, half of the columns each
 constexpr int NUM_THREADS = 64 + 32 * EPI_WARPS;         // 320
 constexpr int EPI_COLS = 8;                              // accumulator columns per tcgen05.ld of the epilogue
-constexpr int PF_BLOCKS = 16;                            // A-operand K-blocks prefetched into L2 ahead
+// A-operand K-blocks prefetched into L2 ahead of the stage loads: 512 K-elements whatever the K-block
+// width (16 blocks of 32, 8 of 64), so that the lines in flight (about 38 MB over 148 SMs) stay well
+// inside L2 and are not evicted before their stage load reads them
+template <int BK>
+constexpr int pf_blocks() {
+    return 512 / BK;
+}
 constexpr unsigned long long WAIT_NS = 2000000000ull;
 
 // Pipeline shape: K-block width BK (64 -> 128-byte swizzle, 32 -> 64-byte
@@ -279,7 +285,7 @@ k_gemm_tc(const __grid_constant__ CUtensorMap mAhi, const __grid_constant__ CUte
             bool pend[STAGES];
             for (int q = 0; q < STAGES; ++q) pend[q] = false;
             bool ok = true;
-            // L2 prefetch cursor, PF_BLOCKS K-blocks ahead of the stage loads (across tiles)
+            // L2 prefetch cursor, pf_blocks<BK>() K-blocks ahead of the stage loads (across tiles)
             int pt = blockIdx.x, pkb = 0;
             auto prefetch_next = [&]() {
                 if (pt >= ntiles) return;
@@ -291,7 +297,7 @@ k_gemm_tc(const __grid_constant__ CUtensorMap mAhi, const __grid_constant__ CUte
                     pt += gridDim.x;
                 }
             };
-            for (int q = 0; q < PF_BLOCKS; ++q) prefetch_next();
+            for (int q = 0; q < pf_blocks<BK>(); ++q) prefetch_next();
             for (int tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x) {
                 const int m0 = (raster == 2 ? tile % m_tiles : tile / n_tiles) * BM;
                 const int n0 = (raster == 2 ? tile / m_tiles : tile % n_tiles) * BN;
@@ -590,7 +596,7 @@ k_gemm_tc2(const __grid_constant__ CUtensorMap mAhi, const __grid_constant__ CUt
             int s = 0;
             uint32_t ph = 0;
             bool ok = true;
-            int pt = pair, pkb = 0;          // L2 prefetch cursor, PF_BLOCKS K-blocks ahead
+            int pt = pair, pkb = 0;          // L2 prefetch cursor, pf_blocks<BK>() K-blocks ahead
             auto prefetch_next = [&]() {
                 if (pt >= ntiles) return;
                 int pm0, pn0;
@@ -602,7 +608,7 @@ k_gemm_tc2(const __grid_constant__ CUtensorMap mAhi, const __grid_constant__ CUt
                     pt += npairs;
                 }
             };
-            for (int q = 0; q < PF_BLOCKS; ++q) prefetch_next();
+            for (int q = 0; q < pf_blocks<BK>(); ++q) prefetch_next();
             for (int tile = pair; tile < ntiles && ok; tile += npairs) {
                 int m0, n0;
                 tile_mn(tile, m0, n0);
