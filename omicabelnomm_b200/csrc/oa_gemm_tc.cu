@@ -870,7 +870,7 @@ cudaError_t oa_launch_pre_tc(const __nv_bfloat16* Xhi, const __nv_bfloat16* Xlo,
     if (c2 <= 64) return tc::go<1, tc::Shape<64, 4, 64>, true>(Xhi, Xlo, xrows, Bhi, Blo, c2, n_pad, none, C, ldc, 1, err, st);
     if (c2 <= 128)
         return tc::go<1, tc::Shape<64, 3, 128>, true>(Xhi, Xlo, xrows, Bhi, Blo, c2, n_pad, none, C, ldc, 1, err, st);
-    return tc::go<1, tc::Shape<32, 4, 256>, true>(Xhi, Xlo, xrows, Bhi, Blo, c2, n_pad, none, C, ldc, 1, err, st);
+    return tc::go<1, tc::Shape<64, 2, 256>, true>(Xhi, Xlo, xrows, Bhi, Blo, c2, n_pad, none, C, ldc, 1, err, st);
 }
 
 }  // namespace oa
