@@ -287,6 +287,7 @@ struct oa_engine {
     DBuf<__nv_bfloat16> Xhi, Xlo;
     DBuf<float> mean, varx, aobs, afull, zA, zD;
     DBuf<float> D, Dset, C2T;   // pre-GEMM path: X'X, per-set X'X, pre-GEMM output
+    DBuf<float> C2part;         // plain pre-GEMM: partial product of the second K half
     DBuf<int> has_nan;
     DBuf<double> sinv, sfinv;
     DBuf<uint8_t> sing;
@@ -368,6 +369,7 @@ void for_each_buf(oa_engine* e, F&& f) {
     f(e->B2); f(e->B2hi); f(e->B2lo);
     f(e->Xstage[0]); f(e->Xstage[1]); f(e->Xmodel); f(e->inter); f(e->Xhi); f(e->Xlo);
     f(e->mean); f(e->varx); f(e->aobs); f(e->afull); f(e->zA); f(e->zD); f(e->D); f(e->Dset); f(e->C2T);
+    f(e->C2part);
     f(e->has_nan); f(e->sinv); f(e->sfinv); f(e->sing);
     f(e->rec); f(e->rec2); f(e->cov); f(e->cov2); f(e->counters); f(e->keys); f(e->keys2); f(e->perm);
     f(e->perm2); f(e->cub_tmp);
@@ -861,7 +863,7 @@ oa_status stats_pre(oa_engine* e, const float* X, size_t ldx, const int* xrows, 
                                reinterpret_cast<int*>(e->counters.p + 3), e->st));
     else
         OA_CU(oa_launch_pre_simt(X, (size_t)e->n, mbc * R, e->B2.p, (size_t)e->n_pad, e->c2, e->n, e->mean.p,
-                                 e->has_nan.p, e->center ? 1 : 0, e->C2T.p, ldc, e->st));
+                                 e->has_nan.p, e->center ? 1 : 0, e->C2T.p, ldc, e->C2part.p, e->st));
     ++e->launches;
     SchurArgs S{};
     S.l = e->l;
@@ -1007,6 +1009,7 @@ oa_status ensure_chunk_buffers(oa_engine* e) {
         OA_CHECK(e->D.ensure(mb * r * r));
         OA_CHECK(e->Dset.ensure((size_t)std::max(e->nsets, 1) * mb * r * r));
         OA_CHECK(e->C2T.ensure((size_t)e->c2 * mb * r));
+        if (e->cfg.precision == OA_PLAIN_FP32) OA_CHECK(e->C2part.ensure((size_t)e->c2 * mb * r));
     }
     return OA_OK;
 }

@@ -45,12 +45,14 @@ __device__ __forceinline__ void sg_load(const float* __restrict__ P, size_t ld, 
 
 // STORE = false: fused statistics epilogue.  STORE = true: the product is
 // written out transposed, C[col * ldc + row] (the pre-GEMM of the per-SNP
-// covariate sums).
+// covariate sums); with kspan > 0 the CTAs of blockIdx.z = 1 take K from
+// kspan on and write their partial product to cpart (summed into cout by
+// k_add_partial, in that fixed order), those of z = 0 take K below kspan.
 template <int R, bool VEC, bool STORE>
 __global__ void __launch_bounds__(256, 2)
 k_gemm_simt(const float* __restrict__ X, size_t ldx, int xrows, const float* __restrict__ Yt, size_t ldy,
             int t, int K, const float* __restrict__ colmean, const int* __restrict__ has_nan, int center, EpiArgs E,
-            float* __restrict__ cout, int ldc) {
+            float* __restrict__ cout, int ldc, float* __restrict__ cpart, int kspan) {
     __shared__ __align__(16) float As[2][SG_BK][SG_BM + SG_PAD];
     __shared__ __align__(16) float Bs[2][SG_BK][SG_BN + SG_PAD];
     const int tid = threadIdx.x;
@@ -59,6 +61,9 @@ k_gemm_simt(const float* __restrict__ X, size_t ldx, int xrows, const float* __r
     const int n0 = blockIdx.x * SG_BN;  // first trait of the tile
     const int lrow = tid >> 2, lk = (tid & 3) * 4;
     const bool fix = center || *has_nan != 0;
+    const bool split = STORE && kspan > 0;
+    const int kb = split ? (int)blockIdx.z * kspan : 0;   // this CTA's K range [kb, ke)
+    const int ke = split ? min(K, kb + kspan) : K;
 
     float acc[8][8];
 #pragma unroll
@@ -70,8 +75,8 @@ k_gemm_simt(const float* __restrict__ X, size_t ldx, int xrows, const float* __r
     auto gload = [&](int k0) {
 #pragma unroll
         for (int h = 0; h < 2; ++h) {
-            sg_load<VEC>(X, ldx, xrows, K, m0 + lrow + 64 * h, k0 + lk, colmean, fix, center != 0, ra[h]);
-            sg_load<VEC>(Yt, ldy, t, K, n0 + lrow + 64 * h, k0 + lk, colmean, false, false, rb[h]);
+            sg_load<VEC>(X, ldx, xrows, ke, m0 + lrow + 64 * h, k0 + lk, colmean, fix, center != 0, ra[h]);
+            sg_load<VEC>(Yt, ldy, t, ke, n0 + lrow + 64 * h, k0 + lk, colmean, false, false, rb[h]);
         }
     };
     auto sstore = [&](int buf) {
@@ -84,13 +89,13 @@ k_gemm_simt(const float* __restrict__ X, size_t ldx, int xrows, const float* __r
             }
     };
 
-    const int nk = (K + SG_BK - 1) / SG_BK;
-    gload(0);
+    const int nk = (ke - kb + SG_BK - 1) / SG_BK;
+    gload(kb);
     sstore(0);
     __syncthreads();
     for (int kt = 0; kt < nk; ++kt) {
         const int buf = kt & 1;
-        if (kt + 1 < nk) gload((kt + 1) * SG_BK);
+        if (kt + 1 < nk) gload(kb + (kt + 1) * SG_BK);
 #pragma unroll
         for (int kk = 0; kk < SG_BK; ++kk) {
             const float4 a0 = *reinterpret_cast<const float4*>(&As[buf][kk][ty * 4]);
@@ -109,13 +114,14 @@ k_gemm_simt(const float* __restrict__ X, size_t ldx, int xrows, const float* __r
     }
 
     if constexpr (STORE) {
+        float* __restrict__ out = (split && blockIdx.z == 1) ? cpart : cout;
 #pragma unroll
         for (int ii = 0; ii < 8; ++ii) {
             const int row = m0 + (ii < 4 ? ty * 4 + ii : 64 + ty * 4 + (ii - 4));
 #pragma unroll
             for (int jj = 0; jj < 8; ++jj) {
                 const int col = n0 + (jj < 4 ? tx * 4 + jj : 64 + tx * 4 + (jj - 4));
-                if (row < xrows && col < t) cout[(size_t)col * ldc + row] = acc[ii][jj];
+                if (row < xrows && col < t) out[(size_t)col * ldc + row] = acc[ii][jj];
             }
         }
     } else {
@@ -140,6 +146,13 @@ k_gemm_simt(const float* __restrict__ X, size_t ldx, int xrows, const float* __r
             }
         }
     }
+}
+
+// cout[i] += cpart[i]: the second K half of a split store-form product.
+__global__ void __launch_bounds__(256) k_add_partial(float* __restrict__ cout, const float* __restrict__ cpart,
+                                                     long long n) {
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+        cout[i] += cpart[i];
 }
 
 }  // namespace oa

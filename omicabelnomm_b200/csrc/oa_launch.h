@@ -17,8 +17,9 @@ cudaError_t oa_launch_schur(int R, const SchurArgs& S, cudaStream_t st);
 cudaError_t oa_launch_pre_tc(const __nv_bfloat16* Xhi, const __nv_bfloat16* Xlo, int xrows,
                              const __nv_bfloat16* Bhi, const __nv_bfloat16* Blo, int c2, int n_pad, float* C, int ldc,
                              int* err, cudaStream_t st);
+// cpart (c2 * ldc floats, or null): scratch for the second K half of a split product
 cudaError_t oa_launch_pre_simt(const float* X, size_t ldx, int xrows, const float* B, size_t ldb, int c2, int K,
-                               const float* colmean, const int* has_nan, int center, float* C, int ldc,
+                               const float* colmean, const int* has_nan, int center, float* C, int ldc, float* cpart,
                                cudaStream_t st);
 // center: dosages taken relative to colmean (NaN -> 0); else NaN -> colmean
 cudaError_t oa_launch_gemm_simt(int R, const float* X, size_t ldx, int xrows, const float* Yt, size_t ldy, int t,
