@@ -165,7 +165,12 @@ def reference_available():
     return os.path.exists(REF_BIN) and os.access(REF_BIN, os.X_OK)
 
 
-def cpu_baseline(snps_per_proc: int = 48, steps: int = 1):
+# SNPs per reference process and step: about 5 s of single-thread work at n = 10,000, t = 1,000 (process
+# start-up and input reading are then a small part of each step)
+REF_SNPS_PER_PROC = 96
+
+
+def cpu_baseline(snps_per_proc: int = REF_SNPS_PER_PROC, steps: int = 1):
     """The reference CPU build on a bounded sample of the workload (~10-30 s of CPU)."""
     if not reference_available():
         return None
@@ -186,7 +191,7 @@ def run_reference_arm(args):
         print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/omicabelnomm_ref was not built"}))
         return 0
     procs = max(1, min(cpu_cores(), 64))
-    snps = 48
+    snps = REF_SNPS_PER_PROC
     with tempfile.TemporaryDirectory(prefix="oa_ref_") as d:
         n, t = prepare_reference_sample(d, snps, procs)
         for _ in range(args.warmup):
@@ -245,6 +250,31 @@ def time_scans(eng, xr_ptr, m, steps, warmup, local, barrier, max_over_ranks):
                 tuning=eng.tuning())
 
 
+def sgemm_peak_tflops(dev) -> float:
+    """Measured FP32 (FFMA, no TF32) matrix-multiply throughput of this GPU: cuBLAS SGEMM on
+    8192^3 operands, best of 5 after warm-up (the plain form's roofline denominator, as the
+    cuBLAS BF16 figure is the mixed form's)."""
+    import torch
+    prev = torch.backends.cuda.matmul.allow_tf32
+    torch.backends.cuda.matmul.allow_tf32 = False
+    try:
+        a = torch.randn(8192, 8192, device=dev)
+        b = torch.randn(8192, 8192, device=dev)
+        c = a @ b
+        best = float("inf")
+        for _ in range(5):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            torch.matmul(a, b, out=c)
+            e1.record()
+            e1.synchronize()
+            best = min(best, e0.elapsed_time(e1) / 1e3)
+        del a, b, c
+        return 2.0 * 8192 ** 3 / best / 1e12
+    finally:
+        torch.backends.cuda.matmul.allow_tf32 = prev
+
+
 def max_dt(eng_a, eng_b, xr_ptr, mb):
     """max |t_a - t_b| over the tests of the first mb SNPs (both finite)."""
     import numpy as np
@@ -257,6 +287,76 @@ def max_dt(eng_a, eng_b, xr_ptr, mb):
     a, b = out
     ok = np.isfinite(a) & np.isfinite(b)
     return float(np.max(np.abs(a[ok] - b[ok]))) if ok.any() else None
+
+
+def accuracy_vs_fp64(engines, XL, XR, Y, r, m_s):
+    """Errors of each form against the FP64 oracle (the checker, oracle/oa_oracle.py) on the first
+    m_s SNPs x all traits at full n, outside every timed region: max and 99.99th percentile of
+    |dt|, max relative SE error, max |d beta| / SE over the tests the oracle finds regular."""
+    import numpy as np
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oa_oracle as O
+    xl = XL.cpu().numpy()
+    xr = XR[:m_s * r].cpu().numpy()
+    y = Y.cpu().numpy()
+    l, n = xl.shape
+    t = y.shape[0]
+    inp = O.Inputs(XL=xl, XR=xr, Y=y, xl_names=[f"c{q}" for q in range(l)],
+                   xr_names=[f"s{i}" for i in range(m_s * r)], y_names=[f"y{j}" for j in range(t)], realN=n,
+                   kept=np.arange(n))
+    t0 = time.perf_counter()
+    D = O.solve(inp, O.Settings(r=r, storePInd=True), keep_dense=True).dense
+    oracle_s = time.perf_counter() - t0
+    ok = ~D.singular
+    tr, ser, br = D.tstat[:, :, l:][ok], D.se[:, :, l:][ok], D.beta[:, :, l:][ok]
+    out = {"sample": f"first {m_s} SNPs x {t} traits at n={n} (r={r})", "tests": int(ok.sum()),
+           "max_abs_t": float(np.abs(tr).max()), "oracle_s": oracle_s}
+    for name, eng in engines.items():
+        eng.enable_dense(True)
+        eng.run_device(XR.data_ptr(), m_s)
+        b, se, tt, _ = eng.dense(m_s)
+        eng.enable_dense(False)
+        dt = np.abs(tt[ok] - tr)
+        out[name] = {"max_dt": float(dt.max()), "p9999_dt": float(np.quantile(dt, 0.9999)),
+                     "max_rel_se": float((np.abs(se[ok] - ser) / np.abs(ser)).max()),
+                     "max_dbeta_over_se": float((np.abs(b[ok] - br) / np.abs(ser)).max())}
+    return out
+
+
+def cli_e2e(xl, xr, y, m_cli: int, precision: str):
+    """The drop-in boundary end to end: the engine's CLI (omicabelnomm_b200/lib/omicabelnomm, the
+    reference's flags and default thresholds) on .fvi/.fvd files of the first m_cli SNPs, written
+    to RAM-backed storage and read once untimed (page cache), then one timed run: file reading,
+    the scan and the _dis.txt output - the scope of the reference arm's CLI runs."""
+    import numpy as np
+    from omicabelnomm_b200 import engine as E
+    from omicabelnomm_b200 import fvformat
+    if not os.path.exists(E.CLI_PATH):
+        return {"error": "CLI not built"}
+    l, n = xl.shape
+    t = y.shape[0]
+    need = (m_cli + t + l) * n * 4 * 1.3 + (2 << 30)
+    base = "/dev/shm" if os.path.isdir("/dev/shm") and shutil.disk_usage("/dev/shm").free > need else None
+    if base is None and shutil.disk_usage(tempfile.gettempdir()).free < need:
+        return {"error": "no room for the input files"}
+    with tempfile.TemporaryDirectory(prefix="oa_cli_", dir=base) as d:
+        obs = fvformat.obs_names(n)
+        fvformat.write_fv(os.path.join(d, "XL"), np.ascontiguousarray(xl), obs, [f"cov{q}" for q in range(l)])
+        fvformat.write_fv(os.path.join(d, "Y"), np.ascontiguousarray(y), obs, [f"ph{j + 1}" for j in range(t)])
+        fvformat.write_fv(os.path.join(d, "XR"), np.ascontiguousarray(xr[:m_cli]), obs,
+                          [f"snp{i + 1}" for i in range(m_cli)])
+        cmd = [E.CLI_PATH, "-c", os.path.join(d, "XL"), "-g", os.path.join(d, "XR"), "-p", os.path.join(d, "Y"),
+               "-o", os.path.join(d, "out"), "--precision", precision]
+        subprocess.run(cmd, check=True, stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL)   # page cache
+        t0 = time.perf_counter()
+        p = subprocess.run(cmd, check=True, capture_output=True, text=True)
+        wall = time.perf_counter() - t0
+        out_bytes = os.path.getsize(os.path.join(d, "out_dis.txt"))
+    sig = p.stdout.split("Number of Significant Results:")[1].split()[0] if "Significant" in p.stdout else None
+    return {"value": m_cli * t / wall, "unit": "tests/s", "wall_s": wall, "precision": precision,
+            "sample": f"first {m_cli} SNPs x {t} traits at n={n}: .fvd files in page cache -> _dis.txt "
+                      f"({out_bytes} bytes), reference flags and default thresholds, one process",
+            "significant_results": int(sig) if sig else None, "storage": base or tempfile.gettempdir()}
 
 
 def batched_section(args, dev, local, rank, barrier, max_over_ranks):
@@ -292,6 +392,9 @@ def batched_section(args, dev, local, rank, barrier, max_over_ranks):
                        "autotune_s": tune_s, "clocks": R["clocks"]}
         engines[name] = eng
     dt = max_dt(engines["mixed"], engines["plain"], XR.data_ptr(), min(m, 4096))
+    acc = None
+    if rank == 0 and args.accuracy_snps > 0:
+        acc = accuracy_vs_fp64(engines, XL, XR, Y, r, min(m, args.accuracy_snps // 2))
     for eng in engines.values():
         eng.close()
     del XR, Y, XL
@@ -301,7 +404,9 @@ def batched_section(args, dev, local, rank, barrier, max_over_ranks):
                         f"4096-SNP blocks, whole scan one CUDA graph",
             "forms": forms,
             "mixed_over_plain": forms["mixed"]["tests_per_s"] / forms["plain"]["tests_per_s"],
-            "max_dt_mixed_vs_plain_first_4096_snps": dt}
+            "max_dt_mixed_vs_plain_first_4096_snps": dt,
+            "accuracy_vs_fp64": acc,
+            "max_dt_vs_fp64": acc["mixed"]["max_dt"] if acc else None}
 
 
 def serve_section(args, dev, local):
@@ -359,6 +464,11 @@ def main():
                     help="keep the engines' default tuning (profiling runs: timings under a profiler would steer "
                          "the autotuner elsewhere)")
     ap.add_argument("--batched-m", type=int, default=200000, help="SNPs of the batched workload (0: skip it)")
+    ap.add_argument("--cli-snps", type=int, default=65536,
+                    help="SNPs of the CLI end-to-end run (.fvd in page cache -> _dis.txt; 0: skip it)")
+    ap.add_argument("--accuracy-snps", type=int, default=512,
+                    help="SNPs of the omics-scale sample checked against the FP64 oracle outside the timed "
+                         "region (half as many for the batched r = 2 workload; 0: skip)")
     ap.add_argument("--serve-requests", type=int, default=120, help="requests of the serving run (0: skip it)")
     ap.add_argument("--serve-m", type=int, default=1_000_000, help="SNPs of the resident serving matrix")
     args = ap.parse_args()
@@ -431,6 +541,9 @@ def main():
     dt_mp = None
     if len(valid) == 2:
         dt_mp = max_dt(results["mixed"]["engine"], results["plain"]["engine"], XR.data_ptr(), min(m, 16384))
+    acc = None
+    if rank == 0 and args.accuracy_snps > 0:
+        acc = accuracy_vs_fp64({k: results[k]["engine"] for k in valid}, XL, XR, Y, 1, min(m, args.accuracy_snps))
     for k in valid:
         if k != head:
             results[k]["engine"].close()
@@ -458,6 +571,12 @@ def main():
             d2h += out.count * (16 + 12 * 1)   # stored rows come back packed by field: 16 + 12 r bytes each
         e2e_s = max_over_ranks((time.perf_counter() - t0) / args.e2e_steps)
     eng.close()
+    cli = None
+    if rank == 0 and world == 1 and args.cli_snps > 0:
+        try:
+            cli = cli_e2e(xl_host, xr_np, y_np, min(m, args.cli_snps), head)
+        except (OSError, subprocess.CalledProcessError) as ex:
+            cli = {"error": str(ex)}
     h2d = int(xr_np.nbytes + y_np.nbytes)
     del xr_host, y_host, xr_np, y_np
     torch.cuda.empty_cache()
@@ -489,6 +608,14 @@ def main():
             dist.destroy_process_group()
         return 0
 
+    sgemm_tf = sgemm_peak_tflops(dev)
+    plain_roof = None
+    if "plain" in valid:
+        g = results["plain"]["gemm_ms"] / 1000.0
+        ach = 2.0 * n * m * t / g / 1e12 if g > 0 else None
+        plain_roof = {"bound": "fp32-simt", "kernel": results["plain"]["kernel"], "achieved": ach, "peak": sgemm_tf,
+                      "unit": "TFLOP/s", "frac": (ach / sgemm_tf) if ach else None,
+                      "peak_source": "measured FP32 SGEMM (cuBLAS, TF32 off, 8192^3) on this GPU in this run"}
     peaks = {}
     try:
         with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
@@ -505,10 +632,9 @@ def main():
                     if "bf16_tflops_sustained" in peaks else "fallback (sustained)")
         bound = "tensor"
     else:
-        clk = (R["clocks"] or {}).get("sm_mhz") or 1965.0
-        peak = 148 * 128 * 2 * clk * 1e6 / 1e12
-        peak_src = f"nominal FP32 FFMA peak at the sampled {clk:.0f} MHz SM clock (148 SMs x 128 lanes)"
-        bound = "tensor"
+        peak = sgemm_tf
+        peak_src = "measured FP32 SGEMM (cuBLAS, TF32 off, 8192^3) on this GPU in this run"
+        bound = "fp32-simt"
     traffic = None
     try:
         with open(os.path.join(ROOT, "profiles", "traffic.json")) as f:
@@ -553,7 +679,12 @@ def main():
                        "autotune_s": v["autotune_s"]}
                       if "error" not in v else v)
                   for k, v in results.items()},
+        "plain_roofline": plain_roof,
+        "e2e_cli": cli,
         "max_dt_mixed_vs_plain_first_16384_snps": dt_mp,
+        "accuracy_vs_fp64": acc,
+        "max_dt_vs_fp64": {"omics": acc[head]["max_dt"] if acc else None,
+                           "batched_r2": (batched or {}).get("max_dt_vs_fp64")},
         "batched": batched,
         "serve": serve,
     }

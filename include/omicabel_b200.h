@@ -132,6 +132,23 @@ oa_status oa_run_snps_device(oa_engine* e, const float* xr_dev, int32_t mb,
 oa_status oa_dense_last(oa_engine* e, float* beta, float* se, float* tstat, float* r2);
 oa_status oa_enable_dense(oa_engine* e, int32_t on);
 
+/* Status of each test of the last SNP block ([t][mb] bytes, trait-major, as
+ * oa_dense_last), with dense output enabled: 0 = evaluated, no SNP term
+ * passed the store filters; otherwise one of
+ *   OA_TEST_SINGULAR  the (l+r) x (l+r) system is singular for this trait's
+ *                     missingness pattern (monomorphic or collinear SNP);
+ *                     skipped.  The reference ignores sposv's info and
+ *                     prints undefined values (src/Algorithm.cpp:767-773);
+ *   OA_TEST_RSS       residual sum of squares <= 0: skipped (src/Algorithm.cpp:1094-1099, 1119);
+ *   OA_TEST_R2        R2 at or below the store threshold (without store_all):
+ *                     no term stored (src/Algorithm.cpp:1119-1123);
+ *   OA_TEST_STORED    at least one SNP term stored: the test has a row in oa_rows. */
+#define OA_TEST_SINGULAR 1u
+#define OA_TEST_RSS 2u
+#define OA_TEST_R2 4u
+#define OA_TEST_STORED 8u
+oa_status oa_dense_flags(oa_engine* e, uint8_t* flags);
+
 /* Row subset of device SNP blocks: after this call oa_run_snps_device reads
  * SNP columns of ld floats (e.g. a genotype matrix kept resident across
  * calls) and takes rows[0..n_rows) of each (ascending, n_rows = the
@@ -184,22 +201,27 @@ oa_status oa_reserve(oa_engine* e, int32_t traits, int32_t snps);
 
 /* Plain-FP32 dense scan of one SNP block that allocates no memory.
  *
- * For callers that cannot call cudaMalloc: code recording a CUDA graph on
- * `stream`, plug-ins whose host framework owns the device memory pool, and
- * processes whose device memory was reserved up front.  All intermediates
- * live in one static device array of OA_NOALLOC_SCRATCH_BYTES; inputs and
- * outputs are the caller's device buffers (column-major, individual index
- * contiguous): covariates n x l (NaN-free), traits n x t (NaN = missing),
- * dosages n x (r*mb) (NaN = mean-imputed); outputs beta/se/|t| [t][mb][r]
- * and R2 [t][mb] (NaN where the test is singular or has RSS <= 0), the same
- * numbers as oa_run_snps_device + oa_dense_last of an engine with
- * store_all.  Limits: r in {1, 2, 4}, l <= OA_MAX_L, t <= 2048, and all
- * intermediates (about 4*n*t + 9*t*mb*r*r + 8*n*l bytes) within the array;
- * larger inputs return OA_ERR_UNSUPPORTED.  Calls share the array: calls that
- * overlap on the GPU (other streams or threads) race.  The first call on a
- * device looks up the array's address and must come before any stream
- * capture.  Synchronises `stream` (a cudaStream_t; NULL = default stream)
- * before returning.  No counterpart in the reference. */
+ * For callers that cannot call cudaMalloc: plug-ins whose host framework
+ * owns the device memory pool and forbids raw allocations, and processes
+ * whose device memory was reserved up front under a hard cap.  All
+ * intermediates live in one static device array of OA_NOALLOC_SCRATCH_BYTES;
+ * inputs and outputs are the caller's device buffers (column-major,
+ * individual index contiguous): covariates n x l (NaN-free), traits n x t
+ * (NaN = missing), dosages n x (r*mb) (NaN = mean-imputed); outputs
+ * beta/se/|t| [t][mb][r] and R2 [t][mb] (NaN where the test is singular or
+ * has RSS <= 0), the same numbers as oa_run_snps_device + oa_dense_last of
+ * an engine with store_all.  Covariates are rejected with OA_ERR_COLLINEAR
+ * by the engine's rule (a singular value below 1e-6), and also when their
+ * condition number is beyond about 1e15 (the device QR breaks down).
+ * Limits: r in {1, 2, 4}, l <= OA_MAX_L, t <= 2048, and all intermediates
+ * (about 4*n*t + 9*t*mb*r*r + 8*n*l bytes) within the array; larger inputs
+ * return OA_ERR_UNSUPPORTED.  Calls share the array: calls that overlap on
+ * the GPU (other streams or threads) race.  The first call on a device looks
+ * up the array's address.  The call reads small status words back to the
+ * host and synchronises `stream` (a cudaStream_t; NULL = default stream)
+ * before returning.  A CUDA error already pending on the calling thread
+ * (cudaPeekAtLastError) is left in place and reported as OA_ERR_CUDA without
+ * running.  No counterpart in the reference. */
 oa_status oa_scan_dense_noalloc(const float* xl_dev, const float* y_dev, const float* xr_dev, int32_t n,
                                 int32_t l, int32_t r, int32_t t, int32_t mb, float* beta_dev, float* se_dev,
                                 float* t_dev, float* r2_dev, void* stream);

@@ -62,6 +62,8 @@ struct EpiArgs {
     const float* zD;         // per (zero set, SNP) sum over zero rows of x x' [Z][mb][r][r]
     const double* zQ;        // per zero set sum of q q' [Z][l][l]
     const double* W;         // (Q_obs'Q_obs)^-1 per pattern [G][l][l]
+    const float* qdel;       // the reference's r >= 2 downdate (quirk mode) per (pattern, SNP) [G][mb][l][r], or null
+    const double* qK;        // its RSS Gram term per (pattern, SNP) [G][mb][r][r], or null
     // thresholds
     float min_r2, min_t;
     int store_all;
@@ -77,6 +79,7 @@ struct EpiArgs {
     float* d_t;
     float* d_r2;
     float* d_sig;
+    uint8_t* d_flags;        // per-test status bits [t][mb] (OA_TEST_*), or null
     int t;
     int snp_base;            // index of the block's first SNP within the API call
     long long dense_ld;      // SNPs per trait row of the dense outputs
@@ -142,6 +145,27 @@ __device__ __host__ inline bool spd_inverse(double* A, int k, double rel_tol) {
             A[j * k + i] = s;
         }
     return true;
+}
+
+// A SNP column whose residual sum of squares after the covariates (the
+// diagonal of its Schur complement) is below this fraction of its own sum of
+// squares over the same rows is taken as collinear with the covariates: the
+// test is singular.  The sums are accumulated in FP32 (relative rounding about
+// 1e-7), so an exactly collinear column (monomorphic on the observed rows, or
+// equal to a covariate) leaves a residual of about 1e-7 of its sum of squares,
+// while a real SNP keeps almost all of it (1 - R2 of the SNP on the covariates).
+constexpr double SCHUR_SING_REL = 1e-5;
+
+// Inverse of the r x r Schur complement S of a test (in place); false if the
+// system is singular: a column collinear with the covariates (S_aa at or below
+// SCHUR_SING_REL of dss[a], the column's sum of squares over the same rows) or
+// SNP columns collinear among themselves (a Cholesky pivot at or below 1e-9 of
+// its diagonal).
+template <int R>
+__device__ __host__ inline bool schur_inverse(double* S, const double* dss) {
+    for (int a = 0; a < R; ++a)
+        if (!(S[a * R + a] > SCHUR_SING_REL * dss[a])) return false;
+    return spd_inverse<R>(S, R, 1e-9);
 }
 
 }  // namespace oa

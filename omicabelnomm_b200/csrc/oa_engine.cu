@@ -290,6 +290,8 @@ struct oa_engine {
     DBuf<float> C2part;         // plain pre-GEMM: partial product of the second K half
     DBuf<int> has_nan;
     DBuf<double> sinv, sfinv;
+    DBuf<float> qdel;           // quirk mode: per (pattern, SNP) terms of the reference's r >= 2 downdate
+    DBuf<double> qK;
     DBuf<uint8_t> sing;
     // stored rows
     DBuf<Rec> rec, rec2;
@@ -323,6 +325,7 @@ struct oa_engine {
     // dense outputs
     bool dense_on = false;
     DBuf<float> d_beta, d_se, d_t, d_r2, d_sig;
+    DBuf<uint8_t> d_flags;
     // row subset of device SNP blocks: columns of x_ld floats, rows xrows[0..n)
     DBuf<int> xrows;
     long long x_ld = 0;
@@ -370,10 +373,10 @@ void for_each_buf(oa_engine* e, F&& f) {
     f(e->Xstage[0]); f(e->Xstage[1]); f(e->Xmodel); f(e->inter); f(e->Xhi); f(e->Xlo);
     f(e->mean); f(e->varx); f(e->aobs); f(e->afull); f(e->zA); f(e->zD); f(e->D); f(e->Dset); f(e->C2T);
     f(e->C2part);
-    f(e->has_nan); f(e->sinv); f(e->sfinv); f(e->sing);
+    f(e->has_nan); f(e->sinv); f(e->sfinv); f(e->sing); f(e->qdel); f(e->qK);
     f(e->rec); f(e->rec2); f(e->cov); f(e->cov2); f(e->counters); f(e->keys); f(e->keys2); f(e->perm);
     f(e->perm2); f(e->cub_tmp);
-    f(e->d_beta); f(e->d_se); f(e->d_t); f(e->d_r2); f(e->d_sig); f(e->xrows);
+    f(e->d_beta); f(e->d_se); f(e->d_t); f(e->d_r2); f(e->d_sig); f(e->d_flags); f(e->xrows);
     f(e->item_start); f(e->set_item_off); f(e->pass_off); f(e->marks);
 }
 
@@ -421,6 +424,11 @@ static __global__ void k_column_model(const float* __restrict__ in, int n, int i
         for (int c = 0; c < in_cols; ++c) out[((size_t)i * in_cols + c) * n + k] = W.w[c] * src[(size_t)c * n];
     }
 }
+
+// The reference's r >= 2 downdate is reproduced (quirk mode; with r = 1 it
+// changes nothing).  It needs raw, uncentred SNP columns and the pre-GEMM
+// statistics path.
+bool quirk_on(const oa_engine* e) { return e->cfg.quirk_r2 && e->r >= 2; }
 
 // Columns per SNP of the caller's SNP blocks.
 int input_cols(const oa_engine* e) { return e->in_cols > 0 ? e->in_cols : e->r; }
@@ -660,7 +668,7 @@ oa_status prepare_tuning(oa_engine* e) {
     e->variant = (e->req.gemm_variant >= 1 && e->req.gemm_variant <= 4) ? e->req.gemm_variant : 4;
     e->raster = e->req.gemm_raster == 2 ? 2 : 1;
     e->lean_spb = e->req.lean_spb > 0 ? std::min(e->req.lean_spb, 8 / e->r) : 0;
-    e->use_pre = e->req.stats_path == 1 || (e->req.stats_path != 2 && e->c2 <= std::max(t, 256));
+    e->use_pre = quirk_on(e) || e->req.stats_path == 1 || (e->req.stats_path != 2 && e->c2 <= std::max(t, 256));
     if (e->use_pre && !e->b2_ready) {
         const size_t nb2 = (size_t)e->c2 * e->n_pad;
         OA_CHECK(e->B2.ensure(nb2));
@@ -885,6 +893,8 @@ oa_status stats_pre(oa_engine* e, const float* X, size_t ldx, const int* xrows, 
     S.sfinv = e->cfg.disp_cov ? e->sfinv.p : nullptr;
     S.zA = e->zA.p;
     S.zD = e->zD.p;
+    S.qdel = quirk_on(e) ? e->qdel.p : nullptr;
+    S.qK = quirk_on(e) ? e->qK.p : nullptr;
     OA_CU(oa_launch_schur(R, S, e->st));
     ++e->launches;
     return OA_OK;
@@ -924,6 +934,8 @@ EpiArgs epi_args(oa_engine* e, int mbc, int snp_base) {
     E.zD = e->zD.p;
     E.zQ = e->zQ.p;
     E.W = e->W.p;
+    E.qdel = quirk_on(e) ? e->qdel.p : nullptr;
+    E.qK = quirk_on(e) ? e->qK.p : nullptr;
     E.min_r2 = e->cfg.min_r2_store;
     E.min_t = e->cfg.min_t_store;
     E.store_all = e->cfg.store_all;
@@ -941,6 +953,7 @@ EpiArgs epi_args(oa_engine* e, int mbc, int snp_base) {
         E.d_t = e->d_t.p;
         E.d_r2 = e->d_r2.p;
         E.d_sig = e->d_sig.p;
+        E.d_flags = e->d_flags.p;
     }
     return E;
 }
@@ -997,6 +1010,10 @@ oa_status ensure_chunk_buffers(oa_engine* e) {
     OA_CHECK(e->zA.ensure(Z * mb * l * r));
     OA_CHECK(e->zD.ensure(Z * mb * r * r));
     if (e->cfg.disp_cov || e->Z > 0) OA_CHECK(e->aobs.ensure(G * mb * l * r));
+    if (quirk_on(e)) {
+        OA_CHECK(e->qdel.ensure(G * mb * l * r));
+        OA_CHECK(e->qK.ensure(G * mb * r * r));
+    }
     if (e->cfg.disp_cov) {
         OA_CHECK(e->afull.ensure(mb * l * r));
         OA_CHECK(e->sfinv.ensure(mb * r * r));
@@ -1254,6 +1271,7 @@ oa_status run_snps_impl(oa_engine* e, const float* xr, int32_t mb, bool host_inp
         OA_CHECK(e->d_t.ensure(nd * e->r));
         OA_CHECK(e->d_r2.ensure(nd));
         OA_CHECK(e->d_sig.ensure(nd));
+        OA_CHECK(e->d_flags.ensure(nd));
         e->dense_ld = mb;
     }
     e->last_ms = 0.f;
@@ -1551,10 +1569,6 @@ oa_status oa_engine_create(const oa_config* cfg, oa_engine** out) {
         set_err("unknown precision %d", cfg->precision);
         return OA_ERR_ARG;
     }
-    if (cfg->quirk_r2 && cfg->r >= 2) {
-        set_err("the reference's r >= 2 downdate quirk is reproduced by the oracle only");
-        return OA_ERR_UNSUPPORTED;
-    }
     int ndev = 0;
     if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
         cudaGetLastError();
@@ -1730,7 +1744,7 @@ oa_status oa_set_covariates(oa_engine* e, const float* xl) {
     // proportional to 1 and the other Q columns are orthogonal to 1); the
     // kernels then work with x - mean, whose sums cancel far less.
     const char* ce = getenv("OA_CENTER");
-    e->center = xl[0] != 0.f && !(ce && ce[0] == '0');
+    e->center = xl[0] != 0.f && !(ce && ce[0] == '0') && !quirk_on(e);
     for (int k = 1; k < n && e->center; ++k) e->center = xl[k] == xl[0];
     e->have_cov = true;
     e->t = 0;
@@ -2003,6 +2017,23 @@ oa_status oa_dense_last(oa_engine* e, float* beta, float* se, float* tstat, floa
     if (se) OA_CU(cudaMemcpyAsync(se, e->d_se.p, sizeof(float) * nd * e->r, cudaMemcpyDeviceToHost, e->st));
     if (tstat) OA_CU(cudaMemcpyAsync(tstat, e->d_t.p, sizeof(float) * nd * e->r, cudaMemcpyDeviceToHost, e->st));
     if (r2) OA_CU(cudaMemcpyAsync(r2, e->d_r2.p, sizeof(float) * nd, cudaMemcpyDeviceToHost, e->st));
+    OA_CU(cudaStreamSynchronize(e->st));
+    return OA_OK;
+}
+
+oa_status oa_dense_flags(oa_engine* e, uint8_t* flags) {
+    clear_stale_error(__func__);
+    if (!e || !flags) {
+        set_err("null argument");
+        return OA_ERR_ARG;
+    }
+    if (!e->dense_on || e->last_mb == 0) {
+        set_err("dense output was not enabled for the last SNP block");
+        return OA_ERR_STATE;
+    }
+    OA_CU(cudaSetDevice(e->cfg.device));
+    const size_t nd = (size_t)e->t * e->last_mb;
+    OA_CU(cudaMemcpyAsync(flags, e->d_flags.p, nd, cudaMemcpyDeviceToHost, e->st));
     OA_CU(cudaStreamSynchronize(e->st));
     return OA_OK;
 }

@@ -35,6 +35,16 @@ __device__ __forceinline__ TraitP load_trait(const EpiArgs& E, int j) {
     return p;
 }
 
+// Status bits of an evaluated (non-singular) test (OA_TEST_*, include/omicabel_b200.h):
+// RSS <= 0 skips it (src/Algorithm.cpp:1094-1099, 1119); otherwise R2 at or
+// below the store threshold without -f skips its terms (:1119-1123); a test
+// with a stored SNP term has a row (:1156-1157, 1197).
+__device__ __forceinline__ uint8_t test_flags(const EpiArgs& E, double rss, float r2, uint32_t mask) {
+    if (!(rss > 0.0)) return OA_TEST_RSS;
+    if (!(r2 > E.min_r2 || E.store_all)) return OA_TEST_R2;
+    return mask ? OA_TEST_STORED : 0;
+}
+
 // Schur inverse of (pattern g, SNP i); false if the system is singular.
 template <int R>
 __device__ __forceinline__ bool load_schur(const EpiArgs& E, int g, int i, double* S) {
@@ -81,21 +91,58 @@ __device__ __noinline__ double zero_rows_rss(const EpiArgs& E, int i, int j, con
     return c;
 }
 
+// SNP coefficients and RSS of the reference's r >= 2 downdate (quirk mode;
+// the per-(pattern, SNP) terms come from schur_quirk in oa_lean.cuh):
+//   beta_x = Sq^-1 (z - dl' b0_j),  RSS = RSS0_j - 2 beta_x' z + beta_x' K beta_x.
+template <int R>
+__device__ __noinline__ double quirk_beta_rss(const EpiArgs& E, int i, int j, const TraitP& tp, const double* S,
+                                              const float* z, double* bx) {
+    const int l = E.l;
+    const size_t gi = (size_t)tp.g * E.mb + i;
+    const float* dl = E.qdel + gi * (size_t)(l * R);
+    const double* b0 = E.b0 + (size_t)j * l;
+    double rhs[R];
+    for (int a = 0; a < R; ++a) {
+        double s = (double)z[a];
+        for (int q = 0; q < l; ++q) s -= (double)dl[q * R + a] * b0[q];
+        rhs[a] = s;
+    }
+    for (int a = 0; a < R; ++a) {
+        double s = 0.0;
+        for (int b = 0; b < R; ++b) s += S[a * R + b] * rhs[b];
+        bx[a] = s;
+    }
+    const double* K = E.qK + gi * (size_t)(R * R);
+    double zb = 0.0, quad = 0.0;
+    for (int a = 0; a < R; ++a) {
+        zb += (double)z[a] * bx[a];
+        double s = 0.0;
+        for (int b = 0; b < R; ++b) s += K[a * R + b] * bx[b];
+        quad += bx[a] * s;
+    }
+    return tp.rss0 - 2.0 * zb + quad;
+}
+
 // One test given its trait constants, Schur inverse S and the SNP's var_x.
 template <int R>
 __device__ __forceinline__ bool epi_core(const EpiArgs& E, int i, int j, const float* z, const TraitP& tp,
                                          const double* S, const float* vx, Rec& rc) {
     double bx[R];
-    double zz = 0.0;
+    double rss;
+    if (E.qK) {
+        rss = quirk_beta_rss<R>(E, i, j, tp, S, z, bx);
+    } else {
+        double zz = 0.0;
 #pragma unroll
-    for (int a = 0; a < R; ++a) {
-        double s = 0.0;
+        for (int a = 0; a < R; ++a) {
+            double s = 0.0;
 #pragma unroll
-        for (int b = 0; b < R; ++b) s += S[a * R + b] * (double)z[b];
-        bx[a] = s;
-        zz += (double)z[a] * s;
+            for (int b = 0; b < R; ++b) s += S[a * R + b] * (double)z[b];
+            bx[a] = s;
+            zz += (double)z[a] * s;
+        }
+        rss = tp.rss0 - zz;
     }
-    double rss = tp.rss0 - zz;
     if (tp.zs >= 0) rss -= zero_rows_rss<R>(E, i, j, tp, bx);
     const float rssf = (float)rss;
     const float r2 = 1.f - rssf * tp.a_r2;
@@ -134,6 +181,7 @@ __device__ __forceinline__ bool epi_core(const EpiArgs& E, int i, int j, const f
             E.d_se[o * R + a] = pos ? rc.se[a] : nanf_;
             E.d_t[o * R + a] = pos ? rc.t[a] : nanf_;
         }
+        if (E.d_flags) E.d_flags[o] = test_flags(E, rss, r2, mask);
     }
     return live && mask != 0u;
 }
@@ -153,16 +201,21 @@ template <int R>
 __device__ __forceinline__ bool epi_decide(const EpiArgs& E, int i, int j, const float* z, const TraitP& tp,
                                            const double* S, const float* vx, EpiTest<R>& o) {
     double bx[R];
-    double zz = 0.0;
+    double rss;
+    if (E.qK) {
+        rss = quirk_beta_rss<R>(E, i, j, tp, S, z, bx);
+    } else {
+        double zz = 0.0;
 #pragma unroll
-    for (int a = 0; a < R; ++a) {
-        double s = 0.0;
+        for (int a = 0; a < R; ++a) {
+            double s = 0.0;
 #pragma unroll
-        for (int b = 0; b < R; ++b) s += S[a * R + b] * (double)z[b];
-        bx[a] = s;
-        zz += (double)z[a] * s;
+            for (int b = 0; b < R; ++b) s += S[a * R + b] * (double)z[b];
+            bx[a] = s;
+            zz += (double)z[a] * s;
+        }
+        rss = tp.rss0 - zz;
     }
-    double rss = tp.rss0 - zz;
     if (tp.zs >= 0) rss -= zero_rows_rss<R>(E, i, j, tp, bx);
     const float rssf = (float)rss;
     o.rss = rss;
@@ -192,6 +245,7 @@ __device__ __forceinline__ bool epi_decide(const EpiArgs& E, int i, int j, const
             E.d_se[off * R + a] = pos ? o.se[a] : nanf_;
             E.d_t[off * R + a] = pos ? o.t[a] : nanf_;
         }
+        if (E.d_flags) E.d_flags[off] = test_flags(E, rss, o.r2, mask);
     }
     const bool live = (rss > 0.0) && (o.r2 > E.min_r2 || E.store_all);
     return live && mask != 0u;
@@ -231,6 +285,7 @@ __device__ __forceinline__ void epi_dense_nan(const EpiArgs& E, int i, const Tra
     E.d_sig[o] = nanf_;
 #pragma unroll
     for (int a = 0; a < R; ++a) E.d_beta[o * R + a] = E.d_se[o * R + a] = E.d_t[o * R + a] = nanf_;
+    if (E.d_flags) E.d_flags[o] = OA_TEST_SINGULAR;
 }
 
 // Self-contained evaluation (loads its own constants): the SIMT GEMM epilogue.

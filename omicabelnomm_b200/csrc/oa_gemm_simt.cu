@@ -51,8 +51,8 @@ cudaError_t oa_launch_pre_simt(const float* X, size_t ldx, int xrows, const floa
                                                           none, C, ldc, cpart, kspan);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess || !cpart) return e;
-    const long long n = (long long)c2 * ldc;
-    k_add_partial<<<(unsigned)std::min<long long>((n + 255) / 256, 4096), 256, 0, st>>>(C, cpart, n);
+    const long long n = (long long)c2 * xrows;
+    k_add_partial<<<(unsigned)std::min<long long>((n + 255) / 256, 4096), 256, 0, st>>>(C, cpart, c2, xrows, ldc);
     return cudaGetLastError();
 }
 

@@ -148,11 +148,16 @@ k_gemm_simt(const float* __restrict__ X, size_t ldx, int xrows, const float* __r
     }
 }
 
-// cout[i] += cpart[i]: the second K half of a split store-form product.
+// The second K half of a split store-form product:
+// C[col * ldc + row] += Cpart[col * ldc + row] for the rows < xrows of each of
+// the c2 columns (a partial last chunk leaves rows [xrows, ldc) unwritten).
 __global__ void __launch_bounds__(256) k_add_partial(float* __restrict__ cout, const float* __restrict__ cpart,
-                                                     long long n) {
-    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+                                                     int c2, int xrows, int ldc) {
+    const long long n = (long long)c2 * xrows;
+    for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n; q += (long long)gridDim.x * blockDim.x) {
+        const long long i = (q / xrows) * ldc + q % xrows;
         cout[i] += cpart[i];
+    }
 }
 
 }  // namespace oa

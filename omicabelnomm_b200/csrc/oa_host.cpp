@@ -50,6 +50,8 @@ struct Fvi {
     uint16_t type = 0;
     uint32_t nelements = 0, nobs = 0, nvar = 0, bytes_per_record = 0, bits_per_record = 0, namelength = 0;
     std::vector<char> names;  // (nobs + nvar) * namelength raw bytes
+    // bytes of one stored value: 4 (float, type 5) or 8 (double, type 6)
+    size_t elem_bytes() const { return type == 6 ? 8 : 4; }
     std::string obs_name(size_t i) const { return cstr(i); }
     std::string var_name(size_t i) const { return cstr(nobs + i); }
     const char* raw(size_t i) const { return names.data() + i * namelength; }
@@ -94,12 +96,48 @@ bool read_fvi(const std::string& path, Fvi& f) {
         return false;
     }
     // the reference reads every .fvd as float32 and never checks `type`
-    // (src/AIOwrapper.cpp:1103-1125); a non-float layout is refused here
-    if (f.type != 5 || f.bytes_per_record != 4) {
-        herr("%s: data type %u / %u bytes per record: only float32 (type 5) is supported", path.c_str(), f.type,
-             f.bytes_per_record);
+    // (src/AIOwrapper.cpp:1103-1125), although its header declares the
+    // DatABEL types (src/AIOwrapper.h:145-153) and a doublefileType flag
+    // (src/AIOwrapper.h:41) that nothing sets.  Here float (type 5) and double
+    // (type 6, converted to float as it is read) are accepted; the integer
+    // types are refused.
+    const bool is_float = f.type == 5 && f.bytes_per_record == 4;
+    const bool is_double = f.type == 6 && f.bytes_per_record == 8;
+    if (!is_float && !is_double) {
+        herr("%s: data type %u with %u bytes per record: only float (type 5, 4 bytes) and double (type 6, "
+             "8 bytes) are supported", path.c_str(), f.type, f.bytes_per_record);
         return false;
     }
+    return true;
+}
+
+// The .fvd beside an .fvi must hold nobs * nvar values of the declared type
+// (a shorter file would end in a failed read halfway through a scan).
+bool check_fvd(const std::string& prefix, const Fvi& f) {
+    struct stat sb;
+    const std::string path = prefix + ".fvd";
+    if (stat(path.c_str(), &sb) != 0) {
+        herr("Error reading file: %s", path.c_str());
+        return false;
+    }
+    const unsigned long long want = (unsigned long long)f.nobs * f.nvar * f.elem_bytes();
+    if ((unsigned long long)sb.st_size < want) {
+        herr("%s: %lld bytes, the header's %u x %u values of %zu bytes need %llu (truncated file)", path.c_str(),
+             (long long)sb.st_size, f.nobs, f.nvar, f.elem_bytes(), want);
+        return false;
+    }
+    return true;
+}
+
+// count values starting at value index `first` of an .fvd, as float (64-bit
+// file offsets: files beyond 2^31 values, which the reference's int offsets
+// cannot address, src/AIOwrapper.cpp:909-913, 1196).
+bool read_values(FILE* fp, size_t elem_bytes, size_t first, size_t count, float* dst, std::vector<double>& dbl) {
+    if (fseeko(fp, (off_t)(elem_bytes * first), SEEK_SET) != 0) return false;
+    if (elem_bytes == 4) return fread(dst, sizeof(float), count, fp) == count;
+    dbl.resize(count);
+    if (fread(dbl.data(), sizeof(double), count, fp) != count) return false;
+    for (size_t q = 0; q < count; ++q) dst[q] = (float)dbl[q];
     return true;
 }
 
@@ -173,16 +211,14 @@ Runs keep_runs(const std::vector<char>& keep) {
     return r;
 }
 
-// Read variables [v0, v0+count) of a .fvd file, keeping only the rows in
-// `runs`, into dst (count columns of `kept` floats each).
-bool read_columns(FILE* fp, size_t fileN, size_t v0, size_t count, const Runs& runs, size_t kept, float* dst,
-                  std::vector<float>& scratch) {
+// Read variables [v0, v0+count) of a .fvd file of elem_bytes-byte values,
+// keeping only the rows in `runs`, into dst (count columns of `kept` floats each).
+bool read_columns(FILE* fp, size_t elem_bytes, size_t fileN, size_t v0, size_t count, const Runs& runs,
+                  size_t kept, float* dst, std::vector<float>& scratch, std::vector<double>& dbl) {
     const bool all = runs.size() == 1 && runs[0].first == 0 && (size_t)runs[0].second == fileN;
-    const size_t bytes = sizeof(float) * fileN * count;
-    if (fseeko(fp, (off_t)(sizeof(float) * fileN * v0), SEEK_SET) != 0) return false;
-    if (all) return fread(dst, 1, bytes, fp) == bytes;
+    if (all) return read_values(fp, elem_bytes, fileN * v0, fileN * count, dst, dbl);
     scratch.resize(fileN * count);
-    if (fread(scratch.data(), 1, bytes, fp) != bytes) return false;
+    if (!read_values(fp, elem_bytes, fileN * v0, fileN * count, scratch.data(), dbl)) return false;
     for (size_t c = 0; c < count; ++c) {
         const float* src = scratch.data() + c * fileN;
         float* out = dst + c * kept;
@@ -492,6 +528,7 @@ oa_status oa_solve(const oa_settings* S, oa_outputs* out) {
                       fy = S->fname_y ? S->fname_y : "", fout = S->fname_out ? S->fname_out : "";
     Fvi FL, FR, FY;
     if (!read_fvi(fy + ".fvi", FY) || !read_fvi(fxl + ".fvi", FL) || !read_fvi(fxr + ".fvi", FR)) return OA_ERR_IO;
+    if (!check_fvd(fy, FY) || !check_fvd(fxl, FL) || !check_fvd(fxr, FR)) return OA_ERR_IO;
     if (FL.nobs != FR.nobs || FR.nobs != FY.nobs) {
         // the reference only stops when all three differ (src/AIOwrapper.cpp:72-85); any mismatch is an error here
         herr("The number of elements/individuals from the input files do not coincide with each other! %s:%u %s:%u "
@@ -559,7 +596,8 @@ oa_status oa_solve(const oa_settings* S, oa_outputs* out) {
                  file_r);
             return OA_ERR_ARG;
         }
-        if (!read_fvi(std::string(S->fname_interactions) + ".fvi", FI)) return OA_ERR_IO;
+        if (!read_fvi(std::string(S->fname_interactions) + ".fvi", FI) || !check_fvd(S->fname_interactions, FI))
+            return OA_ERR_IO;
         if (FI.nobs != FR.nobs) {
             herr("The number of elements/individuals from the input files do not coincide with each other! %s:%u %s:%u",
                  S->fname_interactions, FI.nobs, fxr.c_str(), FR.nobs);
@@ -612,9 +650,10 @@ oa_status oa_solve(const oa_settings* S, oa_outputs* out) {
             herr("Error Reading File %s", fxl.c_str());
             return OA_ERR_IO;
         }
-        const size_t got = fread(xl_all.data(), sizeof(float), xl_all.size(), fp);
+        std::vector<double> dbl;
+        const bool got = read_values(fp, FL.elem_bytes(), 0, xl_all.size(), xl_all.data(), dbl);
         fclose(fp);
-        if (got != xl_all.size()) {
+        if (!got) {
             herr("%s.fvd: short read", fxl.c_str());
             return OA_ERR_IO;
         }
@@ -639,9 +678,10 @@ oa_status oa_solve(const oa_settings* S, oa_outputs* out) {
             }
         inter_all.resize((size_t)n_inter * fileN);
         FILE* fp = fopen((std::string(S->fname_interactions) + ".fvd").c_str(), "rb");
-        const size_t got = fp ? fread(inter_all.data(), sizeof(float), inter_all.size(), fp) : 0;
+        std::vector<double> dbl;
+        const bool got = fp && read_values(fp, FI.elem_bytes(), 0, inter_all.size(), inter_all.data(), dbl);
         if (fp) fclose(fp);
-        if (got != inter_all.size()) {
+        if (!got) {
             herr("Error opening Interactions File %s", S->fname_interactions);
             return OA_ERR_IO;
         }
@@ -844,6 +884,7 @@ oa_status oa_solve(const oa_settings* S, oa_outputs* out) {
             pin[b] = (float*)malloc(sizeof(float) * pin_floats);
         }
     std::vector<float> scratch[2];
+    std::vector<double> dscratch[2], ydbl;
     std::vector<float> Yblk, yscratch;
     int64_t tests = 0, singular = 0;
     uint64_t sig_cov = 0;
@@ -852,7 +893,7 @@ oa_status oa_solve(const oa_settings* S, oa_outputs* out) {
     for (int y0 = 0; y0 < t && st == OA_OK && io_ok; y0 += tb) {
         const int tcur = std::min(tb, t - y0);
         Yblk.resize((size_t)tcur * n);
-        if (!read_columns(fyd, fileN, y0, tcur, runs, n, Yblk.data(), yscratch)) {
+        if (!read_columns(fyd, FY.elem_bytes(), fileN, y0, tcur, runs, n, Yblk.data(), yscratch, ydbl)) {
             herr("Error reading file %s.fvd", fy.c_str());
             io_ok = false;
             break;
@@ -861,8 +902,8 @@ oa_status oa_solve(const oa_settings* S, oa_outputs* out) {
         if (st != OA_OK) break;
         auto read_call = [&](int c, int b) {
             const int s0 = c * call_snps, cnt = std::min(call_snps, m - s0);
-            return read_columns(fr, fileN, (size_t)(first + s0) * file_r, (size_t)cnt * file_r, runs, n, pin[b],
-                                scratch[b]);
+            return read_columns(fr, FR.elem_bytes(), fileN, (size_t)(first + s0) * file_r, (size_t)cnt * file_r, runs,
+                                n, pin[b], scratch[b], dscratch[b]);
         };
         std::future<bool> next = std::async(std::launch::async, read_call, 0, 0);
         for (int c = 0; c < ncalls; ++c) {

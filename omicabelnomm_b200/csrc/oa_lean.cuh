@@ -520,7 +520,89 @@ struct SchurArgs {
     double* sfinv;           // [mb][r*r] or null
     float* zA;               // [Z][mb][l][r]
     float* zD;               // [Z][mb][r][r]
+    // the reference's r >= 2 downdate (quirk mode, raw uncentred columns), or null:
+    float* qdel;             // [G][mb][l][r] the quirk's change of Q_obs'X
+    double* qK;              // [G][mb][r][r] Gram matrix term of the quirk's RSS
 };
+
+// The system of (pattern g, SNP i) as the reference's r >= 2 downdate builds
+// it (correct_missings_S, src/Algorithm.cpp:1370-1399, read through sposv's
+// upper triangle; Sbr_corr filled only for j < min(l, r), :1300): every SNP
+// column's covariate downdate Str_corr is subtracted from the first SNP
+// column only, and with r > l the SNP-block downdates of rows a >= l are
+// missing.  In the orthonormal covariate basis (XL = Q R, raw uncentred SNP
+// columns, Str_corr = R' A_g with A_g = (Q o m_g)'X) the quirk changes the
+// covariate block ao = Q_obs'X to ao + dl with
+//     dl[:, 0] = -sum_{b >= 1} A_g[:, b],   dl[:, b] = A_g[:, b] (b >= 1),
+// and the SNP block Dobs = X_obs'X_obs by +D_g[a][b] for min(a, b) >= l.
+// The quirk's solution is the Frisch-Waugh-Lovell one of that system:
+//     beta_x = Sq^-1 (z - dl' b0_j),  Sq = Dobs + dD - (ao + dl)' W_g (ao + dl),
+// and the reference's explicit RSS of that beta over the observed rows is
+//     RSS = RSS0_j - 2 beta_x' z + beta_x' (Schur_g + dl' W_g dl) beta_x
+// (the cross terms vanish because Q_obs' y~ = 0 and Q_obs'Q_obs = W_g^-1).
+// Stored per (g, i): Sq^-1 (sinv), dl (qdel), Schur_g + dl' W_g dl (qK), and
+// ao + dl (aobs: the covariate fit and the rows with y == 0 use it).
+template <int R>
+__device__ __noinline__ void schur_quirk(const SchurArgs& S, int i, int g, size_t gi, const double* ao,
+                                         const double* Dm, const double* dso, bool full_ok) {
+    const int l = S.l;
+    const double* Wg = S.W + (size_t)g * l * l;
+    double dl[OA_MAX_L * R], aq[OA_MAX_L * R];
+    for (int qq = 0; qq < l; ++qq) {
+        double ag[R];
+#pragma unroll
+        for (int a = 0; a < R; ++a) ag[a] = (double)S.C2[(size_t)(l + g * l + qq) * S.ldc + i * R + a];
+        double rest = 0.0;
+#pragma unroll
+        for (int b = 1; b < R; ++b) rest += ag[b];
+        dl[qq * R] = -rest;
+#pragma unroll
+        for (int b = 1; b < R; ++b) dl[qq * R + b] = ag[b];
+#pragma unroll
+        for (int a = 0; a < R; ++a) aq[qq * R + a] = ao[qq * R + a] + dl[qq * R + a];
+    }
+    // X'W X for the three column sets this needs: (ao, ao), (aq, aq), (dl, dl)
+    auto quad = [&](const double* u, double* out) {
+#pragma unroll
+        for (int a = 0; a < R * R; ++a) out[a] = 0.0;
+        for (int qq = 0; qq < l; ++qq) {
+            double wu[R];
+#pragma unroll
+            for (int b = 0; b < R; ++b) wu[b] = 0.0;
+            for (int v = 0; v < l; ++v) {
+                const double w = Wg[qq * l + v];
+#pragma unroll
+                for (int b = 0; b < R; ++b) wu[b] += w * u[v * R + b];
+            }
+#pragma unroll
+            for (int a = 0; a < R; ++a)
+#pragma unroll
+                for (int b = 0; b < R; ++b) out[a * R + b] += u[qq * R + a] * wu[b];
+        }
+    };
+    double Dobs[R * R], Sq[R * R], t1[R * R], t2[R * R];
+#pragma unroll
+    for (int u = 0; u < R * R; ++u) Dobs[u] = Dm[u] - (double)S.Dset[gi * R * R + u];
+    quad(aq, t1);
+#pragma unroll
+    for (int a = 0; a < R; ++a)
+#pragma unroll
+        for (int b = 0; b < R; ++b) {
+            const double dD = (a >= l && b >= l) ? (double)S.Dset[gi * R * R + a * R + b] : 0.0;
+            Sq[a * R + b] = Dobs[a * R + b] + dD - t1[a * R + b];
+        }
+    quad(ao, t1);
+    quad(dl, t2);
+#pragma unroll
+    for (int u = 0; u < R * R; ++u) S.qK[gi * R * R + u] = Dobs[u] - t1[u] + t2[u];
+    const bool ok = full_ok && !S.pat_bad[g] && schur_inverse<R>(Sq, dso);
+    S.sing[gi] = ok ? 0 : 1;
+#pragma unroll
+    for (int u = 0; u < R * R; ++u) S.sinv[gi * R * R + u] = ok ? Sq[u] : 0.0;
+    for (int u = 0; u < l * R; ++u) S.qdel[gi * l * R + u] = (float)dl[u];
+    if (S.aobs)
+        for (int u = 0; u < l * R; ++u) S.aobs[gi * l * R + u] = (float)aq[u];
+}
 
 // All (SNP, pattern) systems of a SNP block in one persistent launch: a
 // thread per (SNP, slot) work item, grid-stride over the items.  Slot 0 is
@@ -546,7 +628,10 @@ __device__ __forceinline__ void schur_item(const SchurArgs& S, int i, int slot) 
             for (int qq = 0; qq < l; ++qq) v -= a_full[qq * R + a] * a_full[qq * R + b];
             Sf[a * R + b] = v;
         }
-    const bool full_ok = spd_inverse<R>(Sf, R, 1e-9);
+    double dss[R];
+#pragma unroll
+    for (int a = 0; a < R; ++a) dss[a] = Dm[a * R + a];
+    const bool full_ok = schur_inverse<R>(Sf, dss);
     if (slot == 0) {
 #pragma unroll
         for (int a = 0; a < R; ++a) S.varx[(size_t)i * R + a] = full_ok ? (float)Sf[a * R + a] : 0.f;
@@ -578,6 +663,9 @@ __device__ __forceinline__ void schur_item(const SchurArgs& S, int i, int slot) 
     double Sg[R * R];
 #pragma unroll
     for (int u = 0; u < R * R; ++u) Sg[u] = Dm[u] - (double)S.Dset[gi * R * R + u];
+    double dso[R];
+#pragma unroll
+    for (int a = 0; a < R; ++a) dso[a] = Sg[a * R + a];
     const double* Wg = S.W + (size_t)g * l * l;
     for (int qq = 0; qq < l; ++qq) {
         double wa[R];
@@ -593,7 +681,11 @@ __device__ __forceinline__ void schur_item(const SchurArgs& S, int i, int slot) 
 #pragma unroll
             for (int b = 0; b < R; ++b) Sg[a * R + b] -= ao[qq * R + a] * wa[b];
     }
-    const bool ok = full_ok && !S.pat_bad[g] && spd_inverse<R>(Sg, R, 1e-9);
+    if (S.qK) {
+        schur_quirk<R>(S, i, g, gi, ao, Dm, dso, full_ok);
+        return;
+    }
+    const bool ok = full_ok && !S.pat_bad[g] && schur_inverse<R>(Sg, dso);
     S.sing[gi] = ok ? 0 : 1;
 #pragma unroll
     for (int u = 0; u < R * R; ++u) S.sinv[gi * R * R + u] = ok ? Sg[u] : 0.0;

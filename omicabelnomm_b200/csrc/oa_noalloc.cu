@@ -1,26 +1,26 @@
 // oa_scan_dense_noalloc: the plain-FP32 scan of one SNP block for callers
 // that cannot allocate GPU memory.
 //
-// Some callers cannot call cudaMalloc: code running while a CUDA graph is
-// being captured on the caller's stream, plug-ins inside host frameworks
-// that own the device memory pool (and forbid raw allocations), and
-// processes under a hard device-memory cap that was reserved up front.
-// This entry point gives them the engine's plain-FP32 block scan (the SIMT
-// GEMM with fused statistics, plus the small kernels that prepare its
-// tables) with every intermediate buffer carved from one file-scope
+// Some callers cannot call cudaMalloc: plug-ins inside host frameworks that
+// own the device memory pool (and forbid raw allocations), and processes
+// under a hard device-memory cap whose memory was reserved up front.  This
+// entry point gives them the engine's plain-FP32 block scan (the SIMT GEMM
+// with fused statistics, plus the small kernels that prepare its tables)
+// with every intermediate buffer carved from one file-scope
 // `static __device__` array of OA_NOALLOC_SCRATCH_BYTES.  It calls no
-// cudaMalloc / cudaFree and no allocating library routine, and allocates
-// no host heap memory either.
+// cudaMalloc / cudaFree and no allocating library routine, and allocates no
+// host heap memory either.
 //
 // Differences from the block engine, all to avoid allocation: the
-// covariates are orthonormalised on the device (Cholesky QR, twice) instead
-// of a host Householder QR; every trait is its own missingness pattern (no
-// host-side grouping; the math is identical); results are dense arrays.
-// The scratch array is shared by every call in the process and keeps the
-// last call's contents; calls that overlap on the GPU (other streams or
-// host threads) race on it.  The first call on a device looks up the
-// array's device address (cudaGetSymbolAddress) and must therefore come
-// before any stream capture.
+// covariates are orthonormalised on the device (shifted CholeskyQR3) instead
+// of a host Householder QR, with the same rank rule (singular values of R
+// below 1e-6); every trait is its own missingness pattern (no host-side
+// grouping; the math is identical); results are dense arrays.  The call
+// reads two small status words back to the host and synchronises the
+// caller's stream.  The scratch array is shared by every call in the process
+// and keeps the last call's contents; calls that overlap on the GPU (other
+// streams or host threads) race on it.  The first call on a device looks up
+// the array's device address (cudaGetSymbolAddress).
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
@@ -72,29 +72,38 @@ __global__ void __launch_bounds__(256) k_na_gram(const T* __restrict__ X, int n,
     }
 }
 
-// Q = X R^-1 with R = chol(G) upper triangular: one Cholesky-QR pass.
-// Writes Q (FP64, column-major) and, if Qr is given, its FP32 row-major
-// copy padded to LP columns.  flag[0] = 1 if G is not positive definite or
-// R has a diagonal below 1e-6 (linearly dependent covariates).
+// Q = X R^-1 with R = chol(G + s I) upper triangular: one Cholesky-QR pass.
+// shift_u > 0 makes it the shifted first pass of shifted CholeskyQR3
+// (Fukaya, Kannan, Nakatsukasa, Yamamoto, Yanagisawa, "Shifted Cholesky QR
+// for computing the QR factorization of ill-conditioned matrices", SIAM J.
+// Sci. Comput. 42(1), 2020): s = shift_u * ||X||_F^2 with
+// shift_u = 11 (n l + l (l + 1)) 2^-53, which keeps the factorisation from
+// breaking down for condition numbers up to about 1e15; two unshifted passes
+// follow.  Writes Q (FP64, column-major), R (row-major upper, l x l) and, if
+// Qr is given, Q's FP32 row-major copy padded to LP columns.  flag[0] = 1 if
+// G + s I is not numerically positive definite.
 template <class T>
-__global__ void __launch_bounds__(256) k_na_cholq(const T* __restrict__ X, int n, int l, int LP,
+__global__ void __launch_bounds__(256) k_na_cholq(const T* __restrict__ X, int n, int l, int LP, double shift_u,
                                                  const double* __restrict__ G, double* __restrict__ Q,
-                                                 float* __restrict__ Qr, int* __restrict__ flag) {
+                                                 double* __restrict__ Rout, float* __restrict__ Qr,
+                                                 int* __restrict__ flag) {
     __shared__ double Ri[OA_MAX_L * OA_MAX_L];
     __shared__ int bad;
     if (threadIdx.x == 0) {
         double L[OA_MAX_L * OA_MAX_L];
         bad = 0;
+        double fro2 = 0.0;
+        for (int j = 0; j < l; ++j) fro2 += G[j * l + j];
+        const double shift = shift_u * fro2;
         for (int i = 0; i < l * l; ++i) L[i] = 0.0;
         for (int j = 0; j < l && !bad; ++j) {
-            double s = G[j * l + j];
+            double s = G[j * l + j] + shift;
             for (int q = 0; q < j; ++q) s -= L[j * l + q] * L[j * l + q];
             if (!(s > 0.0)) {
                 bad = 1;
                 break;
             }
             const double d = sqrt(s);
-            if (d < 1e-6) bad = 1;
             L[j * l + j] = d;
             for (int i = j + 1; i < l; ++i) {
                 double u = G[i * l + j];
@@ -104,7 +113,9 @@ __global__ void __launch_bounds__(256) k_na_cholq(const T* __restrict__ X, int n
         }
         // R = L' (upper); R^-1 by back substitution
         for (int i = 0; i < l * l; ++i) Ri[i] = 0.0;
-        if (!bad)
+        if (!bad) {
+            for (int i = 0; i < l; ++i)
+                for (int j = 0; j < l; ++j) Rout[i * l + j] = j >= i ? L[j * l + i] : 0.0;
             for (int i = l - 1; i >= 0; --i) {
                 Ri[i * l + i] = 1.0 / L[i * l + i];
                 for (int j = i + 1; j < l; ++j) {
@@ -113,6 +124,7 @@ __global__ void __launch_bounds__(256) k_na_cholq(const T* __restrict__ X, int n
                     Ri[i * l + j] = -s / L[i * l + i];
                 }
             }
+        }
         if (bad) *flag = 1;
     }
     __syncthreads();
@@ -128,6 +140,58 @@ __global__ void __launch_bounds__(256) k_na_cholq(const T* __restrict__ X, int n
         }
         if (Qr)
             for (int q = l; q < LP; ++q) Qr[(size_t)k * LP + q] = 0.f;
+    }
+}
+
+// Rank check of the covariates, the block engine's rule: XL = Q R3 R2 R1
+// with Q orthonormal, so the singular values of XL are those of
+// R = R3 R2 R1; any below 1e-6 sets flag[0] (src/Algorithm.cpp:508-522 takes
+// them from sgesvd of XL).  One-sided Jacobi on R, FP64, one thread; skipped
+// when an earlier pass has already flagged the matrix.
+__global__ void k_na_rank(const double* __restrict__ R1, const double* __restrict__ R2, const double* __restrict__ R3,
+                          int l, const int* __restrict__ broke, int* __restrict__ flag) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    if (broke[0] || broke[1] || broke[2]) return;
+    double T[OA_MAX_L * OA_MAX_L], A[OA_MAX_L * OA_MAX_L];
+    for (int i = 0; i < l; ++i)   // T = R2 R1
+        for (int j = 0; j < l; ++j) {
+            double s = 0.0;
+            for (int k = 0; k < l; ++k) s += R2[i * l + k] * R1[k * l + j];
+            T[i * l + j] = s;
+        }
+    for (int i = 0; i < l; ++i)   // A = R3 T
+        for (int j = 0; j < l; ++j) {
+            double s = 0.0;
+            for (int k = 0; k < l; ++k) s += R3[i * l + k] * T[k * l + j];
+            A[i * l + j] = s;
+        }
+    for (int sweep = 0; sweep < 60; ++sweep) {
+        double off = 0.0;
+        for (int p = 0; p < l; ++p)
+            for (int q = p + 1; q < l; ++q) {
+                double a = 0.0, b = 0.0, c = 0.0;
+                for (int i = 0; i < l; ++i) {
+                    a += A[i * l + p] * A[i * l + p];
+                    b += A[i * l + q] * A[i * l + q];
+                    c += A[i * l + p] * A[i * l + q];
+                }
+                if (fabs(c) <= 1e-300) continue;
+                off = fmax(off, fabs(c) / sqrt(a * b));
+                const double zeta = (b - a) / (2.0 * c);
+                const double tn = (zeta >= 0.0 ? 1.0 : -1.0) / (fabs(zeta) + sqrt(1.0 + zeta * zeta));
+                const double cs = 1.0 / sqrt(1.0 + tn * tn), sn = cs * tn;
+                for (int i = 0; i < l; ++i) {
+                    const double x = A[i * l + p], y = A[i * l + q];
+                    A[i * l + p] = cs * x - sn * y;
+                    A[i * l + q] = sn * x + cs * y;
+                }
+            }
+        if (off < 1e-15) break;
+    }
+    for (int p = 0; p < l; ++p) {
+        double a = 0.0;
+        for (int i = 0; i < l; ++i) a += A[i * l + p] * A[i * l + p];
+        if (!(sqrt(a) >= 1e-6)) *flag = 1;
     }
 }
 
@@ -210,7 +274,11 @@ extern "C" oa_status oa_scan_dense_noalloc(const float* xl, const float* y, cons
                                            float* r2, void* stream) {
     using namespace oa;
     using namespace oa::na;
-    cudaGetLastError();   // an error left by an earlier, already-handled call is not ours
+    // an error still pending from the caller's own earlier work is reported, not consumed
+    const cudaError_t pending = cudaPeekAtLastError();
+    if (pending != cudaSuccess)
+        return fail(OA_ERR_CUDA, "a CUDA error from earlier work is pending on this thread (left in place): %s",
+                    cudaGetErrorString(pending));
     if (!xl || !y || !xr || !beta || !se || !tstat || !r2) return fail(OA_ERR_ARG, "null argument");
     if (l < 1 || l > OA_MAX_L || !(r == 1 || r == 2 || r == 4) || n <= l + r || t < 1 || mb < 1 || t > 2048)
         return fail(OA_ERR_ARG, "invalid sizes n=%d l=%d r=%d t=%d mb=%d (r in {1,2,4}, t <= 2048)", n, l, r, t,
@@ -225,8 +293,9 @@ extern "C" oa_status oa_scan_dense_noalloc(const float* xl, const float* y, cons
     // fixed part of the layout (sizes known before the data is looked at)
     Carve cv{reinterpret_cast<unsigned char*>(sp)};
     unsigned long long* counters = cv.take<unsigned long long>(4);
-    int* info = cv.take<int>(4);
+    int* info = cv.take<int>(8);   // [0] Z, [1] set rows, [2..4] pass breakdown, [5] rank deficient
     double* G = cv.take<double>((size_t)OA_MAX_L * OA_MAX_L);
+    double* Rf = cv.take<double>((size_t)3 * OA_MAX_L * OA_MAX_L);   // R of each CholeskyQR pass
     double* Q1 = cv.take<double>((size_t)n * l);
     double* Q64 = cv.take<double>((size_t)n * l);
     float* Qr = cv.take<float>((size_t)n * LP);
@@ -264,24 +333,34 @@ extern "C" oa_status oa_scan_dense_noalloc(const float* xl, const float* y, cons
 
     // everything that must start at zero
     NA_CU(cudaMemsetAsync(counters, 0, 4 * sizeof(unsigned long long), st));
-    NA_CU(cudaMemsetAsync(info, 0, 4 * sizeof(int), st));
+    NA_CU(cudaMemsetAsync(info, 0, 8 * sizeof(int), st));
     NA_CU(cudaMemsetAsync(has_nan, 0, sizeof(int), st));
 
-    // covariates: two Cholesky-QR passes give an orthonormal basis in FP64
+    // covariates: shifted CholeskyQR3 gives an orthonormal basis in FP64 (Q1 -> Q64 -> Q1), then the
+    // block engine's rank rule on the singular values of R
+    const double shift_u = 11.0 * ((double)n * l + (double)l * (l + 1)) * 0x1p-53;
+    const int LL = OA_MAX_L * OA_MAX_L;
     k_na_gram<float><<<dim3(l, l), 256, 0, st>>>(xl, n, l, G);
-    k_na_cholq<float><<<1, 256, 0, st>>>(xl, n, l, LP, G, Q1, nullptr, info + 2);
+    k_na_cholq<float><<<1, 256, 0, st>>>(xl, n, l, LP, shift_u, G, Q1, Rf, nullptr, info + 2);
     k_na_gram<double><<<dim3(l, l), 256, 0, st>>>(Q1, n, l, G);
-    k_na_cholq<double><<<1, 256, 0, st>>>(Q1, n, l, LP, G, Q64, Qr, info + 3);
+    k_na_cholq<double><<<1, 256, 0, st>>>(Q1, n, l, LP, 0.0, G, Q64, Rf + LL, nullptr, info + 3);
+    k_na_gram<double><<<dim3(l, l), 256, 0, st>>>(Q64, n, l, G);
+    k_na_cholq<double><<<1, 256, 0, st>>>(Q64, n, l, LP, 0.0, G, Q1, Rf + 2 * LL, Qr, info + 4);
+    k_na_rank<<<1, 1, 0, st>>>(Rf, Rf + LL, Rf + 2 * LL, l, info + 2, info + 5);
+    Q64 = Q1;
     // traits: missing counts, sums, Q'y; one row set per trait
     TraitStatsOut tso{tsums, tcounts, thash};
     k_trait_stats<<<t, OA_NTHREADS, 0, st>>>(y, (size_t)n, n, l, Q64, tso);
     k_na_sets<<<1, 1, 0, st>>>(tcounts, t, pat, zset, tperm, set_off, set_rep, set_kind, set_slot, info);
     NA_CU(cudaGetLastError());
-    int hinfo[4] = {0, 0, 0, 0};
+    int hinfo[8] = {0, 0, 0, 0, 0, 0, 0, 0};
     NA_CU(cudaMemcpyAsync(hinfo, info, sizeof hinfo, cudaMemcpyDeviceToHost, st));
     NA_CU(cudaStreamSynchronize(st));
-    if (hinfo[2] || hinfo[3])
-        return fail(OA_ERR_COLLINEAR, "the covariate matrix contains linearly dependent columns");
+    if (hinfo[2] || hinfo[3] || hinfo[4])
+        return fail(OA_ERR_COLLINEAR, "the covariate matrix contains linearly dependent columns (its QR broke down)");
+    if (hinfo[5])
+        return fail(OA_ERR_COLLINEAR,
+                    "the covariate matrix contains linearly dependent columns (singular value below 1e-6)");
     const int Z = hinfo[0], nrows = hinfo[1], nsets = t + Z;
     int* set_rows = cv.take<int>((size_t)(nrows > 0 ? nrows : 1));
     float* qrows = cv.take<float>((size_t)(nrows > 0 ? nrows : 1) * LP);

@@ -314,7 +314,10 @@ k_snp_stats(StatsArgs A) {
                     for (int qq = 0; qq < l; ++qq) v -= f[R * R + qq * R + a] * f[R * R + qq * R + bb];
                     S[a * R + bb] = v;
                 }
-            const bool ok = spd_inverse<R>(S, R, 1e-9);
+            double dss[R];
+#pragma unroll
+            for (int a = 0; a < R; ++a) dss[a] = f[a * R + a];
+            const bool ok = schur_inverse<R>(S, dss);
             fsing[s] = ok ? 0 : 1;
 #pragma unroll
             for (int a = 0; a < R; ++a) A.varx[(size_t)i * R + a] = ok ? (float)S[a * R + a] : 0.f;
@@ -381,6 +384,9 @@ k_snp_stats(StatsArgs A) {
                 for (int a = 0; a < R; ++a)
 #pragma unroll
                     for (int bb = 0; bb < R; ++bb) S[a * R + bb] = f[a * R + bb] - (double)d[a * R + bb];
+                double dso[R];
+#pragma unroll
+                for (int a = 0; a < R; ++a) dso[a] = S[a * R + a];
                 for (int qq = 0; qq < l; ++qq) {
                     double wa[R];
 #pragma unroll
@@ -395,7 +401,7 @@ k_snp_stats(StatsArgs A) {
 #pragma unroll
                         for (int bb = 0; bb < R; ++bb) S[a * R + bb] -= ao[qq * R + a] * wa[bb];
                 }
-                const bool ok = !fsing[s] && !A.pat_bad[g2] && spd_inverse<R>(S, R, 1e-9);
+                const bool ok = !fsing[s] && !A.pat_bad[g2] && schur_inverse<R>(S, dso);
                 const size_t gi = (size_t)g2 * A.mb + i;
                 A.sing[gi] = ok ? 0 : 1;
 #pragma unroll

@@ -24,6 +24,8 @@ OA_OK = 0
 STATUS = {0: "OA_OK", 1: "OA_ERR_ARG", 2: "OA_ERR_CUDA", 3: "OA_ERR_COLLINEAR", 4: "OA_ERR_IO",
           5: "OA_ERR_STATE", 6: "OA_ERR_NOMEM", 7: "OA_ERR_UNSUPPORTED", 8: "OA_ERR_NUMERIC"}
 PLAIN, MIXED = 0, 1
+# per-test status bits of Engine.dense_flags (OA_TEST_* in include/omicabel_b200.h)
+TEST_SINGULAR, TEST_RSS, TEST_R2, TEST_STORED = 1, 2, 4, 8
 
 
 class OAError(RuntimeError):
@@ -95,6 +97,7 @@ def lib() -> C.CDLL:
         "oa_run_snps_device": ([P, P, C.c_int32, C.c_int32, C.POINTER(Rows)], C.c_int),
         "oa_dense_last": ([P, fp, fp, fp, fp], C.c_int),
         "oa_enable_dense": ([P, C.c_int32], C.c_int),
+        "oa_dense_flags": ([P, C.POINTER(C.c_uint8)], C.c_int),
         "oa_kernel_launches": ([P], C.c_int64),
         "oa_last_kernel_ms": ([P, C.POINTER(C.c_char_p)], C.c_float),
         "oa_last_stats_ms": ([P], C.c_float),
@@ -167,12 +170,12 @@ class Engine:
     def __init__(self, n: int, l: int, r: int, max_traits: int, max_snps: int, *, precision: int = PLAIN,
                  device: int = 0, disp_cov: bool = False, store_all: bool = False,
                  min_r2_store: float = 1e-6, min_t_store: Optional[float] = None, min_p_disp: float = 0.05,
-                 real_n: Optional[int] = None):
+                 real_n: Optional[int] = None, quirk_r2: bool = False):
         L = lib()
         if min_t_store is None:
             min_t_store = float(L.oa_t_threshold(C.c_float(0.1)))
-        self.cfg = Config(n, l, r, max_traits, max_snps, precision, device, int(disp_cov), int(store_all), 0,
-                          min_r2_store, min_t_store, min_p_disp, real_n or n)
+        self.cfg = Config(n, l, r, max_traits, max_snps, precision, device, int(disp_cov), int(store_all),
+                          int(quirk_r2), min_r2_store, min_t_store, min_p_disp, real_n or n)
         self.n, self.l, self.r, self.p = n, l, r, l + r
         h = C.c_void_p()
         _check(L.oa_engine_create(C.byref(self.cfg), C.byref(h)))
@@ -258,6 +261,13 @@ class Engine:
         r2 = np.empty((t, mb), np.float32)
         _check(lib().oa_dense_last(self.h, _fptr(b), _fptr(se), _fptr(tt), _fptr(r2)))
         return b, se, tt, r2
+
+    def dense_flags(self, mb: int) -> np.ndarray:
+        """Per-test status bits (t, mb) of the last SNP block: TEST_SINGULAR, TEST_RSS, TEST_R2,
+        TEST_STORED (0 = evaluated, nothing stored); needs enable_dense."""
+        f = np.empty((self.t, mb), np.uint8)
+        _check(lib().oa_dense_flags(self.h, f.ctypes.data_as(C.POINTER(C.c_uint8))))
+        return f
 
     def set_tuning(self, **fields):
         """oa_set_tuning: chunk_snps, gemm_variant, gemm_raster, stats_path, lean_spb (0 = automatic)."""

@@ -358,6 +358,29 @@ def _pair_products(XRc: np.ndarray, r: int):
     return X[:, :, None, :] * X[:, None, :, :]
 
 
+def _masked_cross(M: np.ndarray, A: np.ndarray, B: np.ndarray) -> np.ndarray:
+    """out[t, a, b] = sum_k M[t, k] A[a, k] B[b, k]: per-trait sums over masked rows
+    (the Stl_corr downdates, src/Algorithm.cpp:1324-1362), as one matrix product."""
+    P = (A[:, None, :] * B[None, :, :]).reshape(-1, A.shape[1])
+    return (M @ P.T).reshape(M.shape[0], A.shape[0], B.shape[0])
+
+
+def _masked_snp_cross(M: np.ndarray, XL: np.ndarray, Xs: np.ndarray) -> np.ndarray:
+    """out[t, i, a, b] = sum_k M[t, k] XL[a, k] Xs[i, b, k] (the Str_corr downdates,
+    src/Algorithm.cpp:1260-1315), as one matrix product."""
+    mc, r, n = Xs.shape
+    l = XL.shape[0]
+    P = (XL[None, :, None, :] * Xs[:, None, :, :]).reshape(mc * l * r, n)
+    return (M @ P.T).reshape(M.shape[0], mc, l, r)
+
+
+def _masked_snp_gram(M: np.ndarray, Xs: np.ndarray) -> np.ndarray:
+    """out[t, i, a, b] = sum_k M[t, k] Xs[i, a, k] Xs[i, b, k] (the Sbr_corr downdates)."""
+    mc, r, n = Xs.shape
+    P = (Xs[:, :, None, :] * Xs[:, None, :, :]).reshape(mc * r * r, n)
+    return (M @ P.T).reshape(M.shape[0], mc, r, r)
+
+
 def solve(inp: Inputs, s: Settings, snp_chunk: int = 2048, keep_dense: bool = False) -> Results:
     r = inp.r or s.r
     XL = inp.XL.astype(np.float64)
@@ -391,8 +414,8 @@ def solve(inp: Inputs, s: Settings, snp_chunk: int = 2048, keep_dense: bool = Fa
 
     Stl = XL @ XL.T
     XLY = XL @ Y.T                                 # (l, t)
-    Stl_corr = np.einsum("tk,ak,bk->tab", Mmask.astype(np.float64), XL, XL)  # (t, l, l)
-    Stl_zc = np.einsum("tk,ak,bk->tab", Zmask.astype(np.float64), XL, XL)
+    Stl_corr = _masked_cross(Mmask.astype(np.float64), XL, XL)   # (t, l, l)
+    Stl_zc = _masked_cross(Zmask.astype(np.float64), XL, XL)
 
     rec_trait, rec_snp, rec_h = [], [], []
     rec_B, rec_SE, rec_T, rec_R2 = [], [], [], []
@@ -430,8 +453,8 @@ def solve(inp: Inputs, s: Settings, snp_chunk: int = 2048, keep_dense: bool = Fa
 
         # downdates per trait (src/Algorithm.cpp:1260-1362)
         Mf = Mmask.astype(np.float64)
-        Str_c = np.einsum("tk,ak,ibk->tiab", Mf, XL, Xs)            # (t, mc, l, r)
-        Sbr_c = np.einsum("tk,iak,ibk->tiab", Mf, Xs, Xs)           # (t, mc, r, r)
+        Str_c = _masked_snp_cross(Mf, XL, Xs)                       # (t, mc, l, r)
+        Sbr_c = _masked_snp_gram(Mf, Xs)                            # (t, mc, r, r)
         Sj = np.broadcast_to(S, (t, mc, p, p)).copy()
         Sj[:, :, :l, :l] -= Stl_corr[:, None]
         if s.quirk_r2 and r >= 2:
@@ -451,7 +474,7 @@ def solve(inp: Inputs, s: Settings, snp_chunk: int = 2048, keep_dense: bool = Fa
             Sj[:, :, l:, l:] -= Sbr_c
 
         # right-hand sides [XL'y; XR_i'y] (src/Algorithm.cpp:583-585, 705-707, 734-736)
-        XRY = np.einsum("ibk,tk->tib", Xs, Y)                       # (t, mc, r)
+        XRY = (Y @ Xs.reshape(mc * r, n).T).reshape(t, mc, r)       # (t, mc, r)
         rhs = np.concatenate([np.broadcast_to(XLY.T[:, None, :], (t, mc, l)), XRY], axis=2)
 
         # b = S \ rhs (src/Algorithm.cpp:767-768)
@@ -465,12 +488,12 @@ def solve(inp: Inputs, s: Settings, snp_chunk: int = 2048, keep_dense: bool = Fa
         G = np.broadcast_to(S, (t, mc, p, p)).copy()
         Zf = Zmask.astype(np.float64)
         G[:, :, :l, :l] -= Stl_zc[:, None]
-        Strz = np.einsum("tk,ak,ibk->tiab", Zf, XL, Xs)
+        Strz = _masked_snp_cross(Zf, XL, Xs)
         G[:, :, :l, l:] -= Strz
         G[:, :, l:, :l] -= np.transpose(Strz, (0, 1, 3, 2))
-        G[:, :, l:, l:] -= np.einsum("tk,iak,ibk->tiab", Zf, Xs, Xs)
-        rss = (yy[:, None] - 2.0 * np.einsum("tip,tip->ti", beta, rhs)
-               + np.einsum("tip,tipq,tiq->ti", beta, G, beta))
+        G[:, :, l:, l:] -= _masked_snp_gram(Zf, Xs)
+        rss = (yy[:, None] - 2.0 * (beta * rhs).sum(axis=2)
+               + (beta[..., None, :] @ G @ beta[..., :, None])[..., 0, 0])
 
         # statistics (src/Algorithm.cpp:1034-1134)
         ncorr = (n - miss - p).astype(np.float64)                   # n_corrected

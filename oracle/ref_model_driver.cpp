@@ -6,7 +6,7 @@
 // src/main.cpp:341-358), while its reader implements the models
 // (src/AIOwrapper.cpp:257-340, 1213-1275).
 //
-//   ref_model_driver XL XR Y OUT NGPRED MODEL [FACTORS|-] [-b] [-f] [-i] [-v INTER | -w INTER]
+//   ref_model_driver XL XR Y OUT NGPRED MODEL [FACTORS|-] [-b] [-f] [-i] [-v INTER | -w INTER] [-t THREADS]
 //
 // MODEL is the reference's Settings::model: 0 additive, 1 dominant,
 // 2 recessive, 3 custom linear, 4 custom additive, -1 none.  -v sets the
@@ -42,6 +42,7 @@ int main(int argc, char** argv) {
         if (!std::strcmp(argv[a], "-b")) params.storeBin = true;
         else if (!std::strcmp(argv[a], "-f")) params.storePInd = true;
         else if (!std::strcmp(argv[a], "-i")) params.disp_cov = true;
+        else if (!std::strcmp(argv[a], "-t") && a + 1 < argc) params.threads = std::atoi(argv[++a]);
         else if (!std::strcmp(argv[a], "-v") && a + 1 < argc) {
             params.fname_interactions = argv[++a];
             params.use_interactions = true;

@@ -158,6 +158,24 @@ def flag_tag(flags) -> str:
     return t or "default"
 
 
+def ref_command(flags, pre: str, extra: dict, out: str, threads: int = 0):
+    """Command line of the reference run with these flags (the CLI, or the in-process model
+    driver for the dosage models and interactions); threads > 0 adds the thread count."""
+    args = [f.format(**extra) for f in flags]
+    model = [f for f in args if f in MODEL_FLAGS]
+    inter_flag = [f for f in args if f in ("-v", "-w")]
+    thr = ["-t", str(threads)] if threads > 0 else []
+    if model or inter_flag:
+        ngpred = args[args.index("-n") + 1] if "-n" in args else "1"
+        rest = [f for f in args if f in ("-b", "-f", "-i")]
+        fac = args[args.index(model[0]) + 1] if model and model[0] in ("-z", "-y") else "-"
+        code = str(MODEL_FLAGS[model[0]]) if model else "-1"
+        if inter_flag:
+            rest += [inter_flag[0], args[args.index(inter_flag[0]) + 1]]
+        return [REF_MODEL, pre + "XL", pre + "XR", pre + "Y", out, ngpred, code, fac] + rest + thr
+    return [REF_BIN, "-c", pre + "XL", "-g", pre + "XR", "-p", pre + "Y", "-o", out] + args + thr
+
+
 def main(only=None):
     """Run every case, or only the named ones (merged into the existing manifest)."""
     if not os.path.exists(REF_BIN):
@@ -177,20 +195,8 @@ def main(only=None):
             entry = {"workload": over, "post": post, "inputs": input_digests(pre), "runs": {}}
             for flags in flagsets:
                 tag = flag_tag(flags)
-                args = [f.format(**extra) for f in flags]
                 out = os.path.join(tmp, f"{case}_{tag}")
-                model = [f for f in args if f in MODEL_FLAGS]
-                inter_flag = [f for f in args if f in ("-v", "-w")]
-                if model or inter_flag:
-                    ngpred = args[args.index("-n") + 1] if "-n" in args else "1"
-                    rest = [f for f in args if f in ("-b", "-f", "-i")]
-                    fac = args[args.index(model[0]) + 1] if model and model[0] in ("-z", "-y") else "-"
-                    code = str(MODEL_FLAGS[model[0]]) if model else "-1"
-                    if inter_flag:
-                        rest += [inter_flag[0], args[args.index(inter_flag[0]) + 1]]
-                    cmd = [REF_MODEL, pre + "XL", pre + "XR", pre + "Y", out, ngpred, code, fac] + rest
-                else:
-                    cmd = [REF_BIN, "-c", pre + "XL", "-g", pre + "XR", "-p", pre + "Y", "-o", out] + args
+                cmd = ref_command(flags, pre, extra, out)
                 p = subprocess.run(cmd, capture_output=True, text=True, timeout=600)
                 if p.returncode != 0:
                     raise RuntimeError(f"{case} {flags}: exit {p.returncode}\n{p.stdout[-2000:]}")
