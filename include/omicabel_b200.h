@@ -38,7 +38,7 @@ extern "C" {
 
 #define OA_ABI_VERSION 1
 #define OA_MAX_L 16   /* covariates, intercept included */
-#define OA_MAX_R 4    /* columns per SNP */
+#define OA_MAX_R 8    /* columns per SNP (3, 5, 6 and 7 run as 4 or 8 with zero columns added on the device) */
 
 typedef enum oa_status {
     OA_OK = 0,
@@ -65,7 +65,8 @@ typedef struct oa_engine oa_engine;
 typedef struct oa_config {
     int32_t n;             /* individuals after exclusions (rows) */
     int32_t l;             /* covariates incl. intercept, 1..OA_MAX_L */
-    int32_t r;             /* columns per SNP, 1..OA_MAX_R */
+    int32_t r;             /* columns per SNP, 1..OA_MAX_R (r > 4 needs the SNP's 8 columns in one
+                              SM's shared memory: n up to about 6,000) */
     int32_t max_traits;    /* largest trait block passed to oa_set_traits */
     int32_t max_snps;      /* largest SNP block passed to oa_run_snps* */
     int32_t precision;     /* oa_precision */

@@ -24,8 +24,11 @@ struct TraitP {
 };
 
 // One stored row (a (trait, SNP) test with at least one stored SNP term),
-// the device form of the reference's resultH (src/Definitions.h:271-280).
-struct alignas(16) Rec {
+// the device form of the reference's resultH (src/Definitions.h:271-280),
+// with room for K SNP terms: K = 4 (80 bytes) up to four columns per SNP,
+// K = 8 (128 bytes) for five to eight.
+template <int K>
+struct alignas(16) RecK {
     int32_t trait;      // trait index within the trait block
     int32_t snp;        // SNP index within the SNP block
     float r2;           // R2 (src/Algorithm.cpp:1092)
@@ -33,11 +36,17 @@ struct alignas(16) Rec {
     float sig;          // sqrt(RSS / n_corrected) (src/Algorithm.cpp:1100)
     int32_t tint;       // trait index in the engine's internal (pattern-sorted) order
     float pad[2];
-    float b[OA_MAX_R];
-    float se[OA_MAX_R];
-    float t[OA_MAX_R];
+    float b[K];
+    float se[K];
+    float t[K];
 };
-static_assert(sizeof(Rec) == 80, "Rec layout");
+using Rec = RecK<4>;
+static_assert(sizeof(RecK<4>) == 80 && sizeof(RecK<8>) == 128, "Rec layout");
+// The record of an engine with R columns per SNP.
+template <int R>
+using RecOf = RecK<(R <= 4 ? 4 : 8)>;
+// Rec-sized slots one record of an engine with r columns per SNP takes.
+inline int rec_slots(int r) { return r <= 4 ? 1 : 2; }
 
 // Everything the fused statistics epilogue reads, per trait and per SNP.
 // Per-trait arrays are in the engine's internal trait order (traits sorted
@@ -68,7 +77,7 @@ struct EpiArgs {
     float min_r2, min_t;
     int store_all;
     // outputs
-    Rec* rec;
+    void* rec;                       // RecOf<R> records
     unsigned long long* rec_count;   // record slots handed out (written rows and unused slots of reserved blocks)
     unsigned long long* rec_valid;   // rows written (null: not counted)
     long long cap;

@@ -85,14 +85,14 @@ __device__ __forceinline__ void cov_eval(const CovArgs& C, int i, int j, const f
 // at the record buffer), read on the device after the chunk's GEMM.
 template <int R>
 __global__ void __launch_bounds__(256)
-k_cov_terms(const Rec* __restrict__ rec, const unsigned long long* __restrict__ first_p,
+k_cov_terms(const RecOf<R>* __restrict__ rec, const unsigned long long* __restrict__ first_p,
             const unsigned long long* __restrict__ counters, long long cap, int snp_base, CovArgs C,
             float* __restrict__ cov /* [rec][l][3] */) {
     const long long first = (long long)*first_p;
     const long long last = min((long long)counters[0], cap);
     for (long long idx = first + blockIdx.x * (long long)blockDim.x + threadIdx.x; idx < last;
          idx += (long long)gridDim.x * blockDim.x) {
-        const Rec rc = rec[idx];
+        const RecOf<R> rc = rec[idx];
         if (rc.trait < 0) continue;   // an unused slot of a reserved block
         float b[OA_MAX_L], se[OA_MAX_L], t[OA_MAX_L];
         cov_eval<R>(C, rc.snp - snp_base, rc.tint, rc.b, rc.sig, b, se, t);

@@ -108,25 +108,75 @@ struct DBuf {
 
 int pad_l(int l) { return l <= 4 ? 4 : (l <= 8 ? 8 : 16); }
 
+// Page-locked host buffers shared by every engine of the process, pooled by
+// size: an engine takes the smallest idle buffer that holds what it asks for
+// (at most twice that) and gives its buffers back when it is destroyed.
+// cudaMallocHost is slow while other engines keep the GPU busy and
+// cudaFreeHost waits for the whole device, so a server that creates an
+// engine per request (each with its own individuals and covariates) must not
+// pay either per request.  Idle buffers beyond PINNED_KEEP bytes are freed,
+// largest first.
+constexpr size_t PINNED_KEEP = 16ull << 30;
+struct PinnedPool {
+    std::mutex mu;
+    std::multimap<size_t, void*> idle;
+    size_t idle_bytes = 0;
+    void* take(size_t bytes, size_t* got) {
+        {
+            std::lock_guard<std::mutex> g(mu);
+            auto it = idle.lower_bound(bytes);
+            if (it != idle.end() && it->first <= 2 * bytes + (1u << 20)) {
+                void* p = it->second;
+                *got = it->first;
+                idle_bytes -= it->first;
+                idle.erase(it);
+                return p;
+            }
+        }
+        void* p = nullptr;
+        if (cudaMallocHost(&p, bytes) != cudaSuccess) {
+            cudaGetLastError();
+            return nullptr;
+        }
+        *got = bytes;
+        return p;
+    }
+    void give(void* p, size_t bytes) {
+        if (!p) return;
+        std::lock_guard<std::mutex> g(mu);
+        idle.emplace(bytes, p);
+        idle_bytes += bytes;
+        while (idle_bytes > PINNED_KEEP && !idle.empty()) {
+            auto it = std::prev(idle.end());
+            cudaFreeHost(it->second);
+            idle_bytes -= it->first;
+            idle.erase(it);
+        }
+    }
+};
+PinnedPool& pinned_pool() {
+    static PinnedPool* pool = new PinnedPool();   // never destroyed: engines may outlive static destructors
+    return *pool;
+}
+
 // Grow a pinned host buffer (page-locked so the device-to-host copy runs at
 // full speed), doubling so that growth is rare.  Outgrown buffers go to
-// `retired` and are freed when the engine is destroyed: cudaFreeHost waits
-// for the whole device (every other engine's work).  Allocating pinned
-// memory is itself slow while other engines keep the GPU busy, so serving
-// engines reserve their buffers up front (oa_reserve).
+// `retired` (pointer, bytes) and back to the pool when the engine is
+// destroyed.  Serving engines reserve their buffers up front (oa_reserve).
 template <class T>
-oa_status ensure_pinned(T*& p, size_t& cap, size_t want, std::vector<void*>& retired) {
+oa_status ensure_pinned(T*& p, size_t& cap, size_t want, std::vector<std::pair<void*, size_t>>& retired) {
     if (want <= cap && p) return OA_OK;
-    if (p) retired.push_back(p);
+    if (p) retired.emplace_back(p, cap * sizeof(T));
     p = nullptr;
     const size_t n = std::max<size_t>({want + want / 4, 2 * cap, 1024});
     cap = 0;
-    if (cudaMallocHost(reinterpret_cast<void**>(&p), n * sizeof(T)) != cudaSuccess) {
-        cudaGetLastError();
+    size_t got = 0;
+    p = static_cast<T*>(pinned_pool().take(n * sizeof(T), &got));
+    if (!p) {
         set_err("pinned host allocation of %zu bytes failed", n * sizeof(T));
         return OA_ERR_NOMEM;
     }
-    cap = n;
+    cap = got / sizeof(T);
     return OA_OK;
 }
 
@@ -226,7 +276,9 @@ constexpr int RESULT_PIECES = 8;
 
 struct oa_engine {
     oa_config cfg{};
-    int n = 0, l = 0, r = 0, p = 0, LP = 4, n_pad = 0, sm_count = 148;
+    // r: columns per SNP in the kernels (1, 2, 4 or 8); ru: the caller's (1..8, p = l + ru); columns
+    // [ru, r) are zero padding added on the device
+    int n = 0, l = 0, r = 0, ru = 0, p = 0, LP = 4, n_pad = 0, sm_count = 148;
     cudaStream_t st = nullptr, cp = nullptr;
     cudaEvent_t ev_copied[2]{}, ev_used[2]{}, k0 = nullptr, k1 = nullptr;
     long long launches = 0;
@@ -337,12 +389,13 @@ struct oa_engine {
     size_t h_rec_cap = 0;
     float* h_cov = nullptr;
     size_t h_cov_cap = 0;
-    std::vector<void*> retired_pinned;   // outgrown pinned buffers, freed at destroy
+    std::vector<std::pair<void*, size_t>> retired_pinned;   // outgrown pinned buffers, back to the pool at destroy
     // pinned staging of the small host <-> device transfers (trait grouping,
     // row-set tables, counters): asynchronous copies that need no driver staging
     unsigned char* stage = nullptr;
     size_t stage_cap = 0;
     unsigned long long* h_cnt = nullptr;   // 8 counters read back after each block
+    size_t h_cnt_bytes = 0;
     cudaEvent_t ev_piece[RESULT_PIECES] = {};  // the stored rows' pieces have reached the host
     std::vector<int32_t> o_trait, o_snp, o_nused;
     std::vector<float> o_r2, o_b, o_se, o_t;
@@ -397,13 +450,18 @@ static __global__ void k_gather_rows(const float* __restrict__ in, long long ld,
 struct ModelW {
     float w[OA_MODEL_MAX_COLS];
 };
+// SNP i's columns go to out_r columns of `out`: the model's columns first,
+// zero padding after them (engines whose kernels take 4 or 8 columns per SNP
+// for r = 3, 5, 6, 7).
 static __global__ void k_column_model(const float* __restrict__ in, int n, int in_cols, ModelW W, int combine,
-                                      const float* __restrict__ inter, int n_inter, int keep,
+                                      const float* __restrict__ inter, int n_inter, int keep, int out_r,
                                       float* __restrict__ out) {
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
     const int i = blockIdx.y;
     if (k >= n) return;
     const float* src = in + (size_t)i * in_cols * n + k;
+    float* dst = out + (size_t)i * out_r * n + k;
+    int written;
     if (combine) {   // a zero factor drops its column (the reference does not read it)
         float acc = 0.f;
         bool any = false;
@@ -414,15 +472,18 @@ static __global__ void k_column_model(const float* __restrict__ in, int n, int i
             any = true;
         }
         if (n_inter == 0) {
-            out[(size_t)i * n + k] = acc;
+            dst[0] = acc;
+            written = 1;
         } else {   // [I_1 x, ..., I_k x (, x)] (src/AIOwrapper.cpp:808-840)
-            const int r = n_inter + keep;
-            for (int h = 0; h < n_inter; ++h) out[((size_t)i * r + h) * n + k] = inter[(size_t)h * n + k] * acc;
-            if (keep) out[((size_t)i * r + n_inter) * n + k] = acc;
+            for (int h = 0; h < n_inter; ++h) dst[(size_t)h * n] = inter[(size_t)h * n + k] * acc;
+            if (keep) dst[(size_t)n_inter * n] = acc;
+            written = n_inter + keep;
         }
     } else {
-        for (int c = 0; c < in_cols; ++c) out[((size_t)i * in_cols + c) * n + k] = W.w[c] * src[(size_t)c * n];
+        for (int c = 0; c < in_cols; ++c) dst[(size_t)c * n] = W.w[c] * src[(size_t)c * n];
+        written = in_cols;
     }
+    for (int c = written; c < out_r; ++c) dst[(size_t)c * n] = 0.f;
 }
 
 // The reference's r >= 2 downdate is reproduced (quirk mode; with r = 1 it
@@ -431,7 +492,14 @@ static __global__ void k_column_model(const float* __restrict__ in, int n, int i
 bool quirk_on(const oa_engine* e) { return e->cfg.quirk_r2 && e->r >= 2; }
 
 // Columns per SNP of the caller's SNP blocks.
-int input_cols(const oa_engine* e) { return e->in_cols > 0 ? e->in_cols : e->r; }
+int input_cols(const oa_engine* e) { return e->in_cols > 0 ? e->in_cols : e->ru; }
+
+// The kernels take more columns per SNP than the caller's blocks hold (r = 3, 5, 6, 7): every chunk
+// goes through k_column_model, which adds the zero columns.
+bool padded(const oa_engine* e) { return e->ru != e->r; }
+
+// A chunk passes through k_column_model (a dosage model, interactions or zero padding).
+bool column_pass(const oa_engine* e) { return e->in_cols > 0 || padded(e); }
 
 // Mixed form with the pre-GEMM statistics path: nothing after the column
 // statistics reads the FP32 chunk (the GEMMs read its BF16 split), so a row
@@ -668,7 +736,9 @@ oa_status prepare_tuning(oa_engine* e) {
     e->variant = (e->req.gemm_variant >= 1 && e->req.gemm_variant <= 4) ? e->req.gemm_variant : 4;
     e->raster = e->req.gemm_raster == 2 ? 2 : 1;
     e->lean_spb = e->req.lean_spb > 0 ? std::min(e->req.lean_spb, 8 / e->r) : 0;
-    e->use_pre = quirk_on(e) || e->req.stats_path == 1 || (e->req.stats_path != 2 && e->c2 <= std::max(t, 256));
+    // the row-gather form handles neither the quirk, nor padding columns, nor 8 columns per SNP
+    e->use_pre = quirk_on(e) || padded(e) || e->r > 4 || e->req.stats_path == 1 ||
+                 (e->req.stats_path != 2 && e->c2 <= std::max(t, 256));
     if (e->use_pre && !e->b2_ready) {
         const size_t nb2 = (size_t)e->c2 * e->n_pad;
         OA_CHECK(e->B2.ensure(nb2));
@@ -893,6 +963,7 @@ oa_status stats_pre(oa_engine* e, const float* X, size_t ldx, const int* xrows, 
     S.sfinv = e->cfg.disp_cov ? e->sfinv.p : nullptr;
     S.zA = e->zA.p;
     S.zD = e->zD.p;
+    S.rr = e->ru;
     S.qdel = quirk_on(e) ? e->qdel.p : nullptr;
     S.qK = quirk_on(e) ? e->qK.p : nullptr;
     OA_CU(oa_launch_schur(R, S, e->st));
@@ -903,6 +974,10 @@ oa_status stats_pre(oa_engine* e, const float* X, size_t ldx, const int* xrows, 
 template <int R>
 oa_status stats_dispatch(oa_engine* e, const float* X, size_t ldx, const int* xrows, int mbc) {
     if (e->use_pre) return stats_pre<R>(e, X, ldx, xrows, mbc);
+    if constexpr (R > 4) {
+        set_err("internal: the gather-path statistics kernel takes at most 4 columns per SNP");
+        return OA_ERR_STATE;
+    }
     if (xrows || ldx != (size_t)e->n) {
         set_err("internal: the gather-path statistics kernel reads gathered chunks only");
         return OA_ERR_STATE;
@@ -1038,7 +1113,7 @@ oa_status ensure_cap(oa_engine* e, long long want) {
     e->rec.release();
     e->cov.release();
     e->cap = 0;
-    OA_CHECK(e->rec.ensure((size_t)want));
+    OA_CHECK(e->rec.ensure((size_t)want * rec_slots(e->r)));   // records of RecOf<r>, in Rec units
     if (e->cfg.disp_cov) OA_CHECK(e->cov.ensure((size_t)want * e->l * 3));
     e->cap = want;
     return OA_OK;
@@ -1094,16 +1169,18 @@ oa_status enqueue_block(oa_engine* e, const float* xr, int mb, bool host_input, 
             X = xr + (size_t)c0 * R * e->x_ld;
             ldx = e->x_ld;
             xrows = e->xrows.p;
-        } else if (e->in_cols > 0) {
+        } else if (column_pass(e)) {
             X = xr + (size_t)c0 * IC * e->n;
         } else {
             OA_CHECK(chunk_input<R>(e, xr, c0, mbc, &X));
         }
-        if (e->in_cols > 0) {   // file columns -> model columns
+        if (column_pass(e)) {   // file columns -> model columns (+ zero padding)
             ModelW W;
-            for (int c = 0; c < OA_MODEL_MAX_COLS; ++c) W.w[c] = e->model_w[c];
+            const bool model = e->in_cols > 0;   // else the caller's ru columns as they are
+            for (int c = 0; c < OA_MODEL_MAX_COLS; ++c) W.w[c] = model ? e->model_w[c] : 1.f;
             k_column_model<<<dim3((unsigned)((e->n + 255) / 256), (unsigned)mbc), 256, 0, e->st>>>(
-                X, e->n, e->in_cols, W, e->model_combine, e->inter.p, e->n_inter, e->inter_keep, e->Xmodel.p);
+                X, e->n, IC, W, model ? e->model_combine : 0, e->inter.p, e->n_inter, e->inter_keep, R,
+                e->Xmodel.p);
             ++e->launches;
             OA_CU(cudaGetLastError());
             X = e->Xmodel.p;
@@ -1122,8 +1199,8 @@ oa_status enqueue_block(oa_engine* e, const float* xr, int mb, bool host_input, 
         if (host_input) OA_CU(cudaEventRecord(e->ev_used[c & 1], e->st));
         if (cov) {
             CovArgs C = cov_args(e, mbc);
-            k_cov_terms<R><<<4 * e->sm_count, 256, 0, e->st>>>(e->rec.p, e->marks.p + c, e->counters.p, e->cap, c0, C,
-                                                             e->cov.p);
+            k_cov_terms<R><<<4 * e->sm_count, 256, 0, e->st>>>(reinterpret_cast<const RecOf<R>*>(e->rec.p),
+                                                             e->marks.p + c, e->counters.p, e->cap, c0, C, e->cov.p);
             k_cov_count<R><<<4 * e->sm_count, 256, 0, e->st>>>(e->d_beta.p, e->d_t.p, e->d_r2.p, e->d_sig.p,
                                                              e->dense_ld, c0, mbc, e->t, e->cfg.min_r2_store, C,
                                                              e->counters.p + 2);
@@ -1253,10 +1330,10 @@ oa_status run_snps_impl(oa_engine* e, const float* xr, int32_t mb, bool host_inp
         set_err("SNP block of %d SNPs (engine limit %d)", mb, e->cfg.max_snps);
         return OA_ERR_ARG;
     }
-    if (e->in_cols > 0 && e->model_combine && (e->n_inter > 0 ? e->n_inter + e->inter_keep : 1) != e->r) {
+    if (e->in_cols > 0 && e->model_combine && (e->n_inter > 0 ? e->n_inter + e->inter_keep : 1) != e->ru) {
         set_err("a combined column model gives r = %d columns per SNP%s, the engine has r = %d",
                 e->n_inter > 0 ? e->n_inter + e->inter_keep : 1, e->n_inter > 0 ? " with its interactions" : "",
-                e->r);
+                e->ru);
         return OA_ERR_STATE;
     }
     OA_CHECK(prepare_tuning(e));
@@ -1284,7 +1361,7 @@ oa_status run_snps_impl(oa_engine* e, const float* xr, int32_t mb, bool host_inp
         }
         if (!lean_gathers(e)) OA_CHECK(e->Xstage[0].ensure((size_t)e->chunk * e->r * e->n));
     }
-    if (e->in_cols > 0) OA_CHECK(e->Xmodel.ensure((size_t)e->chunk * e->r * e->n));
+    if (column_pass(e)) OA_CHECK(e->Xmodel.ensure((size_t)e->chunk * e->r * e->n));
     if (host_input) {
         if (!e->cp) OA_CU(cudaStreamCreateWithFlags(&e->cp, cudaStreamNonBlocking));
         for (int b = 0; b < 2; ++b) {
@@ -1310,18 +1387,20 @@ oa_status run_snps_impl(oa_engine* e, const float* xr, int32_t mb, bool host_inp
     const long long NS = (long long)cnt[0];   // slots handed out
     const long long N = (long long)cnt[4];    // rows written
     const int l = e->l, p = e->p;
-    OA_CHECK(ensure_pinned(e->h_rec, e->h_rec_cap, (size_t)N, e->retired_pinned));
+    // the packed fields of N rows (16 + 12 R bytes each) fit in N Rec-sized slots per rec_slots(R)
+    OA_CHECK(ensure_pinned(e->h_rec, e->h_rec_cap, (size_t)N * rec_slots(R), e->retired_pinned));
     if (e->cfg.disp_cov) OA_CHECK(ensure_pinned(e->h_cov, e->h_cov_cap, (size_t)N * l * 3, e->retired_pinned));
     if (N > 0) {
         OA_CHECK(e->keys.ensure(NS));
         OA_CHECK(e->keys2.ensure(NS));
         OA_CHECK(e->perm.ensure(NS));
         OA_CHECK(e->perm2.ensure(NS));
-        OA_CHECK(e->rec2.ensure(N));
+        OA_CHECK(e->rec2.ensure((size_t)N * rec_slots(R)));
         // key bits: enough for t * mb with the all-ones invalid key above every valid one
         int bits = 1;
         while (bits < 64 && (1ull << bits) <= (unsigned long long)e->t * (unsigned long long)mb) ++bits;
-        k_rec_keys<<<(unsigned)((NS + 255) / 256), 256, 0, e->st>>>(e->rec.p, NS, mb, bits, e->keys.p, e->perm.p);
+        k_rec_keys<<<(unsigned)((NS + 255) / 256), 256, 0, e->st>>>(reinterpret_cast<const RecOf<R>*>(e->rec.p), NS,
+                                                                     mb, bits, e->keys.p, e->perm.p);
         ++e->launches;
         size_t tmp = 0;
         OA_CU(cub::DeviceRadixSort::SortPairs(nullptr, tmp, e->keys.p, e->keys2.p, e->perm.p, e->perm2.p, (int)NS, 0,
@@ -1331,7 +1410,8 @@ oa_status run_snps_impl(oa_engine* e, const float* xr, int32_t mb, bool host_inp
                                               0, bits, e->st));
         if (e->cfg.disp_cov) OA_CHECK(e->cov2.ensure((size_t)N * l * 3));
         const RowsSoA dsoa = rows_soa(e->rec2.p, N, R);   // the record buffer holds the packed fields
-        k_rec_gather<R><<<(unsigned)((N + 255) / 256), 256, 0, e->st>>>(e->rec.p, e->perm2.p, N, dsoa,
+        k_rec_gather<R><<<(unsigned)((N + 255) / 256), 256, 0, e->st>>>(reinterpret_cast<const RecOf<R>*>(e->rec.p),
+                                                                        e->perm2.p, N, dsoa,
                                                                         e->cfg.disp_cov ? e->cov.p : nullptr,
                                                                         e->cfg.disp_cov ? e->cov2.p : nullptr, l);
         ++e->launches;
@@ -1367,6 +1447,7 @@ oa_status run_snps_impl(oa_engine* e, const float* xr, int32_t mb, bool host_inp
     e->o_t.resize((size_t)N * p);
     const float minT = e->cfg.min_t_store;
     const bool disp_cov = e->cfg.disp_cov != 0, store_all = e->cfg.store_all != 0;
+    const int ru = e->ru;   // the caller's columns: the padding columns' terms are not reported
     const RowsSoA hs = rows_soa(e->h_rec, N, R);
     auto convert = [&](long long q0, long long q1) {
         for (long long q = q0; q < q1; ++q) {
@@ -1381,7 +1462,7 @@ oa_status run_snps_impl(oa_engine* e, const float* xr, int32_t mb, bool host_inp
             for (int h = 0; h < l; ++h) ob[h] = os[h] = ot[h] = 0.f;
             uint32_t m = 0;
             const uint32_t rm = hs.mask[q];
-            for (int a = 0; a < R; ++a) {
+            for (int a = 0; a < ru; ++a) {
                 ob[l + a] = hs.b[(size_t)q * R + a];
                 os[l + a] = hs.se[(size_t)q * R + a];
                 ot[l + a] = hs.t[(size_t)q * R + a];
@@ -1447,9 +1528,10 @@ oa_status run_snps_any(oa_engine* e, const float* xr, int32_t mb, bool host_inpu
         case 1: return run_snps_impl<1>(e, xr, mb, host_input, results_on_host, out);
         case 2: return run_snps_impl<2>(e, xr, mb, host_input, results_on_host, out);
         case 4: return run_snps_impl<4>(e, xr, mb, host_input, results_on_host, out);
+        case 8: return run_snps_impl<8>(e, xr, mb, host_input, results_on_host, out);
         default:
-            set_err("r = %d is not supported by this build (1, 2 or 4)", e->r);
-            return OA_ERR_UNSUPPORTED;
+            set_err("internal: %d kernel columns per SNP", e->r);
+            return OA_ERR_STATE;
     }
 }
 
@@ -1561,10 +1643,6 @@ oa_status oa_engine_create(const oa_config* cfg, oa_engine** out) {
         set_err("invalid engine configuration (n=%d l=%d r=%d)", cfg->n, cfg->l, cfg->r);
         return OA_ERR_ARG;
     }
-    if (cfg->r == 3) {
-        set_err("r = 3 is not supported by this build (1, 2 or 4)");
-        return OA_ERR_UNSUPPORTED;
-    }
     if (cfg->precision != OA_PLAIN_FP32 && cfg->precision != OA_MIXED_BF16X3) {
         set_err("unknown precision %d", cfg->precision);
         return OA_ERR_ARG;
@@ -1586,12 +1664,27 @@ oa_status oa_engine_create(const oa_config* cfg, oa_engine** out) {
         set_err("device %s (sm_%d%d) is not a Blackwell sm_100 part", prop.name, prop.major, prop.minor);
         return OA_ERR_UNSUPPORTED;
     }
+    {   // bound of the device pipeline and staging waits, per device: 2 s, or OA_WAIT_LIMIT_NS (the
+        // timeout tests shorten it so that the waits run out and the error path is exercised)
+        static std::mutex mu;
+        static unsigned long long cur[64];
+        const char* w = getenv("OA_WAIT_LIMIT_NS");
+        const unsigned long long ns = w ? std::max(1ull, strtoull(w, nullptr, 10)) : 2000000000ull;
+        std::lock_guard<std::mutex> g(mu);
+        unsigned long long& c = cur[cfg->device & 63];
+        if (c != ns && !(c == 0 && ns == 2000000000ull)) {
+            OA_CU(oa_set_wait_limit_tc(ns));
+            OA_CU(oa_set_wait_limit_stats(ns));
+        }
+        c = ns;
+    }
     oa_engine* e = new oa_engine();
     e->cfg = *cfg;
     e->sm_count = prop.multiProcessorCount;
     e->n = cfg->n;
     e->l = cfg->l;
-    e->r = cfg->r;
+    e->ru = cfg->r;
+    e->r = cfg->r <= 1 ? 1 : (cfg->r <= 2 ? 2 : (cfg->r <= 4 ? 4 : 8));
     e->p = cfg->l + cfg->r;
     e->LP = pad_l(cfg->l);
     e->n_pad = (cfg->n + 63) & ~63;
@@ -1602,7 +1695,7 @@ oa_status oa_engine_create(const oa_config* cfg, oa_engine** out) {
     if (const char* v = getenv("OA_LEAN_SPB")) e->req.lean_spb = std::max(0, atoi(v));
     if (const char* v = getenv("OA_LEAN_NBUF")) e->lean_nbuf = atoi(v) == 1 ? 1 : (atoi(v) == 2 ? 2 : 0);
     if (const char* v = getenv("OA_LEAN_XI")) e->lean_xi = atoi(v) == 0 ? 0 : (atoi(v) == 1 ? 1 : -1);
-    e->chunk = std::min(cfg->max_snps, e->req.chunk_snps > 0 ? e->req.chunk_snps : 16384 / cfg->r);
+    e->chunk = std::min(cfg->max_snps, e->req.chunk_snps > 0 ? e->req.chunk_snps : 16384 / e->r);
     const char* gr = getenv("OA_GRAPHS");
     e->use_graphs = !(gr && gr[0] == '0');
     // the copy stream of host SNP blocks is created on first use: a device-resident
@@ -1645,8 +1738,8 @@ oa_status oa_engine_create(const oa_config* cfg, oa_engine** out) {
     }
     live_engines(cfg->device, +1);
     // pinned counters and a first staging area (trait grouping of max_traits traits)
-    if (cudaMallocHost(reinterpret_cast<void**>(&e->h_cnt), 8 * sizeof(unsigned long long)) != cudaSuccess ||
-        stage_reserve(e, (size_t)48 * cfg->max_traits + 65536) != OA_OK) {
+    e->h_cnt = static_cast<unsigned long long*>(pinned_pool().take(8 * sizeof(unsigned long long), &e->h_cnt_bytes));
+    if (!e->h_cnt || stage_reserve(e, (size_t)48 * cfg->max_traits + 65536) != OA_OK) {
         cudaGetLastError();
         set_err("pinned host allocation failed");
         oa_engine_destroy(e);
@@ -1670,11 +1763,12 @@ oa_status oa_engine_destroy(oa_engine* e) {
         if (cudaDeviceGetDefaultMemPool(&pool, e->cfg.device) == cudaSuccess) cudaMemPoolTrimTo(pool, 0);
         cudaGetLastError();
     }
-    if (e->h_rec) cudaFreeHost(e->h_rec);
-    if (e->h_cov) cudaFreeHost(e->h_cov);
-    for (void* q : e->retired_pinned) cudaFreeHost(q);
-    if (e->stage) cudaFreeHost(e->stage);
-    if (e->h_cnt) cudaFreeHost(e->h_cnt);
+    PinnedPool& pp = pinned_pool();
+    pp.give(e->h_rec, e->h_rec_cap * sizeof(Rec));
+    pp.give(e->h_cov, e->h_cov_cap * sizeof(float));
+    for (const auto& q : e->retired_pinned) pp.give(q.first, q.second);
+    pp.give(e->stage, e->stage_cap);
+    pp.give(e->h_cnt, e->h_cnt_bytes);
     for (int b = 0; b < 2; ++b) {
         cudaEventDestroy(e->ev_copied[b]);
         cudaEventDestroy(e->ev_used[b]);
@@ -1841,9 +1935,9 @@ oa_status oa_set_column_model(oa_engine* e, int32_t in_cols, const float* weight
     // a combined column without interactions yet: r = 1, or interaction columns follow (checked when a
     // block runs, so that the model and the interactions may be set in either order)
     const int want_r = combine ? (e->n_inter > 0 ? e->n_inter + e->inter_keep : 1) : in_cols;
-    if ((!combine && (want_r != e->r || e->n_inter > 0)) || (combine && e->n_inter > 0 && want_r != e->r)) {
+    if ((!combine && (want_r != e->ru || e->n_inter > 0)) || (combine && e->n_inter > 0 && want_r != e->ru)) {
         set_err("column model: %s needs r = %d, the engine has r = %d",
-                combine ? "a combined column" : "scaled columns (no interactions)", want_r, e->r);
+                combine ? "a combined column" : "scaled columns (no interactions)", want_r, e->ru);
         return OA_ERR_ARG;
     }
     if (e->subset) {
@@ -1864,9 +1958,9 @@ oa_status oa_set_interactions(oa_engine* e, const float* inter, int32_t k, int32
         set_err("null argument");
         return OA_ERR_ARG;
     }
-    if (k < 1 || k + (keep ? 1 : 0) != e->r) {
+    if (k < 1 || k + (keep ? 1 : 0) != e->ru) {
         set_err("%d interaction columns%s need r = %d, the engine has r = %d", k, keep ? " + the SNP" : "",
-                k + (keep ? 1 : 0), e->r);
+                k + (keep ? 1 : 0), e->ru);
         return OA_ERR_ARG;
     }
     if (e->in_cols > 0 && !e->model_combine) {
@@ -1900,8 +1994,8 @@ oa_status oa_set_snp_rows(oa_engine* e, const int32_t* rows, int32_t n_rows, int
         set_err("null engine");
         return OA_ERR_ARG;
     }
-    if (rows && e->in_cols > 0) {
-        set_err("a row subset does not apply with a column model");
+    if (rows && column_pass(e)) {
+        set_err("a row subset does not apply with a column model or with r = %d (zero columns added)", e->ru);
         return OA_ERR_STATE;
     }
     OA_CU(cudaSetDevice(e->cfg.device));
@@ -1984,12 +2078,12 @@ oa_status oa_reserve(oa_engine* e, int32_t traits, int32_t snps) {
         OA_CHECK(e->keys2.ensure(cap));
         OA_CHECK(e->perm.ensure(cap));
         OA_CHECK(e->perm2.ensure(cap));
-        OA_CHECK(e->rec2.ensure(R));
+        OA_CHECK(e->rec2.ensure(R * rec_slots(e->r)));
         size_t tmp = 0;
         OA_CU(cub::DeviceRadixSort::SortPairs(nullptr, tmp, e->keys.p, e->keys2.p, e->perm.p, e->perm2.p, (int)cap, 0,
                                               64, e->st));
         OA_CHECK(e->cub_tmp.ensure(tmp));
-        OA_CHECK(ensure_pinned(e->h_rec, e->h_rec_cap, R, e->retired_pinned));
+        OA_CHECK(ensure_pinned(e->h_rec, e->h_rec_cap, R * rec_slots(e->r), e->retired_pinned));
         if (e->cfg.disp_cov) {
             OA_CHECK(e->cov2.ensure(R * l * 3));
             OA_CHECK(ensure_pinned(e->h_cov, e->h_cov_cap, R * l * 3, e->retired_pinned));
@@ -2013,9 +2107,21 @@ oa_status oa_dense_last(oa_engine* e, float* beta, float* se, float* tstat, floa
     }
     OA_CU(cudaSetDevice(e->cfg.device));
     const size_t nd = (size_t)e->t * e->last_mb;
-    if (beta) OA_CU(cudaMemcpyAsync(beta, e->d_beta.p, sizeof(float) * nd * e->r, cudaMemcpyDeviceToHost, e->st));
-    if (se) OA_CU(cudaMemcpyAsync(se, e->d_se.p, sizeof(float) * nd * e->r, cudaMemcpyDeviceToHost, e->st));
-    if (tstat) OA_CU(cudaMemcpyAsync(tstat, e->d_t.p, sizeof(float) * nd * e->r, cudaMemcpyDeviceToHost, e->st));
+    // the device arrays hold r (padded) terms per test; the caller's hold ru
+    std::vector<float> tmp(padded(e) ? nd * e->r : 0);
+    auto get = [&](float* dst, const float* src) -> cudaError_t {
+        if (!dst) return cudaSuccess;
+        cudaError_t s = cudaMemcpyAsync(padded(e) ? tmp.data() : dst, src, sizeof(float) * nd * e->r,
+                                        cudaMemcpyDeviceToHost, e->st);
+        if (s != cudaSuccess || !padded(e)) return s;
+        if ((s = cudaStreamSynchronize(e->st)) != cudaSuccess) return s;
+        for (size_t q = 0; q < nd; ++q)
+            for (int a = 0; a < e->ru; ++a) dst[q * e->ru + a] = tmp[q * e->r + a];
+        return cudaSuccess;
+    };
+    OA_CU(get(beta, e->d_beta.p));
+    OA_CU(get(se, e->d_se.p));
+    OA_CU(get(tstat, e->d_t.p));
     if (r2) OA_CU(cudaMemcpyAsync(r2, e->d_r2.p, sizeof(float) * nd, cudaMemcpyDeviceToHost, e->st));
     OA_CU(cudaStreamSynchronize(e->st));
     return OA_OK;

@@ -126,7 +126,7 @@ __device__ __noinline__ double quirk_beta_rss(const EpiArgs& E, int i, int j, co
 // One test given its trait constants, Schur inverse S and the SNP's var_x.
 template <int R>
 __device__ __forceinline__ bool epi_core(const EpiArgs& E, int i, int j, const float* z, const TraitP& tp,
-                                         const double* S, const float* vx, Rec& rc) {
+                                         const double* S, const float* vx, RecOf<R>& rc) {
     double bx[R];
     double rss;
     if (E.qK) {
@@ -166,7 +166,7 @@ __device__ __forceinline__ bool epi_core(const EpiArgs& E, int i, int j, const f
         if (t > E.min_t || E.store_all) mask |= 1u << a;
     }
 #pragma unroll
-    for (int a = R; a < OA_MAX_R; ++a) rc.b[a] = rc.se[a] = rc.t[a] = 0.f;
+    for (int a = R; a < (int)(sizeof(rc.b) / sizeof(float)); ++a) rc.b[a] = rc.se[a] = rc.t[a] = 0.f;
     rc.mask = mask;
     const bool live = (rss > 0.0) && (r2 > E.min_r2 || E.store_all);
     if (E.d_r2) {
@@ -254,8 +254,8 @@ __device__ __forceinline__ bool epi_decide(const EpiArgs& E, int i, int j, const
 // The record of a stored test (the fields epi_core fills).
 template <int R>
 __device__ __forceinline__ void epi_write(const EpiArgs& E, int i, int j, const TraitP& tp, const EpiTest<R>& o,
-                                          Rec* dst) {
-    Rec rc;
+                                          RecOf<R>* dst) {
+    RecOf<R> rc;
     rc.trait = tp.orig;
     rc.snp = E.snp_base + i;
     rc.r2 = o.r2;
@@ -263,8 +263,9 @@ __device__ __forceinline__ void epi_write(const EpiArgs& E, int i, int j, const 
     rc.sig = sqrtf(fmaxf(o.sig2, 0.f));
     rc.tint = j;
     rc.pad[0] = rc.pad[1] = 0.f;
+    constexpr int K = (int)(sizeof(rc.b) / sizeof(float));
 #pragma unroll
-    for (int a = 0; a < OA_MAX_R; ++a) {
+    for (int a = 0; a < K; ++a) {
         rc.b[a] = a < R ? o.b[a] : 0.f;
         rc.se[a] = a < R ? o.se[a] : 0.f;
         rc.t[a] = a < R ? o.t[a] : 0.f;
@@ -272,7 +273,7 @@ __device__ __forceinline__ void epi_write(const EpiArgs& E, int i, int j, const 
     float4* d = reinterpret_cast<float4*>(dst);
     const float4* src = reinterpret_cast<const float4*>(&rc);
 #pragma unroll
-    for (int q = 0; q < (int)(sizeof(Rec) / 16); ++q) d[q] = src[q];
+    for (int q = 0; q < (int)(sizeof(rc) / 16); ++q) d[q] = src[q];
 }
 
 // Dense outputs of a singular test are NaN.
@@ -290,7 +291,7 @@ __device__ __forceinline__ void epi_dense_nan(const EpiArgs& E, int i, const Tra
 
 // Self-contained evaluation (loads its own constants): the SIMT GEMM epilogue.
 template <int R>
-__device__ __forceinline__ bool epi_eval(const EpiArgs& E, int i, int j, const float* z, bool valid, Rec& rc) {
+__device__ __forceinline__ bool epi_eval(const EpiArgs& E, int i, int j, const float* z, bool valid, RecOf<R>& rc) {
     if (!valid) return false;
     const TraitP tp = load_trait(E, j);
     double S[R * R];
@@ -307,7 +308,8 @@ __device__ __forceinline__ bool epi_eval(const EpiArgs& E, int i, int j, const f
 
 // Warp-aggregated append of the stored rows: one atomic on the slot counter
 // per warp and step (the SIMT GEMM, whose epilogue runs a few steps per tile).
-__device__ __forceinline__ void epi_emit(const EpiArgs& E, bool st, const Rec& rc) {
+template <int R>
+__device__ __forceinline__ void epi_emit(const EpiArgs& E, bool st, const RecOf<R>& rc) {
     const unsigned m = __ballot_sync(0xffffffffu, st);
     if (!m) return;
     const int lane = threadIdx.x & 31;
@@ -321,10 +323,10 @@ __device__ __forceinline__ void epi_emit(const EpiArgs& E, bool st, const Rec& r
     if (st) {
         const unsigned long long idx = base + __popc(m & ((1u << lane) - 1u));
         if ((long long)idx < E.cap) {
-            float4* dst = reinterpret_cast<float4*>(E.rec + idx);
+            float4* dst = reinterpret_cast<float4*>(static_cast<RecOf<R>*>(E.rec) + idx);
             const float4* src = reinterpret_cast<const float4*>(&rc);
 #pragma unroll
-            for (int q = 0; q < (int)(sizeof(Rec) / 16); ++q) dst[q] = src[q];
+            for (int q = 0; q < (int)(sizeof(rc) / 16); ++q) dst[q] = src[q];
         }
     }
 }
@@ -340,46 +342,21 @@ struct Emitter {
 
 // Close a warp's reserved block: unused slots are marked invalid (trait -1)
 // and the rows written are counted.  All lanes of the warp take part.
+template <int R>
 __device__ __forceinline__ void epi_retire(const EpiArgs& E, Emitter& em) {
     if (em.cap == 0) return;
     const int lane = threadIdx.x & 31;
     for (int q = em.used + lane; q < em.cap; q += 32) {
         const unsigned long long idx = em.base + (unsigned long long)q;
-        if ((long long)idx < E.cap) E.rec[idx].trait = -1;
+        if ((long long)idx < E.cap) static_cast<RecOf<R>*>(E.rec)[idx].trait = -1;
     }
     if (lane == 0 && E.rec_valid && em.used > 0) atomicAdd(E.rec_valid, (unsigned long long)em.used);
     em.used = em.cap = 0;
 }
 
-__device__ __forceinline__ void epi_emit_blocked(const EpiArgs& E, bool st, const Rec& rc, Emitter& em) {
-    if (!E.rec) return;
-    const unsigned m = __ballot_sync(0xffffffffu, st);
-    if (!m) return;
-    const int lane = threadIdx.x & 31;
-    const int k = __popc(m);
-    if (em.used + k > em.cap) {   // warp-uniform
-        epi_retire(E, em);
-        unsigned long long b = 0;
-        if (lane == 0) b = atomicAdd(E.rec_count, (unsigned long long)EMIT_BLOCK);
-        em.base = __shfl_sync(0xffffffffu, b, 0);
-        em.used = 0;
-        em.cap = EMIT_BLOCK;
-    }
-    if (st) {
-        const unsigned long long idx = em.base + (unsigned long long)(em.used + __popc(m & ((1u << lane) - 1u)));
-        if ((long long)idx < E.cap) {
-            float4* dst = reinterpret_cast<float4*>(E.rec + idx);
-            const float4* src = reinterpret_cast<const float4*>(&rc);
-#pragma unroll
-            for (int q = 0; q < (int)(sizeof(Rec) / 16); ++q) dst[q] = src[q];
-        }
-    }
-    em.used += k;
-}
-
-// epi_emit_blocked for records built only by the lanes that store: `write`
-// receives the slot of the calling lane's row.
-template <class W>
+// Block-reserved row emission for records built only by the lanes that
+// store: `write` receives the slot of the calling lane's row.
+template <int R, class W>
 __device__ __forceinline__ void epi_emit_lazy(const EpiArgs& E, bool st, Emitter& em, W&& write) {
     if (!E.rec) return;
     const unsigned m = __ballot_sync(0xffffffffu, st);
@@ -387,7 +364,7 @@ __device__ __forceinline__ void epi_emit_lazy(const EpiArgs& E, bool st, Emitter
     const int lane = threadIdx.x & 31;
     const int k = __popc(m);
     if (em.used + k > em.cap) {   // warp-uniform
-        epi_retire(E, em);
+        epi_retire<R>(E, em);
         unsigned long long b = 0;
         if (lane == 0) b = atomicAdd(E.rec_count, (unsigned long long)EMIT_BLOCK);
         em.base = __shfl_sync(0xffffffffu, b, 0);
@@ -396,7 +373,7 @@ __device__ __forceinline__ void epi_emit_lazy(const EpiArgs& E, bool st, Emitter
     }
     if (st) {
         const unsigned long long idx = em.base + (unsigned long long)(em.used + __popc(m & ((1u << lane) - 1u)));
-        if ((long long)idx < E.cap) write(E.rec + idx);
+        if ((long long)idx < E.cap) write(static_cast<RecOf<R>*>(E.rec) + idx);
     }
     em.used += k;
 }

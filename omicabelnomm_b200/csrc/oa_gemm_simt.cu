@@ -28,6 +28,7 @@ cudaError_t oa_launch_gemm_simt(int R, const float* X, size_t ldx, int xrows, co
         case 1: return go<1>(X, ldx, xrows, Yt, ldy, t, K, colmean, has_nan, center, E, st);
         case 2: return go<2>(X, ldx, xrows, Yt, ldy, t, K, colmean, has_nan, center, E, st);
         case 4: return go<4>(X, ldx, xrows, Yt, ldy, t, K, colmean, has_nan, center, E, st);
+        case 8: return go<8>(X, ldx, xrows, Yt, ldy, t, K, colmean, has_nan, center, E, st);
         default: return cudaErrorInvalidValue;
     }
 }

@@ -126,22 +126,47 @@ k_gemm_simt(const float* __restrict__ X, size_t ldx, int xrows, const float* __r
         }
     } else {
         // fused epilogue: rows ty*4+{0..3} and 64+ty*4+{0..3}; a SNP's R columns
-        // are consecutive rows held by this thread (R divides 4)
+        // are consecutive rows held by this thread (R divides 4), or, with
+        // R = 8, by this thread (even ty) and the thread of ty + 1 (lane + 16 of
+        // the same warp), whose rows come over by shuffle
+        if constexpr (R <= 4) {
 #pragma unroll
-        for (int half = 0; half < 2; ++half) {
+            for (int half = 0; half < 2; ++half) {
 #pragma unroll
-            for (int sg = 0; sg < 4 / R; ++sg) {
-                const int row0 = m0 + 64 * half + ty * 4 + sg * R;
-                const int i = row0 / R;  // SNP within the block
+                for (int sg = 0; sg < 4 / R; ++sg) {
+                    const int row0 = m0 + 64 * half + ty * 4 + sg * R;
+                    const int i = row0 / R;  // SNP within the block
+#pragma unroll
+                    for (int jj = 0; jj < 8; ++jj) {
+                        const int j = n0 + (jj < 4 ? tx * 4 + jj : 64 + tx * 4 + (jj - 4));
+                        float z[R];
+#pragma unroll
+                        for (int a = 0; a < R; ++a) z[a] = acc[half * 4 + sg * R + a][jj];
+                        RecOf<R> rc;
+                        const bool st = epi_eval<R>(E, i, j, z, (row0 < xrows) && (j < t), rc);
+                        epi_emit<R>(E, st, rc);
+                    }
+                }
+            }
+        } else {
+            static_assert(R == 8, "SNP column groups of 1, 2, 4 or 8");
+            const bool lead = (ty & 1) == 0;
+#pragma unroll
+            for (int half = 0; half < 2; ++half) {
+                const int row0 = m0 + 64 * half + ty * 4;
+                const int i = row0 / R;
 #pragma unroll
                 for (int jj = 0; jj < 8; ++jj) {
                     const int j = n0 + (jj < 4 ? tx * 4 + jj : 64 + tx * 4 + (jj - 4));
                     float z[R];
 #pragma unroll
-                    for (int a = 0; a < R; ++a) z[a] = acc[half * 4 + sg * R + a][jj];
-                    Rec rc;
-                    const bool st = epi_eval<R>(E, i, j, z, (row0 < xrows) && (j < t), rc);
-                    epi_emit(E, st, rc);
+                    for (int a = 0; a < 4; ++a) {
+                        z[a] = acc[half * 4 + a][jj];
+                        z[4 + a] = __shfl_down_sync(0xffffffffu, acc[half * 4 + a][jj], 16);
+                    }
+                    RecOf<R> rc;
+                    const bool st = epi_eval<R>(E, i, j, z, lead && (row0 < xrows) && (j < t), rc);
+                    epi_emit<R>(E, st, rc);
                 }
             }
         }

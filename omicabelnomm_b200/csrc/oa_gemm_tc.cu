@@ -46,7 +46,12 @@ template <int BK>
 constexpr int pf_blocks() {
     return 512 / BK;
 }
-constexpr unsigned long long WAIT_NS = 2000000000ull;
+// Bound of the pipeline waits (2 s by default; oa_set_wait_limit_tc changes
+// it for the device, which the timeout tests use to make the waits run out)
+// and of the drain waits after an abort (own copies and MMAs in flight;
+// never shortened).
+__constant__ unsigned long long c_wait_ns = 2000000000ull;
+constexpr unsigned long long DRAIN_NS = 2000000000ull;
 
 // Pipeline shape: K-block width BK (64 -> 128-byte swizzle, 32 -> 64-byte
 // swizzle), the number of shared-memory stages and the tile width BN.
@@ -98,11 +103,11 @@ __device__ __forceinline__ bool mbar_try(uint64_t* b, uint32_t parity) {
 // Wait for the phase of parity `parity` to complete; false on abort/timeout.
 __device__ __forceinline__ bool mbar_wait(uint64_t* b, uint32_t parity, volatile int* abort_flag) {
     if (mbar_try(b, parity)) return true;
-    const unsigned long long t0 = gtimer();
+    const unsigned long long t0 = gtimer(), lim = c_wait_ns;
     while (true) {
         if (mbar_try(b, parity)) return true;
         if (*abort_flag) return false;
-        if (gtimer() - t0 > WAIT_NS) {
+        if (gtimer() - t0 > lim) {
             *abort_flag = 1;
             return false;
         }
@@ -111,7 +116,7 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* b, uint32_t parity, volatile
 // Bounded wait that ignores the abort flag (draining work in flight).
 __device__ __forceinline__ void mbar_drain(uint64_t* b, uint32_t parity) {
     const unsigned long long t0 = gtimer();
-    while (!mbar_try(b, parity) && gtimer() - t0 < WAIT_NS) {
+    while (!mbar_try(b, parity) && gtimer() - t0 < DRAIN_NS) {
     }
 }
 
@@ -220,7 +225,7 @@ __device__ __forceinline__ void epi_columns(const EpiArgs& E, uint32_t taddr, in
                     st = epi_decide<R>(E, i, j, z, tp, S, vx, o);
                 }
             }
-            epi_emit_lazy(E, st, em, [&](Rec* dst) { epi_write<R>(E, i, j, tp, o, dst); });
+            epi_emit_lazy<R>(E, st, em, [&](RecOf<R>* dst) { epi_write<R>(E, i, j, tp, o, dst); });
         }
     }
 }
@@ -450,7 +455,7 @@ k_gemm_tc(const __grid_constant__ CUtensorMap mAhi, const __grid_constant__ CUte
                 aph ^= 1u;
             }
         }
-        epi_retire(E, em);
+        epi_retire<R>(E, em);
     }
 
     fence_before();
@@ -719,7 +724,7 @@ k_gemm_tc2(const __grid_constant__ CUtensorMap mAhi, const __grid_constant__ CUt
                 aph ^= 1u;
             }
         }
-        epi_retire(E, em);
+        epi_retire<R>(E, em);
     }
 
     fence_before();
@@ -852,6 +857,8 @@ static cudaError_t go_any(int variant, int raster, const __nv_bfloat16* Xhi, con
 
 }  // namespace tc
 
+cudaError_t oa_set_wait_limit_tc(unsigned long long ns) { return cudaMemcpyToSymbol(tc::c_wait_ns, &ns, sizeof ns); }
+
 cudaError_t oa_launch_gemm_tc(int R, int variant, int raster, const __nv_bfloat16* Xhi, const __nv_bfloat16* Xlo,
                               int xrows, const __nv_bfloat16* Yhi, const __nv_bfloat16* Ylo, int t, int n_pad,
                               const EpiArgs& E, int* err, cudaStream_t st) {
@@ -859,6 +866,7 @@ cudaError_t oa_launch_gemm_tc(int R, int variant, int raster, const __nv_bfloat1
         case 1: return tc::go_any<1>(variant, raster, Xhi, Xlo, xrows, Yhi, Ylo, t, n_pad, E, err, st);
         case 2: return tc::go_any<2>(variant, raster, Xhi, Xlo, xrows, Yhi, Ylo, t, n_pad, E, err, st);
         case 4: return tc::go_any<4>(variant, raster, Xhi, Xlo, xrows, Yhi, Ylo, t, n_pad, E, err, st);
+        case 8: return tc::go_any<8>(variant, raster, Xhi, Xlo, xrows, Yhi, Ylo, t, n_pad, E, err, st);
         default: return cudaErrorInvalidValue;
     }
 }

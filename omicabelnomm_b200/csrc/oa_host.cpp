@@ -628,6 +628,10 @@ oa_status oa_solve(const oa_settings* S, oa_outputs* out) {
         herr("%d covariates: this build supports 1..%d", l, OA_MAX_L);
         return OA_ERR_UNSUPPORTED;
     }
+    if (r > OA_MAX_R) {
+        herr("%d columns per SNP: this build supports 1..%d", r, OA_MAX_R);
+        return OA_ERR_UNSUPPORTED;
+    }
     // ID order checks (warnings only, as in the reference, src/AIOwrapper.cpp:148-191)
     for (int i = 0; i < fileN; ++i) {
         const std::string a = FY.obs_name(i), b = FL.obs_name(i), c = FR.obs_name(i);

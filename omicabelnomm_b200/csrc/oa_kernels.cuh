@@ -259,7 +259,8 @@ static __global__ void k_set_qrows(const int* __restrict__ rows, int total, cons
 // Sort keys of the stored-row slots: trait * mb + SNP, an unused slot (trait
 // -1) all ones in the low `bits` bits, so that it sorts last (the sort looks
 // at those bits only; 2^bits > t * mb).
-static __global__ void k_rec_keys(const Rec* __restrict__ rec, long long N, long long mb, int bits,
+template <class RecT>
+static __global__ void k_rec_keys(const RecT* __restrict__ rec, long long N, long long mb, int bits,
                                   unsigned long long* __restrict__ keys, int* __restrict__ perm) {
     const long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x;
     if (q >= N) return;
@@ -271,7 +272,7 @@ static __global__ void k_rec_keys(const Rec* __restrict__ rec, long long N, long
 
 // The stored rows that go back to the host, in sorted order and packed by
 // field: N x {trait, snp, r2, mask} then N x R each of b, se, t (16 + 12 R
-// bytes per row instead of the 80-byte record).
+// bytes per row instead of the 80- or 128-byte record).
 struct RowsSoA {
     int32_t* trait;
     int32_t* snp;
@@ -297,12 +298,12 @@ __host__ __device__ inline RowsSoA rows_soa(void* base, long long N, int R) {
 }
 
 template <int R>
-static __global__ void k_rec_gather(const Rec* __restrict__ rec, const int* __restrict__ perm, long long N,
+static __global__ void k_rec_gather(const RecOf<R>* __restrict__ rec, const int* __restrict__ perm, long long N,
                                     RowsSoA out, const float* __restrict__ cov, float* __restrict__ cov_out, int l) {
     const long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x;
     if (q >= N) return;
     const int src = perm[q];
-    const Rec& rc = rec[src];
+    const RecOf<R>& rc = rec[src];
     out.trait[q] = rc.trait;
     out.snp[q] = rc.snp;
     out.r2[q] = rc.r2;

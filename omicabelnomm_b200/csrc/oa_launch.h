@@ -27,6 +27,10 @@ cudaError_t oa_launch_gemm_simt(int R, const float* X, size_t ldx, int xrows, co
                                 cudaStream_t st);
 // variant: 1 = BK 32 x 4 stages, 2 = BK 64 x 2 stages, 3 = CTA pairs (2-SM MMA) BK 32 x 6, 4 = pairs BK 64 x 3;
 // raster: 1 = trait tiles inner, 2 = SNP tiles inner
+// Bound (ns of %globaltimer) of the pipeline waits of the tensor-core GEMMs and of the staging waits of the
+// per-SNP statistics kernels on the current device (2 s by default); the drain waits keep 2 s
+cudaError_t oa_set_wait_limit_tc(unsigned long long ns);
+cudaError_t oa_set_wait_limit_stats(unsigned long long ns);
 cudaError_t oa_launch_gemm_tc(int R, int variant, int raster, const __nv_bfloat16* Xhi, const __nv_bfloat16* Xlo,
                               int xrows, const __nv_bfloat16* Yhi, const __nv_bfloat16* Ylo, int t, int n_pad,
                               const EpiArgs& E, int* err, cudaStream_t st);

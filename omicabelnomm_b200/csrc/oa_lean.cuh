@@ -465,10 +465,10 @@ k_snp_lean(LeanArgs A) {
     }
     if (!BULK) asm volatile("cp.async.wait_group 0;" ::: "memory");   // nothing in flight at exit
     if (BULK && threadIdx.x == 0 && stop) {
-        st_mbar_wait(&mbar[0], 0);
-        st_mbar_wait(&mbar[0], 1);
-        st_mbar_wait(&mbar[1], 0);
-        st_mbar_wait(&mbar[1], 1);
+        st_mbar_wait(&mbar[0], 0, true);
+        st_mbar_wait(&mbar[0], 1, true);
+        st_mbar_wait(&mbar[1], 0, true);
+        st_mbar_wait(&mbar[1], 1, true);
     }
 }
 
@@ -507,6 +507,7 @@ static __global__ void k_split_bf16(const float* __restrict__ src, long long cou
 
 struct SchurArgs {
     int l, mb, G, Z, ldc;
+    int rr;                  // the caller's columns per SNP; columns [rr, R) are zero padding
     const float* C2;         // pre-GEMM output, column c of SNP column x at C2[c * ldc + x]
     const float* D;          // [mb][r*r]
     const float* Dset;       // [G+Z][mb][r*r]
@@ -595,6 +596,9 @@ __device__ __noinline__ void schur_quirk(const SchurArgs& S, int i, int g, size_
     quad(dl, t2);
 #pragma unroll
     for (int u = 0; u < R * R; ++u) S.qK[gi * R * R + u] = Dobs[u] - t1[u] + t2[u];
+#pragma unroll
+    for (int a = 0; a < R; ++a)
+        if (a >= S.rr) Sq[a * R + a] = 1.0;
     const bool ok = full_ok && !S.pat_bad[g] && schur_inverse<R>(Sq, dso);
     S.sing[gi] = ok ? 0 : 1;
 #pragma unroll
@@ -631,6 +635,11 @@ __device__ __forceinline__ void schur_item(const SchurArgs& S, int i, int slot) 
     double dss[R];
 #pragma unroll
     for (int a = 0; a < R; ++a) dss[a] = Dm[a * R + a];
+    // zero padding columns (r = 3, 5, 6, 7 run as 4 or 8): their rows and columns of every sum are
+    // exactly 0; an identity block keeps them out of the other columns' solution (coefficient 0)
+#pragma unroll
+    for (int a = 0; a < R; ++a)
+        if (a >= S.rr) Sf[a * R + a] = dss[a] = 1.0;
     const bool full_ok = schur_inverse<R>(Sf, dss);
     if (slot == 0) {
 #pragma unroll
@@ -665,7 +674,7 @@ __device__ __forceinline__ void schur_item(const SchurArgs& S, int i, int slot) 
     for (int u = 0; u < R * R; ++u) Sg[u] = Dm[u] - (double)S.Dset[gi * R * R + u];
     double dso[R];
 #pragma unroll
-    for (int a = 0; a < R; ++a) dso[a] = Sg[a * R + a];
+    for (int a = 0; a < R; ++a) dso[a] = a < S.rr ? Sg[a * R + a] : 1.0;
     const double* Wg = S.W + (size_t)g * l * l;
     for (int qq = 0; qq < l; ++qq) {
         double wa[R];
@@ -685,6 +694,9 @@ __device__ __forceinline__ void schur_item(const SchurArgs& S, int i, int slot) 
         schur_quirk<R>(S, i, g, gi, ao, Dm, dso, full_ok);
         return;
     }
+#pragma unroll
+    for (int a = 0; a < R; ++a)
+        if (a >= S.rr) Sg[a * R + a] = 1.0;
     const bool ok = full_ok && !S.pat_bad[g] && schur_inverse<R>(Sg, dso);
     S.sing[gi] = ok ? 0 : 1;
 #pragma unroll

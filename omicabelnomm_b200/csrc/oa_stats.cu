@@ -113,6 +113,7 @@ int oa_lean_ctas_per_sm(int R, int spb, size_t smem) {
         case 204: v = lean_occ<2, 4>(smem); break;
         case 401: v = lean_occ<4, 1>(smem); break;
         case 402: v = lean_occ<4, 2>(smem); break;
+        case 801: v = lean_occ<8, 1>(smem); break;
         default: v = 0;
     }
     std::lock_guard<std::mutex> g(mu);
@@ -131,8 +132,13 @@ cudaError_t oa_launch_snp_lean(int R, int spb, const LeanArgs& A, int grid, size
         case 204: return go_lean<2, 4>(A, grid, smem, st);
         case 401: return go_lean<4, 1>(A, grid, smem, st);
         case 402: return go_lean<4, 2>(A, grid, smem, st);
+        case 801: return go_lean<8, 1>(A, grid, smem, st);
         default: return cudaErrorInvalidValue;
     }
+}
+
+cudaError_t oa_set_wait_limit_stats(unsigned long long ns) {
+    return cudaMemcpyToSymbol(c_st_wait_ns, &ns, sizeof ns);
 }
 
 cudaError_t oa_launch_schur(int R, const SchurArgs& S, cudaStream_t st) {
@@ -148,6 +154,7 @@ cudaError_t oa_launch_schur(int R, const SchurArgs& S, cudaStream_t st) {
         case 1: k_schur<1><<<blocks, 256, 0, st>>>(S); break;
         case 2: k_schur<2><<<blocks, 256, 0, st>>>(S); break;
         case 4: k_schur<4><<<blocks, 256, 0, st>>>(S); break;
+        case 8: k_schur<8><<<blocks, 256, 0, st>>>(S); break;
         default: return cudaErrorInvalidValue;
     }
     return cudaGetLastError();

@@ -92,14 +92,20 @@ __device__ __forceinline__ bool st_mbar_try(uint64_t* b, uint32_t parity) {
     return ok != 0;
 }
 
-// Bounded wait (2 s of %globaltimer).
-__device__ __forceinline__ bool st_mbar_wait(uint64_t* b, uint32_t parity) {
+// Bound of the staging waits (2 s by default; oa_set_wait_limit_stats
+// changes it for the device, which the timeout tests use to make the waits
+// run out).  The drain waits after a stop keep the 2 s bound.
+static __constant__ unsigned long long c_st_wait_ns = 2000000000ull;
+
+// Bounded wait on %globaltimer: the staging bound, or 2 s when draining.
+__device__ __forceinline__ bool st_mbar_wait(uint64_t* b, uint32_t parity, bool drain = false) {
+    const unsigned long long lim = drain ? 2000000000ull : c_st_wait_ns;
     unsigned long long t0;
     asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t0));
     while (!st_mbar_try(b, parity)) {
         unsigned long long t1;
         asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t1));
-        if (t1 - t0 > 2000000000ull) return false;
+        if (t1 - t0 > lim) return false;
     }
     return true;
 }
@@ -428,10 +434,10 @@ k_snp_stats(StatsArgs A) {
     }
     // a stopped CTA leaves no copy in flight behind it
     if (BULK && threadIdx.x == 0 && stop) {
-        st_mbar_wait(&mbar[0], 0);
-        st_mbar_wait(&mbar[0], 1);
-        st_mbar_wait(&mbar[1], 0);
-        st_mbar_wait(&mbar[1], 1);
+        st_mbar_wait(&mbar[0], 0, true);
+        st_mbar_wait(&mbar[0], 1, true);
+        st_mbar_wait(&mbar[1], 0, true);
+        st_mbar_wait(&mbar[1], 1, true);
     }
 }
 

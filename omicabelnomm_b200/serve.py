@@ -2,8 +2,8 @@
 HBM, with continuous batching.
 
 A request names a cohort (a subset of the resident individuals with its own
-covariates), brings its traits (device memory, NaN = missing) and a
-contiguous SNP range.  The loop
+covariates: in the serving workload every request draws its own), brings its
+traits (device memory, NaN = missing) and a contiguous SNP range.  The loop
 
 * admits waiting requests in arrival order whenever a slot is free and the
   request's device-memory footprint fits the budget (first fit: a large
@@ -12,11 +12,13 @@ contiguous SNP range.  The loop
 * runs every admitted request on its own host thread and its own engine
   (own CUDA streams), so the kernels of concurrent requests overlap on the
   device; the ctypes calls release the GIL;
-* keeps every engine after its request ends (covariate factorisation,
-  row-set tables and buffers stay resident) and reuses it for the next
-  request of that cohort (several engines per cohort when its requests
-  overlap); idle engines are evicted, least recently used first, when an
-  admission needs their memory;
+* creates the request's engine inside its latency (covariate factorisation,
+  row subset, reservations) unless an idle engine of the same cohort holds
+  its traits (reuse_engines: requests that repeat a cohort); engine buffers
+  come from pools shared by all engines (device memory from the device's
+  stream-ordered pool, page-locked host buffers from the engine library's
+  pool), so a new engine allocates little; idle engines are evicted, least
+  recently used first, when an admission needs their memory;
 * reports per-request latency (arrival to results on the host), queueing
   and run time, and the aggregate tests/s.
 
@@ -98,7 +100,7 @@ class Server:
     def __init__(self, geno_ptr: int, n_total: int, m_total: int, cohorts: Dict[int, Cohort], *,
                  device: int = 0, budget_bytes: int, max_slots: int = 8, precision: int = E.MIXED,
                  chunk_snps: int = 0, min_p_store: float = 1e-3, max_snps: Optional[int] = None,
-                 engine_factory=None, t_cap_min: int = 64):
+                 engine_factory=None, t_cap_min: int = 64, reuse_engines: bool = True):
         self.geno_ptr = geno_ptr
         self.n_total = n_total
         self.m_total = m_total
@@ -115,6 +117,13 @@ class Server:
         self.evictions = 0
         self.max_bypass_s = 2.0         # later requests may pass a waiting one for this long
         self.t_cap_min = t_cap_min      # trait capacity of a new engine (larger ones are reused more)
+        self.reuse_engines = reuse_engines   # keep an engine for later requests of its cohort
+        self._anchor = None
+        if engine_factory is None:
+            # a small engine held for the server's lifetime: the device keeps the freed memory of
+            # per-request engines in its pool (the engine library returns the pool's memory when the
+            # last engine on a device goes)
+            self._anchor = E.Engine(64, 1, 1, 1, 1, precision=precision, device=device)
         self._lock = threading.Condition()
         self._idle: List[_Slot] = []    # idle engines, least recently used first (several per cohort allowed)
         self._active_bytes = 0
@@ -147,6 +156,8 @@ class Server:
     # -- engines --------------------------------------------------------------
     def _take_engine(self, req: Request) -> Optional[_Slot]:
         """The most recently used idle engine of the request's cohort that holds its traits (caller holds the lock)."""
+        if not self.reuse_engines:
+            return None
         for q in range(len(self._idle) - 1, -1, -1):
             slot = self._idle[q]
             if slot.cohort == req.cohort and slot.t_cap >= req.t:
@@ -188,9 +199,13 @@ class Server:
             t3 = time.perf_counter()
             ph = {"engine": t1 - t0, "traits": t2 - t1, "scan": t3 - t2}
             finished = t3 - t_start
+            slot.bytes = eng.device_bytes()
+            if not self.reuse_engines:      # its buffers go back to the pools (after the results are out)
+                slot.engine.close()
+                slot = None
+                ph["release"] = time.perf_counter() - t3
             results.append(Result(rid=req.rid, rows=out, tests=req.t * req.nsnp, arrival=arrival,
                                   admitted=admitted, finished=finished, phases=ph))
-            slot.bytes = eng.device_bytes()
         except BaseException as ex:  # reported to the caller of run()
             errors.append(ex)
             if slot is not None:
@@ -293,6 +308,9 @@ class Server:
             for s in self._idle:
                 s.engine.close()
             self._idle.clear()
+            if self._anchor is not None:
+                self._anchor.close()
+                self._anchor = None
 
 
 def summarize(results: List[Result]) -> dict:
@@ -303,7 +321,7 @@ def summarize(results: List[Result]) -> dict:
     t0 = min(r.arrival for r in results)
     t1 = max(r.finished for r in results)
     phases = {}
-    for k in ("engine", "traits", "scan"):
+    for k in ("engine", "traits", "scan", "release"):
         v = np.array([r.phases.get(k, 0.0) for r in results])
         phases[k + "_p50_ms"] = float(np.percentile(v, 50) * 1e3)
         phases[k + "_p99_ms"] = float(np.percentile(v, 99) * 1e3)
@@ -325,7 +343,7 @@ class ServeWorkload:
     m_total: int = 1_000_000
     rate: float = 20.0          # Poisson arrivals per second
     requests: int = 120
-    cohorts: int = 12
+    cohorts: int = 0            # 0: every request draws its own subsample and covariates
     n_lo: int = 2000
     n_hi: int = 20000
     t_lo: float = 1.0
@@ -338,27 +356,31 @@ class ServeWorkload:
     seed: int = 4004
 
 
+def draw_cohort(rng, w: ServeWorkload, cid: int) -> Cohort:
+    """n ~ U(n_lo, n_hi) individuals of the resident matrix, l ~ U{l_lo..l_hi} covariates
+    (intercept, sex, age, PCs)."""
+    n = int(rng.integers(w.n_lo, w.n_hi + 1))
+    rows = np.sort(rng.choice(w.n_total, n, replace=False)).astype(np.int32)
+    l = int(rng.integers(w.l_lo, w.l_hi + 1))
+    cols = [np.ones(n), (rng.random(n) < 0.5).astype(np.float64), rng.normal(50, 10, n)]
+    for _ in range(l - 3):
+        cols.append(rng.normal(0, 1, n))
+    return Cohort(cid=cid, rows=rows, XL=np.stack(cols[:l]).astype(np.float32))
+
+
 def make_cohorts(w: ServeWorkload) -> Dict[int, Cohort]:
-    """Cohorts: n ~ U(n_lo, n_hi) individuals of the resident matrix, l ~ U{l_lo..l_hi}
-    covariates (intercept, sex, age, PCs)."""
+    """w.cohorts fixed cohorts that requests share (make_requests with cohorts)."""
     rng = np.random.Generator(np.random.PCG64(w.seed))
-    out = {}
-    for c in range(w.cohorts):
-        n = int(rng.integers(w.n_lo, w.n_hi + 1))
-        rows = np.sort(rng.choice(w.n_total, n, replace=False)).astype(np.int32)
-        l = int(rng.integers(w.l_lo, w.l_hi + 1))
-        cols = [np.ones(n), (rng.random(n) < 0.5).astype(np.float64), rng.normal(50, 10, n)]
-        for _ in range(l - 3):
-            cols.append(rng.normal(0, 1, n))
-        out[c] = Cohort(cid=c, rows=rows, XL=np.stack(cols[:l]).astype(np.float32))
-    return out
+    return {c: draw_cohort(rng, w, c) for c in range(w.cohorts)}
 
 
-def make_requests(w: ServeWorkload, cohorts: Dict[int, Cohort], device, keep: list) -> List[Request]:
-    """Requests with Poisson arrivals; traits drawn on the device (kept alive in `keep`):
-    t ~ LogUniform(t_lo, t_hi) traits Y = XL b + N(0, 1) with b ~ N(0, 1) over the
-    cohort's covariates, SNP range length ~ LogUniform(len_lo, len_hi), 1-4
-    missingness patterns per request with 0-miss_hi missing each."""
+def make_requests(w: ServeWorkload, cohorts: Optional[Dict[int, Cohort]], device, keep: list):
+    """(requests, cohorts): requests with Poisson arrivals; traits drawn on the device (kept
+    alive in `keep`): t ~ LogUniform(t_lo, t_hi) traits Y = XL b + N(0, 1) with b ~ N(0, 1)
+    over the cohort's covariates, SNP range length ~ LogUniform(len_lo, len_hi), 1-4
+    missingness patterns per request with 0-miss_hi missing each.  With cohorts None every
+    request draws its own subsample and covariates (draw_cohort; cohort id = request id);
+    otherwise requests pick one of the given cohorts."""
     import torch
     rng = np.random.Generator(np.random.PCG64(w.seed + 1))
     g = torch.Generator(device=device)
@@ -366,8 +388,15 @@ def make_requests(w: ServeWorkload, cohorts: Dict[int, Cohort], device, keep: li
     arrivals = np.cumsum(rng.exponential(1.0 / w.rate, w.requests))
     arrivals -= arrivals[0]
     reqs = []
+    own = cohorts is None
+    if own:
+        cohorts = {}
     for i in range(w.requests):
-        cid = int(rng.integers(0, len(cohorts)))
+        if own:
+            cid = i
+            cohorts[cid] = draw_cohort(rng, w, cid)
+        else:
+            cid = int(rng.integers(0, len(cohorts)))
         n = cohorts[cid].rows.size
         t = max(1, int(round(np.exp(rng.uniform(np.log(w.t_lo), np.log(w.t_hi))))))
         ln = int(round(np.exp(rng.uniform(np.log(w.len_lo), np.log(min(w.len_hi, w.m_total))))))
@@ -384,7 +413,7 @@ def make_requests(w: ServeWorkload, cohorts: Dict[int, Cohort], device, keep: li
         keep.append(Y)
         reqs.append(Request(rid=i, cohort=cid, snp0=s0, nsnp=ln, y_ptr=Y.data_ptr(), t=t,
                             arrival=float(arrivals[i])))
-    return reqs
+    return reqs, cohorts
 
 
 def resident_genotypes(w: ServeWorkload, device, snp_chunk: int = 16384):

@@ -89,21 +89,35 @@ CASES = {
     "r1_multinter": (dict(n=300, m=230, t=5, l=3, miss_mode="none", seed=36), "inter3",
                      [["-w", "{inter}"], ["-w", "{inter}", "-f"], ["-w", "{inter}", "-f", "-i"],
                       ["-w", "{inter}", "-b"]]),
+    # three columns per SNP without a model (-n 3: consecutive triples of dosage columns form one SNP);
+    # the engine runs them as four columns with a zero column added on the device
+    "r3_cols": (dict(n=400, m=120, t=5, l=4, miss_mode="none", seed=37), None,
+                [["-n", "3"], ["-n", "3", "-f"], ["-n", "3", "-b"]]),
+    # ... with phenotype missingness: the reference's r >= 2 downdate applies
+    "r3_missing": (dict(n=400, m=90, t=6, l=4, seed=38), None, [["-n", "3", "-f"]]),
+    # two interaction columns (-v, r = 3) and four (r = 5: eight kernel columns per SNP)
+    "r1_inter2": (dict(n=400, m=40, t=5, l=3, miss_mode="none", seed=39), "inter2",
+                  [["-v", "{inter}"], ["-v", "{inter}", "-f"]]),
+    "r1_inter4": (dict(n=400, m=30, t=4, l=3, miss_mode="none", seed=40), "inter4",
+                  [["-v", "{inter}"], ["-v", "{inter}", "-f"]]),
 }
 
 FACTORS = "0.5 1.5\n"
 
 
 def interaction_file(n: int, seed: int, prefix: str, k: int):
-    """k interaction columns of n individuals: N(0, 1), then Bernoulli(0.5), then U(0, 2);
-    the first column holds 3 NaN values."""
+    """k interaction columns of n individuals: N(0, 1), then Bernoulli(0.5), then U(0, 2), then
+    N(1, 0.5); the first column holds 3 NaN values."""
     import numpy as np
     from omicabelnomm_b200 import fvformat
     rng = np.random.Generator(np.random.PCG64(seed))
     cols = [rng.normal(0.0, 1.0, n), rng.binomial(1, 0.5, n).astype(np.float64), rng.uniform(0.0, 2.0, n)]
+    nan_rows = rng.choice(n, 3, replace=False)
+    if k > 3:
+        cols.append(rng.normal(1.0, 0.5, n))
     I = np.stack(cols[:k]).astype(np.float32)
-    I[0, rng.choice(n, 3, replace=False)] = np.nan
-    fvformat.write_fv(prefix, I, fvformat.obs_names(n), ["inter_env", "inter_sex", "inter_dose"][:k])
+    I[0, nan_rows] = np.nan
+    fvformat.write_fv(prefix, I, fvformat.obs_names(n), ["inter_env", "inter_sex", "inter_dose", "inter_score"][:k])
 
 EXCLUDE_LIST = "1 2\n5\n7\n9 11\n13\n40 44\n"
 
@@ -127,9 +141,9 @@ def build_inputs(case: str, where: str):
         with open(p, "w") as f:
             f.write(EXCLUDE_LIST)
         extra["excl"] = p
-    if post in ("inter", "inter3"):
+    if post in ("inter", "inter2", "inter3", "inter4"):
         p = os.path.join(where, case + "_INT")
-        interaction_file(over["n"], over["seed"] + 7, p, 1 if post == "inter" else 3)
+        interaction_file(over["n"], over["seed"] + 7, p, {"inter": 1, "inter2": 2, "inter3": 3, "inter4": 4}[post])
         extra["inter"] = p
     if post == "factors":
         p = os.path.join(where, case + "_factors.txt")

@@ -46,7 +46,7 @@ import golden_util as GU  # noqa: E402
 import oa_oracle as O  # noqa: E402
 from golden import make_golden as MG  # noqa: E402
 
-QUIRK_RUNS = {("r2_missing", "nf"), ("r1_dosf", "nz")}   # the reference's r >= 2 downdate applies
+QUIRK_RUNS = {("r2_missing", "nf"), ("r1_dosf", "nz"), ("r3_missing", "nf")}   # the reference's r >= 2 downdate applies
 
 
 def _by_key(rows):

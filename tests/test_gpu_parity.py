@@ -121,7 +121,7 @@ def test_chunked_block_equals_single_block(monkeypatch):
 # the CLI against the reference's own outputs
 # ---------------------------------------------------------------------------
 # golden runs where the reference's r >= 2 downdate applies (r = 2 with phenotype missingness)
-QUIRK_RUNS = {("r2_missing", "nf"), ("r1_dosf", "nz")}
+QUIRK_RUNS = {("r2_missing", "nf"), ("r1_dosf", "nz"), ("r3_missing", "nf")}
 
 
 def run_cli(pre, extra, flags, out, precision="plain"):
@@ -262,24 +262,38 @@ def test_dense_flags_match_oracle_masks(prec, stats_path):
     assert stored == set(zip(rows.trait.tolist(), rows.snp.tolist()))
 
 
+def _multicol(r, seed, **over):
+    """r dosage columns per SNP: consecutive independent dosage columns grouped r at a time."""
+    w = dict(n=500, m=30, t=12, l=4, miss_mode="patterns", n_patterns=3, miss_hi=0.12)
+    w.update(over)
+    w["m"] *= r
+    return synth.generate(synth.scaled(0, seed=seed, **w))
+
+
 @pytest.mark.parametrize("prec", [E.PLAIN, E.MIXED])
-@pytest.mark.parametrize("case", ["r2_missing", "r2_yzero_l1"])
+@pytest.mark.parametrize("case", ["r2_missing", "r2_yzero_l1", "r3_missing", "r5_l2"])
 def test_quirk_r2_matches_oracle_quirk(case, prec):
     """The reference's r >= 2 downdate reproduced on the device (quirk mode) against the
     oracle's restatement of it: dense t, SE, R2 and the singular set; also with observed
-    zero phenotypes (zero sets) and with r > l (l = 1: the SNP-block downdate quirk)."""
+    zero phenotypes (zero sets), with r > l (the SNP-block downdate quirk) and with r = 3
+    and 5 (zero padding columns in the kernels)."""
+    r = 2
     if case == "r2_missing":
         ds = synth.generate(synth.scaled(0, **CASES["r2_missing"]))
-    else:
+    elif case == "r2_yzero_l1":
         ds = _yzero(synth.generate(synth.scaled(0, n=500, m=90, t=12, l=1, r=2, miss_mode="patterns",
                                                 n_patterns=3, miss_hi=0.15, seed=74)), 9)
+    elif case == "r3_missing":
+        r, ds = 3, _multicol(3, 75)
+    else:
+        r, ds = 5, _multicol(5, 76, l=2)
     l, n = ds.XL.shape
-    m, t = ds.XR.shape[0] // 2, ds.Y.shape[0]
+    m, t = ds.XR.shape[0] // r, ds.Y.shape[0]
     inp = O.Inputs(XL=ds.XL, XR=ds.XR, Y=ds.Y, xl_names=ds.xl_names, xr_names=ds.xr_names,
                    y_names=ds.y_names, realN=n, kept=np.arange(n))
-    D = O.solve(inp, O.Settings(r=2, storePInd=True, quirk_r2=True), keep_dense=True).dense
-    Dc = O.solve(inp, O.Settings(r=2, storePInd=True), keep_dense=True).dense
-    eng = E.Engine(n, l, 2, t, m, precision=prec, store_all=True, quirk_r2=True,
+    D = O.solve(inp, O.Settings(r=r, storePInd=True, quirk_r2=True), keep_dense=True).dense
+    Dc = O.solve(inp, O.Settings(r=r, storePInd=True), keep_dense=True).dense
+    eng = E.Engine(n, l, r, t, m, precision=prec, store_all=True, quirk_r2=True,
                    min_t_store=E.t_threshold(0.1), min_r2_store=1e-6)
     eng.set_covariates(ds.XL)
     eng.set_traits(ds.Y)
@@ -297,3 +311,27 @@ def test_quirk_r2_matches_oracle_quirk(case, prec):
     assert rows.singular == int(D.singular.sum())
     # the quirk matters here: its answers are not the corrected ones
     assert np.abs(D.tstat[:, :, l:] - Dc.tstat[:, :, l:])[ok].max() > 1e-2
+
+
+@pytest.mark.parametrize("prec", [E.PLAIN, E.MIXED])
+@pytest.mark.parametrize("r", [3, 5, 6, 8])
+def test_dense_more_columns_per_snp_match_fp64_oracle(r, prec):
+    """r = 3, 5, 6 (kernels with 4 or 8 columns per SNP, zero columns added on the device)
+    and r = 8, with missingness patterns, against the FP64 oracle; plain bars for the
+    plain form, the r >= 2 mixed bars for the mixed form."""
+    ds = _multicol(r, 80 + r, m=24, t=10)
+    res, _, _ = oracle_dense(ds, r)
+    eng, rows, (b, se, tt, r2) = engine_run(ds, r, precision=prec)
+    D = res.dense
+    l = res.l
+    ok = ~D.singular
+    t_ref = D.tstat[:, :, l:][ok]
+    dt = np.abs(tt[ok] - t_ref)
+    t_sys = np.broadcast_to(np.abs(t_ref).max(axis=1, keepdims=True), t_ref.shape)
+    lim = (T_REL * t_sys + T_ABS) if prec == E.PLAIN else (1e-3 + 1e-4 * t_sys)
+    assert np.all(dt <= lim), f"max |dt| {dt.max():.3g}"
+    assert np.allclose(se[ok], D.se[:, :, l:][ok], rtol=SE_REL if prec == E.PLAIN else 1e-3, atol=0)
+    assert tt.shape == (ds.Y.shape[0], ds.XR.shape[0] // r, r)
+    assert rows.singular == int(D.singular.sum())
+    # stored rows carry the r SNP terms (p = l + r coefficients per row)
+    assert rows.B.shape[1] == l + r

@@ -76,7 +76,7 @@ def test_each_request_same_alone_and_in_the_mix(resident):
     w, coh = _cohorts()
     w.requests, w.t_hi, w.len_lo, w.len_hi = 10, 80.0, 500.0, 20000.0
     keep = []
-    reqs = S.make_requests(w, coh, torch.device("cuda", 0), keep)
+    reqs, _ = S.make_requests(w, coh, torch.device("cuda", 0), keep)
     budget = 8 << 30
     alone = {}
     srv = S.Server(Xd.data_ptr(), N_TOTAL, M_TOTAL, coh, budget_bytes=budget, max_slots=1, chunk_snps=4096,
@@ -98,6 +98,32 @@ def test_each_request_same_alone_and_in_the_mix(resident):
             np.testing.assert_array_equal(getattr(a, f), getattr(b, f), err_msg=f"request {res.rid} field {f}")
     s = S.summarize(mix)
     assert s["tests"] == sum(q.t * q.nsnp for q in reqs)
+
+
+def test_own_subsample_requests_same_alone_and_in_the_mix(resident):
+    """The serving workload's form: every request its own subsample and covariates, its
+    engine created inside the request and released after it; each request's stored rows
+    are identical alone and among concurrent requests."""
+    import torch
+    _, Xd = resident
+    w = S.ServeWorkload(n_total=N_TOTAL, m_total=M_TOTAL, requests=8, n_lo=700, n_hi=N_TOTAL, t_hi=60.0,
+                        len_lo=500.0, len_hi=20000.0, seed=96)
+    keep = []
+    reqs, coh = S.make_requests(w, None, torch.device("cuda", 0), keep)
+    assert len(coh) == len(reqs) and len({c.rows.size for c in coh.values()}) > 1
+    kw = dict(budget_bytes=8 << 30, chunk_snps=4096, min_p_store=0.05, reuse_engines=False)
+    srv = S.Server(Xd.data_ptr(), N_TOTAL, M_TOTAL, coh, max_slots=1, **kw)
+    alone = {q.rid: srv.run([q], realtime=False)[0].rows for q in reqs}
+    srv.close()
+    srv = S.Server(Xd.data_ptr(), N_TOTAL, M_TOTAL, coh, max_slots=4, **kw)
+    mix = srv.run(reqs, realtime=False)
+    assert not srv._idle
+    srv.close()
+    for res in mix:
+        a, b = alone[res.rid], res.rows
+        for f in ("trait", "snp", "r2", "n_used", "mask", "B", "SE", "T"):
+            np.testing.assert_array_equal(getattr(a, f), getattr(b, f), err_msg=f"request {res.rid} field {f}")
+        assert res.phases["engine"] > 0
 
 
 @pytest.mark.parametrize("prec", [E.PLAIN, E.MIXED])

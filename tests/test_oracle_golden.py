@@ -20,7 +20,7 @@ def test_oracle_matches_reference(case, tag, tmp_path):
     pre, extra = GU.materialise(case, str(tmp_path))
     run = GU.manifest()["cases"][case]["runs"][tag]
     s = GU.settings_for(run["flags"], extra)
-    if case == "r2_missing" or (case, tag) == ("r1_dosf", "nz"):
+    if case in ("r2_missing", "r3_missing") or (case, tag) == ("r1_dosf", "nz"):
         s.quirk_r2 = True        # the reference's r >= 2 downdate (the linear model keeps r = 2 columns)
     res, inp = O.run_files(pre + "XL", pre + "XR", pre + "Y", s, keep_dense=True)
     ref = GU.golden_rows(case, tag)

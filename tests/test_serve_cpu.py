@@ -14,6 +14,7 @@ class FakeEngine:
     live = 0
     peak = 0
     created = 0
+    closed = 0
     lock = threading.Lock()
 
     def __init__(self, cohort, t_cap, nbytes):
@@ -37,7 +38,8 @@ class FakeEngine:
         return self.nbytes
 
     def close(self):
-        pass
+        with FakeEngine.lock:
+            FakeEngine.closed += 1
 
 
 def _setup(n_req=40, cohorts=5, seed=3):
@@ -53,10 +55,10 @@ def _setup(n_req=40, cohorts=5, seed=3):
     return coh, reqs
 
 
-def _server(coh, budget, slots, nbytes=3 << 20):
-    FakeEngine.live = FakeEngine.peak = FakeEngine.created = 0
+def _server(coh, budget, slots, nbytes=3 << 20, reuse=True):
+    FakeEngine.live = FakeEngine.peak = FakeEngine.created = FakeEngine.closed = 0
     srv = S.Server(0, 200, 2000, coh, budget_bytes=budget, max_slots=slots, min_p_store=1e-3,
-                   engine_factory=lambda c, t: FakeEngine(c, t, nbytes))
+                   engine_factory=lambda c, t: FakeEngine(c, t, nbytes), reuse_engines=reuse)
     srv.footprint = lambda req: 4 << 20
     return srv
 
@@ -109,3 +111,29 @@ def test_warm_creates_the_engines_of_every_cohort():
     assert FakeEngine.created == 6
     assert sorted(s.cohort for s in srv._idle) == [0, 0, 1, 1, 2, 2]
     assert srv.max_slots == 2
+
+
+def test_per_request_engines_are_created_inside_the_request_and_released():
+    """Every request with its own subsample: an engine per request, created inside its
+    latency (the 'engine' phase) and released when its results are out; nothing idles."""
+    coh, reqs = _setup(n_req=25, cohorts=25)
+    for q in reqs:
+        q.cohort = q.rid
+    srv = _server(coh, budget=24 << 20, slots=4, reuse=False)
+    res = srv.run(reqs, realtime=True)
+    assert FakeEngine.created == len(reqs) == FakeEngine.closed
+    assert not srv._idle and srv.evictions == 0
+    assert all("engine" in r.phases and "release" in r.phases for r in res)
+    assert FakeEngine.peak <= 4
+
+
+def test_requests_draw_their_own_subsample_and_covariates():
+    w = S.ServeWorkload(n_total=5000, m_total=50000, requests=6, n_lo=500, n_hi=5000, seed=7)
+    rng = np.random.Generator(np.random.PCG64(1))
+    cohorts = [S.draw_cohort(rng, w, c) for c in range(6)]
+    sizes = {c.rows.size for c in cohorts}
+    assert len(sizes) > 1 and all(w.n_lo <= n <= w.n_hi for n in sizes)
+    for c in cohorts:
+        assert np.all(np.diff(c.rows) > 0) and c.rows.max() < w.n_total
+        assert w.l_lo <= c.XL.shape[0] <= w.l_hi and c.XL.shape[1] == c.rows.size
+        assert np.all(c.XL[0] == 1.0)
