@@ -7,6 +7,7 @@
 // (src/AIOwrapper.cpp:257-340, 1213-1275).
 //
 //   ref_model_driver XL XR Y OUT NGPRED MODEL [FACTORS|-] [-b] [-f] [-i] [-v INTER | -w INTER] [-t THREADS]
+//                    [-k] [-x EXCLUDE]
 //
 // MODEL is the reference's Settings::model: 0 additive, 1 dominant,
 // 2 recessive, 3 custom linear, 4 custom additive, -1 none.  -v sets the
@@ -36,6 +37,7 @@ int main(int argc, char** argv) {
     params.model = std::atoi(argv[6]);
     params.dosages = params.model >= 0;
     int a = 7;
+    bool keep_dep = true;   // -k: interactions without the SNP column itself (the reference's keep_depVar = false)
     if (a < argc && argv[a][0] != '-') params.fname_dosages = argv[a++];
     else if (a < argc && std::strcmp(argv[a], "-") == 0) ++a;
     for (; a < argc; ++a) {
@@ -43,6 +45,8 @@ int main(int argc, char** argv) {
         else if (!std::strcmp(argv[a], "-f")) params.storePInd = true;
         else if (!std::strcmp(argv[a], "-i")) params.disp_cov = true;
         else if (!std::strcmp(argv[a], "-t") && a + 1 < argc) params.threads = std::atoi(argv[++a]);
+        else if (!std::strcmp(argv[a], "-x") && a + 1 < argc) params.fname_excludelist = argv[++a];
+        else if (!std::strcmp(argv[a], "-k")) keep_dep = false;
         else if (!std::strcmp(argv[a], "-v") && a + 1 < argc) {
             params.fname_interactions = argv[++a];
             params.use_interactions = true;
@@ -55,6 +59,7 @@ int main(int argc, char** argv) {
             params.use_multiple_interaction_sets = true;
         }
     }
+    if (params.use_interactions) params.keep_depVar = keep_dep;
     blas_set_num_threads(params.threads);
     Outputs out = {0};
     alg.solve(params, out, P_NEQ_B_OPT_MD);
