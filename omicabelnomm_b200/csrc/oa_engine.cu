@@ -28,6 +28,7 @@
 #include "oa_kernels.cuh"
 #include "oa_launch.h"
 #include "oa_lean.cuh"
+#include "oa_trace.h"
 
 using namespace oa;
 
@@ -542,6 +543,7 @@ oa_status flush_h2d(oa_engine* e, const H2DBatch& b) {
 }
 
 oa_status set_traits_impl(oa_engine* e, const float* y, int32_t t, bool device_ptr) {
+    OA_TRACE("oa_set_traits: grouping, row sets, residuals");
     if (!e->have_cov) {
         set_err("oa_set_traits before oa_set_covariates");
         return OA_ERR_STATE;
@@ -1185,6 +1187,7 @@ oa_status enqueue_block(oa_engine* e, const float* xr, int mb, bool host_input, 
             OA_CU(cudaGetLastError());
             X = e->Xmodel.p;
         }
+        OA_TRACE("chunk: statistics and GEMM launches");
         OA_CU(cudaMemsetAsync(e->has_nan.p, 0, sizeof(int), e->st));
         OA_CU(rec(e->sev0[c]));
         OA_CHECK(stats_dispatch<R>(e, X, ldx, xrows, mbc));
@@ -1322,6 +1325,7 @@ long long slots_needed(const oa_engine* e, long long mb, long long t, long long 
 template <int R>
 oa_status run_snps_impl(oa_engine* e, const float* xr, int32_t mb, bool host_input, bool results_on_host,
                         oa_rows* out) {
+    OA_TRACE("oa_run_snps");
     if (e->t <= 0) {
         set_err("oa_run_snps before oa_set_traits");
         return OA_ERR_STATE;
@@ -1370,7 +1374,11 @@ oa_status run_snps_impl(oa_engine* e, const float* xr, int32_t mb, bool host_inp
         }
     }
     if (e->cfg.disp_cov) OA_CHECK(e->marks.ensure((mb + e->chunk - 1) / e->chunk));
-    OA_CHECK(run_block<R>(e, xr, mb, host_input));
+    {
+        OA_TRACE("SNP block on the device");
+        OA_CHECK(run_block<R>(e, xr, mb, host_input));
+    }
+    OA_TRACE("stored rows: sort, copy back, convert");
     unsigned long long cnt[5];
     OA_CU(cudaMemcpyAsync(e->h_cnt, e->counters.p, sizeof cnt, cudaMemcpyDeviceToHost, e->st));
     OA_CU(cudaStreamSynchronize(e->st));
@@ -1539,6 +1547,7 @@ oa_status run_snps_any(oa_engine* e, const float* xr, int32_t mb, bool host_inpu
 // timed by the device time of its per-block kernels (statistics stage +
 // main GEMM, CUDA events per chunk) on the caller's sample block.
 oa_status autotune_impl(oa_engine* e, const float* xr, int mb, oa_tuning* best_out) {
+    OA_TRACE("oa_autotune");
     if (e->t <= 0) {
         set_err("oa_autotune before oa_set_traits");
         return OA_ERR_STATE;
@@ -1790,6 +1799,7 @@ oa_status oa_engine_destroy(oa_engine* e) {
 
 oa_status oa_set_covariates(oa_engine* e, const float* xl) {
     clear_stale_error(__func__);
+    OA_TRACE("oa_set_covariates: QR and rank check");
     if (!e || !xl) {
         set_err("null argument");
         return OA_ERR_ARG;

@@ -23,6 +23,7 @@
 
 #include <cuda_runtime.h>
 
+#include "oa_trace.h"
 #include "omicabel_b200.h"
 
 extern "C" void oa__set_error(const char* msg);  // oa_engine.cu: shared oa_last_error() text
@@ -511,6 +512,7 @@ void oa_default_settings(oa_settings* s) {
 }
 
 oa_status oa_solve(const oa_settings* S, oa_outputs* out) {
+    OA_TRACE("oa_solve");
     if (!S || !out) {
         herr("null argument");
         return OA_ERR_ARG;
@@ -905,6 +907,7 @@ oa_status oa_solve(const oa_settings* S, oa_outputs* out) {
         st = oa_set_traits(eng, Yblk.data(), tcur);
         if (st != OA_OK) break;
         auto read_call = [&](int c, int b) {
+            OA_TRACE("read SNP block (.fvd)");
             const int s0 = c * call_snps, cnt = std::min(call_snps, m - s0);
             return read_columns(fr, FR.elem_bytes(), fileN, (size_t)(first + s0) * file_r, (size_t)cnt * file_r, runs,
                                 n, pin[b], scratch[b], dscratch[b]);
@@ -948,6 +951,7 @@ oa_status oa_solve(const oa_settings* S, oa_outputs* out) {
             for (int64_t q = 0; q < rows.count; ++q) gsnp[q] = rows.snp[q] + s0;
             oa_rows g = rows;
             g.snp = gsnp.data();
+            OA_TRACE("write outputs");
             for (int k = 0; k < nblk; ++k) W.write_block(g, blocks[k], y0, s0 + k * mb_ref);
             if (verbose) {
                 putchar('*');
