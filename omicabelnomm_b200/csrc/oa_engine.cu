@@ -293,6 +293,8 @@ struct oa_engine {
     DBuf<float> Qr;
     bool have_cov = false;
     bool center = false;   // the first covariate is constant: SNP columns are taken relative to their means
+    bool fuse_split = false;  // the tensor-core GEMMs split FP32 columns in shared memory where they can
+    bool fused_last = false;  // the last enqueued chunk took the fused form
     // traits
     int t = 0;
     DBuf<float> Yraw, Yt;
@@ -902,8 +904,20 @@ oa_status lean_plan(oa_engine* e) {
     return OA_OK;
 }
 
+// The tensor-core GEMMs of this chunk read its FP32 columns and split them
+// into BF16 hi / lo in shared memory, so the statistics kernel writes no
+// split copy to HBM: mixed form, pre-GEMM statistics path with at most 128
+// pre-GEMM columns, contiguous 16-byte aligned columns of a multiple of 4
+// floats, and a GEMM shape that has a fused form (OA_FUSED_SPLIT at engine
+// creation: 1 takes the fused forms, 0 keeps the split copy).
+bool fused_chunk(const oa_engine* e, const float* X, size_t ldx, const int* xrows) {
+    return e->fuse_split && e->cfg.precision == OA_MIXED_BF16X3 && e->use_pre && e->c2 <= 128 && !xrows &&
+           ldx == (size_t)e->n && e->n % 4 == 0 && (reinterpret_cast<uintptr_t>(X) & 15) == 0 &&
+           oa_gemm_tc_fusable(e->variant, e->t);
+}
+
 template <int R>
-oa_status stats_pre(oa_engine* e, const float* X, size_t ldx, const int* xrows, int mbc) {
+oa_status stats_pre(oa_engine* e, const float* X, size_t ldx, const int* xrows, int mbc, bool fused) {
     const int spb = e->lp.spb;
     const size_t smem = e->lp.smem;
     LeanArgs A{};
@@ -926,7 +940,7 @@ oa_status stats_pre(oa_engine* e, const float* X, size_t ldx, const int* xrows, 
     A.D = e->D.p;
     A.Dset = e->Dset.p;
     const bool mixed = e->cfg.precision == OA_MIXED_BF16X3;
-    A.write_split = mixed ? 1 : 0;
+    A.write_split = mixed && !fused ? 1 : 0;
     A.use_xi = e->lp.xi ? 1 : 0;
     A.center = e->center ? 1 : 0;
     A.Xhi = e->Xhi.p;
@@ -938,7 +952,10 @@ oa_status stats_pre(oa_engine* e, const float* X, size_t ldx, const int* xrows, 
     OA_CU(oa_launch_snp_lean(R, spb, A, grid, smem, e->st));
     ++e->launches;
     const int ldc = e->chunk * R;
-    if (mixed)
+    if (fused)
+        OA_CU(oa_launch_pre_tcf(X, ldx, e->n, mbc * R, e->mean.p, e->center ? 1 : 0, e->B2hi.p, e->B2lo.p, e->c2,
+                                e->n_pad, e->C2T.p, ldc, reinterpret_cast<int*>(e->counters.p + 3), e->st));
+    else if (mixed)
         OA_CU(oa_launch_pre_tc(e->Xhi.p, e->Xlo.p, mbc * R, e->B2hi.p, e->B2lo.p, e->c2, e->n_pad, e->C2T.p, ldc,
                                reinterpret_cast<int*>(e->counters.p + 3), e->st));
     else
@@ -974,8 +991,8 @@ oa_status stats_pre(oa_engine* e, const float* X, size_t ldx, const int* xrows, 
 }
 
 template <int R>
-oa_status stats_dispatch(oa_engine* e, const float* X, size_t ldx, const int* xrows, int mbc) {
-    if (e->use_pre) return stats_pre<R>(e, X, ldx, xrows, mbc);
+oa_status stats_dispatch(oa_engine* e, const float* X, size_t ldx, const int* xrows, int mbc, bool fused) {
+    if (e->use_pre) return stats_pre<R>(e, X, ldx, xrows, mbc, fused);
     if constexpr (R > 4) {
         set_err("internal: the gather-path statistics kernel takes at most 4 columns per SNP");
         return OA_ERR_STATE;
@@ -1058,9 +1075,14 @@ CovArgs cov_args(oa_engine* e, int mbc) {
 }
 
 template <int R>
-oa_status gemm_dispatch(oa_engine* e, const float* X, int mbc, int snp_base) {
+oa_status gemm_dispatch(oa_engine* e, const float* X, int mbc, int snp_base, bool fused) {
     EpiArgs E = epi_args(e, mbc, snp_base);
-    if (e->cfg.precision == OA_PLAIN_FP32) {
+    if (fused) {
+        OA_CU(oa_launch_gemm_tcf(R, e->raster, X, (size_t)e->n, e->n, mbc * R, e->mean.p, e->center ? 1 : 0,
+                                 e->Yhi.p, e->Ylo.p, e->t, e->n_pad, E, reinterpret_cast<int*>(e->counters.p + 3),
+                                 e->st));
+        e->last_name = e->t > 128 ? "k_gemm_tc2f" : "k_gemm_tcf";
+    } else if (e->cfg.precision == OA_PLAIN_FP32) {
         // X'y~ does not change when a column is shifted (y~ is orthogonal to the intercept on the
         // observed rows): the main GEMM reads the dosages as they are, imputing NaN only
         OA_CU(oa_launch_gemm_simt(R, X, (size_t)e->n, mbc * R, e->Yt.p, (size_t)e->n_pad, e->t, e->n, e->mean.p,
@@ -1190,14 +1212,16 @@ oa_status enqueue_block(oa_engine* e, const float* xr, int mb, bool host_input, 
         OA_TRACE("chunk: statistics and GEMM launches");
         OA_CU(cudaMemsetAsync(e->has_nan.p, 0, sizeof(int), e->st));
         OA_CU(rec(e->sev0[c]));
-        OA_CHECK(stats_dispatch<R>(e, X, ldx, xrows, mbc));
+        const bool fused = fused_chunk(e, X, ldx, xrows);
+        e->fused_last = fused;
+        OA_CHECK(stats_dispatch<R>(e, X, ldx, xrows, mbc, fused));
         OA_CU(rec(e->sev1[c]));
         if (cov) {
             k_mark<<<1, 1, 0, e->st>>>(e->counters.p, e->marks.p + c);
             ++e->launches;
         }
         OA_CU(rec(e->cev0[c]));
-        OA_CHECK(gemm_dispatch<R>(e, X, mbc, c0));
+        OA_CHECK(gemm_dispatch<R>(e, X, mbc, c0, fused));
         OA_CU(rec(e->cev1[c]));
         if (host_input) OA_CU(cudaEventRecord(e->ev_used[c & 1], e->st));
         if (cov) {
@@ -1299,6 +1323,7 @@ oa_status run_block(oa_engine* e, const float* xr, int mb, bool host_input) {
         e->block_ms = cudaEventElapsedTime(&bms, e->k0, e->k1) == cudaSuccess ? bms : 0.f;
         cudaGetLastError();
         e->last_name = e->cfg.precision == OA_PLAIN_FP32                ? "k_gemm_simt"
+                       : e->fused_last                                  ? (e->t > 128 ? "k_gemm_tc2f" : "k_gemm_tcf")
                        : (e->t > 128 && e->variant >= 3) ? "k_gemm_tc2"
                                                           : "k_gemm_tc";
         return OA_OK;
@@ -1705,6 +1730,7 @@ oa_status oa_engine_create(const oa_config* cfg, oa_engine** out) {
     if (const char* v = getenv("OA_LEAN_NBUF")) e->lean_nbuf = atoi(v) == 1 ? 1 : (atoi(v) == 2 ? 2 : 0);
     if (const char* v = getenv("OA_LEAN_XI")) e->lean_xi = atoi(v) == 0 ? 0 : (atoi(v) == 1 ? 1 : -1);
     e->chunk = std::min(cfg->max_snps, e->req.chunk_snps > 0 ? e->req.chunk_snps : 16384 / e->r);
+    if (const char* v = getenv("OA_FUSED_SPLIT")) e->fuse_split = v[0] != '0';
     const char* gr = getenv("OA_GRAPHS");
     e->use_graphs = !(gr && gr[0] == '0');
     // the copy stream of host SNP blocks is created on first use: a device-resident

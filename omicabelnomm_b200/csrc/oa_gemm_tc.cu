@@ -185,6 +185,20 @@ __device__ __forceinline__ void tmem_ld8(uint32_t taddr, uint32_t (&v)[8]) {
     asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 }
 
+// Named barrier 1 of the epilogue warps, OR-reducing `flag` over them: every
+// warp gets the same answer, so a decision to leave the tile loop (an abort
+// seen by some warps and not yet by others) is taken by all of them together
+// and none is left waiting at the next barrier.
+__device__ __forceinline__ bool epi_bar_any(int flag) {
+    uint32_t r;
+    asm volatile(
+        "{\n\t.reg .pred p, q;\n\tsetp.ne.u32 q, %1, 0;\n\tbar.red.or.pred p, 1, %2, q;\n\tselp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(r)
+        : "r"(flag), "n"(EPI_WARPS * 32)
+        : "memory");
+    return r != 0;
+}
+
 // Statistics epilogue of one accumulator tile for one warp: lane = row
 // (SNP column i of the block, `lead` on its first column), BN traits from
 // TMEM at taddr (32 columns per tcgen05.ld), trait constants from tps.
@@ -426,8 +440,7 @@ k_gemm_tc(const __grid_constant__ CUtensorMap mAhi, const __grid_constant__ CUte
         for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
             const int m0 = (raster == 2 ? tile % m_tiles : tile / n_tiles) * BM;
             const int n0 = (raster == 2 ? tile / m_tiles : tile % n_tiles) * BN;
-            asm volatile("bar.sync 1, %0;" ::"n"(EPI_WARPS * 32) : "memory");   // previous tile's readers are done
-            if (abort_sh) break;
+            if (epi_bar_any(abort_sh)) break;   // previous tile's readers are done; one decision for all warps
             // trait constants of this tile (the main loop of the tile is still running)
             for (int q = et; q < BN; q += EPI_WARPS * 32)
                 if (n0 + q < t) tps[q] = load_trait(E, n0 + q);
@@ -696,8 +709,7 @@ k_gemm_tc2(const __grid_constant__ CUtensorMap mAhi, const __grid_constant__ CUt
             int m0, n0;
             tile_mn(tile, m0, n0);
             m0 += (int)rank * BM;
-            asm volatile("bar.sync 1, %0;" ::"n"(EPI_WARPS * 32) : "memory");
-            if (abort_sh) break;
+            if (epi_bar_any(abort_sh)) break;
             for (int q = et; q < BN; q += EPI_WARPS * 32)
                 if (n0 + q < t) tps[q] = load_trait(E, n0 + q);
             const int row = m0 + lg * 32 + lane;
@@ -730,6 +742,679 @@ k_gemm_tc2(const __grid_constant__ CUtensorMap mAhi, const __grid_constant__ CUt
     fence_before();
     __syncthreads();
     cluster_sync();       // no CTA frees TMEM or leaves while its pair may still touch it
+    if (warp == 1) {
+        fence_after();
+        asm volatile("tcgen05.dealloc.cta_group::2.sync.aligned.b32 %0, %1;" ::"r"(tmem_base), "r"(TMEM_COLS));
+    }
+    if (threadIdx.x == 0 && abort_sh) atomicExch(err, 1);
+}
+
+// ---------------------------------------------------------------------------
+// Fused-operand forms: the X operand is read as FP32 (the SNP columns as the
+// statistics kernel read them) and split into BF16 hi / lo in shared memory,
+// so that no split copy of X is written to or read back from HBM.
+//
+// Per K-block the producer TMA-loads the FP32 tile of this CTA's 128 rows
+// (64 K-elements, 256 bytes per row, no swizzle) into one of FSLOTS staging
+// slots, and the B tiles (the traits' or the pre-GEMM columns' hi / lo, split
+// once per trait block) into the K-block's stage.  Two converter warps wait
+// for the FP32 tile, form each value as the statistics kernel's split does
+// (NaN -> the column's fill value, else x - shift; shift = the column mean
+// when the columns are centred, else 0; fill = 0 when centred, else the
+// imputation mean), split it (hi = bf16(x), lo = bf16(x - hi)) and store hi
+// and lo in the stage's A tiles in the UMMA K-major 128-byte-swizzle layout;
+// then they release the FP32 slot and signal the MMA issuer.  The results are
+// bit-identical to the split path (same FP32 values, same roundings).
+// The MMA issuer waits for the stage's B bytes and for the converters.
+// Warps: 0 producer, 1 MMA issuer, 2..9 epilogue, 10..11 converters.
+// Every wait is bounded as in the split forms; drains keep the 2 s bound.
+// ---------------------------------------------------------------------------
+constexpr int CONV_WARPS = 2;
+constexpr int NUM_THREADS_F = NUM_THREADS + 32 * CONV_WARPS;   // 384
+constexpr int FBK = 64;                                        // K-block of the fused forms (128-byte swizzle)
+
+template <int STAGES_, int BN_, int FSLOTS_, bool PAIR>
+struct ShapeF {
+    static constexpr int BK = FBK, STAGES = STAGES_, BN = BN_, FSLOTS = FSLOTS_;
+    static constexpr int A_BYTES = BM * BK * 2;                         // one of hi / lo
+    static constexpr int B_ROWS = PAIR ? BN / 2 : BN;                   // this CTA's rows of B
+    static constexpr int B_BYTES = B_ROWS * BK * 2;
+    static constexpr int STAGE_BYTES = 2 * A_BYTES + 2 * B_BYTES;
+    static constexpr int AF_BYTES = BM * BK * 4;                        // one FP32 staging slot
+    static constexpr size_t SMEM_BYTES = 1024 + (size_t)STAGES * STAGE_BYTES + (size_t)FSLOTS * AF_BYTES +
+                                         (size_t)BN * sizeof(TraitP) + 2 * BM * sizeof(float);
+    static constexpr uint64_t LAYOUT = 2u;                              // SWIZZLE_128B
+    static constexpr uint32_t SBO = 1024u;
+    static constexpr uint32_t TMEM_COLS = PAIR ? 512u : (2 * BN <= 128 ? 128u : (2 * BN <= 256 ? 256u : 512u));
+    static constexpr uint32_t IDESC = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(BN >> 3) << 17) |
+                                      ((uint32_t)((PAIR ? 256 : BM) >> 4) << 24);
+    static_assert(SMEM_BYTES <= 227u * 1024u, "shared memory of the fused form");
+};
+
+// Converter side of one K-block: FP32 tile (BM x 64, 256 B rows) -> BF16 hi/lo
+// tiles (K-major, 128-byte swizzle: the 16-byte chunk j of row r sits at
+// chunk j ^ (r & 7) of its 128-byte row).  ctid: 0..CONV_WARPS*32-1.
+__device__ __forceinline__ void convert_a_tile(const float* __restrict__ fa, uint8_t* ahi, uint8_t* alo,
+                                               const float* __restrict__ shift, const float* __restrict__ fill,
+                                               int ctid) {
+    constexpr int CT = CONV_WARPS * 32;
+#pragma unroll 4
+    for (int it = 0; it < BM * (FBK / 4) / CT; ++it) {
+        const int q = it * CT + ctid;
+        const int row = q >> 4, c = q & 15;   // 16 float4 per 64-element row
+        const float4 v = *reinterpret_cast<const float4*>(fa + row * FBK + c * 4);
+        const float sh = shift[row], fl = fill[row];
+        const float e0 = isnan(v.x) ? fl : v.x - sh, e1 = isnan(v.y) ? fl : v.y - sh;
+        const float e2 = isnan(v.z) ? fl : v.z - sh, e3 = isnan(v.w) ? fl : v.w - sh;
+        const __nv_bfloat162 h01 = __floats2bfloat162_rn(e0, e1), h23 = __floats2bfloat162_rn(e2, e3);
+        const float2 f01 = __bfloat1622float2(h01), f23 = __bfloat1622float2(h23);
+        const __nv_bfloat162 l01 = __floats2bfloat162_rn(e0 - f01.x, e1 - f01.y);
+        const __nv_bfloat162 l23 = __floats2bfloat162_rn(e2 - f23.x, e3 - f23.y);
+        const uint32_t off = (uint32_t)row * 128u + ((((uint32_t)c >> 1) ^ ((uint32_t)row & 7u)) << 4) +
+                             (((uint32_t)c & 1u) << 3);
+        *reinterpret_cast<uint2*>(ahi + off) =
+            make_uint2(*reinterpret_cast<const uint32_t*>(&h01), *reinterpret_cast<const uint32_t*>(&h23));
+        *reinterpret_cast<uint2*>(alo + off) =
+            make_uint2(*reinterpret_cast<const uint32_t*>(&l01), *reinterpret_cast<const uint32_t*>(&l23));
+    }
+}
+
+// Per-row shift and fill of rows [r0, r0 + BM) (rows at or past xrows: 0).
+__device__ __forceinline__ void load_shift_fill(const float* __restrict__ colmean, int center, int r0, int xrows,
+                                                float* shift, float* fill, int ctid) {
+    for (int q = ctid; q < BM; q += CONV_WARPS * 32) {
+        const int row = r0 + q;
+        const float mu = row < xrows ? colmean[row] : 0.f;
+        shift[q] = center ? mu : 0.f;
+        fill[q] = center ? 0.f : mu;
+    }
+}
+
+__device__ __forceinline__ void conv_bar() {
+    asm volatile("bar.sync 2, %0;" ::"n"(CONV_WARPS * 32) : "memory");
+}
+// Named barrier 2 of the converter warps, AND-reducing `ok` over them: both
+// warps take the same decision to go on or to leave after a wait.
+__device__ __forceinline__ bool conv_bar_all(int ok) {
+    uint32_t r;
+    asm volatile(
+        "{\n\t.reg .pred p, q;\n\tsetp.ne.u32 q, %1, 0;\n\tbar.red.and.pred p, 2, %2, q;\n\tselp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(r)
+        : "r"(ok), "n"(CONV_WARPS * 32)
+        : "memory");
+    return r != 0;
+}
+__device__ __forceinline__ void fence_proxy_async_smem() {
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+
+// 1-SM fused form (statistics epilogue, or the store epilogue of the pre-GEMM).
+template <int R, class SH, bool STORE>
+__global__ void __launch_bounds__(NUM_THREADS_F, 1)
+k_gemm_tcf(const __grid_constant__ CUtensorMap mAf, const __grid_constant__ CUtensorMap mBhi,
+           const __grid_constant__ CUtensorMap mBlo, const float* __restrict__ colmean, int center, int xrows,
+           int t, int nk, EpiArgs E, float* __restrict__ cout, int ldc, int raster, int* err) {
+    constexpr int BK = SH::BK, STAGES = SH::STAGES, BN = SH::BN, FSLOTS = SH::FSLOTS;
+    constexpr uint32_t TMEM_COLS = SH::TMEM_COLS;
+    constexpr int A_BYTES = SH::A_BYTES, B_BYTES = SH::B_BYTES, STAGE_BYTES = SH::STAGE_BYTES;
+    constexpr int AF_BYTES = SH::AF_BYTES;
+    extern __shared__ uint8_t smem_raw[];
+    uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~(uintptr_t)1023);
+    uint8_t* fslots = smem + (size_t)STAGES * STAGE_BYTES;
+    TraitP* tps = reinterpret_cast<TraitP*>(fslots + (size_t)FSLOTS * AF_BYTES);
+    float* shift = reinterpret_cast<float*>(tps + BN);
+    float* fill = shift + BM;
+    __shared__ __align__(8) uint64_t full_b[STAGES], empty_bar[STAGES], conv_bar_s[STAGES], fa_full[FSLOTS],
+        fa_empty[FSLOTS], acc_full[2], acc_empty[2], done_bar;
+    __shared__ uint32_t tmem_base_sh;
+    __shared__ volatile int abort_sh;
+
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int m_tiles = (xrows + BM - 1) / BM, n_tiles = (t + BN - 1) / BN;
+    const int ntiles = m_tiles * n_tiles;
+
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < STAGES; ++s) {
+            mbar_init(&full_b[s], 1);
+            mbar_init(&empty_bar[s], 1);
+            mbar_init(&conv_bar_s[s], CONV_WARPS);
+        }
+        for (int f = 0; f < FSLOTS; ++f) {
+            mbar_init(&fa_full[f], 1);
+            mbar_init(&fa_empty[f], CONV_WARPS);
+        }
+        for (int a = 0; a < 2; ++a) {
+            mbar_init(&acc_full[a], 1);
+            mbar_init(&acc_empty[a], EPI_WARPS * 32);
+        }
+        mbar_init(&done_bar, 1);
+        abort_sh = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (warp == 1) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(su32(&tmem_base_sh)),
+                     "r"(TMEM_COLS));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+    }
+    fence_before();
+    __syncthreads();
+    fence_after();
+    const uint32_t tmem_base = tmem_base_sh;
+
+    auto stage_ptr = [&](int s, int which) -> uint8_t* {   // 0 Ahi, 1 Alo, 2 Bhi, 3 Blo
+        uint8_t* b = smem + (size_t)s * STAGE_BYTES;
+        return which < 2 ? b + which * A_BYTES : b + 2 * A_BYTES + (which - 2) * B_BYTES;
+    };
+    auto tile_mn = [&](int tile, int& m0, int& n0) {
+        m0 = (raster == 2 ? tile % m_tiles : tile / n_tiles) * BM;
+        n0 = (raster == 2 ? tile / m_tiles : tile % n_tiles) * BN;
+    };
+
+    if (warp == 0) {
+        if (lane == 0) {
+            // ---------------- TMA producer ----------------
+            int s = 0, f = 0;
+            uint32_t ph = 0, fph = 0;
+            uint32_t pend_par[FSLOTS];
+            bool pend[FSLOTS];
+            uint32_t bpend_par[STAGES];
+            bool bpend[STAGES];
+            for (int q = 0; q < FSLOTS; ++q) pend[q] = false;
+            for (int q = 0; q < STAGES; ++q) bpend[q] = false;
+            bool ok = true;
+            int pt = blockIdx.x, pkb = 0;
+            auto prefetch_next = [&]() {
+                if (pt >= ntiles) return;
+                int pm0, pn0;
+                tile_mn(pt, pm0, pn0);
+                tma_prefetch_2d(&mAf, pkb * BK, pm0);
+                if (++pkb == nk) {
+                    pkb = 0;
+                    pt += gridDim.x;
+                }
+            };
+            for (int q = 0; q < pf_blocks<BK>(); ++q) prefetch_next();
+            for (int tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x) {
+                int m0, n0;
+                tile_mn(tile, m0, n0);
+                for (int kb = 0; kb < nk; ++kb) {
+                    if (!mbar_wait(&empty_bar[s], ph ^ 1u, &abort_sh) || !mbar_wait(&fa_empty[f], fph ^ 1u, &abort_sh)) {
+                        ok = false;
+                        break;
+                    }
+                    mbar_expect_tx(&fa_full[f], AF_BYTES);
+                    tma_load_2d(&mAf, &fa_full[f], fslots + (size_t)f * AF_BYTES, kb * BK, m0);
+                    pend[f] = true;
+                    pend_par[f] = fph;
+                    mbar_expect_tx(&full_b[s], 2 * B_BYTES);
+                    tma_load_2d(&mBhi, &full_b[s], stage_ptr(s, 2), kb * BK, n0);
+                    tma_load_2d(&mBlo, &full_b[s], stage_ptr(s, 3), kb * BK, n0);
+                    bpend[s] = true;
+                    bpend_par[s] = ph;
+                    prefetch_next();
+                    if (++s == STAGES) {
+                        s = 0;
+                        ph ^= 1u;
+                    }
+                    if (++f == FSLOTS) {
+                        f = 0;
+                        fph ^= 1u;
+                    }
+                }
+            }
+            if (!ok) {   // drain our own copies before the shared memory goes away
+                for (int q = 0; q < FSLOTS; ++q)
+                    if (pend[q]) mbar_drain(&fa_full[q], pend_par[q]);
+                for (int q = 0; q < STAGES; ++q)
+                    if (bpend[q]) mbar_drain(&full_b[q], bpend_par[q]);
+            }
+        }
+    } else if (warp == 1) {
+        if (lane == 0) {
+            // ---------------- MMA issuer ----------------
+            int s = 0, acc = 0;
+            uint32_t ph = 0, aph = 0;
+            bool ok = true, issued = false;
+            for (int tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x) {
+                if (!mbar_wait(&acc_empty[acc], aph ^ 1u, &abort_sh)) break;
+                fence_after();
+                const uint32_t d_tmem = tmem_base + (uint32_t)(acc * BN);
+                for (int kb = 0; kb < nk; ++kb) {
+                    if (!mbar_wait(&full_b[s], ph, &abort_sh) || !mbar_wait(&conv_bar_s[s], ph, &abort_sh)) {
+                        ok = false;
+                        break;
+                    }
+                    fence_after();
+                    const uint32_t ahi = su32(stage_ptr(s, 0)), alo = su32(stage_ptr(s, 1));
+                    const uint32_t bhi = su32(stage_ptr(s, 2)), blo = su32(stage_ptr(s, 3));
+#pragma unroll
+                    for (int kk = 0; kk < BK / 16; ++kk) {
+                        const uint32_t off = (uint32_t)kk * 32u;
+                        const uint64_t dah = smem_desc<SH>(ahi + off), dal = smem_desc<SH>(alo + off);
+                        const uint64_t dbh = smem_desc<SH>(bhi + off), dbl = smem_desc<SH>(blo + off);
+                        mma_bf16(d_tmem, dah, dbh, SH::IDESC, (kb > 0 || kk > 0) ? 1u : 0u);
+                        mma_bf16(d_tmem, dah, dbl, SH::IDESC, 1u);
+                        mma_bf16(d_tmem, dal, dbh, SH::IDESC, 1u);
+                    }
+                    issued = true;
+                    mma_commit(&empty_bar[s]);
+                    if (++s == STAGES) {
+                        s = 0;
+                        ph ^= 1u;
+                    }
+                }
+                if (!ok) break;
+                mma_commit(&acc_full[acc]);
+                if (++acc == 2) {
+                    acc = 0;
+                    aph ^= 1u;
+                }
+            }
+            if (issued) {   // all MMAs of this CTA complete before TMEM is freed
+                mma_commit(&done_bar);
+                mbar_drain(&done_bar, 0);
+            }
+        }
+    } else if (warp >= 2 + EPI_WARPS) {
+        // ---------------- converters ----------------
+        const int ctid = threadIdx.x - 32 * (2 + EPI_WARPS);
+        int s = 0, f = 0;
+        uint32_t ph = 0, fph = 0;
+        bool ok = true;
+        for (int tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x) {
+            int m0, n0;
+            tile_mn(tile, m0, n0);
+            conv_bar();   // the previous tile's conversions have read shift / fill
+            load_shift_fill(colmean, center, m0, xrows, shift, fill, ctid);
+            conv_bar();
+            for (int kb = 0; kb < nk; ++kb) {
+                int okw = 1;
+                if (lane == 0) okw = mbar_wait(&fa_full[f], fph, &abort_sh) ? 1 : 0;
+                okw = __shfl_sync(0xffffffffu, okw, 0);
+                if (!conv_bar_all(okw)) {   // both converter warps leave together
+                    ok = false;
+                    break;
+                }
+                mbar_try(&fa_full[f], fph);
+                convert_a_tile(reinterpret_cast<const float*>(fslots + (size_t)f * AF_BYTES), stage_ptr(s, 0),
+                               stage_ptr(s, 1), shift, fill, ctid);
+                fence_proxy_async_smem();   // the stores reach the tensor cores' (async) view
+                __syncwarp();
+                if (lane == 0) {
+                    mbar_arrive(&fa_empty[f]);
+                    mbar_arrive(&conv_bar_s[s]);
+                }
+                if (++s == STAGES) {
+                    s = 0;
+                    ph ^= 1u;
+                }
+                if (++f == FSLOTS) {
+                    f = 0;
+                    fph ^= 1u;
+                }
+            }
+        }
+        (void)ph;
+    } else if constexpr (STORE) {
+        // ---------------- store epilogue ----------------
+        const int lg = warp & 3;
+        const int cb = ((warp - 2) >> 2) * (BN / 2);
+        int acc = 0;
+        uint32_t aph = 0;
+        for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+            if (abort_sh) break;
+            int m0, n0;
+            tile_mn(tile, m0, n0);
+            int ok = 1;
+            if (lane == 0) ok = mbar_wait(&acc_full[acc], aph, &abort_sh) ? 1 : 0;
+            ok = __shfl_sync(0xffffffffu, ok, 0);
+            if (!ok) break;
+            mbar_try(&acc_full[acc], aph);
+            fence_after();
+            const int row = m0 + lg * 32 + lane;
+            for (int c0 = cb; c0 < cb + BN / 2 && n0 + c0 < t; c0 += 32) {
+                uint32_t v[32];
+                tmem_ld32(tmem_base + ((uint32_t)(lg * 32) << 16) + (uint32_t)(acc * BN + c0), v);
+                const int qmax = min(32, t - n0 - c0);
+                if (row < xrows)
+#pragma unroll
+                    for (int q = 0; q < 32; ++q)
+                        if (q < qmax) cout[(size_t)(n0 + c0 + q) * ldc + row] = __uint_as_float(v[q]);
+            }
+            fence_before();
+            mbar_arrive(&acc_empty[acc]);
+            if (++acc == 2) {
+                acc = 0;
+                aph ^= 1u;
+            }
+        }
+    } else {
+        // ---------------- statistics epilogue ----------------
+        const int ew = warp - 2;
+        const int lg = warp & 3;
+        const int et = ew * 32 + lane;
+        const int cb = (ew >> 2) * (BN / 2);
+        Emitter em;
+        int acc = 0;
+        uint32_t aph = 0;
+        for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+            int m0, n0;
+            tile_mn(tile, m0, n0);
+            if (epi_bar_any(abort_sh)) break;
+            for (int q = et; q < BN; q += EPI_WARPS * 32)
+                if (n0 + q < t) tps[q] = load_trait(E, n0 + q);
+            const int row = m0 + lg * 32 + lane;
+            const bool lead = ((lane & (R - 1)) == 0) && (row < xrows);
+            const int i = row / R;
+            float vx[R];
+#pragma unroll
+            for (int a = 0; a < R; ++a) vx[a] = lead ? E.varx[(size_t)i * R + a] : 1.f;
+            asm volatile("bar.sync 1, %0;" ::"n"(EPI_WARPS * 32) : "memory");
+            int ok = 1;
+            if (lane == 0) ok = mbar_wait(&acc_full[acc], aph, &abort_sh) ? 1 : 0;
+            ok = __shfl_sync(0xffffffffu, ok, 0);
+            if (ok) {
+                mbar_try(&acc_full[acc], aph);
+                fence_after();
+                epi_columns<R, BN>(E, tmem_base + ((uint32_t)(lg * 32) << 16) + (uint32_t)(acc * BN), n0, t, lane,
+                                   i, lead, vx, tps, cb, cb + BN / 2, em);
+                fence_before();
+                mbar_arrive(&acc_empty[acc]);
+            }
+            if (++acc == 2) {
+                acc = 0;
+                aph ^= 1u;
+            }
+        }
+        epi_retire<R>(E, em);
+    }
+
+    fence_before();
+    __syncthreads();
+    if (warp == 1) {
+        fence_after();
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem_base), "r"(TMEM_COLS));
+    }
+    if (threadIdx.x == 0 && abort_sh) atomicExch(err, 1);
+}
+
+// Cluster-scope acquire form of the bounded wait: the converters of both CTAs
+// of a pair arrive (release, cluster scope) on the leader's barrier after
+// writing their A tiles, which the leader's MMAs then read.
+__device__ __forceinline__ bool mbar_try_cluster(uint64_t* b, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.acquire.cluster.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(ok)
+        : "r"(su32(b)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+__device__ __forceinline__ bool mbar_wait_cluster(uint64_t* b, uint32_t parity, volatile int* abort_flag) {
+    if (mbar_try_cluster(b, parity)) return true;
+    const unsigned long long t0 = gtimer(), lim = c_wait_ns;
+    while (true) {
+        if (mbar_try_cluster(b, parity)) return true;
+        if (*abort_flag) return false;
+        if (gtimer() - t0 > lim) {
+            *abort_flag = 1;
+            return false;
+        }
+    }
+}
+
+// CTA-pair fused form (statistics epilogue): as k_gemm_tc2, with each CTA's
+// A rows read as FP32 and split by its converter warps; the leader's MMA
+// issuer waits for the B bytes of both CTAs (leader's full barrier) and for
+// the converters of both CTAs (leader's convert barrier).
+template <int R, class SH>
+__global__ void __launch_bounds__(NUM_THREADS_F, 1)
+k_gemm_tc2f(const __grid_constant__ CUtensorMap mAf, const __grid_constant__ CUtensorMap mBhi,
+            const __grid_constant__ CUtensorMap mBlo, const float* __restrict__ colmean, int center, int xrows, int t,
+            int nk, EpiArgs E, int raster, int* err) {
+    constexpr int BK = SH::BK, STAGES = SH::STAGES, BN = SH::BN, FSLOTS = SH::FSLOTS;
+    constexpr uint32_t TMEM_COLS = SH::TMEM_COLS;
+    constexpr int A_BYTES = SH::A_BYTES, B_BYTES = SH::B_BYTES, STAGE_BYTES = SH::STAGE_BYTES;
+    constexpr int AF_BYTES = SH::AF_BYTES;
+    extern __shared__ uint8_t smem_raw[];
+    uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~(uintptr_t)1023);
+    uint8_t* fslots = smem + (size_t)STAGES * STAGE_BYTES;
+    TraitP* tps = reinterpret_cast<TraitP*>(fslots + (size_t)FSLOTS * AF_BYTES);
+    float* shift = reinterpret_cast<float*>(tps + BN);
+    float* fill = shift + BM;
+    __shared__ __align__(8) uint64_t full_b[STAGES], empty_bar[STAGES], conv_bar_s[STAGES], fa_full[FSLOTS],
+        fa_empty[FSLOTS], acc_full[2], acc_empty[2], done_bar;
+    __shared__ uint32_t tmem_base_sh;
+    __shared__ volatile int abort_sh;
+
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const uint32_t rank = cluster_rank();
+    const bool leader = rank == 0;
+    const int pair = blockIdx.x >> 1, npairs = gridDim.x >> 1;
+    const int m_tiles = (xrows + 2 * BM - 1) / (2 * BM), n_tiles = (t + BN - 1) / BN;
+    const int ntiles = m_tiles * n_tiles;
+
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < STAGES; ++s) {
+            mbar_init(&full_b[s], 1);
+            mbar_init(&empty_bar[s], 1);
+            mbar_init(&conv_bar_s[s], 2 * CONV_WARPS);   // leader's copy: the converter warps of both CTAs
+        }
+        for (int f = 0; f < FSLOTS; ++f) {
+            mbar_init(&fa_full[f], 1);
+            mbar_init(&fa_empty[f], CONV_WARPS);
+        }
+        for (int a = 0; a < 2; ++a) {
+            mbar_init(&acc_full[a], 1);
+            mbar_init(&acc_empty[a], 2 * EPI_WARPS);
+        }
+        mbar_init(&done_bar, 1);
+        abort_sh = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (warp == 1) {
+        asm volatile("tcgen05.alloc.cta_group::2.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(su32(&tmem_base_sh)),
+                     "r"(TMEM_COLS));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::2.sync.aligned;");
+    }
+    fence_before();
+    __syncthreads();
+    cluster_sync();
+    fence_after();
+    const uint32_t tmem_base = tmem_base_sh;
+
+    auto stage_ptr = [&](int s, int which) -> uint8_t* {
+        uint8_t* b = smem + (size_t)s * STAGE_BYTES;
+        return which < 2 ? b + which * A_BYTES : b + 2 * A_BYTES + (which - 2) * B_BYTES;
+    };
+    auto tile_mn = [&](int tile, int& m0, int& n0) {
+        m0 = (raster == 2 ? tile % m_tiles : tile / n_tiles) * 2 * BM;
+        n0 = (raster == 2 ? tile / m_tiles : tile % n_tiles) * BN;
+    };
+
+    if (warp == 0) {
+        if (lane == 0) {
+            // ---------------- TMA producer (both CTAs) ----------------
+            int s = 0, f = 0;
+            uint32_t ph = 0, fph = 0;
+            uint32_t pend_par[FSLOTS];
+            bool pend[FSLOTS];
+            for (int q = 0; q < FSLOTS; ++q) pend[q] = false;
+            bool ok = true;
+            int pt = pair, pkb = 0;
+            auto prefetch_next = [&]() {
+                if (pt >= ntiles) return;
+                int pm0, pn0;
+                tile_mn(pt, pm0, pn0);
+                tma_prefetch_2d(&mAf, pkb * BK, pm0 + (int)rank * BM);
+                if (++pkb == nk) {
+                    pkb = 0;
+                    pt += npairs;
+                }
+            };
+            for (int q = 0; q < pf_blocks<BK>(); ++q) prefetch_next();
+            for (int tile = pair; tile < ntiles && ok; tile += npairs) {
+                int m0, n0;
+                tile_mn(tile, m0, n0);
+                const int ma = m0 + (int)rank * BM, nb = n0 + (int)rank * (BN / 2);
+                for (int kb = 0; kb < nk; ++kb) {
+                    if (!mbar_wait(&empty_bar[s], ph ^ 1u, &abort_sh) || !mbar_wait(&fa_empty[f], fph ^ 1u, &abort_sh)) {
+                        ok = false;
+                        break;
+                    }
+                    mbar_expect_tx(&fa_full[f], AF_BYTES);
+                    tma_load_2d(&mAf, &fa_full[f], fslots + (size_t)f * AF_BYTES, kb * BK, ma);
+                    pend[f] = true;
+                    pend_par[f] = fph;
+                    const uint32_t fb = map_to_rank(&full_b[s], 0);
+                    if (leader) mbar_expect_tx(&full_b[s], 2 * 2 * B_BYTES);
+                    tma_load_2d_pair(&mBhi, fb, stage_ptr(s, 2), kb * BK, nb);
+                    tma_load_2d_pair(&mBlo, fb, stage_ptr(s, 3), kb * BK, nb);
+                    prefetch_next();
+                    if (++s == STAGES) {
+                        s = 0;
+                        ph ^= 1u;
+                    }
+                    if (++f == FSLOTS) {
+                        f = 0;
+                        fph ^= 1u;
+                    }
+                }
+            }
+            if (!ok) {   // own FP32 copies; the leader's full barriers see both CTAs' B copies
+                for (int q = 0; q < FSLOTS; ++q)
+                    if (pend[q]) mbar_drain(&fa_full[q], pend_par[q]);
+                if (leader)
+                    for (int q = 0; q < STAGES; ++q) mbar_drain(&full_b[q], 0), mbar_drain(&full_b[q], 1);
+            }
+        }
+    } else if (warp == 1) {
+        if (lane == 0 && leader) {
+            // ---------------- MMA issuer (leader CTA) ----------------
+            int s = 0, acc = 0;
+            uint32_t ph = 0, aph = 0;
+            bool ok = true, issued = false;
+            for (int tile = pair; tile < ntiles && ok; tile += npairs) {
+                if (!mbar_wait(&acc_empty[acc], aph ^ 1u, &abort_sh)) break;
+                fence_after();
+                const uint32_t d_tmem = tmem_base + (uint32_t)(acc * BN);
+                for (int kb = 0; kb < nk; ++kb) {
+                    if (!mbar_wait(&full_b[s], ph, &abort_sh) || !mbar_wait_cluster(&conv_bar_s[s], ph, &abort_sh)) {
+                        ok = false;
+                        break;
+                    }
+                    fence_after();
+                    const uint32_t ahi = su32(stage_ptr(s, 0)), alo = su32(stage_ptr(s, 1));
+                    const uint32_t bhi = su32(stage_ptr(s, 2)), blo = su32(stage_ptr(s, 3));
+#pragma unroll
+                    for (int kk = 0; kk < BK / 16; ++kk) {
+                        const uint32_t off = (uint32_t)kk * 32u;
+                        const uint64_t dah = smem_desc<SH>(ahi + off), dal = smem_desc<SH>(alo + off);
+                        const uint64_t dbh = smem_desc<SH>(bhi + off), dbl = smem_desc<SH>(blo + off);
+                        mma_bf16_pair(d_tmem, dah, dbh, SH::IDESC, (kb > 0 || kk > 0) ? 1u : 0u);
+                        mma_bf16_pair(d_tmem, dah, dbl, SH::IDESC, 1u);
+                        mma_bf16_pair(d_tmem, dal, dbh, SH::IDESC, 1u);
+                    }
+                    issued = true;
+                    mma_commit_pair(&empty_bar[s]);
+                    if (++s == STAGES) {
+                        s = 0;
+                        ph ^= 1u;
+                    }
+                }
+                if (!ok) break;
+                mma_commit_pair(&acc_full[acc]);
+                if (++acc == 2) {
+                    acc = 0;
+                    aph ^= 1u;
+                }
+            }
+            if (issued) mma_commit_pair(&done_bar);   // both CTAs learn when the last MMA has completed
+        }
+        if (lane == 0) mbar_drain(&done_bar, 0);      // (a CTA pair that issued nothing waits out the bound once)
+    } else if (warp >= 2 + EPI_WARPS) {
+        // ---------------- converters (both CTAs, own 128 rows) ----------------
+        const int ctid = threadIdx.x - 32 * (2 + EPI_WARPS);
+        int s = 0, f = 0;
+        uint32_t fph = 0;
+        bool ok = true;
+        for (int tile = pair; tile < ntiles && ok; tile += npairs) {
+            int m0, n0;
+            tile_mn(tile, m0, n0);
+            conv_bar();
+            load_shift_fill(colmean, center, m0 + (int)rank * BM, xrows, shift, fill, ctid);
+            conv_bar();
+            for (int kb = 0; kb < nk; ++kb) {
+                int okw = 1;
+                if (lane == 0) okw = mbar_wait(&fa_full[f], fph, &abort_sh) ? 1 : 0;
+                okw = __shfl_sync(0xffffffffu, okw, 0);
+                if (!conv_bar_all(okw)) {
+                    ok = false;
+                    break;
+                }
+                mbar_try(&fa_full[f], fph);
+                convert_a_tile(reinterpret_cast<const float*>(fslots + (size_t)f * AF_BYTES), stage_ptr(s, 0),
+                               stage_ptr(s, 1), shift, fill, ctid);
+                fence_proxy_async_smem();
+                __syncwarp();
+                if (lane == 0) {
+                    mbar_arrive(&fa_empty[f]);
+                    mbar_arrive_cluster(map_to_rank(&conv_bar_s[s], 0));
+                }
+                if (++s == STAGES) s = 0;
+                if (++f == FSLOTS) {
+                    f = 0;
+                    fph ^= 1u;
+                }
+            }
+        }
+    } else {
+        // ---------------- epilogue (both CTAs, own 128 rows) ----------------
+        const int ew = warp - 2;
+        const int lg = warp & 3;
+        const int et = ew * 32 + lane;
+        const int cb = (ew >> 2) * (BN / 2);
+        Emitter em;
+        int acc = 0;
+        uint32_t aph = 0;
+        for (int tile = pair; tile < ntiles; tile += npairs) {
+            int m0, n0;
+            tile_mn(tile, m0, n0);
+            m0 += (int)rank * BM;
+            if (epi_bar_any(abort_sh)) break;
+            for (int q = et; q < BN; q += EPI_WARPS * 32)
+                if (n0 + q < t) tps[q] = load_trait(E, n0 + q);
+            const int row = m0 + lg * 32 + lane;
+            const bool lead = ((lane & (R - 1)) == 0) && (row < xrows);
+            const int i = row / R;
+            float vx[R];
+#pragma unroll
+            for (int a = 0; a < R; ++a) vx[a] = lead ? E.varx[(size_t)i * R + a] : 1.f;
+            asm volatile("bar.sync 1, %0;" ::"n"(EPI_WARPS * 32) : "memory");
+            int ok = 1;
+            if (lane == 0) ok = mbar_wait(&acc_full[acc], aph, &abort_sh) ? 1 : 0;
+            ok = __shfl_sync(0xffffffffu, ok, 0);
+            if (ok) {
+                mbar_try(&acc_full[acc], aph);
+                fence_after();
+                epi_columns<R, BN>(E, tmem_base + ((uint32_t)(lg * 32) << 16) + (uint32_t)(acc * BN), n0, t, lane,
+                                   i, lead, vx, tps, cb, cb + BN / 2, em);
+                fence_before();
+                __syncwarp();
+                if (lane == 0) mbar_arrive_cluster(map_to_rank(&acc_empty[acc], 0));
+            }
+            if (++acc == 2) {
+                acc = 0;
+                aph ^= 1u;
+            }
+        }
+        epi_retire<R>(E, em);
+    }
+
+    fence_before();
+    __syncthreads();
+    cluster_sync();
     if (warp == 1) {
         fence_after();
         asm volatile("tcgen05.dealloc.cta_group::2.sync.aligned.b32 %0, %1;" ::"r"(tmem_base), "r"(TMEM_COLS));
@@ -855,6 +1540,105 @@ static cudaError_t go_any(int variant, int raster, const __nv_bfloat16* Xhi, con
     return go<R, Shape<32, 4>, false>(Xhi, Xlo, xrows, Yhi, Ylo, t, n_pad, E, nullptr, 0, raster, err, st);
 }
 
+
+// FP32 K-major matrix of `rows` rows of ld floats (k_valid of them read, the
+// rest of each 64-wide K-block filled with zeros), boxes of 64 x 128, no
+// swizzle (the converter warps read it); ld * 4 and the base must be 16-byte
+// multiples.
+static bool make_map_f32(CUtensorMap* m, const float* ptr, int rows, int k_valid, size_t ld) {
+    EncodeTiledFn fn = encode_fn();
+    if (!fn || rows <= 0 || k_valid <= 0 || (ld * 4) % 16 != 0 || (reinterpret_cast<uintptr_t>(ptr) & 15) != 0)
+        return false;
+    const cuuint64_t gdim[2] = {(cuuint64_t)k_valid, (cuuint64_t)rows};
+    const cuuint64_t gstride[1] = {(cuuint64_t)ld * 4};
+    const cuuint32_t box[2] = {(cuuint32_t)FBK, (cuuint32_t)BM};
+    const cuuint32_t estride[2] = {1, 1};
+    return fn(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, const_cast<float*>(ptr), gdim, gstride, box, estride,
+              CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+              CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+template <int R, class SH, bool STORE>
+static cudaError_t go_f(const float* X, size_t ldx, int n, int xrows, const float* colmean, int center,
+                        const __nv_bfloat16* Bhi, const __nv_bfloat16* Blo, int t, int n_pad, const EpiArgs& E,
+                        float* cout, int ldc, int raster, int* err, cudaStream_t st) {
+    constexpr int BN = SH::BN;
+    CUtensorMap a_f, b_hi, b_lo;
+    if (!make_map_f32(&a_f, X, xrows, n, ldx) || !make_map(&b_hi, Bhi, t, n_pad, BN, SH::BK) ||
+        !make_map(&b_lo, Blo, t, n_pad, BN, SH::BK))
+        return cudaErrorInvalidValue;
+    static int attr_done[64];
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (!attr_done[dev & 63]) {   // once per device, never during a stream capture
+        cudaError_t e = cudaFuncSetAttribute(k_gemm_tcf<R, SH, STORE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             (int)SH::SMEM_BYTES);
+        if (e != cudaSuccess) return e;
+        attr_done[dev & 63] = 1;
+    }
+    const int ntiles = ((xrows + BM - 1) / BM) * ((t + BN - 1) / BN);
+    const int sms = sm_count();
+    const int grid = ntiles < sms ? ntiles : sms;
+    k_gemm_tcf<R, SH, STORE><<<grid, NUM_THREADS_F, SH::SMEM_BYTES, st>>>(
+        a_f, b_hi, b_lo, colmean, center, xrows, t, n_pad / SH::BK, E, cout, ldc, raster, err);
+    return cudaGetLastError();
+}
+
+template <int R, class SH>
+static cudaError_t go2_f(const float* X, size_t ldx, int n, int xrows, const float* colmean, int center,
+                         const __nv_bfloat16* Yhi, const __nv_bfloat16* Ylo, int t, int n_pad, const EpiArgs& E,
+                         int raster, int* err, cudaStream_t st) {
+    CUtensorMap a_f, b_hi, b_lo;
+    if (!make_map_f32(&a_f, X, xrows, n, ldx) || !make_map(&b_hi, Yhi, t, n_pad, SH::BN / 2, SH::BK) ||
+        !make_map(&b_lo, Ylo, t, n_pad, SH::BN / 2, SH::BK))
+        return cudaErrorInvalidValue;
+    static int attr_done[64];
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (!attr_done[dev & 63]) {
+        cudaError_t e = cudaFuncSetAttribute(k_gemm_tc2f<R, SH>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             (int)SH::SMEM_BYTES);
+        if (e != cudaSuccess) return e;
+        attr_done[dev & 63] = 1;
+    }
+    const int ntiles = ((xrows + 2 * BM - 1) / (2 * BM)) * ((t + SH::BN - 1) / SH::BN);
+    const int pairs = std::min(ntiles, sm_count() / 2);
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(2 * pairs, 1, 1);
+    cfg.blockDim = dim3(NUM_THREADS_F, 1, 1);
+    cfg.dynamicSmemBytes = SH::SMEM_BYTES;
+    cfg.stream = st;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = 2;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, k_gemm_tc2f<R, SH>, a_f, b_hi, b_lo, colmean, center, xrows, t, n_pad / SH::BK, E,
+                              raster, err);
+}
+
+using FNarrow64 = ShapeF<3, 64, 2, false>;
+using FNarrow128 = ShapeF<2, 128, 2, false>;
+using FPair = ShapeF<2, 256, 2, true>;
+
+// Fused forms of the statistics GEMM: trait blocks of at most 128 traits on
+// the 1-SM narrow tiles, wider ones on CTA pairs (the fused pair form serves
+// pipeline variants 3 and 4).
+template <int R>
+static cudaError_t go_any_f(int raster, const float* X, size_t ldx, int n, int xrows, const float* colmean, int center,
+                            const __nv_bfloat16* Yhi, const __nv_bfloat16* Ylo, int t, int n_pad, const EpiArgs& E,
+                            int* err, cudaStream_t st) {
+    if (t <= 64)
+        return go_f<R, FNarrow64, false>(X, ldx, n, xrows, colmean, center, Yhi, Ylo, t, n_pad, E, nullptr, 0, raster,
+                                         err, st);
+    if (t <= 128)
+        return go_f<R, FNarrow128, false>(X, ldx, n, xrows, colmean, center, Yhi, Ylo, t, n_pad, E, nullptr, 0,
+                                          raster, err, st);
+    return go2_f<R, FPair>(X, ldx, n, xrows, colmean, center, Yhi, Ylo, t, n_pad, E, raster, err, st);
+}
+
 }  // namespace tc
 
 cudaError_t oa_set_wait_limit_tc(unsigned long long ns) { return cudaMemcpyToSymbol(tc::c_wait_ns, &ns, sizeof ns); }
@@ -879,6 +1663,34 @@ cudaError_t oa_launch_pre_tc(const __nv_bfloat16* Xhi, const __nv_bfloat16* Xlo,
     if (c2 <= 128)
         return tc::go<1, tc::Shape<64, 3, 128>, true>(Xhi, Xlo, xrows, Bhi, Blo, c2, n_pad, none, C, ldc, 1, err, st);
     return tc::go<1, tc::Shape<64, 2, 256>, true>(Xhi, Xlo, xrows, Bhi, Blo, c2, n_pad, none, C, ldc, 1, err, st);
+}
+
+
+bool oa_gemm_tc_fusable(int variant, int t) { return t <= 128 || variant >= 3; }
+
+cudaError_t oa_launch_gemm_tcf(int R, int raster, const float* X, size_t ldx, int n, int xrows, const float* colmean,
+                               int center, const __nv_bfloat16* Yhi, const __nv_bfloat16* Ylo, int t, int n_pad,
+                               const EpiArgs& E, int* err, cudaStream_t st) {
+    switch (R) {
+        case 1: return tc::go_any_f<1>(raster, X, ldx, n, xrows, colmean, center, Yhi, Ylo, t, n_pad, E, err, st);
+        case 2: return tc::go_any_f<2>(raster, X, ldx, n, xrows, colmean, center, Yhi, Ylo, t, n_pad, E, err, st);
+        case 4: return tc::go_any_f<4>(raster, X, ldx, n, xrows, colmean, center, Yhi, Ylo, t, n_pad, E, err, st);
+        case 8: return tc::go_any_f<8>(raster, X, ldx, n, xrows, colmean, center, Yhi, Ylo, t, n_pad, E, err, st);
+        default: return cudaErrorInvalidValue;
+    }
+}
+
+cudaError_t oa_launch_pre_tcf(const float* X, size_t ldx, int n, int xrows, const float* colmean, int center,
+                              const __nv_bfloat16* Bhi, const __nv_bfloat16* Blo, int c2, int n_pad, float* C, int ldc,
+                              int* err, cudaStream_t st) {
+    const EpiArgs none{};
+    if (c2 <= 64)
+        return tc::go_f<1, tc::FNarrow64, true>(X, ldx, n, xrows, colmean, center, Bhi, Blo, c2, n_pad, none, C, ldc, 1,
+                                                err, st);
+    if (c2 <= 128)
+        return tc::go_f<1, tc::FNarrow128, true>(X, ldx, n, xrows, colmean, center, Bhi, Blo, c2, n_pad, none, C, ldc,
+                                                 1, err, st);
+    return cudaErrorInvalidValue;
 }
 
 }  // namespace oa

@@ -93,3 +93,68 @@ def test_mixed_narrow_trait_tiles(t):
     assert np.nanmax(np.abs(tp - tm)) < 1e-3
     np.testing.assert_array_equal(np.isnan(tp), np.isnan(tm))
     assert rp.tests == rm.tests == t * 2333
+
+
+def _mixed_dense(ds, r, monkeypatch, fused, **env):
+    monkeypatch.setenv("OA_FUSED_SPLIT", "1" if fused else "0")
+    for k, v in env.items():
+        monkeypatch.setenv(k, v)
+    eng, rows, dense = engine_run(ds, r, precision=E.MIXED)
+    name = eng.last_kernel_ms()[1]
+    eng.close()
+    return rows, dense, name
+
+
+@pytest.mark.parametrize("case", ["narrow64", "narrow128", "pair", "pair_r2", "pair_r4", "uncentred", "variant3"])
+def test_fused_split_gemms_give_the_split_copy_bits(case, monkeypatch):
+    """The fused forms (FP32 columns split into BF16 hi / lo in shared memory by
+    converter warps, no split copy in HBM) give bit-identical statistics to the
+    split-copy forms: every trait-tile width (1-SM 64 / 128 columns, CTA pairs),
+    r = 1, 2, 4, NaN dosages, centred and uncentred columns, ragged SNP and trait
+    edges, several tiles per CTA."""
+    from test_gpu_parity import _multicol
+    env = {}
+    r = 1
+    if case == "narrow64":
+        ds = synth.generate(synth.scaled(0, n=1000, m=1500, t=40, l=4, miss_mode="patterns", n_patterns=3,
+                                         xr_nan_frac=0.005, seed=71))
+    elif case == "narrow128":
+        ds = synth.generate(synth.scaled(0, n=1024, m=1300, t=120, l=5, miss_mode="patterns", n_patterns=4,
+                                         xr_nan_frac=0.005, seed=72))
+    elif case in ("pair", "variant3"):
+        ds = synth.generate(synth.scaled(0, n=996, m=2333, t=517, l=4, miss_mode="patterns", n_patterns=5,
+                                         xr_nan_frac=0.005, seed=73))
+        if case == "variant3":
+            env["OA_TC_VARIANT"] = "3"
+    elif case == "pair_r2":
+        r = 2
+        ds = synth.generate(synth.scaled(0, n=800, m=700, t=300, l=4, r=2, miss_mode="patterns", n_patterns=3,
+                                         seed=74))
+    elif case == "pair_r4":
+        r = 4
+        ds = _multicol(4, 75, n=600, m=150, t=270)
+    else:
+        env["OA_CENTER"] = "0"
+        ds = synth.generate(synth.scaled(0, n=1000, m=900, t=300, l=4, miss_mode="patterns", n_patterns=3,
+                                         xr_nan_frac=0.005, seed=76))
+    rows_f, dense_f, name_f = _mixed_dense(ds, r, monkeypatch, True, **env)
+    rows_s, dense_s, name_s = _mixed_dense(ds, r, monkeypatch, False, **env)
+    assert name_f.endswith("f") and not name_s.endswith("f"), (name_f, name_s)
+    for a, b in zip(dense_f, dense_s):
+        np.testing.assert_array_equal(a, b)
+    np.testing.assert_array_equal(rows_f.trait, rows_s.trait)
+    np.testing.assert_array_equal(rows_f.snp, rows_s.snp)
+    np.testing.assert_array_equal(rows_f.T, rows_s.T)
+
+
+def test_fused_split_falls_back_when_columns_are_not_16_byte_multiples(monkeypatch):
+    """n % 4 != 0: the FP32 columns cannot be TMA tiles; the split copy is used and the
+    numbers match the FP64 oracle as before."""
+    ds = synth.generate(synth.scaled(0, n=1001, m=600, t=200, seed=77))
+    rows, (b, se, tt, r2), name = _mixed_dense(ds, 1, monkeypatch, True)
+    assert not name.endswith("f")
+    res, _, _ = oracle_dense(ds, 1)
+    D = res.dense
+    ok = ~D.singular
+    t_ref = D.tstat[:, :, res.l:][ok]
+    assert np.all(np.abs(tt[ok] - t_ref) <= T_ABS_MIXED + T_REL_MIXED * np.abs(t_ref))
