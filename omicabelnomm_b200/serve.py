@@ -164,22 +164,28 @@ class Server:
                 return self._idle.pop(q)
         return None
 
-    def _engine(self, cohort: Cohort, t_cap: int):
-        """The default engine factory: an engine over the cohort's rows of the resident matrix."""
+    def _engine(self, cohort: Cohort, t_cap: int, snps: Optional[int] = None):
+        """The default engine factory: an engine over the cohort's rows of the resident matrix,
+        for trait blocks of up to t_cap traits and SNP ranges of up to `snps` SNPs."""
         n, l = cohort.rows.size, cohort.XL.shape[0]
-        eng = E.Engine(n, l, 1, t_cap, self.max_snps, precision=self.precision, device=self.device,
+        snps = snps or self.max_snps
+        eng = E.Engine(n, l, 1, t_cap, snps, precision=self.precision, device=self.device,
                        min_t_store=E.t_threshold(self.min_p_store), min_r2_store=1e-6)
         if self.chunk > 0:
             eng.set_tuning(chunk_snps=self.chunk)
         eng.set_covariates(cohort.XL)
         eng.set_snp_rows(cohort.rows, self.n_total)
-        eng.reserve(t_cap, self.max_snps)     # no pinned allocations once it serves
+        eng.reserve(t_cap, snps)              # no allocations once it scans
         return eng
 
     def _new_engine(self, req: Request) -> _Slot:
         c = self.cohorts[req.cohort]
-        t_cap = max(req.t, self.t_cap_min)
-        eng = self.engine_factory(c, t_cap)
+        if self.reuse_engines:               # kept for later requests: room for any of them
+            t_cap = max(req.t, self.t_cap_min)
+            eng = self.engine_factory(c, t_cap)
+        else:                                # this request only: its own sizes
+            t_cap = req.t
+            eng = self.engine_factory(c, t_cap, req.nsnp)
         return _Slot(engine=eng, cohort=req.cohort, l=c.XL.shape[0], t_cap=t_cap)
 
     # -- one request ----------------------------------------------------------

@@ -58,7 +58,7 @@ def _setup(n_req=40, cohorts=5, seed=3):
 def _server(coh, budget, slots, nbytes=3 << 20, reuse=True):
     FakeEngine.live = FakeEngine.peak = FakeEngine.created = FakeEngine.closed = 0
     srv = S.Server(0, 200, 2000, coh, budget_bytes=budget, max_slots=slots, min_p_store=1e-3,
-                   engine_factory=lambda c, t: FakeEngine(c, t, nbytes), reuse_engines=reuse)
+                   engine_factory=lambda c, t, snps=None: FakeEngine(c, t, nbytes), reuse_engines=reuse)
     srv.footprint = lambda req: 4 << 20
     return srv
 
