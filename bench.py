@@ -430,18 +430,16 @@ def serve_section(args, dev, local):
     reqs, cohorts = S.make_requests(w, None, dev, keep)
     ww = S.ServeWorkload(m_total=args.serve_m, requests=16, seed=w.seed + 17)
     warm_reqs, warm_cohorts = S.make_requests(ww, None, dev, keep)
+    for q in warm_reqs:                      # their own ids beside the timed requests'
+        q.rid += 1_000_000
+        q.cohort += 1_000_000
+    cohorts.update({c + 1_000_000: v for c, v in warm_cohorts.items()})
     torch.cuda.synchronize()
     free, _ = torch.cuda.mem_get_info(dev)
     budget = int(free - (6 << 30))
-
-    def server(coh):
-        return S.Server(G.data_ptr(), w.n_total, w.m_total, coh, device=local, budget_bytes=budget, max_slots=8,
-                        min_p_store=1e-3, reuse_engines=False)
-
-    srv = server(warm_cohorts)
-    srv.run(warm_reqs, realtime=False)      # start-up, not timed: pools and kernel attributes
-    srv.close()
-    srv = server(cohorts)
+    srv = S.Server(G.data_ptr(), w.n_total, w.m_total, cohorts, device=local, budget_bytes=budget, max_slots=8,
+                   min_p_store=1e-3, reuse_engines=False)
+    srv.run(warm_reqs, realtime=False)      # start-up, not timed: fills the buffer pools
     clocks = ClockSampler(local)
     clocks.start()
     res = srv.run(reqs, realtime=True)
