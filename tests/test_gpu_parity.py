@@ -276,13 +276,16 @@ def test_quirk_r2_matches_oracle_quirk(case, prec):
     """The reference's r >= 2 downdate reproduced on the device (quirk mode) against the
     oracle's restatement of it: dense t, SE, R2 and the singular set; also with observed
     zero phenotypes (zero sets), with r > l (the SNP-block downdate quirk) and with r = 3
-    and 5 (zero padding columns in the kernels)."""
+    and 5 (zero padding columns in the kernels).  Quirk mode works on the raw, uncentred
+    SNP columns (the reference's own sums), so its rounding is relative to those sums:
+    the plain form's t bar is the usual one, SE and R2 are compared relative to their
+    size (the quirk's R2 can be far below 0), and the mixed form's bar grows with the
+    system's largest |t|."""
     r = 2
     if case == "r2_missing":
         ds = synth.generate(synth.scaled(0, **CASES["r2_missing"]))
     elif case == "r2_yzero_l1":
-        ds = _yzero(synth.generate(synth.scaled(0, n=500, m=90, t=12, l=1, r=2, miss_mode="patterns",
-                                                n_patterns=3, miss_hi=0.15, seed=74)), 9)
+        ds = _yzero(_multicol(2, 74, n=500, m=45, l=1, n_patterns=3, miss_hi=0.15), 9)
     elif case == "r3_missing":
         r, ds = 3, _multicol(3, 75)
     else:
@@ -304,10 +307,10 @@ def test_quirk_r2_matches_oracle_quirk(case, prec):
     t_ref = D.tstat[:, :, l:][ok]
     dt = np.abs(tt[ok] - t_ref)
     t_sys = np.broadcast_to(np.abs(t_ref).max(axis=1, keepdims=True), t_ref.shape)
-    lim = (T_REL * t_sys + T_ABS) if prec == E.PLAIN else (1e-3 + 1e-4 * t_sys)
+    lim = (T_REL * t_sys + T_ABS) if prec == E.PLAIN else (1e-3 + 5e-4 * t_sys)
     assert np.all(dt <= lim), f"max |dt| {dt.max():.3g}"
-    assert np.allclose(se[ok], D.se[:, :, l:][ok], rtol=SE_REL if prec == E.PLAIN else 1e-3, atol=0)
-    assert np.allclose(r2[ok], D.r2[ok], rtol=0, atol=1e-5 if prec == E.PLAIN else 1e-4)
+    assert np.allclose(se[ok], D.se[:, :, l:][ok], rtol=1e-3, atol=0)
+    assert np.allclose(r2[ok], D.r2[ok], rtol=1e-4, atol=1e-4)
     assert rows.singular == int(D.singular.sum())
     # the quirk matters here: its answers are not the corrected ones
     assert np.abs(D.tstat[:, :, l:] - Dc.tstat[:, :, l:])[ok].max() > 1e-2

@@ -3,15 +3,14 @@ benchmark workloads (full n, t, l, r and pattern structure; a slice of the
 SNPs):
   * omics scale (n = 10,000, t = 1,000, 20 patterns, r = 1);
   * the same with a near-collinear covariate (age2 = age + N(0, 1e-3)) and
-    1 % of SNPs with MAF in [0.005, 0.01];
+    1 % of SNPs with MAF in [0.005, 0.01]; and 5,000 SNPs all from that
+    low-MAF band (as many as the full workload holds) with that covariate;
   * batched interactions (n = 8,000, l = 5, r = 2: SNP x sex and SNP,
     t = 2,000 in 150 Zipf-sized patterns).
 Bars, with |t|max the largest |t| among the r SNP terms of the same test:
-plain |dt| <= 1e-4 |t|max + 1e-4; mixed |dt| <= 1e-3 for r = 1 and
-|dt| <= 1e-3 + 1e-4 |t|max for r = 2 (the rounding of one column's sums
-reaches the other coefficient through the 2 x 2 Schur inverse, scaled by the
-conditioning of the correlated SNP x sex and SNP columns).
-With OA_PRECISION_REPORT set, the measured errors are written there as JSON."""
+plain |dt| <= 1e-4 |t|max + 1e-4; mixed |dt| <= 1e-3 (the target of the
+mixed form on these workloads).  With OA_PRECISION_REPORT set, the measured
+errors are written there as JSON."""
 import json
 import os
 
@@ -27,6 +26,9 @@ pytestmark = pytest.mark.gpu
 SAMPLES = {
     "omics_n10000_t1000_g20": (1, dict(m=128)),
     "collinear_lowmaf_n10000_t1000": (2, dict(m=128)),
+    # as many SNPs with MAF in [0.005, 0.01] as the full workload holds (1 % of 500,000), with the
+    # near-collinear covariate: the systems the FP64 Schur complements are there to protect
+    "all_lowmaf_collinear_n10000_t1000": (2, dict(m=5000, low_maf_frac=1.0)),
     "interaction_r2_n8000_t2000_g150": (3, dict(m=48)),
 }
 REPORT = {}
@@ -40,10 +42,8 @@ def _errors(name, w, ds, res, prec, D, ok, t_ref):
     t_sys = np.broadcast_to(np.abs(t_ref).max(axis=1, keepdims=True), t_ref.shape)
     if prec == E.PLAIN:
         lim = 1e-4 * t_sys + 1e-4
-    elif w.r == 1:
-        lim = np.full_like(t_ref, 1e-3)
     else:
-        lim = 1e-3 + 1e-4 * t_sys
+        lim = np.full_like(t_ref, 1e-3)
     # the worst test relative to its bar, with what it depends on
     q = int(np.argmax((dt / lim).ravel()))
     row, a = q // w.r, q % w.r

@@ -10,8 +10,8 @@ from test_gpu_parity import CASES, engine_run, oracle_dense
 
 pytestmark = pytest.mark.gpu
 
-T_ABS_MIXED = 1e-3          # |t_mixed - t_fp64| <= 1e-3 (plus 1e-4 relative for very large t)
-T_REL_MIXED = 1e-4
+T_ABS_MIXED = 1e-3          # |t_mixed - t_fp64| <= 1e-3
+T_REL_MIXED = 0.0
 
 
 @pytest.mark.parametrize("case", ["r1_uniform", "r1_patterns", "r1_xrnan", "r1_collinear", "r2_complete",
