@@ -953,7 +953,8 @@ oa_status stats_pre(oa_engine* e, const float* X, size_t ldx, const int* xrows, 
     ++e->launches;
     const int ldc = e->chunk * R;
     if (fused)
-        OA_CU(oa_launch_pre_tcf(X, ldx, e->n, mbc * R, e->mean.p, e->center ? 1 : 0, e->B2hi.p, e->B2lo.p, e->c2,
+        OA_CU(oa_launch_pre_tcf(X, ldx, e->n, mbc * R, e->mean.p, e->has_nan.p, e->center ? 1 : 0, e->B2hi.p,
+                                e->B2lo.p, e->c2,
                                 e->n_pad, e->C2T.p, ldc, reinterpret_cast<int*>(e->counters.p + 3), e->st));
     else if (mixed)
         OA_CU(oa_launch_pre_tc(e->Xhi.p, e->Xlo.p, mbc * R, e->B2hi.p, e->B2lo.p, e->c2, e->n_pad, e->C2T.p, ldc,
@@ -1078,7 +1079,8 @@ template <int R>
 oa_status gemm_dispatch(oa_engine* e, const float* X, int mbc, int snp_base, bool fused) {
     EpiArgs E = epi_args(e, mbc, snp_base);
     if (fused) {
-        OA_CU(oa_launch_gemm_tcf(R, e->raster, X, (size_t)e->n, e->n, mbc * R, e->mean.p, e->center ? 1 : 0,
+        OA_CU(oa_launch_gemm_tcf(R, e->raster, X, (size_t)e->n, e->n, mbc * R, e->mean.p, e->has_nan.p,
+                                 e->center ? 1 : 0,
                                  e->Yhi.p, e->Ylo.p, e->t, e->n_pad, E, reinterpret_cast<int*>(e->counters.p + 3),
                                  e->st));
         e->last_name = e->t > 128 ? "k_gemm_tc2f" : "k_gemm_tcf";

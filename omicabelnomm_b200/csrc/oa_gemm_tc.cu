@@ -769,8 +769,21 @@ k_gemm_tc2(const __grid_constant__ CUtensorMap mAhi, const __grid_constant__ CUt
 // Warps: 0 producer, 1 MMA issuer, 2..9 epilogue, 10..11 converters.
 // Every wait is bounded as in the split forms; drains keep the 2 s bound.
 // ---------------------------------------------------------------------------
-constexpr int CONV_WARPS = 2;
-constexpr int NUM_THREADS_F = NUM_THREADS + 32 * CONV_WARPS;   // 384
+// Converter warps: four with one or two columns per SNP (the epilogue's
+// registers leave room for 448 threads), two with four or eight (384 threads)
+template <int R>
+constexpr int conv_warps() {
+    return R <= 2 ? 4 : 2;
+}
+template <int R>
+constexpr int threads_f() {
+    return NUM_THREADS + 32 * conv_warps<R>();
+}
+// registers per thread of one resident CTA (a multiple of 8): 144 at 448 threads, 168 at 384
+template <int R>
+constexpr int regs_f() {
+    return (65536 / threads_f<R>()) / 8 * 8;
+}
 constexpr int FBK = 64;                                        // K-block of the fused forms (128-byte swizzle)
 
 template <int STAGES_, int BN_, int FSLOTS_, bool PAIR>
@@ -793,19 +806,27 @@ struct ShapeF {
 
 // Converter side of one K-block: FP32 tile (BM x 64, 256 B rows) -> BF16 hi/lo
 // tiles (K-major, 128-byte swizzle: the 16-byte chunk j of row r sits at
-// chunk j ^ (r & 7) of its 128-byte row).  ctid: 0..CONV_WARPS*32-1.
+// chunk j ^ (r & 7) of its 128-byte row).  ctid: 0..NC*32-1.  Without NaN
+// values in the chunk (WITH_NAN = false) the fill is never needed.
+template <int NC, bool WITH_NAN>
 __device__ __forceinline__ void convert_a_tile(const float* __restrict__ fa, uint8_t* ahi, uint8_t* alo,
                                                const float* __restrict__ shift, const float* __restrict__ fill,
                                                int ctid) {
-    constexpr int CT = CONV_WARPS * 32;
+    constexpr int CT = NC * 32;
 #pragma unroll 4
     for (int it = 0; it < BM * (FBK / 4) / CT; ++it) {
         const int q = it * CT + ctid;
         const int row = q >> 4, c = q & 15;   // 16 float4 per 64-element row
         const float4 v = *reinterpret_cast<const float4*>(fa + row * FBK + c * 4);
-        const float sh = shift[row], fl = fill[row];
-        const float e0 = isnan(v.x) ? fl : v.x - sh, e1 = isnan(v.y) ? fl : v.y - sh;
-        const float e2 = isnan(v.z) ? fl : v.z - sh, e3 = isnan(v.w) ? fl : v.w - sh;
+        const float sh = shift[row];
+        float e0 = v.x - sh, e1 = v.y - sh, e2 = v.z - sh, e3 = v.w - sh;
+        if constexpr (WITH_NAN) {
+            const float fl = fill[row];
+            e0 = isnan(v.x) ? fl : e0;
+            e1 = isnan(v.y) ? fl : e1;
+            e2 = isnan(v.z) ? fl : e2;
+            e3 = isnan(v.w) ? fl : e3;
+        }
         const __nv_bfloat162 h01 = __floats2bfloat162_rn(e0, e1), h23 = __floats2bfloat162_rn(e2, e3);
         const float2 f01 = __bfloat1622float2(h01), f23 = __bfloat1622float2(h23);
         const __nv_bfloat162 l01 = __floats2bfloat162_rn(e0 - f01.x, e1 - f01.y);
@@ -820,9 +841,10 @@ __device__ __forceinline__ void convert_a_tile(const float* __restrict__ fa, uin
 }
 
 // Per-row shift and fill of rows [r0, r0 + BM) (rows at or past xrows: 0).
+template <int NC>
 __device__ __forceinline__ void load_shift_fill(const float* __restrict__ colmean, int center, int r0, int xrows,
                                                 float* shift, float* fill, int ctid) {
-    for (int q = ctid; q < BM; q += CONV_WARPS * 32) {
+    for (int q = ctid; q < BM; q += NC * 32) {
         const int row = r0 + q;
         const float mu = row < xrows ? colmean[row] : 0.f;
         shift[q] = center ? mu : 0.f;
@@ -830,17 +852,19 @@ __device__ __forceinline__ void load_shift_fill(const float* __restrict__ colmea
     }
 }
 
+template <int NC>
 __device__ __forceinline__ void conv_bar() {
-    asm volatile("bar.sync 2, %0;" ::"n"(CONV_WARPS * 32) : "memory");
+    asm volatile("bar.sync 2, %0;" ::"n"(NC * 32) : "memory");
 }
 // Named barrier 2 of the converter warps, AND-reducing `ok` over them: both
 // warps take the same decision to go on or to leave after a wait.
+template <int NC>
 __device__ __forceinline__ bool conv_bar_all(int ok) {
     uint32_t r;
     asm volatile(
         "{\n\t.reg .pred p, q;\n\tsetp.ne.u32 q, %1, 0;\n\tbar.red.and.pred p, 2, %2, q;\n\tselp.u32 %0, 1, 0, p;\n}\n"
         : "=r"(r)
-        : "r"(ok), "n"(CONV_WARPS * 32)
+        : "r"(ok), "n"(NC * 32)
         : "memory");
     return r != 0;
 }
@@ -850,10 +874,11 @@ __device__ __forceinline__ void fence_proxy_async_smem() {
 
 // 1-SM fused form (statistics epilogue, or the store epilogue of the pre-GEMM).
 template <int R, class SH, bool STORE>
-__global__ void __launch_bounds__(NUM_THREADS_F, 1)
+__global__ void __launch_bounds__(threads_f<R>()) __maxnreg__(regs_f<R>())
 k_gemm_tcf(const __grid_constant__ CUtensorMap mAf, const __grid_constant__ CUtensorMap mBhi,
-           const __grid_constant__ CUtensorMap mBlo, const float* __restrict__ colmean, int center, int xrows,
-           int t, int nk, EpiArgs E, float* __restrict__ cout, int ldc, int raster, int* err) {
+           const __grid_constant__ CUtensorMap mBlo, const float* __restrict__ colmean, const int* __restrict__ has_nan,
+           int center, int xrows, int t, int nk, EpiArgs E, float* __restrict__ cout, int ldc, int raster, int* err) {
+    constexpr int NC = conv_warps<R>();
     constexpr int BK = SH::BK, STAGES = SH::STAGES, BN = SH::BN, FSLOTS = SH::FSLOTS;
     constexpr uint32_t TMEM_COLS = SH::TMEM_COLS;
     constexpr int A_BYTES = SH::A_BYTES, B_BYTES = SH::B_BYTES, STAGE_BYTES = SH::STAGE_BYTES;
@@ -877,11 +902,11 @@ k_gemm_tcf(const __grid_constant__ CUtensorMap mAf, const __grid_constant__ CUte
         for (int s = 0; s < STAGES; ++s) {
             mbar_init(&full_b[s], 1);
             mbar_init(&empty_bar[s], 1);
-            mbar_init(&conv_bar_s[s], CONV_WARPS);
+            mbar_init(&conv_bar_s[s], NC);
         }
         for (int f = 0; f < FSLOTS; ++f) {
             mbar_init(&fa_full[f], 1);
-            mbar_init(&fa_empty[f], CONV_WARPS);
+            mbar_init(&fa_empty[f], NC);
         }
         for (int a = 0; a < 2; ++a) {
             mbar_init(&acc_full[a], 1);
@@ -1018,26 +1043,31 @@ k_gemm_tcf(const __grid_constant__ CUtensorMap mAf, const __grid_constant__ CUte
     } else if (warp >= 2 + EPI_WARPS) {
         // ---------------- converters ----------------
         const int ctid = threadIdx.x - 32 * (2 + EPI_WARPS);
+        const bool any_nan = *has_nan != 0;   // written by the statistics kernel before this launch
         int s = 0, f = 0;
         uint32_t ph = 0, fph = 0;
         bool ok = true;
         for (int tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x) {
             int m0, n0;
             tile_mn(tile, m0, n0);
-            conv_bar();   // the previous tile's conversions have read shift / fill
-            load_shift_fill(colmean, center, m0, xrows, shift, fill, ctid);
-            conv_bar();
+            conv_bar<NC>();   // the previous tile's conversions have read shift / fill
+            load_shift_fill<NC>(colmean, center, m0, xrows, shift, fill, ctid);
+            conv_bar<NC>();
             for (int kb = 0; kb < nk; ++kb) {
                 int okw = 1;
                 if (lane == 0) okw = mbar_wait(&fa_full[f], fph, &abort_sh) ? 1 : 0;
                 okw = __shfl_sync(0xffffffffu, okw, 0);
-                if (!conv_bar_all(okw)) {   // both converter warps leave together
+                if (!conv_bar_all<NC>(okw)) {   // both converter warps leave together
                     ok = false;
                     break;
                 }
                 mbar_try(&fa_full[f], fph);
-                convert_a_tile(reinterpret_cast<const float*>(fslots + (size_t)f * AF_BYTES), stage_ptr(s, 0),
-                               stage_ptr(s, 1), shift, fill, ctid);
+                if (any_nan)
+                    convert_a_tile<NC, true>(reinterpret_cast<const float*>(fslots + (size_t)f * AF_BYTES),
+                                             stage_ptr(s, 0), stage_ptr(s, 1), shift, fill, ctid);
+                else
+                    convert_a_tile<NC, false>(reinterpret_cast<const float*>(fslots + (size_t)f * AF_BYTES),
+                                              stage_ptr(s, 0), stage_ptr(s, 1), shift, fill, ctid);
                 fence_proxy_async_smem();   // the stores reach the tensor cores' (async) view
                 __syncwarp();
                 if (lane == 0) {
@@ -1169,10 +1199,11 @@ __device__ __forceinline__ bool mbar_wait_cluster(uint64_t* b, uint32_t parity, 
 // issuer waits for the B bytes of both CTAs (leader's full barrier) and for
 // the converters of both CTAs (leader's convert barrier).
 template <int R, class SH>
-__global__ void __launch_bounds__(NUM_THREADS_F, 1)
+__global__ void __launch_bounds__(threads_f<R>()) __maxnreg__(regs_f<R>())
 k_gemm_tc2f(const __grid_constant__ CUtensorMap mAf, const __grid_constant__ CUtensorMap mBhi,
-            const __grid_constant__ CUtensorMap mBlo, const float* __restrict__ colmean, int center, int xrows, int t,
-            int nk, EpiArgs E, int raster, int* err) {
+            const __grid_constant__ CUtensorMap mBlo, const float* __restrict__ colmean,
+            const int* __restrict__ has_nan, int center, int xrows, int t, int nk, EpiArgs E, int raster, int* err) {
+    constexpr int NC = conv_warps<R>();
     constexpr int BK = SH::BK, STAGES = SH::STAGES, BN = SH::BN, FSLOTS = SH::FSLOTS;
     constexpr uint32_t TMEM_COLS = SH::TMEM_COLS;
     constexpr int A_BYTES = SH::A_BYTES, B_BYTES = SH::B_BYTES, STAGE_BYTES = SH::STAGE_BYTES;
@@ -1199,11 +1230,11 @@ k_gemm_tc2f(const __grid_constant__ CUtensorMap mAf, const __grid_constant__ CUt
         for (int s = 0; s < STAGES; ++s) {
             mbar_init(&full_b[s], 1);
             mbar_init(&empty_bar[s], 1);
-            mbar_init(&conv_bar_s[s], 2 * CONV_WARPS);   // leader's copy: the converter warps of both CTAs
+            mbar_init(&conv_bar_s[s], 2 * NC);   // leader's copy: the converter warps of both CTAs
         }
         for (int f = 0; f < FSLOTS; ++f) {
             mbar_init(&fa_full[f], 1);
-            mbar_init(&fa_empty[f], CONV_WARPS);
+            mbar_init(&fa_empty[f], NC);
         }
         for (int a = 0; a < 2; ++a) {
             mbar_init(&acc_full[a], 1);
@@ -1336,26 +1367,31 @@ k_gemm_tc2f(const __grid_constant__ CUtensorMap mAf, const __grid_constant__ CUt
     } else if (warp >= 2 + EPI_WARPS) {
         // ---------------- converters (both CTAs, own 128 rows) ----------------
         const int ctid = threadIdx.x - 32 * (2 + EPI_WARPS);
+        const bool any_nan = *has_nan != 0;   // written by the statistics kernel before this launch
         int s = 0, f = 0;
         uint32_t fph = 0;
         bool ok = true;
         for (int tile = pair; tile < ntiles && ok; tile += npairs) {
             int m0, n0;
             tile_mn(tile, m0, n0);
-            conv_bar();
-            load_shift_fill(colmean, center, m0 + (int)rank * BM, xrows, shift, fill, ctid);
-            conv_bar();
+            conv_bar<NC>();
+            load_shift_fill<NC>(colmean, center, m0 + (int)rank * BM, xrows, shift, fill, ctid);
+            conv_bar<NC>();
             for (int kb = 0; kb < nk; ++kb) {
                 int okw = 1;
                 if (lane == 0) okw = mbar_wait(&fa_full[f], fph, &abort_sh) ? 1 : 0;
                 okw = __shfl_sync(0xffffffffu, okw, 0);
-                if (!conv_bar_all(okw)) {
+                if (!conv_bar_all<NC>(okw)) {
                     ok = false;
                     break;
                 }
                 mbar_try(&fa_full[f], fph);
-                convert_a_tile(reinterpret_cast<const float*>(fslots + (size_t)f * AF_BYTES), stage_ptr(s, 0),
-                               stage_ptr(s, 1), shift, fill, ctid);
+                if (any_nan)
+                    convert_a_tile<NC, true>(reinterpret_cast<const float*>(fslots + (size_t)f * AF_BYTES),
+                                             stage_ptr(s, 0), stage_ptr(s, 1), shift, fill, ctid);
+                else
+                    convert_a_tile<NC, false>(reinterpret_cast<const float*>(fslots + (size_t)f * AF_BYTES),
+                                              stage_ptr(s, 0), stage_ptr(s, 1), shift, fill, ctid);
                 fence_proxy_async_smem();
                 __syncwarp();
                 if (lane == 0) {
@@ -1559,7 +1595,8 @@ static bool make_map_f32(CUtensorMap* m, const float* ptr, int rows, int k_valid
 }
 
 template <int R, class SH, bool STORE>
-static cudaError_t go_f(const float* X, size_t ldx, int n, int xrows, const float* colmean, int center,
+static cudaError_t go_f(const float* X, size_t ldx, int n, int xrows, const float* colmean, const int* has_nan,
+                        int center,
                         const __nv_bfloat16* Bhi, const __nv_bfloat16* Blo, int t, int n_pad, const EpiArgs& E,
                         float* cout, int ldc, int raster, int* err, cudaStream_t st) {
     constexpr int BN = SH::BN;
@@ -1579,13 +1616,14 @@ static cudaError_t go_f(const float* X, size_t ldx, int n, int xrows, const floa
     const int ntiles = ((xrows + BM - 1) / BM) * ((t + BN - 1) / BN);
     const int sms = sm_count();
     const int grid = ntiles < sms ? ntiles : sms;
-    k_gemm_tcf<R, SH, STORE><<<grid, NUM_THREADS_F, SH::SMEM_BYTES, st>>>(
-        a_f, b_hi, b_lo, colmean, center, xrows, t, n_pad / SH::BK, E, cout, ldc, raster, err);
+    k_gemm_tcf<R, SH, STORE><<<grid, threads_f<R>(), SH::SMEM_BYTES, st>>>(
+        a_f, b_hi, b_lo, colmean, has_nan, center, xrows, t, n_pad / SH::BK, E, cout, ldc, raster, err);
     return cudaGetLastError();
 }
 
 template <int R, class SH>
-static cudaError_t go2_f(const float* X, size_t ldx, int n, int xrows, const float* colmean, int center,
+static cudaError_t go2_f(const float* X, size_t ldx, int n, int xrows, const float* colmean, const int* has_nan,
+                         int center,
                          const __nv_bfloat16* Yhi, const __nv_bfloat16* Ylo, int t, int n_pad, const EpiArgs& E,
                          int raster, int* err, cudaStream_t st) {
     CUtensorMap a_f, b_hi, b_lo;
@@ -1605,7 +1643,7 @@ static cudaError_t go2_f(const float* X, size_t ldx, int n, int xrows, const flo
     const int pairs = std::min(ntiles, sm_count() / 2);
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3(2 * pairs, 1, 1);
-    cfg.blockDim = dim3(NUM_THREADS_F, 1, 1);
+    cfg.blockDim = dim3(threads_f<R>(), 1, 1);
     cfg.dynamicSmemBytes = SH::SMEM_BYTES;
     cfg.stream = st;
     cudaLaunchAttribute attr[1];
@@ -1615,8 +1653,8 @@ static cudaError_t go2_f(const float* X, size_t ldx, int n, int xrows, const flo
     attr[0].val.clusterDim.z = 1;
     cfg.attrs = attr;
     cfg.numAttrs = 1;
-    return cudaLaunchKernelEx(&cfg, k_gemm_tc2f<R, SH>, a_f, b_hi, b_lo, colmean, center, xrows, t, n_pad / SH::BK, E,
-                              raster, err);
+    return cudaLaunchKernelEx(&cfg, k_gemm_tc2f<R, SH>, a_f, b_hi, b_lo, colmean, has_nan, center, xrows, t,
+                              n_pad / SH::BK, E, raster, err);
 }
 
 using FNarrow64 = ShapeF<3, 64, 2, false>;
@@ -1627,16 +1665,17 @@ using FPair = ShapeF<2, 256, 2, true>;
 // the 1-SM narrow tiles, wider ones on CTA pairs (the fused pair form serves
 // pipeline variants 3 and 4).
 template <int R>
-static cudaError_t go_any_f(int raster, const float* X, size_t ldx, int n, int xrows, const float* colmean, int center,
+static cudaError_t go_any_f(int raster, const float* X, size_t ldx, int n, int xrows, const float* colmean,
+                            const int* has_nan, int center,
                             const __nv_bfloat16* Yhi, const __nv_bfloat16* Ylo, int t, int n_pad, const EpiArgs& E,
                             int* err, cudaStream_t st) {
     if (t <= 64)
-        return go_f<R, FNarrow64, false>(X, ldx, n, xrows, colmean, center, Yhi, Ylo, t, n_pad, E, nullptr, 0, raster,
+        return go_f<R, FNarrow64, false>(X, ldx, n, xrows, colmean, has_nan, center, Yhi, Ylo, t, n_pad, E, nullptr, 0, raster,
                                          err, st);
     if (t <= 128)
-        return go_f<R, FNarrow128, false>(X, ldx, n, xrows, colmean, center, Yhi, Ylo, t, n_pad, E, nullptr, 0,
+        return go_f<R, FNarrow128, false>(X, ldx, n, xrows, colmean, has_nan, center, Yhi, Ylo, t, n_pad, E, nullptr, 0,
                                           raster, err, st);
-    return go2_f<R, FPair>(X, ldx, n, xrows, colmean, center, Yhi, Ylo, t, n_pad, E, raster, err, st);
+    return go2_f<R, FPair>(X, ldx, n, xrows, colmean, has_nan, center, Yhi, Ylo, t, n_pad, E, raster, err, st);
 }
 
 }  // namespace tc
@@ -1669,26 +1708,27 @@ cudaError_t oa_launch_pre_tc(const __nv_bfloat16* Xhi, const __nv_bfloat16* Xlo,
 bool oa_gemm_tc_fusable(int variant, int t) { return t <= 128 || variant >= 3; }
 
 cudaError_t oa_launch_gemm_tcf(int R, int raster, const float* X, size_t ldx, int n, int xrows, const float* colmean,
-                               int center, const __nv_bfloat16* Yhi, const __nv_bfloat16* Ylo, int t, int n_pad,
+                               const int* has_nan, int center, const __nv_bfloat16* Yhi, const __nv_bfloat16* Ylo, int t, int n_pad,
                                const EpiArgs& E, int* err, cudaStream_t st) {
     switch (R) {
-        case 1: return tc::go_any_f<1>(raster, X, ldx, n, xrows, colmean, center, Yhi, Ylo, t, n_pad, E, err, st);
-        case 2: return tc::go_any_f<2>(raster, X, ldx, n, xrows, colmean, center, Yhi, Ylo, t, n_pad, E, err, st);
-        case 4: return tc::go_any_f<4>(raster, X, ldx, n, xrows, colmean, center, Yhi, Ylo, t, n_pad, E, err, st);
-        case 8: return tc::go_any_f<8>(raster, X, ldx, n, xrows, colmean, center, Yhi, Ylo, t, n_pad, E, err, st);
+        case 1: return tc::go_any_f<1>(raster, X, ldx, n, xrows, colmean, has_nan, center, Yhi, Ylo, t, n_pad, E, err, st);
+        case 2: return tc::go_any_f<2>(raster, X, ldx, n, xrows, colmean, has_nan, center, Yhi, Ylo, t, n_pad, E, err, st);
+        case 4: return tc::go_any_f<4>(raster, X, ldx, n, xrows, colmean, has_nan, center, Yhi, Ylo, t, n_pad, E, err, st);
+        case 8: return tc::go_any_f<8>(raster, X, ldx, n, xrows, colmean, has_nan, center, Yhi, Ylo, t, n_pad, E, err, st);
         default: return cudaErrorInvalidValue;
     }
 }
 
-cudaError_t oa_launch_pre_tcf(const float* X, size_t ldx, int n, int xrows, const float* colmean, int center,
+cudaError_t oa_launch_pre_tcf(const float* X, size_t ldx, int n, int xrows, const float* colmean, const int* has_nan,
+                              int center,
                               const __nv_bfloat16* Bhi, const __nv_bfloat16* Blo, int c2, int n_pad, float* C, int ldc,
                               int* err, cudaStream_t st) {
     const EpiArgs none{};
     if (c2 <= 64)
-        return tc::go_f<1, tc::FNarrow64, true>(X, ldx, n, xrows, colmean, center, Bhi, Blo, c2, n_pad, none, C, ldc, 1,
+        return tc::go_f<1, tc::FNarrow64, true>(X, ldx, n, xrows, colmean, has_nan, center, Bhi, Blo, c2, n_pad, none, C, ldc, 1,
                                                 err, st);
     if (c2 <= 128)
-        return tc::go_f<1, tc::FNarrow128, true>(X, ldx, n, xrows, colmean, center, Bhi, Blo, c2, n_pad, none, C, ldc,
+        return tc::go_f<1, tc::FNarrow128, true>(X, ldx, n, xrows, colmean, has_nan, center, Bhi, Blo, c2, n_pad, none, C, ldc,
                                                  1, err, st);
     return cudaErrorInvalidValue;
 }

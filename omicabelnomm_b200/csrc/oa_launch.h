@@ -36,14 +36,15 @@ cudaError_t oa_launch_gemm_tc(int R, int variant, int raster, const __nv_bfloat1
                               const EpiArgs& E, int* err, cudaStream_t st);
 // Fused-operand forms: X read as FP32 (columns of ldx floats, n of them valid; ldx * 4 and X 16-byte aligned)
 // and split into BF16 hi / lo in shared memory, each value taken as NaN -> fill, else x - shift, with
-// shift = center ? colmean : 0 and fill = center ? 0 : colmean per row.  oa_gemm_tc_fusable: the pipeline
+// shift = center ? colmean : 0 and fill = center ? 0 : colmean per row (fill only when *has_nan != 0).  oa_gemm_tc_fusable: the pipeline
 // variant and trait count have a fused form (at most 128 traits, or CTA pairs); the pre-GEMM's fused form
 // takes at most 128 columns.
 bool oa_gemm_tc_fusable(int variant, int t);
 cudaError_t oa_launch_gemm_tcf(int R, int raster, const float* X, size_t ldx, int n, int xrows, const float* colmean,
-                               int center, const __nv_bfloat16* Yhi, const __nv_bfloat16* Ylo, int t, int n_pad,
+                               const int* has_nan, int center, const __nv_bfloat16* Yhi, const __nv_bfloat16* Ylo, int t, int n_pad,
                                const EpiArgs& E, int* err, cudaStream_t st);
-cudaError_t oa_launch_pre_tcf(const float* X, size_t ldx, int n, int xrows, const float* colmean, int center,
+cudaError_t oa_launch_pre_tcf(const float* X, size_t ldx, int n, int xrows, const float* colmean, const int* has_nan,
+                              int center,
                               const __nv_bfloat16* Bhi, const __nv_bfloat16* Blo, int c2, int n_pad, float* C, int ldc,
                               int* err, cudaStream_t st);
 }  // namespace oa

@@ -308,10 +308,13 @@ def test_quirk_r2_matches_oracle_quirk(case, prec):
     dt = np.abs(tt[ok] - t_ref)
     t_sys = np.broadcast_to(np.abs(t_ref).max(axis=1, keepdims=True), t_ref.shape)
     lim = (T_REL * t_sys + T_ABS) if prec == E.PLAIN else (1e-3 + 5e-4 * t_sys)
+    assert rows.singular == int(D.singular.sum()), (rows.singular, int(D.singular.sum()))
     assert np.all(dt <= lim), f"max |dt| {dt.max():.3g}"
-    assert np.allclose(se[ok], D.se[:, :, l:][ok], rtol=1e-3, atol=0)
-    assert np.allclose(r2[ok], D.r2[ok], rtol=1e-4, atol=1e-4)
-    assert rows.singular == int(D.singular.sum())
+    dse = np.abs(se[ok] - D.se[:, :, l:][ok]) / np.abs(D.se[:, :, l:][ok])
+    q = np.unravel_index(np.argmax(dse), dse.shape)
+    assert dse.max() <= 1e-3, (float(dse.max()), float(se[ok][q]), float(D.se[:, :, l:][ok][q]))
+    dr2 = np.abs(r2[ok] - D.r2[ok]) / np.maximum(np.abs(D.r2[ok]), 1.0)
+    assert dr2.max() <= 1e-4, (float(dr2.max()), float(r2[ok][np.argmax(dr2)]), float(D.r2[ok][np.argmax(dr2)]))
     # the quirk matters here: its answers are not the corrected ones
     assert np.abs(D.tstat[:, :, l:] - Dc.tstat[:, :, l:])[ok].max() > 1e-2
 
