@@ -303,6 +303,9 @@ struct oa_engine {
     DBuf<int> tcounts, pat, zset, nobs, set_off, set_rows, set_rep, set_kind, set_slot, tperm, tinv;
     DBuf<float> a_r2, inv_ncorr, vf;
     DBuf<unsigned long long> thash;
+    DBuf<int> tcheck;            // per trait: its pattern's and zero set's representatives; collision flag
+    int hash_bits = 64;          // hash-sum bits used for grouping (fewer only to test the exact regrouping)
+    bool trait_regrouped = false;   // the last trait block was regrouped on exact row masks
     DBuf<float> sst, qrows;
     DBuf<uint8_t> pat_bad;
     int G = 0, Z = 0, nsets = 0;
@@ -424,7 +427,7 @@ void for_each_buf(oa_engine* e, F&& f) {
     f(e->tsums); f(e->rss0); f(e->b0); f(e->W); f(e->zQ);
     f(e->tcounts); f(e->pat); f(e->zset); f(e->nobs); f(e->set_off); f(e->set_rows); f(e->set_rep);
     f(e->set_kind); f(e->set_slot); f(e->tperm); f(e->tinv);
-    f(e->a_r2); f(e->inv_ncorr); f(e->vf); f(e->thash); f(e->sst); f(e->qrows); f(e->pat_bad);
+    f(e->a_r2); f(e->inv_ncorr); f(e->vf); f(e->thash); f(e->tcheck); f(e->sst); f(e->qrows); f(e->pat_bad);
     f(e->B2); f(e->B2hi); f(e->B2lo);
     f(e->Xstage[0]); f(e->Xstage[1]); f(e->Xmodel); f(e->inter); f(e->Xhi); f(e->Xlo);
     f(e->mean); f(e->varx); f(e->aobs); f(e->afull); f(e->zA); f(e->zD); f(e->D); f(e->Dset); f(e->C2T);
@@ -544,6 +547,75 @@ oa_status flush_h2d(oa_engine* e, const H2DBatch& b) {
     return OA_OK;
 }
 
+// The traits are grouped by (count, two hash sums) of their NaN rows and of
+// their observed exact-zero rows.  Equal keys are checked on the device
+// against the group's representative row by row; if any trait's rows differ
+// (a hash collision), the traits are regrouped on their exact row masks, with
+// groups numbered in order of first appearance as the hash grouping does.
+oa_status exact_trait_sets(oa_engine* e, const float* Y, int t, const std::vector<int>& counts,
+                           std::vector<int>& hpat, std::vector<int>& hz, std::vector<int>& prep,
+                           std::vector<int>& zrep, std::vector<int>& pcnt, std::vector<int>& zcnt) {
+    const int n = e->n;
+    std::vector<int> rep((size_t)2 * t);
+    for (int j = 0; j < t; ++j) {
+        rep[2 * j] = prep[hpat[j]];
+        rep[2 * j + 1] = hz[j] >= 0 ? zrep[hz[j]] : -1;
+    }
+    OA_CHECK(e->tcheck.ensure((size_t)2 * t + 4));
+    H2DBatch h2d;
+    h2d.add(e->tcheck.p, rep);
+    OA_CHECK(flush_h2d(e, h2d));
+    int* bad = e->tcheck.p + 2 * t;
+    OA_CU(cudaMemsetAsync(bad, 0, sizeof(int), e->st));
+    k_trait_set_check<<<t, OA_NTHREADS, 0, e->st>>>(Y, (size_t)n, n, e->tcheck.p, bad);
+    ++e->launches;
+    OA_CU(cudaGetLastError());
+    OA_CU(cudaMemcpyAsync(e->stage, bad, sizeof(int), cudaMemcpyDeviceToHost, e->st));
+    OA_CU(cudaStreamSynchronize(e->st));
+    int hbad = 0;
+    std::memcpy(&hbad, e->stage, sizeof(int));
+    e->trait_regrouped = hbad != 0;
+    if (!hbad) return OA_OK;
+    const int nw = (n + 31) / 32;
+    const size_t words = (size_t)2 * t * nw;
+    DBuf<unsigned> masks;
+    struct Release {
+        DBuf<unsigned>& b;
+        ~Release() { b.release(); }
+    } release_masks{masks};
+    OA_CHECK(masks.ensure(words));
+    k_trait_masks<<<t, OA_NTHREADS, 0, e->st>>>(Y, (size_t)n, n, nw, masks.p);
+    ++e->launches;
+    OA_CU(cudaGetLastError());
+    std::vector<unsigned> hm(words);
+    OA_CU(cudaMemcpyAsync(hm.data(), masks.p, words * sizeof(unsigned), cudaMemcpyDeviceToHost, e->st));
+    OA_CU(cudaStreamSynchronize(e->st));
+    std::map<std::vector<unsigned>, int> pmap, zmap;
+    prep.clear(), zrep.clear(), pcnt.clear(), zcnt.clear();
+    for (int j = 0; j < t; ++j) {
+        std::vector<unsigned> pk(hm.begin() + (size_t)(2 * j) * nw, hm.begin() + (size_t)(2 * j + 1) * nw);
+        auto it = pmap.find(pk);
+        if (it == pmap.end()) {
+            it = pmap.emplace(std::move(pk), (int)prep.size()).first;
+            prep.push_back(j);
+            pcnt.push_back(counts[j * 2]);
+        }
+        hpat[j] = it->second;
+        hz[j] = -1;
+        if (counts[j * 2 + 1] > 0) {
+            std::vector<unsigned> zk(hm.begin() + (size_t)(2 * j + 1) * nw, hm.begin() + (size_t)(2 * j + 2) * nw);
+            auto zt = zmap.find(zk);
+            if (zt == zmap.end()) {
+                zt = zmap.emplace(std::move(zk), (int)zrep.size()).first;
+                zrep.push_back(j);
+                zcnt.push_back(counts[j * 2 + 1]);
+            }
+            hz[j] = zt->second;
+        }
+    }
+    return OA_OK;
+}
+
 oa_status set_traits_impl(oa_engine* e, const float* y, int32_t t, bool device_ptr) {
     OA_TRACE("oa_set_traits: grouping, row sets, residuals");
     if (!e->have_cov) {
@@ -582,6 +654,8 @@ oa_status set_traits_impl(oa_engine* e, const float* y, int32_t t, bool device_p
         std::memcpy(counts.data(), e->stage + hb, cb);
     }
 
+    if (e->hash_bits < 64)   // test hook: hash sums cut to their low bits make patterns collide
+        for (auto& h : hashes) h &= (1ull << e->hash_bits) - 1ull;
     // group traits: missingness patterns, then sets of observed exact zeros
     std::map<std::tuple<int, unsigned long long, unsigned long long>, int> pmap, zmap;
     std::vector<int> hpat(t), hz(t, -1), prep, zrep, pcnt, zcnt;
@@ -605,6 +679,7 @@ oa_status set_traits_impl(oa_engine* e, const float* y, int32_t t, bool device_p
             hz[j] = zt->second;
         }
     }
+    OA_CHECK(exact_trait_sets(e, Y, t, counts, hpat, hz, prep, zrep, pcnt, zcnt));
     e->G = (int)prep.size();
     e->Z = (int)zrep.size();
     e->nsets = e->G + e->Z;
@@ -1733,6 +1808,7 @@ oa_status oa_engine_create(const oa_config* cfg, oa_engine** out) {
     if (const char* v = getenv("OA_LEAN_XI")) e->lean_xi = atoi(v) == 0 ? 0 : (atoi(v) == 1 ? 1 : -1);
     e->chunk = std::min(cfg->max_snps, e->req.chunk_snps > 0 ? e->req.chunk_snps : 16384 / e->r);
     if (const char* v = getenv("OA_FUSED_SPLIT")) e->fuse_split = v[0] != '0';
+    if (const char* v = getenv("OA_TEST_HASH_BITS")) e->hash_bits = std::min(64, std::max(0, atoi(v)));
     const char* gr = getenv("OA_GRAPHS");
     e->use_graphs = !(gr && gr[0] == '0');
     // the copy stream of host SNP blocks is created on first use: a device-resident

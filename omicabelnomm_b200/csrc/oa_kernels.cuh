@@ -3,6 +3,9 @@
 //  k_trait_stats  per trait: missing count, sums, zero count, missing-set
 //                 hashes, Q'y  (≙ replace_nans + sumSquares + XL'Y,
 //                 src/Utility.cpp:329-378, src/Algorithm.cpp:558-585, 1222-1251)
+//  k_trait_set_check, k_trait_masks
+//                 exact check of the grouping by hash sums; row masks for
+//                 the exact regrouping after a collision
 //  k_set_rows     ordered row list of each row set (missing pattern / zero set)
 //  k_set_gram     per pattern W = (Q_obs'Q_obs)^-1, per zero set sum q q'
 //                 (≙ generate_correction_missings_Stl, src/Algorithm.cpp:1324-1362)
@@ -134,6 +137,45 @@ k_set_rows(const float* __restrict__ Y, size_t ldy, int n, const int* __restrict
         if (pred) out[base + wbase[w] + __popc(m & ((1u << lane) - 1u))] = k;
         base += total;
         __syncthreads();
+    }
+}
+
+// Exact check of the trait grouping by hash sums: trait j's NaN rows must be
+// those of its pattern's representative rep[2 j], and when rep[2 j + 1] >= 0
+// its observed exact-zero rows those of its zero set's representative.  Any
+// difference sets *bad (the host then groups the traits on their row masks).
+static __global__ void __launch_bounds__(OA_NTHREADS)
+k_trait_set_check(const float* __restrict__ Y, size_t ldy, int n, const int* __restrict__ rep, int* bad) {
+    const int j = blockIdx.x;
+    const float* y = Y + (size_t)j * ldy;
+    const float* yp = Y + (size_t)rep[2 * j] * ldy;
+    const int zr = rep[2 * j + 1];
+    const float* yz = Y + (size_t)(zr >= 0 ? zr : j) * ldy;
+    int diff = 0;
+    for (int k = threadIdx.x; k < n; k += blockDim.x) {
+        const float x = y[k];
+        diff |= isnan(x) != isnan(yp[k]);
+        if (zr >= 0) diff |= (x == 0.0f) != (yz[k] == 0.0f);
+    }
+    if (__syncthreads_or(diff) && threadIdx.x == 0) atomicOr(bad, 1);
+}
+
+// Row masks of each trait, 32 rows per word: masks[(2 j) nw + w] bit b set
+// when row 32 w + b is NaN, masks[(2 j + 1) nw + w] when it is an observed 0.
+static __global__ void __launch_bounds__(OA_NTHREADS)
+k_trait_masks(const float* __restrict__ Y, size_t ldy, int n, int nw, unsigned* __restrict__ masks) {
+    const int j = blockIdx.x;
+    const float* y = Y + (size_t)j * ldy;
+    const int lane = threadIdx.x & 31;
+    for (int k0 = (threadIdx.x >> 5) * 32; k0 < nw * 32; k0 += blockDim.x) {   // one 32-row word per warp
+        const int k = k0 + lane;
+        const float x = k < n ? y[k] : 1.0f;
+        const unsigned mn = __ballot_sync(0xffffffffu, isnan(x));
+        const unsigned mz = __ballot_sync(0xffffffffu, x == 0.0f);
+        if (lane == 0) {
+            masks[(size_t)(2 * j) * nw + k0 / 32] = mn;
+            masks[(size_t)(2 * j + 1) * nw + k0 / 32] = mz;
+        }
     }
 }
 

@@ -124,6 +124,13 @@ def noise():
         return json.load(f)
 
 
+def quirk_noise():
+    """The reference's largest deviation from the FP64 oracle per quirk-mode dense test case
+    (tests/golden/quirk_noise.json, written by tests/golden/measure_quirk_noise.py)."""
+    with open(os.path.join(GOLDEN, "quirk_noise.json")) as f:
+        return json.load(f)
+
+
 def run_tol(case: str, tag: str) -> Tol:
     """Parity bar of the GPU CLI against one golden run: |t - t_ref| <= 1e-4 |t_ref| + delta,
     delta = the reference's own noise on that run (the larger of its thread spread and its

@@ -8,6 +8,7 @@ import pytest
 
 import golden_util as GU
 import oa_oracle as O
+import quirk_cases as QC
 from omicabelnomm_b200 import engine as E
 from omicabelnomm_b200 import synth
 
@@ -115,6 +116,40 @@ def test_chunked_block_equals_single_block(monkeypatch):
     for x, y in zip(dense_a, dense_b):
         np.testing.assert_array_equal(x, y)
     np.testing.assert_array_equal(rows_a.snp, rows_b.snp)
+
+
+def _same_count_patterns(seed=91, n=500, m=120, t=16, l=4, miss=25, zeros=5):
+    """Traits in four missingness patterns and four zero sets, all patterns with
+    the same number of NaN rows and all zero sets with the same number of rows:
+    grouping on row counts alone would merge them."""
+    ds = synth.generate(synth.scaled(0, n=n, m=m, t=t, l=l, miss_mode="none", seed=seed))
+    rng = np.random.Generator(np.random.PCG64(seed))
+    pats = [rng.choice(n, miss, replace=False) for _ in range(4)]
+    zsets = [rng.choice(n, zeros, replace=False) for _ in range(4)]
+    for j in range(t):
+        ds.Y[j, zsets[(j // 4) % 4]] = 0.0
+        ds.Y[j, pats[j % 4]] = np.nan                   # NaN last: a zero row may become missing
+    return ds
+
+
+def test_trait_grouping_is_exact_under_hash_collisions(monkeypatch):
+    """Traits are grouped by (row count, two hash sums) of their NaN rows and
+    of their observed exact-zero rows, then checked row by row on the device;
+    a collision makes the engine regroup on the exact row masks.  With the
+    hash sums cut to 0 bits (every pattern of equal count collides) the
+    results must equal those of the full hashes bit for bit, and the oracle's."""
+    ds = _same_count_patterns()
+    _, rows_a, dense_a = engine_run(ds, 1)
+    monkeypatch.setenv("OA_TEST_HASH_BITS", "0")
+    _, rows_b, dense_b = engine_run(ds, 1)
+    for x, y in zip(dense_a, dense_b):
+        np.testing.assert_array_equal(x, y)
+    res, _, _ = oracle_dense(ds, 1)
+    D = res.dense
+    ok = ~D.singular
+    t_ref = D.tstat[:, :, res.l:][ok]
+    dt = np.abs(dense_b[2][ok] - t_ref)
+    assert np.all(dt <= T_REL * np.abs(t_ref) + T_ABS), dt.max()
 
 
 # ---------------------------------------------------------------------------
@@ -262,34 +297,23 @@ def test_dense_flags_match_oracle_masks(prec, stats_path):
     assert stored == set(zip(rows.trait.tolist(), rows.snp.tolist()))
 
 
-def _multicol(r, seed, **over):
-    """r dosage columns per SNP: consecutive independent dosage columns grouped r at a time."""
-    w = dict(n=500, m=30, t=12, l=4, miss_mode="patterns", n_patterns=3, miss_hi=0.12)
-    w.update(over)
-    w["m"] *= r
-    return synth.generate(synth.scaled(0, seed=seed, **w))
-
-
 @pytest.mark.parametrize("prec", [E.PLAIN, E.MIXED])
-@pytest.mark.parametrize("case", ["r2_missing", "r2_yzero_l1", "r3_missing", "r5_l2"])
+@pytest.mark.parametrize("case", QC.CASES)
 def test_quirk_r2_matches_oracle_quirk(case, prec):
     """The reference's r >= 2 downdate reproduced on the device (quirk mode) against the
     oracle's restatement of it: dense t, SE, R2 and the singular set; also with observed
     zero phenotypes (zero sets), with r > l (the SNP-block downdate quirk) and with r = 3
-    and 5 (zero padding columns in the kernels).  Quirk mode works on the raw, uncentred
-    SNP columns (the reference's own sums), so its rounding is relative to those sums:
-    the plain form's t bar is the usual one, SE and R2 are compared relative to their
-    size (the quirk's R2 can be far below 0), and the mixed form's bar grows with the
-    system's largest |t|."""
-    r = 2
-    if case == "r2_missing":
-        ds = synth.generate(synth.scaled(0, **CASES["r2_missing"]))
-    elif case == "r2_yzero_l1":
-        ds = _yzero(_multicol(2, 74, n=500, m=45, l=1, n_patterns=3, miss_hi=0.15), 9)
-    elif case == "r3_missing":
-        r, ds = 3, _multicol(3, 75)
-    else:
-        r, ds = 5, _multicol(5, 76, l=2)
+    and 5 (zero padding columns in the kernels).
+
+    The quirk's downdate can leave a system far from positive definite, and its SE and R2
+    then carry rounding amplified by the condition number - the reference's own FP32
+    answers too: tests/golden/quirk_noise.json holds, per case, the reference's largest
+    deviation from the FP64 oracle (tests/golden/measure_quirk_noise.py).  Bars: t as the
+    plain form's (relative to the system's largest |t|) or the mixed form's; SE and R2
+    within twice the reference's deviation, scaled for the mixed form by 2^7 (the ratio of
+    its split's unit roundoff, 2^-17, to FP32's), and never below 1e-3 (SE, relative) and
+    1e-4 (R2, relative to max(|R2|, 1))."""
+    r, ds = QC.build(case)
     l, n = ds.XL.shape
     m, t = ds.XR.shape[0] // r, ds.Y.shape[0]
     inp = O.Inputs(XL=ds.XL, XR=ds.XR, Y=ds.Y, xl_names=ds.xl_names, xr_names=ds.xr_names,
@@ -310,11 +334,15 @@ def test_quirk_r2_matches_oracle_quirk(case, prec):
     lim = (T_REL * t_sys + T_ABS) if prec == E.PLAIN else (1e-3 + 5e-4 * t_sys)
     assert rows.singular == int(D.singular.sum()), (rows.singular, int(D.singular.sum()))
     assert np.all(dt <= lim), f"max |dt| {dt.max():.3g}"
+    noise = GU.quirk_noise()[case]
+    scale = 2.0 * (1.0 if prec == E.PLAIN else 2.0 ** 7)
     dse = np.abs(se[ok] - D.se[:, :, l:][ok]) / np.abs(D.se[:, :, l:][ok])
     q = np.unravel_index(np.argmax(dse), dse.shape)
-    assert dse.max() <= 1e-3, (float(dse.max()), float(se[ok][q]), float(D.se[:, :, l:][ok][q]))
+    assert dse.max() <= max(1e-3, scale * noise["dse_rel"]), (float(dse.max()), float(se[ok][q]),
+                                                               float(D.se[:, :, l:][ok][q]))
     dr2 = np.abs(r2[ok] - D.r2[ok]) / np.maximum(np.abs(D.r2[ok]), 1.0)
-    assert dr2.max() <= 1e-4, (float(dr2.max()), float(r2[ok][np.argmax(dr2)]), float(D.r2[ok][np.argmax(dr2)]))
+    assert dr2.max() <= max(1e-4, scale * noise["dr2"]), (float(dr2.max()), float(r2[ok][np.argmax(dr2)]),
+                                                          float(D.r2[ok][np.argmax(dr2)]))
     # the quirk matters here: its answers are not the corrected ones
     assert np.abs(D.tstat[:, :, l:] - Dc.tstat[:, :, l:])[ok].max() > 1e-2
 
@@ -325,7 +353,7 @@ def test_dense_more_columns_per_snp_match_fp64_oracle(r, prec):
     """r = 3, 5, 6 (kernels with 4 or 8 columns per SNP, zero columns added on the device)
     and r = 8, with missingness patterns, against the FP64 oracle; plain bars for the
     plain form, the r >= 2 mixed bars for the mixed form."""
-    ds = _multicol(r, 80 + r, m=24, t=10)
+    ds = QC.multicol(r, 80 + r, m=24, t=10)
     res, _, _ = oracle_dense(ds, r)
     eng, rows, (b, se, tt, r2) = engine_run(ds, r, precision=prec)
     D = res.dense
