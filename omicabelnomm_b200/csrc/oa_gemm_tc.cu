@@ -752,25 +752,32 @@ k_gemm_tc2(const __grid_constant__ CUtensorMap mAhi, const __grid_constant__ CUt
 // ---------------------------------------------------------------------------
 // Fused-operand forms: the X operand is read as FP32 (the SNP columns as the
 // statistics kernel read them) and split into BF16 hi / lo in shared memory,
-// so that no split copy of X is written to or read back from HBM.
+// so that no split copy of X is written to HBM or read back.
 //
-// Per K-block the producer TMA-loads the FP32 tile of this CTA's 128 rows
-// (64 K-elements, 256 bytes per row, no swizzle) into one of FSLOTS staging
-// slots, and the B tiles (the traits' or the pre-GEMM columns' hi / lo, split
-// once per trait block) into the K-block's stage.  Two converter warps wait
-// for the FP32 tile, form each value as the statistics kernel's split does
-// (NaN -> the column's fill value, else x - shift; shift = the column mean
-// when the columns are centred, else 0; fill = 0 when centred, else the
-// imputation mean), split it (hi = bf16(x), lo = bf16(x - hi)) and store hi
-// and lo in the stage's A tiles in the UMMA K-major 128-byte-swizzle layout;
-// then they release the FP32 slot and signal the MMA issuer.  The results are
-// bit-identical to the split path (same FP32 values, same roundings).
-// The MMA issuer waits for the stage's B bytes and for the converters.
-// Warps: 0 producer, 1 MMA issuer, 2..9 epilogue, 10..11 converters.
+// The producer loads each K-block's FP32 A tile (the CTA's 128 rows x 64
+// K-elements, 32 KB, rows at 256-byte strides) and B tiles (the traits' or
+// the pre-GEMM columns' hi / lo, split once per trait block) into the
+// K-block's stage, prefetching the FP32 tiles into L2 ahead of use as the
+// split forms do; the stages' pipeline hides the load latency.  Converter
+// warps then split the A tile in place.  The UMMA operands hi and lo are laid
+// out as interleaved 8-row groups (K-major, 128-byte swizzle: the 16-byte
+// chunk j of row r sits at chunk j ^ (r & 7) of its 128-byte row; hi of rows
+// 8g..8g+7 at 2048 g, lo at 2048 g + 1024, descriptor stride 2048 bytes), so
+// that the hi and lo of an 8-row group occupy exactly the 2 KB of its FP32
+// rows: one warp reads a group, synchronises and writes it, with no barrier
+// between warps.  Each value is formed as the statistics kernel's split
+// forms it (NaN -> the column's fill value, else x - shift; shift = the
+// column mean when the columns are centred, else 0; fill = 0 when centred,
+// else the imputation mean) and split as hi = bf16(x), lo = bf16(x - hi):
+// the results are bit-identical to the split path's.  K past n and rows past
+// the last SNP column read as 0 (TMA fill); the K tail then holds -shift as
+// in the split copy, against zero B rows.  The MMA issuer waits for the
+// stage's bytes and for the converters.
+// Warps: 0 producer, 1 MMA issuer, 2..9 epilogue, then the converters.
 // Every wait is bounded as in the split forms; drains keep the 2 s bound.
 // ---------------------------------------------------------------------------
-// Converter warps: four with one or two columns per SNP (the epilogue's
-// registers leave room for 448 threads), two with four or eight (384 threads)
+// Converter warps: four with one or two columns per SNP, two with four or eight (the epilogue's
+// registers bound the block: 448 threads leave 128 registers a thread, 384 leave 168)
 template <int R>
 constexpr int conv_warps() {
     return R <= 2 ? 4 : 2;
@@ -779,118 +786,205 @@ template <int R>
 constexpr int threads_f() {
     return NUM_THREADS + 32 * conv_warps<R>();
 }
-// registers per thread of one resident CTA (a multiple of 8): 144 at 448 threads, 168 at 384
+// registers per thread of one resident CTA (a multiple of 8): the block's warps are spread
+// over the SM's four sub-partitions of 16,384 registers each, so the sub-partition with the
+// most warps (ceil(warps / 4)) bounds them: 128 at 448 threads (4 warps per sub-partition),
+// 168 at 384 (3)
 template <int R>
 constexpr int regs_f() {
-    return (65536 / threads_f<R>()) / 8 * 8;
+    return (16384 / (((threads_f<R>() / 32 + 3) / 4) * 32)) / 8 * 8;
 }
-constexpr int FBK = 64;                                        // K-block of the fused forms (128-byte swizzle)
+static_assert(regs_f<1>() == 128 && regs_f<8>() == 168, "register caps of the fused forms");
+constexpr int FBK = 64;     // K-block of the fused forms (128-byte swizzle)
+constexpr int FGROUPS = BM / 8;   // 8-row groups of a CTA's A tile
 
-template <int STAGES_, int BN_, int FSLOTS_, bool PAIR>
+template <int STAGES_, int BN_, bool PAIR>
 struct ShapeF {
-    static constexpr int BK = FBK, STAGES = STAGES_, BN = BN_, FSLOTS = FSLOTS_;
-    static constexpr int A_BYTES = BM * BK * 2;                         // one of hi / lo
+    static constexpr int BK = FBK, STAGES = STAGES_, BN = BN_;
+    static constexpr int A_BYTES = BM * BK * 4;                         // FP32 tile = interleaved hi / lo groups
     static constexpr int B_ROWS = PAIR ? BN / 2 : BN;                   // this CTA's rows of B
     static constexpr int B_BYTES = B_ROWS * BK * 2;
-    static constexpr int STAGE_BYTES = 2 * A_BYTES + 2 * B_BYTES;
-    static constexpr int AF_BYTES = BM * BK * 4;                        // one FP32 staging slot
-    static constexpr size_t SMEM_BYTES = 1024 + (size_t)STAGES * STAGE_BYTES + (size_t)FSLOTS * AF_BYTES +
-                                         (size_t)BN * sizeof(TraitP) + 2 * BM * sizeof(float);
+    static constexpr int STAGE_BYTES = A_BYTES + 2 * B_BYTES;
+    // stages, trait constants, per-row shift and fill
+    static constexpr size_t SMEM_BYTES = 1024 + (size_t)STAGES * STAGE_BYTES + (size_t)BN * sizeof(TraitP) +
+                                         2 * BM * sizeof(float);
     static constexpr uint64_t LAYOUT = 2u;                              // SWIZZLE_128B
-    static constexpr uint32_t SBO = 1024u;
+    static constexpr uint32_t SBO = 1024u;                              // B: 8-row groups back to back
+    static constexpr uint32_t SBO_A = 2048u;                            // A: hi and lo groups interleaved
     static constexpr uint32_t TMEM_COLS = PAIR ? 512u : (2 * BN <= 128 ? 128u : (2 * BN <= 256 ? 256u : 512u));
     static constexpr uint32_t IDESC = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(BN >> 3) << 17) |
                                       ((uint32_t)((PAIR ? 256 : BM) >> 4) << 24);
     static_assert(SMEM_BYTES <= 227u * 1024u, "shared memory of the fused form");
 };
 
-// Converter side of one K-block: FP32 tile (BM x 64, 256 B rows) -> BF16 hi/lo
-// tiles (K-major, 128-byte swizzle: the 16-byte chunk j of row r sits at
-// chunk j ^ (r & 7) of its 128-byte row).  ctid: 0..NC*32-1.  Without NaN
-// values in the chunk (WITH_NAN = false) the fill is never needed.
-template <int NC, bool WITH_NAN>
-__device__ __forceinline__ void convert_a_tile(const float* __restrict__ fa, uint8_t* ahi, uint8_t* alo,
-                                               const float* __restrict__ shift, const float* __restrict__ fill,
-                                               int ctid) {
-    constexpr int CT = NC * 32;
-#pragma unroll 4
-    for (int it = 0; it < BM * (FBK / 4) / CT; ++it) {
-        const int q = it * CT + ctid;
-        const int row = q >> 4, c = q & 15;   // 16 float4 per 64-element row
-        const float4 v = *reinterpret_cast<const float4*>(fa + row * FBK + c * 4);
-        const float sh = shift[row];
-        float e0 = v.x - sh, e1 = v.y - sh, e2 = v.z - sh, e3 = v.w - sh;
-        if constexpr (WITH_NAN) {
-            const float fl = fill[row];
-            e0 = isnan(v.x) ? fl : e0;
-            e1 = isnan(v.y) ? fl : e1;
-            e2 = isnan(v.z) ? fl : e2;
-            e3 = isnan(v.w) ? fl : e3;
-        }
-        const __nv_bfloat162 h01 = __floats2bfloat162_rn(e0, e1), h23 = __floats2bfloat162_rn(e2, e3);
-        const float2 f01 = __bfloat1622float2(h01), f23 = __bfloat1622float2(h23);
-        const __nv_bfloat162 l01 = __floats2bfloat162_rn(e0 - f01.x, e1 - f01.y);
-        const __nv_bfloat162 l23 = __floats2bfloat162_rn(e2 - f23.x, e3 - f23.y);
-        const uint32_t off = (uint32_t)row * 128u + ((((uint32_t)c >> 1) ^ ((uint32_t)row & 7u)) << 4) +
-                             (((uint32_t)c & 1u) << 3);
-        *reinterpret_cast<uint2*>(ahi + off) =
-            make_uint2(*reinterpret_cast<const uint32_t*>(&h01), *reinterpret_cast<const uint32_t*>(&h23));
-        *reinterpret_cast<uint2*>(alo + off) =
-            make_uint2(*reinterpret_cast<const uint32_t*>(&l01), *reinterpret_cast<const uint32_t*>(&l23));
-    }
+// UMMA shared-memory descriptor with an explicit stride between 8-row groups
+// (fields as in smem_desc).
+__device__ __forceinline__ uint64_t smem_desc_sbo(uint32_t saddr, uint32_t sbo, uint64_t layout) {
+    uint64_t d = (uint64_t)((saddr >> 4) & 0x3FFFu);
+    d |= (uint64_t)1u << 16;
+    d |= (uint64_t)(sbo >> 4) << 32;
+    d |= (uint64_t)1u << 46;
+    d |= layout << 61;
+    return d;
 }
 
-// Per-row shift and fill of rows [r0, r0 + BM) (rows at or past xrows: 0).
-template <int NC>
-__device__ __forceinline__ void load_shift_fill(const float* __restrict__ colmean, int center, int r0, int xrows,
-                                                float* shift, float* fill, int ctid) {
-    for (int q = ctid; q < BM; q += NC * 32) {
-        const int row = r0 + q;
-        const float mu = row < xrows ? colmean[row] : 0.f;
-        shift[q] = center ? mu : 0.f;
-        fill[q] = center ? 0.f : mu;
-    }
-}
-
-template <int NC>
-__device__ __forceinline__ void conv_bar() {
-    asm volatile("bar.sync 2, %0;" ::"n"(NC * 32) : "memory");
-}
-// Named barrier 2 of the converter warps, AND-reducing `ok` over them: both
-// warps take the same decision to go on or to leave after a wait.
-template <int NC>
-__device__ __forceinline__ bool conv_bar_all(int ok) {
-    uint32_t r;
-    asm volatile(
-        "{\n\t.reg .pred p, q;\n\tsetp.ne.u32 q, %1, 0;\n\tbar.red.and.pred p, 2, %2, q;\n\tselp.u32 %0, 1, 0, p;\n}\n"
-        : "=r"(r)
-        : "r"(ok), "n"(NC * 32)
-        : "memory");
-    return r != 0;
-}
 __device__ __forceinline__ void fence_proxy_async_smem() {
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
 }
 
-// 1-SM fused form (statistics epilogue, or the store epilogue of the pre-GEMM).
+// Cluster-scope acquire form of the bounded wait: the converters of both CTAs
+// of a pair arrive (release, cluster scope) on the leader's barrier after
+// writing their A tiles, which the leader's MMAs then read.
+__device__ __forceinline__ bool mbar_try_cluster(uint64_t* b, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.acquire.cluster.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(ok)
+        : "r"(su32(b)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+__device__ __forceinline__ bool mbar_wait_cluster(uint64_t* b, uint32_t parity, volatile int* abort_flag) {
+    if (mbar_try_cluster(b, parity)) return true;
+    const unsigned long long t0 = gtimer(), lim = c_wait_ns;
+    while (true) {
+        if (mbar_try_cluster(b, parity)) return true;
+        if (*abort_flag) return false;
+        if (gtimer() - t0 > lim) {
+            *abort_flag = 1;
+            return false;
+        }
+    }
+}
+
+// In-place split of the 8-row groups g = wc, wc + NC, ... of one stage's A
+// tile by converter warp wc (of NC).  Lane l takes the 16-byte chunk c = l %
+// 16 of rows l / 16 + 2 u (u < 4) of a group: it reads the four FP32 chunks,
+// the warp synchronises (the group's 2 KB are read), and it writes their hi
+// and lo halves.  The next group's chunks are read before this group's are
+// written (another 2 KB).
+template <int NC, bool WITH_NAN>
+__device__ __forceinline__ void convert_stage(uint8_t* a, const float* __restrict__ shift,
+                                              const float* __restrict__ fill, int wc, int lane) {
+    constexpr int G = FGROUPS / NC;   // groups per warp: 4 or 8
+    const int c = lane & 15, r0 = lane >> 4;
+    const uint32_t cin = (uint32_t)lane * 16u;   // byte offset of the lane's first chunk in a group
+    float4 cur[4], nxt[4];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) cur[u] = *reinterpret_cast<const float4*>(a + wc * 2048 + cin + u * 512);
+#pragma unroll
+    for (int gi = 0; gi < G; ++gi) {
+        const int g = wc + gi * NC;
+        uint8_t* grp = a + g * 2048;
+        if (gi + 1 < G) {
+#pragma unroll
+            for (int u = 0; u < 4; ++u) nxt[u] = *reinterpret_cast<const float4*>(grp + NC * 2048 + cin + u * 512);
+        }
+        uint2 hv[4], lv[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            const int row = g * 8 + r0 + 2 * u;
+            const float sh = shift[row];
+            const float4 v = cur[u];
+            float e0 = v.x - sh, e1 = v.y - sh, e2 = v.z - sh, e3 = v.w - sh;
+            if constexpr (WITH_NAN) {
+                const float fl = fill[row];
+                e0 = isnan(v.x) ? fl : e0;
+                e1 = isnan(v.y) ? fl : e1;
+                e2 = isnan(v.z) ? fl : e2;
+                e3 = isnan(v.w) ? fl : e3;
+            }
+            const __nv_bfloat162 h01 = __floats2bfloat162_rn(e0, e1), h23 = __floats2bfloat162_rn(e2, e3);
+            const float2 f01 = __bfloat1622float2(h01), f23 = __bfloat1622float2(h23);
+            const __nv_bfloat162 l01 = __floats2bfloat162_rn(e0 - f01.x, e1 - f01.y);
+            const __nv_bfloat162 l23 = __floats2bfloat162_rn(e2 - f23.x, e3 - f23.y);
+            hv[u] = make_uint2(*reinterpret_cast<const uint32_t*>(&h01), *reinterpret_cast<const uint32_t*>(&h23));
+            lv[u] = make_uint2(*reinterpret_cast<const uint32_t*>(&l01), *reinterpret_cast<const uint32_t*>(&l23));
+        }
+        __syncwarp();   // every lane has read this group's FP32 chunks
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            const uint32_t rr = (uint32_t)(r0 + 2 * u);
+            const uint32_t off = rr * 128u + ((((uint32_t)c >> 1) ^ rr) << 4) + (((uint32_t)c & 1u) << 3);
+            *reinterpret_cast<uint2*>(grp + off) = hv[u];
+            *reinterpret_cast<uint2*>(grp + 1024 + off) = lv[u];
+        }
+        if (gi + 1 < G) {
+#pragma unroll
+            for (int u = 0; u < 4; ++u) cur[u] = nxt[u];
+        }
+    }
+}
+
+// Converter loop shared by the fused forms: for each tile of this CTA and
+// K-block in order, wait until the stage's FP32 A tile has landed (`full`,
+// this CTA's barrier), split this warp's groups in place and arrive on the
+// stage's convert barrier (`arrive(s)`).  tile_rows(tile) gives the CTA's
+// first row of a tile.  Each warp keeps the shift and fill of its own rows;
+// warps wait, leave and arrive independently.
+template <int NC, class TileRows, class Arrive>
+__device__ __forceinline__ void run_converters(const float* __restrict__ colmean, const int* __restrict__ has_nan,
+                                               int center, int xrows, int first_tile, int tile_step, int ntiles,
+                                               int nk, int stages, int stage_bytes, uint8_t* smem, uint64_t* full,
+                                               float* shift, float* fill, volatile int* abort_sh,
+                                               TileRows&& tile_rows, Arrive&& arrive) {
+    const int lane = threadIdx.x & 31;
+    const int wc = (int)(threadIdx.x >> 5) - (2 + EPI_WARPS);
+    const bool any_nan = *has_nan != 0;   // written by the statistics kernel before this launch
+    int s = 0;
+    uint32_t ph = 0;
+    for (int tile = first_tile; tile < ntiles; tile += tile_step) {
+        const int r0 = tile_rows(tile);
+        __syncwarp();   // this warp's reads of the previous tile's shift / fill are done
+        for (int q = lane; q < 8 * FGROUPS / NC; q += 32) {   // this warp's rows: groups wc + NC i
+            const int row = (wc + NC * (q >> 3)) * 8 + (q & 7);
+            const float mu = r0 + row < xrows ? colmean[r0 + row] : 0.f;
+            shift[row] = center ? mu : 0.f;
+            fill[row] = center ? 0.f : mu;
+        }
+        __syncwarp();
+        for (int kb = 0; kb < nk; ++kb) {
+            int ok = 1;
+            if (lane == 0) ok = mbar_wait(&full[s], ph, abort_sh) ? 1 : 0;
+            if (!__shfl_sync(0xffffffffu, ok, 0)) return;
+            mbar_try(&full[s], ph);   // this lane's own acquire of the completed phase
+            uint8_t* a = smem + (size_t)s * stage_bytes;
+            if (any_nan)
+                convert_stage<NC, true>(a, shift, fill, wc, lane);
+            else
+                convert_stage<NC, false>(a, shift, fill, wc, lane);
+            fence_proxy_async_smem();   // the stores reach the tensor cores' (async) view
+            __syncwarp();
+            if (lane == 0) arrive(s);
+            if (++s == stages) {
+                s = 0;
+                ph ^= 1u;
+            }
+        }
+    }
+}
+
+// 1-SM fused form.  STORE = false: statistics epilogue (t = traits); STORE =
+// true: the FP32 product is written transposed, C[col * ldc + row] (the
+// pre-GEMM of the per-SNP covariate sums, t = its columns).
 template <int R, class SH, bool STORE>
 __global__ void __launch_bounds__(threads_f<R>()) __maxnreg__(regs_f<R>())
 k_gemm_tcf(const __grid_constant__ CUtensorMap mAf, const __grid_constant__ CUtensorMap mBhi,
-           const __grid_constant__ CUtensorMap mBlo, const float* __restrict__ colmean, const int* __restrict__ has_nan,
-           int center, int xrows, int t, int nk, EpiArgs E, float* __restrict__ cout, int ldc, int raster, int* err) {
+           const __grid_constant__ CUtensorMap mBlo, const float* __restrict__ colmean,
+           const int* __restrict__ has_nan, int center, int xrows, int t, int nk, EpiArgs E,
+           float* __restrict__ cout, int ldc, int raster, int* err) {
     constexpr int NC = conv_warps<R>();
-    constexpr int BK = SH::BK, STAGES = SH::STAGES, BN = SH::BN, FSLOTS = SH::FSLOTS;
+    constexpr int BK = SH::BK, STAGES = SH::STAGES, BN = SH::BN;
     constexpr uint32_t TMEM_COLS = SH::TMEM_COLS;
     constexpr int A_BYTES = SH::A_BYTES, B_BYTES = SH::B_BYTES, STAGE_BYTES = SH::STAGE_BYTES;
-    constexpr int AF_BYTES = SH::AF_BYTES;
     extern __shared__ uint8_t smem_raw[];
     uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~(uintptr_t)1023);
-    uint8_t* fslots = smem + (size_t)STAGES * STAGE_BYTES;
-    TraitP* tps = reinterpret_cast<TraitP*>(fslots + (size_t)FSLOTS * AF_BYTES);
+    TraitP* tps = reinterpret_cast<TraitP*>(smem + (size_t)STAGES * STAGE_BYTES);
     float* shift = reinterpret_cast<float*>(tps + BN);
     float* fill = shift + BM;
-    __shared__ __align__(8) uint64_t full_b[STAGES], empty_bar[STAGES], conv_bar_s[STAGES], fa_full[FSLOTS],
-        fa_empty[FSLOTS], acc_full[2], acc_empty[2], done_bar;
+    __shared__ __align__(8) uint64_t full_bar[STAGES], empty_bar[STAGES], conv_bar_s[STAGES], acc_full[2],
+        acc_empty[2], done_bar;
     __shared__ uint32_t tmem_base_sh;
     __shared__ volatile int abort_sh;
 
@@ -900,13 +994,9 @@ k_gemm_tcf(const __grid_constant__ CUtensorMap mAf, const __grid_constant__ CUte
 
     if (threadIdx.x == 0) {
         for (int s = 0; s < STAGES; ++s) {
-            mbar_init(&full_b[s], 1);
+            mbar_init(&full_bar[s], 1);
             mbar_init(&empty_bar[s], 1);
             mbar_init(&conv_bar_s[s], NC);
-        }
-        for (int f = 0; f < FSLOTS; ++f) {
-            mbar_init(&fa_full[f], 1);
-            mbar_init(&fa_empty[f], NC);
         }
         for (int a = 0; a < 2; ++a) {
             mbar_init(&acc_full[a], 1);
@@ -926,9 +1016,9 @@ k_gemm_tcf(const __grid_constant__ CUtensorMap mAf, const __grid_constant__ CUte
     fence_after();
     const uint32_t tmem_base = tmem_base_sh;
 
-    auto stage_ptr = [&](int s, int which) -> uint8_t* {   // 0 Ahi, 1 Alo, 2 Bhi, 3 Blo
+    auto stage_ptr = [&](int s, int which) -> uint8_t* {   // 0 A (FP32, then hi / lo groups), 2 Bhi, 3 Blo
         uint8_t* b = smem + (size_t)s * STAGE_BYTES;
-        return which < 2 ? b + which * A_BYTES : b + 2 * A_BYTES + (which - 2) * B_BYTES;
+        return which < 2 ? b : b + A_BYTES + (which - 2) * B_BYTES;
     };
     auto tile_mn = [&](int tile, int& m0, int& n0) {
         m0 = (raster == 2 ? tile % m_tiles : tile / n_tiles) * BM;
@@ -938,14 +1028,11 @@ k_gemm_tcf(const __grid_constant__ CUtensorMap mAf, const __grid_constant__ CUte
     if (warp == 0) {
         if (lane == 0) {
             // ---------------- TMA producer ----------------
-            int s = 0, f = 0;
-            uint32_t ph = 0, fph = 0;
-            uint32_t pend_par[FSLOTS];
-            bool pend[FSLOTS];
-            uint32_t bpend_par[STAGES];
-            bool bpend[STAGES];
-            for (int q = 0; q < FSLOTS; ++q) pend[q] = false;
-            for (int q = 0; q < STAGES; ++q) bpend[q] = false;
+            int s = 0;
+            uint32_t ph = 0;
+            uint32_t pend_par[STAGES];
+            bool pend[STAGES];
+            for (int q = 0; q < STAGES; ++q) pend[q] = false;
             bool ok = true;
             int pt = blockIdx.x, pkb = 0;
             auto prefetch_next = [&]() {
@@ -963,35 +1050,26 @@ k_gemm_tcf(const __grid_constant__ CUtensorMap mAf, const __grid_constant__ CUte
                 int m0, n0;
                 tile_mn(tile, m0, n0);
                 for (int kb = 0; kb < nk; ++kb) {
-                    if (!mbar_wait(&empty_bar[s], ph ^ 1u, &abort_sh) || !mbar_wait(&fa_empty[f], fph ^ 1u, &abort_sh)) {
+                    if (!mbar_wait(&empty_bar[s], ph ^ 1u, &abort_sh)) {
                         ok = false;
                         break;
                     }
-                    mbar_expect_tx(&fa_full[f], AF_BYTES);
-                    tma_load_2d(&mAf, &fa_full[f], fslots + (size_t)f * AF_BYTES, kb * BK, m0);
-                    pend[f] = true;
-                    pend_par[f] = fph;
-                    mbar_expect_tx(&full_b[s], 2 * B_BYTES);
-                    tma_load_2d(&mBhi, &full_b[s], stage_ptr(s, 2), kb * BK, n0);
-                    tma_load_2d(&mBlo, &full_b[s], stage_ptr(s, 3), kb * BK, n0);
-                    bpend[s] = true;
-                    bpend_par[s] = ph;
+                    mbar_expect_tx(&full_bar[s], A_BYTES + 2 * B_BYTES);
+                    tma_load_2d(&mAf, &full_bar[s], stage_ptr(s, 0), kb * BK, m0);
+                    tma_load_2d(&mBhi, &full_bar[s], stage_ptr(s, 2), kb * BK, n0);
+                    tma_load_2d(&mBlo, &full_bar[s], stage_ptr(s, 3), kb * BK, n0);
+                    pend[s] = true;
+                    pend_par[s] = ph;
                     prefetch_next();
                     if (++s == STAGES) {
                         s = 0;
                         ph ^= 1u;
                     }
-                    if (++f == FSLOTS) {
-                        f = 0;
-                        fph ^= 1u;
-                    }
                 }
             }
             if (!ok) {   // drain our own copies before the shared memory goes away
-                for (int q = 0; q < FSLOTS; ++q)
-                    if (pend[q]) mbar_drain(&fa_full[q], pend_par[q]);
                 for (int q = 0; q < STAGES; ++q)
-                    if (bpend[q]) mbar_drain(&full_b[q], bpend_par[q]);
+                    if (pend[q]) mbar_drain(&full_bar[q], pend_par[q]);
             }
         }
     } else if (warp == 1) {
@@ -1005,17 +1083,18 @@ k_gemm_tcf(const __grid_constant__ CUtensorMap mAf, const __grid_constant__ CUte
                 fence_after();
                 const uint32_t d_tmem = tmem_base + (uint32_t)(acc * BN);
                 for (int kb = 0; kb < nk; ++kb) {
-                    if (!mbar_wait(&full_b[s], ph, &abort_sh) || !mbar_wait(&conv_bar_s[s], ph, &abort_sh)) {
+                    if (!mbar_wait(&full_bar[s], ph, &abort_sh) || !mbar_wait(&conv_bar_s[s], ph, &abort_sh)) {
                         ok = false;
                         break;
                     }
                     fence_after();
-                    const uint32_t ahi = su32(stage_ptr(s, 0)), alo = su32(stage_ptr(s, 1));
+                    const uint32_t ahi = su32(stage_ptr(s, 0)), alo = ahi + 1024u;
                     const uint32_t bhi = su32(stage_ptr(s, 2)), blo = su32(stage_ptr(s, 3));
 #pragma unroll
                     for (int kk = 0; kk < BK / 16; ++kk) {
                         const uint32_t off = (uint32_t)kk * 32u;
-                        const uint64_t dah = smem_desc<SH>(ahi + off), dal = smem_desc<SH>(alo + off);
+                        const uint64_t dah = smem_desc_sbo(ahi + off, SH::SBO_A, SH::LAYOUT);
+                        const uint64_t dal = smem_desc_sbo(alo + off, SH::SBO_A, SH::LAYOUT);
                         const uint64_t dbh = smem_desc<SH>(bhi + off), dbl = smem_desc<SH>(blo + off);
                         mma_bf16(d_tmem, dah, dbh, SH::IDESC, (kb > 0 || kk > 0) ? 1u : 0u);
                         mma_bf16(d_tmem, dah, dbl, SH::IDESC, 1u);
@@ -1042,49 +1121,15 @@ k_gemm_tcf(const __grid_constant__ CUtensorMap mAf, const __grid_constant__ CUte
         }
     } else if (warp >= 2 + EPI_WARPS) {
         // ---------------- converters ----------------
-        const int ctid = threadIdx.x - 32 * (2 + EPI_WARPS);
-        const bool any_nan = *has_nan != 0;   // written by the statistics kernel before this launch
-        int s = 0, f = 0;
-        uint32_t ph = 0, fph = 0;
-        bool ok = true;
-        for (int tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x) {
-            int m0, n0;
-            tile_mn(tile, m0, n0);
-            conv_bar<NC>();   // the previous tile's conversions have read shift / fill
-            load_shift_fill<NC>(colmean, center, m0, xrows, shift, fill, ctid);
-            conv_bar<NC>();
-            for (int kb = 0; kb < nk; ++kb) {
-                int okw = 1;
-                if (lane == 0) okw = mbar_wait(&fa_full[f], fph, &abort_sh) ? 1 : 0;
-                okw = __shfl_sync(0xffffffffu, okw, 0);
-                if (!conv_bar_all<NC>(okw)) {   // both converter warps leave together
-                    ok = false;
-                    break;
-                }
-                mbar_try(&fa_full[f], fph);
-                if (any_nan)
-                    convert_a_tile<NC, true>(reinterpret_cast<const float*>(fslots + (size_t)f * AF_BYTES),
-                                             stage_ptr(s, 0), stage_ptr(s, 1), shift, fill, ctid);
-                else
-                    convert_a_tile<NC, false>(reinterpret_cast<const float*>(fslots + (size_t)f * AF_BYTES),
-                                              stage_ptr(s, 0), stage_ptr(s, 1), shift, fill, ctid);
-                fence_proxy_async_smem();   // the stores reach the tensor cores' (async) view
-                __syncwarp();
-                if (lane == 0) {
-                    mbar_arrive(&fa_empty[f]);
-                    mbar_arrive(&conv_bar_s[s]);
-                }
-                if (++s == STAGES) {
-                    s = 0;
-                    ph ^= 1u;
-                }
-                if (++f == FSLOTS) {
-                    f = 0;
-                    fph ^= 1u;
-                }
-            }
-        }
-        (void)ph;
+        run_converters<NC>(
+            colmean, has_nan, center, xrows, blockIdx.x, gridDim.x, ntiles, nk, STAGES, STAGE_BYTES, smem, full_bar,
+            shift, fill, &abort_sh,
+            [&](int tile) {
+                int m0, n0;
+                tile_mn(tile, m0, n0);
+                return m0;
+            },
+            [&](int s) { mbar_arrive(&conv_bar_s[s]); });
     } else if constexpr (STORE) {
         // ---------------- store epilogue ----------------
         const int lg = warp & 3;
@@ -1092,27 +1137,28 @@ k_gemm_tcf(const __grid_constant__ CUtensorMap mAf, const __grid_constant__ CUte
         int acc = 0;
         uint32_t aph = 0;
         for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
-            if (abort_sh) break;
+            if (epi_bar_any(abort_sh)) break;
             int m0, n0;
             tile_mn(tile, m0, n0);
             int ok = 1;
             if (lane == 0) ok = mbar_wait(&acc_full[acc], aph, &abort_sh) ? 1 : 0;
             ok = __shfl_sync(0xffffffffu, ok, 0);
-            if (!ok) break;
-            mbar_try(&acc_full[acc], aph);
-            fence_after();
-            const int row = m0 + lg * 32 + lane;
-            for (int c0 = cb; c0 < cb + BN / 2 && n0 + c0 < t; c0 += 32) {
-                uint32_t v[32];
-                tmem_ld32(tmem_base + ((uint32_t)(lg * 32) << 16) + (uint32_t)(acc * BN + c0), v);
-                const int qmax = min(32, t - n0 - c0);
-                if (row < xrows)
+            if (ok) {
+                mbar_try(&acc_full[acc], aph);
+                fence_after();
+                const int row = m0 + lg * 32 + lane;
+                for (int c0 = cb; c0 < cb + BN / 2 && n0 + c0 < t; c0 += 32) {
+                    uint32_t v[32];
+                    tmem_ld32(tmem_base + ((uint32_t)(lg * 32) << 16) + (uint32_t)(acc * BN + c0), v);
+                    const int qmax = min(32, t - n0 - c0);
+                    if (row < xrows)
 #pragma unroll
-                    for (int q = 0; q < 32; ++q)
-                        if (q < qmax) cout[(size_t)(n0 + c0 + q) * ldc + row] = __uint_as_float(v[q]);
+                        for (int q = 0; q < 32; ++q)
+                            if (q < qmax) cout[(size_t)(n0 + c0 + q) * ldc + row] = __uint_as_float(v[q]);
+                }
+                fence_before();
+                mbar_arrive(&acc_empty[acc]);
             }
-            fence_before();
-            mbar_arrive(&acc_empty[acc]);
             if (++acc == 2) {
                 acc = 0;
                 aph ^= 1u;
@@ -1168,54 +1214,28 @@ k_gemm_tcf(const __grid_constant__ CUtensorMap mAf, const __grid_constant__ CUte
     if (threadIdx.x == 0 && abort_sh) atomicExch(err, 1);
 }
 
-// Cluster-scope acquire form of the bounded wait: the converters of both CTAs
-// of a pair arrive (release, cluster scope) on the leader's barrier after
-// writing their A tiles, which the leader's MMAs then read.
-__device__ __forceinline__ bool mbar_try_cluster(uint64_t* b, uint32_t parity) {
-    uint32_t ok;
-    asm volatile(
-        "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.acquire.cluster.shared::cta.b64 p, [%1], %2;\n\t"
-        "selp.u32 %0, 1, 0, p;\n}\n"
-        : "=r"(ok)
-        : "r"(su32(b)), "r"(parity)
-        : "memory");
-    return ok != 0;
-}
-__device__ __forceinline__ bool mbar_wait_cluster(uint64_t* b, uint32_t parity, volatile int* abort_flag) {
-    if (mbar_try_cluster(b, parity)) return true;
-    const unsigned long long t0 = gtimer(), lim = c_wait_ns;
-    while (true) {
-        if (mbar_try_cluster(b, parity)) return true;
-        if (*abort_flag) return false;
-        if (gtimer() - t0 > lim) {
-            *abort_flag = 1;
-            return false;
-        }
-    }
-}
-
 // CTA-pair fused form (statistics epilogue): as k_gemm_tc2, with each CTA's
-// A rows read as FP32 and split by its converter warps; the leader's MMA
-// issuer waits for the B bytes of both CTAs (leader's full barrier) and for
-// the converters of both CTAs (leader's convert barrier).
+// FP32 A rows loaded on its own barrier and split in place by its converter
+// warps; the leader's MMA issuer waits for the B bytes of both CTAs (leader's
+// B barrier) and for the converters of both CTAs (leader's convert barrier).
+// The MMA commits reach the empty barriers of both CTAs, which each CTA's
+// producer waits on.
 template <int R, class SH>
 __global__ void __launch_bounds__(threads_f<R>()) __maxnreg__(regs_f<R>())
 k_gemm_tc2f(const __grid_constant__ CUtensorMap mAf, const __grid_constant__ CUtensorMap mBhi,
             const __grid_constant__ CUtensorMap mBlo, const float* __restrict__ colmean,
             const int* __restrict__ has_nan, int center, int xrows, int t, int nk, EpiArgs E, int raster, int* err) {
     constexpr int NC = conv_warps<R>();
-    constexpr int BK = SH::BK, STAGES = SH::STAGES, BN = SH::BN, FSLOTS = SH::FSLOTS;
+    constexpr int BK = SH::BK, STAGES = SH::STAGES, BN = SH::BN;
     constexpr uint32_t TMEM_COLS = SH::TMEM_COLS;
     constexpr int A_BYTES = SH::A_BYTES, B_BYTES = SH::B_BYTES, STAGE_BYTES = SH::STAGE_BYTES;
-    constexpr int AF_BYTES = SH::AF_BYTES;
     extern __shared__ uint8_t smem_raw[];
     uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~(uintptr_t)1023);
-    uint8_t* fslots = smem + (size_t)STAGES * STAGE_BYTES;
-    TraitP* tps = reinterpret_cast<TraitP*>(fslots + (size_t)FSLOTS * AF_BYTES);
+    TraitP* tps = reinterpret_cast<TraitP*>(smem + (size_t)STAGES * STAGE_BYTES);
     float* shift = reinterpret_cast<float*>(tps + BN);
     float* fill = shift + BM;
-    __shared__ __align__(8) uint64_t full_b[STAGES], empty_bar[STAGES], conv_bar_s[STAGES], fa_full[FSLOTS],
-        fa_empty[FSLOTS], acc_full[2], acc_empty[2], done_bar;
+    __shared__ __align__(8) uint64_t full_a[STAGES], full_b[STAGES], empty_bar[STAGES], conv_bar_s[STAGES],
+        acc_full[2], acc_empty[2], done_bar;
     __shared__ uint32_t tmem_base_sh;
     __shared__ volatile int abort_sh;
 
@@ -1228,13 +1248,10 @@ k_gemm_tc2f(const __grid_constant__ CUtensorMap mAf, const __grid_constant__ CUt
 
     if (threadIdx.x == 0) {
         for (int s = 0; s < STAGES; ++s) {
+            mbar_init(&full_a[s], 1);
             mbar_init(&full_b[s], 1);
             mbar_init(&empty_bar[s], 1);
             mbar_init(&conv_bar_s[s], 2 * NC);   // leader's copy: the converter warps of both CTAs
-        }
-        for (int f = 0; f < FSLOTS; ++f) {
-            mbar_init(&fa_full[f], 1);
-            mbar_init(&fa_empty[f], NC);
         }
         for (int a = 0; a < 2; ++a) {
             mbar_init(&acc_full[a], 1);
@@ -1257,7 +1274,7 @@ k_gemm_tc2f(const __grid_constant__ CUtensorMap mAf, const __grid_constant__ CUt
 
     auto stage_ptr = [&](int s, int which) -> uint8_t* {
         uint8_t* b = smem + (size_t)s * STAGE_BYTES;
-        return which < 2 ? b + which * A_BYTES : b + 2 * A_BYTES + (which - 2) * B_BYTES;
+        return which < 2 ? b : b + A_BYTES + (which - 2) * B_BYTES;
     };
     auto tile_mn = [&](int tile, int& m0, int& n0) {
         m0 = (raster == 2 ? tile % m_tiles : tile / n_tiles) * 2 * BM;
@@ -1267,11 +1284,11 @@ k_gemm_tc2f(const __grid_constant__ CUtensorMap mAf, const __grid_constant__ CUt
     if (warp == 0) {
         if (lane == 0) {
             // ---------------- TMA producer (both CTAs) ----------------
-            int s = 0, f = 0;
-            uint32_t ph = 0, fph = 0;
-            uint32_t pend_par[FSLOTS];
-            bool pend[FSLOTS];
-            for (int q = 0; q < FSLOTS; ++q) pend[q] = false;
+            int s = 0;
+            uint32_t ph = 0;
+            uint32_t pend_par[STAGES];
+            bool pend[STAGES];
+            for (int q = 0; q < STAGES; ++q) pend[q] = false;
             bool ok = true;
             int pt = pair, pkb = 0;
             auto prefetch_next = [&]() {
@@ -1290,14 +1307,14 @@ k_gemm_tc2f(const __grid_constant__ CUtensorMap mAf, const __grid_constant__ CUt
                 tile_mn(tile, m0, n0);
                 const int ma = m0 + (int)rank * BM, nb = n0 + (int)rank * (BN / 2);
                 for (int kb = 0; kb < nk; ++kb) {
-                    if (!mbar_wait(&empty_bar[s], ph ^ 1u, &abort_sh) || !mbar_wait(&fa_empty[f], fph ^ 1u, &abort_sh)) {
+                    if (!mbar_wait(&empty_bar[s], ph ^ 1u, &abort_sh)) {
                         ok = false;
                         break;
                     }
-                    mbar_expect_tx(&fa_full[f], AF_BYTES);
-                    tma_load_2d(&mAf, &fa_full[f], fslots + (size_t)f * AF_BYTES, kb * BK, ma);
-                    pend[f] = true;
-                    pend_par[f] = fph;
+                    mbar_expect_tx(&full_a[s], A_BYTES);   // own FP32 rows, own barrier (the converters')
+                    tma_load_2d(&mAf, &full_a[s], stage_ptr(s, 0), kb * BK, ma);
+                    pend[s] = true;
+                    pend_par[s] = ph;
                     const uint32_t fb = map_to_rank(&full_b[s], 0);
                     if (leader) mbar_expect_tx(&full_b[s], 2 * 2 * B_BYTES);
                     tma_load_2d_pair(&mBhi, fb, stage_ptr(s, 2), kb * BK, nb);
@@ -1307,15 +1324,11 @@ k_gemm_tc2f(const __grid_constant__ CUtensorMap mAf, const __grid_constant__ CUt
                         s = 0;
                         ph ^= 1u;
                     }
-                    if (++f == FSLOTS) {
-                        f = 0;
-                        fph ^= 1u;
-                    }
                 }
             }
-            if (!ok) {   // own FP32 copies; the leader's full barriers see both CTAs' B copies
-                for (int q = 0; q < FSLOTS; ++q)
-                    if (pend[q]) mbar_drain(&fa_full[q], pend_par[q]);
+            if (!ok) {   // own FP32 copies; the leader's B barriers see both CTAs' B copies
+                for (int q = 0; q < STAGES; ++q)
+                    if (pend[q]) mbar_drain(&full_a[q], pend_par[q]);
                 if (leader)
                     for (int q = 0; q < STAGES; ++q) mbar_drain(&full_b[q], 0), mbar_drain(&full_b[q], 1);
             }
@@ -1336,12 +1349,13 @@ k_gemm_tc2f(const __grid_constant__ CUtensorMap mAf, const __grid_constant__ CUt
                         break;
                     }
                     fence_after();
-                    const uint32_t ahi = su32(stage_ptr(s, 0)), alo = su32(stage_ptr(s, 1));
+                    const uint32_t ahi = su32(stage_ptr(s, 0)), alo = ahi + 1024u;
                     const uint32_t bhi = su32(stage_ptr(s, 2)), blo = su32(stage_ptr(s, 3));
 #pragma unroll
                     for (int kk = 0; kk < BK / 16; ++kk) {
                         const uint32_t off = (uint32_t)kk * 32u;
-                        const uint64_t dah = smem_desc<SH>(ahi + off), dal = smem_desc<SH>(alo + off);
+                        const uint64_t dah = smem_desc_sbo(ahi + off, SH::SBO_A, SH::LAYOUT);
+                        const uint64_t dal = smem_desc_sbo(alo + off, SH::SBO_A, SH::LAYOUT);
                         const uint64_t dbh = smem_desc<SH>(bhi + off), dbl = smem_desc<SH>(blo + off);
                         mma_bf16_pair(d_tmem, dah, dbh, SH::IDESC, (kb > 0 || kk > 0) ? 1u : 0u);
                         mma_bf16_pair(d_tmem, dah, dbl, SH::IDESC, 1u);
@@ -1366,45 +1380,15 @@ k_gemm_tc2f(const __grid_constant__ CUtensorMap mAf, const __grid_constant__ CUt
         if (lane == 0) mbar_drain(&done_bar, 0);      // (a CTA pair that issued nothing waits out the bound once)
     } else if (warp >= 2 + EPI_WARPS) {
         // ---------------- converters (both CTAs, own 128 rows) ----------------
-        const int ctid = threadIdx.x - 32 * (2 + EPI_WARPS);
-        const bool any_nan = *has_nan != 0;   // written by the statistics kernel before this launch
-        int s = 0, f = 0;
-        uint32_t fph = 0;
-        bool ok = true;
-        for (int tile = pair; tile < ntiles && ok; tile += npairs) {
-            int m0, n0;
-            tile_mn(tile, m0, n0);
-            conv_bar<NC>();
-            load_shift_fill<NC>(colmean, center, m0 + (int)rank * BM, xrows, shift, fill, ctid);
-            conv_bar<NC>();
-            for (int kb = 0; kb < nk; ++kb) {
-                int okw = 1;
-                if (lane == 0) okw = mbar_wait(&fa_full[f], fph, &abort_sh) ? 1 : 0;
-                okw = __shfl_sync(0xffffffffu, okw, 0);
-                if (!conv_bar_all<NC>(okw)) {
-                    ok = false;
-                    break;
-                }
-                mbar_try(&fa_full[f], fph);
-                if (any_nan)
-                    convert_a_tile<NC, true>(reinterpret_cast<const float*>(fslots + (size_t)f * AF_BYTES),
-                                             stage_ptr(s, 0), stage_ptr(s, 1), shift, fill, ctid);
-                else
-                    convert_a_tile<NC, false>(reinterpret_cast<const float*>(fslots + (size_t)f * AF_BYTES),
-                                              stage_ptr(s, 0), stage_ptr(s, 1), shift, fill, ctid);
-                fence_proxy_async_smem();
-                __syncwarp();
-                if (lane == 0) {
-                    mbar_arrive(&fa_empty[f]);
-                    mbar_arrive_cluster(map_to_rank(&conv_bar_s[s], 0));
-                }
-                if (++s == STAGES) s = 0;
-                if (++f == FSLOTS) {
-                    f = 0;
-                    fph ^= 1u;
-                }
-            }
-        }
+        run_converters<NC>(
+            colmean, has_nan, center, xrows, pair, npairs, ntiles, nk, STAGES, STAGE_BYTES, smem, full_a, shift,
+            fill, &abort_sh,
+            [&](int tile) {
+                int m0, n0;
+                tile_mn(tile, m0, n0);
+                return m0 + (int)rank * BM;
+            },
+            [&](int s) { mbar_arrive_cluster(map_to_rank(&conv_bar_s[s], 0)); });
     } else {
         // ---------------- epilogue (both CTAs, own 128 rows) ----------------
         const int ew = warp - 2;
@@ -1578,12 +1562,14 @@ static cudaError_t go_any(int variant, int raster, const __nv_bfloat16* Xhi, con
 
 
 // FP32 K-major matrix of `rows` rows of ld floats (k_valid of them read, the
-// rest of each 64-wide K-block filled with zeros), boxes of 64 x 128, no
-// swizzle (the converter warps read it); ld * 4 and the base must be 16-byte
-// multiples.
+// rest of each 64-wide K-block and rows past `rows` filled with zeros), boxes
+// of 64 x 128, no swizzle (rows at 256-byte strides, split in place by the
+// converter warps); ld * 4 and k_valid * 4 must be 16-byte multiples and the
+// base 16-byte aligned.
 static bool make_map_f32(CUtensorMap* m, const float* ptr, int rows, int k_valid, size_t ld) {
     EncodeTiledFn fn = encode_fn();
-    if (!fn || rows <= 0 || k_valid <= 0 || (ld * 4) % 16 != 0 || (reinterpret_cast<uintptr_t>(ptr) & 15) != 0)
+    if (!fn || rows <= 0 || k_valid <= 0 || (k_valid % 4) != 0 || (ld % 4) != 0 ||
+        (reinterpret_cast<uintptr_t>(ptr) & 15) != 0)
         return false;
     const cuuint64_t gdim[2] = {(cuuint64_t)k_valid, (cuuint64_t)rows};
     const cuuint64_t gstride[1] = {(cuuint64_t)ld * 4};
@@ -1657,9 +1643,10 @@ static cudaError_t go2_f(const float* X, size_t ldx, int n, int xrows, const flo
                               n_pad / SH::BK, E, raster, err);
 }
 
-using FNarrow64 = ShapeF<3, 64, 2, false>;
-using FNarrow128 = ShapeF<2, 128, 2, false>;
-using FPair = ShapeF<2, 256, 2, true>;
+// the stage counts of the split forms' tiles (Shape<64, 4, 64>, Shape<64, 3, 128>, Shape2<64, 3>)
+using FNarrow64 = ShapeF<4, 64, false>;
+using FNarrow128 = ShapeF<3, 128, false>;
+using FPair = ShapeF<3, 256, true>;
 
 // Fused forms of the statistics GEMM: trait blocks of at most 128 traits on
 // the 1-SM narrow tiles, wider ones on CTA pairs (the fused pair form serves

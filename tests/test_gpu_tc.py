@@ -112,7 +112,7 @@ def test_fused_split_gemms_give_the_split_copy_bits(case, monkeypatch):
     split-copy forms: every trait-tile width (1-SM 64 / 128 columns, CTA pairs),
     r = 1, 2, 4, NaN dosages, centred and uncentred columns, ragged SNP and trait
     edges, several tiles per CTA."""
-    from test_gpu_parity import _multicol
+    from quirk_cases import multicol as _multicol
     env = {}
     r = 1
     if case == "narrow64":
