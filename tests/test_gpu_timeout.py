@@ -32,8 +32,15 @@ def _engine(ds, prec):
 
 @pytest.mark.parametrize("prec", [E.MIXED, E.PLAIN])
 def test_wait_timeout_is_reported_and_the_next_engine_is_correct(monkeypatch, prec):
-    # t > 128: the CTA-pair tensor-core GEMM (mixed form); n % 4 == 0: TMA bulk staging in the statistics kernel
-    ds = synth.generate(synth.scaled(0, n=1024, m=300, t=160, l=4, miss_mode="patterns", n_patterns=3, seed=97))
+    """Mixed form: t > 128 takes the CTA-pair tensor-core GEMM, whose accumulator and stage
+    waits last a whole main loop.  Plain form: its only bounded waits are the statistics
+    kernel's staging waits (TMA bulk copies, n % 4 == 0); with 160 KB columns (n = 40,000)
+    each copy outlasts the %globaltimer's update step, so the 1 ns bound runs out."""
+    if prec == E.MIXED:
+        w = dict(n=1024, m=300, t=160)
+    else:
+        w = dict(n=40000, m=64, t=16)
+    ds = synth.generate(synth.scaled(0, l=4, miss_mode="patterns", n_patterns=3, seed=97, **w))
     monkeypatch.setenv("OA_WAIT_LIMIT_NS", "1")
     eng = _engine(ds, prec)
     with pytest.raises(E.OAError) as ei:
