@@ -291,6 +291,8 @@ struct oa_engine {
     // covariates
     DBuf<double> Q64, Rinv;
     DBuf<float> Qr;
+    DBuf<double> qsum;   // [LP] column sums of Qr
+    DBuf<double> Afull_lean;   // [chunk*r][LEAN_QX_L] all-rows projection from k_snp_lean
     bool have_cov = false;
     bool center = false;   // the first covariate is constant: SNP columns are taken relative to their means
     bool fuse_split = false;  // the tensor-core GEMMs split FP32 columns in shared memory where they can
@@ -422,7 +424,7 @@ int live_engines(int device, int delta) {
 // Every device buffer of an engine (release, footprint).
 template <class F>
 void for_each_buf(oa_engine* e, F&& f) {
-    f(e->Q64); f(e->Rinv); f(e->Qr);
+    f(e->Q64); f(e->Rinv); f(e->Qr); f(e->qsum); f(e->Afull_lean);
     f(e->Yraw); f(e->Yt); f(e->Yhi); f(e->Ylo);
     f(e->tsums); f(e->rss0); f(e->b0); f(e->W); f(e->zQ);
     f(e->tcounts); f(e->pat); f(e->zset); f(e->nobs); f(e->set_off); f(e->set_rows); f(e->set_rep);
@@ -919,14 +921,24 @@ oa_status stats_gather(oa_engine* e, const float* X, int mbc) {
 // each row set) -> pre-GEMM C2 = [Q | Q o m_1 | ...]'X -> k_schur.
 // SNPs per CTA group of k_snp_lean: requested, else two CTAs per SM where a
 // double-buffered group fits in half the shared memory (a power of two <= 8 / r)
+// With two or more columns per SNP and at most LEAN_QX_L covariates, k_snp_lean also sums the
+// all-rows covariate projection A = Q'X of every column (short FP32 partial sums, FP64 across
+// warps) for k_schur: the pre-GEMM's A (FP32 sums over all n rows; BF16 hi/lo products in the mixed
+// form) is the largest error of the Schur complements and of var_x when D - A'A cancels, which two
+// correlated columns per SNP make likely (an interaction with a covariate).  Those kernels take
+// groups of at most LEAN_QX_NC columns.
+bool want_lean_qx(const oa_engine* e) { return e->ru >= 2 && e->l <= LEAN_QX_L && e->r <= LEAN_QX_NC; }
+
 int lean_group(const oa_engine* e) {
+    const int cap = want_lean_qx(e) ? LEAN_QX_NC / e->r : 8 / e->r;
     if (e->lean_spb > 0) {
         int s = 1;
         while (s * 2 <= e->lean_spb) s *= 2;
-        return std::min(s, 8 / e->r);
+        return std::min(s, cap);
     }
     int s = 1;
-    while (s * 2 <= 8 / e->r && lean_smem_bytes(e->r, e->n_pad, s * 2, 2, 0) <= 100 * 1024) s *= 2;
+    while (s * 2 <= cap && lean_smem_bytes(e->r, e->n_pad, s * 2, 2, 0, true, want_lean_qx(e)) <= 100 * 1024)
+        s *= 2;
     return s;
 }
 
@@ -944,9 +956,10 @@ oa_status lean_plan(oa_engine* e) {
     const bool heavy_sets = set_rows > e->n;
     int nbuf = e->lean_nbuf ? e->lean_nbuf : (heavy_sets ? 1 : 2);
     const bool xi = e->lean_xi >= 0 ? e->lean_xi == 1 : !heavy_sets;
-    while (spb > 1 && lean_smem_bytes(R, e->n_pad, spb, nbuf, 0, xi) > 200 * 1024) spb /= 2;
-    if (lean_smem_bytes(R, e->n_pad, spb, nbuf, 0, xi) > 200 * 1024) nbuf = 1;
-    const size_t base = lean_smem_bytes(R, e->n_pad, spb, nbuf, 0, xi);
+    const bool qx = want_lean_qx(e);
+    while (spb > 1 && lean_smem_bytes(R, e->n_pad, spb, nbuf, 0, xi, qx) > 200 * 1024) spb /= 2;
+    if (lean_smem_bytes(R, e->n_pad, spb, nbuf, 0, xi, qx) > 200 * 1024) nbuf = 1;
+    const size_t base = lean_smem_bytes(R, e->n_pad, spb, nbuf, 0, xi, qx);
     const size_t per_item = (size_t)spb * R * R * 4;
     int max_items = 1;
     for (int s2 = 0; s2 < e->nsets; ++s2)
@@ -975,7 +988,7 @@ oa_status lean_plan(oa_engine* e) {
     e->lp.items_cap = cap;
     e->lp.npass = e->nsets > 0 ? (int)passes.size() - 1 : 0;
     e->lp.xi = xi;
-    e->lp.smem = lean_smem_bytes(R, e->n_pad, spb, nbuf, cap, xi);
+    e->lp.smem = lean_smem_bytes(R, e->n_pad, spb, nbuf, cap, xi, qx);
     return OA_OK;
 }
 
@@ -1021,8 +1034,17 @@ oa_status stats_pre(oa_engine* e, const float* X, size_t ldx, const int* xrows, 
     A.Xhi = e->Xhi.p;
     A.Xlo = e->Xlo.p;
     A.err = reinterpret_cast<int*>(e->counters.p + 3);
+    const bool qx = want_lean_qx(e) && oa_lean_has_qx(R, spb);
+    if (qx) {
+        OA_CHECK(e->Afull_lean.ensure((size_t)e->chunk * R * LEAN_QX_L));
+        A.Qr = e->Qr.p;
+        A.LP = e->LP;
+        A.l = e->l;
+        A.qsum = e->qsum.p;
+        A.Afull = e->Afull_lean.p;
+    }
     const int groups = (mbc + spb - 1) / spb;
-    const int per_sm = std::max(1, oa_lean_ctas_per_sm(R, spb, smem));
+    const int per_sm = std::max(1, oa_lean_ctas_per_sm(R, spb, smem, qx));
     const int grid = std::min(groups, e->sm_count * per_sm);
     OA_CU(oa_launch_snp_lean(R, spb, A, grid, smem, e->st));
     ++e->launches;
@@ -1061,6 +1083,7 @@ oa_status stats_pre(oa_engine* e, const float* X, size_t ldx, const int* xrows, 
     S.rr = e->ru;
     S.qdel = quirk_on(e) ? e->qdel.p : nullptr;
     S.qK = quirk_on(e) ? e->qK.p : nullptr;
+    S.Afull_lean = qx ? e->Afull_lean.p : nullptr;
     OA_CU(oa_launch_schur(R, S, e->st));
     ++e->launches;
     return OA_OK;
@@ -1940,11 +1963,16 @@ oa_status oa_set_covariates(oa_engine* e, const float* xl) {
     std::vector<float> Qr((size_t)n * e->LP, 0.f);
     for (int k = 0; k < n; ++k)
         for (int q = 0; q < l; ++q) Qr[(size_t)k * e->LP + q] = (float)Q[(size_t)q * n + k];
+    std::vector<double> qsum(e->LP, 0.0);   // column sums of the FP32 basis (the lean kernel's projection)
+    for (int k = 0; k < n; ++k)
+        for (int q = 0; q < l; ++q) qsum[q] += (double)Qr[(size_t)k * e->LP + q];
     OA_CHECK(e->Q64.ensure((size_t)n * l));
     OA_CHECK(e->Qr.ensure(Qr.size()));
+    OA_CHECK(e->qsum.ensure(qsum.size()));
     OA_CHECK(e->Rinv.ensure((size_t)l * l));
     OA_CU(cudaMemcpyAsync(e->Q64.p, Q.data(), sizeof(double) * Q.size(), cudaMemcpyHostToDevice, e->st));
     OA_CU(cudaMemcpyAsync(e->Qr.p, Qr.data(), sizeof(float) * Qr.size(), cudaMemcpyHostToDevice, e->st));
+    OA_CU(cudaMemcpyAsync(e->qsum.p, qsum.data(), sizeof(double) * qsum.size(), cudaMemcpyHostToDevice, e->st));
     OA_CU(cudaMemcpyAsync(e->Rinv.p, Ri.data(), sizeof(double) * Ri.size(), cudaMemcpyHostToDevice, e->st));
     OA_CU(cudaStreamSynchronize(e->st));
     // An intercept as the first covariate makes every quantity of the scan

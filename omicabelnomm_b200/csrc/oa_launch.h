@@ -11,7 +11,8 @@ cudaError_t oa_launch_snp_stats(int R, int LP, const StatsArgs& A, int grid, siz
 // spb: SNPs per CTA group, a power of two <= 8 / R
 cudaError_t oa_launch_snp_lean(int R, int spb, const LeanArgs& A, int grid, size_t smem, cudaStream_t st);
 // resident CTAs of k_snp_lean per SM for this shared-memory size (0 on error)
-int oa_lean_ctas_per_sm(int R, int spb, size_t smem);
+int oa_lean_ctas_per_sm(int R, int spb, size_t smem, bool qx = false);
+bool oa_lean_has_qx(int R, int spb);
 cudaError_t oa_launch_schur(int R, const SchurArgs& S, cudaStream_t st);
 // pre-GEMM C[col * ldc + row] = sum_k X[row][k] B[col][k], col < c2 (tensor-core and SIMT forms)
 cudaError_t oa_launch_pre_tc(const __nv_bfloat16* Xhi, const __nv_bfloat16* Xlo, int xrows,

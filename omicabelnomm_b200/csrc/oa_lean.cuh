@@ -40,29 +40,41 @@ struct LeanArgs {
     int use_xi;           // with several columns per group: keep the row-interleaved copy for the set pass
     int center;           // take each column relative to its mean (valid when XL holds an intercept)
     int* err;
+    // all-rows covariate projection A = Q'(x - shift) of every column, summed here (short FP32
+    // partial sums, FP64 across warps) instead of taken from the pre-GEMM, or null: with two or
+    // more columns per SNP the all-rows Schur complement D - A'A (var_x) and the pattern systems
+    // cancel a large part of D, and the pre-GEMM's long FP32 / BF16-split sums of A are then the
+    // largest error of the statistics (the qx kernels, at most LEAN_QX_L covariates)
+    const float* Qr;      // [n][LP] the orthonormal covariate basis (FP32), rows zero past l
+    int LP, l;
+    const double* qsum;   // [LP] column sums of Qr (FP64)
+    double* Afull;        // [mb*R][LEAN_QX_L]: A of column c, covariate q at Afull[c * LEAN_QX_L + q]
 };
 
 constexpr int LEAN_THREADS = 512;
 constexpr int LEAN_WARPS = LEAN_THREADS / 32;
 constexpr int LEAN_ITEM_ROWS = 256;     // rows per work item of the set pass
 constexpr int LEAN_STAGE_U = 8;         // elements per thread and step of the element-wise staging
+constexpr int LEAN_QX_L = 8;            // covariates of the in-kernel projection (l <= 8)
+constexpr int LEAN_QX_NC = 4;           // columns per group of the qx kernels
 
 // Shared memory of k_snp_lean: nbuf column buffers (stride n_pad floats, the
 // tail [n, n_pad) kept zero) | with several columns per group, the centred
 // columns interleaved by row ([n_pad][spb*R], one vector load per row in the
 // set pass) | per-item partial sums | reduction scratch.
 __host__ __device__ inline size_t lean_smem_bytes(int R, int n_pad, int spb, int nbuf, int items_cap,
-                                                  bool use_xi = true) {
+                                                  bool use_xi = true, bool qx = false) {
     const int NC = spb * R;
-    const int NQ = 2 * NC + spb * R * R;
+    const int NQ = 2 * NC + spb * R * R + (qx ? NC * LEAN_QX_L : 0);
     return (size_t)(nbuf + (NC > 1 && use_xi ? 1 : 0)) * NC * n_pad * 4 + (size_t)items_cap * spb * R * R * 4 +
            (size_t)(LEAN_WARPS + 1) * NQ * 8 + 64;
 }
 
 // Block-wide sum of NV floats per thread: FP32 within a warp, FP64 across
-// warps (warp 0, fixed order); the result is valid in out[] on every thread.
-template <int NV>
-__device__ __forceinline__ void block_sum_fd(float (&v)[NV], double (&out)[NV], double* red /* [warps + 1][NV] */) {
+// warps (warp 0, fixed order); the first NB sums are copied to out[] on every
+// thread, all NV stay at red + LEAN_WARPS * NV until red is reused.
+template <int NV, int NB = NV>
+__device__ __forceinline__ void block_sum_fd(float (&v)[NV], double (&out)[NB], double* red /* [warps + 1][NV] */) {
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
 #pragma unroll
     for (int q = 0; q < NV; ++q) v[q] = warp_sumf(v[q]);
@@ -80,7 +92,7 @@ __device__ __forceinline__ void block_sum_fd(float (&v)[NV], double (&out)[NV], 
     }
     __syncthreads();
 #pragma unroll
-    for (int q = 0; q < NV; ++q) out[q] = bc[q];
+    for (int q = 0; q < NB; ++q) out[q] = bc[q];
 }
 
 // BF16 hi/lo of 8 floats (x = hi + lo to ~2^-17 relative), packed
@@ -121,7 +133,7 @@ __device__ __forceinline__ void split8(const float4 p0, const float4 p1, uint4& 
 //           the interleaved centred columns per row, shuffle reduction)
 //           lands in its own shared-memory slot, and a set's sum adds its
 //           items in order.  No atomics: the sums are bit-reproducible.
-template <int R, int SPB, bool BULK>
+template <int R, int SPB, bool BULK, bool QX = false>
 __global__ void __launch_bounds__(LEAN_THREADS)
 k_snp_lean(LeanArgs A) {
     extern __shared__ __align__(128) unsigned char smem_raw[];
@@ -246,9 +258,13 @@ k_snp_lean(LeanArgs A) {
         float sh[NC];                          // subtracted from every value (centring), 0 without
         bool cnan[NC];
         {
-            constexpr int NV = NC + K2;        // [column sums | cross products]
+            constexpr int NQX = QX ? NC * LEAN_QX_L : 0;
+            constexpr int NV = NC + K2 + NQX;  // [column sums | cross products | Q'x of the raw columns]
+            constexpr int NB = NC + K2;        // sums every thread keeps (Q'x stays in shared memory)
+            static_assert(!QX || NC <= LEAN_QX_NC, "columns of the qx kernels");
             float acc[NV];
-            double tot[NV];
+            double tot[NB];
+            const double* qxs = red + LEAN_WARPS * NV + NB;   // the block's Q'x sums after the last sweep
             auto sweep = [&]() {
 #pragma unroll
                 for (int u = 0; u < NV; ++u) acc[u] = 0.f;
@@ -258,6 +274,30 @@ k_snp_lean(LeanArgs A) {
                     for (int c = 0; c < NC; ++c) {
                         v[c] = c < ncol ? x4[(size_t)c * nS4 + k4] : make_float4(0.f, 0.f, 0.f, 0.f);
                         acc[c] += (v[c].x + v[c].y) + (v[c].z + v[c].w);
+                    }
+                    if constexpr (QX) {
+                        // rows 4 k4 .. 4 k4 + 3 of Q (LP = 4 or 8 floats a row; none past n)
+#pragma unroll
+                        for (int u = 0; u < 4; ++u) {
+                            const int k = 4 * k4 + u;
+                            if (k < n) {
+                                float q[LEAN_QX_L];
+                                const float4 qa = __ldg(reinterpret_cast<const float4*>(A.Qr + (size_t)k * A.LP));
+                                const float4 qb = A.LP > 4
+                                                      ? __ldg(reinterpret_cast<const float4*>(A.Qr + (size_t)k * A.LP + 4))
+                                                      : make_float4(0.f, 0.f, 0.f, 0.f);
+                                q[0] = qa.x, q[1] = qa.y, q[2] = qa.z, q[3] = qa.w;
+                                q[4] = qb.x, q[5] = qb.y, q[6] = qb.z, q[7] = qb.w;
+#pragma unroll
+                                for (int c = 0; c < NC; ++c) {
+                                    const float xv = u == 0 ? v[c].x : (u == 1 ? v[c].y : (u == 2 ? v[c].z : v[c].w));
+#pragma unroll
+                                    for (int qq = 0; qq < LEAN_QX_L; ++qq)
+                                        acc[NC + K2 + c * LEAN_QX_L + qq] =
+                                            fmaf(q[qq], xv, acc[NC + K2 + c * LEAN_QX_L + qq]);
+                                }
+                            }
+                        }
                     }
 #pragma unroll
                     for (int s2 = 0; s2 < SPB; ++s2)
@@ -273,7 +313,7 @@ k_snp_lean(LeanArgs A) {
                                 d = fmaf(xa.w, xb.w, d);
                             }
                 }
-                block_sum_fd<NV>(acc, tot, red);
+                block_sum_fd<NV, NB>(acc, tot, red);
             };
             sweep();
             bool any_nan = false;
@@ -316,6 +356,17 @@ k_snp_lean(LeanArgs A) {
             }
 #pragma unroll
             for (int c = 0; c < NC; ++c) sh[c] = A.center ? cmean[c] : 0.f;
+            if constexpr (QX) {
+                // A = Q'(x - shift) = Q'x - shift * (column sums of Q), in FP64; thread u writes entry u
+                // (compile-time register indices)
+#pragma unroll
+                for (int c = 0; c < NC; ++c)
+                    if ((int)threadIdx.x / LEAN_QX_L == c && c < ncol) {
+                        const int qq = threadIdx.x % LEAN_QX_L;
+                        A.Afull[(size_t)(i0 * R + c) * LEAN_QX_L + qq] =
+                            qq < A.l ? qxs[c * LEAN_QX_L + qq] - (double)sh[c] * A.qsum[qq] : 0.0;
+                    }
+            }
             if (threadIdx.x == 0) {
 #pragma unroll
                 for (int c = 0; c < NC; ++c) {
@@ -524,6 +575,9 @@ struct SchurArgs {
     // the reference's r >= 2 downdate (quirk mode, raw uncentred columns), or null:
     float* qdel;             // [G][mb][l][r] the quirk's change of Q_obs'X
     double* qK;              // [G][mb][r][r] Gram matrix term of the quirk's RSS
+    // all-rows projection A of each SNP column from k_snp_lean ([mb*r][LEAN_QX_L]), or null: A from
+    // the pre-GEMM's first l columns
+    const double* Afull_lean;
 };
 
 // The system of (pattern g, SNP i) as the reference's r >= 2 downdate builds
@@ -616,9 +670,15 @@ template <int R>
 __device__ __forceinline__ void schur_item(const SchurArgs& S, int i, int slot) {
     const int l = S.l;
     double a_full[OA_MAX_L * R];
-    for (int qq = 0; qq < l; ++qq)
+    if (S.Afull_lean) {
+        for (int qq = 0; qq < l; ++qq)
 #pragma unroll
-        for (int a = 0; a < R; ++a) a_full[qq * R + a] = (double)S.C2[(size_t)qq * S.ldc + i * R + a];
+            for (int a = 0; a < R; ++a) a_full[qq * R + a] = S.Afull_lean[((size_t)i * R + a) * LEAN_QX_L + qq];
+    } else {
+        for (int qq = 0; qq < l; ++qq)
+#pragma unroll
+            for (int a = 0; a < R; ++a) a_full[qq * R + a] = (double)S.C2[(size_t)qq * S.ldc + i * R + a];
+    }
     double Dm[R * R];
 #pragma unroll
     for (int u = 0; u < R * R; ++u) Dm[u] = (double)S.D[(size_t)i * R * R + u];

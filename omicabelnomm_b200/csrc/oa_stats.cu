@@ -54,7 +54,7 @@ cudaError_t oa_launch_snp_stats(int R, int LP, const StatsArgs& A, int grid, siz
     }
 }
 
-template <int R, int SPB>
+template <int R, int SPB, bool QX>
 static cudaError_t go_lean(const LeanArgs& A, int grid, size_t smem, cudaStream_t st) {
     const bool bulk = !A.xrows && (A.n % 4 == 0) && (A.ldx % 4 == 0) &&
                       ((reinterpret_cast<uintptr_t>(A.X) & 15) == 0);
@@ -64,57 +64,71 @@ static cudaError_t go_lean(const LeanArgs& A, int grid, size_t smem, cudaStream_
     const int d = dev & 63;
     int* done = bulk ? set_bulk : set_plain;
     if (done[d] < (int)smem) {
-        cudaError_t e = bulk ? cudaFuncSetAttribute(k_snp_lean<R, SPB, true>,
+        cudaError_t e = bulk ? cudaFuncSetAttribute(k_snp_lean<R, SPB, true, QX>,
                                                     cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024 - 1024)
-                             : cudaFuncSetAttribute(k_snp_lean<R, SPB, false>,
+                             : cudaFuncSetAttribute(k_snp_lean<R, SPB, false, QX>,
                                                     cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024 - 1024);
         if (e != cudaSuccess) return e;
         done[d] = 227 * 1024 - 1024;
     }
     if (bulk)
-        k_snp_lean<R, SPB, true><<<grid, LEAN_THREADS, smem, st>>>(A);
+        k_snp_lean<R, SPB, true, QX><<<grid, LEAN_THREADS, smem, st>>>(A);
     else
-        k_snp_lean<R, SPB, false><<<grid, LEAN_THREADS, smem, st>>>(A);
+        k_snp_lean<R, SPB, false, QX><<<grid, LEAN_THREADS, smem, st>>>(A);
     return cudaGetLastError();
 }
 
-template <int R, int SPB>
+template <int R, int SPB, bool QX>
 static int lean_occ(size_t smem) {
     int nb = 0;
-    if (cudaFuncSetAttribute(k_snp_lean<R, SPB, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024 - 1024) !=
-            cudaSuccess ||
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_snp_lean<R, SPB, true>, LEAN_THREADS, smem) != cudaSuccess) {
+    if (cudaFuncSetAttribute(k_snp_lean<R, SPB, true, QX>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             227 * 1024 - 1024) != cudaSuccess ||
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_snp_lean<R, SPB, true, QX>, LEAN_THREADS, smem) !=
+            cudaSuccess) {
         cudaGetLastError();
         return 0;
     }
     return nb;
 }
 
-int oa_lean_ctas_per_sm(int R, int spb, size_t smem) {
-    // cached per (device, R, spb, smem): no runtime calls while a stream is captured
-    static std::map<std::tuple<int, int, int, size_t>, int> cache;
+// The qx kernels (all-rows covariate projection summed in the kernel) exist for groups of at most
+// LEAN_QX_NC columns with two or more columns per SNP.
+bool oa_lean_has_qx(int R, int spb) { return R >= 2 && R * spb <= LEAN_QX_NC; }
+
+int oa_lean_ctas_per_sm(int R, int spb, size_t smem, bool qx) {
+    // cached per (device, R, spb, qx, smem): no runtime calls while a stream is captured
+    static std::map<std::tuple<int, int, int, bool, size_t>, int> cache;
     static std::mutex mu;
     int dev = 0;
     cudaGetDevice(&dev);
-    const auto key = std::make_tuple(dev, R, spb, smem);
+    const auto key = std::make_tuple(dev, R, spb, qx, smem);
     {
         std::lock_guard<std::mutex> g(mu);
         auto it = cache.find(key);
         if (it != cache.end()) return it->second;
     }
     int v = 0;
-    switch (R * 100 + spb) {
-        case 101: v = lean_occ<1, 1>(smem); break;
-        case 102: v = lean_occ<1, 2>(smem); break;
-        case 104: v = lean_occ<1, 4>(smem); break;
-        case 108: v = lean_occ<1, 8>(smem); break;
-        case 201: v = lean_occ<2, 1>(smem); break;
-        case 202: v = lean_occ<2, 2>(smem); break;
-        case 204: v = lean_occ<2, 4>(smem); break;
-        case 401: v = lean_occ<4, 1>(smem); break;
-        case 402: v = lean_occ<4, 2>(smem); break;
-        case 801: v = lean_occ<8, 1>(smem); break;
-        default: v = 0;
+    if (qx) {
+        switch (R * 100 + spb) {
+            case 201: v = lean_occ<2, 1, true>(smem); break;
+            case 202: v = lean_occ<2, 2, true>(smem); break;
+            case 401: v = lean_occ<4, 1, true>(smem); break;
+            default: v = 0;
+        }
+    } else {
+        switch (R * 100 + spb) {
+            case 101: v = lean_occ<1, 1, false>(smem); break;
+            case 102: v = lean_occ<1, 2, false>(smem); break;
+            case 104: v = lean_occ<1, 4, false>(smem); break;
+            case 108: v = lean_occ<1, 8, false>(smem); break;
+            case 201: v = lean_occ<2, 1, false>(smem); break;
+            case 202: v = lean_occ<2, 2, false>(smem); break;
+            case 204: v = lean_occ<2, 4, false>(smem); break;
+            case 401: v = lean_occ<4, 1, false>(smem); break;
+            case 402: v = lean_occ<4, 2, false>(smem); break;
+            case 801: v = lean_occ<8, 1, false>(smem); break;
+            default: v = 0;
+        }
     }
     std::lock_guard<std::mutex> g(mu);
     cache[key] = v;
@@ -122,17 +136,25 @@ int oa_lean_ctas_per_sm(int R, int spb, size_t smem) {
 }
 
 cudaError_t oa_launch_snp_lean(int R, int spb, const LeanArgs& A, int grid, size_t smem, cudaStream_t st) {
+    if (A.Afull) {
+        switch (R * 100 + spb) {
+            case 201: return go_lean<2, 1, true>(A, grid, smem, st);
+            case 202: return go_lean<2, 2, true>(A, grid, smem, st);
+            case 401: return go_lean<4, 1, true>(A, grid, smem, st);
+            default: return cudaErrorInvalidValue;
+        }
+    }
     switch (R * 100 + spb) {
-        case 101: return go_lean<1, 1>(A, grid, smem, st);
-        case 102: return go_lean<1, 2>(A, grid, smem, st);
-        case 104: return go_lean<1, 4>(A, grid, smem, st);
-        case 108: return go_lean<1, 8>(A, grid, smem, st);
-        case 201: return go_lean<2, 1>(A, grid, smem, st);
-        case 202: return go_lean<2, 2>(A, grid, smem, st);
-        case 204: return go_lean<2, 4>(A, grid, smem, st);
-        case 401: return go_lean<4, 1>(A, grid, smem, st);
-        case 402: return go_lean<4, 2>(A, grid, smem, st);
-        case 801: return go_lean<8, 1>(A, grid, smem, st);
+        case 101: return go_lean<1, 1, false>(A, grid, smem, st);
+        case 102: return go_lean<1, 2, false>(A, grid, smem, st);
+        case 104: return go_lean<1, 4, false>(A, grid, smem, st);
+        case 108: return go_lean<1, 8, false>(A, grid, smem, st);
+        case 201: return go_lean<2, 1, false>(A, grid, smem, st);
+        case 202: return go_lean<2, 2, false>(A, grid, smem, st);
+        case 204: return go_lean<2, 4, false>(A, grid, smem, st);
+        case 401: return go_lean<4, 1, false>(A, grid, smem, st);
+        case 402: return go_lean<4, 2, false>(A, grid, smem, st);
+        case 801: return go_lean<8, 1, false>(A, grid, smem, st);
         default: return cudaErrorInvalidValue;
     }
 }
