@@ -291,7 +291,8 @@ struct oa_engine {
     // covariates
     DBuf<double> Q64, Rinv;
     DBuf<float> Qr;
-    DBuf<double> qsum;   // [LP] column sums of Qr
+    DBuf<float> Qb;      // [n_pad / 4][l][4] the basis by blocks of four rows (k_snp_lean's projection)
+    DBuf<double> qsum;   // [l] column sums of the FP32 basis
     DBuf<double> Afull_lean;   // [chunk*r][LEAN_QX_L] all-rows projection from k_snp_lean
     bool have_cov = false;
     bool center = false;   // the first covariate is constant: SNP columns are taken relative to their means
@@ -424,7 +425,7 @@ int live_engines(int device, int delta) {
 // Every device buffer of an engine (release, footprint).
 template <class F>
 void for_each_buf(oa_engine* e, F&& f) {
-    f(e->Q64); f(e->Rinv); f(e->Qr); f(e->qsum); f(e->Afull_lean);
+    f(e->Q64); f(e->Rinv); f(e->Qr); f(e->Qb); f(e->qsum); f(e->Afull_lean);
     f(e->Yraw); f(e->Yt); f(e->Yhi); f(e->Ylo);
     f(e->tsums); f(e->rss0); f(e->b0); f(e->W); f(e->zQ);
     f(e->tcounts); f(e->pat); f(e->zset); f(e->nobs); f(e->set_off); f(e->set_rows); f(e->set_rep);
@@ -1037,8 +1038,7 @@ oa_status stats_pre(oa_engine* e, const float* X, size_t ldx, const int* xrows, 
     const bool qx = want_lean_qx(e) && oa_lean_has_qx(R, spb);
     if (qx) {
         OA_CHECK(e->Afull_lean.ensure((size_t)e->chunk * R * LEAN_QX_L));
-        A.Qr = e->Qr.p;
-        A.LP = e->LP;
+        A.Qb = reinterpret_cast<const float4*>(e->Qb.p);
         A.l = e->l;
         A.qsum = e->qsum.p;
         A.Afull = e->Afull_lean.p;
@@ -1963,15 +1963,23 @@ oa_status oa_set_covariates(oa_engine* e, const float* xl) {
     std::vector<float> Qr((size_t)n * e->LP, 0.f);
     for (int k = 0; k < n; ++k)
         for (int q = 0; q < l; ++q) Qr[(size_t)k * e->LP + q] = (float)Q[(size_t)q * n + k];
-    std::vector<double> qsum(e->LP, 0.0);   // column sums of the FP32 basis (the lean kernel's projection)
+    // the FP32 basis by blocks of four rows and its column sums (the lean kernel's projection)
+    std::vector<float> Qb((size_t)e->n_pad * l, 0.f);
+    std::vector<double> qsum(l, 0.0);
     for (int k = 0; k < n; ++k)
-        for (int q = 0; q < l; ++q) qsum[q] += (double)Qr[(size_t)k * e->LP + q];
+        for (int q = 0; q < l; ++q) {
+            const float v = Qr[(size_t)k * e->LP + q];
+            Qb[((size_t)(k / 4) * l + q) * 4 + k % 4] = v;
+            qsum[q] += (double)v;
+        }
     OA_CHECK(e->Q64.ensure((size_t)n * l));
     OA_CHECK(e->Qr.ensure(Qr.size()));
+    OA_CHECK(e->Qb.ensure(Qb.size()));
     OA_CHECK(e->qsum.ensure(qsum.size()));
     OA_CHECK(e->Rinv.ensure((size_t)l * l));
     OA_CU(cudaMemcpyAsync(e->Q64.p, Q.data(), sizeof(double) * Q.size(), cudaMemcpyHostToDevice, e->st));
     OA_CU(cudaMemcpyAsync(e->Qr.p, Qr.data(), sizeof(float) * Qr.size(), cudaMemcpyHostToDevice, e->st));
+    OA_CU(cudaMemcpyAsync(e->Qb.p, Qb.data(), sizeof(float) * Qb.size(), cudaMemcpyHostToDevice, e->st));
     OA_CU(cudaMemcpyAsync(e->qsum.p, qsum.data(), sizeof(double) * qsum.size(), cudaMemcpyHostToDevice, e->st));
     OA_CU(cudaMemcpyAsync(e->Rinv.p, Ri.data(), sizeof(double) * Ri.size(), cudaMemcpyHostToDevice, e->st));
     OA_CU(cudaStreamSynchronize(e->st));

@@ -45,9 +45,10 @@ struct LeanArgs {
     // more columns per SNP the all-rows Schur complement D - A'A (var_x) and the pattern systems
     // cancel a large part of D, and the pre-GEMM's long FP32 / BF16-split sums of A are then the
     // largest error of the statistics (the qx kernels, at most LEAN_QX_L covariates)
-    const float* Qr;      // [n][LP] the orthonormal covariate basis (FP32), rows zero past l
-    int LP, l;
-    const double* qsum;   // [LP] column sums of Qr (FP64)
+    const float4* Qb;     // [n_pad / 4][l] the orthonormal covariate basis (FP32) by blocks of four
+                          // rows: Qb[k4 * l + q] = rows 4 k4 .. 4 k4 + 3 of covariate q (0 past n)
+    int l;
+    const double* qsum;   // [l] column sums of the basis (FP64)
     double* Afull;        // [mb*R][LEAN_QX_L]: A of column c, covariate q at Afull[c * LEAN_QX_L + q]
 };
 
@@ -276,25 +277,18 @@ k_snp_lean(LeanArgs A) {
                         acc[c] += (v[c].x + v[c].y) + (v[c].z + v[c].w);
                     }
                     if constexpr (QX) {
-                        // rows 4 k4 .. 4 k4 + 3 of Q (LP = 4 or 8 floats a row; none past n)
+                        // rows 4 k4 .. 4 k4 + 3 of each covariate: one 16-byte load per covariate
 #pragma unroll
-                        for (int u = 0; u < 4; ++u) {
-                            const int k = 4 * k4 + u;
-                            if (k < n) {
-                                float q[LEAN_QX_L];
-                                const float4 qa = __ldg(reinterpret_cast<const float4*>(A.Qr + (size_t)k * A.LP));
-                                const float4 qb = A.LP > 4
-                                                      ? __ldg(reinterpret_cast<const float4*>(A.Qr + (size_t)k * A.LP + 4))
-                                                      : make_float4(0.f, 0.f, 0.f, 0.f);
-                                q[0] = qa.x, q[1] = qa.y, q[2] = qa.z, q[3] = qa.w;
-                                q[4] = qb.x, q[5] = qb.y, q[6] = qb.z, q[7] = qb.w;
+                        for (int qq = 0; qq < LEAN_QX_L; ++qq) {
+                            if (qq < A.l) {
+                                const float4 q4 = __ldg(A.Qb + (size_t)k4 * A.l + qq);
 #pragma unroll
                                 for (int c = 0; c < NC; ++c) {
-                                    const float xv = u == 0 ? v[c].x : (u == 1 ? v[c].y : (u == 2 ? v[c].z : v[c].w));
-#pragma unroll
-                                    for (int qq = 0; qq < LEAN_QX_L; ++qq)
-                                        acc[NC + K2 + c * LEAN_QX_L + qq] =
-                                            fmaf(q[qq], xv, acc[NC + K2 + c * LEAN_QX_L + qq]);
+                                    float& a = acc[NC + K2 + c * LEAN_QX_L + qq];
+                                    a = fmaf(q4.x, v[c].x, a);
+                                    a = fmaf(q4.y, v[c].y, a);
+                                    a = fmaf(q4.z, v[c].z, a);
+                                    a = fmaf(q4.w, v[c].w, a);
                                 }
                             }
                         }
