@@ -197,12 +197,15 @@ struct EpiTest {
     uint32_t mask;
 };
 
-template <int R>
+// FAST: the caller knows that neither the quirk terms nor the dense outputs
+// are set and that no trait of the tile has a zero set (the common case):
+// the same arithmetic without those per-test checks.
+template <int R, bool FAST = false>
 __device__ __forceinline__ bool epi_decide(const EpiArgs& E, int i, int j, const float* z, const TraitP& tp,
                                            const double* S, const float* vx, EpiTest<R>& o) {
     double bx[R];
     double rss;
-    if (E.qK) {
+    if (!FAST && E.qK) {
         rss = quirk_beta_rss<R>(E, i, j, tp, S, z, bx);
     } else {
         double zz = 0.0;
@@ -216,7 +219,7 @@ __device__ __forceinline__ bool epi_decide(const EpiArgs& E, int i, int j, const
         }
         rss = tp.rss0 - zz;
     }
-    if (tp.zs >= 0) rss -= zero_rows_rss<R>(E, i, j, tp, bx);
+    if (!FAST && tp.zs >= 0) rss -= zero_rows_rss<R>(E, i, j, tp, bx);
     const float rssf = (float)rss;
     o.rss = rss;
     o.r2 = 1.f - rssf * tp.a_r2;
@@ -233,7 +236,7 @@ __device__ __forceinline__ bool epi_decide(const EpiArgs& E, int i, int j, const
         if (o.t[a] > E.min_t || E.store_all) mask |= 1u << a;
     }
     o.mask = mask;
-    if (E.d_r2) {
+    if (!FAST && E.d_r2) {
         const size_t off = (size_t)tp.orig * E.dense_ld + E.snp_base + i;
         const float nanf_ = __int_as_float(0x7fc00000);
         const bool pos = rss > 0.0;

@@ -199,19 +199,46 @@ __device__ __forceinline__ bool epi_bar_any(int flag) {
     return r != 0;
 }
 
+// TMEM load of 8 accumulator columns without the wait; tmem_wait8 waits for
+// it and hands the registers on (read-write operands, so that no use of them
+// is scheduled before the wait).
+__device__ __forceinline__ void tmem_ld8_async(uint32_t taddr, uint32_t (&v)[8]) {
+    asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];\n"
+                 : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7])
+                 : "r"(taddr));
+}
+__device__ __forceinline__ void tmem_wait8(uint32_t (&v)[8]) {
+    asm volatile("tcgen05.wait::ld.sync.aligned;"
+                 : "+r"(v[0]), "+r"(v[1]), "+r"(v[2]), "+r"(v[3]), "+r"(v[4]), "+r"(v[5]), "+r"(v[6]), "+r"(v[7])
+                 :
+                 : "memory");
+}
+
 // Statistics epilogue of one accumulator tile for one warp: lane = row
 // (SNP column i of the block, `lead` on its first column), BN traits from
-// TMEM at taddr (32 columns per tcgen05.ld), trait constants from tps.
-template <int R, int BN>
+// TMEM at taddr (8 columns per tcgen05.ld, the next 8 loading while these are
+// evaluated when PREFETCH), trait constants from tps.  FAST: no quirk terms,
+// no dense outputs and no zero sets among the tile's traits (epi_decide).
+template <int R, int BN, bool FAST, bool PREFETCH>
 __device__ __forceinline__ void epi_columns(const EpiArgs& E, uint32_t taddr, int n0, int t, int lane, int i,
                                             bool lead, const float* vx, const TraitP* tps, int cb, int ce,
                                             Emitter& em) {
     int cg = -1;            // pattern whose Schur inverse is cached
     bool csing = true;
     double S[R * R];
+    if (!(cb < ce && n0 + cb < t)) return;
+    uint32_t v[EPI_COLS], vn[EPI_COLS];
+    if constexpr (PREFETCH) {
+        tmem_ld8_async(taddr + (uint32_t)cb, v);
+        tmem_wait8(v);
+    }
     for (int c0 = cb; c0 < ce && n0 + c0 < t; c0 += EPI_COLS) {
-        uint32_t v[EPI_COLS];
-        tmem_ld8(taddr + (uint32_t)c0, v);
+        const bool more = PREFETCH && c0 + EPI_COLS < ce && n0 + c0 + EPI_COLS < t;   // warp-uniform
+        if constexpr (PREFETCH) {
+            if (more) tmem_ld8_async(taddr + (uint32_t)(c0 + EPI_COLS), vn);
+        } else {
+            tmem_ld8(taddr + (uint32_t)c0, v);
+        }
 #pragma unroll
         for (int q = 0; q < EPI_COLS; ++q) {
             const int j = n0 + c0 + q;
@@ -236,12 +263,50 @@ __device__ __forceinline__ void epi_columns(const EpiArgs& E, uint32_t taddr, in
                     atomicAdd(E.n_singular, 1ull);
                     epi_dense_nan<R>(E, i, tp);
                 } else {
-                    st = epi_decide<R>(E, i, j, z, tp, S, vx, o);
+                    st = epi_decide<R, FAST>(E, i, j, z, tp, S, vx, o);
                 }
             }
             epi_emit_lazy<R>(E, st, em, [&](RecOf<R>* dst) { epi_write<R>(E, i, j, tp, o, dst); });
         }
+        if constexpr (PREFETCH) {
+            if (more) {
+                tmem_wait8(vn);
+#pragma unroll
+                for (int q = 0; q < EPI_COLS; ++q) v[q] = vn[q];
+            }
+        }
     }
+}
+
+// The statistics epilogue of one tile for one warp.  With one or two columns
+// per SNP a tile without quirk terms, dense outputs or zero sets takes the
+// FAST evaluation; the split-copy forms also prefetch the next 8 TMEM columns
+// (their register budget has room; the fused forms and r >= 4 do not).
+template <int R, int BN, bool FUSED>
+__device__ __forceinline__ void epi_tile(bool fast, const EpiArgs& E, uint32_t taddr, int n0, int t, int lane,
+                                         int i, bool lead, const float* vx, const TraitP* tps, int cb, int ce,
+                                         Emitter& em) {
+    constexpr bool PF = !FUSED && R <= 2;
+    if constexpr (R <= 2) {
+        if (fast) {
+            epi_columns<R, BN, true, PF>(E, taddr, n0, t, lane, i, lead, vx, tps, cb, ce, em);
+            return;
+        }
+    }
+    epi_columns<R, BN, false, PF>(E, taddr, n0, t, lane, i, lead, vx, tps, cb, ce, em);
+}
+
+// Trait constants of a tile's columns for the statistics epilogue (each
+// epilogue thread loads its share), then one barrier of the epilogue warps
+// that also tells whether any of the tile's traits has a zero set.
+__device__ __forceinline__ bool epi_load_traits(const EpiArgs& E, TraitP* tps, int n0, int t, int et, int bn) {
+    int zs = 0;
+    for (int q = et; q < bn; q += EPI_WARPS * 32)
+        if (n0 + q < t) {
+            tps[q] = load_trait(E, n0 + q);
+            zs |= tps[q].zs >= 0;
+        }
+    return epi_bar_any(zs);
 }
 
 // STORE = false: fused statistics epilogue (t = traits).  STORE = true: the
@@ -442,15 +507,14 @@ k_gemm_tc(const __grid_constant__ CUtensorMap mAhi, const __grid_constant__ CUte
             const int n0 = (raster == 2 ? tile / m_tiles : tile % n_tiles) * BN;
             if (epi_bar_any(abort_sh)) break;   // previous tile's readers are done; one decision for all warps
             // trait constants of this tile (the main loop of the tile is still running)
-            for (int q = et; q < BN; q += EPI_WARPS * 32)
-                if (n0 + q < t) tps[q] = load_trait(E, n0 + q);
+            const bool tile_zs = epi_load_traits(E, tps, n0, t, et, BN);
             const int row = m0 + lg * 32 + lane;   // SNP column of this lane
             const bool lead = ((lane & (R - 1)) == 0) && (row < xrows);
             const int i = row / R;
             float vx[R];
 #pragma unroll
             for (int a = 0; a < R; ++a) vx[a] = lead ? E.varx[(size_t)i * R + a] : 1.f;
-            asm volatile("bar.sync 1, %0;" ::"n"(EPI_WARPS * 32) : "memory");
+            const bool fast = !E.qK && !E.d_r2 && !tile_zs;
             // accumulator ready (the wait is per warp: lane 0 waits, the warp follows)
             int ok = 1;
             if (lane == 0) ok = mbar_wait(&acc_full[acc], aph, &abort_sh) ? 1 : 0;
@@ -458,8 +522,8 @@ k_gemm_tc(const __grid_constant__ CUtensorMap mAhi, const __grid_constant__ CUte
             if (ok) {
                 mbar_try(&acc_full[acc], aph);
                 fence_after();
-                epi_columns<R, BN>(E, tmem_base + ((uint32_t)(lg * 32) << 16) + (uint32_t)(acc * BN), n0, t, lane,
-                                   i, lead, vx, tps, cb, cb + BN / 2, em);
+                epi_tile<R, BN, false>(fast, E, tmem_base + ((uint32_t)(lg * 32) << 16) + (uint32_t)(acc * BN), n0, t,
+                                        lane, i, lead, vx, tps, cb, cb + BN / 2, em);
                 fence_before();
                 mbar_arrive(&acc_empty[acc]);
             }
@@ -710,23 +774,22 @@ k_gemm_tc2(const __grid_constant__ CUtensorMap mAhi, const __grid_constant__ CUt
             tile_mn(tile, m0, n0);
             m0 += (int)rank * BM;
             if (epi_bar_any(abort_sh)) break;
-            for (int q = et; q < BN; q += EPI_WARPS * 32)
-                if (n0 + q < t) tps[q] = load_trait(E, n0 + q);
+            const bool tile_zs = epi_load_traits(E, tps, n0, t, et, BN);
             const int row = m0 + lg * 32 + lane;
             const bool lead = ((lane & (R - 1)) == 0) && (row < xrows);
             const int i = row / R;
             float vx[R];
 #pragma unroll
             for (int a = 0; a < R; ++a) vx[a] = lead ? E.varx[(size_t)i * R + a] : 1.f;
-            asm volatile("bar.sync 1, %0;" ::"n"(EPI_WARPS * 32) : "memory");
+            const bool fast = !E.qK && !E.d_r2 && !tile_zs;
             int ok = 1;
             if (lane == 0) ok = mbar_wait(&acc_full[acc], aph, &abort_sh) ? 1 : 0;
             ok = __shfl_sync(0xffffffffu, ok, 0);
             if (ok) {
                 mbar_try(&acc_full[acc], aph);
                 fence_after();
-                epi_columns<R, BN>(E, tmem_base + ((uint32_t)(lg * 32) << 16) + (uint32_t)(acc * BN), n0, t, lane,
-                                   i, lead, vx, tps, cb, cb + BN / 2, em);
+                epi_tile<R, BN, false>(fast, E, tmem_base + ((uint32_t)(lg * 32) << 16) + (uint32_t)(acc * BN), n0, t,
+                                        lane, i, lead, vx, tps, cb, cb + BN / 2, em);
                 fence_before();
                 __syncwarp();
                 if (lane == 0) mbar_arrive_cluster(map_to_rank(&acc_empty[acc], 0));
@@ -1177,23 +1240,22 @@ k_gemm_tcf(const __grid_constant__ CUtensorMap mAf, const __grid_constant__ CUte
             int m0, n0;
             tile_mn(tile, m0, n0);
             if (epi_bar_any(abort_sh)) break;
-            for (int q = et; q < BN; q += EPI_WARPS * 32)
-                if (n0 + q < t) tps[q] = load_trait(E, n0 + q);
+            const bool tile_zs = epi_load_traits(E, tps, n0, t, et, BN);
             const int row = m0 + lg * 32 + lane;
             const bool lead = ((lane & (R - 1)) == 0) && (row < xrows);
             const int i = row / R;
             float vx[R];
 #pragma unroll
             for (int a = 0; a < R; ++a) vx[a] = lead ? E.varx[(size_t)i * R + a] : 1.f;
-            asm volatile("bar.sync 1, %0;" ::"n"(EPI_WARPS * 32) : "memory");
+            const bool fast = !E.qK && !E.d_r2 && !tile_zs;
             int ok = 1;
             if (lane == 0) ok = mbar_wait(&acc_full[acc], aph, &abort_sh) ? 1 : 0;
             ok = __shfl_sync(0xffffffffu, ok, 0);
             if (ok) {
                 mbar_try(&acc_full[acc], aph);
                 fence_after();
-                epi_columns<R, BN>(E, tmem_base + ((uint32_t)(lg * 32) << 16) + (uint32_t)(acc * BN), n0, t, lane,
-                                   i, lead, vx, tps, cb, cb + BN / 2, em);
+                epi_tile<R, BN, true>(fast, E, tmem_base + ((uint32_t)(lg * 32) << 16) + (uint32_t)(acc * BN), n0, t,
+                                        lane, i, lead, vx, tps, cb, cb + BN / 2, em);
                 fence_before();
                 mbar_arrive(&acc_empty[acc]);
             }
@@ -1403,23 +1465,22 @@ k_gemm_tc2f(const __grid_constant__ CUtensorMap mAf, const __grid_constant__ CUt
             tile_mn(tile, m0, n0);
             m0 += (int)rank * BM;
             if (epi_bar_any(abort_sh)) break;
-            for (int q = et; q < BN; q += EPI_WARPS * 32)
-                if (n0 + q < t) tps[q] = load_trait(E, n0 + q);
+            const bool tile_zs = epi_load_traits(E, tps, n0, t, et, BN);
             const int row = m0 + lg * 32 + lane;
             const bool lead = ((lane & (R - 1)) == 0) && (row < xrows);
             const int i = row / R;
             float vx[R];
 #pragma unroll
             for (int a = 0; a < R; ++a) vx[a] = lead ? E.varx[(size_t)i * R + a] : 1.f;
-            asm volatile("bar.sync 1, %0;" ::"n"(EPI_WARPS * 32) : "memory");
+            const bool fast = !E.qK && !E.d_r2 && !tile_zs;
             int ok = 1;
             if (lane == 0) ok = mbar_wait(&acc_full[acc], aph, &abort_sh) ? 1 : 0;
             ok = __shfl_sync(0xffffffffu, ok, 0);
             if (ok) {
                 mbar_try(&acc_full[acc], aph);
                 fence_after();
-                epi_columns<R, BN>(E, tmem_base + ((uint32_t)(lg * 32) << 16) + (uint32_t)(acc * BN), n0, t, lane,
-                                   i, lead, vx, tps, cb, cb + BN / 2, em);
+                epi_tile<R, BN, true>(fast, E, tmem_base + ((uint32_t)(lg * 32) << 16) + (uint32_t)(acc * BN), n0, t,
+                                        lane, i, lead, vx, tps, cb, cb + BN / 2, em);
                 fence_before();
                 __syncwarp();
                 if (lane == 0) mbar_arrive_cluster(map_to_rank(&acc_empty[acc], 0));
