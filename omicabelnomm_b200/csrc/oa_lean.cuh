@@ -52,7 +52,7 @@ struct LeanArgs {
     double* Afull;        // [mb*R][LEAN_QX_L]: A of column c, covariate q at Afull[c * LEAN_QX_L + q]
 };
 
-constexpr int LEAN_THREADS = 512;
+constexpr int LEAN_THREADS = 256;
 constexpr int LEAN_WARPS = LEAN_THREADS / 32;
 constexpr int LEAN_ITEM_ROWS = 256;     // rows per work item of the set pass
 constexpr int LEAN_STAGE_U = 8;         // elements per thread and step of the element-wise staging
