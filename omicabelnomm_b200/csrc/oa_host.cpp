@@ -8,8 +8,11 @@
 // filters), src/Utility.cpp:244-268 (getTvalue, float16 truncation).
 #include <getopt.h>
 #include <sys/stat.h>
+#include <unistd.h>
 
 #include <algorithm>
+#include <atomic>
+#include <cerrno>
 #include <chrono>
 #include <cmath>
 #include <cstdarg>
@@ -18,7 +21,9 @@
 #include <fstream>
 #include <future>
 #include <sstream>
+#include <memory>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include <cuda_runtime.h>
@@ -130,15 +135,64 @@ bool check_fvd(const std::string& prefix, const Fvi& f) {
     return true;
 }
 
+// ---------------------------------------------------------------------------
+// host threads (output formatting, genotype reading)
+// ---------------------------------------------------------------------------
+// All hardware threads, or OA_HOST_THREADS; at most 64.
+int host_threads() {
+    static const int n = [] {
+        int h = (int)std::thread::hardware_concurrency();
+        if (const char* v = getenv("OA_HOST_THREADS")) h = atoi(v);
+        return std::max(1, std::min(h, 64));
+    }();
+    return n;
+}
+
+// f(part) for part = 0 .. parts-1, part 0 on the calling thread.
+template <class F>
+void parallel_parts(int parts, F&& f) {
+    if (parts <= 1) {
+        f(0);
+        return;
+    }
+    std::vector<std::thread> th;
+    th.reserve((size_t)parts - 1);
+    for (int i = 1; i < parts; ++i) th.emplace_back([&f, i] { f(i); });
+    f(0);
+    for (auto& x : th) x.join();
+}
+
 // count values starting at value index `first` of an .fvd, as float (64-bit
 // file offsets: files beyond 2^31 values, which the reference's int offsets
 // cannot address, src/AIOwrapper.cpp:909-913, 1196).
 bool read_values(FILE* fp, size_t elem_bytes, size_t first, size_t count, float* dst, std::vector<double>& dbl) {
-    if (fseeko(fp, (off_t)(elem_bytes * first), SEEK_SET) != 0) return false;
-    if (elem_bytes == 4) return fread(dst, sizeof(float), count, fp) == count;
-    dbl.resize(count);
-    if (fread(dbl.data(), sizeof(double), count, fp) != count) return false;
-    for (size_t q = 0; q < count; ++q) dst[q] = (float)dbl[q];
+    // large reads in parallel slices (pread on the file descriptor: the page cache copies with
+    // several host threads)
+    const int fd = fileno(fp);
+    if (elem_bytes != 4) dbl.resize(count);
+    char* base = elem_bytes == 4 ? reinterpret_cast<char*>(dst) : reinterpret_cast<char*>(dbl.data());
+    const size_t bytes = elem_bytes * count;
+    const off_t off0 = (off_t)(elem_bytes * first);
+    const int parts = bytes >= ((size_t)64 << 20) ? std::min(host_threads(), 16) : 1;
+    std::atomic<bool> ok{true};
+    parallel_parts(parts, [&](int i) {
+        size_t a = bytes * (size_t)i / parts, b = bytes * (size_t)(i + 1) / parts;
+        while (a < b && ok.load(std::memory_order_relaxed)) {
+            const ssize_t got = pread(fd, base + a, b - a, off0 + (off_t)a);
+            if (got <= 0) {
+                if (got < 0 && errno == EINTR) continue;
+                ok = false;
+                return;
+            }
+            a += (size_t)got;
+        }
+    });
+    if (!ok) return false;
+    if (elem_bytes != 4)
+        parallel_parts(parts, [&](int i) {
+            const size_t a = count * (size_t)i / parts, b = count * (size_t)(i + 1) / parts;
+            for (size_t q = a; q < b; ++q) dst[q] = (float)dbl[q];
+        });
     return true;
 }
 
@@ -272,8 +326,114 @@ uint16_t float16_trunc(float v) {
 }
 
 // ---------------------------------------------------------------------------
+// number formatting of the text output (the same characters as printf)
+// ---------------------------------------------------------------------------
+// Decimal digits of v.
+inline char* put_u64(char* o, uint64_t v) {
+    char d[20];
+    int k = 0;
+    do {
+        d[k++] = (char)('0' + v % 10);
+        v /= 10;
+    } while (v);
+    while (k) *o++ = d[--k];
+    return o;
+}
+
+// printf("%.Nf", (double)f), N <= 7: the float's exact binary value m 2^e scaled by 10^N and rounded
+// to the nearest integer, ties to even, as glibc rounds the exact value; the sign of negative values
+// and of -0 is kept.  NaN, infinities and |f| >= 2^40 go to snprintf.
+inline char* put_fixed(char* o, float f, int N) {
+    static constexpr uint64_t P10[8] = {1, 10, 100, 1000, 10000, 100000, 1000000, 10000000};
+    uint32_t u;
+    memcpy(&u, &f, 4);
+    const uint32_t ex = (u >> 23) & 0xffu, fr = u & 0x7fffffu;
+    if (ex == 0xffu || ex >= 127u + 40u) return o + snprintf(o, 64, "%.*f", N, (double)f);
+    const uint64_t m = ex ? (fr | 0x800000u) : fr;
+    const int e = ex ? (int)ex - 150 : -149;
+    const unsigned __int128 num = (unsigned __int128)m * P10[N];   // < 2^48
+    uint64_t q;
+    if (e >= 0) {
+        q = (uint64_t)(num << e);   // < 2^64 for e <= 16
+    } else if (-e >= 127) {
+        q = 0;
+    } else {
+        const int sh = -e;
+        const unsigned __int128 qq = num >> sh, rem = num - (qq << sh), half = (unsigned __int128)1 << (sh - 1);
+        q = (uint64_t)qq + ((rem > half || (rem == half && (qq & 1))) ? 1u : 0u);
+    }
+    if (u >> 31) *o++ = '-';
+    o = put_u64(o, q / P10[N]);
+    if (N > 0) {
+        uint64_t fp = q % P10[N];
+        *o++ = '.';
+        for (int d = N - 1; d >= 0; --d) {
+            o[d] = (char)('0' + fp % 10);
+            fp /= 10;
+        }
+        o += N;
+    }
+    return o;
+}
+
+// ---------------------------------------------------------------------------
 // output writer (≙ async_io's write loop, src/AIOwrapper.cpp:1440-1558)
 // ---------------------------------------------------------------------------
+// The stored rows of one engine call, owned by the writer, and the order in
+// which the reference writes them: write block k (one trait block x one
+// reference SNP block) is rows order[blk_off[k] .. blk_off[k+1]), in (trait,
+// SNP) order, with its trait base and its first SNP (the AR offset).
+struct RowBatch {
+    int p = 0;
+    std::vector<int32_t> trait, snp, n_used;   // snp: index within the shard
+    std::vector<float> r2, b, se, t;           // b, se, t: [row * p + h]
+    std::vector<uint32_t> mask;
+    std::vector<int64_t> order, blk_off{0};
+    std::vector<int32_t> blk_trait_base, blk_ar_off;
+
+    // Copy of an engine call's rows (engine memory, valid until its next call), split into the
+    // reference's SNP blocks of mb_ref SNPs starting at shard SNP s0.
+    static RowBatch from_call(const oa_rows& rr, int p, int s0, int cnt, int mb_ref, int trait_base) {
+        RowBatch B;
+        const size_t c = (size_t)rr.count;
+        B.p = p;
+        B.trait.resize(c);
+        B.snp.resize(c);
+        B.n_used.resize(c);
+        B.r2.resize(c);
+        B.mask.resize(c);
+        B.b.resize(c * p);
+        B.se.resize(c * p);
+        B.t.resize(c * p);
+        // the copies of a large call on all host threads (the next engine call waits for them)
+        const int parts = (int)std::max<size_t>(1, std::min<size_t>((size_t)host_threads(), c / 65536));
+        parallel_parts(parts, [&](int i) {
+            const size_t a = c * (size_t)i / parts, e = c * (size_t)(i + 1) / parts;
+            std::copy(rr.trait + a, rr.trait + e, B.trait.begin() + a);
+            for (size_t q = a; q < e; ++q) B.snp[q] = rr.snp[q] + s0;
+            std::copy(rr.n_used + a, rr.n_used + e, B.n_used.begin() + a);
+            std::copy(rr.r2 + a, rr.r2 + e, B.r2.begin() + a);
+            std::copy(rr.coef_mask + a, rr.coef_mask + e, B.mask.begin() + a);
+            std::copy(rr.coef_b + a * p, rr.coef_b + e * p, B.b.begin() + a * p);
+            std::copy(rr.coef_se + a * p, rr.coef_se + e * p, B.se.begin() + a * p);
+            std::copy(rr.coef_t + a * p, rr.coef_t + e * p, B.t.begin() + a * p);
+        });
+        // stable counting sort by reference block (rows arrive in (trait, SNP) order)
+        const int nblk = (cnt + mb_ref - 1) / mb_ref;
+        std::vector<int64_t> cntb((size_t)nblk + 1, 0);
+        for (size_t q = 0; q < c; ++q) ++cntb[(size_t)rr.snp[q] / mb_ref + 1];
+        for (int k = 0; k < nblk; ++k) cntb[(size_t)k + 1] += cntb[k];
+        B.blk_off = cntb;
+        B.order.resize(c);
+        for (size_t q = 0; q < c; ++q) B.order[(size_t)cntb[(size_t)rr.snp[q] / mb_ref]++] = (int64_t)q;
+        for (int k = 0; k < nblk; ++k) {
+            B.blk_trait_base.push_back(trait_base);
+            B.blk_ar_off.push_back(s0 + k * mb_ref);
+        }
+        return B;
+    }
+};
+
 struct Writer {
     FILE* dis = nullptr;
     FILE* dbin = nullptr;
@@ -293,81 +453,169 @@ struct Writer {
     const Fvi* fr = nullptr;
     uint64_t total_sig = 0;
     int64_t rows_written = 0;
-    std::string buf;
+    std::future<void> pending;   // the batch being formatted and written
 
-    // One reference write block: rows of one trait block x one reference SNP
-    // block, in (trait, SNP) order; snp indices are global.
-    void write_block(const oa_rows& rr, const std::vector<int64_t>& idx, int trait_base, int ar_offset_snps) {
-        if (idx.empty()) return;
-        if (dbin && !store_all) {
-            const int32_t yname = trait_base + rr.trait[idx[0]];
-            const int32_t cnt = (int32_t)idx.size();
-            const int32_t aroff = ar_offset_snps * r;
-            fwrite(&yname, 4, 1, dbin);
-            fwrite(&cnt, 4, 1, dbin);
-            fwrite(&aroff, 4, 1, dbin);
-        }
+    // Output of a contiguous range of a batch's write order: text, binary records, counts.
+    struct Segment {
+        std::string txt, bin;
+        uint64_t sig = 0;
+        int64_t rows = 0;
+    };
+
+    // (pointer, length) of a name of an .fvi name table (NUL-terminated or namelength bytes)
+    static std::pair<const char*, int> name_of(const Fvi* f, size_t var) {
+        const char* s = f->raw((size_t)f->nobs + var);
+        int k = 0;
+        while (k < (int)f->namelength && s[k]) ++k;
+        return {s, k};
+    }
+    template <class T>
+    static void put(std::string& out, T v) {
+        out.append(reinterpret_cast<const char*>(&v), sizeof v);
+    }
+
+    // Rows order[a, b) of the batch, formatted exactly as the reference writes them: the text rows
+    // of the coefficients that pass the display filters, the .dbin block headers, records and
+    // stored coefficients (src/AIOwrapper.cpp:1454-1531).
+    void format_range(const RowBatch& B, int64_t a, int64_t b, Segment& S) const {
         const int start_h = disp_cov ? 1 : l;
-        char line[1024];
-        for (int64_t q : idx) {
-            const int ytr = trait_base + rr.trait[q];
-            const int snp = rr.snp[q];
-            const int ii = snp - ar_offset_snps;
-            const uint32_t mask = rr.coef_mask[q];
-            const int nused_i = rr.n_used[q];
+        const int nl = (int)std::max({fy->namelength, fl->namelength, fr->namelength});
+        std::vector<char> line((size_t)3 * nl + 512), an((size_t)2 * nl + 64);
+        size_t k = (size_t)(std::upper_bound(B.blk_off.begin(), B.blk_off.end(), a) - B.blk_off.begin()) - 1;
+        for (int64_t pos = a; pos < b; ++pos) {
+            while (pos >= B.blk_off[k + 1]) ++k;
+            const int64_t q = B.order[(size_t)pos];
+            if (pos == B.blk_off[k] && dbin && !store_all) {
+                put<int32_t>(S.bin, B.blk_trait_base[k] + B.trait[(size_t)q]);
+                put<int32_t>(S.bin, (int32_t)(B.blk_off[k + 1] - B.blk_off[k]));
+                put<int32_t>(S.bin, B.blk_ar_off[k] * r);
+            }
+            const int ytr = B.blk_trait_base[k] + B.trait[(size_t)q];
+            const int snp = B.snp[(size_t)q];
+            const int ii = snp - B.blk_ar_off[k];
+            const uint32_t mask = B.mask[(size_t)q];
+            const int nused_i = B.n_used[(size_t)q];
             const uint16_t nused = (uint16_t)nused_i;
             const float npct = (float)nused_i / (float)real_n;
-            const float r2 = rr.r2[q];
+            const float r2 = B.r2[(size_t)q];
             if (dbin) {
-                const uint16_t r2h = float16_trunc(r2);
-                fwrite(&nused, 2, 1, dbin);
-                fwrite(&r2h, 2, 1, dbin);
+                put<uint16_t>(S.bin, nused);
+                put<uint16_t>(S.bin, float16_trunc(r2));
                 if (!store_all) {
                     uint8_t sz = 0;
                     for (int h = p - 1; h >= start_h; --h) sz += (mask >> h) & 1u;
-                    fwrite(&sz, 1, 1, dbin);
+                    put<uint8_t>(S.bin, sz);
                 }
             }
             for (int h = p - 1; h >= start_h; --h) {
                 if (!((mask >> h) & 1u)) continue;
-                const float B = rr.coef_b[(size_t)q * p + h];
-                const float SE = rr.coef_se[(size_t)q * p + h];
-                const float T = rr.coef_t[(size_t)q * p + h];
+                const float Bv = B.b[(size_t)q * B.p + h];
+                const float SE = B.se[(size_t)q * B.p + h];
+                const float T = B.t[(size_t)q * B.p + h];
                 const long double P = pvalue_ld(T);
-                if (min_p_disp > P) ++total_sig;
+                if (min_p_disp > P) ++S.sig;
                 const int ar_idx = ii * r + (h >= l ? h - l : 0);
                 const uint8_t al_idx = h >= l ? (uint8_t)255 : (uint8_t)h;
                 if ((P <= min_p_disp && r2 >= min_r2_disp) || store_all) {
-                    std::string aname = " ";
-                    if (h < l) aname = fl->var_name(h) + ":";
+                    // the term's name: " " SNP term name, or AL name ":" SNP term name for a
+                    // covariate term (src/AIOwrapper.cpp:1497-1504)
+                    size_t an_len = 0;
+                    auto add = [&](const char* s, size_t len) {
+                        if (an_len + len + 1 > an.size()) an.resize(an_len + len + 64);
+                        memcpy(an.data() + an_len, s, len);
+                        an_len += len;
+                    };
+                    if (h >= l) {
+                        add(" ", 1);
+                    } else {
+                        const auto al = name_of(fl, (size_t)h);
+                        add(al.first, (size_t)al.second);
+                        add(":", 1);
+                    }
                     const size_t snp_g = (size_t)(name_base + snp);
                     const int term = h >= l ? h - l : 0;
                     if (multi_k > 0) {   // src/AIOwrapper.cpp:618-660
-                        aname += multi_name(snp, term);
-                    } else if (n_inter > 0) {   // src/AIOwrapper.cpp:566-612
-                        if (term < n_inter) aname += "I" + std::to_string(term + 1) + "x";
-                        aname += fr->var_name(snp_g * name_stride);
+                        const std::string mn = multi_name(snp, term);
+                        add(mn.data(), mn.size());
                     } else {
-                        aname += fr->var_name(snp_g * name_stride + (name_first_only ? 0 : (size_t)term));
+                        size_t var = snp_g * name_stride + (name_first_only ? 0 : (size_t)term);
+                        if (n_inter > 0) {   // src/AIOwrapper.cpp:566-612
+                            if (term < n_inter) {
+                                const std::string pre = "I" + std::to_string(term + 1) + "x";
+                                add(pre.data(), pre.size());
+                            }
+                            var = snp_g * name_stride;
+                        }
+                        const auto sn = name_of(fr, var);
+                        add(sn.first, (size_t)sn.second);
                     }
-                    const int len = snprintf(line, sizeof line, "%s\t%s\t%u\t%.2f\t%.7f\t%.4f\t%.7f\t%.7f\t%.7Le\n",
-                                             fy->var_name(ytr).c_str(), aname.c_str(), (unsigned)nused,
-                                             (double)npct, (double)B, (double)r2, (double)SE, (double)T, P);
-                    buf.append(line, (size_t)len);
-                    ++rows_written;
+                    const auto yn = name_of(fy, (size_t)ytr);
+                    const size_t need = (size_t)yn.second + an_len + 512;
+                    if (line.size() < need) line.resize(need);
+                    // "%s\t%s\t%u\t%.2f\t%.7f\t%.4f\t%.7f\t%.7f\t%.7Le\n" (src/AIOwrapper.cpp:1509-1511)
+                    char* o = line.data();
+                    memcpy(o, yn.first, (size_t)yn.second);
+                    o += yn.second;
+                    *o++ = '\t';
+                    memcpy(o, an.data(), an_len);
+                    o += an_len;
+                    *o++ = '\t';
+                    o = put_u64(o, nused);
+                    *o++ = '\t';
+                    o = put_fixed(o, npct, 2);
+                    *o++ = '\t';
+                    o = put_fixed(o, Bv, 7);
+                    *o++ = '\t';
+                    o = put_fixed(o, r2, 4);
+                    *o++ = '\t';
+                    o = put_fixed(o, SE, 7);
+                    *o++ = '\t';
+                    o = put_fixed(o, T, 7);
+                    *o++ = '\t';
+                    o += snprintf(o, 64, "%.7Le\n", P);
+                    S.txt.append(line.data(), (size_t)(o - line.data()));
+                    ++S.rows;
                 }
                 if (dbin) {
-                    if (disp_cov && !store_all) fwrite(&al_idx, 1, 1, dbin);
-                    if (!store_all) {
-                        const uint16_t a16 = (uint16_t)ar_idx;
-                        fwrite(&a16, 2, 1, dbin);
-                    }
-                    fwrite(&B, 4, 1, dbin);
-                    fwrite(&SE, 4, 1, dbin);
+                    if (disp_cov && !store_all) put<uint8_t>(S.bin, al_idx);
+                    if (!store_all) put<uint16_t>(S.bin, (uint16_t)ar_idx);
+                    put<float>(S.bin, Bv);
+                    put<float>(S.bin, SE);
                 }
             }
-            if (buf.size() > (1u << 22)) flush();
         }
+    }
+
+    // Format a batch on all host threads (contiguous ranges of its write order, concatenated in
+    // order: the bytes of a sequential pass) and write it.
+    void write_batch(const RowBatch& B) {
+        const int64_t total = (int64_t)B.order.size();
+        if (total == 0) return;
+        const int parts = (int)std::max<int64_t>(1, std::min<int64_t>(host_threads(), total / 4096));
+        std::vector<Segment> seg((size_t)parts);
+        parallel_parts(parts, [&](int i) {
+            format_range(B, total * i / parts, total * (i + 1) / parts, seg[(size_t)i]);
+        });
+        for (const Segment& s : seg) {
+            if (!s.txt.empty()) fwrite(s.txt.data(), 1, s.txt.size(), dis);
+            if (dbin && !s.bin.empty()) fwrite(s.bin.data(), 1, s.bin.size(), dbin);
+            total_sig += s.sig;
+            rows_written += s.rows;
+        }
+    }
+
+    // Write a batch in the background (after the previous one), so that the next engine call
+    // runs meanwhile.
+    void submit(RowBatch&& B) {
+        finish();
+        auto hold = std::make_shared<RowBatch>(std::move(B));
+        pending = std::async(std::launch::async, [this, hold] {
+            OA_TRACE("write outputs");
+            write_batch(*hold);
+        });
+    }
+    void finish() {
+        if (pending.valid()) pending.get();
     }
     // File SNP (shard-local) and interaction column of a (SNP, column) pair of -w: blocks of
     // multi_fmb file SNPs, each listed once per column (src/AIOwrapper.cpp:441-452, 1208-1241).
@@ -384,9 +632,37 @@ struct Writer {
         return "I" + std::to_string(col + 1) + (term == 0 ? "_" : "_o_") +
                fr->var_name((size_t)(name_base + i) * name_stride);
     }
-    void flush() {
-        if (!buf.empty()) fwrite(buf.data(), 1, buf.size(), dis);
-        buf.clear();
+};
+
+// The two host buffers the SNP blocks are read into, page-locked (the engine copies them with
+// cudaMemcpyAsync), or plain memory when page-locking fails.  Page-locking two buffers of about
+// 1 GB takes most of a second, so it runs on its own thread while the engine is set up.
+struct BlockBuffers {
+    float* p[2] = {nullptr, nullptr};
+    bool locked[2] = {false, false};
+    std::future<void> ready;
+    void start(int device, size_t floats) {
+        ready = std::async(std::launch::async, [this, device, floats] {
+            if (cudaSetDevice(device) != cudaSuccess) cudaGetLastError();
+            for (int b = 0; b < 2; ++b) {
+                locked[b] = cudaMallocHost(&p[b], sizeof(float) * floats) == cudaSuccess;
+                if (!locked[b]) {
+                    cudaGetLastError();
+                    p[b] = static_cast<float*>(malloc(sizeof(float) * floats));
+                }
+            }
+        });
+    }
+    bool wait() {
+        if (ready.valid()) ready.get();
+        return p[0] && p[1];
+    }
+    ~BlockBuffers() {
+        wait();
+        for (int b = 0; b < 2; ++b) {
+            if (locked[b]) cudaFreeHost(p[b]);
+            else free(p[b]);
+        }
     }
 };
 
@@ -440,35 +716,40 @@ oa_status multi_call(oa_engine* eng, const float* xr_pinned, float* xr_dev, int 
         return a.pair < b.pair;
     });
     const size_t cnt_rows = rows.size();
-    std::vector<int32_t> tr(cnt_rows), pr(cnt_rows), nu(cnt_rows);
-    std::vector<float> r2(cnt_rows), B(cnt_rows * p), SE(cnt_rows * p), T(cnt_rows * p);
-    std::vector<uint32_t> mk(cnt_rows);
+    RowBatch g;
+    g.p = p;
+    g.trait.resize(cnt_rows);
+    g.snp.resize(cnt_rows);
+    g.n_used.resize(cnt_rows);
+    g.r2.resize(cnt_rows);
+    g.mask.resize(cnt_rows);
+    g.b.resize(cnt_rows * p);
+    g.se.resize(cnt_rows * p);
+    g.t.resize(cnt_rows * p);
     for (size_t q = 0; q < cnt_rows; ++q) {
         const Row& x = rows[q];
-        tr[q] = x.trait;
-        pr[q] = x.pair;
-        nu[q] = x.n_used;
-        r2[q] = x.r2;
-        mk[q] = x.mask;
-        std::copy(cb.begin() + x.coef, cb.begin() + x.coef + p, B.begin() + q * p);
-        std::copy(cs.begin() + x.coef, cs.begin() + x.coef + p, SE.begin() + q * p);
-        std::copy(ct.begin() + x.coef, ct.begin() + x.coef + p, T.begin() + q * p);
+        g.trait[q] = x.trait;
+        g.snp[q] = x.pair;
+        g.n_used[q] = x.n_used;
+        g.r2[q] = x.r2;
+        g.mask[q] = x.mask;
+        std::copy(cb.begin() + x.coef, cb.begin() + x.coef + p, g.b.begin() + q * p);
+        std::copy(cs.begin() + x.coef, cs.begin() + x.coef + p, g.se.begin() + q * p);
+        std::copy(ct.begin() + x.coef, ct.begin() + x.coef + p, g.t.begin() + q * p);
     }
-    oa_rows g{};
-    g.count = (int64_t)cnt_rows;
-    g.trait = tr.data();
-    g.snp = pr.data();
-    g.r2 = r2.data();
-    g.n_used = nu.data();
-    g.coef_mask = mk.data();
-    g.coef_b = B.data();
-    g.coef_se = SE.data();
-    g.coef_t = T.data();
-    // the call covers whole reference blocks: s0 / fmb .. (s0 + cnt - 1) / fmb
+    // the call covers whole reference blocks s0 / fmb .. (s0 + cnt - 1) / fmb; the sorted rows hold
+    // them one after the other
     const int b_first = s0 / fmb, b_last = (s0 + cnt - 1) / fmb;
-    std::vector<std::vector<int64_t>> blocks(b_last - b_first + 1);
-    for (size_t q = 0; q < cnt_rows; ++q) blocks[pr[q] / mbv - b_first].push_back((int64_t)q);
-    for (int b = b_first; b <= b_last; ++b) W.write_block(g, blocks[b - b_first], trait_base, b * mbv);
+    g.order.resize(cnt_rows);
+    for (size_t q = 0; q < cnt_rows; ++q) g.order[q] = (int64_t)q;
+    g.blk_off.assign((size_t)(b_last - b_first) + 2, 0);
+    for (size_t q = 0; q < cnt_rows; ++q) ++g.blk_off[(size_t)(g.snp[q] / mbv - b_first) + 1];
+    for (int b = b_first; b <= b_last; ++b) {
+        g.blk_off[(size_t)(b - b_first) + 1] += g.blk_off[(size_t)(b - b_first)];
+        g.blk_trait_base.push_back(trait_base);
+        g.blk_ar_off.push_back(b * mbv);
+    }
+    W.submit(std::move(g));
     return OA_OK;
 }
 
@@ -519,6 +800,14 @@ oa_status oa_solve(const oa_settings* S, oa_outputs* out) {
     }
     memset(out, 0, sizeof *out);
     const auto t_start = std::chrono::steady_clock::now();
+    // OA_TIMING: host phase times on stderr at the end of the run
+    double tm_files = 0, tm_create = 0, tm_setup = 0, tm_pin = 0, tm_traits = 0, tm_read = 0, tm_run = 0, tm_submit = 0, tm_finish = 0;
+    auto t_mark = t_start;
+    auto lap = [&t_mark](double& acc) {
+        const auto now = std::chrono::steady_clock::now();
+        acc += std::chrono::duration<double>(now - t_mark).count();
+        t_mark = now;
+    };
     const bool verbose = S->verbose != 0;
     // threshold coupling (src/Algorithm.cpp:338-342)
     float min_r2_store = S->min_r2_store, min_p_store = S->min_p_store;
@@ -805,6 +1094,8 @@ oa_status oa_solve(const oa_settings* S, oa_outputs* out) {
     int call_snps = (int)std::max<int64_t>(1, (int64_t)(1u << 28) / ((int64_t)n * file_r));
     call_snps = std::max(mb_file, call_snps / mb_file * mb_file);
     call_snps = std::min(call_snps, m);
+    BlockBuffers pins;
+    pins.start(S->device, (size_t)call_snps * file_r * n);
     oa_config cfg{};
     cfg.n = n;
     cfg.l = l;
@@ -821,7 +1112,9 @@ oa_status oa_solve(const oa_settings* S, oa_outputs* out) {
     cfg.min_p_disp = S->min_p_disp;
     cfg.real_n = fileN;
     oa_engine* eng = nullptr;
+    lap(tm_files);
     oa_status st = oa_engine_create(&cfg, &eng);
+    lap(tm_create);
     if (st != OA_OK) {
         herr("%s", oa_last_error());
         fclose(W.dis);
@@ -831,7 +1124,7 @@ oa_status oa_solve(const oa_settings* S, oa_outputs* out) {
     auto fail = [&](oa_status s) {
         herr("%s", oa_last_error());
         oa_engine_destroy(eng);
-        W.flush();
+        W.finish();
         fclose(W.dis);
         if (W.dbin) fclose(W.dbin);
         return s;
@@ -881,14 +1174,20 @@ oa_status oa_solve(const oa_settings* S, oa_outputs* out) {
         if (W.dbin) fclose(W.dbin);
         return OA_ERR_IO;
     }
+    lap(tm_setup);
     // pinned double buffers for the SNP blocks (copied with cudaMemcpyAsync by the engine)
-    float* pin[2] = {nullptr, nullptr};
-    const size_t pin_floats = (size_t)call_snps * file_r * n;
-    for (int b = 0; b < 2; ++b)
-        if (cudaMallocHost(&pin[b], sizeof(float) * pin_floats) != cudaSuccess) {
-            cudaGetLastError();
-            pin[b] = (float*)malloc(sizeof(float) * pin_floats);
-        }
+    if (!pins.wait()) {
+        fclose(fr);
+        fclose(fyd);
+        if (xr_dev) cudaFree(xr_dev);
+        herr("host buffers for the SNP blocks: out of memory");
+        oa_engine_destroy(eng);
+        fclose(W.dis);
+        if (W.dbin) fclose(W.dbin);
+        return OA_ERR_NOMEM;
+    }
+    float* pin[2] = {pins.p[0], pins.p[1]};
+    lap(tm_pin);
     std::vector<float> scratch[2];
     std::vector<double> dscratch[2], ydbl;
     std::vector<float> Yblk, yscratch;
@@ -905,6 +1204,7 @@ oa_status oa_solve(const oa_settings* S, oa_outputs* out) {
             break;
         }
         st = oa_set_traits(eng, Yblk.data(), tcur);
+        lap(tm_traits);
         if (st != OA_OK) break;
         auto read_call = [&](int c, int b) {
             OA_TRACE("read SNP block (.fvd)");
@@ -914,7 +1214,9 @@ oa_status oa_solve(const oa_settings* S, oa_outputs* out) {
         };
         std::future<bool> next = std::async(std::launch::async, read_call, 0, 0);
         for (int c = 0; c < ncalls; ++c) {
-            if (!next.get()) {
+            const bool read_ok = next.get();
+            lap(tm_read);
+            if (!read_ok) {
                 herr("Error reading AR File %s.fvd", fxr.c_str());
                 io_ok = false;
                 break;
@@ -936,6 +1238,7 @@ oa_status oa_solve(const oa_settings* S, oa_outputs* out) {
             }
             oa_rows rows{};
             st = oa_run_snps(eng, pin[b], cnt, &rows);
+            lap(tm_run);
             if (st != OA_OK) {
                 if (c + 1 < ncalls) next.wait();
                 break;
@@ -943,16 +1246,10 @@ oa_status oa_solve(const oa_settings* S, oa_outputs* out) {
             tests += rows.tests;
             singular += rows.singular;
             sig_cov += (uint64_t)rows.sig_cov_unrowed;
-            // split into the reference's SNP blocks (rows are in (trait, SNP) order)
-            const int nblk = (cnt + mb_ref - 1) / mb_ref;
-            std::vector<std::vector<int64_t>> blocks(nblk);
-            for (int64_t q = 0; q < rows.count; ++q) blocks[rows.snp[q] / mb_ref].push_back(q);
-            std::vector<int32_t> gsnp(rows.count);
-            for (int64_t q = 0; q < rows.count; ++q) gsnp[q] = rows.snp[q] + s0;
-            oa_rows g = rows;
-            g.snp = gsnp.data();
-            OA_TRACE("write outputs");
-            for (int k = 0; k < nblk; ++k) W.write_block(g, blocks[k], y0, s0 + k * mb_ref);
+            // the rows go to the writer, split into the reference's SNP blocks; it formats and writes
+            // them while the next call runs
+            W.submit(RowBatch::from_call(rows, p, s0, cnt, mb_ref, y0));
+            lap(tm_submit);
             if (verbose) {
                 putchar('*');
                 fflush(stdout);
@@ -962,16 +1259,16 @@ oa_status oa_solve(const oa_settings* S, oa_outputs* out) {
     fclose(fr);
     fclose(fyd);
     if (xr_dev) cudaFree(xr_dev);
-    for (int b = 0; b < 2; ++b) {
-        if (cudaFreeHost(pin[b]) != cudaSuccess) {
-            cudaGetLastError();
-            free(pin[b]);
-        }
-    }
-    W.flush();
+    W.finish();
     fclose(W.dis);
     if (W.dbin) fclose(W.dbin);
     oa_engine_destroy(eng);
+    lap(tm_finish);
+    if (getenv("OA_TIMING"))
+        fprintf(stderr,
+                "[oa timing] input files %.3f s, engine creation %.3f s, covariates and models %.3f s, pinned buffers %.3f s, traits %.3f s, waiting for reads %.3f s, engine "
+                "calls %.3f s, handing rows to the writer %.3f s, last writes and release %.3f s (%d host threads)\n",
+                tm_files, tm_create, tm_setup, tm_pin, tm_traits, tm_read, tm_run, tm_submit, tm_finish, host_threads());
     if (!io_ok) return OA_ERR_IO;
     if (st != OA_OK) {
         if (h_err.empty()) herr("%s", oa_last_error());
