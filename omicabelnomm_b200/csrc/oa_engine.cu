@@ -321,6 +321,7 @@ struct oa_engine {
     // statistics-kernel layout requests (environment; 0 / -1 = the plan's choice): column buffers (1, 2)
     // and the row-interleaved column copy of the set pass (0, 1)
     int lean_nbuf = 0, lean_xi = -1;
+    int lean_threads_req = 0;   // 256 or 512 threads per column-statistics CTA (OA_LEAN_THREADS), 0: by n
     // work items of the lean kernel's set pass (per trait block) and its launch plan
     DBuf<int> item_start, set_item_off, pass_off;
     std::vector<int> h_set_item_off;
@@ -943,6 +944,16 @@ int lean_group(const oa_engine* e) {
     return s;
 }
 
+// Threads per k_snp_lean CTA, from the column length alone (so that every tuning sums in the same
+// order and gives the same bits): 512 where one SNP's columns take 64 KB or more of shared memory
+// (at most three CTAs fit on an SM; n >= 16,384 with one column per SNP), else 256 (more, smaller
+// CTAs per SM with cheaper block barriers); 256 with eight columns per SNP (registers).
+int lean_threads(const oa_engine* e) {
+    const int most = lean_max_threads(e->r);
+    if (e->lean_threads_req) return std::min(e->lean_threads_req, most);
+    return (size_t)e->r * e->n_pad * 4 >= (size_t)64 * 1024 ? most : 256;
+}
+
 // Launch plan of k_snp_lean for the current trait block and tuning: SNPs per
 // group, column buffers, shared memory, and passes over the row sets whose
 // work items fit in shared memory.  Host-only (runs before any capture).
@@ -1044,9 +1055,10 @@ oa_status stats_pre(oa_engine* e, const float* X, size_t ldx, const int* xrows, 
         A.Afull = e->Afull_lean.p;
     }
     const int groups = (mbc + spb - 1) / spb;
-    const int per_sm = std::max(1, oa_lean_ctas_per_sm(R, spb, smem, qx));
+    const int threads = lean_threads(e);
+    const int per_sm = std::max(1, oa_lean_ctas_per_sm(R, spb, smem, qx, threads));
     const int grid = std::min(groups, e->sm_count * per_sm);
-    OA_CU(oa_launch_snp_lean(R, spb, A, grid, smem, e->st));
+    OA_CU(oa_launch_snp_lean(R, spb, A, grid, threads, smem, e->st));
     ++e->launches;
     const int ldc = e->chunk * R;
     if (fused)
@@ -1829,6 +1841,7 @@ oa_status oa_engine_create(const oa_config* cfg, oa_engine** out) {
     if (const char* v = getenv("OA_LEAN_SPB")) e->req.lean_spb = std::max(0, atoi(v));
     if (const char* v = getenv("OA_LEAN_NBUF")) e->lean_nbuf = atoi(v) == 1 ? 1 : (atoi(v) == 2 ? 2 : 0);
     if (const char* v = getenv("OA_LEAN_XI")) e->lean_xi = atoi(v) == 0 ? 0 : (atoi(v) == 1 ? 1 : -1);
+    if (const char* v = getenv("OA_LEAN_THREADS")) e->lean_threads_req = atoi(v) == 512 ? 512 : (atoi(v) == 256 ? 256 : 0);
     e->chunk = std::min(cfg->max_snps, e->req.chunk_snps > 0 ? e->req.chunk_snps : 16384 / e->r);
     if (const char* v = getenv("OA_FUSED_SPLIT")) e->fuse_split = v[0] != '0';
     if (const char* v = getenv("OA_TEST_HASH_BITS")) e->hash_bits = std::min(64, std::max(0, atoi(v)));

@@ -8,10 +8,11 @@ struct StatsArgs;
 struct LeanArgs;
 struct SchurArgs;
 cudaError_t oa_launch_snp_stats(int R, int LP, const StatsArgs& A, int grid, size_t smem, cudaStream_t st);
-// spb: SNPs per CTA group, a power of two <= 8 / R
-cudaError_t oa_launch_snp_lean(int R, int spb, const LeanArgs& A, int grid, size_t smem, cudaStream_t st);
-// resident CTAs of k_snp_lean per SM for this shared-memory size (0 on error)
-int oa_lean_ctas_per_sm(int R, int spb, size_t smem, bool qx = false);
+// spb: SNPs per CTA group, a power of two <= 8 / R; threads: 256 or 512 per CTA
+cudaError_t oa_launch_snp_lean(int R, int spb, const LeanArgs& A, int grid, int threads, size_t smem,
+                               cudaStream_t st);
+// resident CTAs of k_snp_lean per SM for this shared-memory size and thread count (0 on error)
+int oa_lean_ctas_per_sm(int R, int spb, size_t smem, bool qx, int threads);
 bool oa_lean_has_qx(int R, int spb);
 cudaError_t oa_launch_schur(int R, const SchurArgs& S, cudaStream_t st);
 // pre-GEMM C[col * ldc + row] = sum_k X[row][k] B[col][k], col < c2 (tensor-core and SIMT forms)

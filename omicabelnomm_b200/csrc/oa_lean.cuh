@@ -52,8 +52,12 @@ struct LeanArgs {
     double* Afull;        // [mb*R][LEAN_QX_L]: A of column c, covariate q at Afull[c * LEAN_QX_L + q]
 };
 
-constexpr int LEAN_THREADS = 256;
-constexpr int LEAN_WARPS = LEAN_THREADS / 32;
+// Threads per CTA: 256, or 512 where a column group fills so much shared memory that few CTAs fit
+// on an SM (the launch chooses; shared scratch is sized for the larger count).  Eight columns per
+// SNP need more than the 128 registers a thread of a 512-thread CTA may hold: 256 only.
+constexpr int LEAN_MAX_THREADS = 512;
+constexpr int LEAN_MAX_WARPS = LEAN_MAX_THREADS / 32;
+__host__ __device__ constexpr int lean_max_threads(int R) { return R >= 8 ? 256 : LEAN_MAX_THREADS; }
 constexpr int LEAN_ITEM_ROWS = 256;     // rows per work item of the set pass
 constexpr int LEAN_STAGE_U = 8;         // elements per thread and step of the element-wise staging
 constexpr int LEAN_QX_L = 8;            // covariates of the in-kernel projection (l <= 8)
@@ -68,12 +72,12 @@ __host__ __device__ inline size_t lean_smem_bytes(int R, int n_pad, int spb, int
     const int NC = spb * R;
     const int NQ = 2 * NC + spb * R * R + (qx ? NC * LEAN_QX_L : 0);
     return (size_t)(nbuf + (NC > 1 && use_xi ? 1 : 0)) * NC * n_pad * 4 + (size_t)items_cap * spb * R * R * 4 +
-           (size_t)(LEAN_WARPS + 1) * NQ * 8 + 64;
+           (size_t)(LEAN_MAX_WARPS + 1) * NQ * 8 + 64;
 }
 
 // Block-wide sum of NV floats per thread: FP32 within a warp, FP64 across
 // warps (warp 0, fixed order); the first NB sums are copied to out[] on every
-// thread, all NV stay at red + LEAN_WARPS * NV until red is reused.
+// thread, all NV stay at red + LEAN_MAX_WARPS * NV until red is reused.
 template <int NV, int NB = NV>
 __device__ __forceinline__ void block_sum_fd(float (&v)[NV], double (&out)[NB], double* red /* [warps + 1][NV] */) {
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
@@ -83,11 +87,12 @@ __device__ __forceinline__ void block_sum_fd(float (&v)[NV], double (&out)[NB], 
 #pragma unroll
         for (int q = 0; q < NV; ++q) red[w * NV + q] = (double)v[q];
     __syncthreads();
-    double* bc = red + LEAN_WARPS * NV;
+    const int nw = (int)(blockDim.x >> 5);
+    double* bc = red + LEAN_MAX_WARPS * NV;
     if (w == 0) {
 #pragma unroll
         for (int q = 0; q < NV; ++q) {
-            const double s = warp_sum(lane < LEAN_WARPS ? red[lane * NV + q] : 0.0);
+            const double s = warp_sum(lane < nw ? red[lane * NV + q] : 0.0);
             if (lane == 0) bc[q] = s;
         }
     }
@@ -135,12 +140,12 @@ __device__ __forceinline__ void split8(const float4 p0, const float4 p1, uint4& 
 //           lands in its own shared-memory slot, and a set's sum adds its
 //           items in order.  No atomics: the sums are bit-reproducible.
 template <int R, int SPB, bool BULK, bool QX = false>
-__global__ void __launch_bounds__(LEAN_THREADS)
+__global__ void __launch_bounds__(lean_max_threads(R))
 k_snp_lean(LeanArgs A) {
     extern __shared__ __align__(128) unsigned char smem_raw[];
     constexpr int NC = SPB * R;                 // columns per group
     constexpr int K2 = SPB * R * R;             // X'X entries per group
-    constexpr int NWARP = LEAN_WARPS;
+    const int NWARP = (int)(blockDim.x >> 5);
     const int n = A.n, nS = A.n_pad;
     const size_t buf_floats = (size_t)NC * nS;
     float* bufs = reinterpret_cast<float*>(smem_raw);                                   // [nbuf][NC][nS]
@@ -148,7 +153,7 @@ k_snp_lean(LeanArgs A) {
     const bool use_xi = NC > 1 && A.use_xi;
     float* part = xi + (use_xi ? (size_t)NC * nS : 0);                                   // [items_cap][K2]
     double* red = reinterpret_cast<double*>(
-        (reinterpret_cast<uintptr_t>(part + (size_t)A.items_cap * K2) + 7) & ~(uintptr_t)7);   // [NWARP + 1][NQ]
+        (reinterpret_cast<uintptr_t>(part + (size_t)A.items_cap * K2) + 7) & ~(uintptr_t)7);   // [LEAN_MAX_WARPS + 1][NQ]
     __shared__ __align__(8) uint64_t mbar[2];
     __shared__ int stop;
     const int ngroups = (A.mb + SPB - 1) / SPB;
@@ -183,18 +188,19 @@ k_snp_lean(LeanArgs A) {
             const uint32_t dst = st_su32(bufs + (size_t)b * buf_floats + (size_t)c * nS);
             // LEAN_STAGE_U elements per thread and step: the row indices of a step
             // are loaded together, so their latencies overlap
-            for (int k0 = threadIdx.x; k0 < n; k0 += LEAN_STAGE_U * LEAN_THREADS) {
+            const int nt = (int)blockDim.x;
+            for (int k0 = threadIdx.x; k0 < n; k0 += LEAN_STAGE_U * nt) {
                 int kk[LEAN_STAGE_U];
 #pragma unroll
                 for (int u = 0; u < LEAN_STAGE_U; ++u) {
-                    const int k = k0 + u * LEAN_THREADS;
+                    const int k = k0 + u * nt;
                     kk[u] = k < n ? (A.xrows ? __ldg(A.xrows + k) : k) : -1;
                 }
 #pragma unroll
                 for (int u = 0; u < LEAN_STAGE_U; ++u)
                     if (kk[u] >= 0)
                         asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(
-                                         dst + 4u * (uint32_t)(k0 + u * LEAN_THREADS)),
+                                         dst + 4u * (uint32_t)(k0 + u * nt)),
                                      "l"(src + kk[u])
                                      : "memory");
             }
@@ -265,7 +271,7 @@ k_snp_lean(LeanArgs A) {
             static_assert(!QX || NC <= LEAN_QX_NC, "columns of the qx kernels");
             float acc[NV];
             double tot[NB];
-            const double* qxs = red + LEAN_WARPS * NV + NB;   // the block's Q'x sums after the last sweep
+            const double* qxs = red + LEAN_MAX_WARPS * NV + NB;   // the block's Q'x sums after the last sweep
             auto sweep = [&]() {
 #pragma unroll
                 for (int u = 0; u < NV; ++u) acc[u] = 0.f;

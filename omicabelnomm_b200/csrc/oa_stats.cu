@@ -55,7 +55,7 @@ cudaError_t oa_launch_snp_stats(int R, int LP, const StatsArgs& A, int grid, siz
 }
 
 template <int R, int SPB, bool QX>
-static cudaError_t go_lean(const LeanArgs& A, int grid, size_t smem, cudaStream_t st) {
+static cudaError_t go_lean(const LeanArgs& A, int grid, int threads, size_t smem, cudaStream_t st) {
     const bool bulk = !A.xrows && (A.n % 4 == 0) && (A.ldx % 4 == 0) &&
                       ((reinterpret_cast<uintptr_t>(A.X) & 15) == 0);
     static int set_bulk[64], set_plain[64];
@@ -72,18 +72,18 @@ static cudaError_t go_lean(const LeanArgs& A, int grid, size_t smem, cudaStream_
         done[d] = 227 * 1024 - 1024;
     }
     if (bulk)
-        k_snp_lean<R, SPB, true, QX><<<grid, LEAN_THREADS, smem, st>>>(A);
+        k_snp_lean<R, SPB, true, QX><<<grid, threads, smem, st>>>(A);
     else
-        k_snp_lean<R, SPB, false, QX><<<grid, LEAN_THREADS, smem, st>>>(A);
+        k_snp_lean<R, SPB, false, QX><<<grid, threads, smem, st>>>(A);
     return cudaGetLastError();
 }
 
 template <int R, int SPB, bool QX>
-static int lean_occ(size_t smem) {
+static int lean_occ(size_t smem, int threads) {
     int nb = 0;
     if (cudaFuncSetAttribute(k_snp_lean<R, SPB, true, QX>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              227 * 1024 - 1024) != cudaSuccess ||
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_snp_lean<R, SPB, true, QX>, LEAN_THREADS, smem) !=
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_snp_lean<R, SPB, true, QX>, threads, smem) !=
             cudaSuccess) {
         cudaGetLastError();
         return 0;
@@ -95,13 +95,13 @@ static int lean_occ(size_t smem) {
 // LEAN_QX_NC columns with two or more columns per SNP.
 bool oa_lean_has_qx(int R, int spb) { return R >= 2 && R * spb <= LEAN_QX_NC; }
 
-int oa_lean_ctas_per_sm(int R, int spb, size_t smem, bool qx) {
-    // cached per (device, R, spb, qx, smem): no runtime calls while a stream is captured
-    static std::map<std::tuple<int, int, int, bool, size_t>, int> cache;
+int oa_lean_ctas_per_sm(int R, int spb, size_t smem, bool qx, int threads) {
+    // cached per (device, R, spb, qx, smem, threads): no runtime calls while a stream is captured
+    static std::map<std::tuple<int, int, int, bool, size_t, int>, int> cache;
     static std::mutex mu;
     int dev = 0;
     cudaGetDevice(&dev);
-    const auto key = std::make_tuple(dev, R, spb, qx, smem);
+    const auto key = std::make_tuple(dev, R, spb, qx, smem, threads);
     {
         std::lock_guard<std::mutex> g(mu);
         auto it = cache.find(key);
@@ -110,23 +110,23 @@ int oa_lean_ctas_per_sm(int R, int spb, size_t smem, bool qx) {
     int v = 0;
     if (qx) {
         switch (R * 100 + spb) {
-            case 201: v = lean_occ<2, 1, true>(smem); break;
-            case 202: v = lean_occ<2, 2, true>(smem); break;
-            case 401: v = lean_occ<4, 1, true>(smem); break;
+            case 201: v = lean_occ<2, 1, true>(smem, threads); break;
+            case 202: v = lean_occ<2, 2, true>(smem, threads); break;
+            case 401: v = lean_occ<4, 1, true>(smem, threads); break;
             default: v = 0;
         }
     } else {
         switch (R * 100 + spb) {
-            case 101: v = lean_occ<1, 1, false>(smem); break;
-            case 102: v = lean_occ<1, 2, false>(smem); break;
-            case 104: v = lean_occ<1, 4, false>(smem); break;
-            case 108: v = lean_occ<1, 8, false>(smem); break;
-            case 201: v = lean_occ<2, 1, false>(smem); break;
-            case 202: v = lean_occ<2, 2, false>(smem); break;
-            case 204: v = lean_occ<2, 4, false>(smem); break;
-            case 401: v = lean_occ<4, 1, false>(smem); break;
-            case 402: v = lean_occ<4, 2, false>(smem); break;
-            case 801: v = lean_occ<8, 1, false>(smem); break;
+            case 101: v = lean_occ<1, 1, false>(smem, threads); break;
+            case 102: v = lean_occ<1, 2, false>(smem, threads); break;
+            case 104: v = lean_occ<1, 4, false>(smem, threads); break;
+            case 108: v = lean_occ<1, 8, false>(smem, threads); break;
+            case 201: v = lean_occ<2, 1, false>(smem, threads); break;
+            case 202: v = lean_occ<2, 2, false>(smem, threads); break;
+            case 204: v = lean_occ<2, 4, false>(smem, threads); break;
+            case 401: v = lean_occ<4, 1, false>(smem, threads); break;
+            case 402: v = lean_occ<4, 2, false>(smem, threads); break;
+            case 801: v = lean_occ<8, 1, false>(smem, threads); break;
             default: v = 0;
         }
     }
@@ -135,26 +135,28 @@ int oa_lean_ctas_per_sm(int R, int spb, size_t smem, bool qx) {
     return v;
 }
 
-cudaError_t oa_launch_snp_lean(int R, int spb, const LeanArgs& A, int grid, size_t smem, cudaStream_t st) {
+cudaError_t oa_launch_snp_lean(int R, int spb, const LeanArgs& A, int grid, int threads, size_t smem,
+                               cudaStream_t st) {
+    if (threads != 256 && threads != lean_max_threads(R)) return cudaErrorInvalidValue;
     if (A.Afull) {
         switch (R * 100 + spb) {
-            case 201: return go_lean<2, 1, true>(A, grid, smem, st);
-            case 202: return go_lean<2, 2, true>(A, grid, smem, st);
-            case 401: return go_lean<4, 1, true>(A, grid, smem, st);
+            case 201: return go_lean<2, 1, true>(A, grid, threads, smem, st);
+            case 202: return go_lean<2, 2, true>(A, grid, threads, smem, st);
+            case 401: return go_lean<4, 1, true>(A, grid, threads, smem, st);
             default: return cudaErrorInvalidValue;
         }
     }
     switch (R * 100 + spb) {
-        case 101: return go_lean<1, 1, false>(A, grid, smem, st);
-        case 102: return go_lean<1, 2, false>(A, grid, smem, st);
-        case 104: return go_lean<1, 4, false>(A, grid, smem, st);
-        case 108: return go_lean<1, 8, false>(A, grid, smem, st);
-        case 201: return go_lean<2, 1, false>(A, grid, smem, st);
-        case 202: return go_lean<2, 2, false>(A, grid, smem, st);
-        case 204: return go_lean<2, 4, false>(A, grid, smem, st);
-        case 401: return go_lean<4, 1, false>(A, grid, smem, st);
-        case 402: return go_lean<4, 2, false>(A, grid, smem, st);
-        case 801: return go_lean<8, 1, false>(A, grid, smem, st);
+        case 101: return go_lean<1, 1, false>(A, grid, threads, smem, st);
+        case 102: return go_lean<1, 2, false>(A, grid, threads, smem, st);
+        case 104: return go_lean<1, 4, false>(A, grid, threads, smem, st);
+        case 108: return go_lean<1, 8, false>(A, grid, threads, smem, st);
+        case 201: return go_lean<2, 1, false>(A, grid, threads, smem, st);
+        case 202: return go_lean<2, 2, false>(A, grid, threads, smem, st);
+        case 204: return go_lean<2, 4, false>(A, grid, threads, smem, st);
+        case 401: return go_lean<4, 1, false>(A, grid, threads, smem, st);
+        case 402: return go_lean<4, 2, false>(A, grid, threads, smem, st);
+        case 801: return go_lean<8, 1, false>(A, grid, threads, smem, st);
         default: return cudaErrorInvalidValue;
     }
 }
