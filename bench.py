@@ -335,9 +335,16 @@ def cli_e2e(xl, xr, y, m_cli: int, precision: str):
         return {"error": "CLI not built"}
     l, n = xl.shape
     t = y.shape[0]
-    need = (m_cli + t + l) * n * 4 * 1.3 + (2 << 30)
-    base = "/dev/shm" if os.path.isdir("/dev/shm") and shutil.disk_usage("/dev/shm").free > need else None
-    if base is None and shutil.disk_usage(tempfile.gettempdir()).free < need:
+
+    def need(mc):   # input files, the text output (about 80 bytes per test of 16) and headroom
+        return (mc + t + l) * n * 4 * 1.3 + mc * t * 5 + (2 << 30)
+
+    def room(path):
+        return os.path.isdir(path) and shutil.disk_usage(path).free
+    while m_cli > 65536 and max(room("/dev/shm") or 0, room(tempfile.gettempdir()) or 0) < need(m_cli):
+        m_cli //= 2
+    base = "/dev/shm" if (room("/dev/shm") or 0) > need(m_cli) else None
+    if base is None and (room(tempfile.gettempdir()) or 0) < need(m_cli):
         return {"error": "no room for the input files"}
     with tempfile.TemporaryDirectory(prefix="oa_cli_", dir=base) as d:
         obs = fvformat.obs_names(n)
@@ -349,14 +356,16 @@ def cli_e2e(xl, xr, y, m_cli: int, precision: str):
                "-o", os.path.join(d, "out"), "--precision", precision]
         subprocess.run(cmd, check=True, stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL)   # page cache
         t0 = time.perf_counter()
-        p = subprocess.run(cmd, check=True, capture_output=True, text=True)
+        p = subprocess.run(cmd, check=True, capture_output=True, text=True, env=dict(os.environ, OA_TIMING="1"))
         wall = time.perf_counter() - t0
         out_bytes = os.path.getsize(os.path.join(d, "out_dis.txt"))
     sig = p.stdout.split("Number of Significant Results:")[1].split()[0] if "Significant" in p.stdout else None
     return {"value": m_cli * t / wall, "unit": "tests/s", "wall_s": wall, "precision": precision,
             "sample": f"first {m_cli} SNPs x {t} traits at n={n}: .fvd files in page cache -> _dis.txt "
                       f"({out_bytes} bytes), reference flags and default thresholds, one process",
-            "significant_results": int(sig) if sig else None, "storage": base or tempfile.gettempdir()}
+            "significant_results": int(sig) if sig else None, "storage": base or tempfile.gettempdir(),
+            "host_phases": next((ln.split("] ", 1)[1] for ln in p.stderr.splitlines() if ln.startswith("[oa timing]")),
+                                None)}
 
 
 def batched_section(args, dev, local, rank, barrier, max_over_ranks):
@@ -478,8 +487,9 @@ def main():
                     help="keep the engines' default tuning (profiling runs: timings under a profiler would steer "
                          "the autotuner elsewhere)")
     ap.add_argument("--batched-m", type=int, default=200000, help="SNPs of the batched workload (0: skip it)")
-    ap.add_argument("--cli-snps", type=int, default=65536,
-                    help="SNPs of the CLI end-to-end run (.fvd in page cache -> _dis.txt; 0: skip it)")
+    ap.add_argument("--cli-snps", type=int, default=-1,
+                    help="SNPs of the CLI end-to-end run (.fvd in page cache -> _dis.txt; 0: skip it; default: "
+                         "the whole workload, or fewer if the files do not fit in RAM-backed or temporary storage)")
     ap.add_argument("--accuracy-snps", type=int, default=512,
                     help="SNPs of the omics-scale sample checked against the FP64 oracle outside the timed "
                          "region (half as many for the batched r = 2 workload; 0: skip)")
@@ -574,7 +584,24 @@ def main():
     y_np = y_host.numpy()
     e2e_s = None
     d2h = 0
+    link_gbs = None
     if args.e2e_steps > 0:
+        # the host link's copy rate from pinned memory (the bound of the end-to-end number): best of
+        # three 2 GiB copies of the genotype buffer, CUDA events
+        nb = min(xr_host.numel(), (2 << 30) // 4)
+        dst = torch.empty(nb, dtype=torch.float32, device=dev)
+        src = xr_host.view(-1)[:nb]
+        best = None
+        for _ in range(3):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            dst.copy_(src, non_blocking=True)
+            e1.record()
+            e1.synchronize()
+            ms = e0.elapsed_time(e1)
+            best = ms if best is None else min(best, ms)
+        link_gbs = nb * 4 / (best * 1e-3) / 1e9
+        del dst, src
         eng.set_traits(y_np)
         eng.run_raw(xr_np)
         barrier()
@@ -586,9 +613,9 @@ def main():
         e2e_s = max_over_ranks((time.perf_counter() - t0) / args.e2e_steps)
     eng.close()
     cli = None
-    if rank == 0 and world == 1 and args.cli_snps > 0:
+    if rank == 0 and world == 1 and args.cli_snps != 0:
         try:
-            cli = cli_e2e(xl_host, xr_np, y_np, min(m, args.cli_snps), head)
+            cli = cli_e2e(xl_host, xr_np, y_np, m if args.cli_snps < 0 else min(m, args.cli_snps), head)
         except (OSError, subprocess.CalledProcessError) as ex:
             cli = {"error": str(ex)}
     h2d = int(xr_np.nbytes + y_np.nbytes)
@@ -674,7 +701,12 @@ def main():
                    "inputs": "genotypes resident in HBM (20 GB per GPU, larger than L2: no flush needed)",
                    "parallelism": f"independent SNP shards x{world}"},
         "e2e": ({"value": tests * world / e2e_s, "unit": "tests/s", "h2d_bytes_per_step": h2d,
-                 "d2h_bytes_per_step": int(d2h / args.e2e_steps)} if e2e_s else None),
+                 "d2h_bytes_per_step": int(d2h / args.e2e_steps),
+                 "h2d_link": {"achieved_gbs": h2d / e2e_s / 1e9, "measured_copy_gbs": link_gbs,
+                              "frac": (h2d / e2e_s / 1e9) / link_gbs if link_gbs else None,
+                              "note": "genotype bytes per step / step time, against a 2 GiB pinned host-to-device "
+                                      "copy timed in the same run (the bound of this number)"}}
+                if e2e_s else None),
         "gpu_launches": int(R["launches"] * args.steps),
         "roofline": {"bound": bound, "achieved": achieved_tflops, "peak": peak, "unit": "TFLOP/s",
                      "frac": (achieved_tflops / peak) if achieved_tflops else None, "traffic": traffic,

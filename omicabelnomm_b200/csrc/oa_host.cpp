@@ -454,6 +454,7 @@ struct Writer {
     uint64_t total_sig = 0;
     int64_t rows_written = 0;
     std::future<void> pending;   // the batch being formatted and written
+    bool write_failed = false;   // an output write failed (disk full, I/O error)
 
     // Output of a contiguous range of a batch's write order: text, binary records, counts.
     struct Segment {
@@ -597,11 +598,34 @@ struct Writer {
             format_range(B, total * i / parts, total * (i + 1) / parts, seg[(size_t)i]);
         });
         for (const Segment& s : seg) {
-            if (!s.txt.empty()) fwrite(s.txt.data(), 1, s.txt.size(), dis);
-            if (dbin && !s.bin.empty()) fwrite(s.bin.data(), 1, s.bin.size(), dbin);
             total_sig += s.sig;
             rows_written += s.rows;
         }
+        put_segments(dis, seg, &Segment::txt);
+        if (dbin) put_segments(dbin, seg, &Segment::bin);
+    }
+
+    // The segments' bytes at the file's current position, in order: written by several threads at
+    // their offsets (pwrite), the file position then moved past them.
+    void put_segments(FILE* f, const std::vector<Segment>& seg, std::string Segment::*part) {
+        std::vector<off_t> off(seg.size() + 1, 0);
+        for (size_t i = 0; i < seg.size(); ++i) off[i + 1] = off[i] + (off_t)(seg[i].*part).size();
+        if (off.back() == 0) return;
+        fflush(f);
+        const off_t base = ftello(f);
+        const int fd = fileno(f);
+        std::atomic<bool> ok{base >= 0};
+        parallel_parts((int)seg.size(), [&](int i) {
+            const std::string& b = seg[(size_t)i].*part;
+            size_t done = 0;
+            while (done < b.size() && ok.load(std::memory_order_relaxed)) {
+                const ssize_t w = pwrite(fd, b.data() + done, b.size() - done, base + off[(size_t)i] + (off_t)done);
+                if (w < 0 && errno == EINTR) continue;
+                if (w <= 0) ok = false;
+                else done += (size_t)w;
+            }
+        });
+        if (!ok || fseeko(f, base + off.back(), SEEK_SET) != 0) write_failed = true;
     }
 
     // Write a batch in the background (after the previous one), so that the next engine call
@@ -1273,6 +1297,10 @@ oa_status oa_solve(const oa_settings* S, oa_outputs* out) {
     if (st != OA_OK) {
         if (h_err.empty()) herr("%s", oa_last_error());
         return st;
+    }
+    if (W.write_failed) {
+        herr("Error writing the output files %s*", fout_eff.c_str());
+        return OA_ERR_IO;
     }
     out->total_sig_results = W.total_sig + sig_cov;
     out->tests = tests;

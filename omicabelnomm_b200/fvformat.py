@@ -12,7 +12,9 @@ Layout (reference: src/AIOwrapper.h:145-175, reader src/AIOwrapper.cpp:2294-2317
   ``numObservations`` values of variable 0, then variable 1, ...  The
   reference never checks ``type`` and always reads float32
   (src/AIOwrapper.cpp:1103-1125); this module does the same on read and
-  writes ``type = 5`` (FLOAT_TYPE, src/AIOwrapper.h:145-152).
+  writes ``type = 5`` (FLOAT_TYPE, src/AIOwrapper.h:145-152).  ``nelements``
+  is a 32-bit field: files of 2^32 values or more store it modulo 2^32
+  (readers size the data from ``numObservations * numVariables``).
 
 Arrays in this package keep the file's variable-major order: a block of
 ``v`` variables over ``n`` observations is a C-contiguous ``(v, n)``
@@ -101,7 +103,7 @@ def write_fv(prefix: str, data: np.ndarray, obs_names: Sequence[str],
     v, n = data.shape
     if len(obs_names) != n or len(var_names) != v:
         raise ValueError("name counts do not match the data shape")
-    hdr = FVI_HEADER.pack(FLOAT_TYPE, v * n, n, v, 4, 32, namelength, 0, 0, 0, 0, 0)
+    hdr = FVI_HEADER.pack(FLOAT_TYPE, (v * n) & 0xFFFFFFFF, n, v, 4, 32, namelength, 0, 0, 0, 0, 0)
     os.makedirs(os.path.dirname(os.path.abspath(prefix)), exist_ok=True)
     with open(prefix + ".fvi", "wb") as f:
         f.write(hdr)
@@ -114,7 +116,7 @@ def write_fvd_chunked(prefix: str, n: int, var_names: Sequence[str],
                       obs_names: Sequence[str], chunks, namelength: int = DEFAULT_NAMELENGTH) -> None:
     """Write a large file from an iterator of (v_chunk, n) float32 blocks."""
     v = len(var_names)
-    hdr = FVI_HEADER.pack(FLOAT_TYPE, v * n, n, v, 4, 32, namelength, 0, 0, 0, 0, 0)
+    hdr = FVI_HEADER.pack(FLOAT_TYPE, (v * n) & 0xFFFFFFFF, n, v, 4, 32, namelength, 0, 0, 0, 0, 0)
     with open(prefix + ".fvi", "wb") as f:
         f.write(hdr)
         f.write(_pack_names(obs_names, namelength))

@@ -6,7 +6,8 @@
 //      reference's row format (src/AIOwrapper.cpp:1497-1511) and its .dbin records
 //      (src/AIOwrapper.cpp:1454-1531) would, with and without covariate terms (-i), all rows (-f)
 //      and interaction names (-v);
-//   3. the bytes do not depend on how many parts the rows are split into.
+//   3. the bytes do not depend on how many parts the rows are split into, and the files the
+//      background writer leaves (parallel positioned writes after a header) hold the same bytes.
 // The engine entry points the host file calls are stubbed: nothing here touches a device.
 #include "../omicabelnomm_b200/csrc/oa_host.cpp"
 
@@ -191,7 +192,10 @@ void writer_checks() {
         W.disp_cov = variant & 1;
         W.store_all = (variant & 2) != 0;
         W.n_inter = variant >= 4 ? 1 : 0;
-        W.dbin = stdout;   // only tested for non-null: nothing is written to it here
+        char tname[] = "/tmp/oa_writer_txt_XXXXXX", bname[] = "/tmp/oa_writer_bin_XXXXXX";
+        const int tfd = mkstemp(tname), bfd = mkstemp(bname);
+        W.dis = fdopen(tfd, "wb");
+        W.dbin = fdopen(bfd, "wb");
         std::string want_txt, want_bin;
         plain_pass(W, rr, s0, cnt, want_txt, want_bin);
         for (int parts : {1, 7}) {
@@ -209,6 +213,30 @@ void writer_checks() {
                        bin == want_bin ? "same" : "differs");
                 ++failures;
             }
+        }
+        // the files as the background writer leaves them, after a header written through the stream
+        fputs("Phe\tSNP\n", W.dis);
+        W.submit(RowBatch(B));
+        W.submit(RowBatch(B));
+        W.finish();
+        fclose(W.dis);
+        fclose(W.dbin);
+        auto slurp = [](const char* path) {
+            std::string out;
+            FILE* f = fopen(path, "rb");
+            char buf[1 << 16];
+            size_t got;
+            while (f && (got = fread(buf, 1, sizeof buf, f)) > 0) out.append(buf, got);
+            if (f) fclose(f);
+            return out;
+        };
+        const std::string ftxt = slurp(tname), fbin = slurp(bname);
+        unlink(tname);
+        unlink(bname);
+        if (W.write_failed || ftxt != "Phe\tSNP\n" + want_txt + want_txt || fbin != want_bin + want_bin) {
+            printf("writer variant %d: files differ from two sequential passes (%zu text bytes)\n", variant,
+                   ftxt.size());
+            ++failures;
         }
     }
 }
