@@ -376,6 +376,65 @@ inline char* put_fixed(char* o, float f, int N) {
     return o;
 }
 
+// printf("%.7Le", v) for a long double v (the P column): the exact value M 2^e (64-bit M) times
+// 10^(7-d), d = floor(log10 v), in 192-bit integer arithmetic, rounded to nearest with ties to even
+// as glibc rounds the exact value.  1e-30 <= v < 1 takes this path (10^(7-d) < 2^127, e <= -64);
+// anything else (0, NaN, infinities, negative, smaller or larger values) goes to snprintf.
+inline char* put_sci7(char* o, long double v) {
+    using u128 = unsigned __int128;
+    if (!(v >= 1e-30L && v < 1.0L)) return o + snprintf(o, 64, "%.7Le", v);
+    int ex = 0;
+    const long double fr = frexpl(v, &ex);        // v = fr 2^ex, fr in [0.5, 1)
+    const uint64_t M = (uint64_t)ldexpl(fr, 64);   // the 64 mantissa bits, exactly
+    const int sh = 64 - ex;                        // v = M 2^-sh, sh in [65, 164]
+    static const std::vector<u128> P10 = [] {
+        std::vector<u128> t(39, 1);
+        for (size_t i = 1; i < t.size(); ++i) t[i] = t[i - 1] * 10;
+        return t;
+    }();
+    // 2^(ex-1) <= v < 2^ex: d is floor(ex log10 2) or one less (the loop steps down once if needed)
+    int d = (int)std::floor(ex * 0.30102999566398119521);
+    for (int attempt = 0; attempt < 3; ++attempt) {
+        const int k = 7 - d;
+        if (k < 0 || k > 38) break;
+        const u128 p = P10[(size_t)k];
+        // N = M 10^k = n2 2^128 + lo
+        const u128 a = (u128)M * (uint64_t)p, b = (u128)M * (uint64_t)(p >> 64);
+        const u128 mid = (a >> 64) + (uint64_t)b;
+        const u128 lo = (mid << 64) | (uint64_t)a;
+        const uint64_t n2 = (uint64_t)((b >> 64) + (mid >> 64));
+        // q = floor(N 2^-sh), the half bit and the bits below it
+        const u128 q0 = sh >= 128 ? (u128)(n2 >> (sh - 128)) : (((u128)n2 << (128 - sh)) | (lo >> sh));
+        const int hb = sh - 1;
+        const bool half = hb < 128 ? ((lo >> hb) & 1) != 0 : ((n2 >> (hb - 128)) & 1) != 0;
+        const bool sticky = hb <= 128 ? (hb == 128 ? lo != 0 : (lo & (((u128)1 << hb) - 1)) != 0)
+                                      : (lo != 0 || (n2 & ((1ull << (hb - 128)) - 1)) != 0);
+        const u128 q = q0 + ((half && (sticky || (q0 & 1))) ? 1 : 0);
+        if (q < 10000000u) {
+            --d;
+            continue;
+        }
+        if (q >= 100000000u) {
+            ++d;
+            continue;
+        }
+        uint64_t rest = (uint64_t)q % 10000000u;
+        *o++ = (char)('0' + (uint64_t)q / 10000000u);
+        *o++ = '.';
+        for (int i = 6; i >= 0; --i) {
+            o[i] = (char)('0' + rest % 10);
+            rest /= 10;
+        }
+        o += 7;
+        *o++ = 'e';
+        *o++ = d < 0 ? '-' : '+';
+        const int ad = d < 0 ? -d : d;
+        if (ad < 10) *o++ = '0';
+        return put_u64(o, (uint64_t)ad);
+    }
+    return o + snprintf(o, 64, "%.7Le", v);
+}
+
 // ---------------------------------------------------------------------------
 // output writer (≙ async_io's write loop, src/AIOwrapper.cpp:1440-1558)
 // ---------------------------------------------------------------------------
@@ -573,7 +632,8 @@ struct Writer {
                     *o++ = '\t';
                     o = put_fixed(o, T, 7);
                     *o++ = '\t';
-                    o += snprintf(o, 64, "%.7Le\n", P);
+                    o = put_sci7(o, P);
+                    *o++ = '\n';
                     S.txt.append(line.data(), (size_t)(o - line.data()));
                     ++S.rows;
                 }

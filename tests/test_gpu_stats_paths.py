@@ -78,3 +78,33 @@ def test_paths_agree_on_stored_rows(monkeypatch):
     np.testing.assert_array_equal(ra.trait, rb.trait)
     np.testing.assert_array_equal(ra.snp, rb.snp)
     np.testing.assert_allclose(got["pre"][1][2], got["gather"][1][2], rtol=1e-4, atol=1e-4)
+
+
+@functools.lru_cache(maxsize=None)
+def _long_columns():
+    # n_pad = 16,448: one SNP column takes 64 KB of shared memory, so the column-statistics kernel
+    # runs 512 threads per CTA by default
+    w = synth.scaled(0, n=16448, m=160, t=12, l=4, miss_mode="patterns", n_patterns=3, miss_hi=0.1, seed=64)
+    ds = synth.generate(w)
+    res, _, _ = oracle_dense(ds, 1)
+    return ds, res
+
+
+@pytest.mark.parametrize("prec", [E.PLAIN, E.MIXED])
+def test_column_statistics_thread_counts_match_oracle(prec, monkeypatch):
+    """Long columns: the 512-thread launch (default at this n) and the 256-thread launch
+    (OA_LEAN_THREADS=256) both match the FP64 oracle, and each other within FP32 rounding."""
+    ds, res = _long_columns()
+    D = res.dense
+    ok = ~D.singular
+    t_ref = D.tstat[:, :, res.l:][ok]
+    got = {}
+    for threads in ("512", "256"):
+        monkeypatch.setenv("OA_LEAN_THREADS", threads)
+        monkeypatch.setenv("OA_STATS_PATH", "pre")
+        _, _, (_, _, tt, _) = engine_run(ds, 1, precision=prec)
+        got[threads] = tt[ok]
+        dt = np.abs(tt[ok] - t_ref)
+        lim = (T_REL * np.abs(t_ref) + T_ABS) if prec == E.PLAIN else np.full_like(t_ref, 1e-3)
+        assert np.all(dt <= lim), f"{threads} threads: max |dt| {dt.max():.3g}"
+    assert np.all(np.abs(got["512"] - got["256"]) <= 1e-4 * np.abs(got["256"]) + 1e-4)

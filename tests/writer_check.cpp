@@ -1,7 +1,8 @@
 // Host-only check of the CLI's output writer (omicabelnomm_b200/csrc/oa_host.cpp), compiled and run
 // by tests/test_writer.py without a GPU:
-//   1. put_fixed / put_u64 give printf's characters ("%.Nf", "%u") on random float bit patterns,
-//      typical magnitudes, exact decimal ties, subnormals, -0, NaN and infinities;
+//   1. put_fixed / put_sci7 / put_u64 give printf's characters ("%.Nf" of floats, "%.7Le" of long
+//      doubles, "%u") on random bit patterns, typical magnitudes, exact decimal ties, subnormals,
+//      -0, NaN and infinities;
 //   2. Writer::format_range formats random stored rows exactly as a plain snprintf pass with the
 //      reference's row format (src/AIOwrapper.cpp:1497-1511) and its .dbin records
 //      (src/AIOwrapper.cpp:1454-1531) would, with and without covariate terms (-i), all rows (-f)
@@ -63,6 +64,40 @@ void number_checks(long random_cases) {
         memcpy(&f, &u, 4);
         check(f, 7);
     }
+    // "%.7Le" of long doubles: random values over the fast path's range with random low mantissa
+    // bits, the P values of t from 0 to 11.2, dyadic values (exact decimal ties at the eighth
+    // digit), powers of ten and their neighbours, and values outside the fast path
+    auto check_sci = [&](long double v) {
+        char* e = put_sci7(a, v);
+        *e = 0;
+        snprintf(b, sizeof b, "%.7Le", v);
+        if (strcmp(a, b)) {
+            if (failures < 10) printf("put_sci7(%.25Lg) = %s, printf gives %s\n", v, a, b);
+            ++failures;
+        }
+    };
+    std::uniform_real_distribution<double> L(-30.5, 0.5);
+    for (long i = 0; i < random_cases; ++i) {
+        int ex;
+        const long double fr = frexpl(powl(10.0L, (long double)L(g)), &ex);
+        uint64_t M = (uint64_t)ldexpl(fr, 64) ^ (g() & 0xffffffffull);
+        M |= 1ull << 63;
+        check_sci(ldexpl((long double)M, ex - 64));
+    }
+    for (int i = 0; i < 400000; ++i) check_sci(pvalue_ld((float)(11.2 * i / 400000.0)));
+    for (int sft = 1; sft <= 40; ++sft)
+        for (long j = 1; j < (1L << std::min(sft, 14)); j += 2) check_sci(ldexpl((long double)j, -sft));
+    for (int d = -31; d <= 1; ++d) {
+        const long double p10 = powl(10.0L, d);
+        long double up = p10, dn = p10;
+        for (int z = 0; z < 3; ++z) {
+            check_sci(up);
+            check_sci(dn);
+            up = nextafterl(up, 2.0L);
+            dn = nextafterl(dn, 0.0L);
+        }
+    }
+    for (long double v : {0.0L, -0.0L, 1.0L, 0.5L, 1e-31L, 1e-300L, 2.0L, -0.25L}) check_sci(v);
     for (uint64_t v : {0ull, 9ull, 10ull, 65535ull, 4294967295ull, 18446744073709551615ull}) {
         char* e = put_u64(a, v);
         *e = 0;
