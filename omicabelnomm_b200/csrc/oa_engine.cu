@@ -931,7 +931,18 @@ oa_status stats_gather(oa_engine* e, const float* X, int mbc) {
 // groups of at most LEAN_QX_NC columns.
 bool want_lean_qx(const oa_engine* e) { return e->ru >= 2 && e->l <= LEAN_QX_L && e->r <= LEAN_QX_NC; }
 
+// Threads per k_snp_lean CTA, from the column length alone (so that every tuning sums in the same
+// order and gives the same bits): 512 with one column per SNP where the column takes 64 KB or more
+// of shared memory (n >= 16,384: at most three CTAs fit on an SM, and the plan then keeps one SNP
+// per group), else 256 (more, smaller CTAs per SM with cheaper block barriers).
+int lean_threads(const oa_engine* e) {
+    const bool long_col = e->r == 1 && (size_t)e->n_pad * 4 >= (size_t)64 * 1024;
+    if (e->lean_threads_req) return long_col ? e->lean_threads_req : 256;
+    return long_col ? LEAN_MAX_THREADS : 256;
+}
+
 int lean_group(const oa_engine* e) {
+    if (lean_threads(e) == LEAN_MAX_THREADS) return 1;   // the 512-thread kernel takes one SNP per group
     const int cap = want_lean_qx(e) ? LEAN_QX_NC / e->r : 8 / e->r;
     if (e->lean_spb > 0) {
         int s = 1;
@@ -942,16 +953,6 @@ int lean_group(const oa_engine* e) {
     while (s * 2 <= cap && lean_smem_bytes(e->r, e->n_pad, s * 2, 2, 0, true, want_lean_qx(e)) <= 100 * 1024)
         s *= 2;
     return s;
-}
-
-// Threads per k_snp_lean CTA, from the column length alone (so that every tuning sums in the same
-// order and gives the same bits): 512 where one SNP's columns take 64 KB or more of shared memory
-// (at most three CTAs fit on an SM; n >= 16,384 with one column per SNP), else 256 (more, smaller
-// CTAs per SM with cheaper block barriers); 256 with eight columns per SNP (registers).
-int lean_threads(const oa_engine* e) {
-    const int most = lean_max_threads(e->r);
-    if (e->lean_threads_req) return std::min(e->lean_threads_req, most);
-    return (size_t)e->r * e->n_pad * 4 >= (size_t)64 * 1024 ? most : 256;
 }
 
 // Launch plan of k_snp_lean for the current trait block and tuning: SNPs per

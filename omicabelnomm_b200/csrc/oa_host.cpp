@@ -719,31 +719,37 @@ struct Writer {
 };
 
 // The two host buffers the SNP blocks are read into, page-locked (the engine copies them with
-// cudaMemcpyAsync), or plain memory when page-locking fails.  Page-locking two buffers of about
-// 1 GB takes most of a second, so it runs on its own thread while the engine is set up.
+// cudaMemcpyAsync), or plain memory when page-locking fails.  Page-locking a buffer of about 1 GB
+// takes most of half a second, so it runs on a background thread: the first buffer while the
+// engine is set up, the second while the first block is read and scanned.
 struct BlockBuffers {
     float* p[2] = {nullptr, nullptr};
     bool locked[2] = {false, false};
-    std::future<void> ready;
-    void start(int device, size_t floats) {
-        ready = std::async(std::launch::async, [this, device, floats] {
-            if (cudaSetDevice(device) != cudaSuccess) cudaGetLastError();
-            for (int b = 0; b < 2; ++b) {
-                locked[b] = cudaMallocHost(&p[b], sizeof(float) * floats) == cudaSuccess;
-                if (!locked[b]) {
-                    cudaGetLastError();
-                    p[b] = static_cast<float*>(malloc(sizeof(float) * floats));
-                }
-            }
-        });
+    std::shared_future<void> ready[2];
+    void alloc(int b, int device, size_t floats) {
+        if (cudaSetDevice(device) != cudaSuccess) cudaGetLastError();
+        locked[b] = cudaMallocHost(&p[b], sizeof(float) * floats) == cudaSuccess;
+        if (!locked[b]) {
+            cudaGetLastError();
+            p[b] = static_cast<float*>(malloc(sizeof(float) * floats));
+        }
     }
-    bool wait() {
-        if (ready.valid()) ready.get();
-        return p[0] && p[1];
+    void start(int device, size_t floats) {
+        ready[0] = std::async(std::launch::async, [this, device, floats] { alloc(0, device, floats); }).share();
+        std::shared_future<void> first = ready[0];
+        ready[1] = std::async(std::launch::async, [this, device, floats, first] {
+                       first.wait();
+                       alloc(1, device, floats);
+                   }).share();
+    }
+    // buffer b, once it exists (null: out of memory)
+    float* get(int b) {
+        if (ready[b].valid()) ready[b].wait();
+        return p[b];
     }
     ~BlockBuffers() {
-        wait();
         for (int b = 0; b < 2; ++b) {
+            get(b);
             if (locked[b]) cudaFreeHost(p[b]);
             else free(p[b]);
         }
@@ -1260,7 +1266,7 @@ oa_status oa_solve(const oa_settings* S, oa_outputs* out) {
     }
     lap(tm_setup);
     // pinned double buffers for the SNP blocks (copied with cudaMemcpyAsync by the engine)
-    if (!pins.wait()) {
+    if (!pins.get(0)) {
         fclose(fr);
         fclose(fyd);
         if (xr_dev) cudaFree(xr_dev);
@@ -1270,7 +1276,7 @@ oa_status oa_solve(const oa_settings* S, oa_outputs* out) {
         if (W.dbin) fclose(W.dbin);
         return OA_ERR_NOMEM;
     }
-    float* pin[2] = {pins.p[0], pins.p[1]};
+    std::atomic<bool> pin_failed{false};
     lap(tm_pin);
     std::vector<float> scratch[2];
     std::vector<double> dscratch[2], ydbl;
@@ -1292,16 +1298,22 @@ oa_status oa_solve(const oa_settings* S, oa_outputs* out) {
         if (st != OA_OK) break;
         auto read_call = [&](int c, int b) {
             OA_TRACE("read SNP block (.fvd)");
+            float* dst = pins.get(b);
+            if (!dst) {
+                pin_failed = true;
+                return false;
+            }
             const int s0 = c * call_snps, cnt = std::min(call_snps, m - s0);
             return read_columns(fr, FR.elem_bytes(), fileN, (size_t)(first + s0) * file_r, (size_t)cnt * file_r, runs,
-                                n, pin[b], scratch[b], dscratch[b]);
+                                n, dst, scratch[b], dscratch[b]);
         };
         std::future<bool> next = std::async(std::launch::async, read_call, 0, 0);
         for (int c = 0; c < ncalls; ++c) {
             const bool read_ok = next.get();
             lap(tm_read);
             if (!read_ok) {
-                herr("Error reading AR File %s.fvd", fxr.c_str());
+                if (pin_failed) herr("host buffers for the SNP blocks: out of memory");
+                else herr("Error reading AR File %s.fvd", fxr.c_str());
                 io_ok = false;
                 break;
             }
@@ -1309,7 +1321,7 @@ oa_status oa_solve(const oa_settings* S, oa_outputs* out) {
             const int s0 = c * call_snps, cnt = std::min(call_snps, m - s0);
             if (c + 1 < ncalls) next = std::async(std::launch::async, read_call, c + 1, b ^ 1);
             if (multi) {
-                st = multi_call(eng, pin[b], xr_dev, cnt, s0, file_r, n, inter_kept, W, y0, tests, singular, sig_cov);
+                st = multi_call(eng, pins.p[b], xr_dev, cnt, s0, file_r, n, inter_kept, W, y0, tests, singular, sig_cov);
                 if (st != OA_OK) {
                     if (c + 1 < ncalls) next.wait();
                     break;
@@ -1321,7 +1333,7 @@ oa_status oa_solve(const oa_settings* S, oa_outputs* out) {
                 continue;
             }
             oa_rows rows{};
-            st = oa_run_snps(eng, pin[b], cnt, &rows);
+            st = oa_run_snps(eng, pins.p[b], cnt, &rows);
             lap(tm_run);
             if (st != OA_OK) {
                 if (c + 1 < ncalls) next.wait();

@@ -8,7 +8,8 @@ struct StatsArgs;
 struct LeanArgs;
 struct SchurArgs;
 cudaError_t oa_launch_snp_stats(int R, int LP, const StatsArgs& A, int grid, size_t smem, cudaStream_t st);
-// spb: SNPs per CTA group, a power of two <= 8 / R; threads: 256 or 512 per CTA
+// spb: SNPs per CTA group, a power of two <= 8 / R; threads: 256 per CTA, or 512 with one column
+// per group (R = 1, spb = 1, no in-kernel covariate projection)
 cudaError_t oa_launch_snp_lean(int R, int spb, const LeanArgs& A, int grid, int threads, size_t smem,
                                cudaStream_t st);
 // resident CTAs of k_snp_lean per SM for this shared-memory size and thread count (0 on error)

@@ -52,12 +52,11 @@ struct LeanArgs {
     double* Afull;        // [mb*R][LEAN_QX_L]: A of column c, covariate q at Afull[c * LEAN_QX_L + q]
 };
 
-// Threads per CTA: 256, or 512 where a column group fills so much shared memory that few CTAs fit
-// on an SM (the launch chooses; shared scratch is sized for the larger count).  Eight columns per
-// SNP need more than the 128 registers a thread of a 512-thread CTA may hold: 256 only.
+// Threads per CTA (the template's NT): 256; one column per group may also run 512 (launched where
+// the column fills so much shared memory that few CTAs fit on an SM).  Shared scratch is sized
+// for 512.
 constexpr int LEAN_MAX_THREADS = 512;
 constexpr int LEAN_MAX_WARPS = LEAN_MAX_THREADS / 32;
-__host__ __device__ constexpr int lean_max_threads(int R) { return R >= 8 ? 256 : LEAN_MAX_THREADS; }
 constexpr int LEAN_ITEM_ROWS = 256;     // rows per work item of the set pass
 constexpr int LEAN_STAGE_U = 8;         // elements per thread and step of the element-wise staging
 constexpr int LEAN_QX_L = 8;            // covariates of the in-kernel projection (l <= 8)
@@ -75,10 +74,10 @@ __host__ __device__ inline size_t lean_smem_bytes(int R, int n_pad, int spb, int
            (size_t)(LEAN_MAX_WARPS + 1) * NQ * 8 + 64;
 }
 
-// Block-wide sum of NV floats per thread: FP32 within a warp, FP64 across
+// Block-wide sum of NV floats per thread over NW warps: FP32 within a warp, FP64 across
 // warps (warp 0, fixed order); the first NB sums are copied to out[] on every
 // thread, all NV stay at red + LEAN_MAX_WARPS * NV until red is reused.
-template <int NV, int NB = NV>
+template <int NW, int NV, int NB = NV>
 __device__ __forceinline__ void block_sum_fd(float (&v)[NV], double (&out)[NB], double* red /* [warps + 1][NV] */) {
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
 #pragma unroll
@@ -87,12 +86,11 @@ __device__ __forceinline__ void block_sum_fd(float (&v)[NV], double (&out)[NB], 
 #pragma unroll
         for (int q = 0; q < NV; ++q) red[w * NV + q] = (double)v[q];
     __syncthreads();
-    const int nw = (int)(blockDim.x >> 5);
     double* bc = red + LEAN_MAX_WARPS * NV;
     if (w == 0) {
 #pragma unroll
         for (int q = 0; q < NV; ++q) {
-            const double s = warp_sum(lane < nw ? red[lane * NV + q] : 0.0);
+            const double s = warp_sum(lane < NW ? red[lane * NV + q] : 0.0);
             if (lane == 0) bc[q] = s;
         }
     }
@@ -139,13 +137,13 @@ __device__ __forceinline__ void split8(const float4 p0, const float4 p1, uint4& 
 //           the interleaved centred columns per row, shuffle reduction)
 //           lands in its own shared-memory slot, and a set's sum adds its
 //           items in order.  No atomics: the sums are bit-reproducible.
-template <int R, int SPB, bool BULK, bool QX = false>
-__global__ void __launch_bounds__(lean_max_threads(R))
+template <int R, int SPB, bool BULK, bool QX = false, int NT = 256>
+__global__ void __launch_bounds__(NT)
 k_snp_lean(LeanArgs A) {
     extern __shared__ __align__(128) unsigned char smem_raw[];
     constexpr int NC = SPB * R;                 // columns per group
     constexpr int K2 = SPB * R * R;             // X'X entries per group
-    const int NWARP = (int)(blockDim.x >> 5);
+    constexpr int NWARP = NT / 32;
     const int n = A.n, nS = A.n_pad;
     const size_t buf_floats = (size_t)NC * nS;
     float* bufs = reinterpret_cast<float*>(smem_raw);                                   // [nbuf][NC][nS]
@@ -188,7 +186,7 @@ k_snp_lean(LeanArgs A) {
             const uint32_t dst = st_su32(bufs + (size_t)b * buf_floats + (size_t)c * nS);
             // LEAN_STAGE_U elements per thread and step: the row indices of a step
             // are loaded together, so their latencies overlap
-            const int nt = (int)blockDim.x;
+            constexpr int nt = NT;
             for (int k0 = threadIdx.x; k0 < n; k0 += LEAN_STAGE_U * nt) {
                 int kk[LEAN_STAGE_U];
 #pragma unroll
@@ -313,7 +311,7 @@ k_snp_lean(LeanArgs A) {
                                 d = fmaf(xa.w, xb.w, d);
                             }
                 }
-                block_sum_fd<NV, NB>(acc, tot, red);
+                block_sum_fd<NWARP, NV, NB>(acc, tot, red);
             };
             sweep();
             bool any_nan = false;
@@ -341,7 +339,7 @@ k_snp_lean(LeanArgs A) {
                         }
                     }
                 }
-                block_sum_fd<2 * NC>(cs, ct, red);
+                block_sum_fd<NWARP, 2 * NC>(cs, ct, red);
 #pragma unroll
                 for (int c = 0; c < NC; ++c) {
                     if (cnan[c]) {
@@ -765,13 +763,16 @@ __device__ __forceinline__ void schur_item(const SchurArgs& S, int i, int slot) 
         for (int u = 0; u < l * R; ++u) S.aobs[gi * l * R + u] = (float)ao[u];
 }
 
+// Items are numbered slot-major (consecutive threads take consecutive SNPs of one slot), so that
+// a warp's loads of the SNP-indexed sums (pre-GEMM columns, D, D_s) and its stores of the
+// inverses are coalesced and the slot's W_g is one broadcast.
 template <int R>
 __global__ void __launch_bounds__(256) k_schur(SchurArgs S) {
     const int slots = 1 + S.G + S.Z;
     const long long total = (long long)S.mb * slots;
     for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < total;
          q += (long long)gridDim.x * blockDim.x)
-        schur_item<R>(S, (int)(q / slots), (int)(q % slots));
+        schur_item<R>(S, (int)(q % S.mb), (int)(q / S.mb));
 }
 
 }  // namespace oa

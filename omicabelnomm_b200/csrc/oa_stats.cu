@@ -54,8 +54,8 @@ cudaError_t oa_launch_snp_stats(int R, int LP, const StatsArgs& A, int grid, siz
     }
 }
 
-template <int R, int SPB, bool QX>
-static cudaError_t go_lean(const LeanArgs& A, int grid, int threads, size_t smem, cudaStream_t st) {
+template <int R, int SPB, bool QX, int NT = 256>
+static cudaError_t go_lean(const LeanArgs& A, int grid, size_t smem, cudaStream_t st) {
     const bool bulk = !A.xrows && (A.n % 4 == 0) && (A.ldx % 4 == 0) &&
                       ((reinterpret_cast<uintptr_t>(A.X) & 15) == 0);
     static int set_bulk[64], set_plain[64];
@@ -64,26 +64,26 @@ static cudaError_t go_lean(const LeanArgs& A, int grid, int threads, size_t smem
     const int d = dev & 63;
     int* done = bulk ? set_bulk : set_plain;
     if (done[d] < (int)smem) {
-        cudaError_t e = bulk ? cudaFuncSetAttribute(k_snp_lean<R, SPB, true, QX>,
+        cudaError_t e = bulk ? cudaFuncSetAttribute(k_snp_lean<R, SPB, true, QX, NT>,
                                                     cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024 - 1024)
-                             : cudaFuncSetAttribute(k_snp_lean<R, SPB, false, QX>,
+                             : cudaFuncSetAttribute(k_snp_lean<R, SPB, false, QX, NT>,
                                                     cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024 - 1024);
         if (e != cudaSuccess) return e;
         done[d] = 227 * 1024 - 1024;
     }
     if (bulk)
-        k_snp_lean<R, SPB, true, QX><<<grid, threads, smem, st>>>(A);
+        k_snp_lean<R, SPB, true, QX, NT><<<grid, NT, smem, st>>>(A);
     else
-        k_snp_lean<R, SPB, false, QX><<<grid, threads, smem, st>>>(A);
+        k_snp_lean<R, SPB, false, QX, NT><<<grid, NT, smem, st>>>(A);
     return cudaGetLastError();
 }
 
-template <int R, int SPB, bool QX>
-static int lean_occ(size_t smem, int threads) {
+template <int R, int SPB, bool QX, int NT = 256>
+static int lean_occ(size_t smem) {
     int nb = 0;
-    if (cudaFuncSetAttribute(k_snp_lean<R, SPB, true, QX>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    if (cudaFuncSetAttribute(k_snp_lean<R, SPB, true, QX, NT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              227 * 1024 - 1024) != cudaSuccess ||
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_snp_lean<R, SPB, true, QX>, threads, smem) !=
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_snp_lean<R, SPB, true, QX, NT>, NT, smem) !=
             cudaSuccess) {
         cudaGetLastError();
         return 0;
@@ -108,25 +108,27 @@ int oa_lean_ctas_per_sm(int R, int spb, size_t smem, bool qx, int threads) {
         if (it != cache.end()) return it->second;
     }
     int v = 0;
-    if (qx) {
+    if (threads == LEAN_MAX_THREADS) {
+        v = (R == 1 && spb == 1 && !qx) ? lean_occ<1, 1, false, LEAN_MAX_THREADS>(smem) : 0;
+    } else if (qx) {
         switch (R * 100 + spb) {
-            case 201: v = lean_occ<2, 1, true>(smem, threads); break;
-            case 202: v = lean_occ<2, 2, true>(smem, threads); break;
-            case 401: v = lean_occ<4, 1, true>(smem, threads); break;
+            case 201: v = lean_occ<2, 1, true>(smem); break;
+            case 202: v = lean_occ<2, 2, true>(smem); break;
+            case 401: v = lean_occ<4, 1, true>(smem); break;
             default: v = 0;
         }
     } else {
         switch (R * 100 + spb) {
-            case 101: v = lean_occ<1, 1, false>(smem, threads); break;
-            case 102: v = lean_occ<1, 2, false>(smem, threads); break;
-            case 104: v = lean_occ<1, 4, false>(smem, threads); break;
-            case 108: v = lean_occ<1, 8, false>(smem, threads); break;
-            case 201: v = lean_occ<2, 1, false>(smem, threads); break;
-            case 202: v = lean_occ<2, 2, false>(smem, threads); break;
-            case 204: v = lean_occ<2, 4, false>(smem, threads); break;
-            case 401: v = lean_occ<4, 1, false>(smem, threads); break;
-            case 402: v = lean_occ<4, 2, false>(smem, threads); break;
-            case 801: v = lean_occ<8, 1, false>(smem, threads); break;
+            case 101: v = lean_occ<1, 1, false>(smem); break;
+            case 102: v = lean_occ<1, 2, false>(smem); break;
+            case 104: v = lean_occ<1, 4, false>(smem); break;
+            case 108: v = lean_occ<1, 8, false>(smem); break;
+            case 201: v = lean_occ<2, 1, false>(smem); break;
+            case 202: v = lean_occ<2, 2, false>(smem); break;
+            case 204: v = lean_occ<2, 4, false>(smem); break;
+            case 401: v = lean_occ<4, 1, false>(smem); break;
+            case 402: v = lean_occ<4, 2, false>(smem); break;
+            case 801: v = lean_occ<8, 1, false>(smem); break;
             default: v = 0;
         }
     }
@@ -137,26 +139,29 @@ int oa_lean_ctas_per_sm(int R, int spb, size_t smem, bool qx, int threads) {
 
 cudaError_t oa_launch_snp_lean(int R, int spb, const LeanArgs& A, int grid, int threads, size_t smem,
                                cudaStream_t st) {
-    if (threads != 256 && threads != lean_max_threads(R)) return cudaErrorInvalidValue;
+    if (threads == LEAN_MAX_THREADS)
+        return R == 1 && spb == 1 && !A.Afull ? go_lean<1, 1, false, LEAN_MAX_THREADS>(A, grid, smem, st)
+                                              : cudaErrorInvalidValue;
+    if (threads != 256) return cudaErrorInvalidValue;
     if (A.Afull) {
         switch (R * 100 + spb) {
-            case 201: return go_lean<2, 1, true>(A, grid, threads, smem, st);
-            case 202: return go_lean<2, 2, true>(A, grid, threads, smem, st);
-            case 401: return go_lean<4, 1, true>(A, grid, threads, smem, st);
+            case 201: return go_lean<2, 1, true>(A, grid, smem, st);
+            case 202: return go_lean<2, 2, true>(A, grid, smem, st);
+            case 401: return go_lean<4, 1, true>(A, grid, smem, st);
             default: return cudaErrorInvalidValue;
         }
     }
     switch (R * 100 + spb) {
-        case 101: return go_lean<1, 1, false>(A, grid, threads, smem, st);
-        case 102: return go_lean<1, 2, false>(A, grid, threads, smem, st);
-        case 104: return go_lean<1, 4, false>(A, grid, threads, smem, st);
-        case 108: return go_lean<1, 8, false>(A, grid, threads, smem, st);
-        case 201: return go_lean<2, 1, false>(A, grid, threads, smem, st);
-        case 202: return go_lean<2, 2, false>(A, grid, threads, smem, st);
-        case 204: return go_lean<2, 4, false>(A, grid, threads, smem, st);
-        case 401: return go_lean<4, 1, false>(A, grid, threads, smem, st);
-        case 402: return go_lean<4, 2, false>(A, grid, threads, smem, st);
-        case 801: return go_lean<8, 1, false>(A, grid, threads, smem, st);
+        case 101: return go_lean<1, 1, false>(A, grid, smem, st);
+        case 102: return go_lean<1, 2, false>(A, grid, smem, st);
+        case 104: return go_lean<1, 4, false>(A, grid, smem, st);
+        case 108: return go_lean<1, 8, false>(A, grid, smem, st);
+        case 201: return go_lean<2, 1, false>(A, grid, smem, st);
+        case 202: return go_lean<2, 2, false>(A, grid, smem, st);
+        case 204: return go_lean<2, 4, false>(A, grid, smem, st);
+        case 401: return go_lean<4, 1, false>(A, grid, smem, st);
+        case 402: return go_lean<4, 2, false>(A, grid, smem, st);
+        case 801: return go_lean<8, 1, false>(A, grid, smem, st);
         default: return cudaErrorInvalidValue;
     }
 }
