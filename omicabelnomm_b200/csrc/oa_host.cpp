@@ -695,7 +695,11 @@ struct Writer {
         auto hold = std::make_shared<RowBatch>(std::move(B));
         pending = std::async(std::launch::async, [this, hold] {
             OA_TRACE("write outputs");
-            write_batch(*hold);
+            try {
+                write_batch(*hold);
+            } catch (...) {   // out of host memory for the formatted text: an output error, not a crash
+                write_failed = true;
+            }
         });
     }
     void finish() {
