@@ -10,6 +10,7 @@
 //   -> XR'Y~ GEMM with fused statistics epilogue -> (covariate terms)
 // Per API call: sort of the stored rows into reference order (trait, SNP).
 #include <algorithm>
+#include <chrono>
 #include <atomic>
 #include <cmath>
 #include <cstdarg>
@@ -1778,7 +1779,25 @@ const char* oa_last_error(void) { return g_err.c_str(); }
 void oa__set_error(const char* msg) { g_err = msg ? msg : ""; }
 int32_t oa_abi_version(void) { return OA_ABI_VERSION; }
 
+// OA_TIMING: entry points that take 20 ms or more report their host time on stderr (engine
+// sizes beside it), e.g. to see where a serving request's engine set-up spends its time.
+struct ApiClock {
+    const char* what;
+    const oa_engine* e;
+    std::chrono::steady_clock::time_point t0 = std::chrono::steady_clock::now();
+    ApiClock(const char* w, const oa_engine* eng) : what(w), e(eng) {}
+    ~ApiClock() {
+        static const bool on = getenv("OA_TIMING") != nullptr;
+        if (!on) return;
+        const double ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+        if (ms >= 20.0)
+            fprintf(stderr, "[oa timing] %s %.1f ms (n %d, traits %d, max SNPs %d)\n", what, ms, e ? e->n : 0,
+                    e ? e->cfg.max_traits : 0, e ? e->cfg.max_snps : 0);
+    }
+};
+
 oa_status oa_engine_create(const oa_config* cfg, oa_engine** out) {
+    ApiClock api_clock("oa_engine_create", nullptr);
     clear_stale_error(__func__);
     if (!cfg || !out) {
         set_err("null argument");
@@ -1805,10 +1824,26 @@ oa_status oa_engine_create(const oa_config* cfg, oa_engine** out) {
         return OA_ERR_ARG;
     }
     OA_CU(cudaSetDevice(cfg->device));
-    cudaDeviceProp prop;
-    OA_CU(cudaGetDeviceProperties(&prop, cfg->device));
-    if (prop.major < 10) {
-        set_err("device %s (sm_%d%d) is not a Blackwell sm_100 part", prop.name, prop.major, prop.minor);
+    // compute capability and SM count of the device, queried once per device: cudaGetDeviceProperties
+    // took up to 0.3 s while other engines kept the device busy (a serving request's engine set-up)
+    int cc_major = 0, cc_minor = 0, sm_count = 0;
+    {
+        static std::mutex mu;
+        static int have[64], c_major[64], c_minor[64], c_sms[64];
+        std::lock_guard<std::mutex> g(mu);
+        const int d = cfg->device & 63;
+        if (!have[d]) {
+            OA_CU(cudaDeviceGetAttribute(&c_major[d], cudaDevAttrComputeCapabilityMajor, cfg->device));
+            OA_CU(cudaDeviceGetAttribute(&c_minor[d], cudaDevAttrComputeCapabilityMinor, cfg->device));
+            OA_CU(cudaDeviceGetAttribute(&c_sms[d], cudaDevAttrMultiProcessorCount, cfg->device));
+            have[d] = 1;
+        }
+        cc_major = c_major[d];
+        cc_minor = c_minor[d];
+        sm_count = c_sms[d];
+    }
+    if (cc_major < 10) {
+        set_err("device %d (sm_%d%d) is not a Blackwell sm_100 part", cfg->device, cc_major, cc_minor);
         return OA_ERR_UNSUPPORTED;
     }
     {   // bound of the device pipeline and staging waits, per device: 2 s, or OA_WAIT_LIMIT_NS (the
@@ -1827,7 +1862,7 @@ oa_status oa_engine_create(const oa_config* cfg, oa_engine** out) {
     }
     oa_engine* e = new oa_engine();
     e->cfg = *cfg;
-    e->sm_count = prop.multiProcessorCount;
+    e->sm_count = sm_count;
     e->n = cfg->n;
     e->l = cfg->l;
     e->ru = cfg->r;
@@ -1900,6 +1935,7 @@ oa_status oa_engine_create(const oa_config* cfg, oa_engine** out) {
 }
 
 oa_status oa_engine_destroy(oa_engine* e) {
+    ApiClock api_clock("oa_engine_destroy", nullptr);   // e is freed before the clock reports
     if (!e) return OA_OK;
     cudaSetDevice(e->cfg.device);
     if (e->cp) cudaStreamSynchronize(e->cp);
@@ -1939,6 +1975,7 @@ oa_status oa_engine_destroy(oa_engine* e) {
 }
 
 oa_status oa_set_covariates(oa_engine* e, const float* xl) {
+    ApiClock api_clock("oa_set_covariates", e);
     clear_stale_error(__func__);
     OA_TRACE("oa_set_covariates: QR and rank check");
     if (!e || !xl) {
@@ -2021,6 +2058,7 @@ oa_status oa_set_traits(oa_engine* e, const float* y, int32_t t) {
 }
 
 oa_status oa_set_traits_device(oa_engine* e, const float* y, int32_t t) {
+    ApiClock api_clock("oa_set_traits_device", e);
     clear_stale_error(__func__);
     if (!e || !y) {
         set_err("null argument");
@@ -2036,6 +2074,7 @@ oa_status oa_run_snps(oa_engine* e, const float* xr, int32_t mb, oa_rows* out) {
 }
 
 oa_status oa_run_snps_device(oa_engine* e, const float* xr, int32_t mb, int32_t results_on_host, oa_rows* out) {
+    ApiClock api_clock("oa_run_snps_device", e);
     return run_snps_any(e, xr, mb, false, results_on_host != 0, out);
 }
 
@@ -2153,6 +2192,7 @@ oa_status oa_set_interactions(oa_engine* e, const float* inter, int32_t k, int32
 }
 
 oa_status oa_set_snp_rows(oa_engine* e, const int32_t* rows, int32_t n_rows, int64_t ld) {
+    ApiClock api_clock("oa_set_snp_rows", e);
     clear_stale_error(__func__);
     if (!e) {
         set_err("null engine");
@@ -2196,6 +2236,7 @@ int64_t oa_device_bytes(const oa_engine* e) {
 }
 
 oa_status oa_reserve(oa_engine* e, int32_t traits, int32_t snps) {
+    ApiClock api_clock("oa_reserve", e);
     clear_stale_error(__func__);
     if (!e) {
         set_err("null argument");
@@ -2225,6 +2266,7 @@ oa_status oa_reserve(oa_engine* e, int32_t traits, int32_t snps) {
         OA_CHECK(e->b0.ensure(t * l));
         OA_CHECK(stage_reserve(e, 48 * t + 65536 + 16 * n / LEAN_ITEM_ROWS));
     }
+    const auto t_traits = std::chrono::steady_clock::now();
     {
         // the smallest chunk the tuning picks by itself (narrow trait blocks give the most chunks)
         const int chunk = std::min(e->cfg.max_snps, e->req.chunk_snps > 0 ? e->req.chunk_snps : wave_chunk(e, 1));
@@ -2247,13 +2289,27 @@ oa_status oa_reserve(oa_engine* e, int32_t traits, int32_t snps) {
         OA_CU(cub::DeviceRadixSort::SortPairs(nullptr, tmp, e->keys.p, e->keys2.p, e->perm.p, e->perm2.p, (int)cap, 0,
                                               64, e->st));
         OA_CHECK(e->cub_tmp.ensure(tmp));
+        const auto t_dev = std::chrono::steady_clock::now();
         OA_CHECK(ensure_pinned(e->h_rec, e->h_rec_cap, R * rec_slots(e->r), e->retired_pinned));
         if (e->cfg.disp_cov) {
             OA_CHECK(e->cov2.ensure(R * l * 3));
             OA_CHECK(ensure_pinned(e->h_cov, e->h_cov_cap, R * l * 3, e->retired_pinned));
         }
+        const auto t_pin = std::chrono::steady_clock::now();
+        OA_CU(cudaStreamSynchronize(e->st));
+        if (getenv("OA_TIMING")) {
+            auto ms = [](std::chrono::steady_clock::time_point a, std::chrono::steady_clock::time_point b) {
+                return std::chrono::duration<double, std::milli>(b - a).count();
+            };
+            const auto t_end = std::chrono::steady_clock::now();
+            if (ms(api_clock.t0, t_end) >= 20.0)
+                fprintf(stderr,
+                        "[oa timing] oa_reserve: trait buffers %.1f ms, %zu row slots %.1f ms, page-locked rows "
+                        "(%zu bytes) %.1f ms, stream sync %.1f ms\n",
+                        ms(api_clock.t0, t_traits), cap, ms(t_traits, t_dev), (size_t)(R * rec_slots(e->r) * sizeof(Rec)),
+                        ms(t_dev, t_pin), ms(t_pin, t_end));
+        }
     }
-    OA_CU(cudaStreamSynchronize(e->st));
     return OA_OK;
 }
 
