@@ -1,7 +1,7 @@
-"""The CLI's output writer on the host (no GPU): its number formatting gives printf's characters, and
-its parallel formatting of stored rows gives the bytes of a plain sequential snprintf pass with the
-reference's row format and .dbin records (tests/writer_check.cpp, compiled here against the host
-source with the engine calls stubbed)."""
+"""The CLI's host path (no GPU): its number formatting gives printf's characters, its parallel
+formatting of stored rows gives the bytes of a plain sequential snprintf pass with the reference's
+row format and .dbin records, and its parallel genotype reader returns the file's values
+(tests/writer_check.cpp, compiled here against the host source with the engine calls stubbed)."""
 import os
 import shutil
 import subprocess

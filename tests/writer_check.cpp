@@ -9,6 +9,8 @@
 //      and interaction names (-v);
 //   3. the bytes do not depend on how many parts the rows are split into, and the files the
 //      background writer leaves (parallel positioned writes after a header) hold the same bytes.
+//   4. the genotype reader returns the file's values from parallel slices of float and double
+//      files, with and without excluded rows, and fails on a block past the end of the file.
 // The engine entry points the host file calls are stubbed: nothing here touches a device.
 #include "../omicabelnomm_b200/csrc/oa_host.cpp"
 
@@ -276,12 +278,68 @@ void writer_checks() {
     }
 }
 
+// The genotype reader: a block of columns read in parallel slices (reads of 64 MB or more) from
+// float and double files, all rows or the rows of an exclusion list, against the values written;
+// a block running past the end of the file is a failed read.
+void reader_checks() {
+    const size_t fileN = 1000, nvar = 17000;   // 17 million values: 68 MB as float, 136 MB as double
+    std::vector<double> vals(fileN * nvar);
+    for (size_t q = 0; q < vals.size(); ++q) vals[q] = (double)(q % 100003) * 0.001 - 7.0;
+    for (int dbl_file = 0; dbl_file < 2; ++dbl_file) {
+        char name[] = "/tmp/oa_reader_XXXXXX";
+        const int fd = mkstemp(name);
+        FILE* f = fdopen(fd, "w+b");
+        const size_t eb = dbl_file ? 8 : 4;
+        for (size_t q = 0; q < vals.size(); ++q) {
+            if (dbl_file) fwrite(&vals[q], 8, 1, f);
+            else {
+                const float x = (float)vals[q];
+                fwrite(&x, 4, 1, f);
+            }
+        }
+        fflush(f);
+        const Runs all{{0, (int)fileN}}, some{{0, 100}, {250, 500}, {990, 10}};
+        for (const Runs* runs : {&all, &some}) {
+            size_t kept = 0;
+            for (const auto& r : *runs) kept += (size_t)r.second;
+            const size_t v0 = 17, count = nvar - 17;
+            std::vector<float> dst(kept * count), scratch;
+            std::vector<double> dbl;
+            if (!read_columns(f, eb, fileN, v0, count, *runs, kept, dst.data(), scratch, dbl)) {
+                printf("reader: read of %zu columns failed (%s file)\n", count, dbl_file ? "double" : "float");
+                ++failures;
+                continue;
+            }
+            size_t bad = 0;
+            for (size_t c = 0; c < count; ++c) {
+                size_t pos = 0;
+                for (const auto& r : *runs)
+                    for (int k = 0; k < r.second; ++k, ++pos)
+                        bad += dst[c * kept + pos] != (float)vals[(v0 + c) * fileN + (size_t)(r.first + k)];
+            }
+            if (bad) {
+                printf("reader: %zu values differ (%s file, %zu kept rows)\n", bad, dbl_file ? "double" : "float", kept);
+                ++failures;
+            }
+        }
+        std::vector<float> dst(fileN * 2), scratch;
+        std::vector<double> dbl;
+        if (read_columns(f, eb, fileN, nvar - 1, 2, Runs{{0, (int)fileN}}, fileN, dst.data(), scratch, dbl)) {
+            printf("reader: a block past the end of the file was read\n");
+            ++failures;
+        }
+        fclose(f);
+        unlink(name);
+    }
+}
+
 }  // namespace
 
 int main(int argc, char** argv) {
     const long cases = argc > 1 ? atol(argv[1]) : 2000000;
     number_checks(cases);
     writer_checks();
+    reader_checks();
     printf("%s: %ld failures\n", failures ? "FAIL" : "ok", failures);
     return failures ? 1 : 0;
 }
